@@ -1,0 +1,11 @@
+"""B200-native implicit edge-based finite-volume hot path (Euler3D-compatible).
+
+The compute path is the CUDA library ``_lib/libcfd_b200.so`` (sm_100a), bound
+through its C ABI (``include/cfd_b200.h``).  Importing the package loads the
+library and fails loudly if it is missing.
+"""
+from . import _capi as capi  # noqa: F401  (loads the library)
+from .mesh import Mesh, box_mesh, from_cells, perturbed_freestream  # noqa: F401
+from .solver import Euler3DGPU, default_params  # noqa: F401
+
+__all__ = ["capi", "Mesh", "box_mesh", "from_cells", "perturbed_freestream", "Euler3DGPU", "default_params"]

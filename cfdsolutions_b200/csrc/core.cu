@@ -1,0 +1,1272 @@
+// Core of the B200 edge-based finite-volume path: context lifecycle, mesh
+// upload and device layout, boundary conditions, flux residual, local time
+// step, residual RMS, approximate Roe Jacobian assembly, level-scheduled block
+// Gauss-Seidel, solution update, and the C ABI around them.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "ctx.cuh"
+#include "kernels.cuh"
+
+namespace cfd {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+static inline unsigned long long dbits(double x) {
+    unsigned long long u;
+    std::memcpy(&u, &x, 8);
+    return u;
+}
+static inline double bitsd(unsigned long long u) {
+    double x;
+    std::memcpy(&x, &u, 8);
+    return x;
+}
+
+// ----------------------------------------------------------------- kernels
+
+// Characteristic ghost states, one thread per boundary edge
+// (Apply_Characteristic_Boundary_Condition, Euler3D/src/BC.cpp:1440-1487).
+__global__ void k_apply_bc(int nbedge, int64_t ldq, double *__restrict__ Q, const int2 *__restrict__ bn,
+                           const double4 *__restrict__ bg, const int *__restrict__ btype, Flow f,
+                           int *__restrict__ err) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nbedge) return;
+    int2 nd = bn[b];
+    double4 g = bg[b];
+    double qI[5], qG[5], qB[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        qI[k] = Q[k * ldq + nd.x];
+        qG[k] = Q[k * ldq + nd.y];
+    }
+    int st = characteristic_bc(qI, qG, g.x, g.y, g.z, btype[b], f, qB);
+    if (st) atomicOr(err, st == 1 ? ERR_BC_NEG_PRESSURE : ERR_BC_UNCLASSIFIED);
+#pragma unroll
+    for (int k = 0; k < 5; k++) Q[k * ldq + nd.y] = qB[k];
+}
+
+__device__ __forceinline__ void warp_minmax(double &mn, double &mx) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+}
+
+// Block-wide min/max of 3 (min,max) pairs folded into the global extrema
+// words with ordered-bit atomics (values are >= 0, so the IEEE bit pattern
+// orders like the value; min/max are order independent, hence deterministic).
+__device__ __forceinline__ void block_extrema3(double mn[3], double mx[3], unsigned long long *ext) {
+    __shared__ double s_mn[3][32], s_mx[3][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        warp_minmax(mn[j], mx[j]);
+        if (lane == 0) { s_mn[j][wid] = mn[j]; s_mx[j][wid] = mx[j]; }
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            double a = lane < nw ? s_mn[j][lane] : DBL_MAX;
+            double b = lane < nw ? s_mx[j][lane] : 0.0;
+            warp_minmax(a, b);
+            if (lane == 0) {
+                atomicMin(&ext[2 * j], (unsigned long long)__double_as_longlong(a));
+                atomicMax(&ext[2 * j + 1], (unsigned long long)__double_as_longlong(b));
+            }
+        }
+    }
+}
+
+// Second-order face state (Compute_SecondOrderReconstructQ,
+// Euler3D/src/HigherOrderReconstructQ.cpp:21-72) for the side `s` of an edge
+// towards `o`: q = Q_s + phi_s*(frac*(Q_o - Q_s) + (1-frac)*grad_s . r),
+// r = 0.5 (x_o - x_s).
+__device__ __forceinline__ void reconstruct(const double qs[5], const double qo[5], int s, double rx, double ry,
+                                            double rz, const double *__restrict__ grad, const double *__restrict__ phi,
+                                            int nnode, bool limited, double frac, double out[5]) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        const double gx = grad[(3 * k) * (int64_t)nnode + s];
+        const double gy = grad[(3 * k + 1) * (int64_t)nnode + s];
+        const double gz = grad[(3 * k + 2) * (int64_t)nnode + s];
+        const double ph = limited ? phi[k * (int64_t)nnode + s] : 1.0;
+        out[k] = qs[k] + ph * (frac * (qo[k] - qs[k]) + (1.0 - frac) * (gx * rx + gy * ry + gz * rz));
+    }
+}
+
+// Flux residual, node-gather form: one thread per node walks its incident
+// edges in a fixed order and accumulates +flux (node is node_L) or -flux
+// (node is node_R), so every node's sum has a deterministic order and no
+// atomics touch the residual.  The flux of edge (L,R) is always evaluated in
+// the reference's orientation (Q_L, Q_R, n_{L->R}), so both endpoints see
+// bit-identical values (Compute_Residual_Roe_New, FluxTest.cpp:7968-8100).
+template <int FLUX, bool SECOND>
+__global__ void __launch_bounds__(128) k_residual_gather(
+    int nnode, int64_t ldq, const double *__restrict__ Q, const int *__restrict__ n2e_ptr,
+    const int *__restrict__ n2e, const int2 *__restrict__ en, const double4 *__restrict__ eg,
+    const int *__restrict__ n2b_ptr, const int *__restrict__ n2b, const int2 *__restrict__ bn,
+    const double4 *__restrict__ bg, const double *__restrict__ xyz, const double *__restrict__ grad,
+    const double *__restrict__ phi, Flow f, int add_time, double *__restrict__ res,
+    double *__restrict__ resd, double *__restrict__ dtsum, unsigned long long *__restrict__ ext) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
+    if (i < nnode) {
+        double ac[5] = {0, 0, 0, 0, 0}, ad[5] = {0, 0, 0, 0, 0}, adt = 0.0;
+        const bool limited = f.limiter != CFD_LIMITER_NONE;
+        for (int k = n2e_ptr[i]; k < n2e_ptr[i + 1]; k++) {
+            const int s = n2e[k];
+            const int e = s >= 0 ? s : ~s;
+            const int2 nd = en[e];
+            const double4 g = eg[e];
+            double qL[5], qR[5];
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                qL[v] = Q[v * ldq + nd.x];
+                qR[v] = Q[v * ldq + nd.y];
+            }
+            if (SECOND) {
+                const double rx = 0.5 * (xyz[nd.y] - xyz[nd.x]);
+                const double ry = 0.5 * (xyz[nnode + nd.y] - xyz[nnode + nd.x]);
+                const double rz = 0.5 * (xyz[2 * nnode + nd.y] - xyz[2 * nnode + nd.x]);
+                double rL[5], rR[5];
+                reconstruct(qL, qR, nd.x, rx, ry, rz, grad, phi, nnode, limited, f.frac, rL);
+                reconstruct(qR, qL, nd.y, -rx, -ry, -rz, grad, phi, nnode, limited, f.frac, rR);
+#pragma unroll
+                for (int v = 0; v < 5; v++) { qL[v] = rL[v]; qR[v] = rR[v]; }
+            }
+            double cf[5], df[5], lam[3];
+            const double lmax = edge_flux<FLUX>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam);
+            const double sg = s >= 0 ? 1.0 : -1.0;
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                ac[v] += sg * cf[v];
+                ad[v] += sg * df[v];
+            }
+            adt += g.w * lmax;
+#pragma unroll
+            for (int j = 0; j < 3; j++) { mn[j] = fmin(mn[j], lam[j]); mx[j] = fmax(mx[j], lam[j]); }
+        }
+        // boundary edges: first order, flux into node_L only (FluxTest.cpp:8044-8098)
+        for (int k = n2b_ptr[i]; k < n2b_ptr[i + 1]; k++) {
+            const int b = n2b[k];
+            const int2 nd = bn[b];
+            const double4 g = bg[b];
+            double qL[5], qR[5];
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                qL[v] = Q[v * ldq + nd.x];
+                qR[v] = Q[v * ldq + nd.y];
+            }
+            double cf[5], df[5], lam[3];
+            const double lmax = edge_flux<FLUX>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam);
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                ac[v] += cf[v];
+                ad[v] += df[v];
+            }
+            adt += g.w * lmax;
+#pragma unroll
+            for (int j = 0; j < 3; j++) { mn[j] = fmin(mn[j], lam[j]); mx[j] = fmax(mx[j], lam[j]); }
+        }
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            res[v * (int64_t)nnode + i] = ac[v];
+            resd[v * (int64_t)nnode + i] = ad[v];
+        }
+        if (add_time) dtsum[i] = adt;
+    }
+    if (add_time) block_extrema3(mn, mx, ext);
+}
+
+// dt_i = V_i * CFL / sum_i (Compute_DeltaT, Euler3D/src/Time_Step.cpp:23-51).
+__global__ void k_deltat(int nnode, const double *__restrict__ vol, double cfl, double *__restrict__ dt,
+                         unsigned long long *__restrict__ ext) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
+    if (i < nnode) {
+        const double d = vol[i] * cfl / dt[i];
+        dt[i] = d;
+        mn[0] = d;
+        mx[0] = d;
+    }
+    __shared__ double s_mn[32], s_mx[32];
+    warp_minmax(mn[0], mx[0]);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0) { s_mn[wid] = mn[0]; s_mx[wid] = mx[0]; }
+    __syncthreads();
+    if (wid == 0) {
+        double a = lane < nw ? s_mn[lane] : DBL_MAX, b = lane < nw ? s_mx[lane] : 0.0;
+        warp_minmax(a, b);
+        if (lane == 0) {
+            atomicMin(&ext[6], (unsigned long long)__double_as_longlong(a));
+            atomicMax(&ext[7], (unsigned long long)__double_as_longlong(b));
+        }
+    }
+}
+
+__global__ void k_fill_global_dt(int nnode, const unsigned long long *__restrict__ ext, double *__restrict__ dt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nnode) dt[i] = __longlong_as_double((long long)ext[6]);
+}
+
+// Deterministic sum of squares of nvec strided vectors: stage 1 per block.
+__global__ void k_sumsq_partial(const double *__restrict__ x, int64_t n, int64_t stride, int nvec,
+                                double *__restrict__ part) {
+    extern __shared__ double sh[];
+    for (int v = 0; v < nvec; v++) {
+        double s = 0.0;
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+            const double a = x[v * stride + i];
+            s += a * a;
+        }
+        sh[threadIdx.x] = s;
+        __syncthreads();
+        for (int o = blockDim.x >> 1; o > 0; o >>= 1) {
+            if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) part[blockIdx.x * nvec + v] = sh[0];
+        __syncthreads();
+    }
+}
+
+__global__ void k_sum_final(const double *__restrict__ part, int nblk, int nvec, double *__restrict__ out) {
+    extern __shared__ double sh[];
+    for (int v = 0; v < nvec; v++) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += part[b * nvec + v];
+        sh[threadIdx.x] = s;
+        __syncthreads();
+        for (int o = blockDim.x >> 1; o > 0; o >>= 1) {
+            if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[v] = sh[0];
+        __syncthreads();
+    }
+}
+
+__global__ void k_add_diss(int64_t n, const double *__restrict__ a, const double *__restrict__ b,
+                           double *__restrict__ o) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) o[i] = a[i] + b[i];
+}
+
+// ---- approximate Roe Jacobian (Compute_Jacobian_Approximate_Roe,
+//      Euler3D/src/Roe_Jacobian.cpp:29-228)
+
+// Off-diagonal blocks, one thread per interior edge:
+//   A[L,R] = dFdR = 0.5 (J(Q_R) - |A|) area,  A[R,L] = -dFdL = -0.5 (J(Q_L) + |A|) area.
+// Every off-diagonal slot belongs to exactly one edge, so no zeroing and no
+// accumulation is needed.
+template <typename TA>
+__global__ void __launch_bounds__(128) k_jac_edges(int nedge, int64_t ldq, const double *__restrict__ Q,
+                                                   const int2 *__restrict__ en, const double4 *__restrict__ eg,
+                                                   const int2 *__restrict__ eslot, Flow f, double *__restrict__ A64,
+                                                   TA *__restrict__ Alow) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nedge) return;
+    const int2 nd = en[e];
+    const double4 g = eg[e];
+    double qL[5], qR[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        qL[v] = Q[v * ldq + nd.x];
+        qR[v] = Q[v * ldq + nd.y];
+    }
+    double Ab[25], J[25];
+    roe_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
+    const int2 sl = eslot[e];
+    const double ha = 0.5 * g.w;
+    euler_flux_jacobian(qR, g.x, g.y, g.z, f.gamma, J);
+#pragma unroll
+    for (int k = 0; k < 25; k++) {
+        const double val = ha * (J[k] - Ab[k]);
+        A64[(int64_t)sl.x * 25 + k] = val;
+        if (Alow) store_low(Alow + (int64_t)sl.x * 25 + k, val);
+    }
+    euler_flux_jacobian(qL, g.x, g.y, g.z, f.gamma, J);
+#pragma unroll
+    for (int k = 0; k < 25; k++) {
+        const double val = -ha * (J[k] + Ab[k]);
+        A64[(int64_t)sl.y * 25 + k] = val;
+        if (Alow) store_low(Alow + (int64_t)sl.y * 25 + k, val);
+    }
+}
+
+// Diagonal blocks and right-hand side, one thread per row:
+//   A[i,i] = V_i/dt_i I - sum_j A[j,i] + sum_b 0.5 (J(Q_i) + |A|)_b area_b
+//   B_i    = -(Res_i [+ Res_Diss_i])
+template <typename TA>
+__global__ void __launch_bounds__(128) k_jac_rows(
+    int nnode, int64_t ldq, const double *__restrict__ Q, const int *__restrict__ IA, const int *__restrict__ IAU,
+    const int *__restrict__ tslot, const int *__restrict__ n2b_ptr, const int *__restrict__ n2b,
+    const int2 *__restrict__ bn, const double4 *__restrict__ bg, const double *__restrict__ vol,
+    const double *__restrict__ dt, const double *__restrict__ res, const double *__restrict__ resd,
+    int add_time, int include_diss, Flow f, double *__restrict__ A64, TA *__restrict__ Alow,
+    double *__restrict__ B) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nnode) return;
+    double D[25];
+    const double vd = add_time ? vol[i] / dt[i] : 0.0;
+#pragma unroll
+    for (int k = 0; k < 25; k++) D[k] = (k % 6 == 0) ? vd : 0.0;
+    const int dg = IAU[i];
+    for (int k = IA[i]; k < IA[i + 1]; k++) {
+        if (k == dg) continue;
+        const double *blk = A64 + (int64_t)tslot[k] * 25;
+#pragma unroll
+        for (int m = 0; m < 25; m++) D[m] -= blk[m];
+    }
+    for (int k = n2b_ptr[i]; k < n2b_ptr[i + 1]; k++) {
+        const int b = n2b[k];
+        const int2 nd = bn[b];
+        const double4 g = bg[b];
+        double qL[5], qR[5], Ab[25], J[25];
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            qL[v] = Q[v * ldq + nd.x];
+            qR[v] = Q[v * ldq + nd.y];
+        }
+        roe_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
+        euler_flux_jacobian(qL, g.x, g.y, g.z, f.gamma, J);
+        const double ha = 0.5 * g.w;
+#pragma unroll
+        for (int m = 0; m < 25; m++) D[m] += ha * (J[m] + Ab[m]);
+    }
+#pragma unroll
+    for (int m = 0; m < 25; m++) {
+        A64[(int64_t)dg * 25 + m] = D[m];
+        if (Alow) store_low(Alow + (int64_t)dg * 25 + m, D[m]);
+    }
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        double r = res[v * (int64_t)nnode + i];
+        if (include_diss) r += resd[v * (int64_t)nnode + i];
+        B[(int64_t)i * 5 + v] = -r;
+    }
+}
+
+// ---- block Gauss-Seidel (MC_Iterative_Block_LU_Jacobi_CRS,
+//      MATH/src/MC_Iterative_Jacobi.c:346-535), level scheduled.
+// All arithmetic uses explicitly rounded intrinsics so no multiply-add is
+// fused: the row updates then round exactly like the reference's scalar
+// loops, and with identical A, B the iterates agree bit for bit.
+
+__global__ void k_lu_nopivot(int nnode, const double *__restrict__ A, const int *__restrict__ IAU,
+                             double *__restrict__ LU) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nnode) return;
+    double a[25];
+    const double *src = A + (int64_t)IAU[r] * 25;
+#pragma unroll
+    for (int k = 0; k < 25; k++) a[k] = src[k];
+    // MC_Iterative_Jacobi.c:383-394
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+#pragma unroll
+        for (int j = k + 1; j < 5; j++) a[j * 5 + k] = __ddiv_rn(a[j * 5 + k], a[k * 5 + k]);
+#pragma unroll
+        for (int j = k + 1; j < 5; j++)
+#pragma unroll
+            for (int i = k + 1; i < 5; i++) a[i * 5 + j] = __dsub_rn(a[i * 5 + j], __dmul_rn(a[i * 5 + k], a[k * 5 + j]));
+    }
+    double *dst = LU + (int64_t)r * 25;
+#pragma unroll
+    for (int k = 0; k < 25; k++) dst[k] = a[k];
+}
+
+__global__ void __launch_bounds__(128) k_gs_level(int nrows, const int *__restrict__ rows, const int *__restrict__ IA,
+                                                  const int *__restrict__ JA, const int *__restrict__ IAU,
+                                                  const double *__restrict__ A, const double *__restrict__ B,
+                                                  const double *__restrict__ LU, double *__restrict__ X,
+                                                  double *__restrict__ rowrms) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nrows) return;
+    const int r = rows[t];
+    double rhs[5];
+#pragma unroll
+    for (int m = 0; m < 5; m++) rhs[m] = B[(int64_t)r * 5 + m];
+    for (int k = IA[r]; k < IA[r + 1]; k++) {
+        const double *a = A + (int64_t)k * 25;
+        const double *x = X + (int64_t)JA[k] * 5;
+        double xv[5];
+#pragma unroll
+        for (int m = 0; m < 5; m++) xv[m] = x[m];
+#pragma unroll
+        for (int ii = 0; ii < 5; ii++) {
+            double tv = 0.0;
+#pragma unroll
+            for (int jj = 0; jj < 5; jj++) tv = __dadd_rn(tv, __dmul_rn(a[ii * 5 + jj], xv[jj]));
+            rhs[ii] = __dsub_rn(rhs[ii], tv);
+        }
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int m = 0; m < 5; m++) s = __dadd_rn(s, __dmul_rn(rhs[m], rhs[m]));
+    rowrms[r] = s;
+    {
+        const double *a = A + (int64_t)IAU[r] * 25;
+        const double *x = X + (int64_t)r * 5;
+#pragma unroll
+        for (int ii = 0; ii < 5; ii++) {
+            double tv = 0.0;
+#pragma unroll
+            for (int jj = 0; jj < 5; jj++) tv = __dadd_rn(tv, __dmul_rn(a[ii * 5 + jj], x[jj]));
+            rhs[ii] = __dadd_rn(rhs[ii], tv);
+        }
+    }
+    const double *lu = LU + (int64_t)r * 25;
+    double tv[5];
+#pragma unroll
+    for (int ii = 0; ii < 5; ii++) {
+        tv[ii] = rhs[ii];
+#pragma unroll
+        for (int jj = 0; jj < ii; jj++) tv[ii] = __dsub_rn(tv[ii], __dmul_rn(lu[ii * 5 + jj], tv[jj]));
+    }
+    double xo[5];
+#pragma unroll
+    for (int ii = 4; ii >= 0; ii--) {
+        double v = tv[ii];
+#pragma unroll
+        for (int jj = 4; jj > ii; jj--) v = __dsub_rn(v, __dmul_rn(lu[ii * 5 + jj], xo[jj]));
+        xo[ii] = __ddiv_rn(v, lu[ii * 5 + ii]);
+    }
+#pragma unroll
+    for (int m = 0; m < 5; m++) X[(int64_t)r * 5 + m] = xo[m];
+}
+
+__global__ void k_update(int nnode, int64_t ldq, double relax, const double *__restrict__ X, double *__restrict__ Q) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nnode) return;
+#pragma unroll
+    for (int v = 0; v < 5; v++) Q[v * ldq + i] += relax * X[(int64_t)i * 5 + v];
+}
+
+__global__ void k_freestream(int n, int64_t ldq, Flow f, double *__restrict__ Q) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Q[i] = f.inf_rho;
+    Q[ldq + i] = f.inf_rho * f.inf_u;
+    Q[2 * ldq + i] = f.inf_rho * f.inf_v;
+    Q[3 * ldq + i] = f.inf_rho * f.inf_w;
+    Q[4 * ldq + i] = f.inf_rho * f.inf_et;
+}
+
+// ------------------------------------------------------------- host helpers
+
+int reduce_sum_sq(cfd_ctx *c, const double *x, int64_t n, int64_t stride, int nvec, double *out_host) {
+    const int nblk = 296, bs = 256;
+    CFD_CUDA(c->red.alloc((size_t)nblk * 16));
+    CFD_CUDA(c->red_out.alloc(16));
+    k_sumsq_partial<<<nblk, bs, bs * sizeof(double), c->stream>>>(x, n, stride, nvec, c->red.p);
+    CFD_LAUNCH_CHECK();
+    k_sum_final<<<1, bs, bs * sizeof(double), c->stream>>>(c->red.p, nblk, nvec, c->red_out.p);
+    CFD_LAUNCH_CHECK();
+    CFD_CUDA(cudaMemcpyAsync(out_host, c->red_out.p, nvec * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    return CFD_OK;
+}
+
+int check_device_error(cfd_ctx *c) {
+    int h = 0;
+    CFD_CUDA(cudaMemcpyAsync(&h, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    if (h) {
+        CFD_CUDA(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
+        set_error("device reported numerical failure (flags 0x%x)", h);
+        return CFD_ERR_NUMERIC;
+    }
+    return CFD_OK;
+}
+
+// Far-field state with Mach ramping (ComputeFarFieldCondition,
+// Euler3D/src/Material.cpp:185-210) under the generic non-dimensionalisation
+// (Material.cpp:119-124: R = 1/gamma, rho = 1, T = gamma, p = 1).
+static void compute_flow(cfd_ctx *c, int iteration) {
+    const cfd_params &p = c->params;
+    Flow &f = c->flow;
+    f.gamma = p.gamma;
+    f.gm1 = p.gamma - 1.0;
+    double mach;
+    if (p.mach_ramp > 1 && p.mach > p.mach_min) {
+        mach = iteration < p.mach_ramp
+                   ? p.mach_min + (p.mach - p.mach_min) * ((double)iteration / (double)(p.mach_ramp - 1))
+                   : p.mach;
+    } else {
+        mach = p.mach;
+    }
+    const double R = 1.0 / p.gamma, rho = 1.0, T = p.gamma, pr = R * rho * T;
+    const double alpha = p.alpha_deg * M_PI / 180.0, beta = p.beta_deg * M_PI / 180.0;
+    f.inf_mach = mach;
+    f.inf_rho = rho;
+    f.inf_p = pr;
+    f.inf_c = sqrt(p.gamma * R * T);
+    f.inf_u = mach * f.inf_c * cos(alpha) * cos(beta);
+    f.inf_v = mach * f.inf_c * sin(alpha);
+    f.inf_w = mach * f.inf_c * sin(beta) * cos(alpha);
+    f.inf_et = pr / ((p.gamma - 1.0) * rho) + 0.5 * (f.inf_u * f.inf_u + f.inf_v * f.inf_v + f.inf_w * f.inf_w);
+    f.outflow_p = 0.935 * pr;  // Material.cpp:171
+    f.frac = p.limiter_order == 1 ? 0.5 : 0.0;
+    f.venkat_eps_k3 = pow(p.venkat_k, 3.0);
+    f.flux = p.flux_scheme;
+    f.order = p.order;
+    f.limiter = p.limiter;
+    f.limiter_smooth = p.limiter_smooth;
+    f.entropy_fix = p.entropy_fix;
+    f.zpg_iteration = p.zpg_iteration;
+    f.iteration = iteration;
+    // CFL ramp (Time_Step.cpp:27-34)
+    if (p.cfl_ramp > 1 && p.cfl_max > p.cfl_min)
+        c->cfl = iteration < p.cfl_ramp
+                     ? p.cfl_min + (p.cfl_max - p.cfl_min) * ((double)iteration / (double)(p.cfl_ramp - 1))
+                     : p.cfl_max;
+    else
+        c->cfl = p.cfl_max;
+}
+
+template <int FLUX, bool SECOND>
+static void launch_residual(cfd_ctx *c, int add_time) {
+    k_residual_gather<FLUX, SECOND><<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(
+        c->nnode, c->ldq, c->Q.p, c->n2e_ptr.p, c->n2e.p, c->edge_nodes.p, c->edge_geo.p, c->n2b_ptr.p, c->n2b.p,
+        c->bedge_nodes.p, c->bedge_geo.p, c->xyz.p, c->grad.p, c->phi.p, c->flow, add_time, c->res.p, c->resd.p,
+        c->dt.p, c->ext.p);
+}
+
+static Levels *build_levels(const std::vector<int> &IA, const std::vector<int> &JA, int n, bool forward,
+                            Levels &L, cudaStream_t s, int &err) {
+    std::vector<int> lev(n, 0);
+    int maxl = 0;
+    if (forward) {
+        for (int i = 0; i < n; i++) {
+            int l = 0;
+            for (int k = IA[i]; k < IA[i + 1]; k++)
+                if (JA[k] < i) l = std::max(l, lev[JA[k]] + 1);
+            lev[i] = l;
+            maxl = std::max(maxl, l);
+        }
+    } else {
+        for (int i = n - 1; i >= 0; i--) {
+            int l = 0;
+            for (int k = IA[i]; k < IA[i + 1]; k++)
+                if (JA[k] > i) l = std::max(l, lev[JA[k]] + 1);
+            lev[i] = l;
+            maxl = std::max(maxl, l);
+        }
+    }
+    const int nl = n ? maxl + 1 : 0;
+    L.ptr.assign(nl + 1, 0);
+    for (int i = 0; i < n; i++) L.ptr[lev[i] + 1]++;
+    for (int l = 0; l < nl; l++) L.ptr[l + 1] += L.ptr[l];
+    std::vector<int> rows(n), fill(L.ptr.begin(), L.ptr.end() - 1);
+    // rows of a level keep ascending order (coalesced loads)
+    for (int i = 0; i < n; i++) rows[fill[lev[i]]++] = i;
+    L.max_width = 0;
+    for (int l = 0; l < nl; l++) L.max_width = std::max(L.max_width, L.ptr[l + 1] - L.ptr[l]);
+    err = L.rows.upload(rows.data(), rows.size(), s) == cudaSuccess ? 0 : 1;
+    return &L;
+}
+
+}  // namespace cfd
+
+using namespace cfd;
+
+// ====================================================================== C ABI
+extern "C" {
+
+int cfd_abi_version(void) { return CFD_ABI_VERSION; }
+const char *cfd_last_error(void) { return cfd::g_err; }
+
+void cfd_params_default(cfd_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->flux_scheme = CFD_FLUX_ROE;
+    p->order = CFD_ORDER_FIRST;
+    p->limiter = CFD_LIMITER_NONE;
+    p->limiter_order = 0;
+    p->limiter_smooth = 0;
+    p->gradient = CFD_GRAD_LSQ;
+    p->ls_weight = 0;
+    p->entropy_fix = 0;
+    p->global_time = 0;
+    p->cfl_ramp = 0;
+    p->mach_ramp = 0;
+    p->zpg_iteration = 0;
+    p->gamma = 1.4;
+    p->mach = 0.5;
+    p->mach_min = 0.5;
+    p->alpha_deg = 2.0;
+    p->beta_deg = 0.0;
+    p->cfl_min = 10.0;
+    p->cfl_max = 10.0;
+    p->venkat_k = 5.0;
+}
+
+int cfd_create(int device, cfd_ctx **out) {
+    if (!out) { set_error("cfd_create: out is NULL"); return CFD_ERR_ARG; }
+    *out = nullptr;
+    int ndev = 0;
+    CFD_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) { set_error("cfd_create: device %d of %d", device, ndev); return CFD_ERR_ARG; }
+    CFD_CUDA(cudaSetDevice(device));
+    cfd_ctx *c = new cfd_ctx();
+    c->device = device;
+    cfd_params_default(&c->params);
+    if (c->err.alloc(1) != cudaSuccess || c->ext.alloc(8) != cudaSuccess) {
+        delete c;
+        set_error("cfd_create: device allocation failed");
+        return CFD_ERR_CUDA;
+    }
+    cudaMemset(c->err.p, 0, sizeof(int));
+    compute_flow(c, 0);
+    *out = c;
+    return CFD_OK;
+}
+
+int cfd_destroy(cfd_ctx *c) {
+    if (!c) return CFD_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    delete c;
+    return CFD_OK;
+}
+
+int cfd_set_stream(cfd_ctx *c, void *stream) {
+    if (!c) return CFD_ERR_ARG;
+    c->stream = (cudaStream_t)stream;
+    return CFD_OK;
+}
+
+int cfd_set_params(cfd_ctx *c, const cfd_params *p) {
+    if (!c || !p) { set_error("cfd_set_params: NULL"); return CFD_ERR_ARG; }
+    if (p->flux_scheme < CFD_FLUX_ROE || p->flux_scheme > CFD_FLUX_AUSM) {
+        set_error("cfd_set_params: invalid flux scheme %d", p->flux_scheme);
+        return CFD_ERR_ARG;
+    }
+    if (!(p->gamma > 1.0)) { set_error("cfd_set_params: gamma must be > 1"); return CFD_ERR_ARG; }
+    if (p->order != CFD_ORDER_FIRST && p->order != CFD_ORDER_SECOND) {
+        set_error("cfd_set_params: invalid order %d", p->order);
+        return CFD_ERR_ARG;
+    }
+    c->params = *p;
+    compute_flow(c, 0);
+    return CFD_OK;
+}
+
+int cfd_synchronize(cfd_ctx *c) {
+    if (!c) return CFD_ERR_ARG;
+    CFD_CUDA(cudaSetDevice(c->device));
+    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    return CFD_OK;
+}
+
+int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_nodes, const double *edge_areav,
+                 int nbedge, const int *bedge_nodes, const double *bedge_areav, const int *bedge_type,
+                 const double *cvol, const double *coords, const int *n2n_ia, const int *n2n_ja) {
+    if (!c) return CFD_ERR_ARG;
+    if (nnode <= 0 || nghost < 0 || nedge < 0 || nbedge < 0 || (nedge && (!edge_nodes || !edge_areav)) ||
+        (nbedge && (!bedge_nodes || !bedge_areav || !bedge_type)) || !cvol || !coords || !n2n_ia || !n2n_ja) {
+        set_error("cfd_set_mesh: invalid sizes or NULL arrays");
+        return CFD_ERR_ARG;
+    }
+    CFD_CUDA(cudaSetDevice(c->device));
+    // ---- validation (host): the device kernels index with these values
+    for (int e = 0; e < nedge; e++) {
+        const int a = edge_nodes[2 * e], b = edge_nodes[2 * e + 1];
+        if (a < 0 || b >= nnode || a >= b) {
+            set_error("cfd_set_mesh: interior edge %d has nodes (%d,%d); need 0 <= L < R < nNode", e, a, b);
+            return CFD_ERR_MESH;
+        }
+    }
+    std::vector<char> ghost_used(nghost, 0);
+    for (int e = 0; e < nbedge; e++) {
+        const int a = bedge_nodes[2 * e], g = bedge_nodes[2 * e + 1];
+        if (a < 0 || a >= nnode || g < nnode || g >= nnode + nghost || ghost_used[g - nnode]) {
+            set_error("cfd_set_mesh: boundary edge %d has nodes (%d,%d)", e, a, g);
+            return CFD_ERR_MESH;
+        }
+        ghost_used[g - nnode] = 1;
+        if (bedge_type[e] < 0 || bedge_type[e] > 7) {
+            set_error("cfd_set_mesh: boundary edge %d has unsupported BC type %d", e, bedge_type[e]);
+            return CFD_ERR_UNSUPPORTED;
+        }
+    }
+    if (n2n_ia[0] != 0) { set_error("cfd_set_mesh: n2n_ia[0] != 0"); return CFD_ERR_MESH; }
+    for (int i = 0; i < nnode; i++) {
+        if (n2n_ia[i + 1] < n2n_ia[i]) { set_error("cfd_set_mesh: n2n_ia not monotone"); return CFD_ERR_MESH; }
+        for (int k = n2n_ia[i]; k < n2n_ia[i + 1]; k++)
+            if (n2n_ja[k] < 0 || n2n_ja[k] >= nnode || n2n_ja[k] == i) {
+                set_error("cfd_set_mesh: n2n_ja entry %d of row %d out of range", k, i);
+                return CFD_ERR_MESH;
+            }
+    }
+    if ((int64_t)n2n_ia[nnode] != 2 * (int64_t)nedge) {
+        set_error("cfd_set_mesh: node graph has %d entries, expected 2*nEdge=%lld", n2n_ia[nnode], 2LL * nedge);
+        return CFD_ERR_MESH;
+    }
+    for (int i = 0; i < nnode; i++)
+        if (!(cvol[i] > 0.0)) { set_error("cfd_set_mesh: cVolume[%d] = %g", i, cvol[i]); return CFD_ERR_MESH; }
+
+    cudaStream_t s = c->stream;
+    c->has_mesh = false;
+    c->has_system = false;
+    c->has_grad = false;
+    c->nnode = nnode;
+    c->nghost = nghost;
+    c->nedge = nedge;
+    c->nbedge = nbedge;
+    c->ldq = ((int64_t)nnode + nghost + 31) / 32 * 32;
+
+    // ---- edges: unit normal + magnitude (Vector3D::normalize/magnitude, MATH/src/Vector3D.cpp:216-229)
+    auto geo = [](const double *a, double4 &g, double4 &sv) {
+        const double mag = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+        double nx = a[0], ny = a[1], nz = a[2];
+        if (mag > 1.0e-20) { nx = a[0] / mag; ny = a[1] / mag; nz = a[2] / mag; }
+        g = make_double4(nx, ny, nz, mag);
+        sv = make_double4(a[0], a[1], a[2], 0.0);
+    };
+    {
+        std::vector<int2> en(nedge);
+        std::vector<double4> eg(nedge), es(nedge);
+        for (int e = 0; e < nedge; e++) {
+            en[e] = make_int2(edge_nodes[2 * e], edge_nodes[2 * e + 1]);
+            geo(edge_areav + 3 * (size_t)e, eg[e], es[e]);
+        }
+        std::vector<int2> bnv(nbedge);
+        std::vector<double4> bgv(nbedge), bsv(nbedge);
+        for (int e = 0; e < nbedge; e++) {
+            bnv[e] = make_int2(bedge_nodes[2 * e], bedge_nodes[2 * e + 1]);
+            geo(bedge_areav + 3 * (size_t)e, bgv[e], bsv[e]);
+        }
+        CFD_CUDA(c->edge_nodes.upload(en.data(), nedge, s));
+        CFD_CUDA(c->edge_geo.upload(eg.data(), nedge, s));
+        CFD_CUDA(c->edge_sv.upload(es.data(), nedge, s));
+        CFD_CUDA(c->bedge_nodes.upload(bnv.data(), nbedge, s));
+        CFD_CUDA(c->bedge_geo.upload(bgv.data(), nbedge, s));
+        CFD_CUDA(c->bedge_sv.upload(bsv.data(), nbedge, s));
+        CFD_CUDA(c->bedge_type.upload(bedge_type, nbedge, s));
+        CFD_CUDA(cudaStreamSynchronize(s));
+    }
+    CFD_CUDA(c->cvol.upload(cvol, nnode, s));
+    {
+        std::vector<double> x(3 * (size_t)nnode);
+        for (int i = 0; i < nnode; i++)
+            for (int d = 0; d < 3; d++) x[(size_t)d * nnode + i] = coords[3 * (size_t)i + d];
+        CFD_CUDA(c->xyz.upload(x.data(), x.size(), s));
+        CFD_CUDA(cudaStreamSynchronize(s));
+    }
+    // physical graph, rows sorted (the reference's list order is insertion order;
+    // gradients and limiters are order-insensitive to round-off)
+    std::vector<int> gia(n2n_ia, n2n_ia + nnode + 1), gja(n2n_ja, n2n_ja + n2n_ia[nnode]);
+    for (int i = 0; i < nnode; i++) std::sort(gja.begin() + gia[i], gja.begin() + gia[i + 1]);
+    CFD_CUDA(c->n2n_ia.upload(gia.data(), gia.size(), s));
+    CFD_CUDA(c->n2n_ja.upload(gja.data(), gja.size(), s));
+
+    // ---- node -> incident interior edges, ordered by neighbour id
+    {
+        std::vector<int> ptr(nnode + 1, 0);
+        for (int e = 0; e < nedge; e++) { ptr[edge_nodes[2 * e] + 1]++; ptr[edge_nodes[2 * e + 1] + 1]++; }
+        for (int i = 0; i < nnode; i++) ptr[i + 1] += ptr[i];
+        std::vector<int> lst(ptr[nnode]), fill(ptr.begin(), ptr.end() - 1), nb(ptr[nnode]);
+        for (int e = 0; e < nedge; e++) {
+            const int a = edge_nodes[2 * e], b = edge_nodes[2 * e + 1];
+            nb[fill[a]] = b; lst[fill[a]++] = e;
+            nb[fill[b]] = a; lst[fill[b]++] = ~e;
+        }
+        std::vector<int> idx;
+        for (int i = 0; i < nnode; i++) {
+            const int lo = ptr[i], hi = ptr[i + 1];
+            idx.resize(hi - lo);
+            std::iota(idx.begin(), idx.end(), lo);
+            std::sort(idx.begin(), idx.end(), [&](int x, int y) { return nb[x] < nb[y]; });
+            std::vector<int> tmp(hi - lo);
+            for (int k = 0; k < hi - lo; k++) tmp[k] = lst[idx[k]];
+            std::copy(tmp.begin(), tmp.end(), lst.begin() + lo);
+        }
+        CFD_CUDA(c->n2e_ptr.upload(ptr.data(), ptr.size(), s));
+        CFD_CUDA(c->n2e.upload(lst.data(), lst.size(), s));
+        CFD_CUDA(cudaStreamSynchronize(s));
+    }
+    {
+        std::vector<int> ptr(nnode + 1, 0);
+        for (int e = 0; e < nbedge; e++) ptr[bedge_nodes[2 * e] + 1]++;
+        for (int i = 0; i < nnode; i++) ptr[i + 1] += ptr[i];
+        std::vector<int> lst(std::max(ptr[nnode], 1)), fill(ptr.begin(), ptr.end() - 1);
+        for (int e = 0; e < nbedge; e++) lst[fill[bedge_nodes[2 * e]]++] = e;
+        CFD_CUDA(c->n2b_ptr.upload(ptr.data(), ptr.size(), s));
+        CFD_CUDA(c->n2b.upload(lst.data(), lst.size(), s));
+        CFD_CUDA(cudaStreamSynchronize(s));
+    }
+    // ---- block CRS pattern (Create_CRS_SolverBlockMatrix, Euler3D/src/Solver.cpp:612-672)
+    {
+        c->h_IA.assign(nnode + 1, 0);
+        for (int i = 0; i < nnode; i++) c->h_IA[i + 1] = c->h_IA[i] + (gia[i + 1] - gia[i]) + 1;
+        c->nnzb = c->h_IA[nnode];
+        c->h_JA.assign(c->nnzb, 0);
+        c->h_IAU.assign(nnode, 0);
+        for (int i = 0; i < nnode; i++) {
+            int k = c->h_IA[i];
+            bool placed = false;
+            for (int m = gia[i]; m < gia[i + 1]; m++) {
+                if (!placed && gja[m] > i) { c->h_IAU[i] = k; c->h_JA[k++] = i; placed = true; }
+                c->h_JA[k++] = gja[m];
+            }
+            if (!placed) { c->h_IAU[i] = k; c->h_JA[k++] = i; }
+        }
+        auto slot = [&](int r, int col) {
+            auto b = c->h_JA.begin() + c->h_IA[r], e = c->h_JA.begin() + c->h_IA[r + 1];
+            auto it = std::lower_bound(b, e, col);
+            return (int)(it - c->h_JA.begin());
+        };
+        std::vector<int> ts(c->nnzb);
+        for (int i = 0; i < nnode; i++)
+            for (int k = c->h_IA[i]; k < c->h_IA[i + 1]; k++) ts[k] = slot(c->h_JA[k], i);
+        std::vector<int2> es(nedge);
+        for (int e = 0; e < nedge; e++) {
+            const int a = edge_nodes[2 * e], b = edge_nodes[2 * e + 1];
+            es[e] = make_int2(slot(a, b), slot(b, a));
+        }
+        CFD_CUDA(c->IA.upload(c->h_IA.data(), c->h_IA.size(), s));
+        CFD_CUDA(c->JA.upload(c->h_JA.data(), c->h_JA.size(), s));
+        CFD_CUDA(c->IAU.upload(c->h_IAU.data(), c->h_IAU.size(), s));
+        CFD_CUDA(c->tslot.upload(ts.data(), ts.size(), s));
+        CFD_CUDA(c->eslot.upload(es.data(), es.size(), s));
+        int e1 = 0, e2 = 0;
+        build_levels(c->h_IA, c->h_JA, nnode, true, c->lv_fwd, s, e1);
+        build_levels(c->h_IA, c->h_JA, nnode, false, c->lv_bwd, s, e2);
+        if (e1 || e2) { set_error("cfd_set_mesh: level upload failed"); return CFD_ERR_CUDA; }
+        CFD_CUDA(cudaStreamSynchronize(s));
+    }
+    // ---- state and work arrays
+    CFD_CUDA(c->Q.alloc((size_t)5 * c->ldq));
+    CFD_CUDA(c->res.alloc((size_t)5 * nnode));
+    CFD_CUDA(c->resd.alloc((size_t)5 * nnode));
+    CFD_CUDA(c->dt.alloc(nnode));
+    CFD_CUDA(cudaMemsetAsync(c->Q.p, 0, sizeof(double) * 5 * c->ldq, s));
+    CFD_CUDA(cudaMemsetAsync(c->res.p, 0, sizeof(double) * 5 * nnode, s));
+    CFD_CUDA(cudaMemsetAsync(c->resd.p, 0, sizeof(double) * 5 * nnode, s));
+    CFD_CUDA(cudaMemsetAsync(c->dt.p, 0, sizeof(double) * nnode, s));
+    CFD_CUDA(cudaStreamSynchronize(s));
+    c->has_mesh = true;
+    return cfd_set_freestream(c);
+}
+
+int cfd_get_block_pattern(cfd_ctx *c, int64_t *nnzb, int *IA, int *JA, int *IAU) {
+    if (!c || !c->has_mesh) { set_error("cfd_get_block_pattern: no mesh"); return CFD_ERR_STATE; }
+    if (nnzb) *nnzb = c->nnzb;
+    if (IA) std::memcpy(IA, c->h_IA.data(), sizeof(int) * c->h_IA.size());
+    if (JA) std::memcpy(JA, c->h_JA.data(), sizeof(int) * c->h_JA.size());
+    if (IAU) std::memcpy(IAU, c->h_IAU.data(), sizeof(int) * c->h_IAU.size());
+    return CFD_OK;
+}
+
+#define NEED_MESH(fn)                                                      \
+    if (!c) { set_error(fn ": NULL context"); return CFD_ERR_ARG; }        \
+    if (!c->has_mesh) { set_error(fn ": no mesh installed"); return CFD_ERR_STATE; } \
+    CFD_CUDA(cudaSetDevice(c->device))
+
+int cfd_set_state(cfd_ctx *c, const double *Q) {
+    NEED_MESH("cfd_set_state");
+    if (!Q) return CFD_ERR_ARG;
+    const int64_t n = (int64_t)c->nnode + c->nghost;
+    CFD_CUDA(cudaMemcpy2DAsync(c->Q.p, c->ldq * sizeof(double), Q, n * sizeof(double), n * sizeof(double), 5,
+                               cudaMemcpyHostToDevice, c->stream));
+    return CFD_OK;
+}
+
+int cfd_get_state(cfd_ctx *c, double *Q) {
+    NEED_MESH("cfd_get_state");
+    if (!Q) return CFD_ERR_ARG;
+    const int64_t n = (int64_t)c->nnode + c->nghost;
+    CFD_CUDA(cudaMemcpy2DAsync(Q, n * sizeof(double), c->Q.p, c->ldq * sizeof(double), n * sizeof(double), 5,
+                               cudaMemcpyDeviceToHost, c->stream));
+    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    return CFD_OK;
+}
+
+int cfd_state_device_ptr(cfd_ctx *c, double **dQ, int64_t *ld) {
+    NEED_MESH("cfd_state_device_ptr");
+    if (dQ) *dQ = c->Q.p;
+    if (ld) *ld = c->ldq;
+    return CFD_OK;
+}
+
+int cfd_set_freestream(cfd_ctx *c) {
+    NEED_MESH("cfd_set_freestream");
+    compute_flow(c, 0);
+    const int n = c->nnode + c->nghost;
+    k_freestream<<<grid_for(n, 256), 256, 0, c->stream>>>(n, c->ldq, c->flow, c->Q.p);
+    CFD_LAUNCH_CHECK();
+    return CFD_OK;
+}
+
+int cfd_begin_iteration(cfd_ctx *c, int iteration) {
+    NEED_MESH("cfd_begin_iteration");
+    compute_flow(c, iteration);
+    unsigned long long h[8];
+    for (int j = 0; j < 4; j++) {
+        h[2 * j] = dbits(DBL_MAX);
+        h[2 * j + 1] = dbits(DBL_MIN);
+    }
+    CFD_CUDA(cudaMemcpyAsync(c->ext.p, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+    CFD_CUDA(cudaMemsetAsync(c->dt.p, 0, sizeof(double) * c->nnode, c->stream));
+    // the host staging buffer must outlive the async copy
+    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    return CFD_OK;
+}
+
+int cfd_apply_bc(cfd_ctx *c, int iteration) {
+    NEED_MESH("cfd_apply_bc");
+    c->flow.iteration = iteration;
+    if (c->nbedge == 0) return CFD_OK;
+    k_apply_bc<<<grid_for(c->nbedge, 128), 128, 0, c->stream>>>(c->nbedge, c->ldq, c->Q.p, c->bedge_nodes.p,
+                                                                  c->bedge_geo.p, c->bedge_type.p, c->flow, c->err.p);
+    CFD_LAUNCH_CHECK();
+    return CFD_OK;
+}
+
+int cfd_residual(cfd_ctx *c, int add_time) {
+    NEED_MESH("cfd_residual");
+    const bool second = c->params.order == CFD_ORDER_SECOND;
+    if (second && !c->has_grad) {
+        set_error("cfd_residual: second order needs cfd_gradient first");
+        return CFD_ERR_STATE;
+    }
+    if (second && c->params.limiter != CFD_LIMITER_NONE && !c->phi.p) {
+        set_error("cfd_residual: limiter requested but cfd_limiter not called");
+        return CFD_ERR_STATE;
+    }
+    switch (c->params.flux_scheme * 2 + (second ? 1 : 0)) {
+        case 0: launch_residual<CFD_FLUX_ROE, false>(c, add_time); break;
+        case 1: launch_residual<CFD_FLUX_ROE, true>(c, add_time); break;
+        case 2: launch_residual<CFD_FLUX_HLLC, false>(c, add_time); break;
+        case 3: launch_residual<CFD_FLUX_HLLC, true>(c, add_time); break;
+        case 4: launch_residual<CFD_FLUX_AUSM, false>(c, add_time); break;
+        case 5: launch_residual<CFD_FLUX_AUSM, true>(c, add_time); break;
+        default: set_error("cfd_residual: bad flux scheme"); return CFD_ERR_ARG;
+    }
+    CFD_LAUNCH_CHECK();
+    return CFD_OK;
+}
+
+int cfd_deltat(cfd_ctx *c, int iteration) {
+    NEED_MESH("cfd_deltat");
+    compute_flow(c, iteration);
+    k_deltat<<<grid_for(c->nnode, 256), 256, 0, c->stream>>>(c->nnode, c->cvol.p, c->cfl, c->dt.p, c->ext.p);
+    CFD_LAUNCH_CHECK();
+    if (c->params.global_time) {
+        k_fill_global_dt<<<grid_for(c->nnode, 256), 256, 0, c->stream>>>(c->nnode, c->ext.p, c->dt.p);
+        CFD_LAUNCH_CHECK();
+    }
+    return CFD_OK;
+}
+
+int cfd_residual_rms(cfd_ctx *c, int include_diss, double out[6]) {
+    NEED_MESH("cfd_residual_rms");
+    if (!out) return CFD_ERR_ARG;
+    const int64_t n = c->nnode;
+    const double *src = c->res.p;
+    if (include_diss) {
+        CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)5 * n)));
+        k_add_diss<<<grid_for(5 * n, 256), 256, 0, c->stream>>>(5 * n, c->res.p, c->resd.p, c->work.p);
+        CFD_LAUNCH_CHECK();
+        src = c->work.p;
+    }
+    double s[5];
+    int st = reduce_sum_sq(c, src, n, n, 5, s);
+    if (st) return st;
+    // Solver_Steady_Implicit.cpp:107-126
+    double tot = s[0] + s[1] + s[2] + s[3] + s[4];
+    out[5] = sqrt(tot / (5.0 * (double)n));
+    for (int k = 0; k < 5; k++) out[k] = sqrt(s[k] / (double)n);
+    return CFD_OK;
+}
+
+int cfd_jacobian(cfd_ctx *c, int add_time, int include_diss, int precision) {
+    NEED_MESH("cfd_jacobian");
+    if (precision < CFD_PREC_FP64 || precision > CFD_PREC_BF16) return CFD_ERR_ARG;
+    CFD_CUDA(c->A64.alloc((size_t)c->nnzb * 25));
+    CFD_CUDA(c->B.alloc((size_t)c->nnode * 5));
+    CFD_CUDA(c->X.alloc((size_t)c->nnode * 5));
+    c->a_precision = precision;
+    const int ge = grid_for(c->nedge, 128), gr = grid_for(c->nnode, 128);
+    if (precision == CFD_PREC_FP32) {
+        CFD_CUDA(c->A32.alloc((size_t)c->nnzb * 25));
+        if (c->nedge)
+            k_jac_edges<float><<<ge, 128, 0, c->stream>>>(c->nedge, c->ldq, c->Q.p, c->edge_nodes.p, c->edge_geo.p,
+                                                          c->eslot.p, c->flow, c->A64.p, c->A32.p);
+        CFD_LAUNCH_CHECK();
+        k_jac_rows<float><<<gr, 128, 0, c->stream>>>(c->nnode, c->ldq, c->Q.p, c->IA.p, c->IAU.p, c->tslot.p,
+                                                     c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p,
+                                                     c->cvol.p, c->dt.p, c->res.p, c->resd.p, add_time, include_diss,
+                                                     c->flow, c->A64.p, c->A32.p, c->B.p);
+    } else if (precision == CFD_PREC_BF16) {
+        CFD_CUDA(c->A16.alloc((size_t)c->nnzb * 25));
+        if (c->nedge)
+            k_jac_edges<uint16_t><<<ge, 128, 0, c->stream>>>(c->nedge, c->ldq, c->Q.p, c->edge_nodes.p,
+                                                             c->edge_geo.p, c->eslot.p, c->flow, c->A64.p, c->A16.p);
+        CFD_LAUNCH_CHECK();
+        k_jac_rows<uint16_t><<<gr, 128, 0, c->stream>>>(c->nnode, c->ldq, c->Q.p, c->IA.p, c->IAU.p, c->tslot.p,
+                                                        c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p,
+                                                        c->cvol.p, c->dt.p, c->res.p, c->resd.p, add_time,
+                                                        include_diss, c->flow, c->A64.p, c->A16.p, c->B.p);
+    } else {
+        if (c->nedge)
+            k_jac_edges<float><<<ge, 128, 0, c->stream>>>(c->nedge, c->ldq, c->Q.p, c->edge_nodes.p, c->edge_geo.p,
+                                                          c->eslot.p, c->flow, c->A64.p, (float *)nullptr);
+        CFD_LAUNCH_CHECK();
+        k_jac_rows<float><<<gr, 128, 0, c->stream>>>(c->nnode, c->ldq, c->Q.p, c->IA.p, c->IAU.p, c->tslot.p,
+                                                     c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p,
+                                                     c->cvol.p, c->dt.p, c->res.p, c->resd.p, add_time, include_diss,
+                                                     c->flow, c->A64.p, (float *)nullptr, c->B.p);
+    }
+    CFD_LAUNCH_CHECK();
+    c->has_system = true;
+    return CFD_OK;
+}
+
+int cfd_block_gs(cfd_ctx *c, int iterations, int direction, double *rms) {
+    NEED_MESH("cfd_block_gs");
+    if (!c->has_system) { set_error("cfd_block_gs: no system (call cfd_jacobian)"); return CFD_ERR_STATE; }
+    if (direction < 0 || direction > 2) return CFD_ERR_ARG;
+    const int n = c->nnode;
+    CFD_CUDA(c->LUd.alloc((size_t)n * 25));
+    CFD_CUDA(c->rowrms.alloc(n));
+    CFD_CUDA(cudaMemsetAsync(c->X.p, 0, sizeof(double) * 5 * n, c->stream));  // MC_Iterative_Jacobi.c:375
+    k_lu_nopivot<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->A64.p, c->IAU.p, c->LUd.p);
+    CFD_LAUNCH_CHECK();
+    const int maxit = 10000;
+    if (iterations <= 0) iterations = maxit;
+    double r = 0.0;
+    for (int it = 0; it < iterations; it++) {
+        const bool fwd = direction == 0 || (direction == 2 && it % 2 == 0);
+        Levels &L = fwd ? c->lv_fwd : c->lv_bwd;
+        const int nl = (int)L.ptr.size() - 1;
+        for (int l = 0; l < nl; l++) {
+            const int lo = L.ptr[l], cnt = L.ptr[l + 1] - lo;
+            k_gs_level<<<grid_for(cnt, 128), 128, 0, c->stream>>>(cnt, L.rows.p + lo, c->IA.p, c->JA.p, c->IAU.p,
+                                                                    c->A64.p, c->B.p, c->LUd.p, c->X.p, c->rowrms.p);
+        }
+        CFD_LAUNCH_CHECK();
+        double s = 0.0;
+        int st = reduce_sum_plain(c, c->rowrms.p, n, &s);
+        if (st) return st;
+        r = sqrt(s / (double)n);
+        if (r < 100.0 * DBL_EPSILON) break;  // MC_Iterative_Jacobi.c:506
+    }
+    if (rms) *rms = r;
+    return std::isnan(r) ? CFD_ERR_NUMERIC : CFD_OK;
+}
+
+int cfd_update(cfd_ctx *c, double relax) {
+    NEED_MESH("cfd_update");
+    if (!c->X.p) { set_error("cfd_update: no solution vector"); return CFD_ERR_STATE; }
+    k_update<<<grid_for(c->nnode, 256), 256, 0, c->stream>>>(c->nnode, c->ldq, relax, c->X.p, c->Q.p);
+    CFD_LAUNCH_CHECK();
+    return CFD_OK;
+}
+
+int cfd_get_residual(cfd_ctx *c, double *conv, double *diss) {
+    NEED_MESH("cfd_get_residual");
+    const size_t bytes = sizeof(double) * 5 * c->nnode;
+    if (conv) CFD_CUDA(cudaMemcpyAsync(conv, c->res.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    if (diss) CFD_CUDA(cudaMemcpyAsync(diss, c->resd.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    return check_device_error(c);
+}
+
+int cfd_get_deltat(cfd_ctx *c, double *dt) {
+    NEED_MESH("cfd_get_deltat");
+    if (!dt) return CFD_ERR_ARG;
+    CFD_CUDA(cudaMemcpyAsync(dt, c->dt.p, sizeof(double) * c->nnode, cudaMemcpyDeviceToHost, c->stream));
+    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    return CFD_OK;
+}
+
+int cfd_get_extrema(cfd_ctx *c, double out[8]) {
+    NEED_MESH("cfd_get_extrema");
+    unsigned long long h[8];
+    CFD_CUDA(cudaMemcpyAsync(h, c->ext.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < 8; k++) out[k] = bitsd(h[k]);
+    return CFD_OK;
+}
+
+int cfd_get_farfield(cfd_ctx *c, double out[8]) {
+    if (!c || !out) return CFD_ERR_ARG;
+    const Flow &f = c->flow;
+    out[0] = f.inf_rho; out[1] = f.inf_u; out[2] = f.inf_v; out[3] = f.inf_w;
+    out[4] = f.inf_et; out[5] = f.inf_p; out[6] = f.inf_c; out[7] = f.inf_mach;
+    return CFD_OK;
+}
+
+int cfd_get_system(cfd_ctx *c, double *A, double *B, double *X) {
+    NEED_MESH("cfd_get_system");
+    if (!c->has_system) { set_error("cfd_get_system: no system"); return CFD_ERR_STATE; }
+    if (A) CFD_CUDA(cudaMemcpyAsync(A, c->A64.p, sizeof(double) * 25 * c->nnzb, cudaMemcpyDeviceToHost, c->stream));
+    if (B) CFD_CUDA(cudaMemcpyAsync(B, c->B.p, sizeof(double) * 5 * c->nnode, cudaMemcpyDeviceToHost, c->stream));
+    if (X) CFD_CUDA(cudaMemcpyAsync(X, c->X.p, sizeof(double) * 5 * c->nnode, cudaMemcpyDeviceToHost, c->stream));
+    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    return CFD_OK;
+}
+
+int cfd_set_system(cfd_ctx *c, const double *A, const double *B) {
+    NEED_MESH("cfd_set_system");
+    if (!A || !B) return CFD_ERR_ARG;
+    CFD_CUDA(c->A64.upload(A, (size_t)c->nnzb * 25, c->stream));
+    CFD_CUDA(c->B.upload(B, (size_t)c->nnode * 5, c->stream));
+    CFD_CUDA(c->X.alloc((size_t)c->nnode * 5));
+    CFD_CUDA(cudaMemsetAsync(c->X.p, 0, sizeof(double) * 5 * c->nnode, c->stream));
+    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    c->a_precision = CFD_PREC_FP64;
+    c->has_system = true;
+    return CFD_OK;
+}
+
+int cfd_residual_step(cfd_ctx *c, int iteration, const double *Q_host, double *conv_host, double *diss_host) {
+    NEED_MESH("cfd_residual_step");
+    int st;
+    if (Q_host && (st = cfd_set_state(c, Q_host))) return st;
+    if ((st = cfd_begin_iteration(c, iteration))) return st;
+    if ((st = cfd_apply_bc(c, iteration))) return st;
+    if (c->params.order == CFD_ORDER_SECOND) {
+        if ((st = cfd_gradient(c))) return st;
+        if (c->params.limiter != CFD_LIMITER_NONE && (st = cfd_limiter(c))) return st;
+    }
+    if ((st = cfd_residual(c, 1))) return st;
+    if ((st = cfd_deltat(c, iteration))) return st;
+    if (conv_host || diss_host) return cfd_get_residual(c, conv_host, diss_host);
+    return CFD_OK;
+}
+
+// ---------------------------------------------------------- restart files
+int cfd_restart_write(const char *path, int iteration, int nnode, int nghost, const double *Q) {
+    if (!path || !Q || nnode <= 0 || nghost < 0) return CFD_ERR_ARG;
+    FILE *f = std::fopen(path, "wb");
+    if (!f) { set_error("cfd_restart_write: cannot open %s", path); return CFD_ERR_IO; }
+    const int hdr[4] = {iteration, nnode, nghost, 5};
+    std::fwrite(hdr, sizeof(int), 4, f);
+    const int64_t n = (int64_t)nnode + nghost;
+    std::vector<double> row(5);
+    for (int64_t i = 0; i < n; i++) {
+        for (int k = 0; k < 5; k++) row[k] = Q[k * n + i];
+        std::fwrite(row.data(), sizeof(double), 5, f);
+    }
+    std::fclose(f);
+    return CFD_OK;
+}
+
+int cfd_restart_read(const char *path, int *iteration, int nnode, int nghost, double *Q) {
+    if (!path || !Q) return CFD_ERR_ARG;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) { set_error("cfd_restart_read: cannot open %s", path); return CFD_ERR_IO; }
+    int hdr[4];
+    if (std::fread(hdr, sizeof(int), 4, f) != 4 || hdr[1] != nnode || hdr[2] != nghost || hdr[3] != 5) {
+        std::fclose(f);
+        set_error("cfd_restart_read: header mismatch in %s", path);
+        return CFD_ERR_IO;
+    }
+    if (iteration) *iteration = hdr[0];
+    const int64_t n = (int64_t)nnode + nghost;
+    double row[5];
+    for (int64_t i = 0; i < n; i++) {
+        if (std::fread(row, sizeof(double), 5, f) != 5) {
+            std::fclose(f);
+            set_error("cfd_restart_read: short file %s", path);
+            return CFD_ERR_IO;
+        }
+        for (int k = 0; k < 5; k++) Q[k * n + i] = row[k];
+    }
+    std::fclose(f);
+    return CFD_OK;
+}
+
+// ------------------------------------------------------------ mesh builder
+int cfd_mesh_box(int nx, int ny, int nz, double lx, double ly, double lz, double jitter, uint64_t seed, int rcm,
+                 const int face_bc[6], cfd_mesh **out) {
+    if (!out) return CFD_ERR_ARG;
+    *out = nullptr;
+    int fb[6] = {1, 1, 1, 1, 1, 1};
+    if (face_bc) std::memcpy(fb, face_bc, sizeof(fb));
+    cfd_mesh *m = new cfd_mesh();
+    int st = build_box(m->m, nx, ny, nz, lx, ly, lz, jitter, seed, rcm, fb);
+    if (st) { delete m; set_error("cfd_mesh_box: build failed (%d)", st); return st; }
+    *out = m;
+    return CFD_OK;
+}
+
+int cfd_mesh_from_cells(int nnode, const double *coords, int64_t ntet, const int *tets, int64_t ntri,
+                        const int *tris, const int *tri_bc, cfd_mesh **out) {
+    if (!out || !coords || !tets || (ntri && (!tris || !tri_bc)) || nnode <= 0) return CFD_ERR_ARG;
+    cfd_mesh *m = new cfd_mesh();
+    int st = build_from_cells(m->m, nnode, coords, ntet, tets, ntri, tris, tri_bc);
+    if (st) { delete m; set_error("cfd_mesh_from_cells: build failed (%d)", st); return st; }
+    *out = m;
+    return CFD_OK;
+}
+
+int cfd_mesh_sizes(const cfd_mesh *mm, int64_t sizes[7]) {
+    if (!mm || !sizes) return CFD_ERR_ARG;
+    const HostMesh &m = mm->m;
+    sizes[0] = m.nnode; sizes[1] = m.nghost; sizes[2] = m.nedge; sizes[3] = m.nbedge;
+    sizes[4] = (int64_t)m.tets.size() / 4; sizes[5] = (int64_t)m.tris.size() / 3;
+    sizes[6] = m.n2n_ia.empty() ? 0 : m.n2n_ia.back();
+    return CFD_OK;
+}
+
+int cfd_mesh_export(const cfd_mesh *mm, int *edge_nodes, double *edge_areav, int *bedge_nodes, double *bedge_areav,
+                    int *bedge_type, double *cvol, double *coords, int *n2n_ia, int *n2n_ja) {
+    if (!mm) return CFD_ERR_ARG;
+    const HostMesh &m = mm->m;
+    auto cp = [](auto *dst, const auto &v) {
+        if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    cp(edge_nodes, m.edge_nodes); cp(edge_areav, m.edge_areav);
+    cp(bedge_nodes, m.bedge_nodes); cp(bedge_areav, m.bedge_areav); cp(bedge_type, m.bedge_type);
+    cp(cvol, m.cvol); cp(coords, m.coords); cp(n2n_ia, m.n2n_ia); cp(n2n_ja, m.n2n_ja);
+    return CFD_OK;
+}
+
+int cfd_mesh_export_cells(const cfd_mesh *mm, int *tets, int *tris, int *tri_bc) {
+    if (!mm) return CFD_ERR_ARG;
+    const HostMesh &m = mm->m;
+    if (tets) std::memcpy(tets, m.tets.data(), m.tets.size() * sizeof(int));
+    if (tris) std::memcpy(tris, m.tris.data(), m.tris.size() * sizeof(int));
+    if (tri_bc) std::memcpy(tri_bc, m.tri_bc.data(), m.tri_bc.size() * sizeof(int));
+    return CFD_OK;
+}
+
+int cfd_mesh_write_ugrid(const cfd_mesh *mm, const char *path) {
+    if (!mm || !path) return CFD_ERR_ARG;
+    return write_ugrid(mm->m, path, nullptr);
+}
+
+int cfd_set_mesh_from(cfd_ctx *c, const cfd_mesh *mm) {
+    if (!c || !mm) return CFD_ERR_ARG;
+    const HostMesh &m = mm->m;
+    return cfd_set_mesh(c, m.nnode, m.nghost, m.nedge, m.edge_nodes.data(), m.edge_areav.data(), m.nbedge,
+                        m.bedge_nodes.data(), m.bedge_areav.data(), m.bedge_type.data(), m.cvol.data(),
+                        m.coords.data(), m.n2n_ia.data(), m.n2n_ja.data());
+}
+
+void cfd_mesh_free(cfd_mesh *m) { delete m; }
+
+}  // extern "C"

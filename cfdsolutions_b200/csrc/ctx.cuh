@@ -1,0 +1,155 @@
+// Device context of the library: resident mesh, state, residual, block-CRS
+// system and solver workspaces for one mesh on one GPU.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <vector>
+
+#include "cfd_internal.h"
+#include "physics.cuh"
+
+namespace cfd {
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(size_t count) {
+        if (count == n && p) return cudaSuccess;
+        release();
+        if (count == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+        if (e == cudaSuccess) n = count;
+        else p = nullptr;
+        return e;
+    }
+    cudaError_t upload(const T *h, size_t count, cudaStream_t s) {
+        cudaError_t e = alloc(count);
+        if (e != cudaSuccess || count == 0) return e;
+        return cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s);
+    }
+};
+
+// Level schedule of a sparse triangular dependency (rows grouped so that the
+// rows of one level only depend on rows of earlier levels).
+struct Levels {
+    std::vector<int> ptr;  // host, nlevels+1
+    DevBuf<int> rows;      // device, rows in level order
+    int max_width = 0;
+};
+
+}  // namespace cfd
+
+struct cfd_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cfd_params params{};
+    cfd::Flow flow{};
+    double cfl = 0.0;
+    bool has_mesh = false;
+
+    int nnode = 0, nghost = 0, nedge = 0, nbedge = 0;
+    int64_t nnzb = 0;
+    int64_t ldq = 0;  // leading dimension of Q (>= nnode + nghost)
+
+    // mesh
+    cfd::DevBuf<int2> edge_nodes;
+    cfd::DevBuf<double4> edge_geo;    // unit normal (x,y,z) + |S|
+    cfd::DevBuf<int2> bedge_nodes;
+    cfd::DevBuf<double4> bedge_geo;
+    cfd::DevBuf<int> bedge_type;
+    cfd::DevBuf<double> cvol;
+    cfd::DevBuf<double> xyz;          // SoA [3][nnode]
+    cfd::DevBuf<double4> edge_sv;     // raw area vector (x,y,z) + 0, for Green-Gauss
+    cfd::DevBuf<double4> bedge_sv;
+    cfd::DevBuf<int> n2n_ia, n2n_ja;  // physical node graph (no diagonal)
+    cfd::DevBuf<int> n2e_ptr, n2e;    // incident interior edges, ~e when the node is node_R
+    cfd::DevBuf<int> n2b_ptr, n2b;    // incident boundary edges
+    // block CRS (Create_CRS_SolverBlockMatrix layout)
+    std::vector<int> h_IA, h_JA, h_IAU;
+    cfd::DevBuf<int> IA, JA, IAU, tslot;  // tslot[k] = slot of (JA[k], row)
+    cfd::DevBuf<int2> eslot;              // per edge: slot(L,R), slot(R,L)
+    cfd::Levels lv_fwd, lv_bwd;
+
+    // state and residual
+    cfd::DevBuf<double> Q;      // [5][ldq]
+    cfd::DevBuf<double> res;    // [5][nnode] convective
+    cfd::DevBuf<double> resd;   // [5][nnode] dissipative
+    cfd::DevBuf<double> dt;     // [nnode] sum(area*lambda) then DeltaT
+    cfd::DevBuf<double> grad;   // [15][nnode]
+    cfd::DevBuf<double> phi;    // [5][nnode]
+    cfd::DevBuf<double> ggw;    // Green-Gauss / LSQ per-node coefficients
+    cfd::DevBuf<unsigned long long> ext;  // 8 extrema as ordered bit patterns
+    cfd::DevBuf<int> err;       // device error word
+    cfd::DevBuf<double> red;    // reduction partials
+    cfd::DevBuf<double> red_out;
+
+    // linear system
+    cfd::DevBuf<double> A64;    // [nnzb][25]
+    cfd::DevBuf<float> A32;     // [nnzb][25] when FP32 storage requested
+    cfd::DevBuf<uint16_t> A16;  // [nnzb][25] BF16 storage
+    int a_precision = CFD_PREC_FP64;
+    cfd::DevBuf<double> B, X;   // [nnode][5]
+    cfd::DevBuf<double> LUd;    // [nnode][25] diagonal LU for block GS
+    cfd::DevBuf<double> rowrms; // [nnode]
+    // GMRES / ILU workspaces (linsolve.cu)
+    cfd::DevBuf<float> M32;     // ILU0 / block-Jacobi factors, FP32
+    cfd::DevBuf<double> M64;    // ILU0 / block-Jacobi factors, FP64
+    cfd::DevBuf<double> V;      // Krylov basis [(m+1)][5*nnode]
+    cfd::DevBuf<double> Z;      // preconditioned vectors (flexible) [m][5*nnode]
+    cfd::DevBuf<double> work;   // misc vectors
+    cfd::DevBuf<double> dots;   // device dot results
+    cfd::DevBuf<int> ilu_diag_inv_done;
+    int krylov_m = 0;
+    bool has_system = false;
+    bool has_grad = false;
+};
+
+namespace cfd {
+
+#define CFD_CUDA(call)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            cfd::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+            return CFD_ERR_CUDA;                                                         \
+        }                                                                                \
+    } while (0)
+
+#define CFD_LAUNCH_CHECK()                                                               \
+    do {                                                                                 \
+        cudaError_t e_ = cudaGetLastError();                                             \
+        if (e_ != cudaSuccess) {                                                         \
+            cfd::set_error("%s:%d launch: %s", __FILE__, __LINE__, cudaGetErrorString(e_)); \
+            return CFD_ERR_CUDA;                                                         \
+        }                                                                                \
+    } while (0)
+
+inline int grid_for(int64_t n, int block) { return (int)((n + block - 1) / block); }
+
+// Deterministic reductions (fixed grid -> fixed order): implemented in core.cu.
+int reduce_sum_sq(cfd_ctx *c, const double *x, int64_t n, int64_t stride, int nvec, double *out_host);
+
+// error word bits
+enum : int {
+    ERR_BC_NEG_PRESSURE = 1,
+    ERR_BC_UNCLASSIFIED = 2,
+    ERR_NAN = 4,
+    ERR_NEG_STATE = 8,
+};
+
+int check_device_error(cfd_ctx *c);
+
+}  // namespace cfd

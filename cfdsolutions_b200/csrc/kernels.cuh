@@ -1,0 +1,158 @@
+// Edge-flux dispatch (Roe / HLLC / AUSM+) and small device helpers shared by
+// the residual, Jacobian and linear-solver translation units.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "ctx.cuh"
+#include "physics.cuh"
+
+namespace cfd {
+
+// HLLC flux (Compute_HLLCFlux, Euler3D/src/HLLC_Fluxes.cpp:143-326): Roe-averaged
+// wave speeds SL = min(ubar_L - c_L, ubar - c), SR = max(ubar_R + c_R, ubar + c),
+// contact speed SM, star states.  The whole flux goes to the convective
+// residual (Compute_Residual_HLLC, :519-573); the dissipative part is zero.
+__device__ __forceinline__ double hllc_flux(const double qL[5], const double qR[5], double nx, double ny, double nz,
+                                            double area, const Flow &f, double conv[5], double diss[5],
+                                            double lam[3]) {
+    Face L, R;
+    eos_face(qL, nx, ny, nz, f.gm1, f.gamma, true, L);
+    eos_face(qR, nx, ny, nz, f.gm1, f.gamma, true, R);
+    const double rho = sqrt(R.rho * L.rho);
+    const double sigma = rho / (L.rho + rho);
+    const double u = L.u + sigma * (R.u - L.u);
+    const double v = L.v + sigma * (R.v - L.v);
+    const double w = L.w + sigma * (R.w - L.w);
+    const double ht = L.ht + sigma * (R.ht - L.ht);
+    const double phi = 0.5 * f.gm1 * (u * u + v * v + w * w);
+    const double c = sqrt(f.gm1 * ht - phi);
+    const double ubar = u * nx + v * ny + w * nz;
+    const double SL = fmin(L.ubar - L.c, ubar - c);
+    const double SR = fmax(R.ubar + R.c, ubar + c);
+    const double SM = (R.rho * R.ubar * (SR - R.ubar) - L.rho * L.ubar * (SL - L.ubar) + L.p - R.p) /
+                      (R.rho * (SR - R.ubar) - L.rho * (SL - L.ubar));
+    double F[5];
+    if (SL > 0.0 || SR < 0.0) {
+        const Face &S = SL > 0.0 ? L : R;
+        const double m = S.rho * S.ubar;
+        F[0] = m;
+        F[1] = S.u * m + S.p * nx;
+        F[2] = S.v * m + S.p * ny;
+        F[3] = S.w * m + S.p * nz;
+        F[4] = S.ht * m;
+    } else {
+        const bool left = SM > 0.0;
+        const Face &S = left ? L : R;
+        const double Sk = left ? SL : SR;
+        const double pstar = S.p + S.rho * (S.ubar - Sk) * (S.ubar - SM);
+        const double om = 1.0 / (Sk - SM);
+        const double c1 = Sk - S.ubar, c2 = pstar - S.p;
+        const double et = S.ht - S.p / S.rho;
+        const double rs = om * (c1 * S.rho);
+        const double rus = om * (c1 * S.rho * S.u + c2 * nx);
+        const double rvs = om * (c1 * S.rho * S.v + c2 * ny);
+        const double rws = om * (c1 * S.rho * S.w + c2 * nz);
+        const double res_ = om * (c1 * S.rho * et - S.p * S.ubar + pstar * SM);
+        F[0] = rs * SM;
+        F[1] = rus * SM + pstar * nx;
+        F[2] = rvs * SM + pstar * ny;
+        F[3] = rws * SM + pstar * nz;
+        F[4] = (res_ + pstar) * SM;
+    }
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        conv[k] = F[k] * area;
+        diss[k] = 0.0;
+    }
+    // HLLC leaves the eigenvalue extrema untouched in the reference; NaN is
+    // ignored by fmin/fmax.
+    lam[0] = lam[1] = lam[2] = __longlong_as_double(0x7ff8000000000000LL);
+    return fmax(fabs(ubar), fmax(fabs(ubar + c), fabs(ubar - c)));
+}
+
+// AUSM+ (M.-S. Liou, "A sequel to AUSM: AUSM+", J. Comput. Phys. 129, 1996):
+// interface sound speed c_1/2 = min(c^_L, c^_R), c^ = c*^2/max(c*, |u_n|) with
+// c*^2 = 2 (gamma-1)/(gamma+1) H; split Mach numbers of degree 4 (beta = 1/8)
+// and split pressures of degree 5 (alpha = 3/16); upwinded convective flux
+// c_1/2 (m+ Phi_L + m- Phi_R) plus p_1/2 n.  The reference's AUSM entry points
+// are empty stubs (Euler3D/src/AUSM_Fluxes.cpp:45-54), so this follows the
+// published method.  The dissipative residual is zero; the time-step spectral
+// radius is the Roe-averaged |ubar| + c, as for HLLC.
+__device__ __forceinline__ double ausmp_flux(const double qL[5], const double qR[5], double nx, double ny,
+                                             double nz, double area, const Flow &f, double conv[5], double diss[5],
+                                             double lam[3]) {
+    Face L, R;
+    eos_face(qL, nx, ny, nz, f.gm1, f.gamma, false, L);
+    eos_face(qR, nx, ny, nz, f.gm1, f.gamma, false, R);
+    const double k = 2.0 * f.gm1 / (f.gamma + 1.0);
+    const double csL = sqrt(k * L.ht), csR = sqrt(k * R.ht);
+    const double chL = csL * csL / fmax(csL, L.ubar);
+    const double chR = csR * csR / fmax(csR, -R.ubar);
+    const double c12 = fmin(chL, chR);
+    const double ML = L.ubar / c12, MR = R.ubar / c12;
+    const double beta = 0.125, alpha = 3.0 / 16.0;
+    double Mp, Pp, Mm, Pm;
+    if (fabs(ML) >= 1.0) {
+        Mp = 0.5 * (ML + fabs(ML));
+        Pp = ML > 0.0 ? 1.0 : 0.0;
+    } else {
+        const double a = ML + 1.0, b = ML * ML - 1.0;
+        Mp = 0.25 * a * a + beta * b * b;
+        Pp = 0.25 * a * a * (2.0 - ML) + alpha * ML * b * b;
+    }
+    if (fabs(MR) >= 1.0) {
+        Mm = 0.5 * (MR - fabs(MR));
+        Pm = MR < 0.0 ? 1.0 : 0.0;
+    } else {
+        const double a = MR - 1.0, b = MR * MR - 1.0;
+        Mm = -0.25 * a * a - beta * b * b;
+        Pm = 0.25 * a * a * (2.0 + MR) - alpha * MR * b * b;
+    }
+    const double m12 = Mp + Mm;
+    const double mpos = 0.5 * (m12 + fabs(m12)), mneg = 0.5 * (m12 - fabs(m12));
+    const double p12 = Pp * L.p + Pm * R.p;
+    const double aL = c12 * mpos * L.rho, aR = c12 * mneg * R.rho;
+    conv[0] = area * (aL + aR);
+    conv[1] = area * (aL * L.u + aR * R.u + p12 * nx);
+    conv[2] = area * (aL * L.v + aR * R.v + p12 * ny);
+    conv[3] = area * (aL * L.w + aR * R.w + p12 * nz);
+    conv[4] = area * (aL * L.ht + aR * R.ht);
+#pragma unroll
+    for (int j = 0; j < 5; j++) diss[j] = 0.0;
+    lam[0] = lam[1] = lam[2] = __longlong_as_double(0x7ff8000000000000LL);
+    const double rho = sqrt(R.rho * L.rho);
+    const double sigma = rho / (L.rho + rho);
+    const double u = L.u + sigma * (R.u - L.u);
+    const double v = L.v + sigma * (R.v - L.v);
+    const double w = L.w + sigma * (R.w - L.w);
+    const double ht = L.ht + sigma * (R.ht - L.ht);
+    const double c = sqrt(f.gm1 * ht - 0.5 * f.gm1 * (u * u + v * v + w * w));
+    return fabs(u * nx + v * ny + w * nz) + c;
+}
+
+template <int FLUX>
+__device__ __forceinline__ double edge_flux(const double qL[5], const double qR[5], double nx, double ny, double nz,
+                                            double area, const Flow &f, double conv[5], double diss[5],
+                                            double lam[3]) {
+    if (FLUX == CFD_FLUX_HLLC) return hllc_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
+    if (FLUX == CFD_FLUX_AUSM) return ausmp_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
+    return roe_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
+}
+
+__device__ __forceinline__ void store_low(float *p, double v) { *p = (float)v; }
+__device__ __forceinline__ void store_low(uint16_t *p, double v) {
+    __nv_bfloat16 b = __double2bfloat16(v);
+    *p = *reinterpret_cast<uint16_t *>(&b);
+}
+__device__ __forceinline__ double load_low(const float *p) { return (double)*p; }
+__device__ __forceinline__ double load_low(const uint16_t *p) {
+    __nv_bfloat16 b = *reinterpret_cast<const __nv_bfloat16 *>(p);
+    return (double)__bfloat162float(b);
+}
+
+// Deterministic sum of a plain vector (host result).
+int reduce_sum_plain(cfd_ctx *c, const double *x, int64_t n, double *out_host);
+
+}  // namespace cfd

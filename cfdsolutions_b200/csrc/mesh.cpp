@@ -1,0 +1,387 @@
+// Host-side median-dual mesh builder, O(N + E): tet-split box generator,
+// reverse Cuthill-McKee renumbering, node-centred median-dual metrics, ghost
+// nodes for boundary edges, and the node-to-node CRS graph.
+//
+// It produces exactly the arrays the reference's pre-processing produces, in
+// the reference's conventions:
+//   * interior edges (node_L < node_R), area vector pointing from node_L to
+//     node_R, summed over the two dual-face triangles of every cell edge
+//     (Euler3D/src/Area_Volume.cpp:659-800);
+//   * one boundary edge and one private ghost node per boundary-triangle
+//     vertex, ghost index = nNode + boundary-edge index, area = one third of
+//     the triangle's outward area vector (Area_Volume.cpp:461-556, flipped
+//     outward at :912-913);
+//   * control volume = sum of median-dual sub-volumes (V_tet / 4 per vertex);
+//   * node2node CRS without the diagonal (Connectivity_Maps.cpp:915-985).
+// The reference builds node2Edge in O(N*E) (Connectivity_Maps.cpp:766-780) and
+// renumbers with an O(N^2) Cuthill-McKee (Cuthill_Mckee_Reorder.cpp:17-155);
+// this builder is linear in the mesh size so 128^3-hex meshes build in seconds.
+#include "cfd_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+namespace cfd {
+
+namespace {
+
+struct SplitMix64 {
+    uint64_t s;
+    explicit SplitMix64(uint64_t seed) : s(seed) {}
+    uint64_t next() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    }
+    // uniform in [-1, 1)
+    double sym() { return ((next() >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0; }
+};
+
+inline void sub3(const double *a, const double *b, double *o) {
+    o[0] = a[0] - b[0]; o[1] = a[1] - b[1]; o[2] = a[2] - b[2];
+}
+inline void cross3(const double *a, const double *b, double *o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+inline double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+// Symmetric node graph of a tet mesh: CRS without diagonal, rows sorted.
+void build_graph(int nnode, const std::vector<int> &tets, std::vector<int> &ia, std::vector<int> &ja) {
+    const int64_t ntet = (int64_t)tets.size() / 4;
+    static const int pairs[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+    // Upper-neighbour sets with a fixed per-node capacity, grown on overflow.
+    int cap = 24;
+    std::vector<int> cnt, up;
+    for (;;) {
+        cnt.assign(nnode, 0);
+        up.assign((size_t)nnode * cap, -1);
+        bool overflow = false;
+        for (int64_t t = 0; t < ntet && !overflow; t++) {
+            const int *v = &tets[4 * t];
+            for (int p = 0; p < 6; p++) {
+                int a = v[pairs[p][0]], b = v[pairs[p][1]];
+                if (a > b) std::swap(a, b);
+                int *row = &up[(size_t)a * cap];
+                int c = cnt[a], k = 0;
+                for (; k < c; k++)
+                    if (row[k] == b) break;
+                if (k == c) {
+                    if (c == cap) { overflow = true; break; }
+                    row[c] = b;
+                    cnt[a] = c + 1;
+                }
+            }
+        }
+        if (!overflow) break;
+        cap *= 2;
+    }
+    std::vector<int> deg(nnode, 0);
+    for (int a = 0; a < nnode; a++) {
+        deg[a] += cnt[a];
+        for (int k = 0; k < cnt[a]; k++) deg[up[(size_t)a * cap + k]]++;
+    }
+    ia.assign(nnode + 1, 0);
+    for (int a = 0; a < nnode; a++) ia[a + 1] = ia[a] + deg[a];
+    ja.assign(ia[nnode], 0);
+    std::vector<int> fill(ia.begin(), ia.end() - 1);
+    for (int a = 0; a < nnode; a++)
+        for (int k = 0; k < cnt[a]; k++) {
+            int b = up[(size_t)a * cap + k];
+            ja[fill[a]++] = b;
+            ja[fill[b]++] = a;
+        }
+    for (int a = 0; a < nnode; a++) std::sort(ja.begin() + ia[a], ja.begin() + ia[a + 1]);
+}
+
+// Reverse Cuthill-McKee, O(N + E log d).  Start node: a pseudo-peripheral node
+// found by repeated BFS from a minimum-degree node.  Returns perm[new] = old.
+std::vector<int> rcm_order(int n, const std::vector<int> &ia, const std::vector<int> &ja) {
+    std::vector<int> order;
+    order.reserve(n);
+    std::vector<char> seen(n, 0);
+    std::vector<int> level(n, -1), q;
+    auto deg = [&](int v) { return ia[v + 1] - ia[v]; };
+    auto bfs_last = [&](int s, int &depth) {
+        std::fill(level.begin(), level.end(), -1);
+        q.clear();
+        q.push_back(s);
+        level[s] = 0;
+        size_t h = 0;
+        int last = s;
+        while (h < q.size()) {
+            int v = q[h++];
+            for (int k = ia[v]; k < ia[v + 1]; k++) {
+                int w = ja[k];
+                if (level[w] < 0) {
+                    level[w] = level[v] + 1;
+                    q.push_back(w);
+                    // deepest level, minimum degree
+                    if (level[w] > level[last] || (level[w] == level[last] && deg(w) < deg(last))) last = w;
+                }
+            }
+        }
+        depth = level[last];
+        return last;
+    };
+    for (int comp_seed = 0; comp_seed < n; comp_seed++) {
+        if (seen[comp_seed]) continue;
+        int s = comp_seed, d0 = -1;
+        for (int it = 0; it < 4; it++) {
+            int d;
+            int far = bfs_last(s, d);
+            if (d <= d0) break;
+            d0 = d;
+            s = far;
+        }
+        size_t base = order.size();
+        order.push_back(s);
+        seen[s] = 1;
+        std::vector<int> nb;
+        for (size_t h = base; h < order.size(); h++) {
+            int v = order[h];
+            nb.clear();
+            for (int k = ia[v]; k < ia[v + 1]; k++)
+                if (!seen[ja[k]]) { nb.push_back(ja[k]); seen[ja[k]] = 1; }
+            std::sort(nb.begin(), nb.end(), [&](int x, int y) { return deg(x) < deg(y) || (deg(x) == deg(y) && x < y); });
+            order.insert(order.end(), nb.begin(), nb.end());
+        }
+    }
+    std::reverse(order.begin(), order.end());
+    return order;
+}
+
+}  // namespace
+
+// Build the median-dual metrics of a tet mesh into m (coords/tets/tris set).
+static int build_dual(HostMesh &m) {
+    const int nnode = m.nnode;
+    const int64_t ntet = (int64_t)m.tets.size() / 4;
+    build_graph(nnode, m.tets, m.n2n_ia, m.n2n_ja);
+
+    // Interior edges = upper half of the graph, ordered by (L, R).
+    m.edge_nodes.clear();
+    std::vector<int> eoff(nnode + 1, 0);  // first edge of each L
+    for (int a = 0; a < nnode; a++) {
+        eoff[a] = (int)(m.edge_nodes.size() / 2);
+        for (int k = m.n2n_ia[a]; k < m.n2n_ia[a + 1]; k++)
+            if (m.n2n_ja[k] > a) { m.edge_nodes.push_back(a); m.edge_nodes.push_back(m.n2n_ja[k]); }
+    }
+    eoff[nnode] = (int)(m.edge_nodes.size() / 2);
+    const int nedge = eoff[nnode];
+    m.nedge = nedge;
+    m.edge_areav.assign((size_t)3 * nedge, 0.0);
+    m.cvol.assign(nnode, 0.0);
+
+    auto edge_id = [&](int a, int b) {
+        // a < b; upper neighbours of a are sorted within [eoff[a], eoff[a+1])
+        int lo = eoff[a], hi = eoff[a + 1];
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (m.edge_nodes[2 * mid + 1] < b) lo = mid + 1; else hi = mid;
+        }
+        return lo;
+    };
+
+    static const int pairs[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+    static const int others[6][2] = {{2, 3}, {1, 3}, {1, 2}, {0, 3}, {0, 2}, {0, 1}};
+    int bad = 0;
+    for (int64_t t = 0; t < ntet; t++) {
+        const int *v = &m.tets[4 * t];
+        const double *x[4];
+        for (int k = 0; k < 4; k++) x[k] = &m.coords[3 * (size_t)v[k]];
+        double g[3];
+        for (int d = 0; d < 3; d++) g[d] = 0.25 * (x[0][d] + x[1][d] + x[2][d] + x[3][d]);
+        double e1[3], e2[3], e3[3], c[3];
+        sub3(x[1], x[0], e1); sub3(x[2], x[0], e2); sub3(x[3], x[0], e3);
+        cross3(e2, e3, c);
+        double vol = dot3(e1, c) / 6.0;
+        if (!(vol > 0.0)) bad++;
+        for (int k = 0; k < 4; k++) m.cvol[v[k]] += 0.25 * std::fabs(vol);
+        for (int p = 0; p < 6; p++) {
+            int ia_ = pairs[p][0], ib = pairs[p][1];
+            int ic = others[p][0], id = others[p][1];
+            double mid[3], f1[3], f2[3];
+            for (int d = 0; d < 3; d++) {
+                mid[d] = 0.5 * (x[ia_][d] + x[ib][d]);
+                f1[d] = (x[ia_][d] + x[ib][d] + x[ic][d]) / 3.0;
+                f2[d] = (x[ia_][d] + x[ib][d] + x[id][d]) / 3.0;
+            }
+            double r1[3], r2[3], rg[3], s1[3], s2[3], S[3];
+            sub3(f1, mid, r1); sub3(g, mid, rg); sub3(f2, mid, r2);
+            cross3(r1, rg, s1);
+            cross3(rg, r2, s2);
+            for (int d = 0; d < 3; d++) S[d] = 0.5 * (s1[d] + s2[d]);
+            // orient from the lower to the higher node index
+            int a = v[ia_], b = v[ib];
+            double ab[3];
+            sub3(&m.coords[3 * (size_t)std::max(a, b)], &m.coords[3 * (size_t)std::min(a, b)], ab);
+            double sgn = dot3(S, ab) >= 0.0 ? 1.0 : -1.0;
+            int e = edge_id(std::min(a, b), std::max(a, b));
+            for (int d = 0; d < 3; d++) m.edge_areav[3 * (size_t)e + d] += sgn * S[d];
+        }
+    }
+    if (bad) {
+        std::fprintf(stderr, "cfd mesh: %d tetrahedra with non-positive volume\n", bad);
+        return CFD_ERR_MESH;
+    }
+
+    // Boundary edges: one per boundary-triangle vertex, own ghost node.
+    const int64_t ntri = (int64_t)m.tris.size() / 3;
+    m.nbedge = (int)(3 * ntri);
+    m.nghost = m.nbedge;
+    m.bedge_nodes.resize((size_t)2 * m.nbedge);
+    m.bedge_areav.resize((size_t)3 * m.nbedge);
+    m.bedge_type.resize(m.nbedge);
+    for (int64_t t = 0; t < ntri; t++) {
+        const int *v = &m.tris[3 * t];
+        double e1[3], e2[3], nrm[3];
+        sub3(&m.coords[3 * (size_t)v[1]], &m.coords[3 * (size_t)v[0]], e1);
+        sub3(&m.coords[3 * (size_t)v[2]], &m.coords[3 * (size_t)v[0]], e2);
+        cross3(e1, e2, nrm);  // right-hand normal = outward by construction
+        // the reference's UGRID reader reverses triangle winding (MeshIO.cpp:22-45),
+        // so its boundary edges of a triangle run over (v2, v1, v0)
+        for (int k = 0; k < 3; k++) {
+            int64_t be = 3 * t + k;
+            m.bedge_nodes[2 * be] = v[2 - k];
+            m.bedge_nodes[2 * be + 1] = nnode + (int)be;
+            for (int d = 0; d < 3; d++) m.bedge_areav[3 * be + d] = nrm[d] / 6.0;  // (|n|/2)/3
+            m.bedge_type[be] = m.tri_bc[t];
+        }
+    }
+    return CFD_OK;
+}
+
+// Freudenthal split of hex (i,j,k) into 6 positive tets sharing the diagonal
+// v000 -> v111; every face gets the diagonal through its lowest corner, so
+// neighbouring hexes agree on shared faces.
+int build_box(HostMesh &m, int nx, int ny, int nz, double lx, double ly, double lz, double jitter,
+              uint64_t seed, int renumber, const int face_bc[6]) {
+    if (nx < 1 || ny < 1 || nz < 1) return CFD_ERR_ARG;
+    const int px = nx + 1, py = ny + 1, pz = nz + 1;
+    const int64_t nn = (int64_t)px * py * pz;
+    if (nn > 0x7fffffff / 8) return CFD_ERR_ARG;
+    m = HostMesh();
+    m.nnode = (int)nn;
+    m.coords.resize(3 * (size_t)nn);
+    const double hx = lx / nx, hy = ly / ny, hz = lz / nz;
+    SplitMix64 rng(seed);
+    auto nid = [&](int i, int j, int k) { return i + px * (j + py * k); };
+    for (int k = 0; k < pz; k++)
+        for (int j = 0; j < py; j++)
+            for (int i = 0; i < px; i++) {
+                size_t id = (size_t)nid(i, j, k);
+                double x = i * hx, y = j * hy, z = k * hz;
+                double jx = rng.sym(), jy = rng.sym(), jz = rng.sym();
+                bool interior = i > 0 && i < nx && j > 0 && j < ny && k > 0 && k < nz;
+                if (interior) {
+                    x += jitter * hx * jx;
+                    y += jitter * hy * jy;
+                    z += jitter * hz * jz;
+                }
+                m.coords[3 * id] = x;
+                m.coords[3 * id + 1] = y;
+                m.coords[3 * id + 2] = z;
+            }
+    // 6 tets per hex: paths 000 -> +a -> +a+b -> 111 over permutations (a,b,c)
+    static const int perms[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+    m.tets.resize((size_t)24 * nx * ny * nz);
+    size_t tp = 0;
+    for (int k = 0; k < nz; k++)
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++)
+                for (int p = 0; p < 6; p++) {
+                    int o[3] = {0, 0, 0};
+                    int v[4];
+                    v[0] = nid(i, j, k);
+                    for (int s = 0; s < 3; s++) {
+                        o[perms[p][s]] = 1;
+                        v[s + 1] = nid(i + o[0], j + o[1], k + o[2]);
+                    }
+                    // orient positively: swap last two if the permutation is odd
+                    bool odd = (p == 1 || p == 2 || p == 5);
+                    if (odd) std::swap(v[2], v[3]);
+                    for (int s = 0; s < 4; s++) m.tets[tp++] = v[s];
+                }
+    // Boundary triangles with outward right-hand normals, 2 per face quad,
+    // split along the diagonal through the quad's lowest corner.
+    auto add_quad = [&](int a, int b, int c, int d, int bc) {
+        // quad a-b-c-d counter-clockwise seen from outside; diagonal a-c
+        m.tris.push_back(a); m.tris.push_back(b); m.tris.push_back(c); m.tri_bc.push_back(bc);
+        m.tris.push_back(a); m.tris.push_back(c); m.tris.push_back(d); m.tri_bc.push_back(bc);
+    };
+    for (int k = 0; k < nz; k++)
+        for (int j = 0; j < ny; j++) {
+            // x = 0 face, outward -x: (j,k) plane seen from -x
+            add_quad(nid(0, j, k), nid(0, j, k + 1), nid(0, j + 1, k + 1), nid(0, j + 1, k), face_bc[0]);
+            add_quad(nid(nx, j, k), nid(nx, j + 1, k), nid(nx, j + 1, k + 1), nid(nx, j, k + 1), face_bc[1]);
+        }
+    for (int k = 0; k < nz; k++)
+        for (int i = 0; i < nx; i++) {
+            add_quad(nid(i, 0, k), nid(i + 1, 0, k), nid(i + 1, 0, k + 1), nid(i, 0, k + 1), face_bc[2]);
+            add_quad(nid(i, ny, k), nid(i, ny, k + 1), nid(i + 1, ny, k + 1), nid(i + 1, ny, k), face_bc[3]);
+        }
+    for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) {
+            add_quad(nid(i, j, 0), nid(i, j + 1, 0), nid(i + 1, j + 1, 0), nid(i + 1, j, 0), face_bc[4]);
+            add_quad(nid(i, j, nz), nid(i + 1, j, nz), nid(i + 1, j + 1, nz), nid(i, j + 1, nz), face_bc[5]);
+        }
+    if (renumber) {
+        std::vector<int> ia, ja;
+        build_graph(m.nnode, m.tets, ia, ja);
+        std::vector<int> perm = rcm_order(m.nnode, ia, ja);  // perm[new] = old
+        std::vector<int> inv(m.nnode);
+        for (int i = 0; i < m.nnode; i++) inv[perm[i]] = i;
+        std::vector<double> c2(m.coords.size());
+        for (int i = 0; i < m.nnode; i++)
+            for (int d = 0; d < 3; d++) c2[3 * (size_t)i + d] = m.coords[3 * (size_t)perm[i] + d];
+        m.coords.swap(c2);
+        for (auto &v : m.tets) v = inv[v];
+        for (auto &v : m.tris) v = inv[v];
+    }
+    return build_dual(m);
+}
+
+int build_from_cells(HostMesh &m, int nnode, const double *coords, int64_t ntet, const int *tets,
+                     int64_t ntri, const int *tris, const int *tri_bc) {
+    m = HostMesh();
+    m.nnode = nnode;
+    m.coords.assign(coords, coords + 3 * (size_t)nnode);
+    m.tets.assign(tets, tets + 4 * ntet);
+    m.tris.assign(tris, tris + 3 * ntri);
+    m.tri_bc.assign(tri_bc, tri_bc + ntri);
+    for (int v : m.tets)
+        if (v < 0 || v >= nnode) return CFD_ERR_MESH;
+    for (int v : m.tris)
+        if (v < 0 || v >= nnode) return CFD_ERR_MESH;
+    return build_dual(m);
+}
+
+// UGRID ASCII writer in the layout UGrid_Reader parses (Euler3D/src/MeshIO.cpp:50-216):
+// counts line, coordinates, 1-based triangles, tags, 1-based tets.  The reader
+// reverses triangle winding (MeshIO.cpp:22-45), so triangles are written with
+// their outward right-hand normal, as this builder stores them.
+int write_ugrid(const HostMesh &m, const char *path, const int *tri_tag) {
+    FILE *f = std::fopen(path, "w");
+    if (!f) return CFD_ERR_IO;
+    const int64_t ntri = (int64_t)m.tris.size() / 3, ntet = (int64_t)m.tets.size() / 4;
+    std::fprintf(f, "%d %lld 0 %lld 0 0 0\n", m.nnode, (long long)ntri, (long long)ntet);
+    for (int i = 0; i < m.nnode; i++)
+        std::fprintf(f, "%.17g %.17g %.17g\n", m.coords[3 * (size_t)i], m.coords[3 * (size_t)i + 1],
+                     m.coords[3 * (size_t)i + 2]);
+    for (int64_t t = 0; t < ntri; t++)
+        std::fprintf(f, "%d %d %d\n", m.tris[3 * t] + 1, m.tris[3 * t + 1] + 1, m.tris[3 * t + 2] + 1);
+    for (int64_t t = 0; t < ntri; t++) std::fprintf(f, "%d\n", tri_tag ? tri_tag[t] : 1);
+    for (int64_t t = 0; t < ntet; t++)
+        std::fprintf(f, "%d %d %d %d\n", m.tets[4 * t] + 1, m.tets[4 * t + 1] + 1, m.tets[4 * t + 2] + 1,
+                     m.tets[4 * t + 3] + 1);
+    std::fclose(f);
+    return CFD_OK;
+}
+
+}  // namespace cfd

@@ -1,0 +1,305 @@
+/* cfd_b200.h -- C ABI of the B200-native implicit edge-based finite-volume
+ * hot path (node-centred median-dual Euler solver: flux residual, 5x5
+ * block-CRS Jacobian, block-CRS linear solves).
+ *
+ * Everything here is plain C: opaque handles, plain pointers and sizes, int
+ * status codes.  No CUDA, C++ or torch types cross this boundary, so the
+ * reference's C++ drivers (or ctypes, cgo, ...) can bind it directly.
+ *
+ * Data layout at the boundary is the reference's:
+ *   - node state Q: SoA, 5 arrays of nNode+nGhost doubles, conservative
+ *     variables (rho, rho*u, rho*v, rho*w, rho*et)
+ *     (Euler3D/include/Solver.h:27-31);
+ *   - interior edges: node[2] with node[0] < node[1] and the dual-face area
+ *     vector pointing from node[0] to node[1]
+ *     (Euler3D/include/Commons.h:97-105, Area_Volume.cpp:659-800);
+ *   - boundary edges: node[0] physical, node[1] = its private ghost node
+ *     (index >= nNode), outward area vector (Area_Volume.cpp:461-556,912);
+ *   - block CRS: IA (nNode+1), JA (sorted, diagonal included), IAU (diagonal
+ *     slot), A as [nnzb][5][5] row-major blocks, B and X as [nNode][5]
+ *     (MATH/include/MC.h:16-28, Euler3D/src/Solver.cpp:612-704).
+ *
+ * Status codes: CFD_OK (0) or a negative CFD_ERR_*.  A numerical failure
+ * detected on the device (NaN, negative density/pressure, Krylov breakdown)
+ * is reported as CFD_ERR_NUMERIC and, for the linear solves, as a NaN RMS,
+ * mirroring how the reference's drivers detect failure
+ * (Euler3D/src/Solver_Steady_Implicit.cpp:131-150).  No entry point aborts
+ * the process.
+ */
+#ifndef CFD_B200_H
+#define CFD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CFD_ABI_VERSION 1
+
+/* ------------------------------------------------------------ status codes */
+#define CFD_OK                 0
+#define CFD_ERR_ARG           -1  /* bad argument / size                     */
+#define CFD_ERR_MESH          -2  /* inconsistent mesh arrays                */
+#define CFD_ERR_CUDA          -3  /* CUDA runtime error (see cfd_last_error) */
+#define CFD_ERR_IO            -4  /* file I/O                                */
+#define CFD_ERR_STATE         -5  /* call out of order (e.g. no mesh yet)    */
+#define CFD_ERR_NUMERIC       -6  /* NaN / non-physical state on device      */
+#define CFD_ERR_NOT_CONVERGED -7  /* Krylov budget exhausted                 */
+#define CFD_ERR_UNSUPPORTED   -8  /* option not available on this path       */
+#define CFD_ERR_RANGE         -9  /* size beyond a fixed capacity            */
+
+/* ------------------------------------------- option values (reference enums)
+ * Numeric values equal the reference's enums in
+ * Euler3D/include/SolverParameters.h so parameter files map 1:1. */
+#define CFD_FLUX_ROE   0   /* FLUX_SCHEME_ROE  (SolverParameters.h:111) */
+#define CFD_FLUX_HLLC  1   /* FLUX_SCHEME_HLLC (SolverParameters.h:112) */
+#define CFD_FLUX_AUSM  2   /* FLUX_SCHEME_AUSM (:113); AUSM+ (Liou 1996), the reference's is an empty stub */
+
+#define CFD_ORDER_FIRST  0 /* SOLVER_ORDER_FIRST  (SolverParameters.h:316) */
+#define CFD_ORDER_SECOND 1 /* SOLVER_ORDER_SECOND (SolverParameters.h:317) */
+
+#define CFD_LIMITER_NONE  -1 /* LIMITER_METHOD_NONE           (:343) */
+#define CFD_LIMITER_BJ     0 /* LIMITER_METHOD_BERTH_JESPERSEN(:344) */
+#define CFD_LIMITER_VENKAT 1 /* LIMITER_METHOD_VENKATAKRISHNAN(:345) */
+
+#define CFD_GRAD_LSQ 0   /* least squares (Euler3D/src/Gradient.cpp:232) */
+#define CFD_GRAD_GG  1   /* Green-Gauss on the median dual (enum only in the reference, :329) */
+
+#define CFD_BC_EULER_WALL 0  /* BC_TYPE_* (SolverParameters.h:40-58) */
+#define CFD_BC_FAR_FIELD  1
+#define CFD_BC_INFLOW     2
+#define CFD_BC_OUTFLOW    3
+
+#define CFD_PREC_FP64 0  /* Jacobian / preconditioner storage precision */
+#define CFD_PREC_FP32 1
+#define CFD_PREC_BF16 2
+
+#define CFD_PC_NONE      0  /* GMRES right preconditioner */
+#define CFD_PC_BLOCK_JACOBI 1
+#define CFD_PC_ILU0      2
+
+/* Solver options; mirrors the reference parameter file keys named beside
+ * each field (Euler3D/src/SolverParameters.cpp:184-700). */
+typedef struct cfd_params {
+    int    flux_scheme;      /* FLUX_SCHEME                  */
+    int    order;            /* SOLVER_ORDER                 */
+    int    limiter;          /* LIMITER_METHOD               */
+    int    limiter_order;    /* LIMITER_ORDER (0 first, 1 second) */
+    int    limiter_smooth;   /* LIMITER_SMOOTH               */
+    int    gradient;         /* CFD_GRAD_LSQ / CFD_GRAD_GG   */
+    int    ls_weight;        /* 0 unweighted, 1 inverse distance (Gradient.cpp:151) */
+    int    entropy_fix;      /* ENTROPY_FIX                  */
+    int    global_time;      /* TIME_INTEGRATION_TYPE == GLOBAL */
+    int    cfl_ramp;         /* CFL_RAMP                     */
+    int    mach_ramp;        /* MACH_RAMP                    */
+    int    zpg_iteration;    /* ZPG_ITERATION                */
+    double gamma;            /* GAMMA                        */
+    double mach;             /* REF_MACH (== MACH_MAX)       */
+    double mach_min;         /* MACH_MIN                     */
+    double alpha_deg;        /* REF_ALPHA (degrees)          */
+    double beta_deg;         /* REF_BETA  (degrees)          */
+    double cfl_min;          /* CFL_MIN                      */
+    double cfl_max;          /* CFL_MAX                      */
+    double venkat_k;         /* VENKAT_K_THRESHOLD           */
+} cfd_params;
+
+/* Fills p with the defaults used by the reference parameter files of this
+ * path (ideal gas, generic non-dimensionalisation, first-order Roe). */
+void cfd_params_default(cfd_params *p);
+
+/* ------------------------------------------------------------- lifecycle */
+typedef struct cfd_ctx cfd_ctx;
+
+int  cfd_abi_version(void);
+/* Text of the last error recorded on this thread (never NULL). */
+const char *cfd_last_error(void);
+
+int  cfd_create(int device, cfd_ctx **out);
+int  cfd_destroy(cfd_ctx *ctx);
+/* Run all work of ctx on this cudaStream_t (NULL = the legacy stream). */
+int  cfd_set_stream(cfd_ctx *ctx, void *cuda_stream);
+int  cfd_set_params(cfd_ctx *ctx, const cfd_params *p);
+int  cfd_synchronize(cfd_ctx *ctx);
+
+/* Install the median-dual mesh (host arrays, copied; the caller keeps
+ * ownership).  Replaces the device mirror of the reference globals
+ * nNode, nBNode, nEdge, intEdge, nBEdge, bndEdge, cVolume, coordXYZ,
+ * crs_IA/JA_Node2Node (Euler3D/include/Commons.h:64-105) and builds the
+ * block-CRS pattern of Create_CRS_SolverBlockMatrix (Solver.cpp:612-704).
+ *   edge_nodes  [2*nedge]   edge_areav  [3*nedge]
+ *   bedge_nodes [2*nbedge]  bedge_areav [3*nbedge]  bedge_type [nbedge]
+ *   cvol [nnode]  coords [3*nnode] (xyz interleaved, as coordXYZ)
+ *   n2n_ia [nnode+1]  n2n_ja [n2n_ia[nnode]]  (no diagonal) */
+int  cfd_set_mesh(cfd_ctx *ctx, int nnode, int nghost,
+                  int nedge, const int *edge_nodes, const double *edge_areav,
+                  int nbedge, const int *bedge_nodes, const double *bedge_areav,
+                  const int *bedge_type, const double *cvol, const double *coords,
+                  const int *n2n_ia, const int *n2n_ja);
+
+/* Block-CRS pattern built by cfd_set_mesh: sizes[0] = nnzb; IA/JA/IAU as
+ * SolverBlockMatrix (any pointer may be NULL to query sizes only). */
+int  cfd_get_block_pattern(cfd_ctx *ctx, int64_t *nnzb, int *IA, int *JA, int *IAU);
+
+/* ----------------------------------------------------------- state I/O */
+/* Q host SoA [5][nnode+nghost] <-> device. */
+int  cfd_set_state(cfd_ctx *ctx, const double *Q);
+int  cfd_get_state(cfd_ctx *ctx, double *Q);
+/* Device pointer of the resident state (SoA, leading dimension *ld >=
+ * nnode+nghost) for zero-copy callers. */
+int  cfd_state_device_ptr(cfd_ctx *ctx, double **dQ, int64_t *ld);
+/* Freestream state per node (Solver_Set_Initial_Conditions,
+ * Euler3D/src/Solver.cpp:339-393) on the device. */
+int  cfd_set_freestream(cfd_ctx *ctx);
+
+/* --------------------------------------------- hot path (device-resident)
+ * Each call is stream-ordered on the context's stream. */
+
+/* Per-iteration resets of Solver_Steady_Implicit.cpp:45-98: zero the residual
+ * / spectral-radius accumulators, reset extrema, evaluate the far field with
+ * Mach ramping (ComputeFarFieldCondition, Material.cpp:185-210). */
+int  cfd_begin_iteration(cfd_ctx *ctx, int iteration);
+/* Ghost-node states, characteristic BCs (Apply_Boundary_Condition,
+ * Euler3D/src/BC.cpp:1440-1487, 381-677). */
+int  cfd_apply_bc(cfd_ctx *ctx, int iteration);
+/* Node gradients of Q1..Q5 (Compute_Least_Square_Gradient,
+ * Euler3D/src/Gradient.cpp:232-296, or Green-Gauss). */
+int  cfd_gradient(cfd_ctx *ctx);
+/* Limiter (Compute_Limiter, Euler3D/src/Limiters.cpp:20-111). */
+int  cfd_limiter(cfd_ctx *ctx);
+/* Flux residual (Compute_Residual, Euler3D/src/Residual.cpp:18 ->
+ * FluxTest.cpp:7968 Roe / HLLC_Fluxes.cpp:519 HLLC / AUSM+).  Writes the
+ * convective and dissipative residuals separately (Res*, Res*_Diss), and when
+ * add_time != 0 accumulates sum(area*lambda_max) per node and the
+ * eigenvalue extrema. */
+int  cfd_residual(cfd_ctx *ctx, int add_time);
+/* Local time step dt_i = V_i*CFL/sum (Compute_DeltaT, Time_Step.cpp:23-51). */
+int  cfd_deltat(cfd_ctx *ctx, int iteration);
+/* RMS of the residual as Solver_Steady_Implicit.cpp:107-126: out[0..4]
+ * per equation, out[5] = RMS_Res.  include_diss adds Res_Diss first
+ * (MPFLOW3D semantics). */
+int  cfd_residual_rms(cfd_ctx *ctx, int include_diss, double out[6]);
+
+/* Approximate first-order Roe Jacobian + right-hand side
+ * (Compute_Jacobian, Euler3D/src/Jacobian.cpp:18 ->
+ * Roe_Jacobian.cpp:29-228).  B = -(Res + include_diss*Res_Diss);
+ * diagonal += V/dt when add_time.  precision: CFD_PREC_FP64/FP32/BF16 storage
+ * of A (the FP64 copy is always kept for the defect correction). */
+int  cfd_jacobian(cfd_ctx *ctx, int add_time, int include_diss, int precision);
+
+/* Block Gauss-Seidel with LU-factored diagonal blocks, X = 0 start
+ * (MC_Iterative_Block_LU_Jacobi_CRS, MATH/src/MC_Iterative_Jacobi.c:346-535):
+ * direction 0 forward, 1 backward, 2 alternating.  Level-scheduled on the
+ * device, same row order and arithmetic as the reference.  *rms = RMS of the
+ * last sweep's residual. */
+int  cfd_block_gs(cfd_ctx *ctx, int iterations, int direction, double *rms);
+
+typedef struct cfd_gmres_opts {
+    int    restart;        /* Krylov dimension m (30)                       */
+    int    max_iters;      /* total inner iterations budget                 */
+    double rtol;           /* relative residual target, e.g. 1e-6           */
+    int    precond;        /* CFD_PC_*                                      */
+    int    precision;      /* CFD_PREC_* of the preconditioner / A copy     */
+    int    refine;         /* FP64 outer iterative-refinement sweeps (>=1)   */
+} cfd_gmres_opts;
+
+typedef struct cfd_gmres_stats {
+    int    iterations;     /* inner iterations done                          */
+    int    restarts;
+    int    refinements;
+    double rel_residual;   /* ||B - A X|| / ||B|| in FP64 at exit            */
+} cfd_gmres_stats;
+
+void cfd_gmres_default(cfd_gmres_opts *o);
+/* Solves A X = B (A, B from cfd_jacobian) with right-preconditioned
+ * restarted GMRES; FP64 Arnoldi with compensated dot products.  The
+ * reference has no block GMRES on this path (its MPI scalar GMRES,
+ * MATH/src/ParallelLinearAlgebra.cpp:27-278, is unused); this is the solver
+ * the implicit drivers call in its place. */
+int  cfd_gmres(cfd_ctx *ctx, const cfd_gmres_opts *o, cfd_gmres_stats *st);
+
+/* Q += relax * X on physical nodes (Solver_Steady_Implicit.cpp:153-159). */
+int  cfd_update(cfd_ctx *ctx, double relax);
+
+/* -------------------------------------------------------------- readback */
+int  cfd_get_residual(cfd_ctx *ctx, double *conv, double *diss);  /* [5][nnode] each */
+int  cfd_get_deltat(cfd_ctx *ctx, double *dt);                    /* [nnode] */
+/* {minL1,maxL1,minL4,maxL4,minL5,maxL5,minDt,maxDt}, DBL_MAX/DBL_MIN when unset */
+int  cfd_get_extrema(cfd_ctx *ctx, double out[8]);
+/* Far field {rho,u,v,w,et,p,c,mach} of the last cfd_begin_iteration. */
+int  cfd_get_farfield(cfd_ctx *ctx, double out[8]);
+int  cfd_get_gradients(cfd_ctx *ctx, double *g);                  /* [15][nnode] */
+int  cfd_get_limiters(cfd_ctx *ctx, double *phi);                 /* [5][nnode]  */
+/* A [nnzb][25] (FP64 copy), B [nnode][5], X [nnode][5]; NULL skips. */
+int  cfd_get_system(cfd_ctx *ctx, double *A, double *B, double *X);
+/* Replace A/B (host, FP64) -- lets a caller solve a system assembled elsewhere. */
+int  cfd_set_system(cfd_ctx *ctx, const double *A, const double *B);
+
+/* ------------------------------------------- fused steps and whole solves */
+/* One residual evaluation of the hot path: begin_iteration + BC + (gradient
+ * + limiter when second order) + residual + deltat.  With Q_host != NULL the
+ * state is copied in first and, with conv_host/diss_host != NULL, the
+ * residuals are copied back (the end-to-end form of the call). */
+int  cfd_residual_step(cfd_ctx *ctx, int iteration, const double *Q_host,
+                       double *conv_host, double *diss_host);
+
+typedef struct cfd_solve_opts {
+    int    max_iterations;   /* SOLVER_NITERATION                         */
+    double drop;             /* stop when RMS <= drop * RMS(first), e.g. 1e-8 */
+    int    include_diss;     /* 1: B = -(Res+Res_Diss) (MPFLOW3D), 0: Euler3D */
+    int    linear_solver;    /* 0 block GS sweeps, 1 GMRES                 */
+    int    linear_iters;     /* LINEAR_SOLVER_NITERATION / GMRES budget    */
+    double relax;            /* SOLVER_RELAXATION                          */
+    cfd_gmres_opts gmres;
+} cfd_solve_opts;
+
+typedef struct cfd_solve_stats {
+    int    iterations;
+    double rms_first;
+    double rms_last;
+    int    linear_iterations;  /* summed over the solve                   */
+    int    status;
+} cfd_solve_stats;
+
+/* Implicit steady solve (Solver_Steady_Implicit, Euler3D/src/
+ * Solver_Steady_Implicit.cpp:35-184) entirely on the device. */
+int  cfd_solve_steady(cfd_ctx *ctx, const cfd_solve_opts *o, cfd_solve_stats *st);
+
+/* ----------------------------------------------------- host mesh builder */
+typedef struct cfd_mesh cfd_mesh;
+
+/* Tet-split box of nx*ny*nz hexes (6 tets each) over [0,lx]x[0,ly]x[0,lz],
+ * interior nodes jittered by U(+-jitter*h) from seed, optional reverse
+ * Cuthill-McKee renumbering, face BC types {xmin,xmax,ymin,ymax,zmin,zmax}.
+ * Median-dual metrics as Calculate_Area_Volume (Area_Volume.cpp:903). */
+int  cfd_mesh_box(int nx, int ny, int nz, double lx, double ly, double lz,
+                  double jitter, uint64_t seed, int rcm, const int face_bc[6],
+                  cfd_mesh **out);
+/* Same from explicit cells: tets [4*ntet] positively oriented, boundary
+ * triangles [3*ntri] with outward right-hand normals, tri_bc [ntri]. */
+int  cfd_mesh_from_cells(int nnode, const double *coords, int64_t ntet, const int *tets,
+                         int64_t ntri, const int *tris, const int *tri_bc, cfd_mesh **out);
+/* sizes: {nnode, nghost, nedge, nbedge, ntet, ntri, n2n_nnz} */
+int  cfd_mesh_sizes(const cfd_mesh *m, int64_t sizes[7]);
+/* Copies out the arrays cfd_set_mesh takes (any pointer may be NULL). */
+int  cfd_mesh_export(const cfd_mesh *m, int *edge_nodes, double *edge_areav,
+                     int *bedge_nodes, double *bedge_areav, int *bedge_type,
+                     double *cvol, double *coords, int *n2n_ia, int *n2n_ja);
+int  cfd_mesh_export_cells(const cfd_mesh *m, int *tets, int *tris, int *tri_bc);
+/* UGRID ASCII in the layout of UGrid_Reader (Euler3D/src/MeshIO.cpp:50). */
+int  cfd_mesh_write_ugrid(const cfd_mesh *m, const char *path);
+/* Convenience: cfd_set_mesh from a builder mesh. */
+int  cfd_set_mesh_from(cfd_ctx *ctx, const cfd_mesh *m);
+void cfd_mesh_free(cfd_mesh *m);
+
+/* ------------------------------------------------- restart file (binary)
+ * Byte-compatible with Restart_Writer / Restart_Reader
+ * (Euler3D/src/RestartIO.cpp:45-179): int32 {iteration, nNode, nBNode, 5}
+ * then (nNode+nBNode) rows of 5 doubles. */
+int  cfd_restart_write(const char *path, int iteration, int nnode, int nghost, const double *Q);
+int  cfd_restart_read(const char *path, int *iteration, int nnode, int nghost, double *Q);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CFD_B200_H */

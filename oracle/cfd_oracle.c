@@ -1,0 +1,883 @@
+/* CPU restatement of the reference's implicit edge-based FV hot path.
+ * TEST INFRASTRUCTURE ONLY -- the checker of the CUDA path, never part of the
+ * product.  See cfd_oracle.h.  Every routine cites the reference lines it
+ * restates (paths relative to the reference's Trunk/).
+ */
+#include "cfd_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define IDX(v, i, ld) ((size_t)(v) * (size_t)(ld) + (size_t)(i))
+
+static double dmin(double a, double b) { return a < b ? a : b; }
+static double dmax(double a, double b) { return a > b ? a : b; }
+
+/* Vector3D::normalize / magnitude (MATH/src/Vector3D.cpp:216-229) */
+static void unit(const double *a, double *n, double *mag) {
+    double m = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    n[0] = a[0]; n[1] = a[1]; n[2] = a[2];
+    if (m > 1.0e-20) { n[0] = a[0] / m; n[1] = a[1] / m; n[2] = a[2] / m; }
+    *mag = m;
+}
+
+/* ComputeFarFieldCondition, generic non-dimensionalisation
+ * (Euler3D/src/Material.cpp:112-210). */
+void orc_farfield(const orc_params *p, double out[8]) {
+    double R = 1.0 / p->gamma, rho = 1.0, T = p->gamma, pr = R * rho * T;
+    double a = p->alpha_deg * M_PI / 180.0, b = p->beta_deg * M_PI / 180.0;
+    double c = sqrt(p->gamma * R * T);
+    double u = p->mach * c * cos(a) * cos(b), v = p->mach * c * sin(a), w = p->mach * c * sin(b) * cos(a);
+    double q2 = u * u + v * v + w * w;
+    out[0] = rho; out[1] = u; out[2] = v; out[3] = w;
+    out[4] = pr / ((p->gamma - 1.0) * rho) + 0.5 * q2;
+    out[5] = pr; out[6] = c; out[7] = p->mach;
+}
+
+typedef struct { double rho, u, v, w, et, p, ht, ubar, c; } face_t;
+
+/* Compute_EOS_Variables_Face, conservative branch (Material.cpp:216-248). */
+static void eos_face(const double *q, double nx, double ny, double nz, double g, face_t *s) {
+    s->rho = q[0];
+    s->u = q[1] / s->rho;
+    s->v = q[2] / s->rho;
+    s->w = q[3] / s->rho;
+    s->et = q[4] / s->rho;
+    double q2 = s->u * s->u + s->v * s->v + s->w * s->w;
+    s->p = (g - 1.0) * (s->rho * s->et - 0.5 * s->rho * q2);
+    s->ht = (s->rho * s->et + s->p) / s->rho;
+    s->c = sqrt((g * s->p) / s->rho);
+    s->ubar = s->u * nx + s->v * ny + s->w * nz;
+}
+
+/* Characteristic BC ghost state (Compute_Characteristic_BoundaryCondition_New,
+ * Euler3D/src/BC.cpp:381-677), conservative variables.  Returns nonzero where
+ * the reference would abort. */
+static int bc_state(const double *qI, const double *qG, const double *areav, int type, const orc_params *p,
+                    const double *inf, double *qB) {
+    double n[3], mag;
+    unit(areav, n, &mag);
+    face_t I, G, O;
+    double q0[5];
+    eos_face(qI, n[0], n[1], n[2], p->gamma, &I);
+    eos_face(qG, n[0], n[1], n[2], p->gamma, &G);
+    for (int k = 0; k < 5; k++) q0[k] = 0.5 * (qI[k] + qG[k]);
+    eos_face(q0, n[0], n[1], n[2], p->gamma, &O);
+    double l1 = O.ubar, l4 = l1 + O.c, l5 = l1 - O.c;
+    double pb = inf[5], rb = inf[0], ub = inf[1], vb = inf[2], wb = inf[3];
+    double outflow_p = 0.935 * inf[5];
+    int inst = -1, st = 0;
+    switch (type) {
+        case 0: inst = 0; break;
+        case 1:
+            if (l1 <= 0.0 && l4 <= 0.0 && l5 <= 0.0) inst = 10;
+            else if (l1 >= 0.0 && l4 >= 0.0 && l5 >= 0.0) inst = 11;
+            else if (l1 >= 0.0 && l5 <= 0.0 && l4 >= 0.0) inst = 9;
+            else if (l1 <= 0.0 && l4 >= 0.0 && l5 <= 0.0) inst = 8;
+            else st = 2;
+            break;
+        case 2:
+            if (l1 <= 0.0 && l4 >= 0.0 && l5 <= 0.0) inst = 4;
+            else if (l1 <= 0.0 && l4 <= 0.0 && l5 <= 0.0) inst = 6;
+            else inst = fabs(l1) < O.c ? 4 : 6;
+            break;
+        case 3:
+            if (l1 >= 0.0 && l5 <= 0.0 && l4 >= 0.0) inst = 5;
+            else if (l1 >= 0.0 && l4 >= 0.0 && l5 >= 0.0) inst = 7;
+            else inst = fabs(l1) < O.c ? 5 : 7;
+            break;
+        default: inst = type; break;
+    }
+    switch (inst) {
+        case 0:
+            pb = I.p + O.rho * O.c * I.ubar;
+            if (p->iteration < p->zpg_iteration && pb < 0.0) pb = I.p;
+            rb = I.rho + (pb - I.p) / (O.c * O.c);
+            ub = I.u - n[0] * (pb - I.p) / (O.rho * O.c);
+            vb = I.v - n[1] * (pb - I.p) / (O.rho * O.c);
+            wb = I.w - n[2] * (pb - I.p) / (O.rho * O.c);
+            break;
+        case 5: case 9:
+            pb = inst == 5 ? outflow_p : inf[5];
+            rb = I.rho + (pb - I.p) / (O.c * O.c);
+            ub = I.u - n[0] * (pb - I.p) / (O.rho * O.c);
+            vb = I.v - n[1] * (pb - I.p) / (O.rho * O.c);
+            wb = I.w - n[2] * (pb - I.p) / (O.rho * O.c);
+            break;
+        case 7: case 11:
+            pb = I.p; rb = I.rho; ub = I.u; vb = I.v; wb = I.w;
+            break;
+        case 8: {
+            double t = n[0] * (inf[1] - I.u) + n[1] * (inf[2] - I.v) + n[2] * (inf[3] - I.w);
+            pb = 0.5 * (inf[5] + I.p - O.rho * O.c * t);
+            rb = inf[0] + (pb - inf[5]) / (O.c * O.c);
+            ub = inf[1] + n[0] * (pb - inf[5]) / (O.rho * O.c);
+            vb = inf[2] + n[1] * (pb - inf[5]) / (O.rho * O.c);
+            wb = inf[3] + n[2] * (pb - inf[5]) / (O.rho * O.c);
+        } break;
+        default: break;
+    }
+    if (pb < 0.0) st = st ? st : 1;
+    double et = ub * ub + vb * vb + wb * wb;
+    et = pb / ((p->gamma - 1.0) * rb) + 0.5 * et;   /* Get_TotalEnergy, Material.cpp:1012-1040 */
+    qB[0] = rb; qB[1] = rb * ub; qB[2] = rb * vb; qB[3] = rb * wb; qB[4] = rb * et;
+    return st;
+}
+
+/* Apply_Characteristic_Boundary_Condition (BC.cpp:1440-1487). */
+void orc_apply_bc(const orc_mesh *m, const orc_params *p, double *Q) {
+    const int ld = m->nnode + m->nghost;
+    double inf[8];
+    orc_farfield(p, inf);
+    for (int b = 0; b < m->nbedge; b++) {
+        int L = m->bn[2 * b], R = m->bn[2 * b + 1];
+        double qI[5], qG[5], qB[5];
+        for (int k = 0; k < 5; k++) { qI[k] = Q[IDX(k, L, ld)]; qG[k] = Q[IDX(k, R, ld)]; }
+        bc_state(qI, qG, m->ba + 3 * (size_t)b, m->bt[b], p, inf, qB);
+        for (int k = 0; k < 5; k++) Q[IDX(k, R, ld)] = qB[k];
+    }
+}
+
+/* Roe_EntropyFix (Euler3D/src/Roe_EntropyFix.cpp:19-59). */
+static void entropy_fix(double ubL, double cL, double ubR, double cR, double ub, double c, double E[3]) {
+    E[0] = fabs(ub);
+    double lL = ubL + cL, lR = ubR + cR, l = ub + c;
+    double eps = 4.0 * dmax(0.0, dmax(l - lL, lR - l));
+    E[1] = fabs(l) < eps ? (l * l + eps * eps) / (2.0 * eps) : fabs(l);
+    lL = ubL - cL; lR = ubR - cR; l = ub - c;
+    eps = 4.0 * dmax(0.0, dmax(l - lL, lR - l));
+    E[2] = fabs(l) < eps ? (l * l + eps * eps) / (2.0 * eps) : fabs(l);
+}
+
+/* Compute_Flux_Roe_Optimized (Euler3D/src/FluxTest.cpp:3026-3200). */
+static double roe(const double *qL, const double *qR, const double *n, double area, const orc_params *p,
+                  double *conv, double *diss, double lam[3]) {
+    face_t L, R;
+    double g = p->gamma;
+    eos_face(qL, n[0], n[1], n[2], g, &L);
+    eos_face(qR, n[0], n[1], n[2], g, &R);
+    double FL[5], FR[5];
+    FL[0] = L.rho * L.ubar; FL[1] = L.u * FL[0] + L.p * n[0]; FL[2] = L.v * FL[0] + L.p * n[1];
+    FL[3] = L.w * FL[0] + L.p * n[2]; FL[4] = L.ht * FL[0];
+    FR[0] = R.rho * R.ubar; FR[1] = R.u * FR[0] + R.p * n[0]; FR[2] = R.v * FR[0] + R.p * n[1];
+    FR[3] = R.w * FR[0] + R.p * n[2]; FR[4] = R.ht * FR[0];
+    double rho = sqrt(R.rho * L.rho), sigma = rho / (L.rho + rho);
+    double u = L.u + sigma * (R.u - L.u), v = L.v + sigma * (R.v - L.v), w = L.w + sigma * (R.w - L.w);
+    double ht = L.ht + sigma * (R.ht - L.ht);
+    double phi = 0.5 * (g - 1.0) * (u * u + v * v + w * w);
+    double c = sqrt((g - 1.0) * ht - phi);   /* Get_SpeedSound, Material.cpp:939-960 */
+    double ub = u * n[0] + v * n[1] + w * n[2];
+    double E[3];
+    if (p->entropy_fix) entropy_fix(L.ubar, L.c, R.ubar, R.c, ub, c, E);
+    else { E[0] = fabs(ub); E[1] = fabs(ub + c); E[2] = fabs(ub - c); }
+    lam[0] = E[0]; lam[1] = E[1]; lam[2] = E[2];
+    /* M = dQ/dq_RUP (Compute_Transformation_Conservative_To_RUP, Material.cpp:1172-1236) */
+    double M[5][5] = {{1, 0, 0, 0, 0}, {u, rho, 0, 0, 0}, {v, 0, rho, 0, 0}, {w, 0, 0, rho, 0},
+                      {phi / (g - 1.0), rho * u, rho * v, rho * w, 1.0 / (g - 1.0)}};
+    double dQ[5] = {R.rho - L.rho, R.u - L.u, R.v - L.v, R.w - L.w, R.p - L.p};
+    double E0 = E[0], E1 = E[1], E2 = E[2];
+    double dU = dQ[1] * n[0] + dQ[2] * n[1] + dQ[3] * n[2];
+    double dw[5];
+    dw[0] = E0 * dQ[0] + (E1 + E2 - 2.0 * E0) * dQ[4] / (2.0 * c * c) + rho * (E1 - E2) * dU / (2.0 * c);
+    for (int k = 1; k < 4; k++)
+        dw[k] = E0 * dQ[k] + 0.5 * n[k - 1] * dU * ((E1 + E2) - 2.0 * E0) + n[k - 1] * (E1 - E2) * dQ[4] / (2.0 * rho * c);
+    dw[4] = 0.5 * dQ[4] * (E1 + E2) + 0.5 * rho * c * dU * (E1 - E2);
+    for (int i = 0; i < 5; i++) {
+        double fa = 0.0;   /* MC_Matrix_Mul_Vector (MATH/src/MC_Iterative_Jacobi.c:174-187) */
+        for (int j = 0; j < 5; j++) fa += M[i][j] * dw[j];
+        conv[i] = 0.5 * (FL[i] + FR[i]) * area;
+        diss[i] = -0.5 * fa * area;
+    }
+    return dmax(E0, dmax(E1, E2));
+}
+
+/* Compute_HLLCFlux (Euler3D/src/HLLC_Fluxes.cpp:143-326). */
+static double hllc(const double *qL, const double *qR, const double *n, double area, const orc_params *p,
+                   double *conv, double *diss) {
+    face_t L, R;
+    double g = p->gamma;
+    eos_face(qL, n[0], n[1], n[2], g, &L);
+    eos_face(qR, n[0], n[1], n[2], g, &R);
+    double rho = sqrt(R.rho * L.rho), sigma = rho / (L.rho + rho);
+    double u = L.u + sigma * (R.u - L.u), v = L.v + sigma * (R.v - L.v), w = L.w + sigma * (R.w - L.w);
+    double ht = L.ht + sigma * (R.ht - L.ht);
+    double phi = 0.5 * (g - 1.0) * (u * u + v * v + w * w);
+    double c = sqrt((g - 1.0) * ht - phi);
+    double ub = u * n[0] + v * n[1] + w * n[2];
+    double lmax = dmax(fabs(ub), dmax(fabs(ub + c), fabs(ub - c)));
+    double SL = dmin(L.ubar - L.c, ub - c), SR = dmax(R.ubar + R.c, ub + c);
+    double SM = (R.rho * R.ubar * (SR - R.ubar) - L.rho * L.ubar * (SL - L.ubar) + L.p - R.p) /
+                (R.rho * (SR - R.ubar) - L.rho * (SL - L.ubar));
+    double F[5];
+    const face_t *S = 0;
+    double Sk = 0.0;
+    if (SL > 0.0 || SR < 0.0) {
+        S = SL > 0.0 ? &L : &R;
+        F[0] = S->rho * S->ubar; F[1] = S->u * F[0] + S->p * n[0]; F[2] = S->v * F[0] + S->p * n[1];
+        F[3] = S->w * F[0] + S->p * n[2]; F[4] = S->ht * F[0];
+    } else {
+        if (SM > 0.0) { S = &L; Sk = SL; } else { S = &R; Sk = SR; }
+        double pstar = S->p + S->rho * (S->ubar - Sk) * (S->ubar - SM);
+        double om = 1.0 / (Sk - SM), c1 = Sk - S->ubar, c2 = pstar - S->p;
+        double rs = om * (c1 * S->rho), rus = om * (c1 * S->rho * S->u + c2 * n[0]);
+        double rvs = om * (c1 * S->rho * S->v + c2 * n[1]), rws = om * (c1 * S->rho * S->w + c2 * n[2]);
+        double res = om * (c1 * S->rho * S->et - S->p * S->ubar + pstar * SM);
+        F[0] = rs * SM; F[1] = rus * SM + pstar * n[0]; F[2] = rvs * SM + pstar * n[1];
+        F[3] = rws * SM + pstar * n[2]; F[4] = (res + pstar) * SM;
+    }
+    for (int k = 0; k < 5; k++) { conv[k] = F[k] * area; diss[k] = 0.0; }
+    return lmax;
+}
+
+/* AUSM+ restated from Liou, J. Comput. Phys. 129 (1996) 364-382: c_1/2 =
+ * min(c^_L, c^_R), c^ = c*^2/max(c*, |u|), c*^2 = 2(g-1)/(g+1) H; M+-(M)
+ * degree-4 polynomials with beta = 1/8, P+-(M) degree-5 with alpha = 3/16.
+ * (The reference's AUSM is an empty stub, Euler3D/src/AUSM_Fluxes.cpp:45-54.) */
+static double ausmp(const double *qL, const double *qR, const double *n, double area, const orc_params *p,
+                    double *conv, double *diss) {
+    face_t L, R;
+    double g = p->gamma;
+    eos_face(qL, n[0], n[1], n[2], g, &L);
+    eos_face(qR, n[0], n[1], n[2], g, &R);
+    double k = 2.0 * (g - 1.0) / (g + 1.0);
+    double csL = sqrt(k * L.ht), csR = sqrt(k * R.ht);
+    double c12 = dmin(csL * csL / dmax(csL, L.ubar), csR * csR / dmax(csR, -R.ubar));
+    double ML = L.ubar / c12, MR = R.ubar / c12;
+    double Mp, Pp, Mm, Pm;
+    if (fabs(ML) >= 1.0) { Mp = 0.5 * (ML + fabs(ML)); Pp = ML > 0.0 ? 1.0 : 0.0; }
+    else {
+        Mp = 0.25 * (ML + 1.0) * (ML + 1.0) + 0.125 * (ML * ML - 1.0) * (ML * ML - 1.0);
+        Pp = 0.25 * (ML + 1.0) * (ML + 1.0) * (2.0 - ML) + (3.0 / 16.0) * ML * (ML * ML - 1.0) * (ML * ML - 1.0);
+    }
+    if (fabs(MR) >= 1.0) { Mm = 0.5 * (MR - fabs(MR)); Pm = MR < 0.0 ? 1.0 : 0.0; }
+    else {
+        Mm = -0.25 * (MR - 1.0) * (MR - 1.0) - 0.125 * (MR * MR - 1.0) * (MR * MR - 1.0);
+        Pm = 0.25 * (MR - 1.0) * (MR - 1.0) * (2.0 + MR) - (3.0 / 16.0) * MR * (MR * MR - 1.0) * (MR * MR - 1.0);
+    }
+    double m12 = Mp + Mm, mp = 0.5 * (m12 + fabs(m12)), mm = 0.5 * (m12 - fabs(m12));
+    double p12 = Pp * L.p + Pm * R.p;
+    double aL = c12 * mp * L.rho, aR = c12 * mm * R.rho;
+    conv[0] = area * (aL + aR);
+    conv[1] = area * (aL * L.u + aR * R.u + p12 * n[0]);
+    conv[2] = area * (aL * L.v + aR * R.v + p12 * n[1]);
+    conv[3] = area * (aL * L.w + aR * R.w + p12 * n[2]);
+    conv[4] = area * (aL * L.ht + aR * R.ht);
+    for (int j = 0; j < 5; j++) diss[j] = 0.0;
+    double rho = sqrt(R.rho * L.rho), sigma = rho / (L.rho + rho);
+    double u = L.u + sigma * (R.u - L.u), v = L.v + sigma * (R.v - L.v), w = L.w + sigma * (R.w - L.w);
+    double ht = L.ht + sigma * (R.ht - L.ht);
+    double c = sqrt((g - 1.0) * ht - 0.5 * (g - 1.0) * (u * u + v * v + w * w));
+    return fabs(u * n[0] + v * n[1] + w * n[2]) + c;
+}
+
+/* Compute_SecondOrderReconstructQ (Euler3D/src/HigherOrderReconstructQ.cpp:21-72). */
+static void reconstruct(const orc_mesh *m, const orc_params *p, const double *Q, const double *grad,
+                        const double *phi, int a, int b, double *qa) {
+    const int ld = m->nnode + m->nghost, nn = m->nnode;
+    double frac = p->limiter_order == 1 ? 0.5 : 0.0;
+    double r[3];
+    for (int d = 0; d < 3; d++) r[d] = 0.5 * (m->xyz[3 * (size_t)b + d] - m->xyz[3 * (size_t)a + d]);
+    for (int k = 0; k < 5; k++) {
+        double ph = (p->limiter != -1 && phi) ? phi[IDX(k, a, nn)] : 1.0;
+        double gr = grad[IDX(3 * k, a, nn)] * r[0] + grad[IDX(3 * k + 1, a, nn)] * r[1] + grad[IDX(3 * k + 2, a, nn)] * r[2];
+        qa[k] = Q[IDX(k, a, ld)] + ph * (frac * (Q[IDX(k, b, ld)] - Q[IDX(k, a, ld)]) + (1.0 - frac) * gr);
+    }
+}
+
+/* Compute_Residual_Roe_New (FluxTest.cpp:7968-8151) / Compute_Residual_HLLC
+ * (HLLC_Fluxes.cpp:519-573): interior edges then boundary edges, scatter. */
+void orc_residual(const orc_mesh *m, const orc_params *p, const double *Q, const double *grad, const double *phi,
+                  double *conv, double *diss, double *dtsum, double ext[6]) {
+    const int ld = m->nnode + m->nghost, nn = m->nnode;
+    memset(conv, 0, sizeof(double) * 5 * nn);
+    memset(diss, 0, sizeof(double) * 5 * nn);
+    memset(dtsum, 0, sizeof(double) * nn);
+    ext[0] = ext[2] = ext[4] = DBL_MAX;
+    ext[1] = ext[3] = ext[5] = DBL_MIN;
+    for (int pass = 0; pass < 2; pass++) {
+        int ne = pass == 0 ? m->nedge : m->nbedge;
+        const int *en = pass == 0 ? m->en : m->bn;
+        const double *ea = pass == 0 ? m->ea : m->ba;
+        for (int e = 0; e < ne; e++) {
+            int L = en[2 * e], R = en[2 * e + 1];
+            double n[3], area, qL[5], qR[5], fc[5], fd[5], lam[3] = {0, 0, 0}, lmax;
+            unit(ea + 3 * (size_t)e, n, &area);
+            if (pass == 0 && p->order == 1) {
+                reconstruct(m, p, Q, grad, phi, L, R, qL);
+                reconstruct(m, p, Q, grad, phi, R, L, qR);
+            } else {
+                for (int k = 0; k < 5; k++) { qL[k] = Q[IDX(k, L, ld)]; qR[k] = Q[IDX(k, R, ld)]; }
+            }
+            if (p->flux == 1) lmax = hllc(qL, qR, n, area, p, fc, fd);
+            else if (p->flux == 2) lmax = ausmp(qL, qR, n, area, p, fc, fd);
+            else {
+                lmax = roe(qL, qR, n, area, p, fc, fd, lam);
+                ext[0] = dmin(ext[0], lam[0]); ext[1] = dmax(ext[1], lam[0]);
+                ext[2] = dmin(ext[2], lam[1]); ext[3] = dmax(ext[3], lam[1]);
+                ext[4] = dmin(ext[4], lam[2]); ext[5] = dmax(ext[5], lam[2]);
+            }
+            dtsum[L] += area * lmax;
+            if (R < nn) dtsum[R] += area * lmax;
+            for (int k = 0; k < 5; k++) {
+                conv[IDX(k, L, nn)] += fc[k];
+                diss[IDX(k, L, nn)] += fd[k];
+                if (pass == 0) {
+                    conv[IDX(k, R, nn)] -= fc[k];
+                    diss[IDX(k, R, nn)] -= fd[k];
+                }
+            }
+        }
+    }
+}
+
+/* Compute_DeltaT (Euler3D/src/Time_Step.cpp:23-51); p->cfl is the ramped CFL. */
+void orc_deltat(const orc_mesh *m, const orc_params *p, double *dt, double ext2[2]) {
+    ext2[0] = DBL_MAX;
+    ext2[1] = DBL_MIN;
+    for (int i = 0; i < m->nnode; i++) {
+        dt[i] = m->vol[i] * p->cfl / dt[i];
+        ext2[0] = dmin(ext2[0], dt[i]);
+        ext2[1] = dmax(ext2[1], dt[i]);
+    }
+    if (p->global_time)
+        for (int i = 0; i < m->nnode; i++) dt[i] = ext2[0];
+}
+
+/* Least-squares coefficients and gradient (Euler3D/src/Gradient.cpp:137-296). */
+void orc_gradient_lsq(const orc_mesh *m, const orc_params *p, const double *Q, double *grad) {
+    const int ld = m->nnode + m->nghost, nn = m->nnode;
+    for (int i = 0; i < nn; i++) {
+        double r11 = 0, r12 = 0, r13 = 0, r22 = 0, r23 = 0, r33 = 0, ro22 = 0, ro33 = 0;
+        const double *xi = m->xyz + 3 * (size_t)i;
+        for (int pass = 0; pass < 4; pass++) {
+            for (int k = m->ia[i]; k < m->ia[i + 1]; k++) {
+                int j = m->ja[k];
+                const double *xj = m->xyz + 3 * (size_t)j;
+                double dx = xj[0] - xi[0], dy = xj[1] - xi[1], dz = xj[2] - xi[2];
+                double a = p->ls_weight ? 1.0 / sqrt(dx * dx + dy * dy + dz * dz) : 1.0;
+                dx *= a; dy *= a; dz *= a;
+                if (pass == 0) { r11 += dx * dx; r12 += dx * dy; r13 += dx * dz; }
+                else if (pass == 1) {
+                    double t = dy - (r12 / r11) * dx;
+                    r22 += t * t; r23 += t * dz; ro22 += t * dy;
+                } else if (pass == 2) {
+                    double t = dz - (r13 / r11) * dx - (r23 / r22) * (dy - (r12 / r11) * dx);
+                    r33 += t * t; ro33 += t * dz;
+                } else {
+                    double Wz = (dz - (r13 / r11) * dx - (r23 / r22) * (dy - (r12 / r11) * dx)) / ro33;
+                    double Wy = (dy - (r12 / r11) * dx - r23 * Wz) / ro22;
+                    double Wx = (dx - r12 * Wy - r13 * Wz) / r11;
+                    for (int v = 0; v < 5; v++) {
+                        double d = Q[IDX(v, j, ld)] - Q[IDX(v, i, ld)];
+                        if (k == m->ia[i]) {
+                            grad[IDX(3 * v, i, nn)] = grad[IDX(3 * v + 1, i, nn)] = grad[IDX(3 * v + 2, i, nn)] = 0.0;
+                        }
+                        grad[IDX(3 * v, i, nn)] += Wx * a * d;
+                        grad[IDX(3 * v + 1, i, nn)] += Wy * a * d;
+                        grad[IDX(3 * v + 2, i, nn)] += Wz * a * d;
+                    }
+                }
+            }
+        }
+        (void)r33;
+    }
+}
+
+/* Green-Gauss on the median dual (restated: the reference only declares the
+ * option, SolverParameters.h:329): grad_i = (1/V_i) sum_j (Q_j - Q_i)/2 S_ij
+ * over interior dual faces; boundary dual faces carry Q_i and drop out. */
+void orc_gradient_gg(const orc_mesh *m, const double *Q, double *grad) {
+    const int ld = m->nnode + m->nghost, nn = m->nnode;
+    memset(grad, 0, sizeof(double) * 15 * nn);
+    for (int e = 0; e < m->nedge; e++) {
+        int L = m->en[2 * e], R = m->en[2 * e + 1];
+        const double *S = m->ea + 3 * (size_t)e;
+        for (int v = 0; v < 5; v++) {
+            double h = 0.5 * (Q[IDX(v, R, ld)] - Q[IDX(v, L, ld)]);
+            for (int d = 0; d < 3; d++) {
+                grad[IDX(3 * v + d, L, nn)] += h * S[d];
+                grad[IDX(3 * v + d, R, nn)] += h * S[d];
+            }
+        }
+    }
+    for (int i = 0; i < nn; i++)
+        for (int k = 0; k < 15; k++) grad[IDX(k, i, nn)] /= m->vol[i];
+}
+
+/* Compute_Limiter (Euler3D/src/Limiters.cpp:20-111) with Venkatakrishnan
+ * (:185-267) or Barth-Jespersen (:117-178), the pressure correction
+ * (:273-304) and, for the Roe flux, the sequential Roe-average pressure
+ * correction (:61-110, :311-356). */
+void orc_limiter(const orc_mesh *m, const orc_params *p, const double *Q, const double *grad, double *phi) {
+    const int ld = m->nnode + m->nghost, nn = m->nnode;
+    const double frac = p->limiter_order == 1 ? 0.5 : 0.0;
+    for (int i = 0; i < nn; i++)
+        for (int v = 0; v < 5; v++) phi[IDX(v, i, nn)] = 1.0;
+    for (int i = 0; i < nn; i++) {
+        double ph[5] = {1, 1, 1, 1, 1}, qmin[5], qmax[5], qc[5];
+        for (int v = 0; v < 5; v++) qc[v] = qmin[v] = qmax[v] = Q[IDX(v, i, ld)];
+        double eps2 = pow(p->venkat_k, 3.0);
+        eps2 = 6.0 * eps2 * m->vol[i] / M_PI;
+        for (int k = m->ia[i]; k < m->ia[i + 1]; k++)
+            for (int v = 0; v < 5; v++) {
+                qmin[v] = dmin(qmin[v], Q[IDX(v, m->ja[k], ld)]);
+                qmax[v] = dmax(qmax[v], Q[IDX(v, m->ja[k], ld)]);
+            }
+        for (int k = m->ia[i]; k < m->ia[i + 1]; k++) {
+            int j = m->ja[k];
+            double r[3];
+            for (int d = 0; d < 3; d++) r[d] = 0.5 * (m->xyz[3 * (size_t)j + d] - m->xyz[3 * (size_t)i + d]);
+            for (int v = 0; v < 5; v++) {
+                double gr = grad[IDX(3 * v, i, nn)] * r[0] + grad[IDX(3 * v + 1, i, nn)] * r[1] + grad[IDX(3 * v + 2, i, nn)] * r[2];
+                double q = qc[v] + frac * (Q[IDX(v, j, ld)] - qc[v]) + (1.0 - frac) * gr;
+                double dm = q - qc[v];
+                if (p->limiter == 1) {
+                    if (dm != 0.0) {
+                        double dp = (dm > 0.0 ? qmax[v] : qmin[v]) - qc[v];
+                        double t = (dp * dp + eps2) + 2.0 * (dm * dp);
+                        t = t / (dp * dp + 2.0 * dm * dm + dm * dp + eps2);
+                        ph[v] = dmin(ph[v], t);
+                    } else ph[v] = dmin(ph[v], 1.0);
+                } else {
+                    if (dm > 0.0) ph[v] = dmin(ph[v], dmin(1.0, (qmax[v] - qc[v]) / dm));
+                    else if (dm < 0.0) ph[v] = dmin(ph[v], dmin(1.0, (qmin[v] - qc[v]) / dm));
+                    else ph[v] = dmin(ph[v], 1.0);
+                }
+                ph[v] = dmax(0.0, ph[v]);
+            }
+        }
+        if (p->limiter_smooth) {
+            for (int v = 1; v < 5; v++) ph[0] = dmin(ph[0], ph[v]);
+            for (int v = 1; v < 5; v++) ph[v] = ph[0];
+        }
+        for (int k = m->ia[i]; k < m->ia[i + 1]; k++) {
+            int j = m->ja[k];
+            double r[3], q[5];
+            for (int d = 0; d < 3; d++) r[d] = 0.5 * (m->xyz[3 * (size_t)j + d] - m->xyz[3 * (size_t)i + d]);
+            for (int v = 0; v < 5; v++) {
+                double gr = grad[IDX(3 * v, i, nn)] * r[0] + grad[IDX(3 * v + 1, i, nn)] * r[1] + grad[IDX(3 * v + 2, i, nn)] * r[2];
+                q[v] = qc[v] + ph[v] * (frac * (Q[IDX(v, j, ld)] - qc[v]) + (1.0 - frac) * gr);
+            }
+            double pc = (p->gamma - 1.0) * (q[4] - (0.5 / q[0]) * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]));
+            if (pc < 0.0)
+                for (int v = 0; v < 5; v++) ph[v] = 0.0;
+        }
+        for (int v = 0; v < 5; v++) phi[IDX(v, i, nn)] = ph[v];
+    }
+    if (p->flux != 0) return;
+    for (int i = 0; i < nn; i++) {
+        for (int k = m->ia[i]; k < m->ia[i + 1]; k++) {
+            int j = m->ja[k];
+            double r[3], qa[5], qb[5];
+            for (int d = 0; d < 3; d++) r[d] = 0.5 * (m->xyz[3 * (size_t)j + d] - m->xyz[3 * (size_t)i + d]);
+            for (int v = 0; v < 5; v++) {
+                double gi = grad[IDX(3 * v, i, nn)] * r[0] + grad[IDX(3 * v + 1, i, nn)] * r[1] + grad[IDX(3 * v + 2, i, nn)] * r[2];
+                double gj = -(grad[IDX(3 * v, j, nn)] * r[0] + grad[IDX(3 * v + 1, j, nn)] * r[1] + grad[IDX(3 * v + 2, j, nn)] * r[2]);
+                double ci = Q[IDX(v, i, ld)], cj = Q[IDX(v, j, ld)];
+                qa[v] = ci + phi[IDX(v, i, nn)] * (frac * (cj - ci) + (1.0 - frac) * gi);
+                qb[v] = cj + phi[IDX(v, j, nn)] * (frac * (ci - cj) + (1.0 - frac) * gj);
+            }
+            /* Compute_RoeVariables (Roe_Fluxes.cpp:3609-3633) */
+            face_t A, B;
+            eos_face(qa, 0, 0, 0, p->gamma, &A);
+            eos_face(qb, 0, 0, 0, p->gamma, &B);
+            double rho = sqrt(B.rho * A.rho), sg = rho / (A.rho + rho);
+            double u = A.u + sg * (B.u - A.u), v = A.v + sg * (B.v - A.v), w = A.w + sg * (B.w - A.w);
+            double ht = A.ht + sg * (B.ht - A.ht);
+            double qr[5] = {rho, rho * u, rho * v, rho * w,
+                            (rho / p->gamma) * (ht + 0.5 * (p->gamma - 1.0) * (u * u + v * v + w * w))};
+            double pr = (p->gamma - 1.0) * (qr[4] - (0.5 / qr[0]) * (qr[1] * qr[1] + qr[2] * qr[2] + qr[3] * qr[3]));
+            if (pr < 0.0)
+                for (int v2 = 0; v2 < 5; v2++) { phi[IDX(v2, i, nn)] = 0.0; phi[IDX(v2, j, nn)] = 0.0; }
+        }
+    }
+}
+
+/* Create_CRS_SolverBlockMatrix pattern (Euler3D/src/Solver.cpp:612-672). */
+long orc_block_pattern(const orc_mesh *m, int *IA, int *JA, int *IAU) {
+    long nnz = 0;
+    for (int i = 0; i < m->nnode; i++) nnz += m->ia[i + 1] - m->ia[i] + 1;
+    if (!IA) return nnz;
+    IA[0] = 0;
+    for (int i = 0; i < m->nnode; i++) {
+        int k = IA[i], n0 = k;
+        JA[k++] = i;
+        for (int q = m->ia[i]; q < m->ia[i + 1]; q++) JA[k++] = m->ja[q];
+        /* selection sort as the reference does */
+        for (int a = n0; a < k; a++) {
+            int mi = a;
+            for (int b = a + 1; b < k; b++) if (JA[b] < JA[mi]) mi = b;
+            int t = JA[a]; JA[a] = JA[mi]; JA[mi] = t;
+            if (JA[a] == i) IAU[i] = a;
+        }
+        IA[i + 1] = k;
+    }
+    return nnz;
+}
+
+/* ConservativeEulerFluxJacobian (Euler3D/src/CompressibleUtils.cpp:558-609). */
+static void flux_jac(const double *q, const double *n, double g, double J[5][5]) {
+    double rho = q[0], u = q[1] / rho, v = q[2] / rho, w = q[3] / rho, rhoet = q[4];
+    double ek = 0.5 * (u * u + v * v + w * w), p = (g - 1.0) * (rhoet - rho * ek), ht = (rhoet + p) / rho;
+    double ub = u * n[0] + v * n[1] + w * n[2];
+    double nx = n[0], ny = n[1], nz = n[2];
+    J[0][0] = 0.0; J[1][0] = (g - 1.0) * ek * nx - u * ub; J[2][0] = (g - 1.0) * ek * ny - v * ub;
+    J[3][0] = (g - 1.0) * ek * nz - w * ub; J[4][0] = ((g - 1.0) * ek - ht) * ub;
+    J[0][1] = nx; J[1][1] = ub - (g - 2.0) * u * nx; J[2][1] = v * nx - (g - 1.0) * u * ny;
+    J[3][1] = w * nx - (g - 1.0) * u * nz; J[4][1] = ht * nx - (g - 1.0) * u * ub;
+    J[0][2] = ny; J[1][2] = u * ny - (g - 1.0) * v * nx; J[2][2] = ub - (g - 2.0) * v * ny;
+    J[3][2] = w * ny - (g - 1.0) * v * nz; J[4][2] = ht * ny - (g - 1.0) * v * ub;
+    J[0][3] = nz; J[1][3] = u * nz - (g - 1.0) * w * nx; J[2][3] = v * nz - (g - 1.0) * w * ny;
+    J[3][3] = ub - (g - 2.0) * w * nz; J[4][3] = ht * nz - (g - 1.0) * w * ub;
+    J[0][4] = 0.0; J[1][4] = (g - 1.0) * nx; J[2][4] = (g - 1.0) * ny; J[3][4] = (g - 1.0) * nz; J[4][4] = g * ub;
+}
+
+static void mm5(double A[5][5], double B[5][5], double C[5][5]) {
+    for (int i = 0; i < 5; i++)
+        for (int j = 0; j < 5; j++) {
+            C[i][j] = 0.0;
+            for (int k = 0; k < 5; k++) C[i][j] += A[i][k] * B[k][j];
+        }
+}
+
+/* Compute_RoeAJacobian: |A| = M P |Lambda| P^-1 M^-1 (Euler3D/src/Roe_Fluxes.cpp:149-273). */
+static void roe_absA(const double *qL, const double *qR, const double *n, const orc_params *p, double A[5][5]) {
+    face_t L, R;
+    double g = p->gamma;
+    eos_face(qL, n[0], n[1], n[2], g, &L);
+    eos_face(qR, n[0], n[1], n[2], g, &R);
+    double rho = sqrt(R.rho * L.rho), sigma = rho / (L.rho + rho);
+    double u = L.u + sigma * (R.u - L.u), v = L.v + sigma * (R.v - L.v), w = L.w + sigma * (R.w - L.w);
+    double ht = L.ht + sigma * (R.ht - L.ht);
+    double phi = 0.5 * (g - 1.0) * (u * u + v * v + w * w);
+    double c = sqrt((g - 1.0) * ht - phi);
+    double ub = u * n[0] + v * n[1] + w * n[2];
+    double nx = n[0], ny = n[1], nz = n[2];
+    double M[5][5] = {{1, 0, 0, 0, 0}, {u, rho, 0, 0, 0}, {v, 0, rho, 0, 0}, {w, 0, 0, rho, 0},
+                      {phi / (g - 1.0), rho * u, rho * v, rho * w, 1.0 / (g - 1.0)}};
+    double Mi[5][5] = {{1, 0, 0, 0, 0}, {-u / rho, 1.0 / rho, 0, 0, 0}, {-v / rho, 0, 1.0 / rho, 0, 0},
+                       {-w / rho, 0, 0, 1.0 / rho, 0}, {phi, -u * (g - 1.0), -v * (g - 1.0), -w * (g - 1.0), g - 1.0}};
+    double P[5][5] = {{nx, ny, nz, rho / c, rho / c}, {0.0, -nz, ny, nx, -nx}, {nz, 0.0, -nx, ny, -ny},
+                      {-ny, nx, 0.0, nz, -nz}, {0.0, 0.0, 0.0, rho * c, rho * c}};
+    double Pi[5][5] = {{nx, 0.0, nz, -ny, -nx / (c * c)}, {ny, -nz, 0.0, nx, -ny / (c * c)},
+                       {nz, ny, -nx, 0.0, -nz / (c * c)}, {0.0, 0.5 * nx, 0.5 * ny, 0.5 * nz, 1.0 / (2.0 * rho * c)},
+                       {0.0, -0.5 * nx, -0.5 * ny, -0.5 * nz, 1.0 / (2.0 * rho * c)}};
+    double E[3];
+    if (p->entropy_fix) entropy_fix(L.ubar, L.c, R.ubar, R.c, ub, c, E);
+    else { E[0] = fabs(ub); E[1] = fabs(ub + c); E[2] = fabs(ub - c); }
+    double Lm[5][5] = {{0}};
+    Lm[0][0] = Lm[1][1] = Lm[2][2] = E[0]; Lm[3][3] = E[1]; Lm[4][4] = E[2];
+    double T[5][5], Ti[5][5], LT[5][5];
+    mm5(M, P, T);
+    mm5(Pi, Mi, Ti);
+    mm5(Lm, Ti, LT);
+    mm5(T, LT, A);
+}
+
+/* Compute_Jacobian_Approximate_Roe (Euler3D/src/Roe_Jacobian.cpp:29-228);
+ * A is [nnzb][5][5] contiguous, B [nnode][5]. */
+void orc_jacobian(const orc_mesh *m, const orc_params *p, const double *Q, const double *dt, const double *conv,
+                  const double *diss, int add_time, int include_diss, const int *IA, const int *JA, const int *IAU,
+                  double *A, double *B) {
+    const int ld = m->nnode + m->nghost, nn = m->nnode;
+    memset(A, 0, sizeof(double) * 25 * (size_t)IA[nn]);
+    for (int i = 0; i < nn; i++) {
+        for (int k = 0; k < 5; k++)
+            B[5 * (size_t)i + k] = -(conv[IDX(k, i, nn)] + (include_diss ? diss[IDX(k, i, nn)] : 0.0));
+        if (add_time)
+            for (int k = 0; k < 5; k++) A[25 * (size_t)IAU[i] + 6 * k] = m->vol[i] / dt[i];
+    }
+    for (int pass = 0; pass < 2; pass++) {
+        int ne = pass == 0 ? m->nedge : m->nbedge;
+        const int *en = pass == 0 ? m->en : m->bn;
+        const double *ea = pass == 0 ? m->ea : m->ba;
+        for (int e = 0; e < ne; e++) {
+            int L = en[2 * e], R = en[2 * e + 1];
+            double n[3], area, qL[5], qR[5], JL[5][5], JR[5][5], Ab[5][5];
+            unit(ea + 3 * (size_t)e, n, &area);
+            for (int k = 0; k < 5; k++) { qL[k] = Q[IDX(k, L, ld)]; qR[k] = Q[IDX(k, R, ld)]; }
+            flux_jac(qL, n, p->gamma, JL);
+            flux_jac(qR, n, p->gamma, JR);
+            roe_absA(qL, qR, n, p, Ab);
+            double *dL = A + 25 * (size_t)IAU[L];
+            if (pass == 1) {
+                for (int a = 0; a < 5; a++)
+                    for (int b = 0; b < 5; b++) dL[5 * a + b] += 0.5 * (JL[a][b] + Ab[a][b]) * area;
+                continue;
+            }
+            int oL = -1, oR = -1;
+            for (int k = IA[L]; k < IA[L + 1]; k++) if (JA[k] == R) { oL = k; break; }
+            for (int k = IA[R]; k < IA[R + 1]; k++) if (JA[k] == L) { oR = k; break; }
+            double *dR = A + 25 * (size_t)IAU[R], *aL = A + 25 * (size_t)oL, *aR = A + 25 * (size_t)oR;
+            for (int a = 0; a < 5; a++)
+                for (int b = 0; b < 5; b++) {
+                    double fl = 0.5 * (JL[a][b] + Ab[a][b]) * area, fr = 0.5 * (JR[a][b] - Ab[a][b]) * area;
+                    dL[5 * a + b] += fl;
+                    dR[5 * a + b] -= fr;
+                    aL[5 * a + b] += fr;
+                    aR[5 * a + b] -= fl;
+                }
+        }
+    }
+}
+
+/* MC_Iterative_Block_LU_Jacobi_CRS (MATH/src/MC_Iterative_Jacobi.c:346-535). */
+double orc_block_gs(int n, const int *IA, const int *JA, const int *IAU, const double *A, const double *B, double *X,
+                    int iters, int direction) {
+    double *LU = (double *)malloc(sizeof(double) * 25 * (size_t)n);
+    double rms = 0.0;
+    memset(X, 0, sizeof(double) * 5 * (size_t)n);
+    for (int r = 0; r < n; r++) {
+        double *a = LU + 25 * (size_t)r;
+        memcpy(a, A + 25 * (size_t)IAU[r], sizeof(double) * 25);
+        for (int k = 0; k < 4; k++) {
+            for (int j = k + 1; j < 5; j++) a[5 * j + k] = a[5 * j + k] / a[5 * k + k];
+            for (int j = k + 1; j < 5; j++)
+                for (int i = k + 1; i < 5; i++) a[5 * i + j] -= a[5 * i + k] * a[5 * k + j];
+        }
+    }
+    if (iters <= 0) iters = 10000;
+    for (int it = 0; it < iters; it++) {
+        rms = 0.0;
+        int fwd = direction == 0 || (direction == 2 && it % 2 == 0);
+        for (int q = 0; q < n; q++) {
+            int r = fwd ? q : n - 1 - q;
+            double rhs[5], t[5];
+            for (int k = 0; k < 5; k++) rhs[k] = B[5 * (size_t)r + k];
+            for (int k = IA[r]; k < IA[r + 1]; k++) {
+                const double *a = A + 25 * (size_t)k, *x = X + 5 * (size_t)JA[k];
+                for (int ii = 0; ii < 5; ii++) {
+                    t[ii] = 0.0;
+                    for (int jj = 0; jj < 5; jj++) t[ii] += a[5 * ii + jj] * x[jj];
+                }
+                for (int ii = 0; ii < 5; ii++) rhs[ii] -= t[ii];
+            }
+            for (int k = 0; k < 5; k++) rms += rhs[k] * rhs[k];
+            const double *ad = A + 25 * (size_t)IAU[r], *xr = X + 5 * (size_t)r;
+            for (int ii = 0; ii < 5; ii++) {
+                t[ii] = 0.0;
+                for (int jj = 0; jj < 5; jj++) t[ii] += ad[5 * ii + jj] * xr[jj];
+            }
+            for (int ii = 0; ii < 5; ii++) rhs[ii] += t[ii];
+            const double *lu = LU + 25 * (size_t)r;
+            for (int ii = 0; ii < 5; ii++) {
+                t[ii] = rhs[ii];
+                for (int jj = 0; jj < ii; jj++) t[ii] -= lu[5 * ii + jj] * t[jj];
+            }
+            double *xo = X + 5 * (size_t)r;
+            for (int ii = 4; ii >= 0; ii--) {
+                xo[ii] = t[ii];
+                for (int jj = 4; jj > ii; jj--) xo[ii] -= lu[5 * ii + jj] * xo[jj];
+                xo[ii] = xo[ii] / lu[5 * ii + ii];
+            }
+        }
+        rms = sqrt(rms / (double)n);
+        if (rms < 100.0 * DBL_EPSILON) break;
+    }
+    free(LU);
+    return rms;
+}
+
+void orc_bspmv(int n, const int *IA, const int *JA, const double *A, const double *x, double *y) {
+    for (int r = 0; r < n; r++)
+        for (int a = 0; a < 5; a++) {
+            double s = 0.0;
+            for (int k = IA[r]; k < IA[r + 1]; k++)
+                for (int b = 0; b < 5; b++) s += A[25 * (size_t)k + 5 * a + b] * x[5 * (size_t)JA[k] + b];
+            y[5 * (size_t)r + a] = s;
+        }
+}
+
+/* 5x5 inverse, Gauss-Jordan with partial pivoting. */
+static int inv5(const double *in, double *out) {
+    double a[25];
+    memcpy(a, in, sizeof a);
+    for (int k = 0; k < 25; k++) out[k] = (k % 6 == 0) ? 1.0 : 0.0;
+    for (int c = 0; c < 5; c++) {
+        int p = c;
+        for (int r = c + 1; r < 5; r++) if (fabs(a[5 * r + c]) > fabs(a[5 * p + c])) p = r;
+        if (a[5 * p + c] == 0.0) return 1;
+        for (int j = 0; j < 5; j++) {
+            double t = a[5 * c + j]; a[5 * c + j] = a[5 * p + j]; a[5 * p + j] = t;
+            t = out[5 * c + j]; out[5 * c + j] = out[5 * p + j]; out[5 * p + j] = t;
+        }
+        double d = 1.0 / a[5 * c + c];
+        for (int j = 0; j < 5; j++) { a[5 * c + j] *= d; out[5 * c + j] *= d; }
+        for (int r = 0; r < 5; r++) {
+            if (r == c) continue;
+            double f = a[5 * r + c];
+            for (int j = 0; j < 5; j++) { a[5 * r + j] -= f * a[5 * c + j]; out[5 * r + j] -= f * out[5 * c + j]; }
+        }
+    }
+    return 0;
+}
+
+/* Block ILU(0), IKJ variant in natural row order (Saad, "Iterative Methods
+ * for Sparse Linear Systems", 2nd ed., Alg. 10.4, with 5x5 blocks): F holds
+ * the strictly lower L blocks, the strictly upper U blocks and inv(U_ii) on
+ * the diagonal. */
+int orc_ilu0(int n, const int *IA, const int *JA, const int *IAU, const double *A, double *F) {
+    memcpy(F, A, sizeof(double) * 25 * (size_t)IA[n]);
+    for (int i = 0; i < n; i++) {
+        for (int k = IA[i]; k < IAU[i]; k++) {
+            int p = JA[k];
+            double L[25], *Lip = F + 25 * (size_t)k;
+            const double *Dp = F + 25 * (size_t)IAU[p];
+            for (int a = 0; a < 5; a++)
+                for (int b = 0; b < 5; b++) {
+                    double s = 0.0;
+                    for (int q = 0; q < 5; q++) s += Lip[5 * a + q] * Dp[5 * q + b];
+                    L[5 * a + b] = s;
+                }
+            memcpy(Lip, L, sizeof L);
+            for (int mi = k + 1; mi < IA[i + 1]; mi++) {
+                int j = JA[mi];
+                for (int pk = IAU[p] + 1; pk < IA[p + 1]; pk++) {
+                    if (JA[pk] != j) continue;
+                    double *Aij = F + 25 * (size_t)mi;
+                    const double *U = F + 25 * (size_t)pk;
+                    for (int a = 0; a < 5; a++)
+                        for (int b = 0; b < 5; b++)
+                            for (int q = 0; q < 5; q++) Aij[5 * a + b] -= L[5 * a + q] * U[5 * q + b];
+                }
+            }
+        }
+        double inv[25];
+        if (inv5(F + 25 * (size_t)IAU[i], inv)) return 1;
+        memcpy(F + 25 * (size_t)IAU[i], inv, sizeof inv);
+    }
+    return 0;
+}
+
+static void ilu_apply(int n, const int *IA, const int *JA, const int *IAU, const double *F, const double *r,
+                      double *z) {
+    double *y = (double *)malloc(sizeof(double) * 5 * (size_t)n);
+    for (int i = 0; i < n; i++)
+        for (int a = 0; a < 5; a++) {
+            double s = r[5 * (size_t)i + a];
+            for (int k = IA[i]; k < IAU[i]; k++)
+                for (int b = 0; b < 5; b++) s -= F[25 * (size_t)k + 5 * a + b] * y[5 * (size_t)JA[k] + b];
+            y[5 * (size_t)i + a] = s;
+        }
+    for (int i = n - 1; i >= 0; i--) {
+        double t[5];
+        for (int a = 0; a < 5; a++) {
+            double s = y[5 * (size_t)i + a];
+            for (int k = IAU[i] + 1; k < IA[i + 1]; k++)
+                for (int b = 0; b < 5; b++) s -= F[25 * (size_t)k + 5 * a + b] * z[5 * (size_t)JA[k] + b];
+            t[a] = s;
+        }
+        const double *D = F + 25 * (size_t)IAU[i];
+        for (int a = 0; a < 5; a++) {
+            double s = 0.0;
+            for (int b = 0; b < 5; b++) s += D[5 * a + b] * t[b];
+            z[5 * (size_t)i + a] = s;
+        }
+    }
+    free(y);
+}
+
+static double dot(const double *a, const double *b, size_t n) {
+    double s = 0.0;
+    for (size_t i = 0; i < n; i++) s += a[i] * b[i];
+    return s;
+}
+
+/* Restarted right-preconditioned GMRES(m), modified Gram-Schmidt, Givens
+ * rotations (Saad, Alg. 9.5; the restart/Givens structure of the reference's
+ * unused ParallelSparseGMRES, MATH/src/ParallelLinearAlgebra.cpp:27-278).
+ * precond: 0 none, 1 block Jacobi, 2 block ILU(0).  X starts at zero. */
+int orc_gmres(int n, const int *IA, const int *JA, const int *IAU, const double *A, const double *B, double *X, int m,
+              int maxit, double rtol, int precond, int *iters, double *relres) {
+    const size_t N = 5 * (size_t)n;
+    double *F = NULL;
+    if (precond == 2) {
+        F = (double *)malloc(sizeof(double) * 25 * (size_t)IA[n]);
+        if (orc_ilu0(n, IA, JA, IAU, A, F)) { free(F); return 2; }
+    } else if (precond == 1) {
+        F = (double *)malloc(sizeof(double) * 25 * (size_t)n);
+        for (int i = 0; i < n; i++)
+            if (inv5(A + 25 * (size_t)IAU[i], F + 25 * (size_t)i)) { free(F); return 2; }
+    }
+    double *V = (double *)malloc(sizeof(double) * N * (m + 1));
+    double *w = (double *)malloc(sizeof(double) * N), *z = (double *)malloc(sizeof(double) * N);
+    double *H = (double *)calloc((size_t)(m + 1) * m, sizeof(double));
+    double *cs = (double *)malloc(sizeof(double) * m), *sn = (double *)malloc(sizeof(double) * m);
+    double *g = (double *)malloc(sizeof(double) * (m + 1)), *y = (double *)malloc(sizeof(double) * m);
+    memset(X, 0, sizeof(double) * N);
+    double bn = sqrt(dot(B, B, N));
+    int tot = 0, rc = 1;
+    if (bn == 0.0) { *iters = 0; *relres = 0.0; rc = 0; goto done; }
+#define PREC(in, out)                                                                         \
+    do {                                                                                      \
+        if (precond == 2) ilu_apply(n, IA, JA, IAU, F, in, out);                              \
+        else if (precond == 1)                                                                \
+            for (int i_ = 0; i_ < n; i_++)                                                    \
+                for (int a_ = 0; a_ < 5; a_++) {                                              \
+                    double s_ = 0.0;                                                          \
+                    for (int b_ = 0; b_ < 5; b_++) s_ += F[25 * (size_t)i_ + 5 * a_ + b_] * in[5 * (size_t)i_ + b_]; \
+                    out[5 * (size_t)i_ + a_] = s_;                                            \
+                }                                                                             \
+        else memcpy(out, in, sizeof(double) * N);                                             \
+    } while (0)
+    while (tot < maxit) {
+        orc_bspmv(n, IA, JA, A, X, w);
+        for (size_t i = 0; i < N; i++) w[i] = B[i] - w[i];
+        double beta = sqrt(dot(w, w, N));
+        *relres = beta / bn;
+        if (*relres <= rtol) { rc = 0; break; }
+        for (size_t i = 0; i < N; i++) V[i] = w[i] / beta;
+        for (int i = 0; i <= m; i++) g[i] = 0.0;
+        g[0] = beta;
+        int j = 0;
+        for (; j < m && tot < maxit; j++, tot++) {
+            PREC((V + N * j), z);
+            orc_bspmv(n, IA, JA, A, z, w);
+            for (int i = 0; i <= j; i++) {
+                double h = dot(w, V + N * i, N);
+                H[(size_t)i * m + j] = h;
+                for (size_t q = 0; q < N; q++) w[q] -= h * V[N * i + q];
+            }
+            double hn = sqrt(dot(w, w, N));
+            H[(size_t)(j + 1) * m + j] = hn;
+            if (hn > 0.0)
+                for (size_t q = 0; q < N; q++) V[N * (j + 1) + q] = w[q] / hn;
+            for (int i = 0; i < j; i++) {
+                double t = cs[i] * H[(size_t)i * m + j] + sn[i] * H[(size_t)(i + 1) * m + j];
+                H[(size_t)(i + 1) * m + j] = -sn[i] * H[(size_t)i * m + j] + cs[i] * H[(size_t)(i + 1) * m + j];
+                H[(size_t)i * m + j] = t;
+            }
+            double den = hypot(H[(size_t)j * m + j], H[(size_t)(j + 1) * m + j]);
+            cs[j] = H[(size_t)j * m + j] / den;
+            sn[j] = H[(size_t)(j + 1) * m + j] / den;
+            H[(size_t)j * m + j] = den;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            if (fabs(g[j + 1]) / bn <= rtol || hn == 0.0) { j++; tot++; break; }
+        }
+        for (int i = j - 1; i >= 0; i--) {
+            double s = g[i];
+            for (int k = i + 1; k < j; k++) s -= H[(size_t)i * m + k] * y[k];
+            y[i] = s / H[(size_t)i * m + i];
+        }
+        for (size_t q = 0; q < N; q++) {
+            double s = 0.0;
+            for (int i = 0; i < j; i++) s += y[i] * V[N * i + q];
+            w[q] = s;
+        }
+        PREC(w, z);
+        for (size_t q = 0; q < N; q++) X[q] += z[q];
+    }
+    orc_bspmv(n, IA, JA, A, X, w);
+    for (size_t i = 0; i < N; i++) w[i] = B[i] - w[i];
+    *relres = sqrt(dot(w, w, N)) / bn;
+    if (*relres <= rtol) rc = 0;
+    *iters = tot;
+#undef PREC
+done:
+    free(V); free(w); free(z); free(H); free(cs); free(sn); free(g); free(y);
+    if (F) free(F);
+    return rc;
+}

@@ -1,0 +1,57 @@
+/* CPU restatement of the reference's implicit edge-based FV hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the oracle the CUDA path is checked
+ * against; it is never linked into or called by the product library.  Plain
+ * C, FP64, sequential loops in the reference's order.  Parity of this
+ * restatement with the reference itself is pinned by tests/test_oracle_pin.py
+ * against the reference objects compiled in oracle/_ref.  Functions for
+ * methods the reference does not implement (Green-Gauss, AUSM+, block ILU(0),
+ * GMRES) are restated from the published methods; those are "parity unpinned"
+ * by the reference and are pinned by property tests (linear exactness,
+ * conservation, agreement with a dense direct solve).
+ */
+#ifndef CFD_ORACLE_H
+#define CFD_ORACLE_H
+
+typedef struct {
+    double gamma, mach, alpha_deg, beta_deg, cfl, venkat_k;
+    int flux, order, limiter, limiter_order, limiter_smooth, entropy_fix;
+    int global_time, ls_weight, gradient, iteration, zpg_iteration;
+} orc_params;
+
+typedef struct {
+    int nnode, nghost, nedge, nbedge;
+    const int *en;    /* [2*nedge]  L < R            */
+    const double *ea; /* [3*nedge]  area L -> R      */
+    const int *bn;    /* [2*nbedge] node, ghost      */
+    const double *ba; /* [3*nbedge] outward area     */
+    const int *bt;    /* [nbedge]   BC type          */
+    const double *vol;/* [nnode]                     */
+    const double *xyz;/* [3*nnode]  interleaved      */
+    const int *ia, *ja; /* node graph, no diagonal   */
+} orc_mesh;
+
+/* far field {rho,u,v,w,et,p,c,mach} */
+void orc_farfield(const orc_params *p, double out[8]);
+void orc_apply_bc(const orc_mesh *m, const orc_params *p, double *Q);
+void orc_gradient_lsq(const orc_mesh *m, const orc_params *p, const double *Q, double *grad);
+void orc_gradient_gg(const orc_mesh *m, const double *Q, double *grad);
+void orc_limiter(const orc_mesh *m, const orc_params *p, const double *Q, const double *grad, double *phi);
+/* conv/diss [5][nnode], dtsum [nnode], ext {min1,max1,min4,max4,min5,max5} */
+void orc_residual(const orc_mesh *m, const orc_params *p, const double *Q, const double *grad, const double *phi,
+                  double *conv, double *diss, double *dtsum, double ext[6]);
+/* dt: in = sum(area*lambda), out = time step; ext2 {min, max} */
+void orc_deltat(const orc_mesh *m, const orc_params *p, double *dt, double ext2[2]);
+/* block CRS pattern; returns nnzb (arrays may be NULL to query) */
+long orc_block_pattern(const orc_mesh *m, int *IA, int *JA, int *IAU);
+void orc_jacobian(const orc_mesh *m, const orc_params *p, const double *Q, const double *dt, const double *conv,
+                  const double *diss, int add_time, int include_diss, const int *IA, const int *JA, const int *IAU,
+                  double *A, double *B);
+double orc_block_gs(int n, const int *IA, const int *JA, const int *IAU, const double *A, const double *B, double *X,
+                    int iters, int direction);
+int orc_ilu0(int n, const int *IA, const int *JA, const int *IAU, const double *A, double *F);
+int orc_gmres(int n, const int *IA, const int *JA, const int *IAU, const double *A, const double *B, double *X,
+              int m, int maxit, double rtol, int precond, int *iters, double *relres);
+void orc_bspmv(int n, const int *IA, const int *JA, const double *A, const double *x, double *y);
+
+#endif

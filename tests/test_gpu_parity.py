@@ -1,0 +1,167 @@
+"""Parity of the CUDA path with the reference's own functions (the Euler3D
+objects compiled into oracle/_ref, run on the same mesh arrays and state).
+
+Tolerances (north star): residuals within 1e-12 relative in FP64 (normwise
+per equation, max |gpu - ref| / max |ref|); the same bound for ghost states,
+time steps, gradients, limiters and Jacobian blocks.  Block Gauss-Seidel on an
+identical system is bit-exact (level scheduling preserves the sequential
+row order and the kernel avoids fused multiply-adds).
+"""
+import numpy as np
+import pytest
+
+from cfdsolutions_b200 import Euler3DGPU
+from oracle import refharness
+from tests._util import CFG1, make_case, params_from, relerr, relerr_rows
+
+TOL = 1e-12
+
+pytestmark = pytest.mark.gpu
+
+
+def _first_order_steps():
+    return [("begin", 0), ("bc", 0), ("get", "state"), ("residual", 1), ("get", "residual"), ("get", "extrema"),
+            ("deltat", 0), ("get", "deltat"), ("get", "extrema"), ("get", "farfield"), ("jacobian", 1, 0),
+            ("get", "matrix"), ("gs", 10, 0), ("get", "matrix")]
+
+
+def _gpu_first_order(s: Euler3DGPU):
+    out = {}
+    s.begin_iteration(0)
+    s.Apply_Boundary_Condition(0)
+    out["state"] = s.get_state()
+    s.Compute_Residual(1)
+    out["conv"], out["diss"] = s.get_residual()
+    out["extrema_res"] = s.get_extrema()
+    s.Compute_DeltaT(0)
+    out["deltat"] = s.get_deltat()
+    out["extrema"] = s.get_extrema()
+    out["farfield"] = s.get_farfield()
+    s.Compute_Jacobian(1, 0)
+    out["A"], out["B"], _ = s.get_system()
+    out["gs_rms"] = s.MC_Iterative_Block_LU_Jacobi_CRS(10, 0)
+    _, _, out["X"] = s.get_system()
+    return out
+
+
+@pytest.mark.parametrize("n,rcm", [(6, False), (20, False), (12, True)])
+def test_first_order_roe_step_matches_reference(gpu_available, ref_available, n, rcm):
+    m, cfg, Q = make_case(n=n, seed=11 + n, rcm=rcm)
+    ref = refharness.run(m, cfg, Q, _first_order_steps())
+    with Euler3DGPU(m, params_from(cfg)) as s:
+        s.set_state(Q)
+        g = _gpu_first_order(s)
+        IA, JA, IAU = s.get_block_pattern()
+    # far field, ghost states
+    np.testing.assert_allclose(g["farfield"], ref["farfield"], rtol=1e-15, atol=0)
+    assert relerr_rows(g["state"], ref["state"]) <= 1e-14
+    # residuals (convective and dissipative kept separate, as Euler3D)
+    assert relerr_rows(g["conv"], ref["conv"]) <= TOL
+    assert relerr_rows(g["diss"], ref["diss"]) <= TOL
+    # time step and eigenvalue / time-step extrema
+    assert relerr(g["deltat"], ref["deltat"]) <= TOL
+    np.testing.assert_allclose(g["extrema"], ref["extrema"], rtol=1e-13, atol=0)
+    # Jacobian blocks and right-hand side, same block-CRS pattern
+    assert relerr(g["A"], ref["A"]) <= TOL
+    assert relerr(g["B"], ref["B"]) <= TOL
+    # block Gauss-Seidel: X within round-off of the reference solve of (almost) the same system
+    assert relerr(g["X"], ref["X"]) <= 1e-9
+    assert abs(g["gs_rms"] - ref["gs_rms"][0]) <= 1e-9 * abs(ref["gs_rms"][0])
+
+
+@pytest.mark.parametrize("direction", [0, 1, 2])
+def test_block_gauss_seidel_bit_exact(gpu_available, ref_available, direction):
+    m, cfg, Q = make_case(n=8, seed=5)
+    ref0 = refharness.run(m, cfg, Q, [("begin", 0), ("bc", 0), ("residual", 1), ("deltat", 0), ("jacobian", 1, 0),
+                                      ("get", "matrix")])
+    A, B = ref0["A"], ref0["B"]
+    ref = refharness.run(m, cfg, Q, [("set_matrix", A, B), ("gs", 7, direction), ("get", "matrix")])
+    with Euler3DGPU(m, params_from(cfg)) as s:
+        s.set_system(A.reshape(-1, 25), B)
+        rms = s.MC_Iterative_Block_LU_Jacobi_CRS(7, direction)
+        _, _, X = s.get_system()
+    np.testing.assert_array_equal(X, ref["X"])
+    assert abs(rms - ref["gs_rms"][0]) <= 1e-13 * abs(ref["gs_rms"][0])
+
+
+@pytest.mark.parametrize("flux", [0, 1])
+@pytest.mark.parametrize("limiter", [-1, 1])
+def test_second_order_lsq_residual_matches_reference(gpu_available, ref_available, flux, limiter):
+    cfg = dict(CFG1, flux_scheme=flux, order=1, limiter=limiter, limiter_order=1, venkat_k=5.0, mach=0.8,
+               mach_min=0.8, alpha_deg=1.25)
+    m, cfg, Q = make_case(n=10, seed=21, cfg=cfg)
+    steps = [("begin", 0), ("gradient", 0)]
+    if limiter != -1:
+        steps.append(("limiter",))
+    steps += [("bc", 0), ("residual", 1), ("get", "residual"), ("get", "gradients"), ("deltat", 0),
+              ("get", "deltat")]
+    if limiter != -1:
+        steps.append(("get", "limiters"))
+    ref = refharness.run(m, cfg, Q, steps)
+    with Euler3DGPU(m, params_from(cfg)) as s:
+        s.set_state(Q)
+        s.begin_iteration(0)
+        s.Compute_Least_Square_Gradient(0)
+        if limiter != -1:
+            s.Compute_Limiter()
+        s.Apply_Boundary_Condition(0)
+        s.Compute_Residual(1)
+        conv, diss = s.get_residual()
+        grad = s.get_gradients()
+        s.Compute_DeltaT(0)
+        dt = s.get_deltat()
+        phi = s.get_limiters() if limiter != -1 else None
+    assert relerr_rows(grad, ref["gradients"]) <= TOL
+    if limiter != -1:
+        assert np.abs(phi - ref["limiters"]).max() <= 1e-10
+    assert relerr_rows(conv, ref["conv"]) <= TOL
+    if flux == 0:
+        assert relerr_rows(diss, ref["diss"]) <= TOL
+    else:
+        assert np.abs(diss).max() == 0.0 and np.abs(ref["diss"]).max() == 0.0
+    assert relerr(dt, ref["deltat"]) <= TOL
+
+
+def test_hllc_first_order_and_entropy_fix(gpu_available, ref_available):
+    for cfg in (dict(CFG1, flux_scheme=1), dict(CFG1, entropy_fix=1)):
+        m, cfg, Q = make_case(n=8, seed=31, cfg=cfg)
+        ref = refharness.run(m, cfg, Q, [("begin", 0), ("bc", 0), ("residual", 1), ("get", "residual"),
+                                         ("deltat", 0), ("get", "deltat"), ("get", "extrema")])
+        with Euler3DGPU(m, params_from(cfg)) as s:
+            s.set_state(Q)
+            s.begin_iteration(0)
+            s.Apply_Boundary_Condition(0)
+            s.Compute_Residual(1)
+            conv, diss = s.get_residual()
+            s.Compute_DeltaT(0)
+            dt = s.get_deltat()
+            ext = s.get_extrema()
+        assert relerr_rows(conv, ref["conv"]) <= TOL
+        assert relerr_rows(diss, ref["diss"]) <= TOL if np.abs(ref["diss"]).max() > 0 else np.abs(diss).max() == 0
+        assert relerr(dt, ref["deltat"]) <= TOL
+        np.testing.assert_allclose(ext, ref["extrema"], rtol=1e-13)
+
+
+def test_implicit_iterations_track_reference(gpu_available, ref_available):
+    """Three implicit Euler3D iterations (BC, residual, dt, Jacobian, 10 block-GS
+    sweeps, update) on the device against the reference loop."""
+    m, cfg, Q = make_case(n=8, seed=41)
+    steps = []
+    for it in range(3):
+        steps += [("begin", it), ("bc", it), ("residual", 1), ("deltat", it), ("jacobian", 1, it), ("gs", 10, 0),
+                  ("update", 1.0)]
+    steps.append(("get", "state"))
+    ref = refharness.run(m, cfg, Q, steps)
+    with Euler3DGPU(m, params_from(cfg)) as s:
+        s.set_state(Q)
+        for it in range(3):
+            s.begin_iteration(it)
+            s.Apply_Boundary_Condition(it)
+            s.Compute_Residual(1)
+            s.Compute_DeltaT(it)
+            s.Compute_Jacobian(1, it)
+            s.MC_Iterative_Block_LU_Jacobi_CRS(10, 0)
+            s.update(1.0)
+        Qg = s.get_state()
+    k = m.nnode
+    assert relerr_rows(Qg[:, :k], ref["state"][:, :k]) <= 1e-10
