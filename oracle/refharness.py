@@ -104,6 +104,7 @@ def _quiet():
 def _session(mesh_arrays: dict, cfg: dict, Q: np.ndarray | None, steps: list, quiet: bool = True) -> dict:
     if quiet:
         _quiet()
+    os.chdir(tempfile.mkdtemp(prefix="cfdref_"))  # the reference writes Residual.res into the cwd
     lib = _load()
     with tempfile.TemporaryDirectory() as td:
         pf = Path(td) / "param.txt"
@@ -204,6 +205,7 @@ def run(mesh, cfg: dict, Q: np.ndarray | None, steps: list, quiet: bool = True, 
 
 def _ugrid_session(path: str, reorder: int) -> dict:
     _quiet()
+    os.chdir(tempfile.mkdtemp(prefix="cfdref_"))
     lib = _load()
     lib.ref_mesh_from_ugrid(path.encode(), reorder)
     sz = np.zeros(5, np.int32)
