@@ -1,0 +1,326 @@
+"""Benchmark of the hot path: second-order residual evaluation on the
+128^3-hex tet cube (2.15 M nodes, 14.8 M edges), RCM order, Green-Gauss
+gradients, Venkatakrishnan limiter (K = 5), Roe flux, M = 0.8, alpha = 1.25,
+gamma = 1.4, +-1 % seeded noise.  One step = one residual evaluation of the
+hot path: far-field reset, characteristic ghost update, gradients, limiter,
+flux residual, local time step.  HLLC and AUSM+ steps are timed beside it.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+value  = whole-job GEdges/s = (interior + boundary edges) x steps x ranks / max-over-ranks time,
+         state resident in HBM, CUDA events on the library's stream.
+e2e    = the same through the C ABI call cfd_residual_step with pinned host
+         buffers: state H2D and residuals D2H inside the timed region.
+--impl reference: the reference's own CPU code (Euler3D objects compiled from
+         its sources) on a bounded sample of the workload, one single-threaded
+         process per host core (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "residual GEdges/s (%HBM peak)"
+UNIT = "GEdges/s"
+CFG = dict(flux_scheme=0, order=1, limiter=1, limiter_order=0, gradient=1, venkat_k=5.0, gamma=1.4, mach=0.8,
+           mach_min=0.8, alpha_deg=1.25, cfl_min=10.0, cfl_max=10.0)
+FLUX_NAMES = {0: "roe", 1: "hllc", 2: "ausm+"}
+KERNELS_PER_STEP = 7  # begin, bc, gradient, limiter, roe pressure fix, residual, dt
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=128, help="hexes per side of the cube")
+    ap.add_argument("--cpu-sample-n", type=int, default=48, help="hexes per side of the CPU baseline sample")
+    ap.add_argument("--cpu-procs", type=int, default=0, help="reference processes (0 = one per core, max 16)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def algorithmic_bytes(nnode, nedge, nghost):
+    """Compulsory traffic of one second-order residual launch: edge nodes +
+    area (32 B/edge), node Q read + residual write + spectral radius (88 B/node),
+    boundary edge + ghost state (72 B/ghost), plus gradients, limiter and
+    coordinates read per node (184 B/node)."""
+    return 32 * nedge + 88 * nnode + 72 * nghost + 184 * nnode
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profile():
+    """DRAM bytes per residual launch from the committed ncu summary, scaled
+    per edge (None if not captured)."""
+    p = ROOT / "profiles" / "residual_roe2_128.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_edge:"):
+            return float(line.split(":")[1])
+    return None
+
+
+class Clocks:
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                try:
+                    rows.append((float(parts[0]), float(parts[1]), parts[3:7]))
+                except ValueError:
+                    pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "samples": len(rows), "reasons": reasons}
+
+
+def reference_throughput(sample_n, procs, warmup, steps):
+    """Reference CPU residual passes (LSQ gradient + Venkatakrishnan + Roe
+    residual + dt, its own second-order path) on a sample_n^3 cube, one
+    single-threaded reference process per core; returns (GEdges/s, details)."""
+    from cfdsolutions_b200 import box_mesh, perturbed_freestream
+    from oracle import refharness
+
+    m = box_mesh(sample_n, jitter=0.15, seed=1234, rcm=True)
+    Q = perturbed_freestream(m, CFG["gamma"], CFG["mach"], CFG["alpha_deg"], noise=0.01, seed=1235)
+    cfg = dict(CFG, gradient=0, scheme="explicit")
+    one = [("begin", 0), ("gradient", 0), ("limiter",), ("bc", 0), ("residual", 1), ("deltat", 0)]
+    steps_all = one * (warmup + steps)
+    outs = refharness.run_many(m, cfg, Q, steps_all, procs)
+    units = m.nedge + m.nbedge
+    rates, per_pass = [], []
+    for o in outs:
+        t = o["timings"]
+        tot = [sum(x) for x in zip(*(t[k] for k in ("begin", "gradient", "limiter", "bc", "residual", "deltat")))]
+        timed = tot[warmup:]
+        per_pass.append(statistics.mean(timed))
+        rates.append(units / statistics.mean(timed) / 1e9)
+    sample = (f"{sample_n}^3-hex tet cube ({m.nnode} nodes, {units} edges), {warmup}+{steps} passes of "
+              f"LSQ gradient + Venkatakrishnan + Roe residual + dt per process, {procs} concurrent "
+              f"single-threaded reference processes")
+    return sum(rates), dict(per_pass_s=statistics.mean(per_pass), procs=procs, sample=sample,
+                            per_process_gedges=statistics.mean(rates))
+
+
+def cpu_count():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    procs = args.cpu_procs or min(16, cpu_count())
+    val, d = reference_throughput(args.cpu_sample_n, procs, max(1, min(args.warmup, 3)), max(1, args.steps))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": d["per_pass_s"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(args.n),
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": procs, "kind": "reference", "sample": d["sample"]},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(n, mesh=None):
+    c = {"workload": f"second-order residual evaluation, {n}^3-hex tet cube (6 tets/hex), RCM, jitter 0.15h, "
+                     "Green-Gauss + Venkatakrishnan K=5 + Roe, M=0.8, alpha=1.25, +-1% noise",
+         "flux": "roe", "gradient": "green-gauss", "limiter": "venkatakrishnan", "venkat_k": 5.0, "mach": 0.8,
+         "alpha_deg": 1.25, "precision": "fp64", "parallelism": "replicas (one mesh per GPU)",
+         "l2": "inputs larger than L2 (resident working set > 126 MB)"}
+    if mesh is not None:
+        c.update(nodes=mesh.nnode, edges=mesh.nedge, ghosts=mesh.nghost)
+    return c
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+    dev = local
+    torch.cuda.set_device(dev)
+
+    from cfdsolutions_b200 import Euler3DGPU, box_mesh, default_params, perturbed_freestream
+
+    t0 = time.time()
+    mesh = box_mesh(args.n, jitter=0.15, seed=1234, rcm=True)
+    Q = perturbed_freestream(mesh, CFG["gamma"], CFG["mach"], CFG["alpha_deg"], noise=0.01, seed=1235)
+    setup_s = time.time() - t0
+    units = mesh.nedge + mesh.nbedge
+    stream = torch.cuda.Stream(device=dev)
+    s = Euler3DGPU(mesh, default_params(**CFG), device=dev, stream=stream.cuda_stream)
+    s.set_state(Q)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+
+    def timed(fn, k, w):
+        for i in range(w):
+            fn(i)
+        barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for i in range(k):
+            fn(w + i)
+        ev1.record(stream)
+        barrier()
+        ms = ev0.elapsed_time(ev1)
+        if world > 1:
+            t = torch.tensor([ms], device=f"cuda:{dev}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    # ---- headline: resident residual steps (Roe)
+    with Clocks(dev) as clk:
+        ms = timed(lambda i: s.residual_step(i), args.steps, args.warmup)
+    clocks = clk.summary()
+    ms_step = ms / args.steps
+    value = units * args.steps * world / (ms / 1e3) / 1e9
+
+    # ---- per-kernel breakdown of one step (events between calls)
+    names = ["begin", "bc", "gradient", "limiter", "residual", "deltat"]
+    calls = [lambda: s.begin_iteration(0), lambda: s.Apply_Boundary_Condition(0), s.Compute_Gradient,
+             s.Compute_Limiter, lambda: s.Compute_Residual(1), lambda: s.Compute_DeltaT(0)]
+    reps = max(3, args.steps // 2)
+    acc = {n: 0.0 for n in names}
+    for _ in range(reps):
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(len(calls) + 1)]
+        evs[0].record(stream)
+        for c, e in zip(calls, evs[1:]):
+            c()
+            e.record(stream)
+        torch.cuda.synchronize(dev)
+        for j, n in enumerate(names):
+            acc[n] += evs[j].elapsed_time(evs[j + 1])
+    breakdown = {n: acc[n] / reps for n in names}
+
+    # ---- roofline of the dominant kernel (flux residual), timed alone
+    ms_res = timed(lambda i: s.Compute_Residual(1), args.steps, args.warmup) / args.steps
+    peak, peak_kind = measured_peak()
+    abytes = algorithmic_bytes(mesh.nnode, mesh.nedge, mesh.nghost)
+    achieved = abytes / (ms_res / 1e3) / 1e9
+    tpe = traffic_from_profile()
+    roofline = {"bound": "hbm", "kernel": "k_residual_gather<ROE,SECOND>", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                "algorithmic_bytes_per_launch": abytes, "launch_ms": ms_res,
+                "traffic": (tpe * units) if tpe else None}
+
+    # ---- other flux families (HLLC, AUSM+)
+    per_flux = {"roe": {"gedges_per_s": value / world, "ms_per_step": ms_step}}
+    for fl in (1, 2):
+        s.set_params(default_params(**dict(CFG, flux_scheme=fl)))
+        msf = timed(lambda i: s.residual_step(i), args.steps, args.warmup)
+        per_flux[FLUX_NAMES[fl]] = {"gedges_per_s": units * args.steps / (msf / 1e3) / 1e9,
+                                    "ms_per_step": msf / args.steps}
+    s.set_params(default_params(**CFG))
+
+    # ---- end to end through the C ABI with pinned host buffers
+    qh = torch.from_numpy(np.ascontiguousarray(Q)).pin_memory()
+    conv = torch.empty((5, mesh.nnode), dtype=torch.float64).pin_memory()
+    diss = torch.empty((5, mesh.nnode), dtype=torch.float64).pin_memory()
+    qn, cn, dn = qh.numpy(), conv.numpy(), diss.numpy()
+    ms_e2e = timed(lambda i: s.residual_step(i, qn, out=(cn, dn)), args.steps, args.warmup)
+    e2e = {"value": units * args.steps * world / (ms_e2e / 1e3) / 1e9, "unit": UNIT,
+           "h2d_bytes_per_step": int(qn.nbytes), "d2h_bytes_per_step": int(cn.nbytes + dn.nbytes),
+           "ms_per_step": ms_e2e / args.steps}
+
+    # ---- CPU baseline (rank 0, N = 1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import refharness
+        if refharness.available():
+            procs = args.cpu_procs or min(16, cpu_count())
+            val, d = reference_throughput(args.cpu_sample_n, procs, 1, 2)
+            cpu = {"value": val, "unit": UNIT, "cores": procs, "kind": "reference", "sample": d["sample"],
+                   "per_core_value": d["per_process_gedges"]}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                   "sample": "reference oracle library not built"}
+
+    s.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded tet-split cube, seeded +-1% state noise)",
+            "config": workload_config(args.n, mesh), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": KERNELS_PER_STEP * args.steps, "clocks": clocks, "per_flux": per_flux,
+            "breakdown_ms": breakdown, "setup_s": setup_s,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -27,11 +27,6 @@ void set_error(const char *fmt, ...) {
     va_end(ap);
 }
 
-static inline unsigned long long dbits(double x) {
-    unsigned long long u;
-    std::memcpy(&u, &x, 8);
-    return u;
-}
 static inline double bitsd(unsigned long long u) {
     double x;
     std::memcpy(&x, &u, 8);
@@ -454,6 +449,15 @@ __global__ void __launch_bounds__(128) k_gs_level(int nrows, const int *__restri
     for (int m = 0; m < 5; m++) X[(int64_t)r * 5 + m] = xo[m];
 }
 
+// Per-iteration reset: sum(area*lambda) = 0, extrema = (DBL_MAX, DBL_MIN)
+// (Solver_Steady_Implicit.cpp:45-79).
+__global__ void k_begin_iteration(int nnode, double *__restrict__ dt, unsigned long long *__restrict__ ext) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nnode) dt[i] = 0.0;
+    if (i < 8) ext[i] = (i & 1) ? (unsigned long long)__double_as_longlong(DBL_MIN)
+                                : (unsigned long long)__double_as_longlong(DBL_MAX);
+}
+
 __global__ void k_update(int nnode, int64_t ldq, double relax, const double *__restrict__ X, double *__restrict__ Q) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnode) return;
@@ -475,8 +479,8 @@ __global__ void k_freestream(int n, int64_t ldq, Flow f, double *__restrict__ Q)
 
 int reduce_sum_sq(cfd_ctx *c, const double *x, int64_t n, int64_t stride, int nvec, double *out_host) {
     const int nblk = 296, bs = 256;
-    CFD_CUDA(c->red.alloc((size_t)nblk * 16));
-    CFD_CUDA(c->red_out.alloc(16));
+    CFD_CUDA(c->red.alloc(std::max<size_t>(c->red.n, (size_t)nblk * 128)));
+    CFD_CUDA(c->red_out.alloc(std::max<size_t>(c->red_out.n, 64)));
     k_sumsq_partial<<<nblk, bs, bs * sizeof(double), c->stream>>>(x, n, stride, nvec, c->red.p);
     CFD_LAUNCH_CHECK();
     k_sum_final<<<1, bs, bs * sizeof(double), c->stream>>>(c->red.p, nblk, nvec, c->red_out.p);
@@ -729,6 +733,7 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
     c->has_mesh = false;
     c->has_system = false;
     c->has_grad = false;
+    c->lsq_weight = -1;
     c->nnode = nnode;
     c->nghost = nghost;
     c->nedge = nedge;
@@ -921,15 +926,8 @@ int cfd_set_freestream(cfd_ctx *c) {
 int cfd_begin_iteration(cfd_ctx *c, int iteration) {
     NEED_MESH("cfd_begin_iteration");
     compute_flow(c, iteration);
-    unsigned long long h[8];
-    for (int j = 0; j < 4; j++) {
-        h[2 * j] = dbits(DBL_MAX);
-        h[2 * j + 1] = dbits(DBL_MIN);
-    }
-    CFD_CUDA(cudaMemcpyAsync(c->ext.p, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
-    CFD_CUDA(cudaMemsetAsync(c->dt.p, 0, sizeof(double) * c->nnode, c->stream));
-    // the host staging buffer must outlive the async copy
-    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    k_begin_iteration<<<grid_for(c->nnode, 256), 256, 0, c->stream>>>(c->nnode, c->dt.p, c->ext.p);
+    CFD_LAUNCH_CHECK();
     return CFD_OK;
 }
 

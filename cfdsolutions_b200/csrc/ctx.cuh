@@ -90,7 +90,8 @@ struct cfd_ctx {
     cfd::DevBuf<double> dt;     // [nnode] sum(area*lambda) then DeltaT
     cfd::DevBuf<double> grad;   // [15][nnode]
     cfd::DevBuf<double> phi;    // [5][nnode]
-    cfd::DevBuf<double> ggw;    // Green-Gauss / LSQ per-node coefficients
+    cfd::DevBuf<double> ggw;    // least-squares per-node coefficients [nnode][8]
+    int lsq_weight = -1;        // weight the coefficients in ggw were built for
     cfd::DevBuf<unsigned long long> ext;  // 8 extrema as ordered bit patterns
     cfd::DevBuf<int> err;       // device error word
     cfd::DevBuf<double> red;    // reduction partials

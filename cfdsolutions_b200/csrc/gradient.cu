@@ -284,21 +284,12 @@ int cfd_gradient(cfd_ctx *c) {
                                                              c->edge_sv.p, c->cvol.p, c->grad.p);
     } else {
         // coefficients depend on the mesh and the weight only (FlagLSCoeff, Gradient.cpp:245-252)
-        const size_t need = (size_t)8 * n + 1;
-        if (c->ggw.n != need) {
-            CFD_CUDA(c->ggw.alloc(need));
-            CFD_CUDA(cudaMemsetAsync(c->ggw.p + 8 * (size_t)n, 0xff, sizeof(double), c->stream));
-        }
-        double tag;
-        CFD_CUDA(cudaMemcpyAsync(&tag, c->ggw.p + 8 * (size_t)n, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-        CFD_CUDA(cudaStreamSynchronize(c->stream));
-        if (tag != (double)c->params.ls_weight) {
+        if (c->lsq_weight != c->params.ls_weight || c->ggw.n != (size_t)8 * n) {
+            CFD_CUDA(c->ggw.alloc((size_t)8 * n));
             k_lsq_coeff<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->n2n_ia.p, c->n2n_ja.p, c->xyz.p,
                                                                    c->params.ls_weight, c->ggw.p);
             CFD_LAUNCH_CHECK();
-            const double t = (double)c->params.ls_weight;
-            CFD_CUDA(cudaMemcpyAsync(c->ggw.p + 8 * (size_t)n, &t, sizeof(double), cudaMemcpyHostToDevice, c->stream));
-            CFD_CUDA(cudaStreamSynchronize(c->stream));
+            c->lsq_weight = c->params.ls_weight;
         }
         k_lsq_grad<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->n2n_ia.p, c->n2n_ja.p, c->xyz.p,
                                                               c->params.ls_weight, c->ggw.p, c->grad.p);

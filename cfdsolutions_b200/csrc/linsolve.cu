@@ -54,7 +54,7 @@ __global__ void k_sum_one(const double *__restrict__ part, int nblk, double *__r
 
 int reduce_sum_plain(cfd_ctx *c, const double *x, int64_t n, double *out_host) {
     const int nblk = 296;
-    CFD_CUDA(c->red.alloc(std::max<size_t>(c->red.n, (size_t)nblk * 64)));
+    CFD_CUDA(c->red.alloc(std::max<size_t>(c->red.n, (size_t)nblk * 128)));
     CFD_CUDA(c->red_out.alloc(std::max<size_t>(c->red_out.n, 64)));
     k_sum_partial<<<nblk, 256, 0, c->stream>>>(x, n, c->red.p);
     CFD_LAUNCH_CHECK();
@@ -143,7 +143,7 @@ static const int kRedBlocks = 296;  // 2 x 148 SMs
 
 // out_host[j] = <V_j, w>, j < k, compensated, deterministic.
 static int mdot(cfd_ctx *c, const double *V, int64_t ld, int k, const double *w, int64_t n, double *out_host) {
-    CFD_CUDA(c->red.alloc(std::max<size_t>(c->red.n, (size_t)kRedBlocks * MAXK * 2)));
+    CFD_CUDA(c->red.alloc(std::max<size_t>(c->red.n, (size_t)kRedBlocks * 128)));
     CFD_CUDA(c->dots.alloc(std::max<size_t>(c->dots.n, (size_t)MAXK)));
     k_mdot_partial<<<kRedBlocks, 256, 0, c->stream>>>(V, ld, k, w, n, c->red.p);
     CFD_LAUNCH_CHECK();

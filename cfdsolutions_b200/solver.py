@@ -148,9 +148,15 @@ class Euler3DGPU:
         capi.check(capi.lib.cfd_residual_rms(self._h, int(include_diss), capi.ptr(out)), "cfd_residual_rms")
         return out
 
-    def residual_step(self, iteration: int = 0, Q: np.ndarray | None = None, want_residual: bool = False):
+    def residual_step(self, iteration: int = 0, Q: np.ndarray | None = None, want_residual: bool = False,
+                      out: tuple | None = None):
+        """One residual evaluation (cfd_residual_step).  With ``Q`` the state is
+        copied in first; with ``want_residual`` or ``out=(conv, diss)`` the
+        residuals are copied back (pass pinned arrays for full copy speed)."""
         conv = diss = None
-        if want_residual:
+        if out is not None:
+            conv, diss = out
+        elif want_residual:
             conv = np.empty((5, self.mesh.nnode))
             diss = np.empty((5, self.mesh.nnode))
         capi.check(capi.lib.cfd_residual_step(self._h, iteration, capi.ptr(Q), capi.ptr(conv), capi.ptr(diss)),

@@ -38,7 +38,11 @@ def param_text(cfg: dict) -> str:
     mach = g("mach", 0.5)
     lines = {
         "MESH_FILENAME": "none", "BC_FILENAME": "none", "SOLUTION_FILENAME": "none",
-        "MESH_REORDER": "NO", "SOLVER_METHOD": "SOLVER_METHOD_STEADY", "SOLVER_SCHEME": "SOLVER_SCHEME_IMPLICIT",
+        "MESH_REORDER": "NO", "SOLVER_METHOD": "SOLVER_METHOD_STEADY",
+        # explicit skips the reference's block-matrix allocation (one malloc per block row,
+        # Euler3D/src/Solver.cpp:675-685) when only the residual is wanted
+        "SOLVER_SCHEME": "SOLVER_SCHEME_EXPLICIT" if g("scheme", "implicit") == "explicit" else
+        "SOLVER_SCHEME_IMPLICIT",
         "FLUX_SCHEME": FLUX[g("flux_scheme", 0)], "SOLVER_NITERATION": "1", "LINEAR_SOLVER_NITERATION": "10",
         "SOLVER_ORDER": "SOLVER_ORDER_SECOND" if g("order", 0) == 1 else "SOLVER_ORDER_FIRST",
         "TIME_INTEGRATION_METHOD": "TIME_INTEGRATION_METHOD_IMPLICIT_EULER",
@@ -226,3 +230,15 @@ def mesh_from_ugrid(path: str, reorder: int = 0, timeout: float = 600.0) -> dict
     ctx = mp.get_context("spawn")
     with ctx.Pool(1) as pool:
         return pool.apply_async(_ugrid_session, (str(path), reorder)).get(timeout)
+
+
+def run_many(mesh, cfg: dict, Q: np.ndarray | None, steps: list, procs: int, timeout: float = 1800.0) -> list:
+    """The same reference session in ``procs`` concurrent spawned processes
+    (independent single-threaded copies, one per host core)."""
+    if not available():
+        raise FileNotFoundError(f"{REF_LIB} not built (make -C oracle ref)")
+    ctx = mp.get_context("spawn")
+    md = _mesh_dict(mesh)
+    with ctx.Pool(procs) as pool:
+        rs = [pool.apply_async(_session, (md, cfg, Q, steps, True)) for _ in range(procs)]
+        return [r.get(timeout) for r in rs]
