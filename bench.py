@@ -42,13 +42,14 @@ KERNELS_PER_STEP = 7  # begin, bc, gradient, limiter, roe pressure fix, residual
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=128, help="hexes per side of the cube")
     ap.add_argument("--cpu-sample-n", type=int, default=48, help="hexes per side of the CPU baseline sample")
     ap.add_argument("--cpu-procs", type=int, default=0, help="reference processes (0 = one per core, max 16)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--side-rcm", action="store_true", help="also time the plain node-level RCM numbering")
     return ap.parse_args()
 
 
@@ -94,7 +95,7 @@ class Clocks:
                 ["nvidia-smi", f"--id={self.device}", "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "--format=csv,noheader,nounits", "-lms", "20"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
         return self
@@ -181,6 +182,7 @@ def run_reference_arm(args, rank, world):
 def workload_config(n, mesh=None):
     c = {"workload": f"second-order residual evaluation, {n}^3-hex tet cube (6 tets/hex), RCM, jitter 0.15h, "
                      "Green-Gauss + Venkatakrishnan K=5 + Roe, M=0.8, alpha=1.25, +-1% noise",
+         "numbering": "blocked RCM: reverse Cuthill-McKee over 128-node coordinate-bisection patches",
          "flux": "roe", "gradient": "green-gauss", "limiter": "venkatakrishnan", "venkat_k": 5.0, "mach": 0.8,
          "alpha_deg": 1.25, "precision": "fp64", "parallelism": "replicas (one mesh per GPU)",
          "l2": "inputs larger than L2 (resident working set > 126 MB)"}
@@ -208,9 +210,10 @@ def main():
     torch.cuda.set_device(dev)
 
     from cfdsolutions_b200 import Euler3DGPU, box_mesh, default_params, perturbed_freestream
+    from cfdsolutions_b200.mesh import NUMBERING_PATCH_RCM, NUMBERING_RCM
 
     t0 = time.time()
-    mesh = box_mesh(args.n, jitter=0.15, seed=1234, rcm=True)
+    mesh = box_mesh(args.n, jitter=0.15, seed=1234, rcm=NUMBERING_PATCH_RCM)
     Q = perturbed_freestream(mesh, CFG["gamma"], CFG["mach"], CFG["alpha_deg"], noise=0.01, seed=1235)
     setup_s = time.time() - t0
     units = mesh.nedge + mesh.nbedge
@@ -284,6 +287,21 @@ def main():
                                     "ms_per_step": msf / args.steps}
     s.set_params(default_params(**CFG))
 
+    # ---- the same step on the plain node-level RCM numbering, and on the node-gather kernel
+    side = {}
+    s.set_params(default_params(**dict(CFG, residual_kernel=1)))
+    msg = timed(lambda i: s.residual_step(i), args.steps, args.warmup)
+    side["gather_kernel_gedges_per_s"] = units * args.steps / (msg / 1e3) / 1e9
+    s.set_params(default_params(**CFG))
+    if args.side_rcm:
+        m2 = box_mesh(args.n, jitter=0.15, seed=1234, rcm=NUMBERING_RCM)
+        q2 = perturbed_freestream(m2, CFG["gamma"], CFG["mach"], CFG["alpha_deg"], noise=0.01, seed=1235)
+        with Euler3DGPU(m2, default_params(**CFG), device=dev, stream=stream.cuda_stream) as s2:
+            s2.set_state(q2)
+            ms2 = timed(lambda i: s2.residual_step(i), args.steps, args.warmup)
+        side["plain_rcm_numbering_gedges_per_s"] = units * args.steps / (ms2 / 1e3) / 1e9
+        del m2, q2
+
     # ---- end to end through the C ABI with pinned host buffers
     qh = torch.from_numpy(np.ascontiguousarray(Q)).pin_memory()
     conv = torch.empty((5, mesh.nnode), dtype=torch.float64).pin_memory()
@@ -315,7 +333,7 @@ def main():
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded tet-split cube, seeded +-1% state noise)",
             "config": workload_config(args.n, mesh), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": KERNELS_PER_STEP * args.steps, "clocks": clocks, "per_flux": per_flux,
-            "breakdown_ms": breakdown, "setup_s": setup_s,
+            "breakdown_ms": breakdown, "variants": side, "setup_s": setup_s,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

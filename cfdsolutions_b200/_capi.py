@@ -40,6 +40,7 @@ class Params(C.Structure):
         ("global_time", C.c_int), ("cfl_ramp", C.c_int), ("mach_ramp", C.c_int), ("zpg_iteration", C.c_int),
         ("gamma", C.c_double), ("mach", C.c_double), ("mach_min", C.c_double), ("alpha_deg", C.c_double),
         ("beta_deg", C.c_double), ("cfl_min", C.c_double), ("cfl_max", C.c_double), ("venkat_k", C.c_double),
+        ("residual_kernel", C.c_int),
     ]
 
 

@@ -191,6 +191,144 @@ __global__ void __launch_bounds__(128) k_residual_gather(
     if (add_time) block_extrema3(mn, mx, ext);
 }
 
+// Pressure of the Roe-averaged state of two reconstructed face states
+// (Compute_RoeVariables, Roe_Fluxes.cpp:3609-3633, tested in
+// Compute_Limiter_RoePressureCorrection, Limiters.cpp:311-356).
+__device__ __forceinline__ double roe_avg_pressure(const double qa[5], const double qb[5], double g) {
+    const double ra = qa[0], rb = qb[0];
+    const double ia = 1.0 / ra, ib = 1.0 / rb;
+    const double ua = qa[1] * ia, va = qa[2] * ia, wa = qa[3] * ia;
+    const double ub = qb[1] * ib, vb = qb[2] * ib, wb = qb[3] * ib;
+    const double pa = (g - 1.0) * (qa[4] - 0.5 * ra * (ua * ua + va * va + wa * wa));
+    const double pb = (g - 1.0) * (qb[4] - 0.5 * rb * (ub * ub + vb * vb + wb * wb));
+    const double ha = (qa[4] + pa) * ia, hb = (qb[4] + pb) * ib;
+    const double rho = sqrt(ra * rb), sg = rho / (ra + rho);
+    const double u = ua + sg * (ub - ua), v = va + sg * (vb - va), w = wa + sg * (wb - wa);
+    const double ht = ha + sg * (hb - ha);
+    const double q2 = u * u + v * v + w * w;
+    const double e = (rho / g) * (ht + 0.5 * (g - 1.0) * q2);
+    return (g - 1.0) * (e - 0.5 * rho * q2);
+}
+
+// Flux residual, patch form: one CTA per patch of CFD_PATCH_NODES consecutive
+// nodes.  Phase 1 evaluates every edge of the patch once (edges cut by the
+// patch boundary are evaluated by both patches) into shared memory; phase 2
+// lets each owned node sum its incident edges from shared memory in its fixed
+// neighbour order (+ when it is node_L, - when it is node_R) and add its
+// boundary edges.  No atomics on the residual, deterministic summation order,
+// one flux evaluation per edge per patch instead of one per edge end.
+// `gate`: when non-null and *gate == 0 the launch does nothing (conditional
+// re-evaluation after the limiter's pressure fix).
+template <int FLUX, bool SECOND>
+__global__ void __launch_bounds__(256) k_residual_patch(
+    int nnode, int64_t ldq, const double *__restrict__ Q, const int *__restrict__ pe_ptr,
+    const int2 *__restrict__ pe_nodes, const double4 *__restrict__ pe_geo, const int *__restrict__ inc_ptr,
+    const int *__restrict__ inc, const int *__restrict__ n2b_ptr, const int *__restrict__ n2b,
+    const int2 *__restrict__ bn, const double4 *__restrict__ bg, const double *__restrict__ xyz,
+    const double *__restrict__ grad, const double *__restrict__ phi, Flow f, int add_time, int emax,
+    int check_roe, int *__restrict__ roeflag, int *__restrict__ roecount, const int *__restrict__ gate,
+    double *__restrict__ res, double *__restrict__ resd, double *__restrict__ dtsum,
+    unsigned long long *__restrict__ ext) {
+    if (gate && *gate == 0) return;
+    extern __shared__ double eb[];  // [11][emax]
+    const int p = blockIdx.x;
+    const int e0 = pe_ptr[p], ne = pe_ptr[p + 1] - e0;
+    const bool limited = f.limiter != CFD_LIMITER_NONE;
+    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
+    for (int k = threadIdx.x; k < ne; k += blockDim.x) {
+        const int2 nd = pe_nodes[e0 + k];
+        const double4 g = pe_geo[e0 + k];
+        double qL[5], qR[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            qL[v] = Q[v * ldq + nd.x];
+            qR[v] = Q[v * ldq + nd.y];
+        }
+        if (SECOND) {
+            const double rx = 0.5 * (xyz[nd.y] - xyz[nd.x]);
+            const double ry = 0.5 * (xyz[nnode + nd.y] - xyz[nnode + nd.x]);
+            const double rz = 0.5 * (xyz[2 * nnode + nd.y] - xyz[2 * nnode + nd.x]);
+            double rL[5], rR[5];
+            reconstruct(qL, qR, nd.x, rx, ry, rz, grad, phi, nnode, limited, f.frac, rL);
+            reconstruct(qR, qL, nd.y, -rx, -ry, -rz, grad, phi, nnode, limited, f.frac, rR);
+#pragma unroll
+            for (int v = 0; v < 5; v++) { qL[v] = rL[v]; qR[v] = rR[v]; }
+            if (check_roe && roe_avg_pressure(qL, qR, f.gamma) < 0.0) {
+                roeflag[nd.x] = 1;
+                roeflag[nd.y] = 1;
+                atomicAdd(roecount, 1);
+            }
+        }
+        double cf[5], df[5], lam[3];
+        const double lmax = edge_flux<FLUX>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam);
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            eb[v * emax + k] = cf[v];
+            eb[(5 + v) * emax + k] = df[v];
+        }
+        eb[10 * emax + k] = g.w * lmax;
+#pragma unroll
+        for (int j = 0; j < 3; j++) { mn[j] = fmin(mn[j], lam[j]); mx[j] = fmax(mx[j], lam[j]); }
+    }
+    __syncthreads();
+    const int n0 = p * CFD_PATCH_NODES;
+    const int nown = min(CFD_PATCH_NODES, nnode - n0);
+    for (int j = threadIdx.x; j < nown; j += blockDim.x) {
+        const int i = n0 + j;
+        double ac[5] = {0, 0, 0, 0, 0}, ad[5] = {0, 0, 0, 0, 0}, adt = 0.0;
+        for (int q = inc_ptr[i]; q < inc_ptr[i + 1]; q++) {
+            const int t = inc[q];
+            const int k = t >> 1;
+            const double sg = (t & 1) ? -1.0 : 1.0;
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                ac[v] += sg * eb[v * emax + k];
+                ad[v] += sg * eb[(5 + v) * emax + k];
+            }
+            adt += eb[10 * emax + k];
+        }
+        for (int k = n2b_ptr[i]; k < n2b_ptr[i + 1]; k++) {
+            const int b = n2b[k];
+            const int2 nd = bn[b];
+            const double4 g = bg[b];
+            double qL[5], qR[5];
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                qL[v] = Q[v * ldq + nd.x];
+                qR[v] = Q[v * ldq + nd.y];
+            }
+            double cf[5], df[5], lam[3];
+            const double lmax = edge_flux<FLUX>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam);
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                ac[v] += cf[v];
+                ad[v] += df[v];
+            }
+            adt += g.w * lmax;
+#pragma unroll
+            for (int m = 0; m < 3; m++) { mn[m] = fmin(mn[m], lam[m]); mx[m] = fmax(mx[m], lam[m]); }
+        }
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            res[v * (int64_t)nnode + i] = ac[v];
+            resd[v * (int64_t)nnode + i] = ad[v];
+        }
+        if (add_time) dtsum[i] = adt;
+    }
+    if (add_time) block_extrema3(mn, mx, ext);
+}
+
+// Limiter pressure fix selected by the residual's check: zero the limiters of
+// flagged nodes; no-op unless some edge failed (*count == 0).
+__global__ void k_roe_fix_apply(int nnode, const int *__restrict__ count, const int *__restrict__ flag,
+                                double *__restrict__ phi) {
+    if (*count == 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nnode || !flag[i]) return;
+#pragma unroll
+    for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = 0.0;
+}
+
 // dt_i = V_i * CFL / sum_i (Compute_DeltaT, Euler3D/src/Time_Step.cpp:23-51).
 __global__ void k_deltat(int nnode, const double *__restrict__ vol, double cfl, double *__restrict__ dt,
                          unsigned long long *__restrict__ ext) {
@@ -547,12 +685,43 @@ static void compute_flow(cfd_ctx *c, int iteration) {
         c->cfl = p.cfl_max;
 }
 
+static bool patch_kernel(const cfd_ctx *c) { return c->use_patch && c->params.residual_kernel == 0; }
+
 template <int FLUX, bool SECOND>
-static void launch_residual(cfd_ctx *c, int add_time) {
-    k_residual_gather<FLUX, SECOND><<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(
-        c->nnode, c->ldq, c->Q.p, c->n2e_ptr.p, c->n2e.p, c->edge_nodes.p, c->edge_geo.p, c->n2b_ptr.p, c->n2b.p,
-        c->bedge_nodes.p, c->bedge_geo.p, c->xyz.p, c->grad.p, c->phi.p, c->flow, add_time, c->res.p, c->resd.p,
-        c->dt.p, c->ext.p);
+static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, const int *gate) {
+    if (patch_kernel(c)) {
+        const size_t smem = (size_t)c->patch_emax * 11 * sizeof(double);
+        if (smem > 48 * 1024)
+            CFD_CUDA(cudaFuncSetAttribute(k_residual_patch<FLUX, SECOND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)kPatchSmemMax));
+        k_residual_patch<FLUX, SECOND><<<c->npatch, 256, smem, c->stream>>>(
+            c->nnode, c->ldq, c->Q.p, c->pe_ptr.p, c->pe_nodes.p, c->pe_geo.p, c->inc_ptr.p, c->inc.p, c->n2b_ptr.p,
+            c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p, c->xyz.p, c->grad.p, c->phi.p, c->flow, add_time,
+            c->patch_emax, check_roe ? 1 : 0, c->roeflag.p, c->roecount.p, gate, c->res.p, c->resd.p, c->dt.p,
+            c->ext.p);
+    } else {
+        if (gate || check_roe) return CFD_ERR_UNSUPPORTED;
+        k_residual_gather<FLUX, SECOND><<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(
+            c->nnode, c->ldq, c->Q.p, c->n2e_ptr.p, c->n2e.p, c->edge_nodes.p, c->edge_geo.p, c->n2b_ptr.p,
+            c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p, c->xyz.p, c->grad.p, c->phi.p, c->flow, add_time, c->res.p,
+            c->resd.p, c->dt.p, c->ext.p);
+    }
+    CFD_LAUNCH_CHECK();
+    return CFD_OK;
+}
+
+template <int FLUX, bool SECOND>
+static int residual_with_fix(cfd_ctx *c, int add_time) {
+    // Roe flux + limiter: the limiter's Roe-average pressure fix is decided by
+    // the residual's own reconstruction (same states) and applied, followed by
+    // a gated re-evaluation, only when some edge failed the check.
+    const bool fused = SECOND && FLUX == CFD_FLUX_ROE && c->roe_fix_pending && patch_kernel(c);
+    int st = launch_residual<FLUX, SECOND>(c, add_time, fused, nullptr);
+    if (st || !fused) return st;
+    k_roe_fix_apply<<<grid_for(c->nnode, 256), 256, 0, c->stream>>>(c->nnode, c->roecount.p, c->roeflag.p, c->phi.p);
+    CFD_LAUNCH_CHECK();
+    c->roe_fix_pending = false;
+    return launch_residual<FLUX, SECOND>(c, add_time, false, c->roecount.p);
 }
 
 static Levels *build_levels(const std::vector<int> &IA, const std::vector<int> &JA, int n, bool forward,
@@ -666,6 +835,10 @@ int cfd_set_params(cfd_ctx *c, const cfd_params *p) {
         return CFD_ERR_ARG;
     }
     if (!(p->gamma > 1.0)) { set_error("cfd_set_params: gamma must be > 1"); return CFD_ERR_ARG; }
+    if (p->residual_kernel < 0 || p->residual_kernel > 1) {
+        set_error("cfd_set_params: residual_kernel must be 0 or 1");
+        return CFD_ERR_ARG;
+    }
     if (p->order != CFD_ORDER_FIRST && p->order != CFD_ORDER_SECOND) {
         set_error("cfd_set_params: invalid order %d", p->order);
         return CFD_ERR_ARG;
@@ -748,9 +921,10 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         g = make_double4(nx, ny, nz, mag);
         sv = make_double4(a[0], a[1], a[2], 0.0);
     };
+    std::vector<int2> en(nedge);
+    std::vector<double4> eg(nedge);
     {
-        std::vector<int2> en(nedge);
-        std::vector<double4> eg(nedge), es(nedge);
+        std::vector<double4> es(nedge);
         for (int e = 0; e < nedge; e++) {
             en[e] = make_int2(edge_nodes[2 * e], edge_nodes[2 * e + 1]);
             geo(edge_areav + 3 * (size_t)e, eg[e], es[e]);
@@ -786,11 +960,12 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
     CFD_CUDA(c->n2n_ja.upload(gja.data(), gja.size(), s));
 
     // ---- node -> incident interior edges, ordered by neighbour id
+    std::vector<int> ptr(nnode + 1, 0), lst;
     {
-        std::vector<int> ptr(nnode + 1, 0);
         for (int e = 0; e < nedge; e++) { ptr[edge_nodes[2 * e] + 1]++; ptr[edge_nodes[2 * e + 1] + 1]++; }
         for (int i = 0; i < nnode; i++) ptr[i + 1] += ptr[i];
-        std::vector<int> lst(ptr[nnode]), fill(ptr.begin(), ptr.end() - 1), nb(ptr[nnode]);
+        lst.assign(ptr[nnode], 0);
+        std::vector<int> fill(ptr.begin(), ptr.end() - 1), nb(ptr[nnode]);
         for (int e = 0; e < nedge; e++) {
             const int a = edge_nodes[2 * e], b = edge_nodes[2 * e + 1];
             nb[fill[a]] = b; lst[fill[a]++] = e;
@@ -810,6 +985,57 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         CFD_CUDA(c->n2e.upload(lst.data(), lst.size(), s));
         CFD_CUDA(cudaStreamSynchronize(s));
     }
+    // ---- patch layout of the residual kernel: node ranges of CFD_PATCH_NODES,
+    // every interior edge touching a patch copied into the patch's edge list
+    // (edges cut by the patch boundary appear in both patches), and per node
+    // its incident edges as patch-local indices in the fixed neighbour order.
+    {
+        const int P = CFD_PATCH_NODES;
+        const int np = (nnode + P - 1) / P;
+        std::vector<int> pptr(np + 1, 0), stamp(nedge, -1), local(nedge, 0), iptr(nnode + 1, 0), ilist;
+        std::vector<int2> pn;
+        std::vector<double4> pg;
+        ilist.reserve(ptr[nnode]);
+        pn.reserve((size_t)nedge + nedge / 2);
+        pg.reserve((size_t)nedge + nedge / 2);
+        int emax = 0;
+        for (int p = 0; p < np; p++) {
+            int cnt = 0;
+            const int n0 = p * P, n1 = std::min(nnode, n0 + P);
+            for (int i = n0; i < n1; i++) {
+                for (int k = ptr[i]; k < ptr[i + 1]; k++) {
+                    const int sg = lst[k], e = sg >= 0 ? sg : ~sg;
+                    if (stamp[e] != p) {
+                        stamp[e] = p;
+                        local[e] = cnt++;
+                        pn.push_back(en[e]);
+                        pg.push_back(eg[e]);
+                    }
+                    ilist.push_back((local[e] << 1) | (sg < 0 ? 1 : 0));
+                }
+                iptr[i + 1] = (int)ilist.size();
+            }
+            pptr[p + 1] = pptr[p] + cnt;
+            emax = std::max(emax, cnt);
+        }
+        if (ilist.empty()) ilist.push_back(0);  // keep the device array non-empty
+        c->npatch = np;
+        c->patch_emax = emax;
+        c->use_patch = (size_t)emax * 11 * sizeof(double) <= kPatchSmemMax;
+        if (c->use_patch) {
+            CFD_CUDA(c->pe_ptr.upload(pptr.data(), pptr.size(), s));
+            CFD_CUDA(c->pe_nodes.upload(pn.data(), pn.size(), s));
+            CFD_CUDA(c->pe_geo.upload(pg.data(), pg.size(), s));
+            CFD_CUDA(c->inc_ptr.upload(iptr.data(), iptr.size(), s));
+            CFD_CUDA(c->inc.upload(ilist.data(), ilist.size(), s));
+            CFD_CUDA(cudaStreamSynchronize(s));
+        }
+    }
+    CFD_CUDA(c->roeflag.alloc(nnode));
+    CFD_CUDA(c->roecount.alloc(1));
+    CFD_CUDA(cudaMemsetAsync(c->roeflag.p, 0, sizeof(int) * nnode, s));
+    CFD_CUDA(cudaMemsetAsync(c->roecount.p, 0, sizeof(int), s));
+    c->roe_fix_pending = false;
     {
         std::vector<int> ptr(nnode + 1, 0);
         for (int e = 0; e < nbedge; e++) ptr[bedge_nodes[2 * e] + 1]++;
@@ -952,17 +1178,19 @@ int cfd_residual(cfd_ctx *c, int add_time) {
         set_error("cfd_residual: limiter requested but cfd_limiter not called");
         return CFD_ERR_STATE;
     }
+    if (second && c->params.limiter != CFD_LIMITER_NONE && c->roe_fix_pending && !patch_kernel(c)) {
+        int st = roe_fix_standalone(c);
+        if (st) return st;
+    }
     switch (c->params.flux_scheme * 2 + (second ? 1 : 0)) {
-        case 0: launch_residual<CFD_FLUX_ROE, false>(c, add_time); break;
-        case 1: launch_residual<CFD_FLUX_ROE, true>(c, add_time); break;
-        case 2: launch_residual<CFD_FLUX_HLLC, false>(c, add_time); break;
-        case 3: launch_residual<CFD_FLUX_HLLC, true>(c, add_time); break;
-        case 4: launch_residual<CFD_FLUX_AUSM, false>(c, add_time); break;
-        case 5: launch_residual<CFD_FLUX_AUSM, true>(c, add_time); break;
+        case 0: return residual_with_fix<CFD_FLUX_ROE, false>(c, add_time);
+        case 1: return residual_with_fix<CFD_FLUX_ROE, true>(c, add_time);
+        case 2: return residual_with_fix<CFD_FLUX_HLLC, false>(c, add_time);
+        case 3: return residual_with_fix<CFD_FLUX_HLLC, true>(c, add_time);
+        case 4: return residual_with_fix<CFD_FLUX_AUSM, false>(c, add_time);
+        case 5: return residual_with_fix<CFD_FLUX_AUSM, true>(c, add_time);
         default: set_error("cfd_residual: bad flux scheme"); return CFD_ERR_ARG;
     }
-    CFD_LAUNCH_CHECK();
-    return CFD_OK;
 }
 
 int cfd_deltat(cfd_ctx *c, int iteration) {

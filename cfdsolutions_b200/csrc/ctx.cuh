@@ -82,6 +82,18 @@ struct cfd_ctx {
     cfd::DevBuf<int> IA, JA, IAU, tslot;  // tslot[k] = slot of (JA[k], row)
     cfd::DevBuf<int2> eslot;              // per edge: slot(L,R), slot(R,L)
     cfd::Levels lv_fwd, lv_bwd;
+    // patch layout of the residual kernel: patches are contiguous ranges of
+    // CFD_PATCH_NODES nodes; each patch lists every interior edge touching it
+    cfd::DevBuf<int> pe_ptr;          // [npatch+1]
+    cfd::DevBuf<int2> pe_nodes;       // [sum] edge (L, R) copies
+    cfd::DevBuf<double4> pe_geo;      // [sum] unit normal + |S|
+    cfd::DevBuf<int> inc_ptr, inc;    // per node: (patch-local edge << 1) | (node is R)
+    int npatch = 0, patch_emax = 0;
+    bool use_patch = false;
+    // Roe-average pressure positivity fix of the limiter (see cfd_limiter)
+    cfd::DevBuf<int> roeflag;         // [nnode]
+    cfd::DevBuf<int> roecount;        // [1]
+    bool roe_fix_pending = false;
 
     // state and residual
     cfd::DevBuf<double> Q;      // [5][ldq]

@@ -131,9 +131,11 @@ __global__ void __launch_bounds__(128) k_gg_grad(int nnode, int64_t ldq, const d
 __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const double *__restrict__ Q,
                                                 const int *__restrict__ ia, const int *__restrict__ ja,
                                                 const double *__restrict__ xyz, const double *__restrict__ g,
-                                                const double *__restrict__ vol, Flow f, double *__restrict__ phi) {
+                                                const double *__restrict__ vol, Flow f, double *__restrict__ phi,
+                                                int *__restrict__ roeflag) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnode) return;
+    roeflag[i] = 0;
     const double frac = f.frac;
     double qc[5], qmin[5], qmax[5], ph[5], gx[5], gy[5], gz[5];
 #pragma unroll
@@ -157,6 +159,12 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
     }
     const double xi = xyz[i], yi = xyz[nnode + i], zi = xyz[2 * nnode + i];
     if (f.limiter == CFD_LIMITER_VENKAT) {
+        // phi = min(1, min_edges num/den) with num, den >= 0 (dm and dp share
+        // their sign).  The running minimum is kept as a fraction and compared
+        // by cross-multiplication, so one division per variable replaces one
+        // per edge; the result is the same rounded quotient the reference's
+        // per-edge divisions select, except for ties closer than an ulp.
+        double bn[5] = {1, 1, 1, 1, 1}, bd[5] = {1, 1, 1, 1, 1};
         for (int k = ia[i]; k < ia[i + 1]; k++) {
             const int j = ja[k];
             const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
@@ -166,15 +174,14 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
                 const double dm = q - qc[v];
                 if (dm != 0.0) {
                     const double dp = (dm > 0.0 ? qmax[v] : qmin[v]) - qc[v];
-                    double t = (dp * dp + eps2) + 2.0 * (dm * dp);
-                    t = t / (dp * dp + 2.0 * dm * dm + dm * dp + eps2);
-                    ph[v] = fmin(ph[v], t);
-                } else {
-                    ph[v] = fmin(ph[v], 1.0);
+                    const double num = (dp * dp + eps2) + 2.0 * (dm * dp);
+                    const double den = dp * dp + 2.0 * dm * dm + dm * dp + eps2;
+                    if (num * bd[v] < bn[v] * den) { bn[v] = num; bd[v] = den; }
                 }
-                ph[v] = fmax(0.0, ph[v]);
             }
         }
+#pragma unroll
+        for (int v = 0; v < 5; v++) ph[v] = fmax(0.0, bn[v] == bd[v] ? 1.0 : bn[v] / bd[v]);
     } else {  // Barth-Jespersen (Compute_Limiter_Barth_Jespersen, Limiters.cpp:117-178)
         for (int k = ia[i]; k < ia[i + 1]; k++) {
             const int j = ja[k];
@@ -310,18 +317,37 @@ int cfd_limiter(cfd_ctx *c) {
         CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)5 * n)));
         return CFD_OK;
     }
-    CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)5 * n)));
-    double *out = c->params.flux_scheme == CFD_FLUX_ROE ? c->work.p : c->phi.p;
     k_venkat<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->n2n_ia.p, c->n2n_ja.p, c->xyz.p, c->grad.p,
-                                                        c->cvol.p, c->flow, out);
+                                                        c->cvol.p, c->flow, c->phi.p, c->roeflag.p);
     CFD_LAUNCH_CHECK();
     if (c->params.flux_scheme == CFD_FLUX_ROE) {
-        k_roe_pressure_fix<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->n2n_ia.p, c->n2n_ja.p,
-                                                                      c->xyz.p, c->grad.p, c->flow, c->work.p, c->phi.p);
-        CFD_LAUNCH_CHECK();
+        // The Roe-average pressure fix (Limiters.cpp:61-110) needs the
+        // reconstructed face states the residual forms anyway: it is done by
+        // the next cfd_residual (or by roe_fix_standalone when the limiters
+        // are read back first).
+        CFD_CUDA(cudaMemsetAsync(c->roecount.p, 0, sizeof(int), c->stream));
+        c->roe_fix_pending = true;
     }
     return CFD_OK;
 }
+
+}  // extern "C"
+
+namespace cfd {
+int roe_fix_standalone(cfd_ctx *c) {
+    if (!c->roe_fix_pending) return CFD_OK;
+    const int n = c->nnode;
+    CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)5 * n)));
+    CFD_CUDA(cudaMemcpyAsync(c->work.p, c->phi.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToDevice, c->stream));
+    k_roe_pressure_fix<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->n2n_ia.p, c->n2n_ja.p, c->xyz.p,
+                                                                  c->grad.p, c->flow, c->work.p, c->phi.p);
+    CFD_LAUNCH_CHECK();
+    c->roe_fix_pending = false;
+    return CFD_OK;
+}
+}  // namespace cfd
+
+extern "C" {
 
 int cfd_get_gradients(cfd_ctx *c, double *g) {
     if (!c || !g || !c->has_grad) return CFD_ERR_STATE;
@@ -332,6 +358,8 @@ int cfd_get_gradients(cfd_ctx *c, double *g) {
 
 int cfd_get_limiters(cfd_ctx *c, double *phi) {
     if (!c || !phi || !c->phi.p) return CFD_ERR_STATE;
+    int st = roe_fix_standalone(c);
+    if (st) return st;
     CFD_CUDA(cudaMemcpyAsync(phi, c->phi.p, sizeof(double) * 5 * c->nnode, cudaMemcpyDeviceToHost, c->stream));
     CFD_CUDA(cudaStreamSynchronize(c->stream));
     return CFD_OK;

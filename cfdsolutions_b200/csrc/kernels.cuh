@@ -155,4 +155,13 @@ __device__ __forceinline__ double load_low(const uint16_t *p) {
 // Deterministic sum of a plain vector (host result).
 int reduce_sum_plain(cfd_ctx *c, const double *x, int64_t n, double *out_host);
 
+// Largest dynamic shared memory the patch residual kernel may use: 11 doubles
+// per patch edge; 128-node patches of a tet mesh list ~1300 edges (~112 KB, two
+// CTAs per SM); larger lists still run, one CTA per SM, up to this cap.
+constexpr size_t kPatchSmemMax = 200 * 1024;
+
+// The limiter's Roe-average pressure fix as its own pass over the node graph
+// (gradient.cu); used when the fused check in the residual cannot run.
+int roe_fix_standalone(cfd_ctx *c);
+
 }  // namespace cfd

@@ -156,6 +156,72 @@ std::vector<int> rcm_order(int n, const std::vector<int> &ia, const std::vector<
     return order;
 }
 
+// Recursive coordinate bisection into patches of exactly `psz` nodes (the last
+// one may be smaller): split the longest extent at a multiple of psz near the
+// middle.  Returns nodes in patch-major order.
+void rcb_patches(const std::vector<double> &xyz, int psz, std::vector<int> &idx, int lo, int hi) {
+    const int n = hi - lo;
+    if (n <= psz) return;
+    double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+    for (int k = lo; k < hi; k++)
+        for (int d = 0; d < 3; d++) {
+            const double v = xyz[3 * (size_t)idx[k] + d];
+            mn[d] = std::min(mn[d], v);
+            mx[d] = std::max(mx[d], v);
+        }
+    int ax = 0;
+    for (int d = 1; d < 3; d++)
+        if (mx[d] - mn[d] > mx[ax] - mn[ax]) ax = d;
+    const int npatch = (n + psz - 1) / psz;
+    const int mid = lo + ((npatch + 1) / 2) * psz;
+    std::nth_element(idx.begin() + lo, idx.begin() + mid, idx.begin() + hi, [&](int a, int b) {
+        const double va = xyz[3 * (size_t)a + ax], vb = xyz[3 * (size_t)b + ax];
+        return va < vb || (va == vb && a < b);
+    });
+    rcb_patches(xyz, psz, idx, lo, mid);
+    rcb_patches(xyz, psz, idx, mid, hi);
+}
+
+// Blocked reverse Cuthill-McKee: RCB patches of psz nodes, patches ordered by
+// RCM of the patch adjacency graph, nodes inside a patch in their original
+// order.  Every patch is then a contiguous, spatially compact node range
+// (what the patch residual kernel works on) and the matrix stays banded at the
+// patch level.  Returns perm[new] = old.
+std::vector<int> patch_rcm_order(int n, const std::vector<double> &xyz, const std::vector<int> &ia,
+                                 const std::vector<int> &ja, int psz) {
+    std::vector<int> idx(n);
+    for (int i = 0; i < n; i++) idx[i] = i;
+    rcb_patches(xyz, psz, idx, 0, n);
+    const int np = (n + psz - 1) / psz;
+    std::vector<int> pid(n);
+    for (int k = 0; k < n; k++) pid[idx[k]] = k / psz;
+    // patch graph
+    std::vector<std::vector<int>> adj(np);
+    for (int a = 0; a < n; a++)
+        for (int k = ia[a]; k < ia[a + 1]; k++) {
+            const int pa = pid[a], pb = pid[ja[k]];
+            if (pa != pb) adj[pa].push_back(pb);
+        }
+    std::vector<int> pia(np + 1, 0), pja;
+    for (int p = 0; p < np; p++) {
+        std::sort(adj[p].begin(), adj[p].end());
+        adj[p].erase(std::unique(adj[p].begin(), adj[p].end()), adj[p].end());
+        pia[p + 1] = pia[p] + (int)adj[p].size();
+        pja.insert(pja.end(), adj[p].begin(), adj[p].end());
+    }
+    std::vector<int> porder = rcm_order(np, pia, pja);  // porder[new] = old patch
+    std::vector<int> perm;
+    perm.reserve(n);
+    for (int q = 0; q < np; q++) {
+        const int p = porder[q];
+        const int b = p * psz, e = std::min(n, b + psz);
+        std::vector<int> nodes(idx.begin() + b, idx.begin() + e);
+        std::sort(nodes.begin(), nodes.end());
+        perm.insert(perm.end(), nodes.begin(), nodes.end());
+    }
+    return perm;
+}
+
 }  // namespace
 
 // Build the median-dual metrics of a tet mesh into m (coords/tets/tris set).
@@ -334,7 +400,10 @@ int build_box(HostMesh &m, int nx, int ny, int nz, double lx, double ly, double 
     if (renumber) {
         std::vector<int> ia, ja;
         build_graph(m.nnode, m.tets, ia, ja);
-        std::vector<int> perm = rcm_order(m.nnode, ia, ja);  // perm[new] = old
+        // perm[new] = old
+        std::vector<int> perm = renumber == CFD_NUMBERING_PATCH_RCM
+                                    ? patch_rcm_order(m.nnode, m.coords, ia, ja, CFD_PATCH_NODES)
+                                    : rcm_order(m.nnode, ia, ja);
         std::vector<int> inv(m.nnode);
         for (int i = 0; i < m.nnode; i++) inv[perm[i]] = i;
         std::vector<double> c2(m.coords.size());

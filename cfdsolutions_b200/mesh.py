@@ -65,15 +65,22 @@ def _export(handle, with_cells: bool) -> Mesh:
     return m
 
 
+NUMBERING_NATURAL, NUMBERING_RCM, NUMBERING_PATCH_RCM = 0, 1, 2
+PATCH_NODES = 128
+
+
 def box_mesh(n: int | tuple[int, int, int], lengths=(1.0, 1.0, 1.0), jitter: float = 0.15, seed: int = 1,
-             rcm: bool = False, face_bc=(1, 1, 1, 1, 1, 1), with_cells: bool = False,
+             rcm: bool | int = False, face_bc=(1, 1, 1, 1, 1, 1), with_cells: bool = False,
              ugrid_path: str | None = None) -> Mesh:
-    """Tet-split box (6 tets per hex), interior nodes jittered by U(+-jitter*h)."""
+    """Tet-split box (6 tets per hex), interior nodes jittered by U(+-jitter*h).
+
+    ``rcm``: False/0 natural numbering, True/1 reverse Cuthill-McKee,
+    2 blocked RCM over 128-node coordinate-bisection patches."""
     nx, ny, nz = (n, n, n) if isinstance(n, int) else n
     fb = np.ascontiguousarray(face_bc, dtype=np.int32)
     h = C.c_void_p()
     capi.check(capi.lib.cfd_mesh_box(nx, ny, nz, float(lengths[0]), float(lengths[1]), float(lengths[2]),
-                                     float(jitter), int(seed), int(bool(rcm)), capi.ptr(fb), C.byref(h)),
+                                     float(jitter), int(seed), int(rcm), capi.ptr(fb), C.byref(h)),
                "cfd_mesh_box")
     try:
         if ugrid_path is not None:

@@ -102,6 +102,7 @@ typedef struct cfd_params {
     double cfl_min;          /* CFL_MIN                      */
     double cfl_max;          /* CFL_MAX                      */
     double venkat_k;         /* VENKAT_K_THRESHOLD           */
+    int    residual_kernel;  /* 0: patch kernel when the mesh fits it, 1: node-gather kernel */
 } cfd_params;
 
 /* Fills p with the defaults used by the reference parameter files of this
@@ -268,12 +269,22 @@ int  cfd_solve_steady(cfd_ctx *ctx, const cfd_solve_opts *o, cfd_solve_stats *st
 /* ----------------------------------------------------- host mesh builder */
 typedef struct cfd_mesh cfd_mesh;
 
+/* Node numberings of the builder.  PATCH_RCM: recursive-coordinate-bisection
+ * patches of CFD_PATCH_NODES nodes, patches ordered by reverse Cuthill-McKee of
+ * the patch graph; the residual kernel computes each edge flux once per patch
+ * (patches are contiguous node ranges of this size), so this numbering makes
+ * the patches spatially compact. */
+#define CFD_NUMBERING_NATURAL   0
+#define CFD_NUMBERING_RCM       1
+#define CFD_NUMBERING_PATCH_RCM 2
+#define CFD_PATCH_NODES 128
+
 /* Tet-split box of nx*ny*nz hexes (6 tets each) over [0,lx]x[0,ly]x[0,lz],
- * interior nodes jittered by U(+-jitter*h) from seed, optional reverse
- * Cuthill-McKee renumbering, face BC types {xmin,xmax,ymin,ymax,zmin,zmax}.
+ * interior nodes jittered by U(+-jitter*h) from seed, node numbering
+ * CFD_NUMBERING_*, face BC types {xmin,xmax,ymin,ymax,zmin,zmax}.
  * Median-dual metrics as Calculate_Area_Volume (Area_Volume.cpp:903). */
 int  cfd_mesh_box(int nx, int ny, int nz, double lx, double ly, double lz,
-                  double jitter, uint64_t seed, int rcm, const int face_bc[6],
+                  double jitter, uint64_t seed, int numbering, const int face_bc[6],
                   cfd_mesh **out);
 /* Same from explicit cells: tets [4*ntet] positively oriented, boundary
  * triangles [3*ntri] with outward right-hand normals, tri_bc [ntri]. */
