@@ -47,13 +47,13 @@ __global__ void k_apply_bc(int nbedge, int64_t ldq, double *__restrict__ Q, cons
     double qI[5], qG[5], qB[5];
 #pragma unroll
     for (int k = 0; k < 5; k++) {
-        qI[k] = Q[(int64_t)nd.x * 5 + k];
-        qG[k] = Q[(int64_t)nd.y * 5 + k];
+        qI[k] = Q[k * ldq + nd.x];
+        qG[k] = Q[k * ldq + nd.y];
     }
     int st = characteristic_bc(qI, qG, g.x, g.y, g.z, btype[b], f, qB);
     if (st) atomicOr(err, st == 1 ? ERR_BC_NEG_PRESSURE : ERR_BC_UNCLASSIFIED);
 #pragma unroll
-    for (int k = 0; k < 5; k++) Q[(int64_t)nd.y * 5 + k] = qB[k];
+    for (int k = 0; k < 5; k++) Q[k * ldq + nd.y] = qB[k];
 }
 
 __device__ __forceinline__ void warp_minmax(double &mn, double &mx) {
@@ -94,13 +94,15 @@ __device__ __forceinline__ void block_extrema3(double mn[3], double mx[3], unsig
 // Euler3D/src/HigherOrderReconstructQ.cpp:21-72) for the side `s` of an edge
 // towards `o`: q = Q_s + phi_s*(frac*(Q_o - Q_s) + (1-frac)*grad_s . r),
 // r = 0.5 (x_o - x_s).
-__device__ __forceinline__ void reconstruct(const double qs[5], const double qo[5], const double *__restrict__ r,
-                                            double rx, double ry, double rz, bool limited, double frac,
-                                            double out[5]) {
+__device__ __forceinline__ void reconstruct(const double qs[5], const double qo[5], int s, double rx, double ry,
+                                            double rz, const double *__restrict__ grad, const double *__restrict__ phi,
+                                            int nnode, bool limited, double frac, double out[5]) {
 #pragma unroll
     for (int k = 0; k < 5; k++) {
-        const double gx = r[REC_GRAD + 3 * k], gy = r[REC_GRAD + 3 * k + 1], gz = r[REC_GRAD + 3 * k + 2];
-        const double ph = limited ? r[REC_PHI + k] : 1.0;
+        const double gx = grad[(3 * k) * (int64_t)nnode + s];
+        const double gy = grad[(3 * k + 1) * (int64_t)nnode + s];
+        const double gz = grad[(3 * k + 2) * (int64_t)nnode + s];
+        const double ph = limited ? phi[k * (int64_t)nnode + s] : 1.0;
         out[k] = qs[k] + ph * (frac * (qo[k] - qs[k]) + (1.0 - frac) * (gx * rx + gy * ry + gz * rz));
     }
 }
@@ -116,7 +118,8 @@ __global__ void __launch_bounds__(128) k_residual_gather(
     int nnode, int64_t ldq, const double *__restrict__ Q, const int *__restrict__ n2e_ptr,
     const int *__restrict__ n2e, const int2 *__restrict__ en, const double4 *__restrict__ eg,
     const int *__restrict__ n2b_ptr, const int *__restrict__ n2b, const int2 *__restrict__ bn,
-    const double4 *__restrict__ bg, const double *__restrict__ rec, Flow f, int add_time, double *__restrict__ res,
+    const double4 *__restrict__ bg, const double *__restrict__ xyz, const double *__restrict__ grad,
+    const double *__restrict__ phi, Flow f, int add_time, double *__restrict__ res,
     double *__restrict__ resd, double *__restrict__ dtsum, unsigned long long *__restrict__ ext) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
@@ -131,17 +134,16 @@ __global__ void __launch_bounds__(128) k_residual_gather(
             double qL[5], qR[5];
 #pragma unroll
             for (int v = 0; v < 5; v++) {
-                qL[v] = Q[(int64_t)nd.x * 5 + v];
-                qR[v] = Q[(int64_t)nd.y * 5 + v];
+                qL[v] = Q[v * ldq + nd.x];
+                qR[v] = Q[v * ldq + nd.y];
             }
             if (SECOND) {
-                const double *recL = rec + (int64_t)nd.x * REC_SIZE, *recR = rec + (int64_t)nd.y * REC_SIZE;
-                const double rx = 0.5 * (recR[REC_XYZ] - recL[REC_XYZ]);
-                const double ry = 0.5 * (recR[REC_XYZ + 1] - recL[REC_XYZ + 1]);
-                const double rz = 0.5 * (recR[REC_XYZ + 2] - recL[REC_XYZ + 2]);
+                const double rx = 0.5 * (xyz[nd.y] - xyz[nd.x]);
+                const double ry = 0.5 * (xyz[nnode + nd.y] - xyz[nnode + nd.x]);
+                const double rz = 0.5 * (xyz[2 * nnode + nd.y] - xyz[2 * nnode + nd.x]);
                 double rL[5], rR[5];
-                reconstruct(qL, qR, recL, rx, ry, rz, limited, f.frac, rL);
-                reconstruct(qR, qL, recR, -rx, -ry, -rz, limited, f.frac, rR);
+                reconstruct(qL, qR, nd.x, rx, ry, rz, grad, phi, nnode, limited, f.frac, rL);
+                reconstruct(qR, qL, nd.y, -rx, -ry, -rz, grad, phi, nnode, limited, f.frac, rR);
 #pragma unroll
                 for (int v = 0; v < 5; v++) { qL[v] = rL[v]; qR[v] = rR[v]; }
             }
@@ -165,8 +167,8 @@ __global__ void __launch_bounds__(128) k_residual_gather(
             double qL[5], qR[5];
 #pragma unroll
             for (int v = 0; v < 5; v++) {
-                qL[v] = Q[(int64_t)nd.x * 5 + v];
-                qR[v] = Q[(int64_t)nd.y * 5 + v];
+                qL[v] = Q[v * ldq + nd.x];
+                qR[v] = Q[v * ldq + nd.y];
             }
             double cf[5], df[5], lam[3];
             const double lmax = edge_flux<FLUX>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam);
@@ -189,6 +191,25 @@ __global__ void __launch_bounds__(128) k_residual_gather(
     if (add_time) block_extrema3(mn, mx, ext);
 }
 
+// Pressure of the Roe-averaged state of two reconstructed face states
+// (Compute_RoeVariables, Roe_Fluxes.cpp:3609-3633, tested in
+// Compute_Limiter_RoePressureCorrection, Limiters.cpp:311-356).
+__device__ __forceinline__ double roe_avg_pressure(const double qa[5], const double qb[5], double g) {
+    const double ra = qa[0], rb = qb[0];
+    const double ia = 1.0 / ra, ib = 1.0 / rb;
+    const double ua = qa[1] * ia, va = qa[2] * ia, wa = qa[3] * ia;
+    const double ub = qb[1] * ib, vb = qb[2] * ib, wb = qb[3] * ib;
+    const double pa = (g - 1.0) * (qa[4] - 0.5 * ra * (ua * ua + va * va + wa * wa));
+    const double pb = (g - 1.0) * (qb[4] - 0.5 * rb * (ub * ub + vb * vb + wb * wb));
+    const double ha = (qa[4] + pa) * ia, hb = (qb[4] + pb) * ib;
+    const double rho = sqrt(ra * rb), sg = rho / (ra + rho);
+    const double u = ua + sg * (ub - ua), v = va + sg * (vb - va), w = wa + sg * (wb - wa);
+    const double ht = ha + sg * (hb - ha);
+    const double q2 = u * u + v * v + w * w;
+    const double e = (rho / g) * (ht + 0.5 * (g - 1.0) * q2);
+    return (g - 1.0) * (e - 0.5 * rho * q2);
+}
+
 // Flux residual, patch form: one CTA per patch of CFD_PATCH_NODES consecutive
 // nodes.  Phase 1 evaluates every edge of the patch once (edges cut by the
 // patch boundary are evaluated by both patches) into shared memory; phase 2
@@ -203,8 +224,8 @@ __global__ void __launch_bounds__(256) k_residual_patch(
     int nnode, int64_t ldq, const double *__restrict__ Q, const int *__restrict__ pe_ptr,
     const int2 *__restrict__ pe_nodes, const double4 *__restrict__ pe_geo, const int *__restrict__ inc_ptr,
     const int *__restrict__ inc, const int *__restrict__ n2b_ptr, const int *__restrict__ n2b,
-    const int2 *__restrict__ bn, const double4 *__restrict__ bg, const double *__restrict__ rec, Flow f,
-    int add_time, int emax,
+    const int2 *__restrict__ bn, const double4 *__restrict__ bg, const double *__restrict__ xyz,
+    const double *__restrict__ grad, const double *__restrict__ phi, Flow f, int add_time, int emax,
     int check_roe, int *__restrict__ roeflag, int *__restrict__ roecount, const int *__restrict__ gate,
     double *__restrict__ res, double *__restrict__ resd, double *__restrict__ dtsum,
     unsigned long long *__restrict__ ext) {
@@ -220,17 +241,16 @@ __global__ void __launch_bounds__(256) k_residual_patch(
         double qL[5], qR[5];
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-            qL[v] = Q[(int64_t)nd.x * 5 + v];
-            qR[v] = Q[(int64_t)nd.y * 5 + v];
+            qL[v] = Q[v * ldq + nd.x];
+            qR[v] = Q[v * ldq + nd.y];
         }
         if (SECOND) {
-            const double *recL = rec + (int64_t)nd.x * REC_SIZE, *recR = rec + (int64_t)nd.y * REC_SIZE;
-            const double rx = 0.5 * (recR[REC_XYZ] - recL[REC_XYZ]);
-            const double ry = 0.5 * (recR[REC_XYZ + 1] - recL[REC_XYZ + 1]);
-            const double rz = 0.5 * (recR[REC_XYZ + 2] - recL[REC_XYZ + 2]);
+            const double rx = 0.5 * (xyz[nd.y] - xyz[nd.x]);
+            const double ry = 0.5 * (xyz[nnode + nd.y] - xyz[nnode + nd.x]);
+            const double rz = 0.5 * (xyz[2 * nnode + nd.y] - xyz[2 * nnode + nd.x]);
             double rL[5], rR[5];
-            reconstruct(qL, qR, recL, rx, ry, rz, limited, f.frac, rL);
-            reconstruct(qR, qL, recR, -rx, -ry, -rz, limited, f.frac, rR);
+            reconstruct(qL, qR, nd.x, rx, ry, rz, grad, phi, nnode, limited, f.frac, rL);
+            reconstruct(qR, qL, nd.y, -rx, -ry, -rz, grad, phi, nnode, limited, f.frac, rR);
 #pragma unroll
             for (int v = 0; v < 5; v++) { qL[v] = rL[v]; qR[v] = rR[v]; }
             if (check_roe && roe_avg_pressure(qL, qR, f.gamma) < 0.0) {
@@ -274,8 +294,8 @@ __global__ void __launch_bounds__(256) k_residual_patch(
             double qL[5], qR[5];
 #pragma unroll
             for (int v = 0; v < 5; v++) {
-                qL[v] = Q[(int64_t)nd.x * 5 + v];
-                qR[v] = Q[(int64_t)nd.y * 5 + v];
+                qL[v] = Q[v * ldq + nd.x];
+                qR[v] = Q[v * ldq + nd.y];
             }
             double cf[5], df[5], lam[3];
             const double lmax = edge_flux<FLUX>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam);
@@ -301,12 +321,12 @@ __global__ void __launch_bounds__(256) k_residual_patch(
 // Limiter pressure fix selected by the residual's check: zero the limiters of
 // flagged nodes; no-op unless some edge failed (*count == 0).
 __global__ void k_roe_fix_apply(int nnode, const int *__restrict__ count, const int *__restrict__ flag,
-                                double *__restrict__ rec) {
+                                double *__restrict__ phi) {
     if (*count == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnode || !flag[i]) return;
 #pragma unroll
-    for (int v = 0; v < 5; v++) rec[(int64_t)i * REC_SIZE + REC_PHI + v] = 0.0;
+    for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = 0.0;
 }
 
 // dt_i = V_i * CFL / sum_i (Compute_DeltaT, Euler3D/src/Time_Step.cpp:23-51).
@@ -402,8 +422,8 @@ __global__ void __launch_bounds__(128) k_jac_edges(int nedge, int64_t ldq, const
     double qL[5], qR[5];
 #pragma unroll
     for (int v = 0; v < 5; v++) {
-        qL[v] = Q[(int64_t)nd.x * 5 + v];
-        qR[v] = Q[(int64_t)nd.y * 5 + v];
+        qL[v] = Q[v * ldq + nd.x];
+        qR[v] = Q[v * ldq + nd.y];
     }
     double Ab[25], J[25];
     roe_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
@@ -456,8 +476,8 @@ __global__ void __launch_bounds__(128) k_jac_rows(
         double qL[5], qR[5], Ab[25], J[25];
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-            qL[v] = Q[(int64_t)nd.x * 5 + v];
-            qR[v] = Q[(int64_t)nd.y * 5 + v];
+            qL[v] = Q[v * ldq + nd.x];
+            qR[v] = Q[v * ldq + nd.y];
         }
         roe_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
         euler_flux_jacobian(qL, g.x, g.y, g.z, f.gamma, J);
@@ -580,33 +600,7 @@ __global__ void k_update(int nnode, int64_t ldq, double relax, const double *__r
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnode) return;
 #pragma unroll
-    for (int v = 0; v < 5; v++) Q[(int64_t)i * 5 + v] += relax * X[(int64_t)i * 5 + v];
-}
-
-// Boundary layout <-> device layout of the state: SoA [5][n] <-> node-major [n][5].
-__global__ void k_soa_to_aos(int64_t n, const double *__restrict__ a, double *__restrict__ q) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-#pragma unroll
-    for (int v = 0; v < 5; v++) q[i * 5 + v] = a[v * n + i];
-}
-
-__global__ void k_aos_to_soa(int64_t n, const double *__restrict__ q, double *__restrict__ a) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-#pragma unroll
-    for (int v = 0; v < 5; v++) a[v * n + i] = q[i * 5 + v];
-}
-
-// Coordinates into the per-node reconstruction records.
-__global__ void k_rec_coords(int nnode, const double *__restrict__ xyz, double *__restrict__ rec) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nnode) return;
-    double *r = rec + (int64_t)i * REC_SIZE;
-    r[REC_XYZ] = xyz[i];
-    r[REC_XYZ + 1] = xyz[nnode + i];
-    r[REC_XYZ + 2] = xyz[2 * nnode + i];
-    r[REC_SIZE - 1] = 0.0;
+    for (int v = 0; v < 5; v++) Q[v * ldq + i] += relax * X[(int64_t)i * 5 + v];
 }
 
 __global__ void k_freestream(int n, int64_t ldq, Flow f, double *__restrict__ Q) {
@@ -614,9 +608,9 @@ __global__ void k_freestream(int n, int64_t ldq, Flow f, double *__restrict__ Q)
     if (i >= n) return;
     Q[i] = f.inf_rho;
     Q[ldq + i] = f.inf_rho * f.inf_u;
-    Q[(int64_t)i * 5 + 2] = f.inf_rho * f.inf_v;
-    Q[(int64_t)i * 5 + 3] = f.inf_rho * f.inf_w;
-    Q[(int64_t)i * 5 + 4] = f.inf_rho * f.inf_et;
+    Q[2 * ldq + i] = f.inf_rho * f.inf_v;
+    Q[3 * ldq + i] = f.inf_rho * f.inf_w;
+    Q[4 * ldq + i] = f.inf_rho * f.inf_et;
 }
 
 // ------------------------------------------------------------- host helpers
@@ -702,14 +696,14 @@ static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, const int *
                                           (int)kPatchSmemMax));
         k_residual_patch<FLUX, SECOND><<<c->npatch, 256, smem, c->stream>>>(
             c->nnode, c->ldq, c->Q.p, c->pe_ptr.p, c->pe_nodes.p, c->pe_geo.p, c->inc_ptr.p, c->inc.p, c->n2b_ptr.p,
-            c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p, c->rec.p, c->flow, add_time,
+            c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p, c->xyz.p, c->grad.p, c->phi.p, c->flow, add_time,
             c->patch_emax, check_roe ? 1 : 0, c->roeflag.p, c->roecount.p, gate, c->res.p, c->resd.p, c->dt.p,
             c->ext.p);
     } else {
         if (gate || check_roe) return CFD_ERR_UNSUPPORTED;
         k_residual_gather<FLUX, SECOND><<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(
             c->nnode, c->ldq, c->Q.p, c->n2e_ptr.p, c->n2e.p, c->edge_nodes.p, c->edge_geo.p, c->n2b_ptr.p,
-            c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p, c->rec.p, c->flow, add_time, c->res.p,
+            c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p, c->xyz.p, c->grad.p, c->phi.p, c->flow, add_time, c->res.p,
             c->resd.p, c->dt.p, c->ext.p);
     }
     CFD_LAUNCH_CHECK();
@@ -724,7 +718,7 @@ static int residual_with_fix(cfd_ctx *c, int add_time) {
     const bool fused = SECOND && FLUX == CFD_FLUX_ROE && c->roe_fix_pending && patch_kernel(c);
     int st = launch_residual<FLUX, SECOND>(c, add_time, fused, nullptr);
     if (st || !fused) return st;
-    k_roe_fix_apply<<<grid_for(c->nnode, 256), 256, 0, c->stream>>>(c->nnode, c->roecount.p, c->roeflag.p, c->rec.p);
+    k_roe_fix_apply<<<grid_for(c->nnode, 256), 256, 0, c->stream>>>(c->nnode, c->roecount.p, c->roeflag.p, c->phi.p);
     CFD_LAUNCH_CHECK();
     c->roe_fix_pending = false;
     return launch_residual<FLUX, SECOND>(c, add_time, false, c->roecount.p);
@@ -912,7 +906,6 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
     c->has_mesh = false;
     c->has_system = false;
     c->has_grad = false;
-    c->has_phi = false;
     c->lsq_weight = -1;
     c->nnode = nnode;
     c->nghost = nghost;
@@ -1095,10 +1088,6 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
     }
     // ---- state and work arrays
     CFD_CUDA(c->Q.alloc((size_t)5 * c->ldq));
-    CFD_CUDA(c->rec.alloc((size_t)REC_SIZE * nnode));
-    CFD_CUDA(cudaMemsetAsync(c->rec.p, 0, sizeof(double) * REC_SIZE * nnode, s));
-    k_rec_coords<<<grid_for(nnode, 256), 256, 0, s>>>(nnode, c->xyz.p, c->rec.p);
-    CFD_LAUNCH_CHECK();
     CFD_CUDA(c->res.alloc((size_t)5 * nnode));
     CFD_CUDA(c->resd.alloc((size_t)5 * nnode));
     CFD_CUDA(c->dt.alloc(nnode));
@@ -1129,10 +1118,8 @@ int cfd_set_state(cfd_ctx *c, const double *Q) {
     NEED_MESH("cfd_set_state");
     if (!Q) return CFD_ERR_ARG;
     const int64_t n = (int64_t)c->nnode + c->nghost;
-    CFD_CUDA(c->qsoa.alloc((size_t)5 * n));
-    CFD_CUDA(cudaMemcpyAsync(c->qsoa.p, Q, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, c->stream));
-    k_soa_to_aos<<<grid_for(n, 256), 256, 0, c->stream>>>(n, c->qsoa.p, c->Q.p);
-    CFD_LAUNCH_CHECK();
+    CFD_CUDA(cudaMemcpy2DAsync(c->Q.p, c->ldq * sizeof(double), Q, n * sizeof(double), n * sizeof(double), 5,
+                               cudaMemcpyHostToDevice, c->stream));
     return CFD_OK;
 }
 
@@ -1140,10 +1127,8 @@ int cfd_get_state(cfd_ctx *c, double *Q) {
     NEED_MESH("cfd_get_state");
     if (!Q) return CFD_ERR_ARG;
     const int64_t n = (int64_t)c->nnode + c->nghost;
-    CFD_CUDA(c->qsoa.alloc((size_t)5 * n));
-    k_aos_to_soa<<<grid_for(n, 256), 256, 0, c->stream>>>(n, c->Q.p, c->qsoa.p);
-    CFD_LAUNCH_CHECK();
-    CFD_CUDA(cudaMemcpyAsync(Q, c->qsoa.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, c->stream));
+    CFD_CUDA(cudaMemcpy2DAsync(Q, n * sizeof(double), c->Q.p, c->ldq * sizeof(double), n * sizeof(double), 5,
+                               cudaMemcpyDeviceToHost, c->stream));
     CFD_CUDA(cudaStreamSynchronize(c->stream));
     return CFD_OK;
 }
@@ -1151,7 +1136,7 @@ int cfd_get_state(cfd_ctx *c, double *Q) {
 int cfd_state_device_ptr(cfd_ctx *c, double **dQ, int64_t *ld) {
     NEED_MESH("cfd_state_device_ptr");
     if (dQ) *dQ = c->Q.p;
-    if (ld) *ld = 5;
+    if (ld) *ld = c->ldq;
     return CFD_OK;
 }
 
@@ -1189,7 +1174,7 @@ int cfd_residual(cfd_ctx *c, int add_time) {
         set_error("cfd_residual: second order needs cfd_gradient first");
         return CFD_ERR_STATE;
     }
-    if (second && c->params.limiter != CFD_LIMITER_NONE && !c->has_phi) {
+    if (second && c->params.limiter != CFD_LIMITER_NONE && !c->phi.p) {
         set_error("cfd_residual: limiter requested but cfd_limiter not called");
         return CFD_ERR_STATE;
     }

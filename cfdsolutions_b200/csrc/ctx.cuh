@@ -44,11 +44,6 @@ struct DevBuf {
 
 // Level schedule of a sparse triangular dependency (rows grouped so that the
 // rows of one level only depend on rows of earlier levels).
-// Node-major reconstruction record (one 192-byte, 32-byte aligned record per
-// node, so a neighbour gather touches 6 contiguous sectors instead of 23
-// scattered ones): limiter phi[5], gradients d(Q_v)/dx_d at 5+3v+d, coordinates.
-constexpr int REC_PHI = 0, REC_GRAD = 5, REC_XYZ = 20, REC_SIZE = 24;
-
 struct Levels {
     std::vector<int> ptr;  // host, nlevels+1
     DevBuf<int> rows;      // device, rows in level order
@@ -67,7 +62,7 @@ struct cfd_ctx {
 
     int nnode = 0, nghost = 0, nedge = 0, nbedge = 0;
     int64_t nnzb = 0;
-    int64_t ldq = 0;  // rows of Q (>= nnode + nghost)
+    int64_t ldq = 0;  // leading dimension of Q (>= nnode + nghost)
 
     // mesh
     cfd::DevBuf<int2> edge_nodes;
@@ -101,12 +96,12 @@ struct cfd_ctx {
     bool roe_fix_pending = false;
 
     // state and residual
-    cfd::DevBuf<double> Q;      // [ldq][5] node-major (conservative variables of one node contiguous)
+    cfd::DevBuf<double> Q;      // [5][ldq]
     cfd::DevBuf<double> res;    // [5][nnode] convective
     cfd::DevBuf<double> resd;   // [5][nnode] dissipative
     cfd::DevBuf<double> dt;     // [nnode] sum(area*lambda) then DeltaT
-    cfd::DevBuf<double> rec;    // [nnode][REC_SIZE] limiter | gradients | coordinates, node-major
-    cfd::DevBuf<double> qsoa;   // staging of the SoA boundary layout of Q
+    cfd::DevBuf<double> grad;   // [15][nnode]
+    cfd::DevBuf<double> phi;    // [5][nnode]
     cfd::DevBuf<double> ggw;    // least-squares per-node coefficients [nnode][8]
     int lsq_weight = -1;        // weight the coefficients in ggw were built for
     cfd::DevBuf<unsigned long long> ext;  // 8 extrema as ordered bit patterns
@@ -133,7 +128,6 @@ struct cfd_ctx {
     int krylov_m = 0;
     bool has_system = false;
     bool has_grad = false;
-    bool has_phi = false;
 };
 
 namespace cfd {

@@ -1,9 +1,7 @@
 // Node gradients (least squares as the reference, or Green-Gauss on the median
-// dual) and the Venkatakrishnan / Barth-Jespersen limiters with the
-// reference's pressure corrections.  One thread per node, neighbour loops in
-// the node graph's fixed (sorted) order, so every result is deterministic.
-// Gradients, limiters and coordinates live in one node-major record per node
-// (REC_* in ctx.cuh) so that the residual's neighbour gathers stay contiguous.
+// dual) and the Venkatakrishnan limiter with the reference's pressure
+// corrections.  One thread per node, neighbour loops in the node graph's fixed
+// (sorted) order, so every result is deterministic.
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -14,43 +12,32 @@
 
 namespace cfd {
 
-__device__ __forceinline__ void rec_xyz(const double *__restrict__ rec, int i, double &x, double &y, double &z) {
-    const double *r = rec + (int64_t)i * REC_SIZE + REC_XYZ;
-    x = r[0];
-    y = r[1];
-    z = r[2];
-}
-
 // Least-squares Gram-Schmidt coefficients r11..r33, ro22, ro33
 // (Compute_Least_Square_Gradient_Coefficients, Euler3D/src/Gradient.cpp:137-228).
 __global__ void k_lsq_coeff(int nnode, const int *__restrict__ ia, const int *__restrict__ ja,
-                            const double *__restrict__ rec, int weighted, double *__restrict__ cf) {
+                            const double *__restrict__ xyz, int weighted, double *__restrict__ cf) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnode) return;
-    double xi, yi, zi;
-    rec_xyz(rec, i, xi, yi, zi);
+    const double xi = xyz[i], yi = xyz[nnode + i], zi = xyz[2 * nnode + i];
     double r11 = 0, r12 = 0, r13 = 0, r22 = 0, r23 = 0, r33 = 0, ro22 = 0, ro33 = 0;
     for (int k = ia[i]; k < ia[i + 1]; k++) {
-        double xj, yj, zj;
-        rec_xyz(rec, ja[k], xj, yj, zj);
-        double dx = xj - xi, dy = yj - yi, dz = zj - zi;
+        const int j = ja[k];
+        double dx = xyz[j] - xi, dy = xyz[nnode + j] - yi, dz = xyz[2 * nnode + j] - zi;
         const double a = weighted ? 1.0 / sqrt(dx * dx + dy * dy + dz * dz) : 1.0;
         dx *= a; dy *= a; dz *= a;
         r11 += dx * dx; r12 += dx * dy; r13 += dx * dz;
     }
     for (int k = ia[i]; k < ia[i + 1]; k++) {
-        double xj, yj, zj;
-        rec_xyz(rec, ja[k], xj, yj, zj);
-        double dx = xj - xi, dy = yj - yi, dz = zj - zi;
+        const int j = ja[k];
+        double dx = xyz[j] - xi, dy = xyz[nnode + j] - yi, dz = xyz[2 * nnode + j] - zi;
         const double a = weighted ? 1.0 / sqrt(dx * dx + dy * dy + dz * dz) : 1.0;
         dx *= a; dy *= a; dz *= a;
         const double t = dy - (r12 / r11) * dx;
         r22 += t * t; r23 += t * dz; ro22 += t * dy;
     }
     for (int k = ia[i]; k < ia[i + 1]; k++) {
-        double xj, yj, zj;
-        rec_xyz(rec, ja[k], xj, yj, zj);
-        double dx = xj - xi, dy = yj - yi, dz = zj - zi;
+        const int j = ja[k];
+        double dx = xyz[j] - xi, dy = xyz[nnode + j] - yi, dz = xyz[2 * nnode + j] - zi;
         const double a = weighted ? 1.0 / sqrt(dx * dx + dy * dy + dz * dz) : 1.0;
         dx *= a; dy *= a; dz *= a;
         const double t = dz - (r13 / r11) * dx - (r23 / r22) * (dy - (r12 / r11) * dx);
@@ -61,23 +48,21 @@ __global__ void k_lsq_coeff(int nnode, const int *__restrict__ ia, const int *__
 }
 
 // Least-squares gradient of Q1..Q5 (Compute_Least_Square_Gradient, Gradient.cpp:232-296).
-__global__ void __launch_bounds__(128) k_lsq_grad(int nnode, const double *__restrict__ Q, const int *__restrict__ ia,
-                                                  const int *__restrict__ ja, int weighted,
-                                                  const double *__restrict__ cf, double *__restrict__ rec) {
+__global__ void __launch_bounds__(128) k_lsq_grad(int nnode, int64_t ldq, const double *__restrict__ Q,
+                                                  const int *__restrict__ ia, const int *__restrict__ ja,
+                                                  const double *__restrict__ xyz, int weighted,
+                                                  const double *__restrict__ cf, double *__restrict__ g) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnode) return;
     const double *c = cf + (int64_t)i * 8;
     const double r11 = c[0], r12 = c[1], r13 = c[2], r22 = c[3], r23 = c[4], ro22 = c[6], ro33 = c[7];
-    double xi, yi, zi;
-    rec_xyz(rec, i, xi, yi, zi);
+    const double xi = xyz[i], yi = xyz[nnode + i], zi = xyz[2 * nnode + i];
     double qi[5], gx[5] = {0, 0, 0, 0, 0}, gy[5] = {0, 0, 0, 0, 0}, gz[5] = {0, 0, 0, 0, 0};
 #pragma unroll
-    for (int v = 0; v < 5; v++) qi[v] = Q[(int64_t)i * 5 + v];
+    for (int v = 0; v < 5; v++) qi[v] = Q[v * ldq + i];
     for (int k = ia[i]; k < ia[i + 1]; k++) {
         const int j = ja[k];
-        double xj, yj, zj;
-        rec_xyz(rec, j, xj, yj, zj);
-        double dx = xj - xi, dy = yj - yi, dz = zj - zi;
+        double dx = xyz[j] - xi, dy = xyz[nnode + j] - yi, dz = xyz[2 * nnode + j] - zi;
         const double a = weighted ? 1.0 / sqrt(dx * dx + dy * dy + dz * dz) : 1.0;
         dx *= a; dy *= a; dz *= a;
         const double Wz = (dz - (r13 / r11) * dx - (r23 / r22) * (dy - (r12 / r11) * dx)) / ro33;
@@ -85,18 +70,17 @@ __global__ void __launch_bounds__(128) k_lsq_grad(int nnode, const double *__res
         const double Wx = (dx - r12 * Wy - r13 * Wz) / r11;
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-            const double d = Q[(int64_t)j * 5 + v] - qi[v];
+            const double d = Q[v * ldq + j] - qi[v];
             gx[v] += Wx * a * d;
             gy[v] += Wy * a * d;
             gz[v] += Wz * a * d;
         }
     }
-    double *r = rec + (int64_t)i * REC_SIZE + REC_GRAD;
 #pragma unroll
     for (int v = 0; v < 5; v++) {
-        r[3 * v] = gx[v];
-        r[3 * v + 1] = gy[v];
-        r[3 * v + 2] = gz[v];
+        g[(3 * v) * (int64_t)nnode + i] = gx[v];
+        g[(3 * v + 1) * (int64_t)nnode + i] = gy[v];
+        g[(3 * v + 2) * (int64_t)nnode + i] = gz[v];
     }
 }
 
@@ -106,15 +90,15 @@ __global__ void __launch_bounds__(128) k_lsq_grad(int nnode, const double *__res
 // (1/V_i) sum_j (Q_j - Q_i)/2 S_ij so that uniform fields give exactly zero.
 // (The reference declares GRADINET_METHOD_GREEN_GAUSS, SolverParameters.h:329,
 // without implementing it.)
-__global__ void __launch_bounds__(128) k_gg_grad(int nnode, const double *__restrict__ Q,
+__global__ void __launch_bounds__(128) k_gg_grad(int nnode, int64_t ldq, const double *__restrict__ Q,
                                                  const int *__restrict__ n2e_ptr, const int *__restrict__ n2e,
                                                  const int2 *__restrict__ en, const double4 *__restrict__ es,
-                                                 const double *__restrict__ vol, double *__restrict__ rec) {
+                                                 const double *__restrict__ vol, double *__restrict__ g) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnode) return;
     double qi[5], gx[5] = {0, 0, 0, 0, 0}, gy[5] = {0, 0, 0, 0, 0}, gz[5] = {0, 0, 0, 0, 0};
 #pragma unroll
-    for (int v = 0; v < 5; v++) qi[v] = Q[(int64_t)i * 5 + v];
+    for (int v = 0; v < 5; v++) qi[v] = Q[v * ldq + i];
     for (int k = n2e_ptr[i]; k < n2e_ptr[i + 1]; k++) {
         const int s = n2e[k];
         const int e = s >= 0 ? s : ~s;
@@ -125,56 +109,55 @@ __global__ void __launch_bounds__(128) k_gg_grad(int nnode, const double *__rest
         const double sx = sg * S.x, sy = sg * S.y, sz = sg * S.z;
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-            const double d = Q[(int64_t)j * 5 + v] - qi[v];
+            const double d = Q[v * ldq + j] - qi[v];
             gx[v] += d * sx;
             gy[v] += d * sy;
             gz[v] += d * sz;
         }
     }
     const double vi = 1.0 / vol[i];
-    double *r = rec + (int64_t)i * REC_SIZE + REC_GRAD;
 #pragma unroll
     for (int v = 0; v < 5; v++) {
-        r[3 * v] = gx[v] * vi;
-        r[3 * v + 1] = gy[v] * vi;
-        r[3 * v + 2] = gz[v] * vi;
+        g[(3 * v) * (int64_t)nnode + i] = gx[v] * vi;
+        g[(3 * v + 1) * (int64_t)nnode + i] = gy[v] * vi;
+        g[(3 * v + 2) * (int64_t)nnode + i] = gz[v] * vi;
     }
 }
 
 // Venkatakrishnan limiter per node (Compute_Limiter_Venkatakrishnan,
-// Euler3D/src/Limiters.cpp:185-267) or Barth-Jespersen (:117-178), optional
-// variable smoothing (:50-58) and the reconstructed-pressure correction
-// (Compute_Limiter_PressureCorrection, :273-304).  Writes phi into the
-// node's record and clears the node's Roe-pressure flag.
-__global__ void __launch_bounds__(128) k_venkat(int nnode, const double *__restrict__ Q, const int *__restrict__ ia,
-                                                const int *__restrict__ ja, const double *__restrict__ vol, Flow f,
-                                                double *__restrict__ rec, int *__restrict__ roeflag) {
+// Euler3D/src/Limiters.cpp:185-267), optional variable smoothing (:50-58) and
+// the reconstructed-pressure correction (Compute_Limiter_PressureCorrection,
+// :273-304).
+__global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const double *__restrict__ Q,
+                                                const int *__restrict__ ia, const int *__restrict__ ja,
+                                                const double *__restrict__ xyz, const double *__restrict__ g,
+                                                const double *__restrict__ vol, Flow f, double *__restrict__ phi,
+                                                int *__restrict__ roeflag) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnode) return;
     roeflag[i] = 0;
     const double frac = f.frac;
-    const double *ri = rec + (int64_t)i * REC_SIZE;
     double qc[5], qmin[5], qmax[5], ph[5], gx[5], gy[5], gz[5];
 #pragma unroll
     for (int v = 0; v < 5; v++) {
-        qc[v] = Q[(int64_t)i * 5 + v];
+        qc[v] = Q[v * ldq + i];
         qmin[v] = qmax[v] = qc[v];
         ph[v] = 1.0;
-        gx[v] = ri[REC_GRAD + 3 * v];
-        gy[v] = ri[REC_GRAD + 3 * v + 1];
-        gz[v] = ri[REC_GRAD + 3 * v + 2];
+        gx[v] = g[(3 * v) * (int64_t)nnode + i];
+        gy[v] = g[(3 * v + 1) * (int64_t)nnode + i];
+        gz[v] = g[(3 * v + 2) * (int64_t)nnode + i];
     }
     const double eps2 = 6.0 * f.venkat_eps_k3 * vol[i] / M_PI;
     for (int k = ia[i]; k < ia[i + 1]; k++) {
-        const double *qj = Q + (int64_t)ja[k] * 5;
+        const int j = ja[k];
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-            qmin[v] = fmin(qmin[v], qj[v]);
-            qmax[v] = fmax(qmax[v], qj[v]);
+            const double q = Q[v * ldq + j];
+            qmin[v] = fmin(qmin[v], q);
+            qmax[v] = fmax(qmax[v], q);
         }
     }
-    double xi, yi, zi;
-    rec_xyz(rec, i, xi, yi, zi);
+    const double xi = xyz[i], yi = xyz[nnode + i], zi = xyz[2 * nnode + i];
     if (f.limiter == CFD_LIMITER_VENKAT) {
         // phi = min(1, min_edges num/den) with num, den >= 0 (dm and dp share
         // their sign).  The running minimum is kept as a fraction and compared
@@ -184,13 +167,10 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, const double *__restr
         double bn[5] = {1, 1, 1, 1, 1}, bd[5] = {1, 1, 1, 1, 1};
         for (int k = ia[i]; k < ia[i + 1]; k++) {
             const int j = ja[k];
-            double xj, yj, zj;
-            rec_xyz(rec, j, xj, yj, zj);
-            const double rx = 0.5 * (xj - xi), ry = 0.5 * (yj - yi), rz = 0.5 * (zj - zi);
-            const double *qj = Q + (int64_t)j * 5;
+            const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
 #pragma unroll
             for (int v = 0; v < 5; v++) {
-                const double q = qc[v] + frac * (qj[v] - qc[v]) + (1.0 - frac) * (gx[v] * rx + gy[v] * ry + gz[v] * rz);
+                const double q = qc[v] + frac * (Q[v * ldq + j] - qc[v]) + (1.0 - frac) * (gx[v] * rx + gy[v] * ry + gz[v] * rz);
                 const double dm = q - qc[v];
                 if (dm != 0.0) {
                     const double dp = (dm > 0.0 ? qmax[v] : qmin[v]) - qc[v];
@@ -202,16 +182,13 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, const double *__restr
         }
 #pragma unroll
         for (int v = 0; v < 5; v++) ph[v] = fmax(0.0, bn[v] == bd[v] ? 1.0 : bn[v] / bd[v]);
-    } else {  // Barth-Jespersen
+    } else {  // Barth-Jespersen (Compute_Limiter_Barth_Jespersen, Limiters.cpp:117-178)
         for (int k = ia[i]; k < ia[i + 1]; k++) {
             const int j = ja[k];
-            double xj, yj, zj;
-            rec_xyz(rec, j, xj, yj, zj);
-            const double rx = 0.5 * (xj - xi), ry = 0.5 * (yj - yi), rz = 0.5 * (zj - zi);
-            const double *qj = Q + (int64_t)j * 5;
+            const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
 #pragma unroll
             for (int v = 0; v < 5; v++) {
-                const double q = qc[v] + frac * (qj[v] - qc[v]) + (1.0 - frac) * (gx[v] * rx + gy[v] * ry + gz[v] * rz);
+                const double q = qc[v] + frac * (Q[v * ldq + j] - qc[v]) + (1.0 - frac) * (gx[v] * rx + gy[v] * ry + gz[v] * rz);
                 const double dm = q - qc[v];
                 double t = 1.0;
                 if (dm > 0.0) t = fmin(1.0, (qmax[v] - qc[v]) / dm);
@@ -231,91 +208,71 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, const double *__restr
     bool neg = false;
     for (int k = ia[i]; k < ia[i + 1]; k++) {
         const int j = ja[k];
-        double xj, yj, zj;
-        rec_xyz(rec, j, xj, yj, zj);
-        const double rx = 0.5 * (xj - xi), ry = 0.5 * (yj - yi), rz = 0.5 * (zj - zi);
-        const double *qj = Q + (int64_t)j * 5;
+        const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
         double q[5];
 #pragma unroll
         for (int v = 0; v < 5; v++)
-            q[v] = qc[v] + ph[v] * (frac * (qj[v] - qc[v]) + (1.0 - frac) * (gx[v] * rx + gy[v] * ry + gz[v] * rz));
+            q[v] = qc[v] + ph[v] * (frac * (Q[v * ldq + j] - qc[v]) + (1.0 - frac) * (gx[v] * rx + gy[v] * ry + gz[v] * rz));
         const double p = f.gm1 * (q[4] - (0.5 / q[0]) * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]));
         if (p < 0.0) neg = true;
     }
-    double *po = rec + (int64_t)i * REC_SIZE + REC_PHI;
+    if (neg) {
 #pragma unroll
-    for (int v = 0; v < 5; v++) po[v] = neg ? 0.0 : ph[v];
+        for (int v = 0; v < 5; v++) ph[v] = 0.0;
+    }
+#pragma unroll
+    for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = ph[v];
 }
 
 // Roe-average pressure correction (Compute_Limiter_RoePressureCorrection,
 // Limiters.cpp:311-356, applied for the Roe flux at :61-110): a node's limiters
 // drop to zero when the Roe-averaged state of any of its reconstructed edges
 // has negative pressure.  Evaluated against the limiters of the previous
-// pass (phi_in, [5][nnode]) in Jacobi order; the reference sweeps nodes in
-// sequence, which gives the same result whenever the fix does not cascade.
-// (For two states of positive pressure the Roe-averaged pressure is itself
-// positive, so after the per-node correction above this fix only acts at
-// round-off level.)
-__global__ void __launch_bounds__(128) k_roe_pressure_fix(int nnode, const double *__restrict__ Q,
+// pass (Jacobi order); the reference sweeps nodes in sequence, which gives
+// the same result whenever this fix does not cascade.
+__global__ void __launch_bounds__(128) k_roe_pressure_fix(int nnode, int64_t ldq, const double *__restrict__ Q,
                                                           const int *__restrict__ ia, const int *__restrict__ ja,
-                                                          Flow f, const double *__restrict__ phi_in,
-                                                          double *__restrict__ rec) {
+                                                          const double *__restrict__ xyz,
+                                                          const double *__restrict__ g, Flow f,
+                                                          const double *__restrict__ phi_in, double *__restrict__ phi) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnode) return;
     const double frac = f.frac;
     bool neg = false;
-    double xi, yi, zi;
-    rec_xyz(rec, i, xi, yi, zi);
-    const double *ri = rec + (int64_t)i * REC_SIZE;
+    const double xi = xyz[i], yi = xyz[nnode + i], zi = xyz[2 * nnode + i];
     for (int k = ia[i]; k < ia[i + 1] && !neg; k++) {
         const int j = ja[k];
-        const double *rj = rec + (int64_t)j * REC_SIZE;
-        double xj, yj, zj;
-        rec_xyz(rec, j, xj, yj, zj);
-        const double rx = 0.5 * (xj - xi), ry = 0.5 * (yj - yi), rz = 0.5 * (zj - zi);
+        const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
         double qa[5], qb[5];
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-            const double ci = Q[(int64_t)i * 5 + v], cj = Q[(int64_t)j * 5 + v];
+            const double ci = Q[v * ldq + i], cj = Q[v * ldq + j];
             const double pi_ = phi_in[v * (int64_t)nnode + i], pj = phi_in[v * (int64_t)nnode + j];
-            qa[v] = ci + pi_ * (frac * (cj - ci) + (1.0 - frac) * (ri[REC_GRAD + 3 * v] * rx + ri[REC_GRAD + 3 * v + 1] * ry +
-                                                                  ri[REC_GRAD + 3 * v + 2] * rz));
-            qb[v] = cj + pj * (frac * (ci - cj) - (1.0 - frac) * (rj[REC_GRAD + 3 * v] * rx + rj[REC_GRAD + 3 * v + 1] * ry +
-                                                                 rj[REC_GRAD + 3 * v + 2] * rz));
+            qa[v] = ci + pi_ * (frac * (cj - ci) + (1.0 - frac) * (g[(3 * v) * (int64_t)nnode + i] * rx +
+                                                                  g[(3 * v + 1) * (int64_t)nnode + i] * ry +
+                                                                  g[(3 * v + 2) * (int64_t)nnode + i] * rz));
+            qb[v] = cj + pj * (frac * (ci - cj) - (1.0 - frac) * (g[(3 * v) * (int64_t)nnode + j] * rx +
+                                                                 g[(3 * v + 1) * (int64_t)nnode + j] * ry +
+                                                                 g[(3 * v + 2) * (int64_t)nnode + j] * rz));
         }
-        if (roe_avg_pressure(qa, qb, f.gamma) < 0.0) neg = true;
+        // Compute_RoeVariables (Roe_Fluxes.cpp:3609-3633)
+        const double ra = qa[0], rb = qb[0];
+        const double ua = qa[1] / ra, va = qa[2] / ra, wa = qa[3] / ra;
+        const double ub = qb[1] / rb, vb = qb[2] / rb, wb = qb[3] / rb;
+        const double pa = f.gm1 * (qa[4] - 0.5 * ra * (ua * ua + va * va + wa * wa));
+        const double pb = f.gm1 * (qb[4] - 0.5 * rb * (ub * ub + vb * vb + wb * wb));
+        const double ha = (qa[4] + pa) / ra, hb = (qb[4] + pb) / rb;
+        const double rho = sqrt(ra * rb), sg = rho / (ra + rho);
+        const double u = ua + sg * (ub - ua), v = va + sg * (vb - va), w = wa + sg * (wb - wa);
+        const double ht = ha + sg * (hb - ha);
+        double qr[5];
+        qr[0] = rho; qr[1] = rho * u; qr[2] = rho * v; qr[3] = rho * w;
+        qr[4] = (rho / f.gamma) * (ht + 0.5 * f.gm1 * (u * u + v * v + w * w));
+        const double p = f.gm1 * (qr[4] - (0.5 / qr[0]) * (qr[1] * qr[1] + qr[2] * qr[2] + qr[3] * qr[3]));
+        if (p < 0.0) neg = true;
     }
-    if (neg) {
 #pragma unroll
-        for (int v = 0; v < 5; v++) rec[(int64_t)i * REC_SIZE + REC_PHI + v] = 0.0;
-    }
-}
-
-__global__ void k_rec_phi_to_soa(int nnode, const double *__restrict__ rec, double *__restrict__ phi) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nnode) return;
-#pragma unroll
-    for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = rec[(int64_t)i * REC_SIZE + REC_PHI + v];
-}
-
-__global__ void k_rec_grad_to_soa(int nnode, const double *__restrict__ rec, double *__restrict__ g) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nnode) return;
-#pragma unroll
-    for (int k = 0; k < 15; k++) g[k * (int64_t)nnode + i] = rec[(int64_t)i * REC_SIZE + REC_GRAD + k];
-}
-
-int roe_fix_standalone(cfd_ctx *c) {
-    if (!c->roe_fix_pending) return CFD_OK;
-    const int n = c->nnode;
-    CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)5 * n)));
-    k_rec_phi_to_soa<<<grid_for(n, 256), 256, 0, c->stream>>>(n, c->rec.p, c->work.p);
-    CFD_LAUNCH_CHECK();
-    k_roe_pressure_fix<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->Q.p, c->n2n_ia.p, c->n2n_ja.p, c->flow,
-                                                                  c->work.p, c->rec.p);
-    CFD_LAUNCH_CHECK();
-    c->roe_fix_pending = false;
-    return CFD_OK;
+    for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = neg ? 0.0 : phi_in[v * (int64_t)nnode + i];
 }
 
 }  // namespace cfd
@@ -328,20 +285,21 @@ int cfd_gradient(cfd_ctx *c) {
     if (!c || !c->has_mesh) { set_error("cfd_gradient: no mesh"); return CFD_ERR_STATE; }
     CFD_CUDA(cudaSetDevice(c->device));
     const int n = c->nnode;
+    CFD_CUDA(c->grad.alloc((size_t)15 * n));
     if (c->params.gradient == CFD_GRAD_GG) {
-        k_gg_grad<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->Q.p, c->n2e_ptr.p, c->n2e.p, c->edge_nodes.p,
-                                                             c->edge_sv.p, c->cvol.p, c->rec.p);
+        k_gg_grad<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->n2e_ptr.p, c->n2e.p, c->edge_nodes.p,
+                                                             c->edge_sv.p, c->cvol.p, c->grad.p);
     } else {
         // coefficients depend on the mesh and the weight only (FlagLSCoeff, Gradient.cpp:245-252)
         if (c->lsq_weight != c->params.ls_weight || c->ggw.n != (size_t)8 * n) {
             CFD_CUDA(c->ggw.alloc((size_t)8 * n));
-            k_lsq_coeff<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->n2n_ia.p, c->n2n_ja.p, c->rec.p,
+            k_lsq_coeff<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->n2n_ia.p, c->n2n_ja.p, c->xyz.p,
                                                                    c->params.ls_weight, c->ggw.p);
             CFD_LAUNCH_CHECK();
             c->lsq_weight = c->params.ls_weight;
         }
-        k_lsq_grad<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->Q.p, c->n2n_ia.p, c->n2n_ja.p, c->params.ls_weight,
-                                                              c->ggw.p, c->rec.p);
+        k_lsq_grad<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->n2n_ia.p, c->n2n_ja.p, c->xyz.p,
+                                                              c->params.ls_weight, c->ggw.p, c->grad.p);
     }
     CFD_LAUNCH_CHECK();
     c->has_grad = true;
@@ -353,10 +311,14 @@ int cfd_limiter(cfd_ctx *c) {
     if (!c->has_grad) { set_error("cfd_limiter: call cfd_gradient first"); return CFD_ERR_STATE; }
     CFD_CUDA(cudaSetDevice(c->device));
     const int n = c->nnode;
-    c->has_phi = true;
-    if (c->params.limiter == CFD_LIMITER_NONE) return CFD_OK;  // phi = 1 (Limiters.cpp:24-31) is implied
-    k_venkat<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->Q.p, c->n2n_ia.p, c->n2n_ja.p, c->cvol.p, c->flow, c->rec.p,
-                                                        c->roeflag.p);
+    CFD_CUDA(c->phi.alloc((size_t)5 * n));
+    if (c->params.limiter == CFD_LIMITER_NONE) {
+        // Compute_Limiter initialises phi = 1 (Limiters.cpp:24-31)
+        CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)5 * n)));
+        return CFD_OK;
+    }
+    k_venkat<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->n2n_ia.p, c->n2n_ja.p, c->xyz.p, c->grad.p,
+                                                        c->cvol.p, c->flow, c->phi.p, c->roeflag.p);
     CFD_LAUNCH_CHECK();
     if (c->params.flux_scheme == CFD_FLUX_ROE) {
         // The Roe-average pressure fix (Limiters.cpp:61-110) needs the
@@ -369,24 +331,36 @@ int cfd_limiter(cfd_ctx *c) {
     return CFD_OK;
 }
 
+}  // extern "C"
+
+namespace cfd {
+int roe_fix_standalone(cfd_ctx *c) {
+    if (!c->roe_fix_pending) return CFD_OK;
+    const int n = c->nnode;
+    CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)5 * n)));
+    CFD_CUDA(cudaMemcpyAsync(c->work.p, c->phi.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToDevice, c->stream));
+    k_roe_pressure_fix<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->n2n_ia.p, c->n2n_ja.p, c->xyz.p,
+                                                                  c->grad.p, c->flow, c->work.p, c->phi.p);
+    CFD_LAUNCH_CHECK();
+    c->roe_fix_pending = false;
+    return CFD_OK;
+}
+}  // namespace cfd
+
+extern "C" {
+
 int cfd_get_gradients(cfd_ctx *c, double *g) {
     if (!c || !g || !c->has_grad) return CFD_ERR_STATE;
-    CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)15 * c->nnode)));
-    k_rec_grad_to_soa<<<grid_for(c->nnode, 256), 256, 0, c->stream>>>(c->nnode, c->rec.p, c->work.p);
-    CFD_LAUNCH_CHECK();
-    CFD_CUDA(cudaMemcpyAsync(g, c->work.p, sizeof(double) * 15 * c->nnode, cudaMemcpyDeviceToHost, c->stream));
+    CFD_CUDA(cudaMemcpyAsync(g, c->grad.p, sizeof(double) * 15 * c->nnode, cudaMemcpyDeviceToHost, c->stream));
     CFD_CUDA(cudaStreamSynchronize(c->stream));
     return CFD_OK;
 }
 
 int cfd_get_limiters(cfd_ctx *c, double *phi) {
-    if (!c || !phi || !c->has_phi) return CFD_ERR_STATE;
+    if (!c || !phi || !c->phi.p) return CFD_ERR_STATE;
     int st = roe_fix_standalone(c);
     if (st) return st;
-    CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)5 * c->nnode)));
-    k_rec_phi_to_soa<<<grid_for(c->nnode, 256), 256, 0, c->stream>>>(c->nnode, c->rec.p, c->work.p);
-    CFD_LAUNCH_CHECK();
-    CFD_CUDA(cudaMemcpyAsync(phi, c->work.p, sizeof(double) * 5 * c->nnode, cudaMemcpyDeviceToHost, c->stream));
+    CFD_CUDA(cudaMemcpyAsync(phi, c->phi.p, sizeof(double) * 5 * c->nnode, cudaMemcpyDeviceToHost, c->stream));
     CFD_CUDA(cudaStreamSynchronize(c->stream));
     return CFD_OK;
 }
