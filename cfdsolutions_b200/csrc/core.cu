@@ -211,82 +211,125 @@ __device__ __forceinline__ double roe_avg_pressure(const double qa[5], const dou
 }
 
 // Flux residual, patch form: one CTA per patch of CFD_PATCH_NODES consecutive
-// nodes.  Phase 1 evaluates every edge of the patch once (edges cut by the
-// patch boundary are evaluated by both patches) into shared memory; phase 2
-// lets each owned node sum its incident edges from shared memory in its fixed
-// neighbour order (+ when it is node_L, - when it is node_R) and add its
-// boundary edges.  No atomics on the residual, deterministic summation order,
-// one flux evaluation per edge per patch instead of one per edge end.
+// nodes.  Phase 0 stages the node data of the patch and of its halo into
+// shared memory with coalesced loads (SoA, one row per variable).  The edges
+// of the patch (each interior edge touching the patch; edges cut by the patch
+// boundary are evaluated by both patches) are then processed in chunks of
+// PATCH_CHUNK: every thread evaluates one edge flux from shared memory into a
+// chunk buffer, and each owned node adds the contributions of the chunk in
+// increasing local edge order (+ when it is node_L, - when it is node_R).  No
+// atomics on the residual, deterministic summation order, one flux evaluation
+// per edge per patch instead of one per edge end, and the L1 cache stays free
+// for the few global loads left (ghost states of boundary edges).
 // `gate`: when non-null and *gate == 0 the launch does nothing (conditional
 // re-evaluation after the limiter's pressure fix).
 template <int FLUX, bool SECOND>
-__global__ void __launch_bounds__(256) k_residual_patch(
-    int nnode, int64_t ldq, const double *__restrict__ Q, const int *__restrict__ pe_ptr,
-    const int2 *__restrict__ pe_nodes, const double4 *__restrict__ pe_geo, const int *__restrict__ inc_ptr,
-    const int *__restrict__ inc, const int *__restrict__ n2b_ptr, const int *__restrict__ n2b,
-    const int2 *__restrict__ bn, const double4 *__restrict__ bg, const double *__restrict__ xyz,
-    const double *__restrict__ grad, const double *__restrict__ phi, Flow f, int add_time, int emax,
-    int check_roe, int *__restrict__ roeflag, int *__restrict__ roecount, const int *__restrict__ gate,
-    double *__restrict__ res, double *__restrict__ resd, double *__restrict__ dtsum,
-    unsigned long long *__restrict__ ext) {
+__global__ void __launch_bounds__(PATCH_CHUNK, 2) k_residual_patch(
+    int nnode, int64_t ldq, const double *__restrict__ Q, const double *__restrict__ grad,
+    const double *__restrict__ phi, const double *__restrict__ xyz, const int *__restrict__ pe_ptr,
+    const int *__restrict__ pe_loc, const double4 *__restrict__ pe_geo, const int *__restrict__ ph_ptr,
+    const int *__restrict__ halo, const int *__restrict__ inc_ptr, const int *__restrict__ inc,
+    const int *__restrict__ n2b_ptr, const int *__restrict__ n2b, const int2 *__restrict__ bn,
+    const double4 *__restrict__ bg, Flow f, int add_time, int nlm, int check_roe, int *__restrict__ roeflag,
+    int *__restrict__ roecount, const int *__restrict__ gate, double *__restrict__ res, double *__restrict__ resd,
+    double *__restrict__ dtsum, unsigned long long *__restrict__ ext) {
     if (gate && *gate == 0) return;
-    extern __shared__ double eb[];  // [11][emax]
-    const int p = blockIdx.x;
-    const int e0 = pe_ptr[p], ne = pe_ptr[p + 1] - e0;
-    const bool limited = f.limiter != CFD_LIMITER_NONE;
-    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
-    for (int k = threadIdx.x; k < ne; k += blockDim.x) {
-        const int2 nd = pe_nodes[e0 + k];
-        const double4 g = pe_geo[e0 + k];
-        double qL[5], qR[5];
-#pragma unroll
-        for (int v = 0; v < 5; v++) {
-            qL[v] = Q[v * ldq + nd.x];
-            qR[v] = Q[v * ldq + nd.y];
-        }
-        if (SECOND) {
-            const double rx = 0.5 * (xyz[nd.y] - xyz[nd.x]);
-            const double ry = 0.5 * (xyz[nnode + nd.y] - xyz[nnode + nd.x]);
-            const double rz = 0.5 * (xyz[2 * nnode + nd.y] - xyz[2 * nnode + nd.x]);
-            double rL[5], rR[5];
-            reconstruct(qL, qR, nd.x, rx, ry, rz, grad, phi, nnode, limited, f.frac, rL);
-            reconstruct(qR, qL, nd.y, -rx, -ry, -rz, grad, phi, nnode, limited, f.frac, rR);
-#pragma unroll
-            for (int v = 0; v < 5; v++) { qL[v] = rL[v]; qR[v] = rR[v]; }
-            if (check_roe && roe_avg_pressure(qL, qR, f.gamma) < 0.0) {
-                roeflag[nd.x] = 1;
-                roeflag[nd.y] = 1;
-                atomicAdd(roecount, 1);
-            }
-        }
-        double cf[5], df[5], lam[3];
-        const double lmax = edge_flux<FLUX>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam);
-#pragma unroll
-        for (int v = 0; v < 5; v++) {
-            eb[v * emax + k] = cf[v];
-            eb[(5 + v) * emax + k] = df[v];
-        }
-        eb[10 * emax + k] = g.w * lmax;
-#pragma unroll
-        for (int j = 0; j < 3; j++) { mn[j] = fmin(mn[j], lam[j]); mx[j] = fmax(mx[j], lam[j]); }
-    }
-    __syncthreads();
+    constexpr int NV = SECOND ? PATCH_NV2 : 5;
+    extern __shared__ double sm[];
+    double *nv = sm;                       // [NV][nlm]: Q 0-4 | grad 5-19 | phi 20-24 | xyz 25-27
+    double *cb = sm + (size_t)NV * nlm;    // [11][PATCH_CHUNK]
+    const int p = blockIdx.x, tid = threadIdx.x;
     const int n0 = p * CFD_PATCH_NODES;
     const int nown = min(CFD_PATCH_NODES, nnode - n0);
-    for (int j = threadIdx.x; j < nown; j += blockDim.x) {
-        const int i = n0 + j;
-        double ac[5] = {0, 0, 0, 0, 0}, ad[5] = {0, 0, 0, 0, 0}, adt = 0.0;
-        for (int q = inc_ptr[i]; q < inc_ptr[i + 1]; q++) {
+    const int h0 = ph_ptr[p], nloc = nown + ph_ptr[p + 1] - h0;
+    const bool limited = f.limiter != CFD_LIMITER_NONE;
+    // phase 0: stage owned + halo node data
+    for (int l = tid; l < nloc; l += PATCH_CHUNK) {
+        const int g = l < nown ? n0 + l : halo[h0 + l - nown];
+#pragma unroll
+        for (int v = 0; v < 5; v++) nv[v * nlm + l] = Q[v * ldq + g];
+        if (SECOND) {
+#pragma unroll
+            for (int k = 0; k < 15; k++) nv[(5 + k) * nlm + l] = grad[k * (int64_t)nnode + g];
+#pragma unroll
+            for (int v = 0; v < 5; v++) nv[(20 + v) * nlm + l] = limited ? phi[v * (int64_t)nnode + g] : 1.0;
+#pragma unroll
+            for (int d = 0; d < 3; d++) nv[(25 + d) * nlm + l] = xyz[d * (int64_t)nnode + g];
+        }
+    }
+    __syncthreads();
+    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
+    double ac[5] = {0, 0, 0, 0, 0}, ad[5] = {0, 0, 0, 0, 0}, adt = 0.0;
+    int q = 0, qe = 0;
+    if (tid < nown) {
+        q = inc_ptr[n0 + tid];
+        qe = inc_ptr[n0 + tid + 1];
+    }
+    const int e0 = pe_ptr[p], ne = pe_ptr[p + 1] - e0;
+    for (int c0 = 0; c0 < ne; c0 += PATCH_CHUNK) {
+        const int k = c0 + tid;
+        if (k < ne) {
+            const int lp = pe_loc[e0 + k];
+            const int a = lp & 0xffff, b = lp >> 16;
+            const double4 g = pe_geo[e0 + k];
+            double qL[5], qR[5];
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                qL[v] = nv[v * nlm + a];
+                qR[v] = nv[v * nlm + b];
+            }
+            if (SECOND) {
+                const double rx = 0.5 * (nv[25 * nlm + b] - nv[25 * nlm + a]);
+                const double ry = 0.5 * (nv[26 * nlm + b] - nv[26 * nlm + a]);
+                const double rz = 0.5 * (nv[27 * nlm + b] - nv[27 * nlm + a]);
+                double rL[5], rR[5];
+#pragma unroll
+                for (int v = 0; v < 5; v++) {
+                    const double gL = nv[(5 + 3 * v) * nlm + a] * rx + nv[(6 + 3 * v) * nlm + a] * ry +
+                                      nv[(7 + 3 * v) * nlm + a] * rz;
+                    const double gR = -(nv[(5 + 3 * v) * nlm + b] * rx + nv[(6 + 3 * v) * nlm + b] * ry +
+                                        nv[(7 + 3 * v) * nlm + b] * rz);
+                    rL[v] = qL[v] + nv[(20 + v) * nlm + a] * (f.frac * (qR[v] - qL[v]) + (1.0 - f.frac) * gL);
+                    rR[v] = qR[v] + nv[(20 + v) * nlm + b] * (f.frac * (qL[v] - qR[v]) + (1.0 - f.frac) * gR);
+                }
+#pragma unroll
+                for (int v = 0; v < 5; v++) { qL[v] = rL[v]; qR[v] = rR[v]; }
+                if (check_roe && roe_avg_pressure(qL, qR, f.gamma) < 0.0) {
+                    roeflag[a < nown ? n0 + a : halo[h0 + a - nown]] = 1;
+                    roeflag[b < nown ? n0 + b : halo[h0 + b - nown]] = 1;
+                    atomicAdd(roecount, 1);
+                }
+            }
+            double cf[5], df[5], lam[3];
+            const double lmax = edge_flux<FLUX>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam);
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                cb[v * PATCH_CHUNK + tid] = cf[v];
+                cb[(5 + v) * PATCH_CHUNK + tid] = df[v];
+            }
+            cb[10 * PATCH_CHUNK + tid] = g.w * lmax;
+#pragma unroll
+            for (int j = 0; j < 3; j++) { mn[j] = fmin(mn[j], lam[j]); mx[j] = fmax(mx[j], lam[j]); }
+        }
+        __syncthreads();
+        const int cend = c0 + PATCH_CHUNK;
+        for (; q < qe; q++) {
             const int t = inc[q];
-            const int k = t >> 1;
+            const int kk = (t >> 1);
+            if (kk >= cend) break;
+            const int s = kk - c0;
             const double sg = (t & 1) ? -1.0 : 1.0;
 #pragma unroll
             for (int v = 0; v < 5; v++) {
-                ac[v] += sg * eb[v * emax + k];
-                ad[v] += sg * eb[(5 + v) * emax + k];
+                ac[v] += sg * cb[v * PATCH_CHUNK + s];
+                ad[v] += sg * cb[(5 + v) * PATCH_CHUNK + s];
             }
-            adt += eb[10 * emax + k];
+            adt += cb[10 * PATCH_CHUNK + s];
         }
+        __syncthreads();
+    }
+    if (tid < nown) {
+        const int i = n0 + tid;
         for (int k = n2b_ptr[i]; k < n2b_ptr[i + 1]; k++) {
             const int b = n2b[k];
             const int2 nd = bn[b];
@@ -294,7 +337,7 @@ __global__ void __launch_bounds__(256) k_residual_patch(
             double qL[5], qR[5];
 #pragma unroll
             for (int v = 0; v < 5; v++) {
-                qL[v] = Q[v * ldq + nd.x];
+                qL[v] = nv[v * nlm + tid];
                 qR[v] = Q[v * ldq + nd.y];
             }
             double cf[5], df[5], lam[3];
@@ -690,15 +733,15 @@ static bool patch_kernel(const cfd_ctx *c) { return c->use_patch && c->params.re
 template <int FLUX, bool SECOND>
 static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, const int *gate) {
     if (patch_kernel(c)) {
-        const size_t smem = (size_t)c->patch_emax * 11 * sizeof(double);
+        const size_t smem = patch_smem_bytes(c->patch_nlocmax, SECOND);
         if (smem > 48 * 1024)
             CFD_CUDA(cudaFuncSetAttribute(k_residual_patch<FLUX, SECOND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)kPatchSmemMax));
-        k_residual_patch<FLUX, SECOND><<<c->npatch, 256, smem, c->stream>>>(
-            c->nnode, c->ldq, c->Q.p, c->pe_ptr.p, c->pe_nodes.p, c->pe_geo.p, c->inc_ptr.p, c->inc.p, c->n2b_ptr.p,
-            c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p, c->xyz.p, c->grad.p, c->phi.p, c->flow, add_time,
-            c->patch_emax, check_roe ? 1 : 0, c->roeflag.p, c->roecount.p, gate, c->res.p, c->resd.p, c->dt.p,
-            c->ext.p);
+                                          (int)smem));
+        k_residual_patch<FLUX, SECOND><<<c->npatch, PATCH_CHUNK, smem, c->stream>>>(
+            c->nnode, c->ldq, c->Q.p, c->grad.p, c->phi.p, c->xyz.p, c->pe_ptr.p, c->pe_loc.p, c->pe_geo.p,
+            c->ph_ptr.p, c->halo.p, c->inc_ptr.p, c->inc.p, c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p,
+            c->flow, add_time, c->patch_nlocmax, check_roe ? 1 : 0, c->roeflag.p, c->roecount.p, gate, c->res.p,
+            c->resd.p, c->dt.p, c->ext.p);
     } else {
         if (gate || check_roe) return CFD_ERR_UNSUPPORTED;
         k_residual_gather<FLUX, SECOND><<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(
@@ -985,47 +1028,72 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         CFD_CUDA(c->n2e.upload(lst.data(), lst.size(), s));
         CFD_CUDA(cudaStreamSynchronize(s));
     }
-    // ---- patch layout of the residual kernel: node ranges of CFD_PATCH_NODES,
-    // every interior edge touching a patch copied into the patch's edge list
-    // (edges cut by the patch boundary appear in both patches), and per node
-    // its incident edges as patch-local indices in the fixed neighbour order.
+    // ---- patch layout of the residual kernel: node ranges of CFD_PATCH_NODES
+    // nodes; per patch its halo (neighbours outside the range, sorted), every
+    // interior edge touching the patch with patch-local endpoint indices
+    // (owned 0..np-1, halo np..), and per owned node its incident edges as
+    // patch-local edge indices in increasing order (the fixed summation order).
     {
         const int P = CFD_PATCH_NODES;
         const int np = (nnode + P - 1) / P;
-        std::vector<int> pptr(np + 1, 0), stamp(nedge, -1), local(nedge, 0), iptr(nnode + 1, 0), ilist;
-        std::vector<int2> pn;
+        std::vector<int> pptr(np + 1, 0), hptr(np + 1, 0), halo, stamp(nedge, -1), local(nedge, 0);
+        std::vector<int> iptr(nnode + 1, 0), ilist, pl;
         std::vector<double4> pg;
+        std::vector<int> hstamp(nnode, -1), hloc(nnode, 0);
         ilist.reserve(ptr[nnode]);
-        pn.reserve((size_t)nedge + nedge / 2);
+        pl.reserve((size_t)nedge + nedge / 2);
         pg.reserve((size_t)nedge + nedge / 2);
-        int emax = 0;
+        int nlocmax = 0;
         for (int p = 0; p < np; p++) {
+            const int n0 = p * P, n1 = std::min(nnode, n0 + P), nown = n1 - n0;
+            // halo, sorted by global index
+            std::vector<int> h;
+            for (int i = n0; i < n1; i++)
+                for (int k = ptr[i]; k < ptr[i + 1]; k++) {
+                    const int sg = lst[k], e = sg >= 0 ? sg : ~sg;
+                    const int j = sg >= 0 ? en[e].y : en[e].x;
+                    if ((j < n0 || j >= n1) && hstamp[j] != p) { hstamp[j] = p; h.push_back(j); }
+                }
+            std::sort(h.begin(), h.end());
+            for (size_t q = 0; q < h.size(); q++) hloc[h[q]] = nown + (int)q;
+            halo.insert(halo.end(), h.begin(), h.end());
+            hptr[p + 1] = (int)halo.size();
+            nlocmax = std::max(nlocmax, nown + (int)h.size());
+            auto lid = [&](int g) { return (g >= n0 && g < n1) ? g - n0 : hloc[g]; };
             int cnt = 0;
-            const int n0 = p * P, n1 = std::min(nnode, n0 + P);
-            for (int i = n0; i < n1; i++) {
+            for (int i = n0; i < n1; i++)
                 for (int k = ptr[i]; k < ptr[i + 1]; k++) {
                     const int sg = lst[k], e = sg >= 0 ? sg : ~sg;
                     if (stamp[e] != p) {
                         stamp[e] = p;
                         local[e] = cnt++;
-                        pn.push_back(en[e]);
+                        pl.push_back(lid(en[e].x) | (lid(en[e].y) << 16));
                         pg.push_back(eg[e]);
                     }
+                }
+            for (int i = n0; i < n1; i++) {
+                const size_t b = ilist.size();
+                for (int k = ptr[i]; k < ptr[i + 1]; k++) {
+                    const int sg = lst[k], e = sg >= 0 ? sg : ~sg;
                     ilist.push_back((local[e] << 1) | (sg < 0 ? 1 : 0));
                 }
+                std::sort(ilist.begin() + b, ilist.end());
                 iptr[i + 1] = (int)ilist.size();
             }
             pptr[p + 1] = pptr[p] + cnt;
-            emax = std::max(emax, cnt);
         }
-        if (ilist.empty()) ilist.push_back(0);  // keep the device array non-empty
+        if (ilist.empty()) ilist.push_back(0);  // keep the device arrays non-empty
+        if (halo.empty()) halo.push_back(0);
+        if (pl.empty()) { pl.push_back(0); pg.push_back(make_double4(0, 0, 0, 0)); }
         c->npatch = np;
-        c->patch_emax = emax;
-        c->use_patch = (size_t)emax * 11 * sizeof(double) <= kPatchSmemMax;
+        c->patch_nlocmax = nlocmax;
+        c->use_patch = nlocmax < 65536 && patch_smem_bytes(nlocmax, true) <= kPatchSmemMax;
         if (c->use_patch) {
             CFD_CUDA(c->pe_ptr.upload(pptr.data(), pptr.size(), s));
-            CFD_CUDA(c->pe_nodes.upload(pn.data(), pn.size(), s));
+            CFD_CUDA(c->pe_loc.upload(pl.data(), pl.size(), s));
             CFD_CUDA(c->pe_geo.upload(pg.data(), pg.size(), s));
+            CFD_CUDA(c->ph_ptr.upload(hptr.data(), hptr.size(), s));
+            CFD_CUDA(c->halo.upload(halo.data(), halo.size(), s));
             CFD_CUDA(c->inc_ptr.upload(iptr.data(), iptr.size(), s));
             CFD_CUDA(c->inc.upload(ilist.data(), ilist.size(), s));
             CFD_CUDA(cudaStreamSynchronize(s));

@@ -85,10 +85,11 @@ struct cfd_ctx {
     // patch layout of the residual kernel: patches are contiguous ranges of
     // CFD_PATCH_NODES nodes; each patch lists every interior edge touching it
     cfd::DevBuf<int> pe_ptr;          // [npatch+1]
-    cfd::DevBuf<int2> pe_nodes;       // [sum] edge (L, R) copies
+    cfd::DevBuf<int> pe_loc;          // [sum] patch-local (L | R << 16)
     cfd::DevBuf<double4> pe_geo;      // [sum] unit normal + |S|
-    cfd::DevBuf<int> inc_ptr, inc;    // per node: (patch-local edge << 1) | (node is R)
-    int npatch = 0, patch_emax = 0;
+    cfd::DevBuf<int> ph_ptr, halo;    // per patch: halo node list (global ids, sorted)
+    cfd::DevBuf<int> inc_ptr, inc;    // per node: (patch-local edge << 1) | (node is R), increasing
+    int npatch = 0, patch_nlocmax = 0;
     bool use_patch = false;
     // Roe-average pressure positivity fix of the limiter (see cfd_limiter)
     cfd::DevBuf<int> roeflag;         // [nnode]

@@ -155,10 +155,17 @@ __device__ __forceinline__ double load_low(const uint16_t *p) {
 // Deterministic sum of a plain vector (host result).
 int reduce_sum_plain(cfd_ctx *c, const double *x, int64_t n, double *out_host);
 
-// Largest dynamic shared memory the patch residual kernel may use: 11 doubles
-// per patch edge; 128-node patches of a tet mesh list ~1300 edges (~112 KB, two
-// CTAs per SM); larger lists still run, one CTA per SM, up to this cap.
-constexpr size_t kPatchSmemMax = 200 * 1024;
+// Patch residual kernel: threads per CTA (= edges per chunk), node variables
+// staged per patch node for second order (Q 5, gradients 15, limiters 5,
+// coordinates 3), and the dynamic shared memory it needs.  128-node patches of
+// a tet mesh have ~350 patch + halo nodes (~78 KB + 22 KB chunk buffer, two
+// CTAs per SM); larger halos still run, one CTA per SM, up to kPatchSmemMax.
+constexpr int PATCH_CHUNK = 256;
+constexpr int PATCH_NV2 = 28;
+constexpr size_t kPatchSmemMax = 220 * 1024;
+inline size_t patch_smem_bytes(int nlocmax, bool second) {
+    return ((size_t)(second ? PATCH_NV2 : 5) * nlocmax + 11 * PATCH_CHUNK) * sizeof(double);
+}
 
 // The limiter's Roe-average pressure fix as its own pass over the node graph
 // (gradient.cu); used when the fused check in the residual cannot run.
