@@ -108,48 +108,80 @@ __device__ __forceinline__ void reconstruct(const double qs[5], const double qo[
 }
 
 // Flux residual, node-gather form: one thread per node walks its incident
-// edges in a fixed order and accumulates +flux (node is node_L) or -flux
-// (node is node_R), so every node's sum has a deterministic order and no
-// atomics touch the residual.  The flux of edge (L,R) is always evaluated in
+// interior edges in a fixed order (neighbour id) and accumulates +flux (the node
+// is node_L) or -flux (node_R); no atomics touch the residual, so every node's
+// sum has a deterministic order.  The flux of edge (L,R) is always evaluated in
 // the reference's orientation (Q_L, Q_R, n_{L->R}), so both endpoints see
 // bit-identical values (Compute_Residual_Roe_New, FluxTest.cpp:7968-8100).
+// Incidence is stored sliced-ELL (slices of 32 nodes, slot k of a slice's
+// lanes contiguous): neighbour id (~id when the node is node_R) and the edge's
+// unit normal + area per slot, so the per-edge loads of a warp are coalesced;
+// the node's own state, gradients, limiters and coordinates stay in registers.
 template <int FLUX, bool SECOND>
-__global__ void __launch_bounds__(128) k_residual_gather(
-    int nnode, int64_t ldq, const double *__restrict__ Q, const int *__restrict__ n2e_ptr,
-    const int *__restrict__ n2e, const int2 *__restrict__ en, const double4 *__restrict__ eg,
+__global__ void __launch_bounds__(128, 3) k_residual_gather(
+    int nnode, int64_t ldq, const double *__restrict__ Q, const double *__restrict__ grad,
+    const double *__restrict__ phi, const double *__restrict__ xyz, const int64_t *__restrict__ sell_ptr,
+    const int *__restrict__ sell_nbr, const double4 *__restrict__ sell_geo, const int *__restrict__ deg,
     const int *__restrict__ n2b_ptr, const int *__restrict__ n2b, const int2 *__restrict__ bn,
-    const double4 *__restrict__ bg, const double *__restrict__ xyz, const double *__restrict__ grad,
-    const double *__restrict__ phi, Flow f, int add_time, double *__restrict__ res,
-    double *__restrict__ resd, double *__restrict__ dtsum, unsigned long long *__restrict__ ext) {
+    const double4 *__restrict__ bg, Flow f, int add_time, int check_roe, int *__restrict__ roeflag,
+    int *__restrict__ roecount, const int *__restrict__ gate, double *__restrict__ res, double *__restrict__ resd,
+    double *__restrict__ dtsum, unsigned long long *__restrict__ ext) {
+    if (gate && *gate == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
     if (i < nnode) {
-        double ac[5] = {0, 0, 0, 0, 0}, ad[5] = {0, 0, 0, 0, 0}, adt = 0.0;
         const bool limited = f.limiter != CFD_LIMITER_NONE;
-        for (int k = n2e_ptr[i]; k < n2e_ptr[i + 1]; k++) {
-            const int s = n2e[k];
-            const int e = s >= 0 ? s : ~s;
-            const int2 nd = en[e];
-            const double4 g = eg[e];
+        double qo[5], go[15], po[5], xo[3];
+#pragma unroll
+        for (int v = 0; v < 5; v++) qo[v] = Q[v * ldq + i];
+        if (SECOND) {
+#pragma unroll
+            for (int k = 0; k < 15; k++) go[k] = grad[k * (int64_t)nnode + i];
+#pragma unroll
+            for (int v = 0; v < 5; v++) po[v] = limited ? phi[v * (int64_t)nnode + i] : 1.0;
+#pragma unroll
+            for (int d = 0; d < 3; d++) xo[d] = xyz[d * (int64_t)nnode + i];
+        }
+        double ac[5] = {0, 0, 0, 0, 0}, ad[5] = {0, 0, 0, 0, 0}, adt = 0.0;
+        bool roe_bad = false;
+        const int64_t base = sell_ptr[i >> 5] + (i & 31);
+        const int d = deg[i];
+        for (int k = 0; k < d; k++) {
+            const int sn = sell_nbr[base + 32 * k];
+            const double4 g = sell_geo[base + 32 * k];
+            const bool own_is_L = sn >= 0;
+            const int j = own_is_L ? sn : ~sn;
+            double qn[5], fo[5], fn[5];
+#pragma unroll
+            for (int v = 0; v < 5; v++) qn[v] = Q[v * ldq + j];
+            if (SECOND) {
+                const double rx = 0.5 * (xyz[j] - xo[0]);
+                const double ry = 0.5 * (xyz[nnode + j] - xo[1]);
+                const double rz = 0.5 * (xyz[2 * (int64_t)nnode + j] - xo[2]);
+#pragma unroll
+                for (int v = 0; v < 5; v++) {
+                    const double gno = go[3 * v] * rx + go[3 * v + 1] * ry + go[3 * v + 2] * rz;
+                    const double gnn = -(grad[(3 * v) * (int64_t)nnode + j] * rx +
+                                         grad[(3 * v + 1) * (int64_t)nnode + j] * ry +
+                                         grad[(3 * v + 2) * (int64_t)nnode + j] * rz);
+                    const double pn = limited ? phi[v * (int64_t)nnode + j] : 1.0;
+                    fo[v] = qo[v] + po[v] * (f.frac * (qn[v] - qo[v]) + (1.0 - f.frac) * gno);
+                    fn[v] = qn[v] + pn * (f.frac * (qo[v] - qn[v]) + (1.0 - f.frac) * gnn);
+                }
+            } else {
+#pragma unroll
+                for (int v = 0; v < 5; v++) { fo[v] = qo[v]; fn[v] = qn[v]; }
+            }
             double qL[5], qR[5];
 #pragma unroll
             for (int v = 0; v < 5; v++) {
-                qL[v] = Q[v * ldq + nd.x];
-                qR[v] = Q[v * ldq + nd.y];
+                qL[v] = own_is_L ? fo[v] : fn[v];
+                qR[v] = own_is_L ? fn[v] : fo[v];
             }
-            if (SECOND) {
-                const double rx = 0.5 * (xyz[nd.y] - xyz[nd.x]);
-                const double ry = 0.5 * (xyz[nnode + nd.y] - xyz[nnode + nd.x]);
-                const double rz = 0.5 * (xyz[2 * nnode + nd.y] - xyz[2 * nnode + nd.x]);
-                double rL[5], rR[5];
-                reconstruct(qL, qR, nd.x, rx, ry, rz, grad, phi, nnode, limited, f.frac, rL);
-                reconstruct(qR, qL, nd.y, -rx, -ry, -rz, grad, phi, nnode, limited, f.frac, rR);
-#pragma unroll
-                for (int v = 0; v < 5; v++) { qL[v] = rL[v]; qR[v] = rR[v]; }
-            }
+            if (SECOND && check_roe && roe_avg_pressure(qL, qR, f.gamma) < 0.0) roe_bad = true;
             double cf[5], df[5], lam[3];
             const double lmax = edge_flux<FLUX>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam);
-            const double sg = s >= 0 ? 1.0 : -1.0;
+            const double sg = own_is_L ? 1.0 : -1.0;
 #pragma unroll
             for (int v = 0; v < 5; v++) {
                 ac[v] += sg * cf[v];
@@ -157,21 +189,22 @@ __global__ void __launch_bounds__(128) k_residual_gather(
             }
             adt += g.w * lmax;
 #pragma unroll
-            for (int j = 0; j < 3; j++) { mn[j] = fmin(mn[j], lam[j]); mx[j] = fmax(mx[j], lam[j]); }
+            for (int m = 0; m < 3; m++) { mn[m] = fmin(mn[m], lam[m]); mx[m] = fmax(mx[m], lam[m]); }
+        }
+        if (roe_bad) {
+            roeflag[i] = 1;
+            atomicAdd(roecount, 1);
         }
         // boundary edges: first order, flux into node_L only (FluxTest.cpp:8044-8098)
         for (int k = n2b_ptr[i]; k < n2b_ptr[i + 1]; k++) {
             const int b = n2b[k];
             const int2 nd = bn[b];
             const double4 g = bg[b];
-            double qL[5], qR[5];
+            double qR[5];
 #pragma unroll
-            for (int v = 0; v < 5; v++) {
-                qL[v] = Q[v * ldq + nd.x];
-                qR[v] = Q[v * ldq + nd.y];
-            }
+            for (int v = 0; v < 5; v++) qR[v] = Q[v * ldq + nd.y];
             double cf[5], df[5], lam[3];
-            const double lmax = edge_flux<FLUX>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam);
+            const double lmax = edge_flux<FLUX>(qo, qR, g.x, g.y, g.z, g.w, f, cf, df, lam);
 #pragma unroll
             for (int v = 0; v < 5; v++) {
                 ac[v] += cf[v];
@@ -179,7 +212,7 @@ __global__ void __launch_bounds__(128) k_residual_gather(
             }
             adt += g.w * lmax;
 #pragma unroll
-            for (int j = 0; j < 3; j++) { mn[j] = fmin(mn[j], lam[j]); mx[j] = fmax(mx[j], lam[j]); }
+            for (int m = 0; m < 3; m++) { mn[m] = fmin(mn[m], lam[m]); mx[m] = fmax(mx[m], lam[m]); }
         }
 #pragma unroll
         for (int v = 0; v < 5; v++) {
@@ -189,25 +222,6 @@ __global__ void __launch_bounds__(128) k_residual_gather(
         if (add_time) dtsum[i] = adt;
     }
     if (add_time) block_extrema3(mn, mx, ext);
-}
-
-// Pressure of the Roe-averaged state of two reconstructed face states
-// (Compute_RoeVariables, Roe_Fluxes.cpp:3609-3633, tested in
-// Compute_Limiter_RoePressureCorrection, Limiters.cpp:311-356).
-__device__ __forceinline__ double roe_avg_pressure(const double qa[5], const double qb[5], double g) {
-    const double ra = qa[0], rb = qb[0];
-    const double ia = 1.0 / ra, ib = 1.0 / rb;
-    const double ua = qa[1] * ia, va = qa[2] * ia, wa = qa[3] * ia;
-    const double ub = qb[1] * ib, vb = qb[2] * ib, wb = qb[3] * ib;
-    const double pa = (g - 1.0) * (qa[4] - 0.5 * ra * (ua * ua + va * va + wa * wa));
-    const double pb = (g - 1.0) * (qb[4] - 0.5 * rb * (ub * ub + vb * vb + wb * wb));
-    const double ha = (qa[4] + pa) * ia, hb = (qb[4] + pb) * ib;
-    const double rho = sqrt(ra * rb), sg = rho / (ra + rho);
-    const double u = ua + sg * (ub - ua), v = va + sg * (vb - va), w = wa + sg * (wb - wa);
-    const double ht = ha + sg * (hb - ha);
-    const double q2 = u * u + v * v + w * w;
-    const double e = (rho / g) * (ht + 0.5 * (g - 1.0) * q2);
-    return (g - 1.0) * (e - 0.5 * rho * q2);
 }
 
 // Flux residual, patch form: one CTA per patch of CFD_PATCH_NODES consecutive
@@ -728,7 +742,7 @@ static void compute_flow(cfd_ctx *c, int iteration) {
         c->cfl = p.cfl_max;
 }
 
-static bool patch_kernel(const cfd_ctx *c) { return c->use_patch && c->params.residual_kernel == 0; }
+static bool patch_kernel(const cfd_ctx *c) { return c->use_patch && c->params.residual_kernel == 1; }
 
 template <int FLUX, bool SECOND>
 static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, const int *gate) {
@@ -743,11 +757,10 @@ static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, const int *
             c->flow, add_time, c->patch_nlocmax, check_roe ? 1 : 0, c->roeflag.p, c->roecount.p, gate, c->res.p,
             c->resd.p, c->dt.p, c->ext.p);
     } else {
-        if (gate || check_roe) return CFD_ERR_UNSUPPORTED;
         k_residual_gather<FLUX, SECOND><<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(
-            c->nnode, c->ldq, c->Q.p, c->n2e_ptr.p, c->n2e.p, c->edge_nodes.p, c->edge_geo.p, c->n2b_ptr.p,
-            c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p, c->xyz.p, c->grad.p, c->phi.p, c->flow, add_time, c->res.p,
-            c->resd.p, c->dt.p, c->ext.p);
+            c->nnode, c->ldq, c->Q.p, c->grad.p, c->phi.p, c->xyz.p, c->sell_ptr.p, c->sell_nbr.p, c->sell_geo.p,
+            c->deg.p, c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p, c->flow, add_time,
+            check_roe ? 1 : 0, c->roeflag.p, c->roecount.p, gate, c->res.p, c->resd.p, c->dt.p, c->ext.p);
     }
     CFD_LAUNCH_CHECK();
     return CFD_OK;
@@ -758,7 +771,7 @@ static int residual_with_fix(cfd_ctx *c, int add_time) {
     // Roe flux + limiter: the limiter's Roe-average pressure fix is decided by
     // the residual's own reconstruction (same states) and applied, followed by
     // a gated re-evaluation, only when some edge failed the check.
-    const bool fused = SECOND && FLUX == CFD_FLUX_ROE && c->roe_fix_pending && patch_kernel(c);
+    const bool fused = SECOND && FLUX == CFD_FLUX_ROE && c->roe_fix_pending;
     int st = launch_residual<FLUX, SECOND>(c, add_time, fused, nullptr);
     if (st || !fused) return st;
     k_roe_fix_apply<<<grid_for(c->nnode, 256), 256, 0, c->stream>>>(c->nnode, c->roecount.p, c->roeflag.p, c->phi.p);
@@ -1028,6 +1041,34 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         CFD_CUDA(c->n2e.upload(lst.data(), lst.size(), s));
         CFD_CUDA(cudaStreamSynchronize(s));
     }
+    // ---- sliced-ELL incidence of the node-gather kernel (slices of 32 nodes)
+    {
+        const int nsl = (nnode + 31) / 32;
+        std::vector<int64_t> sp(nsl + 1, 0);
+        std::vector<int> dg(nnode);
+        for (int i = 0; i < nnode; i++) dg[i] = ptr[i + 1] - ptr[i];
+        for (int sl = 0; sl < nsl; sl++) {
+            int w = 0;
+            for (int i = sl * 32; i < std::min(nnode, sl * 32 + 32); i++) w = std::max(w, dg[i]);
+            sp[sl + 1] = sp[sl] + 32 * (int64_t)w;
+        }
+        std::vector<int> sn(std::max<int64_t>(sp[nsl], 1), 0);
+        std::vector<double4> sg(std::max<int64_t>(sp[nsl], 1), make_double4(0, 0, 0, 0));
+        for (int i = 0; i < nnode; i++) {
+            const int64_t b = sp[i >> 5] + (i & 31);
+            for (int k = ptr[i]; k < ptr[i + 1]; k++) {
+                const int t = lst[k], e = t >= 0 ? t : ~t;
+                const int64_t slot = b + 32 * (int64_t)(k - ptr[i]);
+                sn[slot] = t >= 0 ? en[e].y : ~en[e].x;
+                sg[slot] = eg[e];
+            }
+        }
+        CFD_CUDA(c->sell_ptr.upload(sp.data(), sp.size(), s));
+        CFD_CUDA(c->sell_nbr.upload(sn.data(), sn.size(), s));
+        CFD_CUDA(c->sell_geo.upload(sg.data(), sg.size(), s));
+        CFD_CUDA(c->deg.upload(dg.data(), dg.size(), s));
+        CFD_CUDA(cudaStreamSynchronize(s));
+    }
     // ---- patch layout of the residual kernel: node ranges of CFD_PATCH_NODES
     // nodes; per patch its halo (neighbours outside the range, sorted), every
     // interior edge touching the patch with patch-local endpoint indices
@@ -1245,10 +1286,6 @@ int cfd_residual(cfd_ctx *c, int add_time) {
     if (second && c->params.limiter != CFD_LIMITER_NONE && !c->phi.p) {
         set_error("cfd_residual: limiter requested but cfd_limiter not called");
         return CFD_ERR_STATE;
-    }
-    if (second && c->params.limiter != CFD_LIMITER_NONE && c->roe_fix_pending && !patch_kernel(c)) {
-        int st = roe_fix_standalone(c);
-        if (st) return st;
     }
     switch (c->params.flux_scheme * 2 + (second ? 1 : 0)) {
         case 0: return residual_with_fix<CFD_FLUX_ROE, false>(c, add_time);

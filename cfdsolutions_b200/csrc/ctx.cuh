@@ -82,6 +82,11 @@ struct cfd_ctx {
     cfd::DevBuf<int> IA, JA, IAU, tslot;  // tslot[k] = slot of (JA[k], row)
     cfd::DevBuf<int2> eslot;              // per edge: slot(L,R), slot(R,L)
     cfd::Levels lv_fwd, lv_bwd;
+    // sliced-ELL incidence of the node-gather residual kernel
+    cfd::DevBuf<int64_t> sell_ptr;    // [nslice+1] slot offset of each 32-node slice
+    cfd::DevBuf<int> sell_nbr;        // [slots] neighbour id, ~id when the node is node_R
+    cfd::DevBuf<double4> sell_geo;    // [slots] edge unit normal (L->R) + |S|
+    cfd::DevBuf<int> deg;             // [nnode] interior edges per node
     // patch layout of the residual kernel: patches are contiguous ranges of
     // CFD_PATCH_NODES nodes; each patch lists every interior edge touching it
     cfd::DevBuf<int> pe_ptr;          // [npatch+1]

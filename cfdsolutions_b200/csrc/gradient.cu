@@ -14,29 +14,35 @@ namespace cfd {
 
 // Least-squares Gram-Schmidt coefficients r11..r33, ro22, ro33
 // (Compute_Least_Square_Gradient_Coefficients, Euler3D/src/Gradient.cpp:137-228).
-__global__ void k_lsq_coeff(int nnode, const int *__restrict__ ia, const int *__restrict__ ja,
+__global__ void k_lsq_coeff(int nnode, const int64_t *__restrict__ sell_ptr, const int *__restrict__ sell_nbr,
+                            const int *__restrict__ deg,
                             const double *__restrict__ xyz, int weighted, double *__restrict__ cf) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnode) return;
+    const int64_t sb = sell_ptr[i >> 5] + (i & 31);
+    const int dgi = deg[i];
     const double xi = xyz[i], yi = xyz[nnode + i], zi = xyz[2 * nnode + i];
     double r11 = 0, r12 = 0, r13 = 0, r22 = 0, r23 = 0, r33 = 0, ro22 = 0, ro33 = 0;
-    for (int k = ia[i]; k < ia[i + 1]; k++) {
-        const int j = ja[k];
+    for (int k = 0; k < dgi; k++) {
+        int j = sell_nbr[sb + 32 * k];
+        j = j >= 0 ? j : ~j;
         double dx = xyz[j] - xi, dy = xyz[nnode + j] - yi, dz = xyz[2 * nnode + j] - zi;
         const double a = weighted ? 1.0 / sqrt(dx * dx + dy * dy + dz * dz) : 1.0;
         dx *= a; dy *= a; dz *= a;
         r11 += dx * dx; r12 += dx * dy; r13 += dx * dz;
     }
-    for (int k = ia[i]; k < ia[i + 1]; k++) {
-        const int j = ja[k];
+    for (int k = 0; k < dgi; k++) {
+        int j = sell_nbr[sb + 32 * k];
+        j = j >= 0 ? j : ~j;
         double dx = xyz[j] - xi, dy = xyz[nnode + j] - yi, dz = xyz[2 * nnode + j] - zi;
         const double a = weighted ? 1.0 / sqrt(dx * dx + dy * dy + dz * dz) : 1.0;
         dx *= a; dy *= a; dz *= a;
         const double t = dy - (r12 / r11) * dx;
         r22 += t * t; r23 += t * dz; ro22 += t * dy;
     }
-    for (int k = ia[i]; k < ia[i + 1]; k++) {
-        const int j = ja[k];
+    for (int k = 0; k < dgi; k++) {
+        int j = sell_nbr[sb + 32 * k];
+        j = j >= 0 ? j : ~j;
         double dx = xyz[j] - xi, dy = xyz[nnode + j] - yi, dz = xyz[2 * nnode + j] - zi;
         const double a = weighted ? 1.0 / sqrt(dx * dx + dy * dy + dz * dz) : 1.0;
         dx *= a; dy *= a; dz *= a;
@@ -49,19 +55,23 @@ __global__ void k_lsq_coeff(int nnode, const int *__restrict__ ia, const int *__
 
 // Least-squares gradient of Q1..Q5 (Compute_Least_Square_Gradient, Gradient.cpp:232-296).
 __global__ void __launch_bounds__(128) k_lsq_grad(int nnode, int64_t ldq, const double *__restrict__ Q,
-                                                  const int *__restrict__ ia, const int *__restrict__ ja,
+                                                  const int64_t *__restrict__ sell_ptr, const int *__restrict__ sell_nbr,
+                            const int *__restrict__ deg,
                                                   const double *__restrict__ xyz, int weighted,
                                                   const double *__restrict__ cf, double *__restrict__ g) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnode) return;
+    const int64_t sb = sell_ptr[i >> 5] + (i & 31);
+    const int dgi = deg[i];
     const double *c = cf + (int64_t)i * 8;
     const double r11 = c[0], r12 = c[1], r13 = c[2], r22 = c[3], r23 = c[4], ro22 = c[6], ro33 = c[7];
     const double xi = xyz[i], yi = xyz[nnode + i], zi = xyz[2 * nnode + i];
     double qi[5], gx[5] = {0, 0, 0, 0, 0}, gy[5] = {0, 0, 0, 0, 0}, gz[5] = {0, 0, 0, 0, 0};
 #pragma unroll
     for (int v = 0; v < 5; v++) qi[v] = Q[v * ldq + i];
-    for (int k = ia[i]; k < ia[i + 1]; k++) {
-        const int j = ja[k];
+    for (int k = 0; k < dgi; k++) {
+        int j = sell_nbr[sb + 32 * k];
+        j = j >= 0 ? j : ~j;
         double dx = xyz[j] - xi, dy = xyz[nnode + j] - yi, dz = xyz[2 * nnode + j] - zi;
         const double a = weighted ? 1.0 / sqrt(dx * dx + dy * dy + dz * dz) : 1.0;
         dx *= a; dy *= a; dz *= a;
@@ -91,21 +101,21 @@ __global__ void __launch_bounds__(128) k_lsq_grad(int nnode, int64_t ldq, const 
 // (The reference declares GRADINET_METHOD_GREEN_GAUSS, SolverParameters.h:329,
 // without implementing it.)
 __global__ void __launch_bounds__(128) k_gg_grad(int nnode, int64_t ldq, const double *__restrict__ Q,
-                                                 const int *__restrict__ n2e_ptr, const int *__restrict__ n2e,
-                                                 const int2 *__restrict__ en, const double4 *__restrict__ es,
+                                                 const int64_t *__restrict__ sell_ptr, const int *__restrict__ sell_nbr,
+                                                 const int *__restrict__ deg, const double4 *__restrict__ sell_geo,
                                                  const double *__restrict__ vol, double *__restrict__ g) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnode) return;
+    const int64_t sb = sell_ptr[i >> 5] + (i & 31);
+    const int dgi = deg[i];
     double qi[5], gx[5] = {0, 0, 0, 0, 0}, gy[5] = {0, 0, 0, 0, 0}, gz[5] = {0, 0, 0, 0, 0};
 #pragma unroll
     for (int v = 0; v < 5; v++) qi[v] = Q[v * ldq + i];
-    for (int k = n2e_ptr[i]; k < n2e_ptr[i + 1]; k++) {
-        const int s = n2e[k];
-        const int e = s >= 0 ? s : ~s;
-        const int2 nd = en[e];
-        const int j = s >= 0 ? nd.y : nd.x;
-        const double4 S = es[e];
-        const double sg = s >= 0 ? 0.5 : -0.5;  // outward from i
+    for (int k = 0; k < dgi; k++) {
+        const int sn = sell_nbr[sb + 32 * k];
+        const int j = sn >= 0 ? sn : ~sn;
+        const double4 S = sell_geo[sb + 32 * k];  // unit normal L->R and |S|
+        const double sg = sn >= 0 ? 0.5 * S.w : -0.5 * S.w;  // outward from i
         const double sx = sg * S.x, sy = sg * S.y, sz = sg * S.z;
 #pragma unroll
         for (int v = 0; v < 5; v++) {
@@ -129,12 +139,15 @@ __global__ void __launch_bounds__(128) k_gg_grad(int nnode, int64_t ldq, const d
 // the reconstructed-pressure correction (Compute_Limiter_PressureCorrection,
 // :273-304).
 __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const double *__restrict__ Q,
-                                                const int *__restrict__ ia, const int *__restrict__ ja,
+                                                const int64_t *__restrict__ sell_ptr, const int *__restrict__ sell_nbr,
+                            const int *__restrict__ deg,
                                                 const double *__restrict__ xyz, const double *__restrict__ g,
                                                 const double *__restrict__ vol, Flow f, double *__restrict__ phi,
                                                 int *__restrict__ roeflag) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnode) return;
+    const int64_t sb = sell_ptr[i >> 5] + (i & 31);
+    const int dgi = deg[i];
     roeflag[i] = 0;
     const double frac = f.frac;
     double qc[5], qmin[5], qmax[5], ph[5], gx[5], gy[5], gz[5];
@@ -148,8 +161,9 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
         gz[v] = g[(3 * v + 2) * (int64_t)nnode + i];
     }
     const double eps2 = 6.0 * f.venkat_eps_k3 * vol[i] / M_PI;
-    for (int k = ia[i]; k < ia[i + 1]; k++) {
-        const int j = ja[k];
+    for (int k = 0; k < dgi; k++) {
+        int j = sell_nbr[sb + 32 * k];
+        j = j >= 0 ? j : ~j;
 #pragma unroll
         for (int v = 0; v < 5; v++) {
             const double q = Q[v * ldq + j];
@@ -165,8 +179,9 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
         // per edge; the result is the same rounded quotient the reference's
         // per-edge divisions select, except for ties closer than an ulp.
         double bn[5] = {1, 1, 1, 1, 1}, bd[5] = {1, 1, 1, 1, 1};
-        for (int k = ia[i]; k < ia[i + 1]; k++) {
-            const int j = ja[k];
+        for (int k = 0; k < dgi; k++) {
+            int j = sell_nbr[sb + 32 * k];
+            j = j >= 0 ? j : ~j;
             const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
 #pragma unroll
             for (int v = 0; v < 5; v++) {
@@ -183,8 +198,9 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
 #pragma unroll
         for (int v = 0; v < 5; v++) ph[v] = fmax(0.0, bn[v] == bd[v] ? 1.0 : bn[v] / bd[v]);
     } else {  // Barth-Jespersen (Compute_Limiter_Barth_Jespersen, Limiters.cpp:117-178)
-        for (int k = ia[i]; k < ia[i + 1]; k++) {
-            const int j = ja[k];
+        for (int k = 0; k < dgi; k++) {
+            int j = sell_nbr[sb + 32 * k];
+            j = j >= 0 ? j : ~j;
             const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
 #pragma unroll
             for (int v = 0; v < 5; v++) {
@@ -206,8 +222,9 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
     }
     // pressure correction: any negative reconstructed pressure -> first order
     bool neg = false;
-    for (int k = ia[i]; k < ia[i + 1]; k++) {
-        const int j = ja[k];
+    for (int k = 0; k < dgi; k++) {
+        int j = sell_nbr[sb + 32 * k];
+        j = j >= 0 ? j : ~j;
         const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
         double q[5];
 #pragma unroll
@@ -231,17 +248,21 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
 // pass (Jacobi order); the reference sweeps nodes in sequence, which gives
 // the same result whenever this fix does not cascade.
 __global__ void __launch_bounds__(128) k_roe_pressure_fix(int nnode, int64_t ldq, const double *__restrict__ Q,
-                                                          const int *__restrict__ ia, const int *__restrict__ ja,
+                                                          const int64_t *__restrict__ sell_ptr, const int *__restrict__ sell_nbr,
+                            const int *__restrict__ deg,
                                                           const double *__restrict__ xyz,
                                                           const double *__restrict__ g, Flow f,
                                                           const double *__restrict__ phi_in, double *__restrict__ phi) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnode) return;
+    const int64_t sb = sell_ptr[i >> 5] + (i & 31);
+    const int dgi = deg[i];
     const double frac = f.frac;
     bool neg = false;
     const double xi = xyz[i], yi = xyz[nnode + i], zi = xyz[2 * nnode + i];
-    for (int k = ia[i]; k < ia[i + 1] && !neg; k++) {
-        const int j = ja[k];
+    for (int k = 0; k < dgi && !neg; k++) {
+        int j = sell_nbr[sb + 32 * k];
+        j = j >= 0 ? j : ~j;
         const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
         double qa[5], qb[5];
 #pragma unroll
@@ -287,18 +308,18 @@ int cfd_gradient(cfd_ctx *c) {
     const int n = c->nnode;
     CFD_CUDA(c->grad.alloc((size_t)15 * n));
     if (c->params.gradient == CFD_GRAD_GG) {
-        k_gg_grad<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->n2e_ptr.p, c->n2e.p, c->edge_nodes.p,
-                                                             c->edge_sv.p, c->cvol.p, c->grad.p);
+        k_gg_grad<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p, c->deg.p,
+                                                             c->sell_geo.p, c->cvol.p, c->grad.p);
     } else {
         // coefficients depend on the mesh and the weight only (FlagLSCoeff, Gradient.cpp:245-252)
         if (c->lsq_weight != c->params.ls_weight || c->ggw.n != (size_t)8 * n) {
             CFD_CUDA(c->ggw.alloc((size_t)8 * n));
-            k_lsq_coeff<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->n2n_ia.p, c->n2n_ja.p, c->xyz.p,
+            k_lsq_coeff<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->sell_ptr.p, c->sell_nbr.p, c->deg.p, c->xyz.p,
                                                                    c->params.ls_weight, c->ggw.p);
             CFD_LAUNCH_CHECK();
             c->lsq_weight = c->params.ls_weight;
         }
-        k_lsq_grad<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->n2n_ia.p, c->n2n_ja.p, c->xyz.p,
+        k_lsq_grad<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p, c->deg.p, c->xyz.p,
                                                               c->params.ls_weight, c->ggw.p, c->grad.p);
     }
     CFD_LAUNCH_CHECK();
@@ -317,7 +338,7 @@ int cfd_limiter(cfd_ctx *c) {
         CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)5 * n)));
         return CFD_OK;
     }
-    k_venkat<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->n2n_ia.p, c->n2n_ja.p, c->xyz.p, c->grad.p,
+    k_venkat<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p, c->deg.p, c->xyz.p, c->grad.p,
                                                         c->cvol.p, c->flow, c->phi.p, c->roeflag.p);
     CFD_LAUNCH_CHECK();
     if (c->params.flux_scheme == CFD_FLUX_ROE) {
@@ -339,7 +360,7 @@ int roe_fix_standalone(cfd_ctx *c) {
     const int n = c->nnode;
     CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)5 * n)));
     CFD_CUDA(cudaMemcpyAsync(c->work.p, c->phi.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToDevice, c->stream));
-    k_roe_pressure_fix<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->n2n_ia.p, c->n2n_ja.p, c->xyz.p,
+    k_roe_pressure_fix<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p, c->deg.p, c->xyz.p,
                                                                   c->grad.p, c->flow, c->work.p, c->phi.p);
     CFD_LAUNCH_CHECK();
     c->roe_fix_pending = false;

@@ -141,6 +141,25 @@ __device__ __forceinline__ double edge_flux(const double qL[5], const double qR[
     return roe_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
 }
 
+// Pressure of the Roe-averaged state of two reconstructed face states
+// (Compute_RoeVariables, Roe_Fluxes.cpp:3609-3633, tested in
+// Compute_Limiter_RoePressureCorrection, Limiters.cpp:311-356).
+__device__ __forceinline__ double roe_avg_pressure(const double qa[5], const double qb[5], double g) {
+    const double ra = qa[0], rb = qb[0];
+    const double ia = 1.0 / ra, ib = 1.0 / rb;
+    const double ua = qa[1] * ia, va = qa[2] * ia, wa = qa[3] * ia;
+    const double ub = qb[1] * ib, vb = qb[2] * ib, wb = qb[3] * ib;
+    const double pa = (g - 1.0) * (qa[4] - 0.5 * ra * (ua * ua + va * va + wa * wa));
+    const double pb = (g - 1.0) * (qb[4] - 0.5 * rb * (ub * ub + vb * vb + wb * wb));
+    const double ha = (qa[4] + pa) * ia, hb = (qb[4] + pb) * ib;
+    const double rho = sqrt(ra * rb), sg = rho / (ra + rho);
+    const double u = ua + sg * (ub - ua), v = va + sg * (vb - va), w = wa + sg * (wb - wa);
+    const double ht = ha + sg * (hb - ha);
+    const double q2 = u * u + v * v + w * w;
+    const double e = (rho / g) * (ht + 0.5 * (g - 1.0) * q2);
+    return (g - 1.0) * (e - 0.5 * rho * q2);
+}
+
 __device__ __forceinline__ void store_low(float *p, double v) { *p = (float)v; }
 __device__ __forceinline__ void store_low(uint16_t *p, double v) {
     __nv_bfloat16 b = __double2bfloat16(v);

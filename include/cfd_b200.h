@@ -102,7 +102,7 @@ typedef struct cfd_params {
     double cfl_min;          /* CFL_MIN                      */
     double cfl_max;          /* CFL_MAX                      */
     double venkat_k;         /* VENKAT_K_THRESHOLD           */
-    int    residual_kernel;  /* 0: patch kernel when the mesh fits it, 1: node-gather kernel */
+    int    residual_kernel;  /* 0: node-gather kernel (sliced-ELL), 1: shared-memory patch kernel */
 } cfd_params;
 
 /* Fills p with the defaults used by the reference parameter files of this
