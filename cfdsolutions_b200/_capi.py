@@ -104,6 +104,7 @@ SIGNATURES = {
     "cfd_get_deltat": (I, [P, P]),
     "cfd_get_extrema": (I, [P, P]),
     "cfd_get_farfield": (I, [P, P]),
+    "cfd_set_farfield": (I, [P, P]),
     "cfd_get_gradients": (I, [P, P]),
     "cfd_get_limiters": (I, [P, P]),
     "cfd_get_system": (I, [P, P, P, P]),
@@ -125,7 +126,7 @@ SIGNATURES = {
 
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
-        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m cfdsolutions_b200.build`")
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python cfdsolutions_b200/build.py`")
     lib = C.CDLL(str(LIB_PATH))
     for name, (res, args) in SIGNATURES.items():
         fn = getattr(lib, name)

@@ -3,7 +3,8 @@
 Every translation unit is compiled by nvcc for sm_100a only
 (``-gencode arch=compute_100a,code=sm_100a``) with ``-lineinfo``; the result
 lives inside the package so it travels with the source tree.  Run as
-``python -m cfdsolutions_b200.build`` or call :func:`build`.
+``python cfdsolutions_b200/build.py`` (as a script, so the stale library is not
+loaded by the package import first) or call :func:`build`.
 """
 from __future__ import annotations
 

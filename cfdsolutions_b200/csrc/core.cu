@@ -705,6 +705,7 @@ static void compute_flow(cfd_ctx *c, int iteration) {
     Flow &f = c->flow;
     f.gamma = p.gamma;
     f.gm1 = p.gamma - 1.0;
+    f.inv_gm1 = 1.0 / (p.gamma - 1.0);
     double mach;
     if (p.mach_ramp > 1 && p.mach > p.mach_min) {
         mach = iteration < p.mach_ramp
@@ -1446,6 +1447,14 @@ int cfd_get_farfield(cfd_ctx *c, double out[8]) {
     const Flow &f = c->flow;
     out[0] = f.inf_rho; out[1] = f.inf_u; out[2] = f.inf_v; out[3] = f.inf_w;
     out[4] = f.inf_et; out[5] = f.inf_p; out[6] = f.inf_c; out[7] = f.inf_mach;
+    return CFD_OK;
+}
+
+int cfd_set_farfield(cfd_ctx *c, const double in[8]) {
+    if (!c || !in) return CFD_ERR_ARG;
+    Flow &f = c->flow;
+    f.inf_rho = in[0]; f.inf_u = in[1]; f.inf_v = in[2]; f.inf_w = in[3];
+    f.inf_et = in[4]; f.inf_p = in[5]; f.inf_c = in[6]; f.inf_mach = in[7];
     return CFD_OK;
 }
 

@@ -230,8 +230,11 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
 #pragma unroll
         for (int v = 0; v < 5; v++)
             q[v] = qc[v] + ph[v] * (frac * (Q[v * ldq + j] - qc[v]) + (1.0 - frac) * (gx[v] * rx + gy[v] * ry + gz[v] * rz));
-        const double p = f.gm1 * (q[4] - (0.5 / q[0]) * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]));
-        if (p < 0.0) neg = true;
+        // p < 0 of (Limiters.cpp:296-301) without the division when rho > 0
+        const double m2 = q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+        const bool pneg = q[0] > 0.0 ? (2.0 * q[0] * q[4] < m2)
+                                     : (f.gm1 * (q[4] - (0.5 / q[0]) * m2) < 0.0);
+        if (pneg) neg = true;
     }
     if (neg) {
 #pragma unroll

@@ -12,7 +12,7 @@ namespace cfd {
 // Flow constants of one iteration (ComputeFarFieldCondition,
 // Euler3D/src/Material.cpp:185-210) and the options the kernels branch on.
 struct Flow {
-    double gamma, gm1;
+    double gamma, gm1, inv_gm1;
     double inf_rho, inf_u, inf_v, inf_w, inf_p, inf_et, inf_c, inf_mach;
     double outflow_p;
     double frac;          // 0.5 for LIMITER_ORDER_SECOND else 0 (HigherOrderReconstructQ.cpp:27-29)
@@ -84,8 +84,11 @@ __device__ __forceinline__ double roe_flux(const double qL[5], const double qR[5
     conv[3] = ha * ((L.w * mL + L.p * nz) + (R.w * mR + R.p * nz));
     conv[4] = ha * (L.ht * mL + R.ht * mR);
 
-    // Roe averages (FluxTest.cpp:3107-3115)
-    const double rho = sqrt(R.rho * L.rho);
+    // Roe averages (FluxTest.cpp:3107-3115); rho and 1/rho, c and 1/c from one
+    // reciprocal square root each
+    const double rr = R.rho * L.rho;
+    const double rho_i = rsqrt(rr);
+    const double rho = rr * rho_i;
     const double sigma = rho / (L.rho + rho);
     const double u = L.u + sigma * (R.u - L.u);
     const double v = L.v + sigma * (R.v - L.v);
@@ -93,7 +96,9 @@ __device__ __forceinline__ double roe_flux(const double qL[5], const double qR[5
     const double ht = L.ht + sigma * (R.ht - L.ht);
     const double q2 = u * u + v * v + w * w;
     // Get_SpeedSound(u,v,w,ht), generic non-dimensionalisation (Material.cpp:939-960)
-    const double c = sqrt(f.gm1 * ht - 0.5 * f.gm1 * q2);
+    const double c2 = f.gm1 * ht - 0.5 * f.gm1 * q2;
+    const double ci = rsqrt(c2);
+    const double c = c2 * ci;
     const double ubar = u * nx + v * ny + w * nz;
 
     double E0, E1, E2;
@@ -110,11 +115,10 @@ __device__ __forceinline__ double roe_flux(const double qL[5], const double qR[5
 
     const double drho = R.rho - L.rho, du = R.u - L.u, dv = R.v - L.v, dw_ = R.w - L.w, dp = R.p - L.p;
     const double dU = du * nx + dv * ny + dw_ * nz;
-    const double ci = 1.0 / c;
     const double Es = E1 + E2 - 2.0 * E0;
     const double Ed = E1 - E2;
     const double t1 = 0.5 * dU * Es;
-    const double t2 = Ed * dp * (0.5 * ci) / rho;
+    const double t2 = Ed * dp * (0.5 * ci) * rho_i;
     const double w0 = E0 * drho + Es * dp * (0.5 * ci * ci) + rho * Ed * dU * (0.5 * ci);
     const double w1 = E0 * du + nx * t1 + nx * t2;
     const double w2 = E0 * dv + ny * t1 + ny * t2;
@@ -126,7 +130,7 @@ __device__ __forceinline__ double roe_flux(const double qL[5], const double qR[5
     diss[1] = hd * (u * w0 + rho * w1);
     diss[2] = hd * (v * w0 + rho * w2);
     diss[3] = hd * (w * w0 + rho * w3);
-    diss[4] = hd * (0.5 * q2 * w0 + rho * (u * w1 + v * w2 + w * w3) + w4 / f.gm1);
+    diss[4] = hd * (0.5 * q2 * w0 + rho * (u * w1 + v * w2 + w * w3) + w4 * f.inv_gm1);
     return fmax(E0, fmax(E1, E2));
 }
 

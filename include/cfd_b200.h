@@ -229,6 +229,11 @@ int  cfd_get_deltat(cfd_ctx *ctx, double *dt);                    /* [nnode] */
 int  cfd_get_extrema(cfd_ctx *ctx, double out[8]);
 /* Far field {rho,u,v,w,et,p,c,mach} of the last cfd_begin_iteration. */
 int  cfd_get_farfield(cfd_ctx *ctx, double out[8]);
+/* Override the far field with values a driver computed itself (its globals
+ * Inf_Rho, Inf_U, Inf_V, Inf_W, Inf_Et, Inf_Pressure, Inf_SpeedSound, Inf_Mach
+ * after ComputeFarFieldCondition, Euler3D/src/Material.cpp:185-210); holds
+ * until the next cfd_begin_iteration / cfd_deltat. */
+int  cfd_set_farfield(cfd_ctx *ctx, const double in[8]);
 int  cfd_get_gradients(cfd_ctx *ctx, double *g);                  /* [15][nnode] */
 int  cfd_get_limiters(cfd_ctx *ctx, double *phi);                 /* [5][nnode]  */
 /* A [nnzb][25] (FP64 copy), B [nnode][5], X [nnode][5]; NULL skips. */
