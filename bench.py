@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--cpu-procs", type=int, default=0, help="reference processes (0 = one per core, max 16)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--side-rcm", action="store_true", help="also time the plain node-level RCM numbering")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling case for ncu: two residual steps per kernel variant, no timing, no output line")
     return ap.parse_args()
 
 
@@ -179,6 +181,23 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def profile_case(n):
+    """Small fixed case for ncu captures (`--profile --n 64`): the bench
+    workload on an n^3 cube, two residual steps with the node-gather kernel then
+    two with the patch kernel."""
+    from cfdsolutions_b200 import Euler3DGPU, box_mesh, default_params, perturbed_freestream
+    from cfdsolutions_b200.mesh import NUMBERING_PATCH_RCM
+
+    m = box_mesh(n, jitter=0.15, seed=1234, rcm=NUMBERING_PATCH_RCM)
+    Q = perturbed_freestream(m, CFG["gamma"], CFG["mach"], CFG["alpha_deg"], noise=0.01, seed=1235)
+    for kern in (0, 1):
+        with Euler3DGPU(m, default_params(**dict(CFG, residual_kernel=kern))) as s:
+            s.set_state(Q)
+            for i in range(2):
+                s.residual_step(i)
+            s.synchronize()
+
+
 def workload_config(n, mesh=None):
     c = {"workload": f"second-order residual evaluation, {n}^3-hex tet cube (6 tets/hex), RCM, jitter 0.15h, "
                      "Green-Gauss + Venkatakrishnan K=5 + Roe, M=0.8, alpha=1.25, +-1% noise",
@@ -198,6 +217,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.profile:
+        profile_case(args.n)
         return
 
     import torch
