@@ -25,6 +25,7 @@ GRAD_LSQ, GRAD_GG = 0, 1
 PREC_FP64, PREC_FP32, PREC_BF16 = 0, 1, 2
 PC_NONE, PC_BLOCK_JACOBI, PC_ILU0 = 0, 1, 2
 BC_EULER_WALL, BC_FAR_FIELD, BC_INFLOW, BC_OUTFLOW = 0, 1, 2, 3
+GS_STATIC_MAX_ROWS = 16384
 
 
 class CfdError(RuntimeError):
@@ -97,6 +98,7 @@ SIGNATURES = {
     "cfd_residual_rms": (I, [P, I, P]),
     "cfd_jacobian": (I, [P, I, I, I]),
     "cfd_block_gs": (I, [P, I, I, C.POINTER(D)]),
+    "cfd_block_gs_static": (I, [I, P, P, P, P, P, P, I, I, P, C.POINTER(D)]),
     "cfd_gmres_default": (None, [C.POINTER(GmresOpts)]),
     "cfd_gmres": (I, [P, C.POINTER(GmresOpts), C.POINTER(GmresStats)]),
     "cfd_update": (I, [P, D]),

@@ -171,6 +171,16 @@ __device__ __forceinline__ double load_low(const uint16_t *p) {
     return (double)__bfloat162float(b);
 }
 
+// Kernels shared across translation units (defined in core.cu / linsolve.cu).
+__global__ void k_lu_nopivot(int nnode, const double *__restrict__ A, const int *__restrict__ IAU,
+                             double *__restrict__ LU);
+__global__ void k_gs_level(int nrows, const int *__restrict__ rows, const int *__restrict__ IA,
+                           const int *__restrict__ JA, const int *__restrict__ IAU, const double *__restrict__ A,
+                           const double *__restrict__ B, const double *__restrict__ LU, double *__restrict__ X,
+                           double *__restrict__ rowrms);
+__global__ void k_sum_partial(const double *__restrict__ x, int64_t n, double *__restrict__ part);
+__global__ void k_sum_one(const double *__restrict__ part, int nblk, double *__restrict__ out);
+
 // Deterministic sum of a plain vector (host result).
 int reduce_sum_plain(cfd_ctx *c, const double *x, int64_t n, double *out_host);
 

@@ -219,6 +219,25 @@ void cfd_gmres_default(cfd_gmres_opts *o);
  * the implicit drivers call in its place. */
 int  cfd_gmres(cfd_ctx *ctx, const cfd_gmres_opts *o, cfd_gmres_stats *st);
 
+/* Block Gauss-Seidel that allocates no device memory.  No counterpart in the
+ * reference: it exists for callers that cannot let a library call cudaMalloc
+ * (a host framework that reserved all device memory up front and passes in only
+ * its own buffers, or a running solver loop that must not reach the CUDA
+ * allocator).  Same sweeps and arithmetic as cfd_block_gs, on a system the
+ * caller holds in device memory: IA/JA/IAU block-CRS pattern (as
+ * SolverBlockMatrix), A [nnzb][5][5], B and X [nrow][5]; X is overwritten
+ * (starts at zero), *rms as cfd_block_gs.  Its scratch is one static device
+ * array of this library for up to CFD_GS_STATIC_MAX_ROWS rows (about 3.5 MB,
+ * reserved on every GPU that loads the library until the process exits);
+ * larger systems return CFD_ERR_RANGE.  The array is shared: calls that
+ * overlap on the GPU race, so keep them on one stream.  The first call on a
+ * device looks up the array's device address (make it before any stream
+ * capture).  Work runs on `stream` (a cudaStream_t, NULL = legacy stream). */
+#define CFD_GS_STATIC_MAX_ROWS 16384
+int  cfd_block_gs_static(int nrow, const int *IA, const int *JA, const int *IAU, const double *A,
+                         const double *B, double *X, int iterations, int direction, void *stream,
+                         double *rms);
+
 /* Q += relax * X on physical nodes (Solver_Steady_Implicit.cpp:153-159). */
 int  cfd_update(cfd_ctx *ctx, double relax);
 
