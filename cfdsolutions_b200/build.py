@@ -20,9 +20,9 @@ OUT_DIR = PKG / "_lib"
 LIB = OUT_DIR / "libcfd_b200.so"
 OBJ_DIR = PKG / "_build"
 
-CU_SOURCES = ["core.cu", "gradient.cu", "linsolve.cu", "gs_static.cu"]
+CU_SOURCES = ["core.cu", "gradient.cu", "linsolve.cu", "ilu_mc.cu", "gs_static.cu"]
 CXX_SOURCES = ["mesh.cpp"]
-HEADERS = ["cfd_internal.h", "ctx.cuh", "kernels.cuh", "physics.cuh"]
+HEADERS = ["cfd_internal.h", "ctx.cuh", "kernels.cuh", "physics.cuh", "ilu_mc.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",

@@ -490,14 +490,14 @@ __global__ void __launch_bounds__(128) k_jac_edges(int nedge, int64_t ldq, const
 #pragma unroll
     for (int k = 0; k < 25; k++) {
         const double val = ha * (J[k] - Ab[k]);
-        A64[(int64_t)sl.x * 25 + k] = val;
+        if (A64) A64[(int64_t)sl.x * 25 + k] = val;
         if (Alow) store_low(Alow + (int64_t)sl.x * 25 + k, val);
     }
     euler_flux_jacobian(qL, g.x, g.y, g.z, f.gamma, J);
 #pragma unroll
     for (int k = 0; k < 25; k++) {
         const double val = -ha * (J[k] + Ab[k]);
-        A64[(int64_t)sl.y * 25 + k] = val;
+        if (A64) A64[(int64_t)sl.y * 25 + k] = val;
         if (Alow) store_low(Alow + (int64_t)sl.y * 25 + k, val);
     }
 }
@@ -522,9 +522,15 @@ __global__ void __launch_bounds__(128) k_jac_rows(
     const int dg = IAU[i];
     for (int k = IA[i]; k < IA[i + 1]; k++) {
         if (k == dg) continue;
-        const double *blk = A64 + (int64_t)tslot[k] * 25;
+        if (A64) {
+            const double *blk = A64 + (int64_t)tslot[k] * 25;
 #pragma unroll
-        for (int m = 0; m < 25; m++) D[m] -= blk[m];
+            for (int m = 0; m < 25; m++) D[m] -= blk[m];
+        } else {  // low-precision-only system: sum the stored blocks
+            const TA *blk = Alow + (int64_t)tslot[k] * 25;
+#pragma unroll
+            for (int m = 0; m < 25; m++) D[m] -= load_low(blk + m);
+        }
     }
     for (int k = n2b_ptr[i]; k < n2b_ptr[i + 1]; k++) {
         const int b = n2b[k];
@@ -544,7 +550,7 @@ __global__ void __launch_bounds__(128) k_jac_rows(
     }
 #pragma unroll
     for (int m = 0; m < 25; m++) {
-        A64[(int64_t)dg * 25 + m] = D[m];
+        if (A64) A64[(int64_t)dg * 25 + m] = D[m];
         if (Alow) store_low(Alow + (int64_t)dg * 25 + m, D[m]);
     }
 #pragma unroll
@@ -1191,6 +1197,7 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         CFD_CUDA(c->tslot.upload(ts.data(), ts.size(), s));
         CFD_CUDA(c->eslot.upload(es.data(), es.size(), s));
         int e1 = 0, e2 = 0;
+        c->mc.built = false;  // block multicolour ILU ordering is rebuilt on first use
         build_levels(c->h_IA, c->h_JA, nnode, true, c->lv_fwd, s, e1);
         build_levels(c->h_IA, c->h_JA, nnode, false, c->lv_bwd, s, e2);
         if (e1 || e2) { set_error("cfd_set_mesh: level upload failed"); return CFD_ERR_CUDA; }
@@ -1334,41 +1341,48 @@ int cfd_residual_rms(cfd_ctx *c, int include_diss, double out[6]) {
 
 int cfd_jacobian(cfd_ctx *c, int add_time, int include_diss, int precision) {
     NEED_MESH("cfd_jacobian");
-    if (precision < CFD_PREC_FP64 || precision > CFD_PREC_BF16) return CFD_ERR_ARG;
-    CFD_CUDA(c->A64.alloc((size_t)c->nnzb * 25));
+    const bool low_only = (precision & CFD_PREC_LOW_ONLY) != 0;
+    precision &= ~CFD_PREC_LOW_ONLY;
+    if (precision < CFD_PREC_FP64 || precision > CFD_PREC_BF16 || (low_only && precision == CFD_PREC_FP64)) {
+        set_error("cfd_jacobian: precision must be FP64, FP32 or BF16 (LOW_ONLY with FP32/BF16)");
+        return CFD_ERR_ARG;
+    }
+    if (!low_only) CFD_CUDA(c->A64.alloc((size_t)c->nnzb * 25));
     CFD_CUDA(c->B.alloc((size_t)c->nnode * 5));
     CFD_CUDA(c->X.alloc((size_t)c->nnode * 5));
     c->a_precision = precision;
+    c->a64_valid = !low_only;
+    double *A64 = low_only ? nullptr : c->A64.p;
     const int ge = grid_for(c->nedge, 128), gr = grid_for(c->nnode, 128);
     if (precision == CFD_PREC_FP32) {
         CFD_CUDA(c->A32.alloc((size_t)c->nnzb * 25));
         if (c->nedge)
             k_jac_edges<float><<<ge, 128, 0, c->stream>>>(c->nedge, c->ldq, c->Q.p, c->edge_nodes.p, c->edge_geo.p,
-                                                          c->eslot.p, c->flow, c->A64.p, c->A32.p);
+                                                          c->eslot.p, c->flow, A64, c->A32.p);
         CFD_LAUNCH_CHECK();
         k_jac_rows<float><<<gr, 128, 0, c->stream>>>(c->nnode, c->ldq, c->Q.p, c->IA.p, c->IAU.p, c->tslot.p,
                                                      c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p,
                                                      c->cvol.p, c->dt.p, c->res.p, c->resd.p, add_time, include_diss,
-                                                     c->flow, c->A64.p, c->A32.p, c->B.p);
+                                                     c->flow, A64, c->A32.p, c->B.p);
     } else if (precision == CFD_PREC_BF16) {
         CFD_CUDA(c->A16.alloc((size_t)c->nnzb * 25));
         if (c->nedge)
             k_jac_edges<uint16_t><<<ge, 128, 0, c->stream>>>(c->nedge, c->ldq, c->Q.p, c->edge_nodes.p,
-                                                             c->edge_geo.p, c->eslot.p, c->flow, c->A64.p, c->A16.p);
+                                                             c->edge_geo.p, c->eslot.p, c->flow, A64, c->A16.p);
         CFD_LAUNCH_CHECK();
         k_jac_rows<uint16_t><<<gr, 128, 0, c->stream>>>(c->nnode, c->ldq, c->Q.p, c->IA.p, c->IAU.p, c->tslot.p,
                                                         c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p,
                                                         c->cvol.p, c->dt.p, c->res.p, c->resd.p, add_time,
-                                                        include_diss, c->flow, c->A64.p, c->A16.p, c->B.p);
+                                                        include_diss, c->flow, A64, c->A16.p, c->B.p);
     } else {
         if (c->nedge)
             k_jac_edges<float><<<ge, 128, 0, c->stream>>>(c->nedge, c->ldq, c->Q.p, c->edge_nodes.p, c->edge_geo.p,
-                                                          c->eslot.p, c->flow, c->A64.p, (float *)nullptr);
+                                                          c->eslot.p, c->flow, A64, (float *)nullptr);
         CFD_LAUNCH_CHECK();
         k_jac_rows<float><<<gr, 128, 0, c->stream>>>(c->nnode, c->ldq, c->Q.p, c->IA.p, c->IAU.p, c->tslot.p,
                                                      c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p,
                                                      c->cvol.p, c->dt.p, c->res.p, c->resd.p, add_time, include_diss,
-                                                     c->flow, c->A64.p, (float *)nullptr, c->B.p);
+                                                     c->flow, A64, (float *)nullptr, c->B.p);
     }
     CFD_LAUNCH_CHECK();
     c->has_system = true;
@@ -1378,6 +1392,10 @@ int cfd_jacobian(cfd_ctx *c, int add_time, int include_diss, int precision) {
 int cfd_block_gs(cfd_ctx *c, int iterations, int direction, double *rms) {
     NEED_MESH("cfd_block_gs");
     if (!c->has_system) { set_error("cfd_block_gs: no system (call cfd_jacobian)"); return CFD_ERR_STATE; }
+    if (!c->a64_valid) {
+        set_error("cfd_block_gs: the system is stored in low precision only (CFD_PREC_LOW_ONLY)");
+        return CFD_ERR_STATE;
+    }
     if (direction < 0 || direction > 2) return CFD_ERR_ARG;
     const int n = c->nnode;
     CFD_CUDA(c->LUd.alloc((size_t)n * 25));
@@ -1461,7 +1479,27 @@ int cfd_set_farfield(cfd_ctx *c, const double in[8]) {
 int cfd_get_system(cfd_ctx *c, double *A, double *B, double *X) {
     NEED_MESH("cfd_get_system");
     if (!c->has_system) { set_error("cfd_get_system: no system"); return CFD_ERR_STATE; }
-    if (A) CFD_CUDA(cudaMemcpyAsync(A, c->A64.p, sizeof(double) * 25 * c->nnzb, cudaMemcpyDeviceToHost, c->stream));
+    if (A && c->a64_valid) {
+        CFD_CUDA(cudaMemcpyAsync(A, c->A64.p, sizeof(double) * 25 * c->nnzb, cudaMemcpyDeviceToHost, c->stream));
+    } else if (A) {  // low-precision-only system: widen on the host
+        const size_t nz = (size_t)c->nnzb * 25;
+        if (c->a_precision == CFD_PREC_FP32) {
+            std::vector<float> h(nz);
+            CFD_CUDA(cudaMemcpyAsync(h.data(), c->A32.p, sizeof(float) * nz, cudaMemcpyDeviceToHost, c->stream));
+            CFD_CUDA(cudaStreamSynchronize(c->stream));
+            for (size_t k = 0; k < nz; k++) A[k] = h[k];
+        } else {
+            std::vector<uint16_t> h(nz);
+            CFD_CUDA(cudaMemcpyAsync(h.data(), c->A16.p, sizeof(uint16_t) * nz, cudaMemcpyDeviceToHost, c->stream));
+            CFD_CUDA(cudaStreamSynchronize(c->stream));
+            for (size_t k = 0; k < nz; k++) {
+                const uint32_t bits = (uint32_t)h[k] << 16;
+                float f;
+                std::memcpy(&f, &bits, sizeof f);
+                A[k] = f;
+            }
+        }
+    }
     if (B) CFD_CUDA(cudaMemcpyAsync(B, c->B.p, sizeof(double) * 5 * c->nnode, cudaMemcpyDeviceToHost, c->stream));
     if (X) CFD_CUDA(cudaMemcpyAsync(X, c->X.p, sizeof(double) * 5 * c->nnode, cudaMemcpyDeviceToHost, c->stream));
     CFD_CUDA(cudaStreamSynchronize(c->stream));
@@ -1477,6 +1515,7 @@ int cfd_set_system(cfd_ctx *c, const double *A, const double *B) {
     CFD_CUDA(cudaMemsetAsync(c->X.p, 0, sizeof(double) * 5 * c->nnode, c->stream));
     CFD_CUDA(cudaStreamSynchronize(c->stream));
     c->a_precision = CFD_PREC_FP64;
+    c->a64_valid = true;
     c->has_system = true;
     return CFD_OK;
 }

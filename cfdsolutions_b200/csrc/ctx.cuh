@@ -50,6 +50,25 @@ struct Levels {
     int max_width = 0;
 };
 
+// Block multicolour ordering of the ILU(0) preconditioner (ilu_mc.cu): rows
+// are grouped in patches of consecutive rows, the patch graph is coloured
+// greedily, and the factorisation order is colour by colour, row index within
+// a colour.
+struct Abmc {
+    bool built = false;
+    int ncolor = 0, maxrow = 0, maxlev = 0, maxstage = 0;
+    std::vector<int> cptr;            // host [ncolor+1] into patches
+    std::vector<int> h_pcolor;        // host colour of each patch
+    DevBuf<int> patches;              // patch ids in colour order
+    DevBuf<int> slot;                 // [nnzb] per row: lower slots (factorisation order) | diag | upper slots
+    DevBuf<int> scol;                 // [nnzb] column of each slot entry
+    DevBuf<int4> meta;                // per row: external lower, lower, intra-patch upper, lev_f | lev_b << 16
+    DevBuf<int2> plev;                // per patch: last forward level, last backward level
+    DevBuf<int4> hdr;                 // [nnzb] per lower block: slot of inv(U_pp), pairs, local slot
+    DevBuf<int64_t> pair_ptr;         // [n+1] update pairs of each row
+    DevBuf<int2> pairs;               // (slot of U_pj, local slot of (i,j))
+};
+
 }  // namespace cfd
 
 struct cfd_ctx {
@@ -120,6 +139,7 @@ struct cfd_ctx {
     cfd::DevBuf<float> A32;     // [nnzb][25] when FP32 storage requested
     cfd::DevBuf<uint16_t> A16;  // [nnzb][25] BF16 storage
     int a_precision = CFD_PREC_FP64;
+    bool a64_valid = false;     // A64 holds the current system
     cfd::DevBuf<double> B, X;   // [nnode][5]
     cfd::DevBuf<double> LUd;    // [nnode][25] diagonal LU for block GS
     cfd::DevBuf<double> rowrms; // [nnode]
@@ -131,6 +151,7 @@ struct cfd_ctx {
     cfd::DevBuf<double> work;   // misc vectors
     cfd::DevBuf<double> dots;   // device dot results
     cfd::DevBuf<int> ilu_diag_inv_done;
+    cfd::Abmc mc;               // block multicolour ILU(0) ordering
     int krylov_m = 0;
     bool has_system = false;
     bool has_grad = false;

@@ -1,0 +1,578 @@
+// Block ILU(0) in block multicolour order.
+//
+// The level-scheduled ILU(0) in mesh order needs one launch per dependency
+// level in the factorisation and in each triangular solve; on a banded
+// (RCM-like) numbering of an n^3 mesh that is O(n) levels of a few thousand
+// rows each, so the solves are bound by launch latency, not by HBM.  Here the
+// rows are grouped in patches of kMcRows (64) consecutive rows and the
+// patch graph (two patches adjacent when a matrix block couples them) is
+// coloured greedily.  The factorisation order is: colours in increasing
+// order, rows of a colour in increasing index.  Two patches of one colour are
+// never coupled, so every patch of a colour is factored (or solved) by its own
+// CTA in one launch per colour; inside a patch the rows follow their local
+// dependency levels, separated by __syncthreads().  This is ILU(0) of P A P^T
+// for the permutation P of that order (the ordering idea is the algebraic block
+// multicolour ordering of Iwashita, Nakashima and Takahashi, IPDPS 2012).
+//
+// Storage: `slot` lists each row's CRS slots as [lower, in factorisation
+// order | diagonal | upper, in factorisation order]; the factors are stored
+// in that order (entry u of row i at block IA[i] + u): L (unit diagonal) for
+// the lower entries, inv(U_ii) for the diagonal, U for the upper entries.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <vector>
+
+#include "ctx.cuh"
+#include "kernels.cuh"
+#include "ilu_mc.cuh"
+
+namespace cfd {
+
+namespace {
+
+// Rows per patch of the ordering (five solve threads per row).
+constexpr int kMcRows = 64;
+
+template <typename T>
+__device__ __forceinline__ double ld(const T *p);
+template <>
+__device__ __forceinline__ double ld<double>(const double *p) { return *p; }
+template <>
+__device__ __forceinline__ double ld<float>(const float *p) { return (double)*p; }
+template <>
+__device__ __forceinline__ double ld<uint16_t>(const uint16_t *p) { return load_low(p); }
+
+template <typename T>
+__device__ __forceinline__ void st(T *p, double v);
+template <>
+__device__ __forceinline__ void st<double>(double *p, double v) { *p = v; }
+template <>
+__device__ __forceinline__ void st<float>(float *p, double v) { *p = (float)v; }
+
+// 5x5 inverse by Gauss-Jordan with partial pivoting across a warp: lane
+// r*5+c (r, c < 5) holds entry (r,c) of the matrix (a) and of the inverse
+// being formed (v); lanes 25-31 carry zeros.  The pivot of column k is the
+// first row >= k of largest magnitude, as in the sequential elimination, and
+// every entry sees the same operations in the same order.  Returns false
+// (on every lane) when a pivot is zero.
+__device__ __forceinline__ bool warp_inverse5(double &a, double &v, int lane) {
+    const int r = lane / 5, c = lane - 5 * (lane / 5);
+    const bool on = lane < 25;
+    v = (on && r == c) ? 1.0 : 0.0;
+    if (!on) a = 0.0;
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        // pivot: largest |a(r,k)| over r >= k, lowest r on ties
+        double best = (on && c == k && r >= k) ? fabs(a) : -1.0;
+        int brow = r;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int orow = __shfl_xor_sync(0xffffffffu, brow, o);
+            if (ob > best || (ob == best && orow < brow)) { best = ob; brow = orow; }
+        }
+        if (!(best > 0.0)) ok = false;
+        // swap rows k and brow
+        const int sr = r == k ? brow : (r == brow ? k : r);
+        const int from = on ? sr * 5 + c : lane;
+        a = __shfl_sync(0xffffffffu, a, from);
+        v = __shfl_sync(0xffffffffu, v, from);
+        // scale row k by 1/a(k,k)
+        const double d = 1.0 / __shfl_sync(0xffffffffu, a, k * 5 + k);
+        if (on && r == k) { a *= d; v *= d; }
+        // eliminate column k from the other rows
+        const double f = __shfl_sync(0xffffffffu, a, (on ? r : 0) * 5 + k);
+        const double ak = __shfl_sync(0xffffffffu, a, k * 5 + (on ? c : 0));
+        const double vk = __shfl_sync(0xffffffffu, v, k * 5 + (on ? c : 0));
+        if (on && r != k) { a -= f * ak; v -= f * vk; }
+    }
+    return ok;
+}
+
+// Shared-memory bytes of one warp of k_mc_factor, rounded up to 16.
+__host__ __device__ inline size_t mc_factor_warp_bytes(int maxrow, int maxstage) {
+    const size_t b = (size_t)maxrow * sizeof(int4) + (size_t)(maxrow + maxstage) * 25 * sizeof(double) +
+                     (size_t)(2 * maxstage + maxrow) * sizeof(int);
+    return (b + 15) & ~(size_t)15;
+}
+
+// Factorisation of the patches of one colour, one warp per patch: the warp
+// factors the patch's rows in increasing order (a row's lower blocks inside
+// the patch belong to earlier rows of the same warp; the others to earlier
+// colours), so no CTA-wide barrier is needed.  Row i's
+// blocks are staged in shared memory in FP64 (CRS slot order) together with
+// every factor block the row needs from earlier rows: inv(U_pp) for each lower
+// block (i,p) and U_pj for each pair (p,j) with j in row i, listed per row at
+// setup.  All those loads are issued together, then the elimination runs from
+// shared memory: for each lower block, in factorisation order,
+// L_ip = A_ip inv(U_pp) and A_ij -= L_ip U_pj over the row's pairs of p.
+// The factors are stored in each row's factorisation order (row i's entry u of
+// the slot list at M[(IA[i] + u) * 25]), so the solves read them as a stream.
+// hdr[IA[i]+u] = (M position of inv(U_pp), pairs, CRS-local slot of (i,p));
+// pairs are (M position of U_pj, CRS-local slot of (i,j)).
+template <typename TA, typename TM>
+__global__ void k_mc_factor(const int *__restrict__ patches, int npatch, int n, int maxrow, int maxstage,
+                            const int *__restrict__ IA, const int *__restrict__ slot, const int4 *__restrict__ meta,
+                            const int4 *__restrict__ hdr,
+                            const int64_t *__restrict__ pair_ptr, const int2 *__restrict__ pairs,
+                            const TA *__restrict__ A, TM *__restrict__ M, int *__restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int nwarp = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // per-warp region (a multiple of 16 bytes): headers first, so they stay
+    // 16-byte aligned, then the FP64 blocks, then the integer lists
+    unsigned char *reg = smraw + (size_t)wid * mc_factor_warp_bytes(maxrow, maxstage);
+    int4 *hd = reinterpret_cast<int4 *>(reg);                                     // [maxrow]
+    double *w = reinterpret_cast<double *>(reg + (size_t)maxrow * sizeof(int4));  // [maxrow][25] row blocks
+    double *stg = w + (size_t)maxrow * 25;                            // [maxstage][25] staged factor blocks
+    int *pm = reinterpret_cast<int *>(stg + (size_t)maxstage * 25);  // [maxstage] CRS-local slot of each pair
+    int *src = pm + maxstage;                                         // [maxstage] M position of staged blocks
+    int *sl = src + maxstage;                                         // [maxrow] CRS-local slot of list entry u
+    const int pidx = blockIdx.x * nwarp + wid;
+    if (pidx >= npatch) return;  // whole warp; no CTA barrier follows
+    const int P = patches[pidx];
+    const int p0 = P * kMcRows, nr = min(kMcRows, n - p0);
+    const int a = lane / 5, b = lane - 5 * (lane / 5);
+    {
+        for (int q = 0; q < nr; q++) {
+            const int i = p0 + q;
+            const int4 mt = meta[i];
+            const int base = IA[i], len = IA[i + 1] - base, nlo = mt.y;
+            const int64_t pp = pair_ptr[i];
+            const int npair = (int)(pair_ptr[i + 1] - pp);
+            for (int e = lane; e < nlo; e += 32) {
+                const int4 h = hdr[base + e];
+                hd[e] = h;
+                src[e] = h.x;
+            }
+            for (int e = lane; e < npair; e += 32) {
+                const int2 pr = pairs[pp + e];
+                pm[e] = pr.y;
+                src[nlo + e] = pr.x;
+            }
+            for (int e = lane; e < len; e += 32) sl[e] = slot[base + e] - base;
+            // one block per lane, its 25 loads in flight together
+            for (int t = lane; t < len; t += 32) {
+                const TA *ab = A + (int64_t)(base + t) * 25;
+#pragma unroll
+                for (int k = 0; k < 25; k++) w[t * 25 + k] = ld<TA>(ab + k);
+            }
+            __syncwarp();
+            const int nst = nlo + npair;
+            for (int t = lane; t < nst; t += 32) {
+                const TM *mb = M + (int64_t)src[t] * 25;
+#pragma unroll
+                for (int k = 0; k < 25; k++) stg[t * 25 + k] = ld<TM>(mb + k);
+            }
+            __syncwarp();
+            int t0 = 0;
+            for (int u = 0; u < nlo; u++) {
+                const int4 h = hd[u];
+                const int tk = h.z;
+                // L_ip = A_ip inv(U_pp)
+                double Lab = 0.0;
+                if (lane < 25) {
+#pragma unroll
+                    for (int c = 0; c < 5; c++) Lab = fma(w[tk * 25 + a * 5 + c], stg[u * 25 + c * 5 + b], Lab);
+                }
+                __syncwarp();
+                if (lane < 25) w[tk * 25 + lane] = Lab;
+                __syncwarp();
+                // A_ij -= L_ip U_pj, the pairs' 25 entries spread over the lanes
+                for (int e = lane; e < h.y * 25; e += 32) {
+                    const int t = e / 25, ab = e - 25 * t, ea = ab / 5, eb = ab - 5 * ea;
+                    const int mj = pm[t0 + t];
+                    const double *U = stg + (size_t)(nlo + t0 + t) * 25;
+                    double s = w[mj * 25 + ab];
+#pragma unroll
+                    for (int c = 0; c < 5; c++) s = fma(-w[tk * 25 + ea * 5 + c], U[c * 5 + eb], s);
+                    w[mj * 25 + ab] = s;
+                }
+                __syncwarp();
+                t0 += h.y;
+            }
+            const int td = sl[nlo];  // the diagonal follows the lower entries
+            {
+                double av = lane < 25 ? w[td * 25 + lane] : 0.0, iv;
+                const bool ok = warp_inverse5(av, iv, lane);
+                if (!ok && lane == 0) atomicOr(err, ERR_NAN);
+                __syncwarp();
+                if (lane < 25) w[td * 25 + lane] = iv;
+            }
+            __syncwarp();
+            for (int e = lane; e < len * 25; e += 32) {
+                const int u = e / 25;
+                st<TM>(M + (int64_t)base * 25 + e, w[sl[u] * 25 + (e - 25 * u)]);
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Blocks of a row inside its own patch staged in shared memory before the
+// level loop of a triangular solve (more go through the load path).
+template <typename TM>
+struct IntraCap {
+    static constexpr int K = sizeof(TM) == 8 ? 3 : 6;
+};
+
+// Forward solve y = L^-1 r over the patches of one colour: five threads per
+// row (thread m forms component m).  Lower blocks in other patches belong to
+// earlier colours (complete in y) and are summed first; the row's blocks
+// inside the patch are staged in shared memory before the level loop, which
+// then only waits on shared memory.  Factors are in factorisation order
+// (entry u of row i at M[(IA[i] + u) * 25]); scol holds their columns.
+template <typename TM>
+__global__ void __launch_bounds__(5 * kMcRows, 3) k_mc_fwd(const int *__restrict__ patches, int n,
+                                                          const int *__restrict__ IA, const int *__restrict__ scol,
+                                                          const int4 *__restrict__ meta,
+                                                          const int2 *__restrict__ plev, const TM *__restrict__ M,
+                                                          const double *__restrict__ r, double *__restrict__ y) {
+    constexpr int K = IntraCap<TM>::K;
+    constexpr int T = 5 * kMcRows;
+    __shared__ double ys[T];
+    __shared__ TM pa[K * 5][T];  // [t*5+c][thread]
+    __shared__ unsigned char pj[K][T];
+    const int P = patches[blockIdx.x];
+    const int p0 = P * kMcRows, nr = min(kMcRows, n - p0);
+    const int tid = threadIdx.x;
+    const int q = tid / 5, m = tid - 5 * q;
+    const bool act = q < nr;
+    const int i = p0 + q;
+    double s = 0.0;
+    int lev = -1, ui = 0, ue = 0;
+    if (act) {
+        const int4 mt = meta[i];
+        const int base = IA[i];
+        lev = mt.w & 0xffff;
+        ui = base + mt.x;
+        ue = base + mt.y;
+#pragma unroll
+        for (int t = 0; t < K; t++)
+            if (ui + t < ue) {
+                pj[t][tid] = (unsigned char)(scol[ui + t] - p0);
+                const TM *am = M + (int64_t)(ui + t) * 25 + m * 5;
+#pragma unroll
+                for (int c = 0; c < 5; c++) pa[t * 5 + c][tid] = am[c];
+            }
+        s = r[(int64_t)i * 5 + m];
+#pragma unroll 4
+        for (int u = base; u < ui; u++) {
+            const TM *am = M + (int64_t)u * 25 + m * 5;
+            const double *yv = y + (int64_t)scol[u] * 5;
+#pragma unroll
+            for (int c = 0; c < 5; c++) s = fma(-ld<TM>(am + c), yv[c], s);
+        }
+    }
+    const int last = plev[P].x;
+    for (int l = 0; l <= last; l++) {
+        if (act && lev == l) {
+#pragma unroll
+            for (int t = 0; t < K; t++)
+                if (ui + t < ue) {
+                    const double *yv = ys + pj[t][tid] * 5;
+#pragma unroll
+                    for (int c = 0; c < 5; c++) s = fma(-(double)pa[t * 5 + c][tid], yv[c], s);
+                }
+            for (int u = ui + K; u < ue; u++) {
+                const TM *am = M + (int64_t)u * 25 + m * 5;
+                const double *yv = ys + (scol[u] - p0) * 5;
+#pragma unroll
+                for (int c = 0; c < 5; c++) s = fma(-ld<TM>(am + c), yv[c], s);
+            }
+            ys[tid] = s;
+        }
+        __syncthreads();
+    }
+    if (act) y[(int64_t)i * 5 + m] = s;
+}
+
+// Backward solve z = U^-1 y over the patches of one colour (colours in
+// decreasing order): upper blocks in other patches belong to later colours.
+template <typename TM>
+__global__ void __launch_bounds__(5 * kMcRows, 3) k_mc_bwd(const int *__restrict__ patches, int n,
+                                                          const int *__restrict__ IA, const int *__restrict__ scol,
+                                                          const int4 *__restrict__ meta,
+                                                          const int2 *__restrict__ plev, const TM *__restrict__ M,
+                                                          const double *__restrict__ y, double *__restrict__ z) {
+    constexpr int K = IntraCap<TM>::K;
+    constexpr int T = 5 * kMcRows;
+    __shared__ double zs[T], ts[T];
+    __shared__ TM pa[K * 5][T];
+    __shared__ unsigned char pj[K][T];
+    const int P = patches[blockIdx.x];
+    const int p0 = P * kMcRows, nr = min(kMcRows, n - p0);
+    const int tid = threadIdx.x;
+    const int q = tid / 5, m = tid - 5 * q;
+    const bool act = q < nr;
+    const int i = p0 + q;
+    double s = 0.0;
+    int lev = -1, u0 = 0, u1 = 0;
+    TM dg[5];
+    if (act) {
+        const int4 mt = meta[i];
+        const int base = IA[i];
+        lev = mt.w >> 16;
+        u0 = base + mt.y + 1;  // first upper entry
+        u1 = u0 + mt.z;        // first upper entry outside the patch
+        const int end = IA[i + 1];
+#pragma unroll
+        for (int t = 0; t < K; t++)
+            if (u0 + t < u1) {
+                pj[t][tid] = (unsigned char)(scol[u0 + t] - p0);
+                const TM *am = M + (int64_t)(u0 + t) * 25 + m * 5;
+#pragma unroll
+                for (int c = 0; c < 5; c++) pa[t * 5 + c][tid] = am[c];
+            }
+        const TM *d = M + (int64_t)(u0 - 1) * 25 + m * 5;
+#pragma unroll
+        for (int c = 0; c < 5; c++) dg[c] = d[c];
+        s = y[(int64_t)i * 5 + m];
+#pragma unroll 4
+        for (int u = u1; u < end; u++) {
+            const TM *am = M + (int64_t)u * 25 + m * 5;
+            const double *zv = z + (int64_t)scol[u] * 5;
+#pragma unroll
+            for (int c = 0; c < 5; c++) s = fma(-ld<TM>(am + c), zv[c], s);
+        }
+    }
+    const int last = plev[P].y;
+    for (int l = 0; l <= last; l++) {
+        const bool mine = act && lev == l;
+        if (mine) {
+#pragma unroll
+            for (int t = 0; t < K; t++)
+                if (u0 + t < u1) {
+                    const double *zv = zs + pj[t][tid] * 5;
+#pragma unroll
+                    for (int c = 0; c < 5; c++) s = fma(-(double)pa[t * 5 + c][tid], zv[c], s);
+                }
+            for (int u = u0 + K; u < u1; u++) {
+                const TM *am = M + (int64_t)u * 25 + m * 5;
+                const double *zv = zs + (scol[u] - p0) * 5;
+#pragma unroll
+                for (int c = 0; c < 5; c++) s = fma(-ld<TM>(am + c), zv[c], s);
+            }
+            ts[tid] = s;
+        }
+        __syncthreads();
+        if (mine) {
+            double o = 0.0;
+#pragma unroll
+            for (int c = 0; c < 5; c++) o = fma((double)dg[c], ts[q * 5 + c], o);
+            zs[tid] = o;
+        }
+        __syncthreads();
+    }
+    if (act) z[(int64_t)i * 5 + m] = zs[tid];
+}
+
+}  // namespace
+
+// Ordering, slot lists, patch-local levels and the factorisation's update
+// lists (host, once per mesh).
+int mc_build(cfd_ctx *c) {
+    Abmc &mc = c->mc;
+    if (mc.built) return CFD_OK;
+    const int n = c->nnode;
+    const std::vector<int> &IA = c->h_IA, &JA = c->h_JA, &IAU = c->h_IAU;
+    const int np = (n + kMcRows - 1) / kMcRows;
+    // greedy colouring of the patch graph in patch order
+    std::vector<int> color(np, -1), stamp;
+    int ncolor = 0;
+    for (int P = 0; P < np; P++) {
+        const int r0 = P * kMcRows, r1 = std::min(n, r0 + kMcRows);
+        for (int i = r0; i < r1; i++)
+            for (int k = IA[i]; k < IA[i + 1]; k++) {
+                const int Q = JA[k] / kMcRows;
+                if (Q != P && color[Q] >= 0) {
+                    if ((int)stamp.size() <= color[Q]) stamp.resize(color[Q] + 1, -1);
+                    stamp[color[Q]] = P;
+                }
+            }
+        int col = 0;
+        while (col < (int)stamp.size() && stamp[col] == P) col++;
+        color[P] = col;
+        ncolor = std::max(ncolor, col + 1);
+    }
+    mc.ncolor = ncolor;
+    mc.h_pcolor = color;
+    mc.cptr.assign(ncolor + 1, 0);
+    for (int P = 0; P < np; P++) mc.cptr[color[P] + 1]++;
+    for (int k = 0; k < ncolor; k++) mc.cptr[k + 1] += mc.cptr[k];
+    std::vector<int> patches(np), fill(mc.cptr.begin(), mc.cptr.end() - 1);
+    for (int P = 0; P < np; P++) patches[fill[color[P]]++] = P;
+    // position key of a row in the factorisation order
+    auto key = [&](int j) { return (int64_t)color[j / kMcRows] * n + j; };
+    std::vector<int> slot(c->nnzb), scol(c->nnzb);
+    std::vector<int4> meta(n);
+    std::vector<int> lf(n, 0), lb(n, 0);
+    std::vector<std::pair<int64_t, int>> lo, up;
+    int maxrow = 0;
+    for (int i = 0; i < n; i++) {
+        lo.clear();
+        up.clear();
+        const int64_t ki = key(i);
+        const int Pi = i / kMcRows;
+        int next = 0, nint = 0;
+        for (int k = IA[i]; k < IA[i + 1]; k++) {
+            if (k == IAU[i]) continue;
+            const int64_t kj = key(JA[k]);
+            if (kj < ki) lo.push_back({kj, k});
+            else up.push_back({kj, k});
+        }
+        std::sort(lo.begin(), lo.end());
+        std::sort(up.begin(), up.end());
+        int w = IA[i];
+        for (auto &e : lo) {
+            slot[w++] = e.second;
+            if (JA[e.second] / kMcRows != Pi) next++;
+        }
+        slot[w++] = IAU[i];
+        for (auto &e : up) {
+            slot[w++] = e.second;
+            if (JA[e.second] / kMcRows == Pi) nint++;
+        }
+        // external lower blocks come first in key order (smaller colours),
+        // intra-patch upper blocks first among the upper ones
+        meta[i] = make_int4(next, (int)lo.size(), nint, 0);
+        maxrow = std::max(maxrow, IA[i + 1] - IA[i]);
+    }
+    for (int64_t u = 0; u < c->nnzb; u++) scol[u] = JA[slot[u]];
+    // patch-local dependency levels
+    std::vector<int2> plev(np, make_int2(0, 0));
+    int maxlev = 0;
+    for (int P = 0; P < np; P++) {
+        const int r0 = P * kMcRows, r1 = std::min(n, r0 + kMcRows);
+        for (int i = r0; i < r1; i++) {
+            int l = 0;
+            for (int u = IA[i] + meta[i].x; u < IA[i] + meta[i].y; u++) l = std::max(l, lf[scol[u]] + 1);
+            lf[i] = l;
+            plev[P].x = std::max(plev[P].x, l);
+        }
+        for (int i = r1 - 1; i >= r0; i--) {
+            int l = 0;
+            const int u0 = IA[i] + meta[i].y + 1;
+            for (int u = u0; u < u0 + meta[i].z; u++) l = std::max(l, lb[scol[u]] + 1);
+            lb[i] = l;
+            plev[P].y = std::max(plev[P].y, l);
+        }
+        maxlev = std::max(maxlev, std::max(plev[P].x, plev[P].y));
+    }
+    for (int i = 0; i < n; i++) meta[i].w = lf[i] | (lb[i] << 16);
+    // update lists of the factorisation: for lower block (i,p), the upper
+    // blocks (p,j) of row p whose column j row i also holds
+    std::vector<int4> hdr(c->nnzb, make_int4(0, 0, 0, 0));
+    std::vector<int64_t> pair_ptr(n + 1, 0);
+    std::vector<int2> pairs;
+    pairs.reserve((size_t)c->nnzb * 2);
+    std::vector<int> where(n, -1);  // local slot of column j in the current row
+    int maxstage = 1;
+    for (int i = 0; i < n; i++) {
+        const int base = IA[i];
+        for (int k = base; k < IA[i + 1]; k++) where[JA[k]] = k - base;
+        const int nlo = meta[i].y;
+        for (int u = 0; u < nlo; u++) {
+            const int kk = slot[base + u], p = JA[kk];
+            int cnt = 0;
+            for (int v = IA[p] + meta[p].y + 1; v < IA[p + 1]; v++) {
+                const int j = scol[v];
+                if (where[j] >= 0) {
+                    pairs.push_back(make_int2(v, where[j]));
+                    cnt++;
+                }
+            }
+            hdr[base + u] = make_int4(IA[p] + meta[p].y, cnt, kk - base, 0);
+        }
+        pair_ptr[i + 1] = (int64_t)pairs.size();
+        maxstage = std::max<int64_t>(maxstage, nlo + (pair_ptr[i + 1] - pair_ptr[i]));
+        for (int k = base; k < IA[i + 1]; k++) where[JA[k]] = -1;
+    }
+    mc.maxrow = maxrow;
+    mc.maxlev = maxlev;
+    mc.maxstage = maxstage;
+    CFD_CUDA(mc.patches.upload(patches.data(), patches.size(), c->stream));
+    CFD_CUDA(mc.slot.upload(slot.data(), slot.size(), c->stream));
+    CFD_CUDA(mc.scol.upload(scol.data(), scol.size(), c->stream));
+    CFD_CUDA(mc.meta.upload(meta.data(), meta.size(), c->stream));
+    CFD_CUDA(mc.plev.upload(plev.data(), plev.size(), c->stream));
+    CFD_CUDA(mc.hdr.upload(hdr.data(), hdr.size(), c->stream));
+    CFD_CUDA(mc.pair_ptr.upload(pair_ptr.data(), pair_ptr.size(), c->stream));
+    CFD_CUDA(mc.pairs.upload(pairs.data(), pairs.size(), c->stream));
+    CFD_CUDA(cudaStreamSynchronize(c->stream));  // host vectors go out of scope
+    mc.built = true;
+    return CFD_OK;
+}
+
+template <typename TA, typename TM>
+int mc_factor(cfd_ctx *c, const TA *A, TM *M) {
+    Abmc &mc = c->mc;
+    int st = mc_build(c);
+    if (st) return st;
+    // warps (patches) per CTA: as many as fit 200 KB of staged blocks (at most 16)
+    const size_t per_warp = mc_factor_warp_bytes(mc.maxrow, mc.maxstage);
+    const int nwarp = (int)std::max<size_t>(1, std::min<size_t>(16, (200u << 10) / per_warp));
+    if (per_warp > (200u << 10)) {
+        set_error("ILU(0) multicolour: a row needs %d staged blocks, more than fit in shared memory",
+                  mc.maxrow + mc.maxstage);
+        return CFD_ERR_RANGE;
+    }
+    const size_t smem = per_warp * nwarp;
+    CFD_CUDA(cudaFuncSetAttribute(k_mc_factor<TA, TM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    for (int k = 0; k < mc.ncolor; k++) {
+        const int cnt = mc.cptr[k + 1] - mc.cptr[k];
+        k_mc_factor<TA, TM><<<grid_for(cnt, nwarp), 32 * nwarp, smem, c->stream>>>(
+            mc.patches.p + mc.cptr[k], cnt, c->nnode, mc.maxrow, mc.maxstage, c->IA.p, mc.slot.p, mc.meta.p,
+            mc.hdr.p, mc.pair_ptr.p, mc.pairs.p, A, M, c->err.p);
+    }
+    CFD_LAUNCH_CHECK();
+    return CFD_OK;
+}
+
+template <typename TM>
+int mc_apply(cfd_ctx *c, const TM *M, const double *r, double *tmp, double *z) {
+    Abmc &mc = c->mc;
+    for (int k = 0; k < mc.ncolor; k++) {
+        const int cnt = mc.cptr[k + 1] - mc.cptr[k];
+        k_mc_fwd<TM><<<cnt, 5 * kMcRows, 0, c->stream>>>(mc.patches.p + mc.cptr[k], c->nnode, c->IA.p, mc.scol.p,
+                                                           mc.meta.p, mc.plev.p, M, r, tmp);
+    }
+    for (int k = mc.ncolor - 1; k >= 0; k--) {
+        const int cnt = mc.cptr[k + 1] - mc.cptr[k];
+        k_mc_bwd<TM><<<cnt, 5 * kMcRows, 0, c->stream>>>(mc.patches.p + mc.cptr[k], c->nnode, c->IA.p, mc.scol.p,
+                                                           mc.meta.p, mc.plev.p, M, tmp, z);
+    }
+    CFD_LAUNCH_CHECK();
+    return CFD_OK;
+}
+
+template int mc_factor<double, double>(cfd_ctx *, const double *, double *);
+template int mc_factor<double, float>(cfd_ctx *, const double *, float *);
+template int mc_factor<float, float>(cfd_ctx *, const float *, float *);
+template int mc_factor<uint16_t, float>(cfd_ctx *, const uint16_t *, float *);
+template int mc_apply<double>(cfd_ctx *, const double *, const double *, double *, double *);
+template int mc_apply<float>(cfd_ctx *, const float *, const double *, double *, double *);
+
+}  // namespace cfd
+
+using namespace cfd;
+
+extern "C" int cfd_ilu_mc_order(cfd_ctx *c, int *order, int *ncolor) {
+    if (!c || !c->has_mesh) { cfd::set_error("cfd_ilu_mc_order: no mesh"); return CFD_ERR_STATE; }
+    CFD_CUDA(cudaSetDevice(c->device));
+    int st = mc_build(c);
+    if (st) return st;
+    const Abmc &mc = c->mc;
+    if (ncolor) *ncolor = mc.ncolor;
+    if (order) {
+        const int n = c->nnode;
+        int k = 0;
+        for (int col = 0; col < mc.ncolor; col++)
+            for (int P = 0; P * kMcRows < n; P++)
+                if (mc.h_pcolor[P] == col)
+                    for (int i = P * kMcRows; i < std::min(n, (P + 1) * kMcRows); i++) order[k++] = i;
+    }
+    return CFD_OK;
+}

@@ -20,6 +20,7 @@
 
 #include "ctx.cuh"
 #include "kernels.cuh"
+#include "ilu_mc.cuh"
 
 namespace cfd {
 
@@ -75,39 +76,56 @@ __device__ __forceinline__ void two_sum(double a, double b, double &s, double &e
 }
 
 // Dot2 of k vectors V[j] (stride ld) against w, one (sum, compensation)
-// pair per vector per block.
+// pair per vector per block.  Vectors are taken MD_CHUNK at a time so w is
+// read once per chunk; per vector the summation order (thread-strided loop,
+// then the block tree) does not depend on the chunking.
 constexpr int MAXK = 64;
+constexpr int MD_CHUNK = 8;
 __global__ void __launch_bounds__(256) k_mdot_partial(const double *__restrict__ V, int64_t ld, int k,
                                                       const double *__restrict__ w, int64_t n,
                                                       double *__restrict__ part) {
-    __shared__ double shs[256], shc[256];
-    for (int j = 0; j < k; j++) {
-        const double *v = V + (int64_t)j * ld;
-        double s = 0.0, c = 0.0;
+    __shared__ double shs[MD_CHUNK][256], shc[MD_CHUNK][256];
+    for (int j0 = 0; j0 < k; j0 += MD_CHUNK) {
+        const int nj = min(MD_CHUNK, k - j0);
+        double s[MD_CHUNK], c[MD_CHUNK];
+#pragma unroll
+        for (int jj = 0; jj < MD_CHUNK; jj++) { s[jj] = 0.0; c[jj] = 0.0; }
         for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-            const double a = v[i], b = w[i];
-            const double p = a * b;
-            const double pe = fma(a, b, -p);
-            double t, e;
-            two_sum(s, p, t, e);
-            s = t;
-            c += e + pe;
+            const double b = w[i];
+#pragma unroll
+            for (int jj = 0; jj < MD_CHUNK; jj++)
+                if (jj < nj) {
+                    const double a = V[(int64_t)(j0 + jj) * ld + i];
+                    const double p = a * b;
+                    const double pe = fma(a, b, -p);
+                    double t, e;
+                    two_sum(s[jj], p, t, e);
+                    s[jj] = t;
+                    c[jj] += e + pe;
+                }
         }
-        shs[threadIdx.x] = s;
-        shc[threadIdx.x] = c;
+#pragma unroll
+        for (int jj = 0; jj < MD_CHUNK; jj++) {
+            shs[jj][threadIdx.x] = s[jj];
+            shc[jj][threadIdx.x] = c[jj];
+        }
         __syncthreads();
         for (int o = blockDim.x >> 1; o > 0; o >>= 1) {
             if (threadIdx.x < o) {
-                double t, e;
-                two_sum(shs[threadIdx.x], shs[threadIdx.x + o], t, e);
-                shs[threadIdx.x] = t;
-                shc[threadIdx.x] += shc[threadIdx.x + o] + e;
+#pragma unroll
+                for (int jj = 0; jj < MD_CHUNK; jj++) {
+                    double t, e;
+                    two_sum(shs[jj][threadIdx.x], shs[jj][threadIdx.x + o], t, e);
+                    shs[jj][threadIdx.x] = t;
+                    shc[jj][threadIdx.x] += shc[jj][threadIdx.x + o] + e;
+                }
             }
             __syncthreads();
         }
-        if (threadIdx.x == 0) {
-            part[(blockIdx.x * MAXK + j) * 2] = shs[0];
-            part[(blockIdx.x * MAXK + j) * 2 + 1] = shc[0];
+        if (threadIdx.x < nj) {
+            const int jj = threadIdx.x;
+            part[(blockIdx.x * MAXK + j0 + jj) * 2] = shs[jj][0];
+            part[(blockIdx.x * MAXK + j0 + jj) * 2 + 1] = shc[jj][0];
         }
         __syncthreads();
     }
@@ -305,14 +323,19 @@ __global__ void __launch_bounds__(64) k_ilu0_level(int nrows, const int *__restr
         const int p = JA[k];
         double *Lip = F + (int64_t)k * 25;
         const double *Dp = F + (int64_t)IAU[p] * 25;  // inverse of U_pp
-        double L[25];
+        // blocks are staged in registers: F is read and written through the
+        // same pointer, so direct use would serialise every load behind the
+        // previous store
+        double a_ip[25], d_p[25], L[25];
+#pragma unroll
+        for (int q = 0; q < 25; q++) { a_ip[q] = Lip[q]; d_p[q] = Dp[q]; }
 #pragma unroll
         for (int a = 0; a < 5; a++)
 #pragma unroll
             for (int b = 0; b < 5; b++) {
                 double s = 0.0;
 #pragma unroll
-                for (int q = 0; q < 5; q++) s = fma(Lip[a * 5 + q], Dp[q * 5 + b], s);
+                for (int q = 0; q < 5; q++) s = fma(a_ip[a * 5 + q], d_p[q * 5 + b], s);
                 L[a * 5 + b] = s;
             }
 #pragma unroll
@@ -327,15 +350,20 @@ __global__ void __launch_bounds__(64) k_ilu0_level(int nrows, const int *__restr
             if (jp < jm) { pk++; continue; }
             double *Aij = F + (int64_t)m * 25;
             const double *Upj = F + (int64_t)pk * 25;
+            double u[25], t[25];
+#pragma unroll
+            for (int q = 0; q < 25; q++) { u[q] = Upj[q]; t[q] = Aij[q]; }
 #pragma unroll
             for (int a = 0; a < 5; a++)
 #pragma unroll
                 for (int b = 0; b < 5; b++) {
-                    double s = Aij[a * 5 + b];
+                    double s = t[a * 5 + b];
 #pragma unroll
-                    for (int q = 0; q < 5; q++) s = fma(-L[a * 5 + q], Upj[q * 5 + b], s);
-                    Aij[a * 5 + b] = s;
+                    for (int q = 0; q < 5; q++) s = fma(-L[a * 5 + q], u[q * 5 + b], s);
+                    t[a * 5 + b] = s;
                 }
+#pragma unroll
+            for (int q = 0; q < 25; q++) Aij[q] = t[q];
             m++;
             pk++;
         }
@@ -419,6 +447,10 @@ struct Precond {
 static int precond_setup(cfd_ctx *c, const Precond &pc) {
     const int n = c->nnode;
     if (pc.kind == CFD_PC_NONE) return CFD_OK;
+    if (!c->a64_valid && pc.kind != CFD_PC_ILU0_MC) {
+        set_error("gmres: with a low-precision-only system the preconditioner must be CFD_PC_ILU0_MC or none");
+        return CFD_ERR_STATE;
+    }
     if (pc.kind == CFD_PC_BLOCK_JACOBI) {
         if (pc.prec == CFD_PREC_FP64) {
             CFD_CUDA(c->M64.alloc((size_t)n * 25));
@@ -430,8 +462,26 @@ static int precond_setup(cfd_ctx *c, const Precond &pc) {
         CFD_LAUNCH_CHECK();
         return check_device_error(c);
     }
-    // ILU(0): factor in FP64 in M64, then cast when FP32 storage is wanted
     const size_t nz = (size_t)c->nnzb * 25;
+    if (pc.kind == CFD_PC_ILU0_MC) {
+        // block multicolour order: factors read straight from the stored
+        // matrix (its own precision), FP64 arithmetic, stored in pc.prec
+        if (pc.prec == CFD_PREC_FP64) {
+            CFD_CUDA(c->M64.alloc(nz));
+            int st = mc_factor<double, double>(c, c->A64.p, c->M64.p);
+            if (st) return st;
+        } else {
+            CFD_CUDA(c->M32.alloc(nz));
+            int st;
+            if (c->a_precision == CFD_PREC_FP32 && c->A32.p) st = mc_factor<float, float>(c, c->A32.p, c->M32.p);
+            else if (c->a_precision == CFD_PREC_BF16 && c->A16.p)
+                st = mc_factor<uint16_t, float>(c, c->A16.p, c->M32.p);
+            else st = mc_factor<double, float>(c, c->A64.p, c->M32.p);
+            if (st) return st;
+        }
+        return check_device_error(c);
+    }
+    // ILU(0): factor in FP64 in M64, then cast when FP32 storage is wanted
     CFD_CUDA(c->M64.alloc(nz));
     CFD_CUDA(cudaMemcpyAsync(c->M64.p, c->A64.p, nz * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     Levels &L = c->lv_fwd;
@@ -478,6 +528,12 @@ static int precond_apply(cfd_ctx *c, const Precond &pc, const double *r, double 
             else
                 k_bjacobi_apply<float><<<grid_for(len, 160), 160, 0, c->stream>>>(n, c->M32.p, r, z);
             break;
+        case CFD_PC_ILU0_MC: {
+            const int st = pc.prec == CFD_PREC_FP64 ? mc_apply<double>(c, c->M64.p, r, tmp, z)
+                                                    : mc_apply<float>(c, c->M32.p, r, tmp, z);
+            if (st) return st;
+            break;
+        }
         default:
             if (pc.prec == CFD_PREC_FP64) ilu_apply<double>(c, c->M64.p, r, tmp, z);
             else ilu_apply<float>(c, c->M32.p, r, tmp, z);
@@ -490,6 +546,7 @@ static int precond_apply(cfd_ctx *c, const Precond &pc, const double *r, double 
 static void spmv(cfd_ctx *c, int prec, const double *x, double *y) {
     const int n = c->nnode;
     const int g = grid_for(5 * (int64_t)n, 160);
+    if (prec == CFD_PREC_FP64 && !c->a64_valid) prec = c->a_precision;  // low-precision-only system
     if (prec == CFD_PREC_FP32 && c->A32.p)
         k_bspmv<float><<<g, 160, 0, c->stream>>>(n, c->IA.p, c->JA.p, c->A32.p, x, y);
     else if (prec == CFD_PREC_BF16 && c->A16.p)
@@ -620,7 +677,9 @@ int cfd_gmres(cfd_ctx *c, const cfd_gmres_opts *o, cfd_gmres_stats *stats) {
         set_error("cfd_gmres: restart must be in [1,%d], max_iters >= 1, rtol > 0", MAXK / 2 - 1);
         return CFD_ERR_ARG;
     }
-    if (opt.precond < CFD_PC_NONE || opt.precond > CFD_PC_ILU0) return CFD_ERR_ARG;
+    if (opt.precond < CFD_PC_NONE || opt.precond > CFD_PC_ILU0_MC) return CFD_ERR_ARG;
+    opt.precision &= ~CFD_PREC_LOW_ONLY;  // the matrix storage is decided by cfd_jacobian
+    if (opt.precision < CFD_PREC_FP64 || opt.precision > CFD_PREC_BF16) return CFD_ERR_ARG;
     CFD_CUDA(cudaSetDevice(c->device));
     const int64_t n5 = (int64_t)c->nnode * 5;
     const int m = opt.restart;
@@ -630,9 +689,10 @@ int cfd_gmres(cfd_ctx *c, const cfd_gmres_opts *o, cfd_gmres_stats *stats) {
     int aprec = opt.precision;
     if (aprec == CFD_PREC_FP32 && c->a_precision != CFD_PREC_FP32) aprec = CFD_PREC_FP64;
     if (aprec == CFD_PREC_BF16 && c->a_precision != CFD_PREC_BF16) aprec = CFD_PREC_FP64;
+    if (!c->a64_valid) aprec = c->a_precision;  // only the low-precision matrix exists
     Precond pc;
     pc.kind = opt.precond;
-    pc.prec = opt.precision == CFD_PREC_FP64 ? CFD_PREC_FP64 : CFD_PREC_FP32;
+    pc.prec = (opt.precision == CFD_PREC_FP64 && c->a64_valid) ? CFD_PREC_FP64 : CFD_PREC_FP32;
     int st = precond_setup(c, pc);
     if (st) return st;
     double *x = c->X.p;

@@ -74,10 +74,15 @@ extern "C" {
 #define CFD_PREC_FP64 0  /* Jacobian / preconditioner storage precision */
 #define CFD_PREC_FP32 1
 #define CFD_PREC_BF16 2
+#define CFD_PREC_LOW_ONLY 0x10  /* or'ed with FP32/BF16 in cfd_jacobian / the GMRES precision: keep only the
+                                   low-precision matrix (no FP64 copy); the outer FP64 correction is then the
+                                   caller's nonlinear defect, and GMRES works with the stored matrix */
 
 #define CFD_PC_NONE      0  /* GMRES right preconditioner */
 #define CFD_PC_BLOCK_JACOBI 1
-#define CFD_PC_ILU0      2
+#define CFD_PC_ILU0      2  /* ILU(0) in the mesh (row) order, level-scheduled */
+#define CFD_PC_ILU0_MC   3  /* ILU(0) in block multicolour order: 64-row patches, patch graph coloured
+                               greedily, one launch per colour in factorisation and solves */
 
 /* Solver options; mirrors the reference parameter file keys named beside
  * each field (Euler3D/src/SolverParameters.cpp:184-700). */
@@ -185,7 +190,11 @@ int  cfd_residual_rms(cfd_ctx *ctx, int include_diss, double out[6]);
  * (Compute_Jacobian, Euler3D/src/Jacobian.cpp:18 ->
  * Roe_Jacobian.cpp:29-228).  B = -(Res + include_diss*Res_Diss);
  * diagonal += V/dt when add_time.  precision: CFD_PREC_FP64/FP32/BF16 storage
- * of A (the FP64 copy is always kept for the defect correction). */
+ * of A; the FP64 copy is kept for the linear defect correction unless
+ * CFD_PREC_LOW_ONLY is or'ed in, in which case the diagonal blocks are summed
+ * (in FP64) from the stored low-precision off-diagonal blocks and only the
+ * low-precision matrix exists (cfd_block_gs and the mesh-order ILU(0) /
+ * block-Jacobi preconditioners then need a new FP64 Jacobian). */
 int  cfd_jacobian(cfd_ctx *ctx, int add_time, int include_diss, int precision);
 
 /* Block Gauss-Seidel with LU-factored diagonal blocks, X = 0 start
@@ -218,6 +227,11 @@ void cfd_gmres_default(cfd_gmres_opts *o);
  * MATH/src/ParallelLinearAlgebra.cpp:27-278, is unused); this is the solver
  * the implicit drivers call in its place. */
 int  cfd_gmres(cfd_ctx *ctx, const cfd_gmres_opts *o, cfd_gmres_stats *st);
+
+/* Factorisation order of CFD_PC_ILU0_MC: order[k] = row at position k
+ * (nnode entries; colours in increasing order, rows of a colour in increasing
+ * index) and the number of colours.  Either pointer may be NULL. */
+int  cfd_ilu_mc_order(cfd_ctx *ctx, int *order, int *ncolor);
 
 /* Block Gauss-Seidel that allocates no device memory.  No counterpart in the
  * reference: it exists for callers that cannot let a library call cudaMalloc
