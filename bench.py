@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--cpu-procs", type=int, default=0, help="reference processes (0 = one per core, max 16)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--side-rcm", action="store_true", help="also time the plain node-level RCM numbering")
+    ap.add_argument("--no-steady", action="store_true", help="skip the time-to-steady-state solves")
     ap.add_argument("--profile", action="store_true",
                     help="profiling case for ncu: two residual steps per kernel variant, no timing, no output line")
     return ap.parse_args()
@@ -156,6 +157,88 @@ def reference_throughput(sample_n, procs, warmup, steps):
               f"single-threaded reference processes")
     return sum(rates), dict(per_pass_s=statistics.mean(per_pass), procs=procs, sample=sample,
                             per_process_gedges=statistics.mean(rates))
+
+
+STEADY = dict(CFG, cfl_min=10.0, cfl_max=1000.0, cfl_ramp=20)
+STEADY_DROP = 1e-8
+STEADY_RTOL = 0.1  # inner GMRES tolerance of each implicit iteration
+
+
+def steady_config(n):
+    return {"workload": f"implicit steady solve to a {STEADY_DROP:g} L2 residual drop, {n}^3-hex tet cube, "
+                        "second-order Roe residual (Green-Gauss + Venkatakrishnan K=5), approximate first-order Roe "
+                        "Jacobian, CFL 10->1000 over 20 iterations, B = -(Res + Res_Diss)",
+            "linear": f"GMRES(30), inner rtol {STEADY_RTOL}, ILU(0) in block multicolour order (32-row patches)",
+            "mixed": "fp32/bf16: Jacobian and ILU(0) stored in FP32 (BF16 Jacobian), FP64 residual, Arnoldi with "
+                     "compensated FP64 dots, FP64 nonlinear update; no FP64 copy of the Jacobian"}
+
+
+def steady_solves(mesh, Q, dev, stream, timed_once):
+    """Time to the steady residual drop, plain FP64 and mixed precision, on the
+    bench mesh; the converged mixed-precision states are compared with FP64."""
+    from cfdsolutions_b200 import Euler3DGPU, capi, default_params
+
+    out, states = {}, {}
+    for name, prec in (("fp64", capi.PREC_FP64), ("fp32", capi.PREC_FP32 | capi.PREC_LOW_ONLY),
+                       ("bf16", capi.PREC_BF16 | capi.PREC_LOW_ONLY)):
+        with Euler3DGPU(mesh, default_params(**STEADY), device=dev, stream=stream.cuda_stream) as ss:
+            ss.set_state(Q)
+            capi.check(capi.lib.cfd_ilu_mc_order(ss.handle, None, None), "cfd_ilu_mc_order")  # mesh setup
+            g = capi.GmresOpts(30, 30, STEADY_RTOL, capi.PC_ILU0_MC, prec, 1)
+            box = {}
+
+            def run():
+                box["st"] = ss.solve_steady(max_iterations=800, drop=STEADY_DROP, include_diss=1, linear_solver=1,
+                                            gmres=g)
+
+            ms = timed_once(run)
+            st = box["st"]
+            out[name] = {"seconds": ms / 1e3, "newton_iterations": st.iterations,
+                         "gmres_iterations": st.linear_iterations, "rms_drop": st.rms_last / st.rms_first,
+                         "converged": bool(st.rms_last <= STEADY_DROP * st.rms_first)}
+            # untimed: continue at the final CFL to a 1e-11 drop, so the
+            # precisions are compared at convergence, not at the stopping point
+            ss.set_params(default_params(**dict(STEADY, cfl_min=STEADY["cfl_max"], cfl_ramp=0)))
+            st2 = ss.solve_steady(max_iterations=400, drop=1e-11 * st.rms_first / max(st.rms_last, 1e-300),
+                                  include_diss=1, linear_solver=1, gmres=g)
+            out[name]["rms_drop_compared"] = st2.rms_last / st.rms_first
+            states[name] = ss.get_state()[:, :mesh.nnode]
+    ref = states["fp64"]
+    mom = float(np.abs(ref[1:4]).max())
+    for name in ("fp32", "bf16"):
+        err = 0.0
+        for v in range(5):
+            scale = max(float(np.abs(ref[v]).max()), mom if 1 <= v <= 3 else 0.0)
+            err = max(err, float(np.abs(states[name][v] - ref[v]).max()) / scale)
+        out[name]["max_rel_err_vs_fp64"] = err  # converged fields (1e-11 drop), per-field scale
+        out[name]["speedup_vs_fp64"] = out["fp64"]["seconds"] / out[name]["seconds"]
+    return out
+
+
+def reference_implicit_rate(sample_n, procs, iters):
+    """The reference's own implicit iteration (second-order residual, Jacobian,
+    10 block Gauss-Seidel sweeps, update) on a sample_n^3 cube, one
+    single-threaded process per core; returns node-iterations per second."""
+    from cfdsolutions_b200 import box_mesh, perturbed_freestream
+    from oracle import refharness
+
+    m = box_mesh(sample_n, jitter=0.15, seed=1234, rcm=True)
+    Q = perturbed_freestream(m, CFG["gamma"], CFG["mach"], CFG["alpha_deg"], noise=0.01, seed=1235)
+    cfg = dict(STEADY, gradient=0)
+    one = [("begin", 0), ("gradient", 0), ("limiter",), ("bc", 0), ("residual", 1), ("deltat", 0),
+           ("jacobian", 1, 0), ("gs", 10, 0), ("update", 1.0)]
+    outs = refharness.run_many(m, cfg, Q, one * (iters + 1), procs)
+    per_it = []
+    for o in outs:
+        t = o["timings"]
+        tot = [sum(x) for x in zip(*(t[k] for k in ("begin", "gradient", "limiter", "bc", "residual", "deltat",
+                                                     "jacobian", "gs", "update")))]
+        per_it.append(statistics.mean(tot[1:]))
+    rate = sum(m.nnode / x for x in per_it)
+    sample = (f"{sample_n}^3-hex tet cube ({m.nnode} nodes), 1+{iters} implicit iterations of the reference "
+              f"(LSQ gradient, Venkatakrishnan, Roe residual, dt, approximate Roe Jacobian, 10 block Gauss-Seidel "
+              f"sweeps, update) per process, {procs} concurrent single-threaded processes")
+    return rate, statistics.mean(per_it), sample
 
 
 def cpu_count():
@@ -309,11 +392,11 @@ def main():
                                     "ms_per_step": msf / args.steps}
     s.set_params(default_params(**CFG))
 
-    # ---- the same step on the plain node-level RCM numbering, and on the node-gather kernel
+    # ---- the same step with the shared-memory patch kernel, and on the plain node-level RCM numbering
     side = {}
     s.set_params(default_params(**dict(CFG, residual_kernel=1)))
     msg = timed(lambda i: s.residual_step(i), args.steps, args.warmup)
-    side["gather_kernel_gedges_per_s"] = units * args.steps / (msg / 1e3) / 1e9
+    side["patch_kernel_gedges_per_s"] = units * args.steps / (msg / 1e3) / 1e9
     s.set_params(default_params(**CFG))
     if args.side_rcm:
         m2 = box_mesh(args.n, jitter=0.15, seed=1234, rcm=NUMBERING_RCM)
@@ -348,6 +431,37 @@ def main():
                    "sample": "reference oracle library not built"}
 
     s.close()
+
+    # ---- time to the steady residual drop (plain FP64 and mixed precision)
+    steady = None
+    if not args.no_steady:
+        def timed_once(fn):
+            barrier()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            fn()
+            ev1.record(stream)
+            barrier()
+            ms = ev0.elapsed_time(ev1)
+            if world > 1:
+                t = torch.tensor([ms], device=f"cuda:{dev}")
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                ms = float(t.item())
+            return ms
+
+        steady = {"metric": "time to steady residual drop", "unit": "s", "higher_is_better": False,
+                  "config": steady_config(args.n)}
+        steady.update(steady_solves(mesh, Q, dev, stream, timed_once))
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            from oracle import refharness
+            if refharness.available():
+                procs = args.cpu_procs or min(16, cpu_count())
+                rate, per_it, sample = reference_implicit_rate(32, procs, 2)
+                gpu_rate = mesh.nnode * steady["fp64"]["newton_iterations"] / steady["fp64"]["seconds"]
+                steady["cpu_baseline"] = {"value": rate, "unit": "node-iterations/s", "cores": procs,
+                                          "kind": "reference", "sample": sample, "seconds_per_iteration": per_it,
+                                          "gpu_fp64_value": gpu_rate}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -355,7 +469,7 @@ def main():
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded tet-split cube, seeded +-1% state noise)",
             "config": workload_config(args.n, mesh), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": KERNELS_PER_STEP * args.steps, "clocks": clocks, "per_flux": per_flux,
-            "breakdown_ms": breakdown, "variants": side, "setup_s": setup_s,
+            "breakdown_ms": breakdown, "variants": side, "setup_s": setup_s, "steady": steady,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

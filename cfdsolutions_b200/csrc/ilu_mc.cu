@@ -4,7 +4,7 @@
 // level in the factorisation and in each triangular solve; on a banded
 // (RCM-like) numbering of an n^3 mesh that is O(n) levels of a few thousand
 // rows each, so the solves are bound by launch latency, not by HBM.  Here the
-// rows are grouped in patches of kMcRows (64) consecutive rows and the
+// rows are grouped in patches of kMcRows (32) consecutive rows and the
 // patch graph (two patches adjacent when a matrix block couples them) is
 // coloured greedily.  The factorisation order is: colours in increasing
 // order, rows of a colour in increasing index.  Two patches of one colour are
@@ -33,7 +33,7 @@ namespace cfd {
 namespace {
 
 // Rows per patch of the ordering (five solve threads per row).
-constexpr int kMcRows = 64;
+constexpr int kMcRows = 32;
 
 template <typename T>
 __device__ __forceinline__ double ld(const T *p);
@@ -92,10 +92,12 @@ __device__ __forceinline__ bool warp_inverse5(double &a, double &v, int lane) {
     return ok;
 }
 
-// Shared-memory bytes of one warp of k_mc_factor, rounded up to 16.
+// Shared-memory bytes of one warp of k_mc_factor (factor blocks staged in
+// their storage type TM), rounded up to 16.
+template <typename TM>
 __host__ __device__ inline size_t mc_factor_warp_bytes(int maxrow, int maxstage) {
-    const size_t b = (size_t)maxrow * sizeof(int4) + (size_t)(maxrow + maxstage) * 25 * sizeof(double) +
-                     (size_t)(2 * maxstage + maxrow) * sizeof(int);
+    const size_t b = (size_t)maxrow * sizeof(int4) + (size_t)maxrow * 25 * sizeof(double) +
+                     (size_t)maxstage * 25 * sizeof(TM) + (size_t)(2 * maxstage + maxrow) * sizeof(int);
     return (b + 15) & ~(size_t)15;
 }
 
@@ -123,10 +125,10 @@ __global__ void k_mc_factor(const int *__restrict__ patches, int npatch, int n, 
     const int nwarp = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // per-warp region (a multiple of 16 bytes): headers first, so they stay
     // 16-byte aligned, then the FP64 blocks, then the integer lists
-    unsigned char *reg = smraw + (size_t)wid * mc_factor_warp_bytes(maxrow, maxstage);
+    unsigned char *reg = smraw + (size_t)wid * mc_factor_warp_bytes<TM>(maxrow, maxstage);
     int4 *hd = reinterpret_cast<int4 *>(reg);                                     // [maxrow]
     double *w = reinterpret_cast<double *>(reg + (size_t)maxrow * sizeof(int4));  // [maxrow][25] row blocks
-    double *stg = w + (size_t)maxrow * 25;                            // [maxstage][25] staged factor blocks
+    TM *stg = reinterpret_cast<TM *>(w + (size_t)maxrow * 25);       // [maxstage][25] staged factor blocks
     int *pm = reinterpret_cast<int *>(stg + (size_t)maxstage * 25);  // [maxstage] CRS-local slot of each pair
     int *src = pm + maxstage;                                         // [maxstage] M position of staged blocks
     int *sl = src + maxstage;                                         // [maxrow] CRS-local slot of list entry u
@@ -164,7 +166,7 @@ __global__ void k_mc_factor(const int *__restrict__ patches, int npatch, int n, 
             for (int t = lane; t < nst; t += 32) {
                 const TM *mb = M + (int64_t)src[t] * 25;
 #pragma unroll
-                for (int k = 0; k < 25; k++) stg[t * 25 + k] = ld<TM>(mb + k);
+                for (int k = 0; k < 25; k++) stg[t * 25 + k] = mb[k];
             }
             __syncwarp();
             int t0 = 0;
@@ -175,7 +177,7 @@ __global__ void k_mc_factor(const int *__restrict__ patches, int npatch, int n, 
                 double Lab = 0.0;
                 if (lane < 25) {
 #pragma unroll
-                    for (int c = 0; c < 5; c++) Lab = fma(w[tk * 25 + a * 5 + c], stg[u * 25 + c * 5 + b], Lab);
+                    for (int c = 0; c < 5; c++) Lab = fma(w[tk * 25 + a * 5 + c], (double)stg[u * 25 + c * 5 + b], Lab);
                 }
                 __syncwarp();
                 if (lane < 25) w[tk * 25 + lane] = Lab;
@@ -184,10 +186,10 @@ __global__ void k_mc_factor(const int *__restrict__ patches, int npatch, int n, 
                 for (int e = lane; e < h.y * 25; e += 32) {
                     const int t = e / 25, ab = e - 25 * t, ea = ab / 5, eb = ab - 5 * ea;
                     const int mj = pm[t0 + t];
-                    const double *U = stg + (size_t)(nlo + t0 + t) * 25;
+                    const TM *U = stg + (size_t)(nlo + t0 + t) * 25;
                     double s = w[mj * 25 + ab];
 #pragma unroll
-                    for (int c = 0; c < 5; c++) s = fma(-w[tk * 25 + ea * 5 + c], U[c * 5 + eb], s);
+                    for (int c = 0; c < 5; c++) s = fma(-w[tk * 25 + ea * 5 + c], (double)U[c * 5 + eb], s);
                     w[mj * 25 + ab] = s;
                 }
                 __syncwarp();
@@ -225,7 +227,7 @@ struct IntraCap {
 // then only waits on shared memory.  Factors are in factorisation order
 // (entry u of row i at M[(IA[i] + u) * 25]); scol holds their columns.
 template <typename TM>
-__global__ void __launch_bounds__(5 * kMcRows, 3) k_mc_fwd(const int *__restrict__ patches, int n,
+__global__ void __launch_bounds__(5 * kMcRows, 6) k_mc_fwd(const int *__restrict__ patches, int n,
                                                           const int *__restrict__ IA, const int *__restrict__ scol,
                                                           const int4 *__restrict__ meta,
                                                           const int2 *__restrict__ plev, const TM *__restrict__ M,
@@ -292,7 +294,7 @@ __global__ void __launch_bounds__(5 * kMcRows, 3) k_mc_fwd(const int *__restrict
 // Backward solve z = U^-1 y over the patches of one colour (colours in
 // decreasing order): upper blocks in other patches belong to later colours.
 template <typename TM>
-__global__ void __launch_bounds__(5 * kMcRows, 3) k_mc_bwd(const int *__restrict__ patches, int n,
+__global__ void __launch_bounds__(5 * kMcRows, 6) k_mc_bwd(const int *__restrict__ patches, int n,
                                                           const int *__restrict__ IA, const int *__restrict__ scol,
                                                           const int4 *__restrict__ meta,
                                                           const int2 *__restrict__ plev, const TM *__restrict__ M,
@@ -511,9 +513,10 @@ int mc_factor(cfd_ctx *c, const TA *A, TM *M) {
     Abmc &mc = c->mc;
     int st = mc_build(c);
     if (st) return st;
-    // warps (patches) per CTA: as many as fit 200 KB of staged blocks (at most 16)
-    const size_t per_warp = mc_factor_warp_bytes(mc.maxrow, mc.maxstage);
-    const int nwarp = (int)std::max<size_t>(1, std::min<size_t>(16, (200u << 10) / per_warp));
+    // four warps (patches) per CTA, fewer when their staging does not fit in
+    // 200 KB; several CTAs share an SM so every SM gets patches
+    const size_t per_warp = mc_factor_warp_bytes<TM>(mc.maxrow, mc.maxstage);
+    const int nwarp = (int)std::max<size_t>(1, std::min<size_t>(4, (200u << 10) / per_warp));
     if (per_warp > (200u << 10)) {
         set_error("ILU(0) multicolour: a row needs %d staged blocks, more than fit in shared memory",
                   mc.maxrow + mc.maxstage);

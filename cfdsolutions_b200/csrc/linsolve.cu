@@ -77,14 +77,19 @@ __device__ __forceinline__ void two_sum(double a, double b, double &s, double &e
 
 // Dot2 of k vectors V[j] (stride ld) against w, one (sum, compensation)
 // pair per vector per block.  Vectors are taken MD_CHUNK at a time so w is
-// read once per chunk; per vector the summation order (thread-strided loop,
-// then the block tree) does not depend on the chunking.
+// read once per chunk.  Per vector: thread-strided compensated sums, then a
+// warp butterfly and a combine over the block's warps (error-free TwoSum is
+// symmetric in its arguments, so every lane of the butterfly holds the same
+// pair); the order depends only on the grid, so results repeat run to run.
 constexpr int MAXK = 64;
 constexpr int MD_CHUNK = 8;
-__global__ void __launch_bounds__(256) k_mdot_partial(const double *__restrict__ V, int64_t ld, int k,
-                                                      const double *__restrict__ w, int64_t n,
-                                                      double *__restrict__ part) {
-    __shared__ double shs[MD_CHUNK][256], shc[MD_CHUNK][256];
+constexpr int MD_THREADS = 256;
+__global__ void __launch_bounds__(MD_THREADS) k_mdot_partial(const double *__restrict__ V, int64_t ld, int k,
+                                                             const double *__restrict__ w, int64_t n,
+                                                             double *__restrict__ part) {
+    constexpr int NW = MD_THREADS / 32;
+    __shared__ double shs[MD_CHUNK][NW], shc[MD_CHUNK][NW];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int j0 = 0; j0 < k; j0 += MD_CHUNK) {
         const int nj = min(MD_CHUNK, k - j0);
         double s[MD_CHUNK], c[MD_CHUNK];
@@ -106,26 +111,28 @@ __global__ void __launch_bounds__(256) k_mdot_partial(const double *__restrict__
         }
 #pragma unroll
         for (int jj = 0; jj < MD_CHUNK; jj++) {
-            shs[jj][threadIdx.x] = s[jj];
-            shc[jj][threadIdx.x] = c[jj];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double so = __shfl_xor_sync(0xffffffffu, s[jj], o);
+                const double co = __shfl_xor_sync(0xffffffffu, c[jj], o);
+                double t, e;
+                two_sum(s[jj], so, t, e);
+                s[jj] = t;
+                c[jj] = (c[jj] + co) + e;
+            }
+            if (lane == 0) { shs[jj][wid] = s[jj]; shc[jj][wid] = c[jj]; }
         }
         __syncthreads();
-        for (int o = blockDim.x >> 1; o > 0; o >>= 1) {
-            if (threadIdx.x < o) {
-#pragma unroll
-                for (int jj = 0; jj < MD_CHUNK; jj++) {
-                    double t, e;
-                    two_sum(shs[jj][threadIdx.x], shs[jj][threadIdx.x + o], t, e);
-                    shs[jj][threadIdx.x] = t;
-                    shc[jj][threadIdx.x] += shc[jj][threadIdx.x + o] + e;
-                }
+        if (wid == 0 && lane < nj) {
+            double ss = shs[lane][0], cc = shc[lane][0];
+            for (int q = 1; q < NW; q++) {
+                double t, e;
+                two_sum(ss, shs[lane][q], t, e);
+                ss = t;
+                cc = (cc + shc[lane][q]) + e;
             }
-            __syncthreads();
-        }
-        if (threadIdx.x < nj) {
-            const int jj = threadIdx.x;
-            part[(blockIdx.x * MAXK + j0 + jj) * 2] = shs[jj][0];
-            part[(blockIdx.x * MAXK + j0 + jj) * 2 + 1] = shc[jj][0];
+            part[(blockIdx.x * MAXK + j0 + lane) * 2] = ss;
+            part[(blockIdx.x * MAXK + j0 + lane) * 2 + 1] = cc;
         }
         __syncthreads();
     }
@@ -157,13 +164,13 @@ __global__ void k_mdot_final(const double *__restrict__ part, int nblk, int k, d
     if (threadIdx.x == 0) out[j] = shs[0] + shc[0];
 }
 
-static const int kRedBlocks = 296;  // 2 x 148 SMs
+static const int kRedBlocks = 1184;  // 8 x 148 SMs
 
 // out_host[j] = <V_j, w>, j < k, compensated, deterministic.
 static int mdot(cfd_ctx *c, const double *V, int64_t ld, int k, const double *w, int64_t n, double *out_host) {
     CFD_CUDA(c->red.alloc(std::max<size_t>(c->red.n, (size_t)kRedBlocks * 128)));
     CFD_CUDA(c->dots.alloc(std::max<size_t>(c->dots.n, (size_t)MAXK)));
-    k_mdot_partial<<<kRedBlocks, 256, 0, c->stream>>>(V, ld, k, w, n, c->red.p);
+    k_mdot_partial<<<kRedBlocks, MD_THREADS, 0, c->stream>>>(V, ld, k, w, n, c->red.p);
     CFD_LAUNCH_CHECK();
     k_mdot_final<<<k, 256, 0, c->stream>>>(c->red.p, kRedBlocks, k, c->dots.p);
     CFD_LAUNCH_CHECK();

@@ -81,7 +81,7 @@ extern "C" {
 #define CFD_PC_NONE      0  /* GMRES right preconditioner */
 #define CFD_PC_BLOCK_JACOBI 1
 #define CFD_PC_ILU0      2  /* ILU(0) in the mesh (row) order, level-scheduled */
-#define CFD_PC_ILU0_MC   3  /* ILU(0) in block multicolour order: 64-row patches, patch graph coloured
+#define CFD_PC_ILU0_MC   3  /* ILU(0) in block multicolour order: 32-row patches, patch graph coloured
                                greedily, one launch per colour in factorisation and solves */
 
 /* Solver options; mirrors the reference parameter file keys named beside
