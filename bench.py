@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--side-rcm", action="store_true", help="also time the plain node-level RCM numbering")
     ap.add_argument("--no-steady", action="store_true", help="skip the time-to-steady-state solves")
+    ap.add_argument("--profile-linear", action="store_true",
+                    help="small linear-solve case for ncu captures (Jacobian + one GMRES(30) call per precision)")
     ap.add_argument("--profile", action="store_true",
                     help="profiling case for ncu: two residual steps per kernel variant, no timing, no output line")
     return ap.parse_args()
@@ -281,6 +283,25 @@ def profile_case(n):
             s.synchronize()
 
 
+def profile_linear_case(n):
+    """Small fixed case for ncu captures of the linear solver
+    (`--profile-linear --n 64`): the steady workload's Jacobian at CFL 1000 on
+    an n^3 cube, then GMRES(30) with the block multicolour ILU(0): once with
+    the FP64 system, once with the FP32 low-precision-only system."""
+    from cfdsolutions_b200 import Euler3DGPU, box_mesh, capi, default_params, perturbed_freestream
+    from cfdsolutions_b200.mesh import NUMBERING_PATCH_RCM
+
+    m = box_mesh(n, jitter=0.15, seed=1234, rcm=NUMBERING_PATCH_RCM)
+    Q = perturbed_freestream(m, CFG["gamma"], CFG["mach"], CFG["alpha_deg"], noise=0.01, seed=1235)
+    with Euler3DGPU(m, default_params(**dict(STEADY, cfl_min=1000.0))) as s:
+        s.set_state(Q)
+        s.residual_step(0)
+        for prec in (capi.PREC_FP64, capi.PREC_FP32 | capi.PREC_LOW_ONLY):
+            s.Compute_Jacobian(1, 0, 1, prec)
+            s.solve_gmres(30, 30, 1e-12, capi.PC_ILU0_MC, prec, 1, allow_not_converged=True)
+        s.synchronize()
+
+
 def workload_config(n, mesh=None):
     c = {"workload": f"second-order residual evaluation, {n}^3-hex tet cube (6 tets/hex), RCM, jitter 0.15h, "
                      "Green-Gauss + Venkatakrishnan K=5 + Roe, M=0.8, alpha=1.25, +-1% noise",
@@ -303,6 +324,9 @@ def main():
         return
     if args.profile:
         profile_case(args.n)
+        return
+    if args.profile_linear:
+        profile_linear_case(args.n)
         return
 
     import torch
