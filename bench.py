@@ -51,6 +51,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--side-rcm", action="store_true", help="also time the plain node-level RCM numbering")
     ap.add_argument("--no-steady", action="store_true", help="skip the time-to-steady-state solves")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served batch")
+    ap.add_argument("--serve-requests", type=int, default=32)
+    ap.add_argument("--serve-nmax", type=int, default=64, help="largest cube side of the served mix (config: 96)")
+    ap.add_argument("--serve-rate", type=float, default=2.0, help="Poisson arrival rate, requests per second")
+    ap.add_argument("--serve-workers", type=int, default=8)
     ap.add_argument("--profile-linear", action="store_true",
                     help="small linear-solve case for ncu captures (Jacobian + one GMRES(30) call per precision)")
     ap.add_argument("--profile", action="store_true",
@@ -241,6 +246,49 @@ def reference_implicit_rate(sample_n, procs, iters):
               f"(LSQ gradient, Venkatakrishnan, Roe residual, dt, approximate Roe Jacobian, 10 block Gauss-Seidel "
               f"sweeps, update) per process, {procs} concurrent single-threaded processes")
     return rate, statistics.mean(per_it), sample
+
+
+def serve_requests(count, nmax, rate, seed=7):
+    """Seeded request mix of the served batch: cube side log-uniform in
+    [16, nmax] hexes, Mach U[0.3, 0.85], alpha U[-5, 10] deg, Poisson arrivals
+    at `rate` per second (arrival offsets in seconds)."""
+    rng = np.random.default_rng(seed)
+    ns = np.round(np.exp(rng.uniform(np.log(16), np.log(nmax), count))).astype(int)
+    machs = rng.uniform(0.3, 0.85, count)
+    alphas = rng.uniform(-5.0, 10.0, count)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
+    return ns, machs, alphas, arrivals - arrivals[0]
+
+
+def serve_run(ns, machs, alphas, arrivals, workers, precision, dev):
+    """Submits the requests at their arrival times to a server with `workers`
+    concurrent solves (all at once when arrivals is None) and waits for all;
+    returns the results and the wall time from the first submission."""
+    from cfdsolutions_b200 import capi, default_params
+    from cfdsolutions_b200.serve import Server, request, steady_opts
+
+    reqs = []
+    for k, (n, m, a) in enumerate(zip(ns, machs, alphas)):
+        p = default_params(**dict(STEADY, mach=float(m), mach_min=float(m), alpha_deg=float(a)))
+        reqs.append(request(int(n), p, steady_opts(drop=STEADY_DROP, rtol=STEADY_RTOL, precision=precision),
+                            mesh_seed=1000 + k, state_seed=2000 + k))
+    with Server(device=dev, workers=workers, budget_bytes=150e9) as srv:
+        t0 = time.perf_counter()
+        if arrivals is None:  # sequential: one request at a time
+            res = []
+            for r in reqs:
+                res.append(srv.wait(srv.submit(r)))
+        else:
+            ids = []
+            for k, r in enumerate(reqs):
+                dt = arrivals[k] - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                ids.append(srv.submit(r))
+            res = [srv.wait(i) for i in ids]
+        wall = time.perf_counter() - t0
+        peak = srv.stats()["peak_reserved_bytes"]
+    return res, wall, peak
 
 
 def cpu_count():
@@ -486,6 +534,34 @@ def main():
                                           "kind": "reference", "sample": sample, "seconds_per_iteration": per_it,
                                           "gpu_fp64_value": gpu_rate}
 
+    # ---- served batch (continuous admission) vs sequential plain FP64 solves
+    serve = None
+    if not args.no_serve:
+        from cfdsolutions_b200 import capi
+        ns, machs, alphas, arr = serve_requests(args.serve_requests, args.serve_nmax, args.serve_rate)
+        barrier()
+        res, wall, peak = serve_run(ns, machs, alphas, arr, args.serve_workers,
+                                    capi.PREC_FP32 | capi.PREC_LOW_ONLY, dev)
+        barrier()
+        seq, seq_wall, _ = serve_run(ns, machs, alphas, None, 1, capi.PREC_FP64, dev)
+        lat = np.array([r.latency for r in res])
+        ok = sum(r.status == 0 and r.rms_last <= STEADY_DROP * r.rms_first for r in res)
+        ok_seq = sum(r.status == 0 and r.rms_last <= STEADY_DROP * r.rms_first for r in seq)
+        serve = {
+            "metric": "served steady solves", "unit": "solves/s",
+            "config": {"requests": args.serve_requests, "cube_side": f"log-uniform in [16, {args.serve_nmax}] hexes",
+                       "mach": "U[0.3, 0.85]", "alpha_deg": "U[-5, 10]", "arrivals": f"Poisson, {args.serve_rate}/s",
+                       "workers": args.serve_workers, "budget_gb": 150.0, "physics": "as steady",
+                       "served_precision": "fp32 low-precision-only Jacobian + ILU(0)",
+                       "sequential": "plain fp64 solves one at a time through the same server (1 worker)"},
+            "value": len(res) / wall * world, "p50_s": float(np.percentile(lat, 50)),
+            "p99_s": float(np.percentile(lat, 99)), "converged": ok, "wall_s": wall,
+            "peak_reserved_gb": peak / 1e9,
+            "sequential_fp64": {"value": len(seq) / seq_wall * world, "wall_s": seq_wall, "converged": ok_seq,
+                                "p50_solve_s": float(np.percentile([r.t_done - r.t_admit for r in seq], 50))},
+        }
+        serve["speedup_vs_sequential_fp64"] = serve["value"] / serve["sequential_fp64"]["value"]
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -493,7 +569,7 @@ def main():
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded tet-split cube, seeded +-1% state noise)",
             "config": workload_config(args.n, mesh), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": KERNELS_PER_STEP * args.steps, "clocks": clocks, "per_flux": per_flux,
-            "breakdown_ms": breakdown, "variants": side, "setup_s": setup_s, "steady": steady,
+            "breakdown_ms": breakdown, "variants": side, "setup_s": setup_s, "steady": steady, "serve": serve,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -27,6 +27,7 @@ PC_NONE, PC_BLOCK_JACOBI, PC_ILU0, PC_ILU0_MC = 0, 1, 2, 3
 PREC_LOW_ONLY = 0x10
 BC_EULER_WALL, BC_FAR_FIELD, BC_INFLOW, BC_OUTFLOW = 0, 1, 2, 3
 GS_STATIC_MAX_ROWS = 16384
+PENDING = 1
 
 
 class CfdError(RuntimeError):
@@ -65,6 +66,19 @@ class SolveOpts(C.Structure):
 class SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("rms_first", C.c_double), ("rms_last", C.c_double),
                 ("linear_iterations", C.c_int), ("status", C.c_int)]
+
+
+class ServeRequest(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("lx", C.c_double), ("ly", C.c_double),
+                ("lz", C.c_double), ("jitter", C.c_double), ("mesh_seed", C.c_uint64), ("numbering", C.c_int),
+                ("face_bc", C.c_int * 6), ("noise", C.c_double), ("state_seed", C.c_uint64), ("params", Params),
+                ("opts", SolveOpts), ("keep_state", C.c_int)]
+
+
+class ServeResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("stats", SolveStats), ("nnode", C.c_int), ("nghost", C.c_int),
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_start_solve", C.c_double),
+                ("t_done", C.c_double), ("bytes_estimate", C.c_double), ("message", C.c_char * 160)]
 
 
 P = C.c_void_p
@@ -123,6 +137,14 @@ SIGNATURES = {
     "cfd_mesh_write_ugrid": (I, [P, C.c_char_p]),
     "cfd_set_mesh_from": (I, [P, P]),
     "cfd_mesh_free": (None, [P]),
+    "cfd_perturbed_freestream": (I, [P, D, D, D, D, D, C.c_uint64, P]),
+    "cfd_server_create": (I, [I, I, D, C.POINTER(P)]),
+    "cfd_server_submit": (I, [P, C.POINTER(ServeRequest), C.POINTER(I64)]),
+    "cfd_server_wait": (I, [P, I64, D, C.POINTER(ServeResult)]),
+    "cfd_server_state": (I, [P, I64, P]),
+    "cfd_server_release": (I, [P, I64]),
+    "cfd_server_stats": (I, [P, P]),
+    "cfd_server_destroy": (I, [P]),
     "cfd_restart_write": (I, [C.c_char_p, I, I, I, P]),
     "cfd_restart_read": (I, [C.c_char_p, C.POINTER(I), I, I, P]),
 }

@@ -20,7 +20,7 @@ OUT_DIR = PKG / "_lib"
 LIB = OUT_DIR / "libcfd_b200.so"
 OBJ_DIR = PKG / "_build"
 
-CU_SOURCES = ["core.cu", "gradient.cu", "linsolve.cu", "ilu_mc.cu", "gs_static.cu"]
+CU_SOURCES = ["core.cu", "gradient.cu", "linsolve.cu", "ilu_mc.cu", "gs_static.cu", "serve.cu"]
 CXX_SOURCES = ["mesh.cpp"]
 HEADERS = ["cfd_internal.h", "ctx.cuh", "kernels.cuh", "physics.cuh", "ilu_mc.cuh"]
 

@@ -755,9 +755,14 @@ template <int FLUX, bool SECOND>
 static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, const int *gate) {
     if (patch_kernel(c)) {
         const size_t smem = patch_smem_bytes(c->patch_nlocmax, SECOND);
-        if (smem > 48 * 1024)
-            CFD_CUDA(cudaFuncSetAttribute(k_residual_patch<FLUX, SECOND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem));
+        if (smem > 48 * 1024) {
+            int smax = 0;
+            CFD_CUDA(allow_max_dynamic_smem(k_residual_patch<FLUX, SECOND>, c->device, &smax));
+            if (smem > (size_t)smax) {
+                set_error("residual patch kernel: %zu bytes of shared memory needed, %d available", smem, smax);
+                return CFD_ERR_RANGE;
+            }
+        }
         k_residual_patch<FLUX, SECOND><<<c->npatch, PATCH_CHUNK, smem, c->stream>>>(
             c->nnode, c->ldq, c->Q.p, c->grad.p, c->phi.p, c->xyz.p, c->pe_ptr.p, c->pe_loc.p, c->pe_geo.p,
             c->ph_ptr.p, c->halo.p, c->inc_ptr.p, c->inc.p, c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p,
@@ -865,13 +870,15 @@ int cfd_create(int device, cfd_ctx **out) {
     CFD_CUDA(cudaSetDevice(device));
     cfd_ctx *c = new cfd_ctx();
     c->device = device;
+    if (g_alloc_async) c->stream = g_alloc_stream;  // serving worker: its own stream from the start
     cfd_params_default(&c->params);
     if (c->err.alloc(1) != cudaSuccess || c->ext.alloc(8) != cudaSuccess) {
         delete c;
         set_error("cfd_create: device allocation failed");
         return CFD_ERR_CUDA;
     }
-    cudaMemset(c->err.p, 0, sizeof(int));
+    if (g_alloc_async) cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream);
+    else cudaMemset(c->err.p, 0, sizeof(int));
     compute_flow(c, 0);
     *out = c;
     return CFD_OK;

@@ -13,6 +13,13 @@
 
 namespace cfd {
 
+// Stream-ordered allocation for the serving workers (serve.cu): while set on
+// the calling thread, DevBuf allocates and frees with cudaMallocAsync /
+// cudaFreeAsync on that stream, so a worker never synchronises the device
+// (cudaFree waits for all streams).  Off (plain cudaMalloc/cudaFree) otherwise.
+inline thread_local bool g_alloc_async = false;
+inline thread_local cudaStream_t g_alloc_stream = nullptr;
+
 template <typename T>
 struct DevBuf {
     T *p = nullptr;
@@ -22,7 +29,10 @@ struct DevBuf {
     DevBuf &operator=(const DevBuf &) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (g_alloc_async) cudaFreeAsync(p, g_alloc_stream);
+            else cudaFree(p);
+        }
         p = nullptr;
         n = 0;
     }
@@ -30,7 +40,8 @@ struct DevBuf {
         if (count == n && p) return cudaSuccess;
         release();
         if (count == 0) return cudaSuccess;
-        cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+        cudaError_t e = g_alloc_async ? cudaMallocAsync((void **)&p, count * sizeof(T), g_alloc_stream)
+                                      : cudaMalloc((void **)&p, count * sizeof(T));
         if (e == cudaSuccess) n = count;
         else p = nullptr;
         return e;
@@ -178,6 +189,19 @@ namespace cfd {
     } while (0)
 
 inline int grid_for(int64_t n, int block) { return (int)((n + block - 1) / block); }
+
+// Raises a kernel's dynamic shared-memory limit to the device's opt-in
+// maximum.  The limit is a process-wide attribute of the kernel: setting it to
+// one fixed value (rather than each context's own need) keeps contexts that
+// launch the kernel from different threads from undoing each other's setting.
+template <typename K>
+inline cudaError_t allow_max_dynamic_smem(K *kernel, int device, int *max_bytes) {
+    int v = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (e != cudaSuccess) return e;
+    if (max_bytes) *max_bytes = v;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+}
 
 // Deterministic reductions (fixed grid -> fixed order): implemented in core.cu.
 int reduce_sum_sq(cfd_ctx *c, const double *x, int64_t n, int64_t stride, int nvec, double *out_host);

@@ -523,7 +523,12 @@ int mc_factor(cfd_ctx *c, const TA *A, TM *M) {
         return CFD_ERR_RANGE;
     }
     const size_t smem = per_warp * nwarp;
-    CFD_CUDA(cudaFuncSetAttribute(k_mc_factor<TA, TM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int smax = 0;
+    CFD_CUDA(allow_max_dynamic_smem(k_mc_factor<TA, TM>, c->device, &smax));
+    if (smem > (size_t)smax) {
+        set_error("ILU(0) multicolour: %zu bytes of shared memory needed, %d available", smem, smax);
+        return CFD_ERR_RANGE;
+    }
     for (int k = 0; k < mc.ncolor; k++) {
         const int cnt = mc.cptr[k + 1] - mc.cptr[k];
         k_mc_factor<TA, TM><<<grid_for(cnt, nwarp), 32 * nwarp, smem, c->stream>>>(

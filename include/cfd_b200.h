@@ -341,6 +341,67 @@ int  cfd_mesh_write_ugrid(const cfd_mesh *m, const char *path);
 int  cfd_set_mesh_from(cfd_ctx *ctx, const cfd_mesh *m);
 void cfd_mesh_free(cfd_mesh *m);
 
+/* Initial state of a request: the generic freestream (rho = 1, p = 1,
+ * c = sqrt(gamma), velocity from mach, alpha, beta) with density, each
+ * velocity component and pressure of every physical node multiplied by
+ * (1 + noise * U(-1,1)), U from a counter-based hash of (seed, variable,
+ * node); ghosts at freestream.  Q is SoA [5][nnode+nghost] (host). */
+int  cfd_perturbed_freestream(const cfd_mesh *m, double gamma, double mach, double alpha_deg, double beta_deg,
+                              double noise, uint64_t seed, double *Q);
+
+/* ------------------------------------------------------------ serving loop
+ * No counterpart in the reference (its drivers run one solve per process).
+ * A server runs steady-solve requests concurrently on one GPU: requests queue
+ * in arrival order; a worker (one host thread and one CUDA stream each) takes
+ * the head request when its device-memory estimate fits in what is left of
+ * the budget, builds its tet-split box mesh on the host, sets the seeded
+ * initial state and runs cfd_solve_steady.  Workers allocate device memory
+ * stream-ordered, so solves of different sizes overlap on the GPU without
+ * device-wide synchronisation.  Results do not depend on the other requests
+ * (all kernels are deterministic). */
+#define CFD_PENDING 1  /* cfd_server_wait: not finished within the timeout */
+
+typedef struct cfd_server cfd_server;
+
+typedef struct cfd_serve_request {
+    int      nx, ny, nz;        /* tet-split box of nx*ny*nz hexes ...        */
+    double   lx, ly, lz;        /* ... over [0,lx]x[0,ly]x[0,lz]               */
+    double   jitter;            /* interior node jitter (fraction of h)       */
+    uint64_t mesh_seed;
+    int      numbering;         /* CFD_NUMBERING_*                           */
+    int      face_bc[6];        /* CFD_BC_* of xmin,xmax,ymin,ymax,zmin,zmax  */
+    double   noise;             /* initial state, see cfd_perturbed_freestream */
+    uint64_t state_seed;
+    cfd_params params;
+    cfd_solve_opts opts;
+    int      keep_state;        /* 1: keep the final state (cfd_server_state) */
+} cfd_serve_request;
+
+typedef struct cfd_serve_result {
+    int    status;              /* CFD_OK, CFD_PENDING, or the failing call's code */
+    cfd_solve_stats stats;
+    int    nnode, nghost;
+    double t_submit, t_admit, t_start_solve, t_done;  /* seconds on the server's clock */
+    double bytes_estimate;      /* device memory reserved against the budget  */
+    char   message[160];        /* error text when status < 0                  */
+} cfd_serve_result;
+
+/* workers: concurrent solves; budget_bytes: device memory the admitted
+ * requests may reserve together (estimates, see DESIGN). */
+int  cfd_server_create(int device, int workers, double budget_bytes, cfd_server **out);
+/* Queues a request; CFD_ERR_RANGE when its estimate exceeds the budget. */
+int  cfd_server_submit(cfd_server *srv, const cfd_serve_request *req, int64_t *id);
+/* Waits up to timeout_s (< 0: forever); CFD_PENDING on timeout. */
+int  cfd_server_wait(cfd_server *srv, int64_t id, double timeout_s, cfd_serve_result *out);
+/* Final state [5][nnode+nghost] of a finished request that kept it. */
+int  cfd_server_state(cfd_server *srv, int64_t id, double *Q);
+/* Forgets a finished request (its result and state). */
+int  cfd_server_release(cfd_server *srv, int64_t id);
+/* {active, queued, reserved bytes, peak reserved bytes, server clock s} */
+int  cfd_server_stats(cfd_server *srv, double out[5]);
+/* Running requests finish; queued ones are dropped. */
+int  cfd_server_destroy(cfd_server *srv);
+
 /* ------------------------------------------------- restart file (binary)
  * Byte-compatible with Restart_Writer / Restart_Reader
  * (Euler3D/src/RestartIO.cpp:45-179): int32 {iteration, nNode, nBNode, 5}

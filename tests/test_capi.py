@@ -101,3 +101,32 @@ def test_mesh_rejects_bad_cells():
     with pytest.raises(capi.CfdError):
         from cfdsolutions_b200 import from_cells
         from_cells(coords, tets, np.zeros((0, 3), np.int32), np.zeros(0, np.int32))
+
+
+def test_perturbed_freestream_matches_the_freestream_without_noise():
+    """cfd_perturbed_freestream (host code, the serving loop's initial state)
+    is the generic freestream at noise 0, and stays within +-noise of it."""
+    import ctypes as C
+
+    from cfdsolutions_b200.mesh import perturbed_freestream
+    from cfdsolutions_b200 import box_mesh
+
+    fb = np.ones(6, np.int32)
+    h = C.c_void_p()
+    capi.check(capi.lib.cfd_mesh_box(4, 4, 4, 1.0, 1.0, 1.0, 0.1, 3, 0, capi.ptr(fb), C.byref(h)), "cfd_mesh_box")
+    try:
+        m = box_mesh(4, jitter=0.1, seed=3)
+        n = m.nnode + m.nghost
+        Q0 = np.empty((5, n))
+        capi.check(capi.lib.cfd_perturbed_freestream(h, 1.4, 0.7, 3.0, 1.0, 0.0, 9, capi.ptr(Q0)), "pf")
+        np.testing.assert_allclose(Q0, perturbed_freestream(m, 1.4, 0.7, 3.0, 1.0, noise=0.0), rtol=1e-15, atol=1e-15)
+        Q1 = np.empty((5, n))
+        capi.check(capi.lib.cfd_perturbed_freestream(h, 1.4, 0.7, 3.0, 1.0, 0.02, 9, capi.ptr(Q1)), "pf")
+        rho = Q1[0, :m.nnode]
+        assert np.all(np.abs(rho - 1.0) <= 0.02) and np.std(rho) > 0.005
+        np.testing.assert_array_equal(Q1[:, m.nnode:], Q0[:, m.nnode:])
+        Q2 = np.empty((5, n))
+        capi.check(capi.lib.cfd_perturbed_freestream(h, 1.4, 0.7, 3.0, 1.0, 0.02, 9, capi.ptr(Q2)), "pf")
+        np.testing.assert_array_equal(Q1, Q2)
+    finally:
+        capi.lib.cfd_mesh_free(h)
