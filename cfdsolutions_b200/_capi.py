@@ -49,7 +49,7 @@ class Params(C.Structure):
 
 class GmresOpts(C.Structure):
     _fields_ = [("restart", C.c_int), ("max_iters", C.c_int), ("rtol", C.c_double), ("precond", C.c_int),
-                ("precision", C.c_int), ("refine", C.c_int)]
+                ("precision", C.c_int), ("refine", C.c_int), ("reuse_precond", C.c_int)]
 
 
 class GmresStats(C.Structure):
@@ -60,7 +60,7 @@ class GmresStats(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("max_iterations", C.c_int), ("drop", C.c_double), ("include_diss", C.c_int),
                 ("linear_solver", C.c_int), ("linear_iters", C.c_int), ("relax", C.c_double),
-                ("gmres", GmresOpts)]
+                ("gmres", GmresOpts), ("precond_update", C.c_int)]
 
 
 class SolveStats(C.Structure):

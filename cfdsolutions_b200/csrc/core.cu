@@ -1205,6 +1205,8 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         CFD_CUDA(c->eslot.upload(es.data(), es.size(), s));
         int e1 = 0, e2 = 0;
         c->mc.built = false;  // block multicolour ILU ordering is rebuilt on first use
+        c->mc.clear_graphs();
+        c->pc_valid = false;
         build_levels(c->h_IA, c->h_JA, nnode, true, c->lv_fwd, s, e1);
         build_levels(c->h_IA, c->h_JA, nnode, false, c->lv_bwd, s, e2);
         if (e1 || e2) { set_error("cfd_set_mesh: level upload failed"); return CFD_ERR_CUDA; }

@@ -78,6 +78,18 @@ struct Abmc {
     DevBuf<int4> hdr;                 // [nnzb] per lower block: slot of inv(U_pp), pairs, local slot
     DevBuf<int64_t> pair_ptr;         // [n+1] update pairs of each row
     DevBuf<int2> pairs;               // (slot of U_pj, local slot of (i,j))
+    // captured applies (one CUDA graph per factor / input / scratch / output
+    // pointer set; the GMRES driver reuses a few such sets)
+    struct Graph {
+        const void *M, *r, *tmp, *z;
+        cudaGraphExec_t exec;
+    };
+    std::vector<Graph> graphs;
+    void clear_graphs() {
+        for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+    }
+    ~Abmc() { clear_graphs(); }
 };
 
 }  // namespace cfd
@@ -163,6 +175,8 @@ struct cfd_ctx {
     cfd::DevBuf<double> dots;   // device dot results
     cfd::DevBuf<int> ilu_diag_inv_done;
     cfd::Abmc mc;               // block multicolour ILU(0) ordering
+    bool pc_valid = false;      // M64/M32 hold factors of kind pc_kind, precision pc_prec
+    int pc_kind = -1, pc_prec = -1;
     int krylov_m = 0;
     bool has_system = false;
     bool has_grad = false;
@@ -199,6 +213,9 @@ inline cudaError_t allow_max_dynamic_smem(K *kernel, int device, int *max_bytes)
     int v = 0;
     cudaError_t e = cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa;
+    if ((e = cudaFuncGetAttributes(&fa, kernel)) != cudaSuccess) return e;
+    v -= (int)fa.sharedSizeBytes;  // the kernel's static shared memory counts against the same limit
     if (max_bytes) *max_bytes = v;
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
 }

@@ -540,7 +540,7 @@ int mc_factor(cfd_ctx *c, const TA *A, TM *M) {
 }
 
 template <typename TM>
-int mc_apply(cfd_ctx *c, const TM *M, const double *r, double *tmp, double *z) {
+static int mc_apply_launch(cfd_ctx *c, const TM *M, const double *r, double *tmp, double *z) {
     Abmc &mc = c->mc;
     for (int k = 0; k < mc.ncolor; k++) {
         const int cnt = mc.cptr[k + 1] - mc.cptr[k];
@@ -553,6 +553,38 @@ int mc_apply(cfd_ctx *c, const TM *M, const double *r, double *tmp, double *z) {
                                                            mc.meta.p, mc.plev.p, M, tmp, z);
     }
     CFD_LAUNCH_CHECK();
+    return CFD_OK;
+}
+
+// The 2 x ncolor launches of an apply, replayed as one captured CUDA graph
+// when the context has its own stream (the legacy stream cannot be
+// captured): the host then issues one launch instead of 2 x ncolor, which is
+// what bounds small systems.  Graphs are cached per pointer set.
+template <typename TM>
+int mc_apply(cfd_ctx *c, const TM *M, const double *r, double *tmp, double *z) {
+    Abmc &mc = c->mc;
+    if (!c->stream) return mc_apply_launch<TM>(c, M, r, tmp, z);
+    for (const auto &g : mc.graphs)
+        if (g.M == M && g.r == r && g.tmp == tmp && g.z == z) {
+            CFD_CUDA(cudaGraphLaunch(g.exec, c->stream));
+            return CFD_OK;
+        }
+    if (mc.graphs.size() >= 64) mc.clear_graphs();
+    cudaGraph_t graph = nullptr;
+    CFD_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int st = mc_apply_launch<TM>(c, M, r, tmp, z);
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    if (st) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    CFD_CUDA(e);
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    CFD_CUDA(ei);
+    mc.graphs.push_back({M, r, tmp, z, exec});
+    CFD_CUDA(cudaGraphLaunch(exec, c->stream));
     return CFD_OK;
 }
 

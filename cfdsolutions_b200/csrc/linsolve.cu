@@ -166,17 +166,48 @@ __global__ void k_mdot_final(const double *__restrict__ part, int nblk, int k, d
 
 static const int kRedBlocks = 1184;  // 8 x 148 SMs
 
-// out_host[j] = <V_j, w>, j < k, compensated, deterministic.
-static int mdot(cfd_ctx *c, const double *V, int64_t ld, int k, const double *w, int64_t n, double *out_host) {
-    CFD_CUDA(c->red.alloc(std::max<size_t>(c->red.n, (size_t)kRedBlocks * 128)));
-    CFD_CUDA(c->dots.alloc(std::max<size_t>(c->dots.n, (size_t)MAXK)));
+// Device scalars of the GMRES driver, in c->dots (doubles):
+//   [0, MAXK)        dot results read back by the host; [MAXK/2, MAXK) also
+//                    holds the host-computed combination coefficients y
+//   [MAXK, 2 MAXK)   first Gram-Schmidt coefficients h1
+//   [2 MAXK, 3 MAXK) re-orthogonalisation coefficients h2
+//   [3 MAXK, 4 MAXK) Hessenberg column h1 + h2 | ||w|| ; last entry 1/||w||
+//   [4 MAXK]         ||w||^2
+constexpr int DOT_H1 = MAXK, DOT_H2 = 2 * MAXK, DOT_COL = 3 * MAXK, DOT_NRM = 4 * MAXK, DOT_LEN = 5 * MAXK;
+
+// out_dev[j] = <V_j, w>, j < k, compensated, deterministic; stays on the device.
+static int mdot_dev(cfd_ctx *c, const double *V, int64_t ld, int k, const double *w, int64_t n, double *out_dev) {
     k_mdot_partial<<<kRedBlocks, MD_THREADS, 0, c->stream>>>(V, ld, k, w, n, c->red.p);
     CFD_LAUNCH_CHECK();
-    k_mdot_final<<<k, 256, 0, c->stream>>>(c->red.p, kRedBlocks, k, c->dots.p);
+    k_mdot_final<<<k, 256, 0, c->stream>>>(c->red.p, kRedBlocks, k, out_dev);
     CFD_LAUNCH_CHECK();
+    return CFD_OK;
+}
+
+static int dot_buffers(cfd_ctx *c) {
+    CFD_CUDA(c->red.alloc(std::max<size_t>(c->red.n, (size_t)kRedBlocks * 128)));
+    CFD_CUDA(c->dots.alloc(std::max<size_t>(c->dots.n, (size_t)DOT_LEN)));
+    return CFD_OK;
+}
+
+// out_host[j] = <V_j, w>, j < k, compensated, deterministic.
+static int mdot(cfd_ctx *c, const double *V, int64_t ld, int k, const double *w, int64_t n, double *out_host) {
+    int st = dot_buffers(c);
+    if (st || (st = mdot_dev(c, V, ld, k, w, n, c->dots.p))) return st;
     CFD_CUDA(cudaMemcpyAsync(out_host, c->dots.p, sizeof(double) * k, cudaMemcpyDeviceToHost, c->stream));
     CFD_CUDA(cudaStreamSynchronize(c->stream));
     return CFD_OK;
+}
+
+// Hessenberg column j of the Arnoldi step: h1 + h2 (CGS2), ||w||, 1/||w||.
+__global__ void k_arnoldi_column(int j, double *__restrict__ dots) {
+    const int i = threadIdx.x;
+    if (i <= j) dots[DOT_COL + i] = dots[DOT_H1 + i] + dots[DOT_H2 + i];
+    if (i == 0) {
+        const double hn = sqrt(fmax(dots[DOT_NRM], 0.0));
+        dots[DOT_COL + j + 1] = hn;
+        dots[DOT_COL + MAXK - 1] = hn > 0.0 ? 1.0 / hn : 0.0;
+    }
 }
 
 // --------------------------------------------------------- vector kernels
@@ -194,6 +225,14 @@ __global__ void k_axpy_multi(int64_t n, int k, const double *__restrict__ V, int
 __global__ void k_scale_copy(int64_t n, double a, const double *__restrict__ x, double *__restrict__ y) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         y[i] = a * x[i];
+}
+
+// y = (*a) x with the factor read on the device.
+__global__ void k_scale_copy_dev(int64_t n, const double *__restrict__ a, const double *__restrict__ x,
+                                 double *__restrict__ y) {
+    const double f = *a;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = f * x[i];
 }
 
 __global__ void k_comb(int64_t n, int k, const double *__restrict__ V, int64_t ld, const double *__restrict__ y,
@@ -582,7 +621,9 @@ static int gmres_inner(cfd_ctx *c, int aprec, const Precond &pc, int m, int max_
     double *w = c->work.p;           // [n5]
     double *tmp = c->work.p + n5;    // [n5]
     double *zz = c->work.p + 2 * n5; // [n5]
-    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), h(m + 1), h2(m + 1), y(m);
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), h(m + 1), y(m);
+    int st0 = dot_buffers(c);
+    if (st0) return st0;
     CFD_CUDA(cudaMemsetAsync(d, 0, n5 * sizeof(double), c->stream));
     CFD_CUDA(cudaMemcpyAsync(w, r, n5 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     int total = 0, nrst = 0;
@@ -601,21 +642,22 @@ static int gmres_inner(cfd_ctx *c, int aprec, const Precond &pc, int m, int max_
             if ((st = precond_apply(c, pc, V + j * ld, tmp, zz))) return st;
             spmv(c, aprec, zz, w);
             CFD_LAUNCH_CHECK();
-            // CGS2
-            if ((st = mdot(c, V, ld, j + 1, w, n5, h.data()))) return st;
-            CFD_CUDA(cudaMemcpyAsync(c->dots.p + MAXK / 2, h.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice,
+            // CGS2 with the coefficients kept on the device; one read-back
+            // of the Hessenberg column per step
+            double *dd = c->dots.p;
+            if ((st = mdot_dev(c, V, ld, j + 1, w, n5, dd + DOT_H1))) return st;
+            k_axpy_multi<<<1184, 256, 0, c->stream>>>(n5, j + 1, V, ld, dd + DOT_H1, w);
+            if ((st = mdot_dev(c, V, ld, j + 1, w, n5, dd + DOT_H2))) return st;
+            k_axpy_multi<<<1184, 256, 0, c->stream>>>(n5, j + 1, V, ld, dd + DOT_H2, w);
+            if ((st = mdot_dev(c, w, n5, 1, w, n5, dd + DOT_NRM))) return st;
+            k_arnoldi_column<<<1, MAXK, 0, c->stream>>>(j, dd);
+            k_scale_copy_dev<<<1184, 256, 0, c->stream>>>(n5, dd + DOT_COL + MAXK - 1, w, V + (j + 1) * ld);
+            CFD_LAUNCH_CHECK();
+            CFD_CUDA(cudaMemcpyAsync(h.data(), dd + DOT_COL, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost,
                                      c->stream));
-            k_axpy_multi<<<1184, 256, 0, c->stream>>>(n5, j + 1, V, ld, c->dots.p + MAXK / 2, w);
-            if ((st = mdot(c, V, ld, j + 1, w, n5, h2.data()))) return st;
-            CFD_CUDA(cudaMemcpyAsync(c->dots.p + MAXK / 2, h2.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice,
-                                     c->stream));
-            k_axpy_multi<<<1184, 256, 0, c->stream>>>(n5, j + 1, V, ld, c->dots.p + MAXK / 2, w);
-            for (int i = 0; i <= j; i++) h[i] += h2[i];
-            double hn;
-            if ((st = vnorm(c, w, n5, &hn))) return st;
-            h[j + 1] = hn;
+            CFD_CUDA(cudaStreamSynchronize(c->stream));
+            const double hn = h[j + 1];
             if (!std::isfinite(hn)) { set_error("gmres: breakdown (non-finite)"); return CFD_ERR_NUMERIC; }
-            if (hn > 0.0) k_scale_copy<<<1184, 256, 0, c->stream>>>(n5, 1.0 / hn, w, V + (j + 1) * ld);
             // apply previous rotations, form a new one
             for (int i = 0; i < j; i++) {
                 const double t = cs[i] * h[i] + sn[i] * h[i + 1];
@@ -673,6 +715,7 @@ void cfd_gmres_default(cfd_gmres_opts *o) {
     o->precond = CFD_PC_ILU0;
     o->precision = CFD_PREC_FP64;
     o->refine = 1;
+    o->reuse_precond = 0;
 }
 
 int cfd_gmres(cfd_ctx *c, const cfd_gmres_opts *o, cfd_gmres_stats *stats) {
@@ -700,8 +743,14 @@ int cfd_gmres(cfd_ctx *c, const cfd_gmres_opts *o, cfd_gmres_stats *stats) {
     Precond pc;
     pc.kind = opt.precond;
     pc.prec = (opt.precision == CFD_PREC_FP64 && c->a64_valid) ? CFD_PREC_FP64 : CFD_PREC_FP32;
-    int st = precond_setup(c, pc);
-    if (st) return st;
+    int st = CFD_OK;
+    if (!(opt.reuse_precond && c->pc_valid && c->pc_kind == pc.kind && c->pc_prec == pc.prec)) {
+        c->pc_valid = false;
+        if ((st = precond_setup(c, pc))) return st;
+        c->pc_valid = true;
+        c->pc_kind = pc.kind;
+        c->pc_prec = pc.prec;
+    }
     double *x = c->X.p;
     double *r = c->work.p + 3 * n5;
     double *d = c->work.p + 4 * n5;
@@ -777,7 +826,9 @@ int cfd_solve_steady(cfd_ctx *c, const cfd_solve_opts *o, cfd_solve_stats *stats
         if ((st = cfd_jacobian(c, 1, o->include_diss, prec))) break;
         if (o->linear_solver == 1) {
             cfd_gmres_stats gs{};
-            st = cfd_gmres(c, &o->gmres, &gs);
+            cfd_gmres_opts go = o->gmres;
+            go.reuse_precond = (o->precond_update > 1 && iter % o->precond_update != 0) ? 1 : 0;
+            st = cfd_gmres(c, &go, &gs);
             s.linear_iterations += gs.iterations;
             if (st == CFD_ERR_NOT_CONVERGED) st = CFD_OK;  // inexact Newton step
             if (st) break;

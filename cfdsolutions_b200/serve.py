@@ -18,9 +18,9 @@ from .solver import default_params
 
 def steady_opts(max_iterations=800, drop=1e-8, include_diss=1, linear_solver=1, linear_iters=10, relax=1.0,
                 restart=30, gmres_iters=30, rtol=0.1, precond=capi.PC_ILU0_MC,
-                precision=capi.PREC_FP32 | capi.PREC_LOW_ONLY) -> capi.SolveOpts:
-    g = capi.GmresOpts(restart, gmres_iters, rtol, precond, precision, 1)
-    return capi.SolveOpts(max_iterations, drop, include_diss, linear_solver, linear_iters, relax, g)
+                precision=capi.PREC_FP32 | capi.PREC_LOW_ONLY, precond_update=1) -> capi.SolveOpts:
+    g = capi.GmresOpts(restart, gmres_iters, rtol, precond, precision, 1, 0)
+    return capi.SolveOpts(max_iterations, drop, include_diss, linear_solver, linear_iters, relax, g, precond_update)
 
 
 def request(n, params: capi.Params, opts: capi.SolveOpts, lengths=(1.0, 1.0, 1.0), jitter=0.15, mesh_seed=1,

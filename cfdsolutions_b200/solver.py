@@ -164,9 +164,10 @@ class Euler3DGPU:
         return conv, diss
 
     def solve_steady(self, max_iterations=100, drop=1e-8, include_diss=1, linear_solver=1, linear_iters=10,
-                     relax=1.0, gmres: capi.GmresOpts | None = None) -> capi.SolveStats:
+                     relax=1.0, gmres: capi.GmresOpts | None = None, precond_update: int = 1) -> capi.SolveStats:
         g = gmres if gmres is not None else capi.GmresOpts(30, 300, 1e-6, capi.PC_ILU0, capi.PREC_FP64, 1)
-        o = capi.SolveOpts(max_iterations, drop, include_diss, linear_solver, linear_iters, relax, g)
+        o = capi.SolveOpts(max_iterations, drop, include_diss, linear_solver, linear_iters, relax, g,
+                           int(precond_update))
         st = capi.SolveStats()
         capi.check(capi.lib.cfd_solve_steady(self._h, C.byref(o), C.byref(st)), "cfd_solve_steady")
         return st

@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define CFD_ABI_VERSION 1
+#define CFD_ABI_VERSION 2
 
 /* ------------------------------------------------------------ status codes */
 #define CFD_OK                 0
@@ -211,6 +211,9 @@ typedef struct cfd_gmres_opts {
     int    precond;        /* CFD_PC_*                                      */
     int    precision;      /* CFD_PREC_* of the preconditioner / A copy     */
     int    refine;         /* FP64 outer iterative-refinement sweeps (>=1)   */
+    int    reuse_precond;  /* 1: keep the preconditioner factored by the previous
+                              call (same kind and precision) instead of
+                              factoring the current matrix again            */
 } cfd_gmres_opts;
 
 typedef struct cfd_gmres_stats {
@@ -290,6 +293,9 @@ typedef struct cfd_solve_opts {
     int    linear_iters;     /* LINEAR_SOLVER_NITERATION / GMRES budget    */
     double relax;            /* SOLVER_RELAXATION                          */
     cfd_gmres_opts gmres;
+    int    precond_update;   /* factor the GMRES preconditioner every k implicit
+                                iterations (<= 1: every one); the Jacobian itself
+                                is rebuilt every iteration                  */
 } cfd_solve_opts;
 
 typedef struct cfd_solve_stats {

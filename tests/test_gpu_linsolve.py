@@ -204,3 +204,24 @@ def test_steady_solve_low_only_reaches_the_fp64_converged_state(gpu_available, p
     for v in range(5):
         scale = max(np.abs(out[0][v]).max(), mom if 1 <= v <= 3 else 0.0)
         assert np.abs(out[1][v] - out[0][v]).max() <= 1e-8 * scale
+
+
+def test_steady_solve_with_lagged_preconditioner_reaches_the_same_state(gpu_available):
+    """precond_update = 4: the ILU(0) factors are reused for 4 implicit
+    iterations (the Jacobian is rebuilt every iteration); the converged state
+    is the one of refactoring every iteration."""
+    m, cfg, Q = make_case(n=8, seed=3)
+    cfg = dict(cfg, cfl_min=10.0, cfl_max=1000.0, cfl_ramp=10)
+    out = []
+    for k in (1, 4):
+        with Euler3DGPU(m, params_from(cfg)) as s:
+            s.set_state(Q)
+            st = s.solve_steady(max_iterations=300, drop=1e-11, include_diss=1, linear_solver=1,
+                                gmres=capi.GmresOpts(30, 60, 1e-2, capi.PC_ILU0_MC, capi.PREC_FP64, 1, 0),
+                                precond_update=k)
+            assert st.rms_last <= 1e-11 * st.rms_first
+            out.append(s.get_state()[:, :m.nnode])
+    mom = np.abs(out[0][1:4]).max()
+    for v in range(5):
+        scale = max(np.abs(out[0][v]).max(), mom if 1 <= v <= 3 else 0.0)
+        assert np.abs(out[1][v] - out[0][v]).max() <= 1e-8 * scale
