@@ -113,6 +113,7 @@ SIGNATURES = {
     "cfd_residual_rms": (I, [P, I, P]),
     "cfd_jacobian": (I, [P, I, I, I]),
     "cfd_block_gs": (I, [P, I, I, C.POINTER(D)]),
+    "cfd_block_lusgs": (I, [P, I, C.POINTER(D)]),
     "cfd_block_gs_static": (I, [I, P, P, P, P, P, P, I, I, P, C.POINTER(D)]),
     "cfd_ilu_mc_order": (I, [P, P, C.POINTER(I)]),
     "cfd_gmres_default": (None, [C.POINTER(GmresOpts)]),

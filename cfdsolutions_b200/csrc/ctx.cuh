@@ -164,7 +164,8 @@ struct cfd_ctx {
     int a_precision = CFD_PREC_FP64;
     bool a64_valid = false;     // A64 holds the current system
     cfd::DevBuf<double> B, X;   // [nnode][5]
-    cfd::DevBuf<double> LUd;    // [nnode][25] diagonal LU for block GS
+    cfd::DevBuf<double> LUd;    // [nnode][25] diagonal LU for block GS / LU-SGS
+    cfd::DevBuf<int> lupiv;     // [nnode][5] row permutation of the LU-SGS pivoted factors
     cfd::DevBuf<double> rowrms; // [nnode]
     // GMRES / ILU workspaces (linsolve.cu)
     cfd::DevBuf<float> M32;     // ILU0 / block-Jacobi factors, FP32

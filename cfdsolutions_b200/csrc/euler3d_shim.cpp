@@ -12,6 +12,7 @@
 //   void   Compute_DeltaT(int)                          (Euler3D/src/Time_Step.cpp:23)
 //   void   Compute_Jacobian(int, int)                   (Euler3D/src/Jacobian.cpp:18)
 //   double MC_Iterative_Block_LU_Jacobi_CRS(int, int, MC_CRS)  (MATH/src/MC_Iterative_Jacobi.c:346)
+//   double MC_Iterative_Block_LUSGS_CRS(int, MC_CRS)           (MATH/src/MC_Iterative_Jacobi.c:539)
 //
 // The mesh, state and block system live on the GPU; the host globals the
 // driver reads (Q after the BC update, Res*/Res*_Diss for the RMS, DeltaT and
@@ -257,6 +258,19 @@ extern "C" double MC_Iterative_Block_LU_Jacobi_CRS(int Iteration, int Direction,
         if (rc == CFD_ERR_NUMERIC) return NAN;
         if (rc != CFD_OK) die("cfd_block_gs", rc);
     }
+    g.buf.resize(5 * (size_t)g.nnode);
+    CHECK(cfd_get_system(g.ctx, nullptr, nullptr, g.buf.data()));
+    for (int i = 0; i < Object.nROW; i++)
+        for (int k = 0; k < 5; k++) Object.X[i][k] = g.buf[5 * (size_t)i + k];
+    return rms;
+}
+
+extern "C" double MC_Iterative_Block_LUSGS_CRS(int Iteration, MC_CRS Object) {
+    ensure_init();
+    double rms = 0.0;
+    const int rc = cfd_block_lusgs(g.ctx, Iteration, &rms);
+    if (rc == CFD_ERR_NUMERIC) return NAN;
+    if (rc != CFD_OK) die("cfd_block_lusgs", rc);
     g.buf.resize(5 * (size_t)g.nnode);
     CHECK(cfd_get_system(g.ctx, nullptr, nullptr, g.buf.data()));
     for (int i = 0; i < Object.nROW; i++)

@@ -131,6 +131,14 @@ class Euler3DGPU:
         capi.check(code, "MC_Iterative_Block_LU_Jacobi_CRS")
         return rms.value
 
+    def MC_Iterative_Block_LUSGS_CRS(self, iterations: int) -> float:
+        rms = C.c_double()
+        code = capi.lib.cfd_block_lusgs(self._h, int(iterations), C.byref(rms))
+        if code == -6:  # numerical failure: NaN RMS, as the reference returns
+            return float("nan")
+        capi.check(code, "MC_Iterative_Block_LUSGS_CRS")
+        return rms.value
+
     def solve_gmres(self, restart=30, max_iters=300, rtol=1e-6, precond=capi.PC_ILU0, precision=capi.PREC_FP64,
                     refine=1, allow_not_converged=False) -> capi.GmresStats:
         o = capi.GmresOpts(restart, max_iters, rtol, precond, precision, refine)

@@ -204,6 +204,14 @@ int  cfd_jacobian(cfd_ctx *ctx, int add_time, int include_diss, int precision);
  * last sweep's residual. */
 int  cfd_block_gs(cfd_ctx *ctx, int iterations, int direction, double *rms);
 
+/* Block LU-SGS (MC_Iterative_Block_LUSGS_CRS, MATH/src/MC_Iterative_Jacobi.c:539):
+ * X starts at each row's mean of B; each iteration is a forward then a
+ * backward Gauss-Seidel sweep in which the diagonal block is solved by
+ * Gaussian elimination with partial pivoting.  Bit-exact with the reference
+ * (level-scheduled sweeps, explicitly rounded arithmetic).  *rms is the
+ * reference's returned value (computed as it computes it). */
+int  cfd_block_lusgs(cfd_ctx *ctx, int iterations, double *rms);
+
 typedef struct cfd_gmres_opts {
     int    restart;        /* Krylov dimension m (30)                       */
     int    max_iters;      /* total inner iterations budget                 */

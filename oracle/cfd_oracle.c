@@ -680,6 +680,78 @@ double orc_block_gs(int n, const int *IA, const int *JA, const int *IAU, const d
     return rms;
 }
 
+/* MC_Iterative_Block_LUSGS_CRS (MATH/src/MC_Iterative_Jacobi.c:539-717) with
+ * the pivoted elimination of GaussainLUDecompose and the pivoted
+ * substitutions (MATH/src/LinearAlgebra.c:20-43, 117-150); the returned RMS is
+ * computed as the reference computes it (block 6 of the storage against X at
+ * its column for every row, the running sum divided by 5 after each row). */
+static void lu_pivot5(double a[25], int P[5]) {
+    for (int i = 0; i < 5; i++) P[i] = i;
+    for (int c = 0; c < 5; c++) {
+        double pmax = a[P[c] * 5 + c];
+        int pi = c;
+        for (int i = c + 1; i < 5; i++)
+            if (fabs(a[P[i] * 5 + c]) > fabs(pmax)) { pmax = a[P[i] * 5 + c]; pi = i; }
+        if (pi != c) { int t = P[c]; P[c] = P[pi]; P[pi] = t; }
+        for (int i = c + 1; i < 5; i++) a[P[i] * 5 + c] /= a[P[c] * 5 + c];
+        for (int i = c + 1; i < 5; i++)
+            for (int j = c + 1; j < 5; j++) a[P[i] * 5 + j] -= a[P[i] * 5 + c] * a[P[c] * 5 + j];
+    }
+}
+
+double orc_block_lusgs(int n, const int *IA, const int *JA, const int *IAU, const double *A, const double *B,
+                       double *X, int iters) {
+    for (int r = 0; r < n; r++) {
+        double m = 0.0;
+        for (int j = 0; j < 5; j++) m += B[5 * (size_t)r + j];
+        m /= 5;
+        for (int j = 0; j < 5; j++) X[5 * (size_t)r + j] = m;
+    }
+    if (iters <= 0) iters = 100;
+    for (int it = 0; it < iters; it++)
+        for (int dir = 0; dir < 2; dir++)
+            for (int q = 0; q < n; q++) {
+                const int r = dir == 0 ? q : n - 1 - q;
+                double rhs[5], t[5], lu[25], y[5], x[5];
+                int P[5];
+                for (int k = 0; k < 5; k++) rhs[k] = B[5 * (size_t)r + k];
+                for (int k = IA[r]; k < IA[r + 1]; k++) {
+                    if (k == IAU[r]) continue;
+                    const double *a = A + 25 * (size_t)k, *xv = X + 5 * (size_t)JA[k];
+                    for (int ii = 0; ii < 5; ii++) {
+                        t[ii] = 0.0;
+                        for (int jj = 0; jj < 5; jj++) t[ii] += a[5 * ii + jj] * xv[jj];
+                    }
+                    for (int ii = 0; ii < 5; ii++) rhs[ii] -= t[ii];
+                }
+                memcpy(lu, A + 25 * (size_t)IAU[r], sizeof lu);
+                lu_pivot5(lu, P);
+                y[0] = rhs[P[0]];
+                for (int i = 1; i < 5; i++) {
+                    y[i] = rhs[P[i]];
+                    for (int j = 0; j < i; j++) y[i] -= y[j] * lu[P[i] * 5 + j];
+                }
+                x[4] = y[4] / lu[P[4] * 5 + 4];
+                for (int i = 3; i >= 0; i--) {
+                    x[i] = y[i];
+                    for (int j = 4; j > i; j--) x[i] -= x[j] * lu[P[i] * 5 + j];
+                    x[i] /= lu[P[i] * 5 + i];
+                }
+                for (int k = 0; k < 5; k++) X[5 * (size_t)r + k] = x[k];
+            }
+    double t[5], rms = 0.0;
+    const double *a = A + 25 * 5, *xv = X + 5 * (size_t)JA[5];
+    for (int ii = 0; ii < 5; ii++) {
+        t[ii] = 0.0;
+        for (int jj = 0; jj < 5; jj++) t[ii] += a[5 * ii + jj] * xv[jj];
+    }
+    for (int r = 0; r < n; r++) {
+        for (int j = 0; j < 5; j++) rms += (B[5 * (size_t)r + j] - t[j]) * (B[5 * (size_t)r + j] - t[j]);
+        rms /= 5;
+    }
+    return sqrt(rms / (double)n);
+}
+
 void orc_bspmv(int n, const int *IA, const int *JA, const double *A, const double *x, double *y) {
     for (int r = 0; r < n; r++)
         for (int a = 0; a < 5; a++) {

@@ -52,6 +52,8 @@ double orc_block_gs(int n, const int *IA, const int *JA, const int *IAU, const d
 int orc_ilu0(int n, const int *IA, const int *JA, const int *IAU, const double *A, double *F);
 int orc_gmres(int n, const int *IA, const int *JA, const int *IAU, const double *A, const double *B, double *X,
               int m, int maxit, double rtol, int precond, int *iters, double *relres);
+double orc_block_lusgs(int n, const int *IA, const int *JA, const int *IAU, const double *A, const double *B,
+                       double *X, int iters);
 void orc_bspmv(int n, const int *IA, const int *JA, const double *A, const double *x, double *y);
 
 #endif

@@ -44,6 +44,7 @@ def _lib():
         "orc_deltat": (None, [PM, PP, P, P]), "orc_block_pattern": (C.c_long, [PM, P, P, P]),
         "orc_jacobian": (None, [PM, PP, P, P, P, P, C.c_int, C.c_int, P, P, P, P, P]),
         "orc_block_gs": (C.c_double, [C.c_int, P, P, P, P, P, P, C.c_int, C.c_int]),
+        "orc_block_lusgs": (C.c_double, [C.c_int, P, P, P, P, P, P, C.c_int]),
         "orc_ilu0": (C.c_int, [C.c_int, P, P, P, P, P]),
         "orc_gmres": (C.c_int, [C.c_int, P, P, P, P, P, P, C.c_int, C.c_int, C.c_double, C.c_int,
                                 C.POINTER(C.c_int), C.POINTER(C.c_double)]),
@@ -120,6 +121,12 @@ class Session:
         X = np.zeros((self.n, 5))
         rms = lib.orc_block_gs(self.n, _p(self.IA), _p(self.JA), _p(self.IAU), _p(np.ascontiguousarray(A)),
                                _p(np.ascontiguousarray(B)), _p(X), iters, direction)
+        return X, rms
+
+    def block_lusgs(self, A, B, iters):
+        X = np.zeros((self.n, 5))
+        rms = lib.orc_block_lusgs(self.n, _p(self.IA), _p(self.JA), _p(self.IAU), _p(np.ascontiguousarray(A)),
+                                  _p(np.ascontiguousarray(B)), _p(X), iters)
         return X, rms
 
     def gmres(self, A, B, m=30, maxit=300, rtol=1e-6, precond=2):

@@ -165,3 +165,21 @@ def test_implicit_iterations_track_reference(gpu_available, ref_available):
         Qg = s.get_state()
     k = m.nnode
     assert relerr_rows(Qg[:, :k], ref["state"][:, :k]) <= 1e-10
+
+
+@pytest.mark.parametrize("iters", [1, 5])
+def test_block_lusgs_bit_exact(gpu_available, ref_available, iters):
+    """LU-SGS on the GPU (level-scheduled forward and backward sweeps, pivoted
+    diagonal solves) equals the reference's MC_Iterative_Block_LUSGS_CRS bit
+    for bit, including its returned RMS."""
+    m, cfg, Q = make_case(n=8, seed=6)
+    ref0 = refharness.run(m, cfg, Q, [("begin", 0), ("bc", 0), ("residual", 1), ("deltat", 0), ("jacobian", 1, 0),
+                                      ("get", "matrix")])
+    A, B = ref0["A"], ref0["B"]
+    ref = refharness.run(m, cfg, Q, [("set_matrix", A, B), ("lusgs", iters), ("get", "matrix")])
+    with Euler3DGPU(m, params_from(cfg)) as s:
+        s.set_system(A.reshape(-1, 25), B)
+        rms = s.MC_Iterative_Block_LUSGS_CRS(iters)
+        _, _, X = s.get_system()
+    np.testing.assert_array_equal(X, ref["X"])
+    assert rms == ref["lusgs_rms"][0]

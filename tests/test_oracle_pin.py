@@ -148,3 +148,16 @@ def test_ilu_gmres_agrees_with_dense_solve():
     it_none = s.gmres(o["A"], o["B"], rtol=1e-8, precond=0)[2]
     it_ilu = s.gmres(o["A"], o["B"], rtol=1e-8, precond=2)[2]
     assert it_ilu < it_none
+
+
+def test_block_lusgs_restatement_is_the_reference(ref_available):
+    """LU-SGS (MC_Iterative_Block_LUSGS_CRS): the restatement's sweeps,
+    pivoted diagonal solves and returned RMS equal the reference's bit for bit."""
+    m, cfg, Q = make_case(n=7, seed=9)
+    ref0 = refharness.run(m, cfg, Q, [("begin", 0), ("bc", 0), ("residual", 1), ("deltat", 0), ("jacobian", 1, 0),
+                                      ("get", "matrix")])
+    A, B = ref0["A"], ref0["B"]
+    ref = refharness.run(m, cfg, Q, [("set_matrix", A, B), ("lusgs", 4), ("get", "matrix")])
+    X, rms = restatement.Session(m, cfg).block_lusgs(A, B, 4)
+    np.testing.assert_array_equal(X, ref["X"])
+    assert rms == ref["lusgs_rms"][0]
