@@ -25,6 +25,7 @@ GRAD_LSQ, GRAD_GG = 0, 1
 PREC_FP64, PREC_FP32, PREC_BF16 = 0, 1, 2
 PC_NONE, PC_BLOCK_JACOBI, PC_ILU0, PC_ILU0_MC = 0, 1, 2, 3
 PREC_LOW_ONLY = 0x10
+JAC_CENTRAL, JAC_FORWARD, JAC_BACKWARD, JAC_ALTERNATE = 0, 1, 2, 3
 BC_EULER_WALL, BC_FAR_FIELD, BC_INFLOW, BC_OUTFLOW = 0, 1, 2, 3
 GS_STATIC_MAX_ROWS = 16384
 PENDING = 1
@@ -114,6 +115,7 @@ SIGNATURES = {
     "cfd_jacobian": (I, [P, I, I, I]),
     "cfd_block_gs": (I, [P, I, I, C.POINTER(D)]),
     "cfd_block_lusgs": (I, [P, I, C.POINTER(D)]),
+    "cfd_jacobian_fd": (I, [P, I, I, I, I]),
     "cfd_block_gs_static": (I, [I, P, P, P, P, P, P, I, I, P, C.POINTER(D)]),
     "cfd_ilu_mc_order": (I, [P, P, C.POINTER(I)]),
     "cfd_gmres_default": (None, [C.POINTER(GmresOpts)]),

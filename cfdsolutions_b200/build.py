@@ -20,7 +20,10 @@ OUT_DIR = PKG / "_lib"
 LIB = OUT_DIR / "libcfd_b200.so"
 OBJ_DIR = PKG / "_build"
 
-CU_SOURCES = ["core.cu", "gradient.cu", "linsolve.cu", "ilu_mc.cu", "gs_static.cu", "serve.cu"]
+CU_SOURCES = ["core.cu", "gradient.cu", "linsolve.cu", "ilu_mc.cu", "gs_static.cu", "serve.cu", "fd_jacobian.cu"]
+# per-file nvcc flags: the finite-difference Jacobian must round every
+# expression as written (no fused multiply-add) to reproduce the reference
+FILE_FLAGS = {"fd_jacobian.cu": ["-fmad=false"]}
 CXX_SOURCES = ["mesh.cpp"]
 HEADERS = ["cfd_internal.h", "ctx.cuh", "kernels.cuh", "physics.cuh", "ilu_mc.cuh"]
 
@@ -56,7 +59,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         s = CSRC / src
         o = OBJ_DIR / (src + ".o")
         if force or _stale(o, [s, *headers]):
-            cmd = [nvcc, *ARCH, *NVCC_FLAGS, *include, "-c", str(s), "-o", str(o)]
+            cmd = [nvcc, *ARCH, *NVCC_FLAGS, *FILE_FLAGS.get(src, []), *include, "-c", str(s), "-o", str(o)]
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)

@@ -68,6 +68,7 @@ extern double *Q1x, *Q1y, *Q1z, *Q2x, *Q2y, *Q2z, *Q3x, *Q3y, *Q3z, *Q4x, *Q4y, 
 extern double *Limiter_Phi1, *Limiter_Phi2, *Limiter_Phi3, *Limiter_Phi4, *Limiter_Phi5;
 extern int FluxScheme, SolverOrder, LimiterMethod, LimiterOrder, LimiterSmooth, EntropyFix;
 extern int TimeIntegrationType, CFL_Ramp, Mach_Ramp, ZPGIteration, JacobianUpdate, VariableType, PrecondMethod;
+extern int JacobianMethod;
 extern double CFL_MIN, CFL_MAX, Mach_MIN, Mach_MAX, Gamma, Ref_Alpha, Ref_Beta, Venkat_KThreshold;
 extern double Inf_Rho, Inf_U, Inf_V, Inf_W, Inf_Et, Inf_Pressure, Inf_SpeedSound, Inf_Mach;
 
@@ -237,7 +238,10 @@ void Compute_Jacobian(int AddTime, int Iteration) {
     ensure_init();
     if (Iteration % JacobianUpdate != 0) return;  // Jacobian.cpp:26-28
     // Euler3D's right-hand side is B = -Res (its Res_Diss is never added, FluxTest.cpp:8143-8150)
-    CHECK(cfd_jacobian(g.ctx, AddTime, 0, g.gmres ? CFD_PREC_FP32 : CFD_PREC_FP64));
+    if (JacobianMethod >= CFD_JAC_CENTRAL && JacobianMethod <= CFD_JAC_ALTERNATE)  // Roe_Jacobian.cpp:780-793
+        CHECK(cfd_jacobian_fd(g.ctx, AddTime, 0, JacobianMethod, Iteration));
+    else
+        CHECK(cfd_jacobian(g.ctx, AddTime, 0, g.gmres ? CFD_PREC_FP32 : CFD_PREC_FP64));
 }
 
 extern "C" double MC_Iterative_Block_LU_Jacobi_CRS(int Iteration, int Direction, MC_CRS Object) {

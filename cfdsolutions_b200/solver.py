@@ -131,6 +131,11 @@ class Euler3DGPU:
         capi.check(code, "MC_Iterative_Block_LU_Jacobi_CRS")
         return rms.value
 
+    def Compute_Jacobian_FiniteDifference(self, add_time: int = 1, iteration: int = 0,
+                                          method: int = capi.JAC_CENTRAL, include_diss: int = 0):
+        capi.check(capi.lib.cfd_jacobian_fd(self._h, int(add_time), int(include_diss), int(method), int(iteration)),
+                   "Compute_Jacobian_FiniteDifference_Roe")
+
     def MC_Iterative_Block_LUSGS_CRS(self, iterations: int) -> float:
         rms = C.c_double()
         code = capi.lib.cfd_block_lusgs(self._h, int(iterations), C.byref(rms))

@@ -204,6 +204,20 @@ int  cfd_jacobian(cfd_ctx *ctx, int add_time, int include_diss, int precision);
  * last sweep's residual. */
 int  cfd_block_gs(cfd_ctx *ctx, int iterations, int direction, double *rms);
 
+/* Finite-difference Roe Jacobian (Compute_Jacobian_FiniteDifference_Roe,
+ * Euler3D/src/Roe_Jacobian.cpp:236): difference quotients (eps = 1e-8) of the
+ * reference's matrix-form Roe flux (Roe_Fluxes.cpp:552) of first-order states;
+ * interior edges by `method`, boundary edges by central differences with the
+ * ghost state rebuilt by the older characteristic BC (BC.cpp:33) for every
+ * perturbed state.  FP64 system; B = -(Res + include_diss * Res_Diss).
+ * method: JACOBIAN_METHOD_* (SolverParameters.h:274-279); ALTERNATE is forward
+ * on even iterations, backward on odd ones. */
+#define CFD_JAC_CENTRAL   0
+#define CFD_JAC_FORWARD   1
+#define CFD_JAC_BACKWARD  2
+#define CFD_JAC_ALTERNATE 3
+int  cfd_jacobian_fd(cfd_ctx *ctx, int add_time, int include_diss, int method, int iteration);
+
 /* Block LU-SGS (MC_Iterative_Block_LUSGS_CRS, MATH/src/MC_Iterative_Jacobi.c:539):
  * X starts at each row's mean of B; each iteration is a forward then a
  * backward Gauss-Seidel sweep in which the diagonal block is solved by

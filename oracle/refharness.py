@@ -32,6 +32,10 @@ def available() -> bool:
     return REF_LIB.exists()
 
 
+JACOBIAN = {0: "JACOBIAN_METHOD_CENTRAL", 1: "JACOBIAN_METHOD_FORWARD", 2: "JACOBIAN_METHOD_BACKWARD",
+            3: "JACOBIAN_METHOD_ALTERNATE", 4: "JACOBIAN_METHOD_APPROX"}
+
+
 def param_text(cfg: dict) -> str:
     """Reference parameter file for the options in ``cfg`` (same keys as cfd_params)."""
     g = lambda k, d: cfg.get(k, d)  # noqa: E731
@@ -51,7 +55,7 @@ def param_text(cfg: dict) -> str:
         "PRECOND_METHOD": "PRECOND_METHOD_NONE", "BC_METHOD": "BC_METHOD_CHARCTERISTIC",
         "ZPG_ITERATION": str(g("zpg_iteration", 0)),
         "VARIABLE_TYPE": "VARIABLE_CONSERVATIVE", "ENTROPY_FIX": "YES" if g("entropy_fix", 0) else "NO",
-        "JACOBIAN_METHOD": "JACOBIAN_METHOD_APPROX", "JACOBIAN_UPDATE": "1", "FIRST_ORDER_NITERATION": "0",
+        "JACOBIAN_METHOD": JACOBIAN[g("jacobian_method", 4)], "JACOBIAN_UPDATE": "1", "FIRST_ORDER_NITERATION": "0",
         "SOLVER_RELAXATION": "1.0", "RESIDUAL_SMOOTH_METHOD": "RESIDUAL_SMOOTH_METHOD_NONE",
         "LIMITER_METHOD": LIMITER[g("limiter", -1)], "LIMITER_SMOOTH": "YES" if g("limiter_smooth", 0) else "NO",
         "LIMITER_ORDER": "LIMITER_ORDER_SECOND" if g("limiter_order", 0) == 1 else "LIMITER_ORDER_FIRST",

@@ -22,13 +22,13 @@ EXE_CPU = REF_DIR / "euler3d"
 EXE_GPU = REF_DIR / "euler3d_gpu"
 
 
-def write_case(d: Path, n: int, order: int, iters: int, seed: int = 5):
+def write_case(d: Path, n: int, order: int, iters: int, seed: int = 5, jacobian_method: int = 4):
     m = box_mesh(n, jitter=0.15, seed=seed, ugrid_path=str(d / "mesh.ugrid"))
     _, cfg, Q = make_case(mesh=m, noise=0.01)
     (d / "bc.txt").write_text("# number of boundaries\n1\n# boundary 1\n1\n")
     rst = str(d / "in.rst").encode()
     capi.check(capi.lib.cfd_restart_write(rst, 0, m.nnode, m.nghost, capi.ptr(np.ascontiguousarray(Q))), "restart")
-    cfg = dict(cfg, order=order, limiter=1 if order else -1, venkat_k=5.0)
+    cfg = dict(cfg, order=order, limiter=1 if order else -1, venkat_k=5.0, jacobian_method=jacobian_method)
     text = refharness.param_text(cfg)
     text = text.replace("MESH_FILENAME=none", f"MESH_FILENAME={d / 'mesh.ugrid'}")
     text = text.replace("BC_FILENAME=none", f"BC_FILENAME={d / 'bc.txt'}")
@@ -87,3 +87,21 @@ def test_euler3d_executable_gmres_converges(gpu_available, ref_available, tmp_pa
             if ln.strip() and ln.strip()[0].isdigit()]
     rms = np.array(rows)[:, 6]
     assert rms[-1] < 0.8 * rms[0]
+
+
+def test_euler3d_executable_with_finite_difference_jacobian(gpu_available, ref_available, tmp_path):
+    """JACOBIAN_METHOD_CENTRAL: the executable's Compute_Jacobian runs the GPU
+    finite-difference Jacobian.  Its boundary blocks are difference quotients
+    through ghost states that differ from the reference's in the last bits, so
+    the states agree to 1e-9 rather than 1e-10."""
+    if not EXE_GPU.exists():
+        pytest.skip("drop-in executable not built (make -C oracle gpu)")
+    iters = 4
+    write_case(tmp_path, 6, 0, iters, jacobian_method=0)
+    res_cpu, rst_cpu = run(EXE_CPU, tmp_path / "cpu", tmp_path / "param.txt")
+    res_gpu, rst_gpu = run(EXE_GPU, tmp_path / "gpu", tmp_path / "param.txt")
+    assert res_cpu.shape == res_gpu.shape and res_cpu.shape[0] == iters
+    np.testing.assert_allclose(res_gpu, res_cpu, rtol=2e-5, atol=0)
+    qc = np.frombuffer(rst_cpu[16:], np.float64)
+    qg = np.frombuffer(rst_gpu[16:], np.float64)
+    assert np.abs(qg - qc).max() <= 1e-9 * np.abs(qc).max()
