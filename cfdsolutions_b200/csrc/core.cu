@@ -733,7 +733,8 @@ static void compute_flow(cfd_ctx *c, int iteration) {
     f.outflow_p = 0.935 * pr;  // Material.cpp:171
     f.frac = p.limiter_order == 1 ? 0.5 : 0.0;
     f.venkat_eps_k3 = pow(p.venkat_k, 3.0);
-    f.flux = p.flux_scheme;
+    f.flux = p.flux_scheme == CFD_FLUX_ROE_LMFIX ? CFD_FLUX_ROE : p.flux_scheme;
+    f.lmfix = p.flux_scheme == CFD_FLUX_ROE_LMFIX ? 1 : 0;
     f.order = p.order;
     f.limiter = p.limiter;
     f.limiter_smooth = p.limiter_smooth;
@@ -997,7 +998,7 @@ int cfd_set_stream(cfd_ctx *c, void *stream) {
 
 int cfd_set_params(cfd_ctx *c, const cfd_params *p) {
     if (!c || !p) { set_error("cfd_set_params: NULL"); return CFD_ERR_ARG; }
-    if (p->flux_scheme < CFD_FLUX_ROE || p->flux_scheme > CFD_FLUX_AUSM) {
+    if (p->flux_scheme < CFD_FLUX_ROE || p->flux_scheme > CFD_FLUX_ROE_LMFIX) {
         set_error("cfd_set_params: invalid flux scheme %d", p->flux_scheme);
         return CFD_ERR_ARG;
     }
@@ -1401,7 +1402,8 @@ int cfd_residual(cfd_ctx *c, int add_time) {
         set_error("cfd_residual: limiter requested but cfd_limiter not called");
         return CFD_ERR_STATE;
     }
-    switch (c->params.flux_scheme * 2 + (second ? 1 : 0)) {
+    const int family = c->params.flux_scheme == CFD_FLUX_ROE_LMFIX ? CFD_FLUX_ROE : c->params.flux_scheme;
+    switch (family * 2 + (second ? 1 : 0)) {
         case 0: return residual_with_fix<CFD_FLUX_ROE, false>(c, add_time);
         case 1: return residual_with_fix<CFD_FLUX_ROE, true>(c, add_time);
         case 2: return residual_with_fix<CFD_FLUX_HLLC, false>(c, add_time);

@@ -95,11 +95,13 @@ void die(const char *where, int code) {
 void sync_params() {
     cfd_params p;
     cfd_params_default(&p);
-    if (VariableType != 0 || PrecondMethod != -1) {
-        std::fprintf(stderr, "cfd_b200 shim: only VARIABLE_CONSERVATIVE without preconditioning is supported\n");
+    // PRECOND_METHOD_NONE (-1) or PRECOND_METHOD_ROE_LMFIX (0) with the Roe flux
+    if (VariableType != 0 || !(PrecondMethod == -1 || (PrecondMethod == 0 && FluxScheme == CFD_FLUX_ROE))) {
+        std::fprintf(stderr, "cfd_b200 shim: only VARIABLE_CONSERVATIVE without preconditioning or with the Roe "
+                             "low-Mach fix is supported\n");
         std::exit(EXIT_FAILURE);
     }
-    p.flux_scheme = FluxScheme;
+    p.flux_scheme = PrecondMethod == 0 ? CFD_FLUX_ROE_LMFIX : FluxScheme;
     p.order = SolverOrder;
     p.limiter = LimiterMethod;
     p.limiter_order = LimiterOrder;

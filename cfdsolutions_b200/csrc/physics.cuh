@@ -23,6 +23,7 @@ struct Flow {
     int limiter_smooth;
     int entropy_fix;
     int zpg_iteration, iteration;
+    int lmfix;            // Roe low-Mach fix and the preconditioned characteristic BC (CFD_FLUX_ROE_LMFIX)
 };
 
 struct Face {
@@ -114,7 +115,29 @@ __device__ __forceinline__ double roe_flux(const double qL[5], const double qR[5
     lam[2] = E2;
 
     const double drho = R.rho - L.rho, du = R.u - L.u, dv = R.v - L.v, dw_ = R.w - L.w, dp = R.p - L.p;
-    const double dU = du * nx + dv * ny + dw_ * nz;
+    double dU = du * nx + dv * ny + dw_ * nz;
+    if (f.lmfix) {
+        // Low-Mach fix (Compute_Flux_Roe_LMFIX, Euler3D/src/FluxTest.cpp:2929-2966): the normal
+        // velocity jump scaled by min(1, (|u.n| + |u.t1| + |u.t2|) / c), t1 from the largest normal
+        // component, t2 = t1 x n, both normalised
+        double nmax = fabs(nx);
+        int mc = 1;
+        if (nmax < fabs(ny)) { nmax = fabs(ny); mc = 2; }
+        if (nmax < fabs(nz)) { nmax = fabs(nz); mc = 3; }
+        double a0 = 1.0, a1 = 1.0, a2 = 1.0;
+        if (mc == 1) a0 = -(ny + nz) / nx;
+        else if (mc == 2) a1 = -(nx + nz) / ny;
+        else a2 = -(nx + ny) / nz;
+        double m1 = sqrt(a0 * a0 + a1 * a1 + a2 * a2);
+        if (m1 > 1.0e-20) { a0 = a0 / m1; a1 = a1 / m1; a2 = a2 / m1; }
+        const double ub1 = u * a0 + v * a1 + w * a2;
+        double b0 = a1 * nz - a2 * ny, b1 = -a0 * nz + a2 * nx, b2 = a0 * ny - a1 * nx;
+        const double m2 = sqrt(b0 * b0 + b1 * b1 + b2 * b2);
+        if (m2 > 1.0e-20) { b0 = b0 / m2; b1 = b1 / m2; b2 = b2 / m2; }
+        const double ub2 = u * b0 + v * b1 + w * b2;
+        const double mach = (fabs(ubar) + fabs(ub1) + fabs(ub2)) / c;
+        dU = (mach < 1.0 ? mach : 1.0) * dU;
+    }
     const double Es = E1 + E2 - 2.0 * E0;
     const double Ed = E1 - E2;
     const double t1 = 0.5 * dU * Es;
@@ -185,7 +208,13 @@ __device__ __forceinline__ int characteristic_bc(const double qI[5], const doubl
             w_b = I.w - nz * dp / rc;
         } break;
         case 4: case 6: case 10: case 1: break;  // freestream values
-        case 5: case 9: {                         // subsonic outflow / far-field subsonic outflow
+        case 5: case 7:
+            // the preconditioned characteristic BC (used with the low-Mach fix,
+            // BC.cpp:1229-1236) keeps the freestream values for these two
+            if (f.lmfix) break;
+            if (inst == 7) { p_b = I.p; rho_b = I.rho; u_b = I.u; v_b = I.v; w_b = I.w; break; }
+            [[fallthrough]];
+        case 9: {                                 // subsonic outflow / far-field subsonic outflow
             p_b = (inst == 5) ? f.outflow_p : f.inf_p;
             const double dp = p_b - I.p;
             rho_b = I.rho + dp / c2;
@@ -193,7 +222,7 @@ __device__ __forceinline__ int characteristic_bc(const double qI[5], const doubl
             v_b = I.v - ny * dp / rc;
             w_b = I.w - nz * dp / rc;
         } break;
-        case 7: case 11:  // supersonic outflow: extrapolate
+        case 11:  // far-field supersonic outflow: extrapolate
             p_b = I.p; rho_b = I.rho; u_b = I.u; v_b = I.v; w_b = I.w;
             break;
         case 8: {  // far-field subsonic inflow (BC.cpp:621-628)

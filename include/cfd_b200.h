@@ -55,6 +55,9 @@ extern "C" {
 #define CFD_FLUX_ROE   0   /* FLUX_SCHEME_ROE  (SolverParameters.h:111) */
 #define CFD_FLUX_HLLC  1   /* FLUX_SCHEME_HLLC (SolverParameters.h:112) */
 #define CFD_FLUX_AUSM  2   /* FLUX_SCHEME_AUSM (:113); AUSM+ (Liou 1996), the reference's is an empty stub */
+#define CFD_FLUX_ROE_LMFIX 3 /* FLUX_SCHEME_ROE with PRECOND_METHOD_ROE_LMFIX (SolverParameters.h:136): the
+                                low-Mach fix of Compute_Flux_Roe_LMFIX (Euler3D/src/FluxTest.cpp:2801) and the
+                                preconditioned characteristic BC (BC.cpp:700) */
 
 #define CFD_ORDER_FIRST  0 /* SOLVER_ORDER_FIRST  (SolverParameters.h:316) */
 #define CFD_ORDER_SECOND 1 /* SOLVER_ORDER_SECOND (SolverParameters.h:317) */

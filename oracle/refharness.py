@@ -24,7 +24,7 @@ HERE = Path(__file__).resolve().parent
 REF_LIB = HERE / "_ref" / "libeuler3d_ref.so"
 REF_EXE = HERE / "_ref" / "euler3d"
 
-FLUX = {0: "FLUX_SCHEME_ROE", 1: "FLUX_SCHEME_HLLC", 2: "FLUX_SCHEME_AUSM"}
+FLUX = {0: "FLUX_SCHEME_ROE", 1: "FLUX_SCHEME_HLLC", 2: "FLUX_SCHEME_AUSM", 3: "FLUX_SCHEME_ROE"}
 LIMITER = {-1: "LIMITER_METHOD_NONE", 0: "LIMITER_METHOD_BERTH_JESPERSEN", 1: "LIMITER_METHOD_VENKATAKRISHNAN"}
 
 
@@ -52,7 +52,8 @@ def param_text(cfg: dict) -> str:
         "TIME_INTEGRATION_METHOD": "TIME_INTEGRATION_METHOD_IMPLICIT_EULER",
         "TIME_INTEGRATION_TYPE": "TIME_INTEGRATION_TYPE_GLOBAL" if g("global_time", 0) else
         "TIME_INTEGRATION_TYPE_LOCAL",
-        "PRECOND_METHOD": "PRECOND_METHOD_NONE", "BC_METHOD": "BC_METHOD_CHARCTERISTIC",
+        "PRECOND_METHOD": "PRECOND_METHOD_ROE_LMFIX" if g("flux_scheme", 0) == 3 else "PRECOND_METHOD_NONE",
+        "BC_METHOD": "BC_METHOD_CHARCTERISTIC",
         "ZPG_ITERATION": str(g("zpg_iteration", 0)),
         "VARIABLE_TYPE": "VARIABLE_CONSERVATIVE", "ENTROPY_FIX": "YES" if g("entropy_fix", 0) else "NO",
         "JACOBIAN_METHOD": JACOBIAN[g("jacobian_method", 4)], "JACOBIAN_UPDATE": "1", "FIRST_ORDER_NITERATION": "0",

@@ -22,13 +22,14 @@ EXE_CPU = REF_DIR / "euler3d"
 EXE_GPU = REF_DIR / "euler3d_gpu"
 
 
-def write_case(d: Path, n: int, order: int, iters: int, seed: int = 5, jacobian_method: int = 4):
+def write_case(d: Path, n: int, order: int, iters: int, seed: int = 5, jacobian_method: int = 4, flux: int = 0):
     m = box_mesh(n, jitter=0.15, seed=seed, ugrid_path=str(d / "mesh.ugrid"))
     _, cfg, Q = make_case(mesh=m, noise=0.01)
     (d / "bc.txt").write_text("# number of boundaries\n1\n# boundary 1\n1\n")
     rst = str(d / "in.rst").encode()
     capi.check(capi.lib.cfd_restart_write(rst, 0, m.nnode, m.nghost, capi.ptr(np.ascontiguousarray(Q))), "restart")
-    cfg = dict(cfg, order=order, limiter=1 if order else -1, venkat_k=5.0, jacobian_method=jacobian_method)
+    cfg = dict(cfg, order=order, limiter=1 if order else -1, venkat_k=5.0, jacobian_method=jacobian_method,
+               flux_scheme=flux)
     text = refharness.param_text(cfg)
     text = text.replace("MESH_FILENAME=none", f"MESH_FILENAME={d / 'mesh.ugrid'}")
     text = text.replace("BC_FILENAME=none", f"BC_FILENAME={d / 'bc.txt'}")
@@ -50,12 +51,13 @@ def run(exe: Path, d: Path, param: Path):
     return np.array(rows), raw
 
 
-@pytest.mark.parametrize("order", [0, 1])
-def test_euler3d_executable_with_gpu_hot_path(gpu_available, ref_available, tmp_path, order):
+@pytest.mark.parametrize("order,flux", [(0, 0), (1, 0), (1, 3)])
+def test_euler3d_executable_with_gpu_hot_path(gpu_available, ref_available, tmp_path, order, flux):
+    """flux 3: Roe with the low-Mach fix (PRECOND_METHOD_ROE_LMFIX)."""
     if not EXE_GPU.exists():
         pytest.skip("drop-in executable not built (make -C oracle gpu)")
     iters = 6
-    m = write_case(tmp_path, 8, order, iters)
+    m = write_case(tmp_path, 8, order, iters, flux=flux)
     res_cpu, rst_cpu = run(EXE_CPU, tmp_path / "cpu", tmp_path / "param.txt")
     res_gpu, rst_gpu = run(EXE_GPU, tmp_path / "gpu", tmp_path / "param.txt")
     assert res_cpu.shape == res_gpu.shape and res_cpu.shape[0] == iters

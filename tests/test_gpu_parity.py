@@ -225,3 +225,33 @@ def test_finite_difference_jacobian_matches_reference(gpu_available, ref_availab
         err = np.abs(A[diag] - ref["A"][diag]).reshape(len(IAU), -1).max(axis=1)
         assert np.all(err <= tol * scale), (tol, float((err / scale).max()))
         np.testing.assert_allclose(B, ref["B"], rtol=0, atol=1e-12 * np.abs(ref["B"]).max())
+
+
+@pytest.mark.parametrize("face_bc,mach", [((1, 1, 1, 1, 1, 1), 0.1), ((2, 3, 0, 0, 0, 0), 0.2)])
+def test_low_mach_fix_residual_and_ghosts_match_reference(gpu_available, ref_available, face_bc, mach):
+    """Roe with the low-Mach fix (PRECOND_METHOD_ROE_LMFIX): second-order
+    residual (Compute_Flux_Roe_LMFIX) and the ghost states of the
+    preconditioned characteristic BC, on an all-far-field cube and on a
+    channel (inflow at x = 0, outflow at x = 1, walls elsewhere)."""
+    from cfdsolutions_b200 import box_mesh
+    cfg = dict(CFG1, flux_scheme=3, order=1, limiter=1, limiter_order=1, venkat_k=5.0, mach=mach, mach_min=mach,
+               alpha_deg=0.0 if face_bc[0] == 2 else 2.0)
+    m = box_mesh(8, jitter=0.15, seed=41, face_bc=face_bc)
+    _, cfg, Q = make_case(cfg=cfg, mesh=m, seed=41)
+    ref = refharness.run(m, cfg, Q, [("begin", 0), ("gradient", 0), ("limiter",), ("bc", 0), ("get", "state"),
+                                     ("residual", 1), ("get", "residual"), ("deltat", 0), ("get", "deltat")])
+    with Euler3DGPU(m, params_from(cfg)) as s:
+        s.set_state(Q)
+        s.begin_iteration(0)
+        s.Compute_Least_Square_Gradient(0)
+        s.Compute_Limiter()
+        s.Apply_Boundary_Condition(0)
+        state = s.get_state()
+        s.Compute_Residual(1)
+        conv, diss = s.get_residual()
+        s.Compute_DeltaT(0)
+        dt = s.get_deltat()
+    assert relerr_rows(state, ref["state"]) <= TOL
+    assert relerr_rows(conv, ref["conv"]) <= TOL
+    assert relerr_rows(diss, ref["diss"]) <= TOL
+    assert relerr(dt, ref["deltat"]) <= TOL
