@@ -733,7 +733,7 @@ static void compute_flow(cfd_ctx *c, int iteration) {
     f.outflow_p = 0.935 * pr;  // Material.cpp:171
     f.frac = p.limiter_order == 1 ? 0.5 : 0.0;
     f.venkat_eps_k3 = pow(p.venkat_k, 3.0);
-    f.flux = p.flux_scheme == CFD_FLUX_ROE_LMFIX ? CFD_FLUX_ROE : p.flux_scheme;
+    f.flux = p.flux_scheme;
     f.lmfix = p.flux_scheme == CFD_FLUX_ROE_LMFIX ? 1 : 0;
     f.order = p.order;
     f.limiter = p.limiter;
@@ -881,7 +881,7 @@ static int residual_with_fix(cfd_ctx *c, int add_time) {
     // Roe flux + limiter: the limiter's Roe-average pressure fix is decided by
     // the residual's own reconstruction (same states) and applied, followed by
     // a gated re-evaluation, only when some edge failed the check.
-    const bool fused = SECOND && FLUX == CFD_FLUX_ROE && c->roe_fix_pending;
+    const bool fused = SECOND && is_roe_flux(FLUX) && c->roe_fix_pending;
     int st = launch_residual<FLUX, SECOND>(c, add_time, fused, nullptr);
     if (st || !fused) return st;
     k_roe_fix_apply<<<grid_for(c->nnode, 256), 256, 0, c->stream>>>(c->nnode, c->roecount.p, c->roeflag.p, c->phi.p);
@@ -1402,14 +1402,15 @@ int cfd_residual(cfd_ctx *c, int add_time) {
         set_error("cfd_residual: limiter requested but cfd_limiter not called");
         return CFD_ERR_STATE;
     }
-    const int family = c->params.flux_scheme == CFD_FLUX_ROE_LMFIX ? CFD_FLUX_ROE : c->params.flux_scheme;
-    switch (family * 2 + (second ? 1 : 0)) {
+    switch (c->params.flux_scheme * 2 + (second ? 1 : 0)) {
         case 0: return residual_with_fix<CFD_FLUX_ROE, false>(c, add_time);
         case 1: return residual_with_fix<CFD_FLUX_ROE, true>(c, add_time);
         case 2: return residual_with_fix<CFD_FLUX_HLLC, false>(c, add_time);
         case 3: return residual_with_fix<CFD_FLUX_HLLC, true>(c, add_time);
         case 4: return residual_with_fix<CFD_FLUX_AUSM, false>(c, add_time);
         case 5: return residual_with_fix<CFD_FLUX_AUSM, true>(c, add_time);
+        case 6: return residual_with_fix<CFD_FLUX_ROE_LMFIX, false>(c, add_time);
+        case 7: return residual_with_fix<CFD_FLUX_ROE_LMFIX, true>(c, add_time);
         default: set_error("cfd_residual: bad flux scheme"); return CFD_ERR_ARG;
     }
 }

@@ -69,6 +69,7 @@ __device__ __forceinline__ void roe_entropy_fix(double ubar_L, double c_L, doubl
 // |A| dQ = M_{cons<-RUP} * dw, dw in closed form (FluxTest.cpp:3180-3190).
 // Returns the largest |eigenvalue| (for the time step) and the three
 // eigenvalue magnitudes |ubar|, |ubar+c|, |ubar-c| in lam[3].
+template <bool LMFIX>
 __device__ __forceinline__ double roe_flux(const double qL[5], const double qR[5], double nx, double ny,
                                            double nz, double area, const Flow &f, double conv[5],
                                            double diss[5], double lam[3]) {
@@ -116,7 +117,7 @@ __device__ __forceinline__ double roe_flux(const double qL[5], const double qR[5
 
     const double drho = R.rho - L.rho, du = R.u - L.u, dv = R.v - L.v, dw_ = R.w - L.w, dp = R.p - L.p;
     double dU = du * nx + dv * ny + dw_ * nz;
-    if (f.lmfix) {
+    if (LMFIX) {
         // Low-Mach fix (Compute_Flux_Roe_LMFIX, Euler3D/src/FluxTest.cpp:2929-2966): the normal
         // velocity jump scaled by min(1, (|u.n| + |u.t1| + |u.t2|) / c), t1 from the largest normal
         // component, t2 = t1 x n, both normalised
