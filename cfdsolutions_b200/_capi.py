@@ -18,7 +18,7 @@ ERRORS = {
     -1: "CFD_ERR_ARG", -2: "CFD_ERR_MESH", -3: "CFD_ERR_CUDA", -4: "CFD_ERR_IO", -5: "CFD_ERR_STATE",
     -6: "CFD_ERR_NUMERIC", -7: "CFD_ERR_NOT_CONVERGED", -8: "CFD_ERR_UNSUPPORTED", -9: "CFD_ERR_RANGE",
 }
-FLUX_ROE, FLUX_HLLC, FLUX_AUSM = 0, 1, 2
+FLUX_ROE, FLUX_HLLC, FLUX_AUSM, FLUX_ROE_LMFIX = 0, 1, 2, 3
 ORDER_FIRST, ORDER_SECOND = 0, 1
 LIMITER_NONE, LIMITER_BJ, LIMITER_VENKAT = -1, 0, 1
 GRAD_LSQ, GRAD_GG = 0, 1
@@ -44,7 +44,7 @@ class Params(C.Structure):
         ("global_time", C.c_int), ("cfl_ramp", C.c_int), ("mach_ramp", C.c_int), ("zpg_iteration", C.c_int),
         ("gamma", C.c_double), ("mach", C.c_double), ("mach_min", C.c_double), ("alpha_deg", C.c_double),
         ("beta_deg", C.c_double), ("cfl_min", C.c_double), ("cfl_max", C.c_double), ("venkat_k", C.c_double),
-        ("residual_kernel", C.c_int),
+        ("residual_kernel", C.c_int), ("pinf", C.c_double),
     ]
 
 
@@ -141,6 +141,7 @@ SIGNATURES = {
     "cfd_set_mesh_from": (I, [P, P]),
     "cfd_mesh_free": (None, [P]),
     "cfd_perturbed_freestream": (I, [P, D, D, D, D, D, C.c_uint64, P]),
+    "cfd_initial_state": (I, [P, P, P, C.c_uint64, P]),
     "cfd_server_create": (I, [I, I, D, C.POINTER(P)]),
     "cfd_server_submit": (I, [P, C.POINTER(ServeRequest), C.POINTER(I64)]),
     "cfd_server_wait": (I, [P, I64, D, C.POINTER(ServeResult)]),

@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(128, 3) k_residual_gather(
                 qL[v] = own_is_L ? fo[v] : fn[v];
                 qR[v] = own_is_L ? fn[v] : fo[v];
             }
-            if (SECOND && check_roe && roe_avg_pressure(qL, qR, f.gamma) < 0.0) roe_bad = true;
+            if (SECOND && check_roe && roe_avg_pressure(qL, qR, f.gamma, f.gpinf) < 0.0) roe_bad = true;
             double cf[5], df[5], lam[3];
             const double lmax = edge_flux<FLUX>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam);
             const double sg = own_is_L ? 1.0 : -1.0;
@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(PATCH_CHUNK, 2) k_residual_patch(
                 }
 #pragma unroll
                 for (int v = 0; v < 5; v++) { qL[v] = rL[v]; qR[v] = rR[v]; }
-                if (check_roe && roe_avg_pressure(qL, qR, f.gamma) < 0.0) {
+                if (check_roe && roe_avg_pressure(qL, qR, f.gamma, f.gpinf) < 0.0) {
                     roeflag[a < nown ? n0 + a : halo[h0 + a - nown]] = 1;
                     roeflag[b < nown ? n0 + b : halo[h0 + b - nown]] = 1;
                     atomicAdd(roecount, 1);
@@ -486,14 +486,14 @@ __global__ void __launch_bounds__(128) k_jac_edges(int nedge, int64_t ldq, const
     roe_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
     const int2 sl = eslot[e];
     const double ha = 0.5 * g.w;
-    euler_flux_jacobian(qR, g.x, g.y, g.z, f.gamma, J);
+    euler_flux_jacobian(qR, g.x, g.y, g.z, f.gamma, f.gpinf, J);
 #pragma unroll
     for (int k = 0; k < 25; k++) {
         const double val = ha * (J[k] - Ab[k]);
         if (A64) A64[(int64_t)sl.x * 25 + k] = val;
         if (Alow) store_low(Alow + (int64_t)sl.x * 25 + k, val);
     }
-    euler_flux_jacobian(qL, g.x, g.y, g.z, f.gamma, J);
+    euler_flux_jacobian(qL, g.x, g.y, g.z, f.gamma, f.gpinf, J);
 #pragma unroll
     for (int k = 0; k < 25; k++) {
         const double val = -ha * (J[k] + Ab[k]);
@@ -543,7 +543,7 @@ __global__ void __launch_bounds__(128) k_jac_rows(
             qR[v] = Q[v * ldq + nd.y];
         }
         roe_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
-        euler_flux_jacobian(qL, g.x, g.y, g.z, f.gamma, J);
+        euler_flux_jacobian(qL, g.x, g.y, g.z, f.gamma, f.gpinf, J);
         const double ha = 0.5 * g.w;
 #pragma unroll
         for (int m = 0; m < 25; m++) D[m] += ha * (J[m] + Ab[m]);
@@ -722,14 +722,17 @@ static void compute_flow(cfd_ctx *c, int iteration) {
     }
     const double R = 1.0 / p.gamma, rho = 1.0, T = p.gamma, pr = R * rho * T;
     const double alpha = p.alpha_deg * M_PI / 180.0, beta = p.beta_deg * M_PI / 180.0;
+    f.pinf = p.pinf;
+    f.gpinf = p.gamma * p.pinf;
     f.inf_mach = mach;
     f.inf_rho = rho;
     f.inf_p = pr;
-    f.inf_c = sqrt(p.gamma * R * T);
+    // stiffened gas: c^2 = gamma (p + pinf) / rho (the ideal-gas expression when pinf = 0)
+    f.inf_c = p.pinf != 0.0 ? sqrt(p.gamma * (pr + p.pinf) / rho) : sqrt(p.gamma * R * T);
     f.inf_u = mach * f.inf_c * cos(alpha) * cos(beta);
     f.inf_v = mach * f.inf_c * sin(alpha);
     f.inf_w = mach * f.inf_c * sin(beta) * cos(alpha);
-    f.inf_et = pr / ((p.gamma - 1.0) * rho) + 0.5 * (f.inf_u * f.inf_u + f.inf_v * f.inf_v + f.inf_w * f.inf_w);
+    f.inf_et = (pr + f.gpinf) / ((p.gamma - 1.0) * rho) + 0.5 * (f.inf_u * f.inf_u + f.inf_v * f.inf_v + f.inf_w * f.inf_w);
     f.outflow_p = 0.935 * pr;  // Material.cpp:171
     f.frac = p.limiter_order == 1 ? 0.5 : 0.0;
     f.venkat_eps_k3 = pow(p.venkat_k, 3.0);
@@ -1003,6 +1006,10 @@ int cfd_set_params(cfd_ctx *c, const cfd_params *p) {
         return CFD_ERR_ARG;
     }
     if (!(p->gamma > 1.0)) { set_error("cfd_set_params: gamma must be > 1"); return CFD_ERR_ARG; }
+    if (!(p->pinf >= 0.0 && p->pinf < 1.0e300)) {
+        set_error("cfd_set_params: pinf must be finite and >= 0");
+        return CFD_ERR_ARG;
+    }
     if (p->residual_kernel < 0 || p->residual_kernel > 1) {
         set_error("cfd_set_params: residual_kernel must be 0 or 1");
         return CFD_ERR_ARG;

@@ -36,17 +36,19 @@ struct RefFace {
 };
 
 // Compute_EOS_Variables_Face, generic non-dimensionalisation, conservative
-// variables (Euler3D/src/Material.cpp:216-240), in the reference's order.
-__device__ void ref_face(const double q[5], double nx, double ny, double nz, double gamma, RefFace &s) {
+// variables (Euler3D/src/Material.cpp:216-240), in the reference's order, with
+// the stiffened-gas terms (exact zeros at pinf = 0).
+__device__ void ref_face(const double q[5], double nx, double ny, double nz, const Flow &f, RefFace &s) {
+    const double gamma = f.gamma;
     s.rho = q[0];
     s.u = q[1] / s.rho;
     s.v = q[2] / s.rho;
     s.w = q[3] / s.rho;
     s.et = q[4] / s.rho;
     s.q2 = s.u * s.u + s.v * s.v + s.w * s.w;
-    s.p = (gamma - 1.0) * (s.rho * s.et - 0.5 * s.rho * s.q2);
+    s.p = (gamma - 1.0) * (s.rho * s.et - 0.5 * s.rho * s.q2) - f.gpinf;
     s.ht = (s.rho * s.et + s.p) / s.rho;
-    s.c = sqrt((gamma * s.p) / s.rho);
+    s.c = sqrt((gamma * (s.p + f.pinf)) / s.rho);
     s.ubar = s.u * nx + s.v * ny + s.w * nz;
 }
 
@@ -68,8 +70,8 @@ __device__ void ref_roe_flux(const double qL[5], const double qR[5], double nx, 
                              const Flow &f, double conv[5], double diss[5]) {
     const double g = f.gamma;
     RefFace L, R;
-    ref_face(qL, nx, ny, nz, g, L);
-    ref_face(qR, nx, ny, nz, g, R);
+    ref_face(qL, nx, ny, nz, f, L);
+    ref_face(qR, nx, ny, nz, f, R);
     double fl[5], fr[5];
     fl[0] = L.rho * L.ubar;
     fl[1] = L.u * fl[0] + L.p * nx;
@@ -149,10 +151,10 @@ __device__ void old_characteristic_bc(const double qi[5], const double qg[5], do
                                       int type, int iteration, const Flow &f, double qb[5], int *err) {
     const double g = f.gamma;
     RefFace I, Z;
-    ref_face(qi, nx, ny, nz, g, I);
+    ref_face(qi, nx, ny, nz, f, I);
     double q0[5];
     for (int k = 0; k < 5; k++) q0[k] = 0.5 * (qi[k] + qg[k]);
-    ref_face(q0, nx, ny, nz, g, Z);
+    ref_face(q0, nx, ny, nz, f, Z);
     const double l1 = Z.ubar, l4 = l1 + Z.c, l5 = l1 - Z.c;
     int inst = type;
     switch (type) {
@@ -181,7 +183,7 @@ __device__ void old_characteristic_bc(const double qi[5], const double qg[5], do
     switch (inst) {
         case 0:
             pb = I.p + Z.rho * Z.c * I.ubar;
-            if (iteration < f.zpg_iteration && pb < 0.0) pb = I.p;
+            if (iteration < f.zpg_iteration && pb + f.pinf < 0.0) pb = I.p;
             rb = I.rho + (pb - I.p) / cc;
             ub = I.u - nx * (pb - I.p) / rc;
             vb = I.v - ny * (pb - I.p) / rc;
@@ -208,10 +210,10 @@ __device__ void old_characteristic_bc(const double qi[5], const double qg[5], do
         }
         default: break;  // 1, 4, 6, 10: freestream values
     }
-    if (pb < 0.0) atomicOr(err, ERR_BC_NEG_PRESSURE);
+    if (pb + f.pinf < 0.0) atomicOr(err, ERR_BC_NEG_PRESSURE);
     // Get_TotalEnergy (Material.cpp:1012-1021)
     double et = ub * ub + vb * vb + wb * wb;
-    et = pb / ((g - 1.0) * rb) + 0.5 * et;
+    et = (pb + f.gpinf) / ((g - 1.0) * rb) + 0.5 * et;
     qb[0] = rb;
     qb[1] = rb * ub;
     qb[2] = rb * vb;

@@ -230,10 +230,11 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
 #pragma unroll
         for (int v = 0; v < 5; v++)
             q[v] = qc[v] + ph[v] * (frac * (Q[v * ldq + j] - qc[v]) + (1.0 - frac) * (gx[v] * rx + gy[v] * ry + gz[v] * rz));
-        // p < 0 of (Limiters.cpp:296-301) without the division when rho > 0
+        // p < 0 of (Limiters.cpp:296-301) without the division when rho > 0 (p + pinf < 0
+        // for the stiffened gas)
         const double m2 = q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
-        const bool pneg = q[0] > 0.0 ? (2.0 * q[0] * q[4] < m2)
-                                     : (f.gm1 * (q[4] - (0.5 / q[0]) * m2) < 0.0);
+        const bool pneg = q[0] > 0.0 ? (2.0 * q[0] * (q[4] - f.pinf) < m2)
+                                     : (f.gm1 * ((q[4] - f.pinf) - (0.5 / q[0]) * m2) < 0.0);
         if (pneg) neg = true;
     }
     if (neg) {
@@ -283,8 +284,8 @@ __global__ void __launch_bounds__(128) k_roe_pressure_fix(int nnode, int64_t ldq
         const double ra = qa[0], rb = qb[0];
         const double ua = qa[1] / ra, va = qa[2] / ra, wa = qa[3] / ra;
         const double ub = qb[1] / rb, vb = qb[2] / rb, wb = qb[3] / rb;
-        const double pa = f.gm1 * (qa[4] - 0.5 * ra * (ua * ua + va * va + wa * wa));
-        const double pb = f.gm1 * (qb[4] - 0.5 * rb * (ub * ub + vb * vb + wb * wb));
+        const double pa = f.gm1 * (qa[4] - 0.5 * ra * (ua * ua + va * va + wa * wa)) - f.gpinf;
+        const double pb = f.gm1 * (qb[4] - 0.5 * rb * (ub * ub + vb * vb + wb * wb)) - f.gpinf;
         const double ha = (qa[4] + pa) / ra, hb = (qb[4] + pb) / rb;
         const double rho = sqrt(ra * rb), sg = rho / (ra + rho);
         const double u = ua + sg * (ub - ua), v = va + sg * (vb - va), w = wa + sg * (wb - wa);

@@ -18,8 +18,8 @@ __device__ __forceinline__ double hllc_flux(const double qL[5], const double qR[
                                             double area, const Flow &f, double conv[5], double diss[5],
                                             double lam[3]) {
     Face L, R;
-    eos_face(qL, nx, ny, nz, f.gm1, f.gamma, true, L);
-    eos_face(qR, nx, ny, nz, f.gm1, f.gamma, true, R);
+    eos_face(qL, nx, ny, nz, f, true, L);
+    eos_face(qR, nx, ny, nz, f, true, R);
     const double rho = sqrt(R.rho * L.rho);
     const double sigma = rho / (L.rho + rho);
     const double u = L.u + sigma * (R.u - L.u);
@@ -84,8 +84,8 @@ __device__ __forceinline__ double ausmp_flux(const double qL[5], const double qR
                                              double nz, double area, const Flow &f, double conv[5], double diss[5],
                                              double lam[3]) {
     Face L, R;
-    eos_face(qL, nx, ny, nz, f.gm1, f.gamma, false, L);
-    eos_face(qR, nx, ny, nz, f.gm1, f.gamma, false, R);
+    eos_face(qL, nx, ny, nz, f, false, L);
+    eos_face(qR, nx, ny, nz, f, false, R);
     const double k = 2.0 * f.gm1 / (f.gamma + 1.0);
     const double csL = sqrt(k * L.ht), csR = sqrt(k * R.ht);
     const double chL = csL * csL / fmax(csL, L.ubar);
@@ -147,13 +147,15 @@ __host__ __device__ constexpr bool is_roe_flux(int flux) { return flux == CFD_FL
 // Pressure of the Roe-averaged state of two reconstructed face states
 // (Compute_RoeVariables, Roe_Fluxes.cpp:3609-3633, tested in
 // Compute_Limiter_RoePressureCorrection, Limiters.cpp:311-356).
-__device__ __forceinline__ double roe_avg_pressure(const double qa[5], const double qb[5], double g) {
+// For the stiffened gas the value returned is p + pinf of the Roe state (its
+// c^2 = (g - 1) h holds for either gas), the quantity whose sign matters.
+__device__ __forceinline__ double roe_avg_pressure(const double qa[5], const double qb[5], double g, double gpinf) {
     const double ra = qa[0], rb = qb[0];
     const double ia = 1.0 / ra, ib = 1.0 / rb;
     const double ua = qa[1] * ia, va = qa[2] * ia, wa = qa[3] * ia;
     const double ub = qb[1] * ib, vb = qb[2] * ib, wb = qb[3] * ib;
-    const double pa = (g - 1.0) * (qa[4] - 0.5 * ra * (ua * ua + va * va + wa * wa));
-    const double pb = (g - 1.0) * (qb[4] - 0.5 * rb * (ub * ub + vb * vb + wb * wb));
+    const double pa = (g - 1.0) * (qa[4] - 0.5 * ra * (ua * ua + va * va + wa * wa)) - gpinf;
+    const double pb = (g - 1.0) * (qb[4] - 0.5 * rb * (ub * ub + vb * vb + wb * wb)) - gpinf;
     const double ha = (qa[4] + pa) * ia, hb = (qb[4] + pb) * ib;
     const double rho = sqrt(ra * rb), sg = rho / (ra + rho);
     const double u = ua + sg * (ub - ua), v = va + sg * (vb - va), w = wa + sg * (wb - wa);

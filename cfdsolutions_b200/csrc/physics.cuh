@@ -1,5 +1,6 @@
 // Device physics of the node-centred edge-based Euler path: ideal-gas EOS in
-// the generic non-dimensionalisation, Roe / HLLC / AUSM+ edge fluxes,
+// the generic non-dimensionalisation (or the stiffened gas
+// p = (gamma - 1) rho e - gamma pinf, which is the ideal gas at pinf = 0), Roe / HLLC / AUSM+ edge fluxes,
 // characteristic ghost states and the approximate Roe flux Jacobian.
 // Conservative variables (rho, rho u, rho v, rho w, rho et) throughout, as
 // Euler3D with VARIABLE_TYPE=VARIABLE_CONSERVATIVE.
@@ -15,6 +16,7 @@ struct Flow {
     double gamma, gm1, inv_gm1;
     double inf_rho, inf_u, inf_v, inf_w, inf_p, inf_et, inf_c, inf_mach;
     double outflow_p;
+    double pinf, gpinf;   // stiffened-gas constant and gamma * pinf (both 0 for the ideal gas)
     double frac;          // 0.5 for LIMITER_ORDER_SECOND else 0 (HigherOrderReconstructQ.cpp:27-29)
     double venkat_eps_k3; // K^3 (Limiters.cpp:205)
     int flux;             // CFD_FLUX_*
@@ -30,20 +32,22 @@ struct Face {
     double rho, u, v, w, p, ht, ubar, c;
 };
 
-// Compute_EOS_Variables_Face, conservative branch (Euler3D/src/Material.cpp:216-248).
-// c is only formed when `want_c` (entropy fix / HLLC / AUSM+ need it).
-__device__ __forceinline__ void eos_face(const double q[5], double nx, double ny, double nz, double gm1,
-                                         double gamma, bool want_c, Face &s) {
+// Compute_EOS_Variables_Face, conservative branch (Euler3D/src/Material.cpp:216-248),
+// with the stiffened-gas terms: p = (gamma - 1)(rho et - rho q^2 / 2) - gamma pinf and
+// c^2 = gamma (p + pinf) / rho.  At pinf = 0 both added terms are exact zeros, so
+// the ideal-gas results are bit-identical.  c is only formed when `want_c`.
+__device__ __forceinline__ void eos_face(const double q[5], double nx, double ny, double nz, const Flow &f,
+                                         bool want_c, Face &s) {
     s.rho = q[0];
     const double ri = 1.0 / s.rho;
     s.u = q[1] * ri;
     s.v = q[2] * ri;
     s.w = q[3] * ri;
     const double q2 = s.u * s.u + s.v * s.v + s.w * s.w;
-    s.p = gm1 * (q[4] - 0.5 * s.rho * q2);
+    s.p = f.gm1 * (q[4] - 0.5 * s.rho * q2) - f.gpinf;
     s.ht = (q[4] + s.p) * ri;
     s.ubar = s.u * nx + s.v * ny + s.w * nz;
-    s.c = want_c ? sqrt(gamma * s.p * ri) : 0.0;
+    s.c = want_c ? sqrt(f.gamma * (s.p + f.pinf) * ri) : 0.0;
 }
 
 // Kermani entropy fix on the acoustic eigenvalues (Euler3D/src/Roe_EntropyFix.cpp:19-59).
@@ -75,8 +79,8 @@ __device__ __forceinline__ double roe_flux(const double qL[5], const double qR[5
                                            double diss[5], double lam[3]) {
     Face L, R;
     const bool want_c = f.entropy_fix != 0;
-    eos_face(qL, nx, ny, nz, f.gm1, f.gamma, want_c, L);
-    eos_face(qR, nx, ny, nz, f.gm1, f.gamma, want_c, R);
+    eos_face(qL, nx, ny, nz, f, want_c, L);
+    eos_face(qR, nx, ny, nz, f, want_c, R);
 
     const double mL = L.rho * L.ubar, mR = R.rho * R.ubar;
     const double ha = 0.5 * area;
@@ -165,11 +169,11 @@ __device__ __forceinline__ double roe_flux(const double qL[5], const double qR[5
 __device__ __forceinline__ int characteristic_bc(const double qI[5], const double qG[5], double nx, double ny,
                                                  double nz, int bc_type, const Flow &f, double qB[5]) {
     Face I, G, O;
-    eos_face(qI, nx, ny, nz, f.gm1, f.gamma, true, I);
-    eos_face(qG, nx, ny, nz, f.gm1, f.gamma, true, G);
+    eos_face(qI, nx, ny, nz, f, true, I);
+    eos_face(qG, nx, ny, nz, f, true, G);
     double q0[5];
     for (int k = 0; k < 5; k++) q0[k] = 0.5 * (qI[k] + qG[k]);
-    eos_face(q0, nx, ny, nz, f.gm1, f.gamma, true, O);
+    eos_face(q0, nx, ny, nz, f, true, O);
     const double l1 = O.ubar, l4 = O.ubar + O.c, l5 = O.ubar - O.c;
     double p_b = f.inf_p, rho_b = f.inf_rho, u_b = f.inf_u, v_b = f.inf_v, w_b = f.inf_w;
     int inst;
@@ -201,7 +205,7 @@ __device__ __forceinline__ int characteristic_bc(const double qI[5], const doubl
     switch (inst) {
         case 0: {  // Euler wall (BC.cpp:582-594)
             p_b = I.p + rc * I.ubar;
-            if (f.iteration < f.zpg_iteration && p_b < 0.0) p_b = I.p;
+            if (f.iteration < f.zpg_iteration && p_b + f.pinf < 0.0) p_b = I.p;
             const double dp = p_b - I.p;
             rho_b = I.rho + dp / c2;
             u_b = I.u - nx * dp / rc;
@@ -237,9 +241,9 @@ __device__ __forceinline__ int characteristic_bc(const double qI[5], const doubl
         } break;
         default: break;
     }
-    if (p_b < 0.0) status = status ? status : 1;
-    // Get_TotalEnergy (Material.cpp:1012-1040)
-    const double et = p_b / (f.gm1 * rho_b) + 0.5 * (u_b * u_b + v_b * v_b + w_b * w_b);
+    if (p_b + f.pinf < 0.0) status = status ? status : 1;
+    // Get_TotalEnergy (Material.cpp:1012-1040), rho e = (p + gamma pinf) / (gamma - 1)
+    const double et = (p_b + f.gpinf) / (f.gm1 * rho_b) + 0.5 * (u_b * u_b + v_b * v_b + w_b * w_b);
     qB[0] = rho_b;
     qB[1] = rho_b * u_b;
     qB[2] = rho_b * v_b;
@@ -249,13 +253,14 @@ __device__ __forceinline__ int characteristic_bc(const double qI[5], const doubl
 }
 
 // Conservative Euler flux Jacobian dF.n/dQ (ConservativeEulerFluxJacobian,
-// Euler3D/src/CompressibleUtils.cpp:558-609).  J row-major [5][5].
+// Euler3D/src/CompressibleUtils.cpp:558-609).  J row-major [5][5].  The
+// stiffened gas only shifts p (dp/dQ is unchanged), so only ht carries gpinf.
 __device__ __forceinline__ void euler_flux_jacobian(const double q[5], double nx, double ny, double nz,
-                                                    double g, double J[25]) {
+                                                    double g, double gpinf, double J[25]) {
     const double rho = q[0], ri = 1.0 / rho;
     const double u = q[1] * ri, v = q[2] * ri, w = q[3] * ri, rhoet = q[4];
     const double ek = 0.5 * (u * u + v * v + w * w);
-    const double p = (g - 1.0) * (rhoet - rho * ek);
+    const double p = (g - 1.0) * (rhoet - rho * ek) - gpinf;
     const double ht = (rhoet + p) * ri;
     const double ub = u * nx + v * ny + w * nz;
     const double g1 = g - 1.0, g2 = g - 2.0;
@@ -274,8 +279,8 @@ __device__ __forceinline__ void roe_abs_jacobian(const double qL[5], const doubl
                                                  double nz, const Flow &f, double Aout[25]) {
     Face L, R;
     const bool want_c = f.entropy_fix != 0;
-    eos_face(qL, nx, ny, nz, f.gm1, f.gamma, want_c, L);
-    eos_face(qR, nx, ny, nz, f.gm1, f.gamma, want_c, R);
+    eos_face(qL, nx, ny, nz, f, want_c, L);
+    eos_face(qR, nx, ny, nz, f, want_c, R);
     const double rho = sqrt(R.rho * L.rho);
     const double sigma = rho / (L.rho + rho);
     const double u = L.u + sigma * (R.u - L.u);

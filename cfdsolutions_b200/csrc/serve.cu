@@ -111,9 +111,8 @@ int run_job(int device, cudaStream_t s, const cfd_serve_request &r, cfd_serve_re
         res.nghost = mesh->m.nghost;
         Q.resize((size_t)5 * (res.nnode + res.nghost));
         const cfd_params &p = r.params;
-        if ((st = cfd_perturbed_freestream(mesh, p.gamma, p.mach, p.alpha_deg, p.beta_deg, r.noise, r.state_seed,
-                                           Q.data())))
-            break;
+        const double noise[3] = {r.noise, r.noise, r.noise};
+        if ((st = cfd_initial_state(mesh, &p, noise, r.state_seed, Q.data()))) break;
         if ((st = cfd_set_state(ctx, Q.data()))) break;
         if (r.opts.linear_solver == 1 && r.opts.gmres.precond == CFD_PC_ILU0_MC &&
             (st = cfd_ilu_mc_order(ctx, nullptr, nullptr)))
@@ -187,20 +186,34 @@ extern "C" {
 
 int cfd_perturbed_freestream(const cfd_mesh *m, double gamma, double mach, double alpha_deg, double beta_deg,
                              double noise, uint64_t seed, double *Q) {
-    if (!m || !Q || !(gamma > 1.0)) return CFD_ERR_ARG;
+    cfd_params p;
+    cfd_params_default(&p);
+    p.gamma = gamma;
+    p.mach = p.mach_min = mach;
+    p.alpha_deg = alpha_deg;
+    p.beta_deg = beta_deg;
+    const double nz[3] = {noise, noise, noise};
+    return cfd_initial_state(m, &p, nz, seed, Q);
+}
+
+int cfd_initial_state(const cfd_mesh *m, const cfd_params *p, const double noise[3], uint64_t seed, double *Q) {
+    if (!m || !p || !noise || !Q || !(p->gamma > 1.0) || !(p->pinf >= 0.0)) return CFD_ERR_ARG;
+    const double gamma = p->gamma, pinf = p->pinf;
     const int64_t N = m->m.nnode, n = N + m->m.nghost;
-    const double c = std::sqrt(gamma), deg = 3.14159265358979323846 / 180.0;
-    const double a = alpha_deg * deg, b = beta_deg * deg;
+    // rho = 1, p = 1: c^2 = gamma (1 + pinf)
+    const double c = pinf != 0.0 ? std::sqrt(gamma * (1.0 + pinf)) : std::sqrt(gamma);
+    const double deg = 3.14159265358979323846 / 180.0;
+    const double a = p->alpha_deg * deg, b = p->beta_deg * deg, mach = p->mach;
     const double u0[3] = {mach * c * std::cos(a) * std::cos(b), mach * c * std::sin(a),
                           mach * c * std::sin(b) * std::cos(a)};
     for (int64_t i = 0; i < n; i++) {
         const bool phys = i < N;
-        const double rho = 1.0 * (phys ? 1.0 + noise * unit_pm1(seed, (uint64_t)i) : 1.0);
+        const double rho = 1.0 * (phys ? 1.0 + noise[0] * unit_pm1(seed, (uint64_t)i) : 1.0);
         double v[3];
         for (int d = 0; d < 3; d++)
-            v[d] = u0[d] * (phys ? 1.0 + noise * unit_pm1(seed, (uint64_t)((1 + d) * N + i)) : 1.0);
-        const double p = 1.0 * (phys ? 1.0 + noise * unit_pm1(seed, (uint64_t)(4 * N + i)) : 1.0);
-        const double et = p / ((gamma - 1.0) * rho) + 0.5 * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            v[d] = u0[d] * (phys ? 1.0 + noise[1] * unit_pm1(seed, (uint64_t)((1 + d) * N + i)) : 1.0);
+        const double pr = 1.0 * (phys ? 1.0 + noise[2] * unit_pm1(seed, (uint64_t)(4 * N + i)) : 1.0);
+        const double et = (pr + gamma * pinf) / ((gamma - 1.0) * rho) + 0.5 * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
         Q[i] = rho;
         Q[n + i] = rho * v[0];
         Q[2 * n + i] = rho * v[1];

@@ -106,13 +106,16 @@ def from_cells(coords: np.ndarray, tets: np.ndarray, tris: np.ndarray, tri_bc: n
 
 
 def perturbed_freestream(mesh: Mesh, gamma: float, mach: float, alpha_deg: float, beta_deg: float = 0.0,
-                         noise: float = 0.01, seed: int = 2) -> np.ndarray:
+                         noise=0.01, seed: int = 2, pinf: float = 0.0) -> np.ndarray:
     """Conservative state SoA [5, nnode+nghost]: freestream of the generic
     non-dimensionalisation (rho=1, p=1, c=sqrt(gamma); Euler3D/src/Material.cpp:119-124,
-    :185-210) with density, velocity and pressure of physical nodes multiplied
-    by (1 + U(+-noise)) from ``seed``."""
+    :185-210), or of the stiffened gas with constant ``pinf`` (c = sqrt(gamma (1 + pinf))),
+    with density, velocity and pressure of physical nodes multiplied by
+    (1 + U(+-noise)) from ``seed``; ``noise`` is one amplitude or a
+    (density, velocity, pressure) triple."""
+    nr, nv, npr = (noise, noise, noise) if np.isscalar(noise) else tuple(noise)
     n = mesh.nnode + mesh.nghost
-    c = np.sqrt(gamma)
+    c = np.sqrt(gamma * (1.0 + pinf))
     a, b = np.deg2rad(alpha_deg), np.deg2rad(beta_deg)
     u = mach * c * np.cos(a) * np.cos(b)
     v = mach * c * np.sin(a)
@@ -122,10 +125,10 @@ def perturbed_freestream(mesh: Mesh, gamma: float, mach: float, alpha_deg: float
     p = np.ones(n)
     rng = np.random.default_rng(seed)
     k = mesh.nnode
-    rho[:k] *= 1.0 + noise * rng.uniform(-1, 1, k)
-    vel[:, :k] *= 1.0 + noise * rng.uniform(-1, 1, (3, k))
-    p[:k] *= 1.0 + noise * rng.uniform(-1, 1, k)
-    et = p / ((gamma - 1.0) * rho) + 0.5 * (vel ** 2).sum(0)
+    rho[:k] *= 1.0 + nr * rng.uniform(-1, 1, k)
+    vel[:, :k] *= 1.0 + nv * rng.uniform(-1, 1, (3, k))
+    p[:k] *= 1.0 + npr * rng.uniform(-1, 1, k)
+    et = (p + gamma * pinf) / ((gamma - 1.0) * rho) + 0.5 * (vel ** 2).sum(0)
     Q = np.empty((5, n))
     Q[0] = rho
     Q[1:4] = rho * vel

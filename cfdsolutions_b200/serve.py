@@ -38,8 +38,8 @@ def request(n, params: capi.Params, opts: capi.SolveOpts, lengths=(1.0, 1.0, 1.0
 
 
 def initial_state(req: capi.ServeRequest) -> np.ndarray:
-    """The initial state the server gives ``req`` (cfd_perturbed_freestream on
-    the same mesh), for running the same solve through the plain API."""
+    """The initial state the server gives ``req`` (cfd_initial_state on the
+    same mesh), for running the same solve through the plain API."""
     fb = np.array(list(req.face_bc), np.int32)
     h = C.c_void_p()
     capi.check(capi.lib.cfd_mesh_box(req.nx, req.ny, req.nz, req.lx, req.ly, req.lz, req.jitter, req.mesh_seed,
@@ -48,9 +48,9 @@ def initial_state(req: capi.ServeRequest) -> np.ndarray:
         sizes = np.zeros(7, np.int64)
         capi.check(capi.lib.cfd_mesh_sizes(h, capi.ptr(sizes)), "cfd_mesh_sizes")
         Q = np.empty((5, int(sizes[0] + sizes[1])))
-        p = req.params
-        capi.check(capi.lib.cfd_perturbed_freestream(h, p.gamma, p.mach, p.alpha_deg, p.beta_deg, req.noise,
-                                                     req.state_seed, capi.ptr(Q)), "cfd_perturbed_freestream")
+        noise = np.full(3, req.noise)
+        capi.check(capi.lib.cfd_initial_state(h, C.byref(req.params), capi.ptr(noise), req.state_seed, capi.ptr(Q)),
+                   "cfd_initial_state")
         return Q
     finally:
         capi.lib.cfd_mesh_free(h)

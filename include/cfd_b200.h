@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define CFD_ABI_VERSION 2
+#define CFD_ABI_VERSION 3
 
 /* ------------------------------------------------------------ status codes */
 #define CFD_OK                 0
@@ -111,6 +111,13 @@ typedef struct cfd_params {
     double cfl_max;          /* CFL_MAX                      */
     double venkat_k;         /* VENKAT_K_THRESHOLD           */
     int    residual_kernel;  /* 0: node-gather kernel (sliced-ELL), 1: shared-memory patch kernel */
+    /* Stiffened-gas constant p_inf / p_ref (0: the reference's ideal gas).
+     * p = (gamma - 1) rho e - gamma pinf, c^2 = gamma (p + pinf) / rho; the
+     * freestream keeps rho = 1, p = 1 and c = sqrt(gamma (1 + pinf)).  No
+     * counterpart in the reference (Euler3D/MPFLOW3D are ideal-gas only,
+     * EOS/src/EOS_IdealGas.c:73); at pinf = 0 every result is bit-identical
+     * to the ideal-gas path. */
+    double pinf;
 } cfd_params;
 
 /* Fills p with the defaults used by the reference parameter files of this
@@ -379,6 +386,11 @@ void cfd_mesh_free(cfd_mesh *m);
  * node); ghosts at freestream.  Q is SoA [5][nnode+nghost] (host). */
 int  cfd_perturbed_freestream(const cfd_mesh *m, double gamma, double mach, double alpha_deg, double beta_deg,
                               double noise, uint64_t seed, double *Q);
+/* The same for any gas of p (gamma, pinf, mach, alpha, beta): the freestream
+ * of p with density, velocity and pressure noise of their own amplitudes
+ * noise[0..2] (same hash streams as above); with pinf = 0 and three equal
+ * amplitudes it equals cfd_perturbed_freestream. */
+int  cfd_initial_state(const cfd_mesh *m, const cfd_params *p, const double noise[3], uint64_t seed, double *Q);
 
 /* ------------------------------------------------------------ serving loop
  * No counterpart in the reference (its drivers run one solve per process).

@@ -28,27 +28,30 @@ static void unit(const double *a, double *n, double *mag) {
 void orc_farfield(const orc_params *p, double out[8]) {
     double R = 1.0 / p->gamma, rho = 1.0, T = p->gamma, pr = R * rho * T;
     double a = p->alpha_deg * M_PI / 180.0, b = p->beta_deg * M_PI / 180.0;
-    double c = sqrt(p->gamma * R * T);
+    /* stiffened gas: c^2 = gamma (p + pinf) / rho, rho e = (p + gamma pinf) / (gamma - 1) */
+    double c = p->pinf != 0.0 ? sqrt(p->gamma * (pr + p->pinf) / rho) : sqrt(p->gamma * R * T);
     double u = p->mach * c * cos(a) * cos(b), v = p->mach * c * sin(a), w = p->mach * c * sin(b) * cos(a);
     double q2 = u * u + v * v + w * w;
     out[0] = rho; out[1] = u; out[2] = v; out[3] = w;
-    out[4] = pr / ((p->gamma - 1.0) * rho) + 0.5 * q2;
+    out[4] = (pr + p->gamma * p->pinf) / ((p->gamma - 1.0) * rho) + 0.5 * q2;
     out[5] = pr; out[6] = c; out[7] = p->mach;
 }
 
 typedef struct { double rho, u, v, w, et, p, ht, ubar, c; } face_t;
 
-/* Compute_EOS_Variables_Face, conservative branch (Material.cpp:216-248). */
-static void eos_face(const double *q, double nx, double ny, double nz, double g, face_t *s) {
+/* Compute_EOS_Variables_Face, conservative branch (Material.cpp:216-248),
+ * extended to the stiffened gas p = (g - 1) rho e - g pinf, c^2 = g (p + pinf) / rho
+ * (pinf = 0: the reference's ideal gas). */
+static void eos_face(const double *q, double nx, double ny, double nz, double g, double pinf, face_t *s) {
     s->rho = q[0];
     s->u = q[1] / s->rho;
     s->v = q[2] / s->rho;
     s->w = q[3] / s->rho;
     s->et = q[4] / s->rho;
     double q2 = s->u * s->u + s->v * s->v + s->w * s->w;
-    s->p = (g - 1.0) * (s->rho * s->et - 0.5 * s->rho * q2);
+    s->p = (g - 1.0) * (s->rho * s->et - 0.5 * s->rho * q2) - g * pinf;
     s->ht = (s->rho * s->et + s->p) / s->rho;
-    s->c = sqrt((g * s->p) / s->rho);
+    s->c = sqrt((g * (s->p + pinf)) / s->rho);
     s->ubar = s->u * nx + s->v * ny + s->w * nz;
 }
 
@@ -61,10 +64,10 @@ static int bc_state(const double *qI, const double *qG, const double *areav, int
     unit(areav, n, &mag);
     face_t I, G, O;
     double q0[5];
-    eos_face(qI, n[0], n[1], n[2], p->gamma, &I);
-    eos_face(qG, n[0], n[1], n[2], p->gamma, &G);
+    eos_face(qI, n[0], n[1], n[2], p->gamma, p->pinf, &I);
+    eos_face(qG, n[0], n[1], n[2], p->gamma, p->pinf, &G);
     for (int k = 0; k < 5; k++) q0[k] = 0.5 * (qI[k] + qG[k]);
-    eos_face(q0, n[0], n[1], n[2], p->gamma, &O);
+    eos_face(q0, n[0], n[1], n[2], p->gamma, p->pinf, &O);
     double l1 = O.ubar, l4 = l1 + O.c, l5 = l1 - O.c;
     double pb = inf[5], rb = inf[0], ub = inf[1], vb = inf[2], wb = inf[3];
     double outflow_p = 0.935 * inf[5];
@@ -90,10 +93,13 @@ static int bc_state(const double *qI, const double *qG, const double *areav, int
             break;
         default: inst = type; break;
     }
+    /* the preconditioned characteristic BC used with the low-Mach fix keeps the
+     * freestream at subsonic and supersonic outflow (BC.cpp:1229-1236) */
+    if (p->flux == 3 && (inst == 5 || inst == 7)) inst = 4;
     switch (inst) {
         case 0:
             pb = I.p + O.rho * O.c * I.ubar;
-            if (p->iteration < p->zpg_iteration && pb < 0.0) pb = I.p;
+            if (p->iteration < p->zpg_iteration && pb + p->pinf < 0.0) pb = I.p;
             rb = I.rho + (pb - I.p) / (O.c * O.c);
             ub = I.u - n[0] * (pb - I.p) / (O.rho * O.c);
             vb = I.v - n[1] * (pb - I.p) / (O.rho * O.c);
@@ -119,9 +125,9 @@ static int bc_state(const double *qI, const double *qG, const double *areav, int
         } break;
         default: break;
     }
-    if (pb < 0.0) st = st ? st : 1;
+    if (pb + p->pinf < 0.0) st = st ? st : 1;
     double et = ub * ub + vb * vb + wb * wb;
-    et = pb / ((p->gamma - 1.0) * rb) + 0.5 * et;   /* Get_TotalEnergy, Material.cpp:1012-1040 */
+    et = (pb + p->gamma * p->pinf) / ((p->gamma - 1.0) * rb) + 0.5 * et;   /* Get_TotalEnergy, Material.cpp:1012-1040 */
     qB[0] = rb; qB[1] = rb * ub; qB[2] = rb * vb; qB[3] = rb * wb; qB[4] = rb * et;
     return st;
 }
@@ -156,8 +162,8 @@ static double roe(const double *qL, const double *qR, const double *n, double ar
                   double *conv, double *diss, double lam[3]) {
     face_t L, R;
     double g = p->gamma;
-    eos_face(qL, n[0], n[1], n[2], g, &L);
-    eos_face(qR, n[0], n[1], n[2], g, &R);
+    eos_face(qL, n[0], n[1], n[2], g, p->pinf, &L);
+    eos_face(qR, n[0], n[1], n[2], g, p->pinf, &R);
     double FL[5], FR[5];
     FL[0] = L.rho * L.ubar; FL[1] = L.u * FL[0] + L.p * n[0]; FL[2] = L.v * FL[0] + L.p * n[1];
     FL[3] = L.w * FL[0] + L.p * n[2]; FL[4] = L.ht * FL[0];
@@ -179,6 +185,25 @@ static double roe(const double *qL, const double *qR, const double *n, double ar
     double dQ[5] = {R.rho - L.rho, R.u - L.u, R.v - L.v, R.w - L.w, R.p - L.p};
     double E0 = E[0], E1 = E[1], E2 = E[2];
     double dU = dQ[1] * n[0] + dQ[2] * n[1] + dQ[3] * n[2];
+    if (p->flux == 3) {
+        /* low-Mach fix (Compute_Flux_Roe_LMFIX, FluxTest.cpp:2943-3005): the normal velocity
+         * jump times min(1, (|u.n| + |u.t1| + |u.t2|) / c); t1 in the face plane from the
+         * largest normal component, t2 = t1 x n, both normalised */
+        double nmax = fabs(n[0]), t1[3] = {1.0, 1.0, 1.0}, t2[3];
+        int mc = 0;
+        if (nmax < fabs(n[1])) { nmax = fabs(n[1]); mc = 1; }
+        if (nmax < fabs(n[2])) { nmax = fabs(n[2]); mc = 2; }
+        t1[mc] = -(n[(mc + 1) % 3] + n[(mc + 2) % 3]) / n[mc];
+        double m1 = sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+        if (m1 > 1.0e-20) for (int k = 0; k < 3; k++) t1[k] /= m1;
+        t2[0] = t1[1] * n[2] - t1[2] * n[1];
+        t2[1] = -t1[0] * n[2] + t1[2] * n[0];
+        t2[2] = t1[0] * n[1] - t1[1] * n[0];
+        double m2 = sqrt(t2[0] * t2[0] + t2[1] * t2[1] + t2[2] * t2[2]);
+        if (m2 > 1.0e-20) for (int k = 0; k < 3; k++) t2[k] /= m2;
+        double mach = (fabs(ub) + fabs(u * t1[0] + v * t1[1] + w * t1[2]) + fabs(u * t2[0] + v * t2[1] + w * t2[2])) / c;
+        dU = dmin(mach, 1.0) * dU;
+    }
     double dw[5];
     dw[0] = E0 * dQ[0] + (E1 + E2 - 2.0 * E0) * dQ[4] / (2.0 * c * c) + rho * (E1 - E2) * dU / (2.0 * c);
     for (int k = 1; k < 4; k++)
@@ -198,8 +223,8 @@ static double hllc(const double *qL, const double *qR, const double *n, double a
                    double *conv, double *diss) {
     face_t L, R;
     double g = p->gamma;
-    eos_face(qL, n[0], n[1], n[2], g, &L);
-    eos_face(qR, n[0], n[1], n[2], g, &R);
+    eos_face(qL, n[0], n[1], n[2], g, p->pinf, &L);
+    eos_face(qR, n[0], n[1], n[2], g, p->pinf, &R);
     double rho = sqrt(R.rho * L.rho), sigma = rho / (L.rho + rho);
     double u = L.u + sigma * (R.u - L.u), v = L.v + sigma * (R.v - L.v), w = L.w + sigma * (R.w - L.w);
     double ht = L.ht + sigma * (R.ht - L.ht);
@@ -239,8 +264,8 @@ static double ausmp(const double *qL, const double *qR, const double *n, double 
                     double *conv, double *diss) {
     face_t L, R;
     double g = p->gamma;
-    eos_face(qL, n[0], n[1], n[2], g, &L);
-    eos_face(qR, n[0], n[1], n[2], g, &R);
+    eos_face(qL, n[0], n[1], n[2], g, p->pinf, &L);
+    eos_face(qR, n[0], n[1], n[2], g, p->pinf, &R);
     double k = 2.0 * (g - 1.0) / (g + 1.0);
     double csL = sqrt(k * L.ht), csR = sqrt(k * R.ht);
     double c12 = dmin(csL * csL / dmax(csL, L.ubar), csR * csR / dmax(csR, -R.ubar));
@@ -460,13 +485,14 @@ void orc_limiter(const orc_mesh *m, const orc_params *p, const double *Q, const 
                 double gr = grad[IDX(3 * v, i, nn)] * r[0] + grad[IDX(3 * v + 1, i, nn)] * r[1] + grad[IDX(3 * v + 2, i, nn)] * r[2];
                 q[v] = qc[v] + ph[v] * (frac * (Q[IDX(v, j, ld)] - qc[v]) + (1.0 - frac) * gr);
             }
-            double pc = (p->gamma - 1.0) * (q[4] - (0.5 / q[0]) * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]));
+            /* p < 0 (Limiters.cpp:296-301); for the stiffened gas p + pinf < 0 */
+            double pc = (p->gamma - 1.0) * ((q[4] - p->pinf) - (0.5 / q[0]) * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]));
             if (pc < 0.0)
                 for (int v = 0; v < 5; v++) ph[v] = 0.0;
         }
         for (int v = 0; v < 5; v++) phi[IDX(v, i, nn)] = ph[v];
     }
-    if (p->flux != 0) return;
+    if (p->flux != 0 && p->flux != 3) return;
     for (int i = 0; i < nn; i++) {
         for (int k = m->ia[i]; k < m->ia[i + 1]; k++) {
             int j = m->ja[k];
@@ -481,13 +507,14 @@ void orc_limiter(const orc_mesh *m, const orc_params *p, const double *Q, const 
             }
             /* Compute_RoeVariables (Roe_Fluxes.cpp:3609-3633) */
             face_t A, B;
-            eos_face(qa, 0, 0, 0, p->gamma, &A);
-            eos_face(qb, 0, 0, 0, p->gamma, &B);
+            eos_face(qa, 0, 0, 0, p->gamma, p->pinf, &A);
+            eos_face(qb, 0, 0, 0, p->gamma, p->pinf, &B);
             double rho = sqrt(B.rho * A.rho), sg = rho / (A.rho + rho);
             double u = A.u + sg * (B.u - A.u), v = A.v + sg * (B.v - A.v), w = A.w + sg * (B.w - A.w);
             double ht = A.ht + sg * (B.ht - A.ht);
             double qr[5] = {rho, rho * u, rho * v, rho * w,
                             (rho / p->gamma) * (ht + 0.5 * (p->gamma - 1.0) * (u * u + v * v + w * w))};
+            /* for the stiffened gas this is p + pinf of the Roe state (c^2 = (g - 1) h) */
             double pr = (p->gamma - 1.0) * (qr[4] - (0.5 / qr[0]) * (qr[1] * qr[1] + qr[2] * qr[2] + qr[3] * qr[3]));
             if (pr < 0.0)
                 for (int v2 = 0; v2 < 5; v2++) { phi[IDX(v2, i, nn)] = 0.0; phi[IDX(v2, j, nn)] = 0.0; }
@@ -518,9 +545,9 @@ long orc_block_pattern(const orc_mesh *m, int *IA, int *JA, int *IAU) {
 }
 
 /* ConservativeEulerFluxJacobian (Euler3D/src/CompressibleUtils.cpp:558-609). */
-static void flux_jac(const double *q, const double *n, double g, double J[5][5]) {
+static void flux_jac(const double *q, const double *n, double g, double pinf, double J[5][5]) {
     double rho = q[0], u = q[1] / rho, v = q[2] / rho, w = q[3] / rho, rhoet = q[4];
-    double ek = 0.5 * (u * u + v * v + w * w), p = (g - 1.0) * (rhoet - rho * ek), ht = (rhoet + p) / rho;
+    double ek = 0.5 * (u * u + v * v + w * w), p = (g - 1.0) * (rhoet - rho * ek) - g * pinf, ht = (rhoet + p) / rho;
     double ub = u * n[0] + v * n[1] + w * n[2];
     double nx = n[0], ny = n[1], nz = n[2];
     J[0][0] = 0.0; J[1][0] = (g - 1.0) * ek * nx - u * ub; J[2][0] = (g - 1.0) * ek * ny - v * ub;
@@ -546,8 +573,8 @@ static void mm5(double A[5][5], double B[5][5], double C[5][5]) {
 static void roe_absA(const double *qL, const double *qR, const double *n, const orc_params *p, double A[5][5]) {
     face_t L, R;
     double g = p->gamma;
-    eos_face(qL, n[0], n[1], n[2], g, &L);
-    eos_face(qR, n[0], n[1], n[2], g, &R);
+    eos_face(qL, n[0], n[1], n[2], g, p->pinf, &L);
+    eos_face(qR, n[0], n[1], n[2], g, p->pinf, &R);
     double rho = sqrt(R.rho * L.rho), sigma = rho / (L.rho + rho);
     double u = L.u + sigma * (R.u - L.u), v = L.v + sigma * (R.v - L.v), w = L.w + sigma * (R.w - L.w);
     double ht = L.ht + sigma * (R.ht - L.ht);
@@ -598,8 +625,8 @@ void orc_jacobian(const orc_mesh *m, const orc_params *p, const double *Q, const
             double n[3], area, qL[5], qR[5], JL[5][5], JR[5][5], Ab[5][5];
             unit(ea + 3 * (size_t)e, n, &area);
             for (int k = 0; k < 5; k++) { qL[k] = Q[IDX(k, L, ld)]; qR[k] = Q[IDX(k, R, ld)]; }
-            flux_jac(qL, n, p->gamma, JL);
-            flux_jac(qR, n, p->gamma, JR);
+            flux_jac(qL, n, p->gamma, p->pinf, JL);
+            flux_jac(qR, n, p->gamma, p->pinf, JR);
             roe_absA(qL, qR, n, p, Ab);
             double *dL = A + 25 * (size_t)IAU[L];
             if (pass == 1) {

@@ -17,6 +17,7 @@ typedef struct {
     double gamma, mach, alpha_deg, beta_deg, cfl, venkat_k;
     int flux, order, limiter, limiter_order, limiter_smooth, entropy_fix;
     int global_time, ls_weight, gradient, iteration, zpg_iteration;
+    double pinf; /* stiffened-gas constant (0: ideal gas) */
 } orc_params;
 
 typedef struct {

@@ -13,7 +13,7 @@ def make_case(n=20, seed=11, rcm=False, cfg=None, noise=0.01, mesh=None):
     cfg = dict(CFG1 if cfg is None else cfg)
     m = mesh if mesh is not None else box_mesh(n, jitter=0.15, seed=seed, rcm=rcm)
     Q = perturbed_freestream(m, cfg.get("gamma", 1.4), cfg.get("mach", 0.5), cfg.get("alpha_deg", 2.0),
-                             cfg.get("beta_deg", 0.0), noise=noise, seed=seed + 1)
+                             cfg.get("beta_deg", 0.0), noise=noise, seed=seed + 1, pinf=cfg.get("pinf", 0.0))
     return m, cfg, Q
 
 

@@ -161,3 +161,105 @@ def test_block_lusgs_restatement_is_the_reference(ref_available):
     X, rms = restatement.Session(m, cfg).block_lusgs(A, B, 4)
     np.testing.assert_array_equal(X, ref["X"])
     assert rms == ref["lusgs_rms"][0]
+
+
+@pytest.mark.parametrize("face_bc,mach", [((1, 1, 1, 1, 1, 1), 0.1), ((2, 3, 0, 0, 0, 0), 0.2)])
+def test_low_mach_fix_restatement_matches_reference(ref_available, face_bc, mach):
+    """Flux 3 of the restatement (Roe with the low-Mach fix and the
+    preconditioned characteristic BC) against Compute_Flux_Roe_LMFIX and
+    Compute_Precondition_Characteristic_BoundaryCondition of the reference,
+    second order with the Venkatakrishnan limiter."""
+    from cfdsolutions_b200 import box_mesh
+    cfg = dict(CFG1, flux_scheme=3, order=1, limiter=1, limiter_order=1, venkat_k=5.0, mach=mach, mach_min=mach,
+               alpha_deg=0.0 if face_bc[0] == 2 else 2.0)
+    m = box_mesh(8, jitter=0.15, seed=41, face_bc=face_bc)
+    _, cfg, Q = make_case(cfg=cfg, mesh=m, seed=41)
+    ref = refharness.run(m, cfg, Q, [("begin", 0), ("gradient", 0), ("limiter",), ("bc", 0), ("get", "state"),
+                                     ("residual", 1), ("get", "residual"), ("get", "limiters"), ("deltat", 0),
+                                     ("get", "deltat")])
+    s = restatement.Session(m, cfg)
+    g = s.gradient(Q)
+    phi = s.limiter(Q, g)
+    Qb = s.apply_bc(Q)
+    conv, diss, dts, _ = s.residual(Qb, g, phi)
+    dt, _ = s.deltat(dts)
+    assert np.abs(phi - ref["limiters"]).max() <= 1e-13
+    assert relerr_rows(Qb, ref["state"]) <= 1e-15
+    assert relerr_rows(conv, ref["conv"]) <= TOL
+    assert relerr_rows(diss, ref["diss"]) <= TOL
+    assert relerr(dt, ref["deltat"]) <= TOL
+
+
+def _two_node_mesh(areav):
+    """One interior edge 0 -> 1 with area vector ``areav``, no boundary."""
+    from cfdsolutions_b200.mesh import Mesh
+    z2, zb = np.zeros((0, 2), np.int32), np.zeros((0, 3))
+    return Mesh(nnode=2, nghost=0, edge_nodes=np.array([[0, 1]], np.int32), edge_areav=np.array([areav], float),
+                bedge_nodes=z2, bedge_areav=zb, bedge_type=np.zeros(0, np.int32), cvol=np.ones(2),
+                coords=np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0]]), n2n_ia=np.array([0, 1, 2], np.int32),
+                n2n_ja=np.array([1, 0], np.int32))
+
+
+def _stiffened_flux(q, a, gamma, pinf):
+    """F(q).a of the Euler equations with p = (gamma - 1)(rho et - rho q^2 / 2) - gamma pinf."""
+    rho, u = q[0], q[1:4] / q[0]
+    p = (gamma - 1.0) * (q[4] - 0.5 * rho * (u @ u)) - gamma * pinf
+    un = u @ a
+    return np.r_[rho * un, rho * u * un + p * a, (q[4] + p) * un]
+
+
+@pytest.mark.parametrize("flux", [0, 1, 2, 3])
+@pytest.mark.parametrize("pinf", [0.0, 3.0, 6000.0])
+def test_stiffened_gas_fluxes_upwind_when_supersonic(flux, pinf):
+    """Stiffened-gas algebra of every flux family, with no reference to pin
+    it: when all waves run one way the Roe flux (the Roe property A dQ = dF
+    must hold for the stiffened-gas averages), HLLC and AUSM+ all reduce to
+    the upwind state's exact flux F(q).a."""
+    gamma = 4.4
+    a = np.array([0.3, -0.2, 0.25])
+    n = a / np.linalg.norm(a)
+    c_ref = np.sqrt(gamma * (1.0 + pinf))
+
+    def state(rho, p, vel):
+        return np.r_[rho, rho * vel, (p + gamma * pinf) / (gamma - 1.0) + 0.5 * rho * (vel @ vel)]
+
+    t = np.cross(n, [0.0, 0.0, 1.0])
+    qa = state(1.0, 1.0, 3.0 * c_ref * n + 0.1 * c_ref * t)
+    qb = state(1.1, 1.3, 2.6 * c_ref * n - 0.2 * c_ref * t)
+    cfg = dict(CFG1, flux_scheme=flux, gamma=gamma, pinf=pinf)
+    for sign in (1.0, -1.0):
+        m = _two_node_mesh(sign * a)
+        Q = np.stack([qa, qb], axis=1)
+        conv, diss, _, _ = restatement.Session(m, cfg).residual(Q)
+        F = conv[:, 0] + diss[:, 0]
+        # with the area vector reversed both states move against it: node 1 is upwind
+        up = qa if sign > 0 else qb
+        exact = _stiffened_flux(up, sign * a, gamma, pinf)
+        # round-off scale: the flux plus the pressure cancellation (gamma pinf) in p
+        scale = np.abs(exact).max() + gamma * pinf * np.abs(a).max()
+        assert np.abs(F - exact).max() <= 1e-13 * scale, (F, exact)
+        np.testing.assert_allclose(conv[:, 1] + diss[:, 1], -F, rtol=0, atol=0)
+
+
+@pytest.mark.parametrize("face_bc,flux", [((1, 1, 1, 1, 1, 1), 0), ((1, 1, 1, 1, 1, 1), 1), ((1, 1, 1, 1, 1, 1), 2),
+                                          ((1, 1, 1, 1, 1, 1), 3), ((2, 3, 0, 0, 0, 0), 3)])
+def test_stiffened_gas_freestream_preserved(face_bc, flux):
+    """A uniform stiffened-gas freestream (gamma 4.4, pinf 6000, u ~ c/160)
+    is a steady state: ghost states are the freestream and the residual
+    vanishes to round-off of the energy flux scale.  The channel (inflow,
+    outflow, slip walls) uses the low-Mach fix, whose outflow keeps the
+    freestream (without it the subsonic outflow imposes 0.935 p)."""
+    from cfdsolutions_b200 import box_mesh
+    m = box_mesh((8, 4, 4), lengths=(2.0, 1.0, 1.0), jitter=0.1, seed=5, face_bc=face_bc)
+    cfg = dict(CFG1, flux_scheme=flux, gamma=4.4, pinf=6000.0, mach=0.0062, mach_min=0.0062,
+               alpha_deg=0.0 if face_bc[0] == 2 else 2.0)
+    _, cfg, Q0 = make_case(mesh=m, cfg=cfg, noise=0.0)
+    s = restatement.Session(m, cfg)
+    Qb = s.apply_bc(Q0)
+    np.testing.assert_allclose(Qb, Q0, rtol=1e-14, atol=0)
+    conv, diss, _, _ = s.residual(Qb)
+    amax = np.abs(m.edge_areav).max()
+    for v in range(5):
+        # each equation against its own flux scale: rho u, rho u^2 + p, (rho et + p) u
+        fscale = np.abs(Qb[v]).max() * np.abs(Qb[1]).max() / Qb[0].min() + (1.0 if 1 <= v <= 3 else 0.0)
+        assert np.abs(conv[v] + diss[v]).max() <= 1e-12 * fscale * amax * 20
