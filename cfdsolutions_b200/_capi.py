@@ -18,7 +18,9 @@ ERRORS = {
     -1: "CFD_ERR_ARG", -2: "CFD_ERR_MESH", -3: "CFD_ERR_CUDA", -4: "CFD_ERR_IO", -5: "CFD_ERR_STATE",
     -6: "CFD_ERR_NUMERIC", -7: "CFD_ERR_NOT_CONVERGED", -8: "CFD_ERR_UNSUPPORTED", -9: "CFD_ERR_RANGE",
 }
-FLUX_ROE, FLUX_HLLC, FLUX_AUSM, FLUX_ROE_LMFIX = 0, 1, 2, 3
+FLUX_ROE, FLUX_HLLC, FLUX_AUSM, FLUX_ROE_LMFIX, FLUX_ROE_PRECOND = 0, 1, 2, 3, 4
+PRECOND_BTW, PRECOND_ERIKSSON, PRECOND_TURKEL = 2, 3, 5
+PRECOND_LOCAL, PRECOND_GLOBAL, PRECOND_URLOCAL = 0, 1, 2
 ORDER_FIRST, ORDER_SECOND = 0, 1
 LIMITER_NONE, LIMITER_BJ, LIMITER_VENKAT = -1, 0, 1
 GRAD_LSQ, GRAD_GG = 0, 1
@@ -44,7 +46,8 @@ class Params(C.Structure):
         ("global_time", C.c_int), ("cfl_ramp", C.c_int), ("mach_ramp", C.c_int), ("zpg_iteration", C.c_int),
         ("gamma", C.c_double), ("mach", C.c_double), ("mach_min", C.c_double), ("alpha_deg", C.c_double),
         ("beta_deg", C.c_double), ("cfl_min", C.c_double), ("cfl_max", C.c_double), ("venkat_k", C.c_double),
-        ("residual_kernel", C.c_int), ("pinf", C.c_double),
+        ("residual_kernel", C.c_int), ("pinf", C.c_double), ("precond_method", C.c_int), ("precond_type", C.c_int),
+        ("precond_mach", C.c_double), ("outflow_pressure", C.c_double),
     ]
 
 

@@ -50,7 +50,8 @@ __global__ void k_apply_bc(int nbedge, int64_t ldq, double *__restrict__ Q, cons
         qI[k] = Q[k * ldq + nd.x];
         qG[k] = Q[k * ldq + nd.y];
     }
-    int st = characteristic_bc(qI, qG, g.x, g.y, g.z, btype[b], f, qB);
+    const int st = f.flux == CFD_FLUX_ROE_PRECOND ? precond_characteristic_bc(qI, qG, g.x, g.y, g.z, btype[b], f, qB)
+                                                  : characteristic_bc(qI, qG, g.x, g.y, g.z, btype[b], f, qB);
     if (st) atomicOr(err, st == 1 ? ERR_BC_NEG_PRESSURE : ERR_BC_UNCLASSIFIED);
 #pragma unroll
     for (int k = 0; k < 5; k++) Q[k * ldq + nd.y] = qB[k];
@@ -467,7 +468,7 @@ __global__ void k_add_diss(int64_t n, const double *__restrict__ a, const double
 //   A[L,R] = dFdR = 0.5 (J(Q_R) - |A|) area,  A[R,L] = -dFdL = -0.5 (J(Q_L) + |A|) area.
 // Every off-diagonal slot belongs to exactly one edge, so no zeroing and no
 // accumulation is needed.
-template <typename TA>
+template <typename TA, bool PC>
 __global__ void __launch_bounds__(128) k_jac_edges(int nedge, int64_t ldq, const double *__restrict__ Q,
                                                    const int2 *__restrict__ en, const double4 *__restrict__ eg,
                                                    const int2 *__restrict__ eslot, Flow f, double *__restrict__ A64,
@@ -483,7 +484,8 @@ __global__ void __launch_bounds__(128) k_jac_edges(int nedge, int64_t ldq, const
         qR[v] = Q[v * ldq + nd.y];
     }
     double Ab[25], J[25];
-    roe_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
+    if (PC) pc_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
+    else roe_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
     const int2 sl = eslot[e];
     const double ha = 0.5 * g.w;
     euler_flux_jacobian(qR, g.x, g.y, g.z, f.gamma, f.gpinf, J);
@@ -505,7 +507,7 @@ __global__ void __launch_bounds__(128) k_jac_edges(int nedge, int64_t ldq, const
 // Diagonal blocks and right-hand side, one thread per row:
 //   A[i,i] = V_i/dt_i I - sum_j A[j,i] + sum_b 0.5 (J(Q_i) + |A|)_b area_b
 //   B_i    = -(Res_i [+ Res_Diss_i])
-template <typename TA>
+template <typename TA, bool PC>
 __global__ void __launch_bounds__(128) k_jac_rows(
     int nnode, int64_t ldq, const double *__restrict__ Q, const int *__restrict__ IA, const int *__restrict__ IAU,
     const int *__restrict__ tslot, const int *__restrict__ n2b_ptr, const int *__restrict__ n2b,
@@ -517,8 +519,18 @@ __global__ void __launch_bounds__(128) k_jac_rows(
     if (i >= nnode) return;
     double D[25];
     const double vd = add_time ? vol[i] / dt[i] : 0.0;
+    if (PC && add_time) {
+        // preconditioned pseudo-time term (V/dt) Cinv (Roe_Jacobian.cpp:241-264)
+        double qi[5];
 #pragma unroll
-    for (int k = 0; k < 25; k++) D[k] = (k % 6 == 0) ? vd : 0.0;
+        for (int v = 0; v < 5; v++) qi[v] = Q[v * ldq + i];
+        pc_node_cinv(qi, f, D);
+#pragma unroll
+        for (int k = 0; k < 25; k++) D[k] *= vd;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 25; k++) D[k] = (k % 6 == 0) ? vd : 0.0;
+    }
     const int dg = IAU[i];
     for (int k = IA[i]; k < IA[i + 1]; k++) {
         if (k == dg) continue;
@@ -542,7 +554,8 @@ __global__ void __launch_bounds__(128) k_jac_rows(
             qL[v] = Q[v * ldq + nd.x];
             qR[v] = Q[v * ldq + nd.y];
         }
-        roe_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
+        if (PC) pc_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
+        else roe_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
         euler_flux_jacobian(qL, g.x, g.y, g.z, f.gamma, f.gpinf, J);
         const double ha = 0.5 * g.w;
 #pragma unroll
@@ -559,6 +572,20 @@ __global__ void __launch_bounds__(128) k_jac_rows(
         if (include_diss) r += resd[v * (int64_t)nnode + i];
         B[(int64_t)i * 5 + v] = -r;
     }
+}
+
+// Edge blocks then diagonal blocks and right-hand side of the approximate
+// Roe Jacobian (PC: the preconditioned Roe's dissipation and pseudo-time term).
+template <typename TA, bool PC>
+static void launch_jacobian(cfd_ctx *c, int add_time, int include_diss, double *A64, TA *Alow) {
+    const int ge = grid_for(c->nedge, 128), gr = grid_for(c->nnode, 128);
+    if (c->nedge)
+        k_jac_edges<TA, PC><<<ge, 128, 0, c->stream>>>(c->nedge, c->ldq, c->Q.p, c->edge_nodes.p, c->edge_geo.p,
+                                                       c->eslot.p, c->flow, A64, Alow);
+    k_jac_rows<TA, PC><<<gr, 128, 0, c->stream>>>(c->nnode, c->ldq, c->Q.p, c->IA.p, c->IAU.p, c->tslot.p,
+                                                  c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p,
+                                                  c->cvol.p, c->dt.p, c->res.p, c->resd.p, add_time, include_diss,
+                                                  c->flow, A64, Alow, c->B.p);
 }
 
 // ---- block Gauss-Seidel (MC_Iterative_Block_LU_Jacobi_CRS,
@@ -738,6 +765,10 @@ static void compute_flow(cfd_ctx *c, int iteration) {
     f.venkat_eps_k3 = pow(p.venkat_k, 3.0);
     f.flux = p.flux_scheme;
     f.lmfix = p.flux_scheme == CFD_FLUX_ROE_LMFIX ? 1 : 0;
+    f.pc_method = p.precond_method;
+    f.pc_type = p.precond_type;
+    f.pc_mach = p.precond_mach;
+    f.pc_outflow_p = p.outflow_pressure != 0.0 ? p.outflow_pressure : pr;
     f.order = p.order;
     f.limiter = p.limiter;
     f.limiter_smooth = p.limiter_smooth;
@@ -1001,11 +1032,21 @@ int cfd_set_stream(cfd_ctx *c, void *stream) {
 
 int cfd_set_params(cfd_ctx *c, const cfd_params *p) {
     if (!c || !p) { set_error("cfd_set_params: NULL"); return CFD_ERR_ARG; }
-    if (p->flux_scheme < CFD_FLUX_ROE || p->flux_scheme > CFD_FLUX_ROE_LMFIX) {
+    if (p->flux_scheme < CFD_FLUX_ROE || p->flux_scheme > CFD_FLUX_ROE_PRECOND) {
         set_error("cfd_set_params: invalid flux scheme %d", p->flux_scheme);
         return CFD_ERR_ARG;
     }
     if (!(p->gamma > 1.0)) { set_error("cfd_set_params: gamma must be > 1"); return CFD_ERR_ARG; }
+    if (p->flux_scheme == CFD_FLUX_ROE_PRECOND) {
+        const int m = p->precond_method, t = p->precond_type;
+        if ((m != CFD_PRECOND_BTW && m != CFD_PRECOND_ERIKSSON && m != CFD_PRECOND_TURKEL) ||
+            (t != CFD_PRECOND_LOCAL && t != CFD_PRECOND_GLOBAL && t != CFD_PRECOND_URLOCAL) ||
+            (t != CFD_PRECOND_URLOCAL && !(p->precond_mach > 0.0))) {
+            set_error("cfd_set_params: preconditioned Roe needs precond_method BTW/ERIKSSON/TURKEL, "
+                      "precond_type LOCAL/GLOBAL/URLOCAL and precond_mach > 0");
+            return CFD_ERR_ARG;
+        }
+    }
     if (!(p->pinf >= 0.0 && p->pinf < 1.0e300)) {
         set_error("cfd_set_params: pinf must be finite and >= 0");
         return CFD_ERR_ARG;
@@ -1418,6 +1459,8 @@ int cfd_residual(cfd_ctx *c, int add_time) {
         case 5: return residual_with_fix<CFD_FLUX_AUSM, true>(c, add_time);
         case 6: return residual_with_fix<CFD_FLUX_ROE_LMFIX, false>(c, add_time);
         case 7: return residual_with_fix<CFD_FLUX_ROE_LMFIX, true>(c, add_time);
+        case 8: return residual_with_fix<CFD_FLUX_ROE_PRECOND, false>(c, add_time);
+        case 9: return residual_with_fix<CFD_FLUX_ROE_PRECOND, true>(c, add_time);
         default: set_error("cfd_residual: bad flux scheme"); return CFD_ERR_ARG;
     }
 }
@@ -1469,36 +1512,18 @@ int cfd_jacobian(cfd_ctx *c, int add_time, int include_diss, int precision) {
     c->a_precision = precision;
     c->a64_valid = !low_only;
     double *A64 = low_only ? nullptr : c->A64.p;
-    const int ge = grid_for(c->nedge, 128), gr = grid_for(c->nnode, 128);
+    const bool pc = c->params.flux_scheme == CFD_FLUX_ROE_PRECOND;
     if (precision == CFD_PREC_FP32) {
         CFD_CUDA(c->A32.alloc((size_t)c->nnzb * 25));
-        if (c->nedge)
-            k_jac_edges<float><<<ge, 128, 0, c->stream>>>(c->nedge, c->ldq, c->Q.p, c->edge_nodes.p, c->edge_geo.p,
-                                                          c->eslot.p, c->flow, A64, c->A32.p);
-        CFD_LAUNCH_CHECK();
-        k_jac_rows<float><<<gr, 128, 0, c->stream>>>(c->nnode, c->ldq, c->Q.p, c->IA.p, c->IAU.p, c->tslot.p,
-                                                     c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p,
-                                                     c->cvol.p, c->dt.p, c->res.p, c->resd.p, add_time, include_diss,
-                                                     c->flow, A64, c->A32.p, c->B.p);
+        if (pc) launch_jacobian<float, true>(c, add_time, include_diss, A64, c->A32.p);
+        else launch_jacobian<float, false>(c, add_time, include_diss, A64, c->A32.p);
     } else if (precision == CFD_PREC_BF16) {
         CFD_CUDA(c->A16.alloc((size_t)c->nnzb * 25));
-        if (c->nedge)
-            k_jac_edges<uint16_t><<<ge, 128, 0, c->stream>>>(c->nedge, c->ldq, c->Q.p, c->edge_nodes.p,
-                                                             c->edge_geo.p, c->eslot.p, c->flow, A64, c->A16.p);
-        CFD_LAUNCH_CHECK();
-        k_jac_rows<uint16_t><<<gr, 128, 0, c->stream>>>(c->nnode, c->ldq, c->Q.p, c->IA.p, c->IAU.p, c->tslot.p,
-                                                        c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p,
-                                                        c->cvol.p, c->dt.p, c->res.p, c->resd.p, add_time,
-                                                        include_diss, c->flow, A64, c->A16.p, c->B.p);
+        if (pc) launch_jacobian<uint16_t, true>(c, add_time, include_diss, A64, c->A16.p);
+        else launch_jacobian<uint16_t, false>(c, add_time, include_diss, A64, c->A16.p);
     } else {
-        if (c->nedge)
-            k_jac_edges<float><<<ge, 128, 0, c->stream>>>(c->nedge, c->ldq, c->Q.p, c->edge_nodes.p, c->edge_geo.p,
-                                                          c->eslot.p, c->flow, A64, (float *)nullptr);
-        CFD_LAUNCH_CHECK();
-        k_jac_rows<float><<<gr, 128, 0, c->stream>>>(c->nnode, c->ldq, c->Q.p, c->IA.p, c->IAU.p, c->tslot.p,
-                                                     c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p,
-                                                     c->cvol.p, c->dt.p, c->res.p, c->resd.p, add_time, include_diss,
-                                                     c->flow, A64, (float *)nullptr, c->B.p);
+        if (pc) launch_jacobian<float, true>(c, add_time, include_diss, A64, (float *)nullptr);
+        else launch_jacobian<float, false>(c, add_time, include_diss, A64, (float *)nullptr);
     }
     CFD_LAUNCH_CHECK();
     c->has_system = true;

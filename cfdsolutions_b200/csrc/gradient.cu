@@ -345,7 +345,7 @@ int cfd_limiter(cfd_ctx *c) {
     k_venkat<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p, c->deg.p, c->xyz.p, c->grad.p,
                                                         c->cvol.p, c->flow, c->phi.p, c->roeflag.p);
     CFD_LAUNCH_CHECK();
-    if (c->params.flux_scheme == CFD_FLUX_ROE || c->params.flux_scheme == CFD_FLUX_ROE_LMFIX) {
+    if (is_roe_flux(c->params.flux_scheme)) {
         // The Roe-average pressure fix (Limiters.cpp:61-110) needs the
         // reconstructed face states the residual forms anyway: it is done by
         // the next cfd_residual (or by roe_fix_standalone when the limiters

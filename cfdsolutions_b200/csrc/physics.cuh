@@ -8,6 +8,8 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/cfd_b200.h"
+
 namespace cfd {
 
 // Flow constants of one iteration (ComputeFarFieldCondition,
@@ -26,6 +28,10 @@ struct Flow {
     int entropy_fix;
     int zpg_iteration, iteration;
     int lmfix;            // Roe low-Mach fix and the preconditioned characteristic BC (CFD_FLUX_ROE_LMFIX)
+    // preconditioned Roe (CFD_FLUX_ROE_PRECOND): CFD_PRECOND_* method and type,
+    // reference Mach and the pressure its subsonic outflow imposes
+    int pc_method, pc_type;
+    double pc_mach, pc_outflow_p;
 };
 
 struct Face {
@@ -331,6 +337,358 @@ __device__ __forceinline__ void roe_abs_jacobian(const double qL[5], const doubl
         Aout[15 + j] = w * d0 + rho * d3;
         Aout[20 + j] = (phi / f.gm1) * d0 + rho * (u * d1 + v * d2 + w * d3) + d4 / f.gm1;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Low-Mach preconditioned Roe of the Turkel family (MPFLOW3D:
+// Compute_Flux_Roe_Precondition_Turkel, MPFLOW3D/src/Roe_Fluxes.cpp:2043-2526;
+// Compute_Dissipation_Matrix_Roe_Precondition_Turkel, :3440-3810;
+// Compute_Transformed_Preconditioner_Matrix_Roe_Turkel, :261-441).  The
+// preconditioner K acts on (rho, u, v, w, p):
+//   K = I except K[0][4] = (delta - 1)/c^2, K[1..3][4] = -alpha (u,v,w)/(rho c^2), K[4][4] = beta
+// with beta = Mr^2 and (alpha, delta) = (0, 1) BTW, (0, beta) Eriksson,
+// (0.4, beta) Turkel.  The edge dissipation is Mop Kinv R |Lambda| L Mpr dQ
+// with L, R the left/right eigenvectors of K A at the Roe average and the
+// eigenvalues |u.n|, |zp u.n +- c'|, zp = (1 + beta - alpha)/2,
+// c'^2 = beta (c^2 - (u.n)^2) + zp^2 (u.n)^2.  Conservative solution
+// variables, pressure smoothing off (PRECOND_SMOOTH NO).
+
+// beta = Mr^2 for CFD_PRECOND_LOCAL / GLOBAL / URLOCAL (Roe_Fluxes.cpp:2225-2248)
+__device__ __forceinline__ double pc_beta(const Flow &f, double mach, double mach_max) {
+    double b;
+    if (f.pc_type == CFD_PRECOND_LOCAL) {
+        const double M = fmax(mach, mach_max), G = f.pc_mach;
+        b = M < G ? 0.5 * (M * M) / (G * G) - M / G + 1.0 : 0.5;
+        b = fmin(1.0, b * (sqrt(M * G) + M));
+    } else if (f.pc_type == CFD_PRECOND_URLOCAL) {
+        b = fmin(1.0, mach);
+    } else {
+        b = fmin(1.0, f.pc_mach);
+    }
+    return b * b;
+}
+
+struct PcSys {
+    double L[25];                 // left eigenvectors of K A (rows)
+    double rho, u, v, w, c, beta, alpha, delta, zp, zm, ubar, ubp, cp;
+    double lam0, lam3, lam4;      // |u.n|, |ubp + cp|, |ubp - cp|
+};
+
+__device__ __forceinline__ void pc_system(double rho, double u, double v, double w, double c, double nx, double ny,
+                                          double nz, double beta, const Flow &f, PcSys &S) {
+    const double alpha = f.pc_method == CFD_PRECOND_TURKEL ? 0.4 : 0.0;
+    const double delta = f.pc_method == CFD_PRECOND_BTW ? 1.0 : beta;
+    const double ubar = u * nx + v * ny + w * nz, c2 = c * c, bc2 = beta * c2;
+    const double zp = 0.5 * (1.0 + beta - alpha), zm = 0.5 * (1.0 - beta + alpha);
+    const double ubp = zp * ubar, cp = sqrt(beta * (c2 - ubar * ubar) + zp * zp * ubar * ubar);
+    const double pv1 = rho * (beta - delta), pv2 = pv1 * ubar, pv3 = bc2 - alpha * ubar * ubar;
+    const double ipv3 = 1.0 / pv3, irc = 1.0 / (rho * c2 * pv3);
+    const double pv4 = (bc2 * (cp + ubar * zm)) / (2.0 * cp * pv3), pv5 = (bc2 * (cp - ubar * zm)) / (2.0 * cp * pv3);
+    const double aub = alpha * ubar, aub2r = alpha * rho * ubar * ubar, rdc = rho * delta * c2;
+    S.rho = rho; S.u = u; S.v = v; S.w = w; S.c = c;
+    S.beta = beta; S.alpha = alpha; S.delta = delta; S.zp = zp; S.zm = zm;
+    S.ubar = ubar; S.ubp = ubp; S.cp = cp;
+    S.lam0 = fabs(ubar);
+    S.lam3 = fabs(ubp + cp);
+    S.lam4 = fabs(ubp - cp);
+    double *L = S.L;
+    L[0] = nx;
+    L[1] = nx * ubar * (alpha * (v * nz - w * ny) + pv1 * nx) * ipv3;
+    L[2] = (bc2 * nz - aub * (w * ny * ny + u * nx * nz + w * nz * nz) + pv2 * nx * ny) * ipv3;
+    L[3] = (-bc2 * ny + aub * (v * ny * ny + u * nx * ny + v * nz * nz) + pv2 * nx * nz) * ipv3;
+    L[4] = (-rdc * nx + alpha * c2 * (v * nz - w * ny) + aub2r * nx) * irc;
+    L[5] = ny;
+    L[6] = (-bc2 * nz + aub * (w * nx * nx + v * ny * nz + w * nz * nz) + pv2 * nx * ny) * ipv3;
+    L[7] = ny * ubar * (alpha * (w * nx - u * nz) + pv1 * ny) * ipv3;
+    L[8] = (bc2 * nx - aub * (u * nx * nx + v * nx * ny + u * nz * nz) + pv2 * ny * nz) * ipv3;
+    L[9] = (-rdc * ny + alpha * c2 * (w * nx - u * nz) + aub2r * ny) * irc;
+    L[10] = nz;
+    L[11] = (bc2 * ny - aub * (v * nx * nx + w * ny * nz + v * ny * ny) + pv2 * nx * nz) * ipv3;
+    L[12] = (-bc2 * nx + aub * (u * nx * nx + w * nx * nz + u * ny * ny) + pv2 * ny * nz) * ipv3;
+    L[13] = nz * ubar * (alpha * (u * ny - v * nx) + pv1 * nz) * ipv3;
+    L[14] = (-rdc * nz + alpha * c2 * (u * ny - v * nx) + aub2r * nz) * irc;
+    L[15] = 0.0; L[16] = pv4 * nx; L[17] = pv4 * ny; L[18] = pv4 * nz;
+    L[19] = (bc2 + aub * (cp - ubar * zp)) / (2.0 * rho * cp * pv3);
+    L[20] = 0.0; L[21] = -pv5 * nx; L[22] = -pv5 * ny; L[23] = -pv5 * nz;
+    L[24] = (bc2 - aub * (cp + ubar * zp)) / (2.0 * rho * cp * pv3);
+}
+
+// out = Mop Kinv R |Lambda| L Mpr dQ at the system's averaged state, with
+// Mpr = d(rho,u,v,w,p)/dQ and Mop its inverse (the same for either gas).
+__device__ __forceinline__ void pc_dissipation(const PcSys &S, double nx, double ny, double nz, const Flow &f,
+                                               const double dQ[5], double out[5]) {
+    const double rho = S.rho, u = S.u, v = S.v, w = S.w, ri = 1.0 / rho;
+    const double q2 = u * u + v * v + w * w;
+    double dq[5];
+    dq[0] = dQ[0];
+    dq[1] = (dQ[1] - u * dQ[0]) * ri;
+    dq[2] = (dQ[2] - v * dQ[0]) * ri;
+    dq[3] = (dQ[3] - w * dQ[0]) * ri;
+    dq[4] = f.gm1 * (0.5 * q2 * dQ[0] - u * dQ[1] - v * dQ[2] - w * dQ[3] + dQ[4]);
+    double a[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++)
+        a[k] = S.L[5 * k] * dq[0] + S.L[5 * k + 1] * dq[1] + S.L[5 * k + 2] * dq[2] + S.L[5 * k + 3] * dq[3] +
+               S.L[5 * k + 4] * dq[4];
+    a[0] *= S.lam0; a[1] *= S.lam0; a[2] *= S.lam0; a[3] *= S.lam3; a[4] *= S.lam4;
+    // right eigenvectors
+    const double bc2 = S.beta * S.c * S.c, ibc2 = 1.0 / bc2, zp = S.zp, zm = S.zm, ub = S.ubar, cp = S.cp;
+    const double r03 = rho * ((zp * S.delta - S.beta) * ub + cp * S.delta) * ibc2;
+    const double r04 = -rho * ((zp * S.delta - S.beta) * ub - cp * S.delta) * ibc2;
+    const double sp = S.alpha * (cp + zp * ub) * ibc2, sm = S.alpha * (cp - zp * ub) * ibc2;
+    double z[5];
+    z[0] = nx * a[0] + ny * a[1] + nz * a[2] + r03 * a[3] + r04 * a[4];
+    z[1] = -nz * a[1] + ny * a[2] + (nx - u * sp) * a[3] + (-nx - u * sm) * a[4];
+    z[2] = nz * a[0] - nx * a[2] + (ny - v * sp) * a[3] + (-ny - v * sm) * a[4];
+    z[3] = -ny * a[0] + nx * a[1] + (nz - w * sp) * a[3] + (-nz - w * sm) * a[4];
+    z[4] = rho * (cp - zm * ub) * a[3] + rho * (cp + zm * ub) * a[4];
+    // Kinv: identity except column 4
+    const double k4 = z[4] / S.beta, kr = S.alpha * z[4] / (S.beta * rho * S.c * S.c);
+    z[0] += (1.0 - S.delta) * ibc2 * z[4];
+    z[1] += u * kr;
+    z[2] += v * kr;
+    z[3] += w * kr;
+    z[4] = k4;
+    out[0] = z[0];
+    out[1] = u * z[0] + rho * z[1];
+    out[2] = v * z[0] + rho * z[2];
+    out[3] = w * z[0] + rho * z[3];
+    out[4] = 0.5 * q2 * z[0] + rho * (u * z[1] + v * z[2] + w * z[3]) + z[4] * f.inv_gm1;
+}
+
+// Roe-averaged eigen-system of an edge; beta from the average's Mach and the
+// larger of the two states' (PRECOND_TYPE LOCAL without smoothing).
+__device__ __forceinline__ void pc_edge_system(const Face &L, const Face &R, double nx, double ny, double nz,
+                                               const Flow &f, PcSys &S) {
+    const double rr = R.rho * L.rho;
+    const double rho = sqrt(rr);
+    const double sigma = rho / (L.rho + rho);
+    const double u = L.u + sigma * (R.u - L.u);
+    const double v = L.v + sigma * (R.v - L.v);
+    const double w = L.w + sigma * (R.w - L.w);
+    const double ht = L.ht + sigma * (R.ht - L.ht);
+    const double q2 = u * u + v * v + w * w;
+    const double c = sqrt(f.gm1 * (ht - 0.5 * q2));  // c^2 = (gamma - 1) h for either gas
+    const double mach = sqrt(q2) / c;
+    const double mL = sqrt(L.u * L.u + L.v * L.v + L.w * L.w) / L.c;
+    const double mR = sqrt(R.u * R.u + R.v * R.v + R.w * R.w) / R.c;
+    pc_system(rho, u, v, w, c, nx, ny, nz, pc_beta(f, mach, fmax(mL, mR)), f, S);
+}
+
+// Preconditioned Roe flux: central part as Roe, dissipation -1/2 |A|_p dQ area;
+// returns the spectral radius of K A (time step), lam = |u.n|, |ubp+cp|, |ubp-cp|.
+__device__ __forceinline__ double roe_precond_flux(const double qL[5], const double qR[5], double nx, double ny,
+                                                   double nz, double area, const Flow &f, double conv[5],
+                                                   double diss[5], double lam[3]) {
+    Face L, R;
+    eos_face(qL, nx, ny, nz, f, true, L);
+    eos_face(qR, nx, ny, nz, f, true, R);
+    const double mL = L.rho * L.ubar, mR = R.rho * R.ubar;
+    const double ha = 0.5 * area;
+    conv[0] = ha * (mL + mR);
+    conv[1] = ha * ((L.u * mL + L.p * nx) + (R.u * mR + R.p * nx));
+    conv[2] = ha * ((L.v * mL + L.p * ny) + (R.v * mR + R.p * ny));
+    conv[3] = ha * ((L.w * mL + L.p * nz) + (R.w * mR + R.p * nz));
+    conv[4] = ha * (L.ht * mL + R.ht * mR);
+    PcSys S;
+    pc_edge_system(L, R, nx, ny, nz, f, S);
+    double dQ[5], d[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) dQ[k] = qR[k] - qL[k];
+    pc_dissipation(S, nx, ny, nz, f, dQ, d);
+#pragma unroll
+    for (int k = 0; k < 5; k++) diss[k] = -ha * d[k];
+    lam[0] = S.lam0;
+    lam[1] = S.lam3;
+    lam[2] = S.lam4;
+    return fmax(S.lam0, fmax(S.lam3, S.lam4));
+}
+
+// |A|_p as a matrix (row-major), column j = the dissipation of dQ = e_j.
+__device__ __forceinline__ void pc_abs_jacobian(const double qL[5], const double qR[5], double nx, double ny,
+                                                double nz, const Flow &f, double A[25]) {
+    Face L, R;
+    eos_face(qL, nx, ny, nz, f, true, L);
+    eos_face(qR, nx, ny, nz, f, true, R);
+    PcSys S;
+    pc_edge_system(L, R, nx, ny, nz, f, S);
+#pragma unroll 1
+    for (int j = 0; j < 5; j++) {
+        double e[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, col[5];
+        e[j] = 1.0;
+        pc_dissipation(S, nx, ny, nz, f, e, col);
+#pragma unroll
+        for (int i = 0; i < 5; i++) A[5 * i + j] = col[i];
+    }
+}
+
+// Pseudo-time matrix Cinv = Mop Kinv Mpr at a node state (beta from the
+// node's Mach; Roe_Jacobian.cpp:241-264 adds (V/dt) Cinv to the diagonal).
+__device__ __forceinline__ void pc_node_cinv(const double q[5], const Flow &f, double C[25]) {
+    Face F;
+    eos_face(q, 1.0, 0.0, 0.0, f, true, F);
+    const double mach = sqrt(F.u * F.u + F.v * F.v + F.w * F.w) / F.c;
+    const double beta = pc_beta(f, mach, 0.0);
+    const double alpha = f.pc_method == CFD_PRECOND_TURKEL ? 0.4 : 0.0;
+    const double delta = f.pc_method == CFD_PRECOND_BTW ? 1.0 : beta;
+    const double rho = F.rho, u = F.u, v = F.v, w = F.w, c2 = F.c * F.c, q2 = u * u + v * v + w * w;
+    const double kc0 = (1.0 - delta) / (beta * c2), kr = alpha / (beta * rho * c2), k4 = 1.0 / beta;
+    // Mpr rows: (1,0,0,0,0), (-u,1,0,0,0)/rho, (-v,0,1,0,0)/rho, (-w,0,0,1,0)/rho, gm1 (q2/2,-u,-v,-w,1)
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+        double m[5];
+        m[0] = j == 0 ? 1.0 : 0.0;
+        m[1] = (j == 0 ? -u : (j == 1 ? 1.0 : 0.0)) / rho;
+        m[2] = (j == 0 ? -v : (j == 2 ? 1.0 : 0.0)) / rho;
+        m[3] = (j == 0 ? -w : (j == 3 ? 1.0 : 0.0)) / rho;
+        m[4] = f.gm1 * (j == 0 ? 0.5 * q2 : (j == 4 ? 1.0 : (j == 1 ? -u : (j == 2 ? -v : -w))));
+        double z0 = m[0] + kc0 * m[4], z1 = m[1] + u * kr * m[4], z2 = m[2] + v * kr * m[4], z3 = m[3] + w * kr * m[4];
+        double z4 = k4 * m[4];
+        C[j] = z0;
+        C[5 + j] = u * z0 + rho * z1;
+        C[10 + j] = v * z0 + rho * z2;
+        C[15 + j] = w * z0 + rho * z3;
+        C[20 + j] = 0.5 * q2 * z0 + rho * (u * z1 + v * z2 + w * z3) + z4 * f.inv_gm1;
+    }
+}
+
+// x = A^-1 b for a 5x5 system by Gaussian elimination with partial pivoting
+// (the pivoted LU the preconditioned BC solves with); A is overwritten.
+__device__ __forceinline__ void solve5_pivot(double A[25], double b[5], double x[5]) {
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+        int p = c;
+#pragma unroll
+        for (int i = c + 1; i < 5; i++)
+            if (fabs(A[5 * i + c]) > fabs(A[5 * p + c])) p = i;
+        if (p != c) {
+#pragma unroll
+            for (int j = 0; j < 5; j++) {
+                const double t = A[5 * c + j];
+                A[5 * c + j] = A[5 * p + j];
+                A[5 * p + j] = t;
+            }
+            const double t = b[c];
+            b[c] = b[p];
+            b[p] = t;
+        }
+#pragma unroll
+        for (int i = c + 1; i < 5; i++) {
+            const double m = A[5 * i + c] / A[5 * c + c];
+#pragma unroll
+            for (int j = c; j < 5; j++) A[5 * i + j] -= m * A[5 * c + j];
+            b[i] -= m * b[c];
+        }
+    }
+#pragma unroll
+    for (int i = 4; i >= 0; i--) {
+        double t = b[i];
+#pragma unroll
+        for (int j = i + 1; j < 5; j++) t -= A[5 * i + j] * x[j];
+        x[i] = t / A[5 * i + i];
+    }
+}
+
+// Ghost state of the preconditioned characteristic BC
+// (Compute_Precondition_Characteristic_BoundaryCondition_Turkel,
+// MPFLOW3D/src/BC.cpp:113-700, BC_METHOD_CHARCTERISTIC) through the
+// characteristic variables L (rho,u,v,w,p) at the interior/ghost average:
+// wall = four outgoing characteristics and zero normal velocity; subsonic
+// inflow = freestream (rho, u, v, w) with the interior's p and the u.n + c'
+// characteristic from inside; subsonic outflow = four characteristics from
+// inside and the outflow pressure.  Returns as characteristic_bc.
+__device__ __forceinline__ int precond_characteristic_bc(const double qI[5], const double qG[5], double nx,
+                                                         double ny, double nz, int bc_type, const Flow &f,
+                                                         double qB[5]) {
+    Face I, G, O;
+    eos_face(qI, nx, ny, nz, f, true, I);
+    eos_face(qG, nx, ny, nz, f, true, G);
+    double q0[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) q0[k] = 0.5 * (qI[k] + qG[k]);
+    eos_face(q0, nx, ny, nz, f, true, O);
+    const double mach = sqrt(O.u * O.u + O.v * O.v + O.w * O.w) / O.c;
+    const double mI = sqrt(I.u * I.u + I.v * I.v + I.w * I.w) / I.c;
+    const double mG = sqrt(G.u * G.u + G.v * G.v + G.w * G.w) / G.c;
+    PcSys S;
+    pc_system(O.rho, O.u, O.v, O.w, O.c, nx, ny, nz, pc_beta(f, mach, fmax(mI, mG)), f, S);
+    const double l1 = S.ubar, l4 = S.ubp + S.cp, l5 = S.ubp - S.cp;
+    int inst, status = 0;
+    switch (bc_type) {
+        case 0: inst = 0; break;
+        case 1:
+            if (l1 <= 0.0 && l4 <= 0.0 && l5 <= 0.0) inst = 10;
+            else if (l1 >= 0.0 && l4 >= 0.0 && l5 >= 0.0) inst = 11;
+            else if (l1 >= 0.0 && l5 <= 0.0 && l4 >= 0.0) inst = 9;
+            else if (l1 <= 0.0 && l4 >= 0.0 && l5 <= 0.0) inst = 8;
+            else { inst = 1; status = 2; }
+            break;
+        case 2:
+            if (l1 <= 0.0 && l4 >= 0.0 && l5 <= 0.0) inst = 4;
+            else if (l1 <= 0.0 && l4 <= 0.0 && l5 <= 0.0) inst = 6;
+            else inst = (fabs(l1) < O.c) ? 4 : 6;
+            break;
+        case 3:
+            if (l1 >= 0.0 && l5 <= 0.0 && l4 >= 0.0) inst = 5;
+            else if (l1 >= 0.0 && l4 >= 0.0 && l5 >= 0.0) inst = 7;
+            else inst = (fabs(l1) < O.c) ? 5 : 7;
+            break;
+        case 4: case 5: case 6: case 7: inst = bc_type; break;
+        default: inst = -1; status = 2; break;
+    }
+    const double qi[5] = {I.rho, I.u, I.v, I.w, I.p};
+    const double qf[5] = {f.inf_rho, f.inf_u, f.inf_v, f.inf_w, f.inf_p};
+    double xb[5] = {f.inf_rho, f.inf_u, f.inf_v, f.inf_w, f.inf_p};
+    auto lrow = [&](int k, const double q[5]) {
+        return S.L[5 * k] * q[0] + S.L[5 * k + 1] * q[1] + S.L[5 * k + 2] * q[2] + S.L[5 * k + 3] * q[3] +
+               S.L[5 * k + 4] * q[4];
+    };
+    double B[5];
+    switch (inst) {
+        case 0:
+#pragma unroll
+            for (int k = 0; k < 4; k++) B[k] = lrow(k, qi);
+            B[4] = 0.0;
+            S.L[20] = 0.0; S.L[21] = nx; S.L[22] = ny; S.L[23] = nz; S.L[24] = 0.0;
+            solve5_pivot(S.L, B, xb);
+            if (f.iteration < f.zpg_iteration && xb[4] + f.pinf < 0.0) {
+                xb[0] = I.rho; xb[4] = I.p;
+                xb[1] = I.u - nx * I.ubar; xb[2] = I.v - ny * I.ubar; xb[3] = I.w - nz * I.ubar;
+            }
+            if (xb[4] + f.pinf < 0.0) status = status ? status : 1;
+            break;
+        case 4: case 8: {
+            const double qe[5] = {qf[0], qf[1], qf[2], qf[3], inst == 4 ? I.p : qf[4]};
+#pragma unroll
+            for (int k = 0; k < 5; k++) B[k] = k == 3 ? lrow(3, qi) : lrow(k, qe);
+            solve5_pivot(S.L, B, xb);
+        } break;
+        case 5:
+#pragma unroll
+            for (int k = 0; k < 4; k++) B[k] = lrow(k, qi);
+            B[4] = f.pc_outflow_p;
+            S.L[20] = 0.0; S.L[21] = 0.0; S.L[22] = 0.0; S.L[23] = 0.0; S.L[24] = 1.0;
+            solve5_pivot(S.L, B, xb);
+            break;
+        case 9:
+#pragma unroll
+            for (int k = 0; k < 5; k++) B[k] = k == 4 ? lrow(4, qf) : lrow(k, qi);
+            solve5_pivot(S.L, B, xb);
+            break;
+        case 7: case 11:
+#pragma unroll
+            for (int k = 0; k < 5; k++) xb[k] = qi[k];
+            break;
+        default: break;  // 1, 6, 10: freestream
+    }
+    const double rb = xb[0], ub = xb[1], vb = xb[2], wb = xb[3], pb = xb[4];
+    const double et = (pb + f.gpinf) / (f.gm1 * rb) + 0.5 * (ub * ub + vb * vb + wb * wb);
+    qB[0] = rb;
+    qB[1] = rb * ub;
+    qB[2] = rb * vb;
+    qB[3] = rb * wb;
+    qB[4] = rb * et;
+    return status;
 }
 
 }  // namespace cfd

@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define CFD_ABI_VERSION 3
+#define CFD_ABI_VERSION 4
 
 /* ------------------------------------------------------------ status codes */
 #define CFD_OK                 0
@@ -58,6 +58,20 @@ extern "C" {
 #define CFD_FLUX_ROE_LMFIX 3 /* FLUX_SCHEME_ROE with PRECOND_METHOD_ROE_LMFIX (SolverParameters.h:136): the
                                 low-Mach fix of Compute_Flux_Roe_LMFIX (Euler3D/src/FluxTest.cpp:2801) and the
                                 preconditioned characteristic BC (BC.cpp:700) */
+#define CFD_FLUX_ROE_PRECOND 4 /* FLUX_SCHEME_ROE with MPFLOW3D's Turkel-family preconditioning
+                                (PRECOND_METHOD_BTW / _ERIKSSON / _TURKEL, MPFLOW3D/include/SolverParameters.h:141-144):
+                                preconditioned Roe dissipation (Compute_Flux_Roe_Precondition_Turkel,
+                                MPFLOW3D/src/Roe_Fluxes.cpp:2043), its eigenvalues in the time step,
+                                the preconditioned pseudo-time term of the Jacobian (Roe_Jacobian.cpp:241)
+                                and the preconditioned characteristic BC (MPFLOW3D/src/BC.cpp:113) */
+/* cfd_params.precond_method (MPFLOW3D PRECOND_METHOD values) */
+#define CFD_PRECOND_BTW      2  /* Briley-Taylor-Whitfield: alpha 0, delta 1    */
+#define CFD_PRECOND_ERIKSSON 3  /* Eriksson: alpha 0, delta beta                */
+#define CFD_PRECOND_TURKEL   5  /* Turkel: alpha 0.4, delta beta                */
+/* cfd_params.precond_type (MPFLOW3D PRECOND_TYPE values) */
+#define CFD_PRECOND_LOCAL    0  /* beta from the local Mach and precond_mach    */
+#define CFD_PRECOND_GLOBAL   1  /* beta = min(1, precond_mach)                  */
+#define CFD_PRECOND_URLOCAL  2  /* beta = min(1, local Mach)                    */
 
 #define CFD_ORDER_FIRST  0 /* SOLVER_ORDER_FIRST  (SolverParameters.h:316) */
 #define CFD_ORDER_SECOND 1 /* SOLVER_ORDER_SECOND (SolverParameters.h:317) */
@@ -118,6 +132,15 @@ typedef struct cfd_params {
      * EOS/src/EOS_IdealGas.c:73); at pinf = 0 every result is bit-identical
      * to the ideal-gas path. */
     double pinf;
+    /* CFD_FLUX_ROE_PRECOND only (MPFLOW3D SolverParameters.cpp:75-78, Material.cpp:57):
+     * PRECOND_METHOD, PRECOND_TYPE, PRECOND_GLOBAL_MACH and OUTFLOW_PRESSURE
+     * (the subsonic-outflow pressure of the preconditioned BC; 0 = the
+     * freestream pressure).  PRECOND_SMOOTH is NO (beta from the edge's own
+     * states); the averages are Roe averages (AVERAGE_TYPE_ROE). */
+    int    precond_method;
+    int    precond_type;
+    double precond_mach;
+    double outflow_pressure;
 } cfd_params;
 
 /* Fills p with the defaults used by the reference parameter files of this

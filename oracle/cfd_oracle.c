@@ -55,6 +55,312 @@ static void eos_face(const double *q, double nx, double ny, double nz, double g,
     s->ubar = s->u * nx + s->v * ny + s->w * nz;
 }
 
+/* ---- Low-Mach preconditioned Roe of the Turkel family (MPFLOW3D) ----------
+ * Compute_Flux_Roe_Precondition_Turkel (MPFLOW3D/src/Roe_Fluxes.cpp:2043-2526):
+ * preconditioner K in (rho, u, v, w, p) with parameters alpha, delta and
+ * beta = Mr^2 (BTW: alpha 0, delta 1; Eriksson: alpha 0, delta beta; Turkel:
+ * alpha 0.4, delta beta), dissipation Mop Kinv R |Lambda| L Mpr dQ with the
+ * eigenvalues |u.n|, |u'.n +- c'| of K A, the Roe average, the solution in
+ * conservative variables and the pressure smoothing off (PRECOND_SMOOTH NO). */
+typedef struct {
+    double L[5][5], R[5][5], lam[5], kc[5]; /* left/right eigenvectors, |eigenvalues|, Kinv column 4 */
+    double ubar, ubp, cp;
+} pc_sys_t;
+
+/* beta (squared) of PRECOND_TYPE LOCAL (0) / GLOBAL (1) / URLOCAL (2) (Roe_Fluxes.cpp:2225-2248). */
+static double pc_beta(const orc_params *p, double mach, double mach_max) {
+    double b = 1.0;
+    if (p->pc_type == 0) {
+        double M = dmax(mach, mach_max), G = p->pc_mach;
+        b = M < G ? 0.5 * (M * M) / (G * G) - M / G + 1.0 : 0.5;
+        b = dmin(1.0, b * (sqrt(M * G) + M));
+    } else if (p->pc_type == 2) {
+        b = dmin(1.0, mach);
+    } else {
+        b = dmin(1.0, p->pc_mach);
+    }
+    return b * b;
+}
+
+static void pc_params(const orc_params *p, double beta, double *alpha, double *delta) {
+    *alpha = p->pc_method == 5 ? 0.4 : 0.0;
+    *delta = p->pc_method == 2 ? 1.0 : beta;
+}
+
+/* Eigen-system of K A in (rho, u, v, w, p) at (rho, u, v, w, c), normal n
+ * (Roe_Fluxes.cpp:2266-2400; BC.cpp:260-305). */
+static void pc_system(double rho, double u, double v, double w, double c, const double *n, double beta, double alpha,
+                      double delta, pc_sys_t *S) {
+    double nx = n[0], ny = n[1], nz = n[2];
+    double ubar = u * nx + v * ny + w * nz, c2 = c * c, bc2 = beta * c2;
+    double zp = 0.5 * (1.0 + beta - alpha), zm = 0.5 * (1.0 - beta + alpha);
+    double ubp = zp * ubar, cp = sqrt(beta * (c2 - ubar * ubar) + zp * zp * ubar * ubar);
+    double pv1 = rho * (beta - delta), pv2 = pv1 * ubar, pv3 = bc2 - alpha * ubar * ubar;
+    double pv4 = (bc2 * (cp + ubar * zm)) / (2.0 * cp * pv3), pv5 = (bc2 * (cp - ubar * zm)) / (2.0 * cp * pv3);
+    S->ubar = ubar; S->ubp = ubp; S->cp = cp;
+    S->lam[0] = S->lam[1] = S->lam[2] = fabs(ubar);
+    S->lam[3] = fabs(ubp + cp);
+    S->lam[4] = fabs(ubp - cp);
+    /* left eigenvectors (rows) */
+    double (*L)[5] = S->L;
+    L[0][0] = nx;
+    L[0][1] = nx * ubar * (alpha * (v * nz - w * ny) + pv1 * nx) / pv3;
+    L[0][2] = (bc2 * nz - alpha * ubar * (w * ny * ny + u * nx * nz + w * nz * nz) + pv2 * nx * ny) / pv3;
+    L[0][3] = (-bc2 * ny + alpha * ubar * (v * ny * ny + u * nx * ny + v * nz * nz) + pv2 * nx * nz) / pv3;
+    L[0][4] = (-rho * delta * c2 * nx + alpha * c2 * (v * nz - w * ny) + alpha * rho * ubar * ubar * nx) / (rho * c2 * pv3);
+    L[1][0] = ny;
+    L[1][1] = (-bc2 * nz + alpha * ubar * (w * nx * nx + v * ny * nz + w * nz * nz) + pv2 * nx * ny) / pv3;
+    L[1][2] = ny * ubar * (alpha * (w * nx - u * nz) + pv1 * ny) / pv3;
+    L[1][3] = (bc2 * nx - alpha * ubar * (u * nx * nx + v * nx * ny + u * nz * nz) + pv2 * ny * nz) / pv3;
+    L[1][4] = (-rho * delta * c2 * ny + alpha * c2 * (w * nx - u * nz) + alpha * rho * ubar * ubar * ny) / (rho * c2 * pv3);
+    L[2][0] = nz;
+    L[2][1] = (bc2 * ny - alpha * ubar * (v * nx * nx + w * ny * nz + v * ny * ny) + pv2 * nx * nz) / pv3;
+    L[2][2] = (-bc2 * nx + alpha * ubar * (u * nx * nx + w * nx * nz + u * ny * ny) + pv2 * ny * nz) / pv3;
+    L[2][3] = nz * ubar * (alpha * (u * ny - v * nx) + pv1 * nz) / pv3;
+    L[2][4] = (-rho * delta * c2 * nz + alpha * c2 * (u * ny - v * nx) + alpha * rho * ubar * ubar * nz) / (rho * c2 * pv3);
+    L[3][0] = 0.0; L[3][1] = pv4 * nx; L[3][2] = pv4 * ny; L[3][3] = pv4 * nz;
+    L[3][4] = (bc2 + alpha * ubar * (cp - ubar * zp)) / (2.0 * rho * cp * pv3);
+    L[4][0] = 0.0; L[4][1] = -pv5 * nx; L[4][2] = -pv5 * ny; L[4][3] = -pv5 * nz;
+    L[4][4] = (bc2 - alpha * ubar * (cp + ubar * zp)) / (2.0 * rho * cp * pv3);
+    /* right eigenvectors (columns) */
+    double (*R)[5] = S->R;
+    R[0][0] = nx; R[0][1] = ny; R[0][2] = nz;
+    R[0][3] = rho * ((zp * delta - beta) * ubar + cp * delta) / bc2;
+    R[0][4] = -rho * ((zp * delta - beta) * ubar - cp * delta) / bc2;
+    R[1][0] = 0.0; R[1][1] = -nz; R[1][2] = ny;
+    R[1][3] = nx - alpha * u * (cp + zp * ubar) / bc2;
+    R[1][4] = -nx - alpha * u * (cp - zp * ubar) / bc2;
+    R[2][0] = nz; R[2][1] = 0.0; R[2][2] = -nx;
+    R[2][3] = ny - alpha * v * (cp + zp * ubar) / bc2;
+    R[2][4] = -ny - alpha * v * (cp - zp * ubar) / bc2;
+    R[3][0] = -ny; R[3][1] = nx; R[3][2] = 0.0;
+    R[3][3] = nz - alpha * w * (cp + zp * ubar) / bc2;
+    R[3][4] = -nz - alpha * w * (cp - zp * ubar) / bc2;
+    R[4][0] = 0.0; R[4][1] = 0.0; R[4][2] = 0.0;
+    R[4][3] = rho * (cp - zm * ubar);
+    R[4][4] = rho * (cp + zm * ubar);
+    /* Kinv = I except column 4 */
+    S->kc[0] = (1.0 - delta) / bc2;
+    S->kc[1] = (alpha * u) / (beta * rho * c2);
+    S->kc[2] = (alpha * v) / (beta * rho * c2);
+    S->kc[3] = (alpha * w) / (beta * rho * c2);
+    S->kc[4] = 1.0 / beta;
+}
+
+/* Mpr = d(rho, u, v, w, p) / dQ_cons and Mop = dQ_cons / d(rho, u, v, w, p) at
+ * (rho, u, v, w) (Material_Get_Transformation_Matrix; the stiffened gas has
+ * the same derivatives as the ideal gas). */
+static void pc_transforms(double rho, double u, double v, double w, double g, double Mpr[5][5], double Mop[5][5]) {
+    double q2 = u * u + v * v + w * w, g1 = g - 1.0;
+    double a[5][5] = {{1, 0, 0, 0, 0}, {-u / rho, 1.0 / rho, 0, 0, 0}, {-v / rho, 0, 1.0 / rho, 0, 0},
+                      {-w / rho, 0, 0, 1.0 / rho, 0}, {0.5 * g1 * q2, -g1 * u, -g1 * v, -g1 * w, g1}};
+    double b[5][5] = {{1, 0, 0, 0, 0}, {u, rho, 0, 0, 0}, {v, 0, rho, 0, 0}, {w, 0, 0, rho, 0},
+                      {0.5 * q2, rho * u, rho * v, rho * w, 1.0 / g1}};
+    memcpy(Mpr, a, sizeof a);
+    memcpy(Mop, b, sizeof b);
+}
+
+static void mm5g(double A[5][5], double B[5][5], double C[5][5]) {
+    for (int i = 0; i < 5; i++)
+        for (int j = 0; j < 5; j++) {
+            C[i][j] = 0.0;
+            for (int k = 0; k < 5; k++) C[i][j] += A[i][k] * B[k][j];
+        }
+}
+
+/* The edge's averaged state and eigen-system (first-order states or
+ * reconstructed face states); returns the spectral radius. */
+static double pc_edge(const double *qL, const double *qR, const double *n, const orc_params *p, face_t *Lf, face_t *Rf,
+                      double avg[4], pc_sys_t *S) {
+    double g = p->gamma;
+    eos_face(qL, n[0], n[1], n[2], g, p->pinf, Lf);
+    eos_face(qR, n[0], n[1], n[2], g, p->pinf, Rf);
+    double rho = sqrt(Rf->rho * Lf->rho), sigma = rho / (Lf->rho + rho);
+    double u = Lf->u + sigma * (Rf->u - Lf->u), v = Lf->v + sigma * (Rf->v - Lf->v), w = Lf->w + sigma * (Rf->w - Lf->w);
+    double ht = Lf->ht + sigma * (Rf->ht - Lf->ht);
+    double q2 = u * u + v * v + w * w, h = ht - 0.5 * q2;
+    double c = sqrt((g - 1.0) * h); /* Material_Get_DH_SpeedSound: c^2 = (g - 1) h for either gas */
+    double mach = sqrt(q2) / c;
+    double mL = sqrt(Lf->u * Lf->u + Lf->v * Lf->v + Lf->w * Lf->w) / Lf->c;
+    double mR = sqrt(Rf->u * Rf->u + Rf->v * Rf->v + Rf->w * Rf->w) / Rf->c;
+    double beta = pc_beta(p, mach, dmax(mL, mR)), alpha, delta;
+    pc_params(p, beta, &alpha, &delta);
+    pc_system(rho, u, v, w, c, n, beta, alpha, delta, S);
+    avg[0] = rho; avg[1] = u; avg[2] = v; avg[3] = w;
+    return dmax(S->lam[0], dmax(S->lam[3], S->lam[4]));
+}
+
+/* |A|_p = Mop Kinv R |Lambda| L Mpr (Compute_Dissipation_Matrix_Roe_Precondition_Turkel,
+ * Roe_Fluxes.cpp:3440-3810). */
+static void pc_absA(const pc_sys_t *S, const double avg[4], double g, double A[5][5]) {
+    double Mpr[5][5], Mop[5][5], T[5][5], U[5][5], V[5][5];
+    pc_transforms(avg[0], avg[1], avg[2], avg[3], g, Mpr, Mop);
+    for (int i = 0; i < 5; i++)
+        for (int j = 0; j < 5; j++) U[i][j] = S->lam[i] * S->L[i][j];       /* |Lambda| L */
+    mm5g((double (*)[5])S->R, U, T);                                       /* R |Lambda| L */
+    for (int j = 0; j < 5; j++) {                                          /* Kinv (R |Lambda| L) */
+        double t4 = T[4][j];
+        for (int i = 0; i < 5; i++) V[i][j] = (i == 4 ? 0.0 : T[i][j]) + S->kc[i] * t4;
+    }
+    mm5g(Mop, V, T);
+    mm5g(T, Mpr, A);
+}
+
+static double roe_pc(const double *qL, const double *qR, const double *n, double area, const orc_params *p,
+                     double *conv, double *diss, double lam[3]) {
+    face_t L, R;
+    pc_sys_t S;
+    double avg[4], A[5][5];
+    double lmax = pc_edge(qL, qR, n, p, &L, &R, avg, &S);
+    double mL = L.rho * L.ubar, mR = R.rho * R.ubar;
+    double FL[5] = {mL, L.u * mL + L.p * n[0], L.v * mL + L.p * n[1], L.w * mL + L.p * n[2], L.ht * mL};
+    double FR[5] = {mR, R.u * mR + R.p * n[0], R.v * mR + R.p * n[1], R.w * mR + R.p * n[2], R.ht * mR};
+    pc_absA(&S, avg, p->gamma, A);
+    for (int i = 0; i < 5; i++) {
+        double fa = 0.0;
+        for (int j = 0; j < 5; j++) fa += A[i][j] * (qR[j] - qL[j]);
+        conv[i] = 0.5 * (FL[i] + FR[i]) * area;
+        diss[i] = -0.5 * fa * area;
+    }
+    lam[0] = S.lam[0]; lam[1] = S.lam[3]; lam[2] = S.lam[4];
+    return lmax;
+}
+
+/* Cinv = Mop Kinv Mpr at a node (Compute_Transformed_Preconditioner_Matrix_Roe_Turkel
+ * with reqInv, Roe_Fluxes.cpp:261-441): the pseudo-time term of the Jacobian. */
+static void pc_node_cinv(const double *q, const orc_params *p, double C[5][5]) {
+    face_t F;
+    double n0[3] = {1.0, 0.0, 0.0};
+    eos_face(q, n0[0], n0[1], n0[2], p->gamma, p->pinf, &F);
+    double mach = sqrt(F.u * F.u + F.v * F.v + F.w * F.w) / F.c;
+    double beta = pc_beta(p, mach, 0.0), alpha, delta;
+    pc_params(p, beta, &alpha, &delta);
+    double c2 = F.c * F.c, kc[5] = {(1.0 - delta) / (beta * c2), (alpha * F.u) / (beta * F.rho * c2),
+                                    (alpha * F.v) / (beta * F.rho * c2), (alpha * F.w) / (beta * F.rho * c2), 1.0 / beta};
+    double Mpr[5][5], Mop[5][5], K[5][5] = {{0}}, T[5][5];
+    pc_transforms(F.rho, F.u, F.v, F.w, p->gamma, Mpr, Mop);
+    for (int i = 0; i < 5; i++) { K[i][i] = i == 4 ? 0.0 : 1.0; K[i][4] += kc[i]; }
+    mm5g(Mop, K, T);
+    mm5g(T, Mpr, C);
+}
+
+/* Gaussian elimination with partial pivoting on a 5x5 system (the
+ * GaussainLUDecompose + pivoted substitutions the preconditioned BC uses). */
+static void solve5(double A[5][5], const double *b, double *x) {
+    double M[5][6];
+    for (int i = 0; i < 5; i++) { for (int j = 0; j < 5; j++) M[i][j] = A[i][j]; M[i][5] = b[i]; }
+    for (int c = 0; c < 5; c++) {
+        int pi = c;
+        for (int i = c + 1; i < 5; i++) if (fabs(M[i][c]) > fabs(M[pi][c])) pi = i;
+        if (pi != c) for (int j = 0; j < 6; j++) { double t = M[c][j]; M[c][j] = M[pi][j]; M[pi][j] = t; }
+        for (int i = c + 1; i < 5; i++) {
+            double f = M[i][c] / M[c][c];
+            for (int j = c; j < 6; j++) M[i][j] -= f * M[c][j];
+        }
+    }
+    for (int i = 4; i >= 0; i--) {
+        double t = M[i][5];
+        for (int j = i + 1; j < 5; j++) t -= M[i][j] * x[j];
+        x[i] = t / M[i][i];
+    }
+}
+
+static void lmul5(double L[5][5], const double *q, double *out) {
+    for (int i = 0; i < 5; i++) {
+        out[i] = 0.0;
+        for (int j = 0; j < 5; j++) out[i] += L[i][j] * q[j];
+    }
+}
+
+/* Ghost state of Compute_Precondition_Characteristic_BoundaryCondition_Turkel
+ * (MPFLOW3D/src/BC.cpp:113-700), BC_METHOD_CHARCTERISTIC, in (rho, u, v, w, p)
+ * through the preconditioned characteristic variables L q.  The subsonic
+ * outflow imposes p->outflow_p (the freestream pressure when 0). */
+static int bc_state_pc(const double *qI, const double *qG, const double *areav, int type, const orc_params *p,
+                       const double *inf, double *qB) {
+    double n[3], mag;
+    unit(areav, n, &mag);
+    face_t I, G, O;
+    double q0[5];
+    eos_face(qI, n[0], n[1], n[2], p->gamma, p->pinf, &I);
+    eos_face(qG, n[0], n[1], n[2], p->gamma, p->pinf, &G);
+    for (int k = 0; k < 5; k++) q0[k] = 0.5 * (qI[k] + qG[k]);
+    eos_face(q0, n[0], n[1], n[2], p->gamma, p->pinf, &O);
+    double mach = sqrt(O.u * O.u + O.v * O.v + O.w * O.w) / O.c;
+    double mI = sqrt(I.u * I.u + I.v * I.v + I.w * I.w) / I.c, mG = sqrt(G.u * G.u + G.v * G.v + G.w * G.w) / G.c;
+    double beta = pc_beta(p, mach, dmax(mI, mG)), alpha, delta;
+    pc_params(p, beta, &alpha, &delta);
+    pc_sys_t S;
+    pc_system(O.rho, O.u, O.v, O.w, O.c, n, beta, alpha, delta, &S);
+    double l1 = S.ubar, l4 = S.ubp + S.cp, l5 = S.ubp - S.cp;
+    int inst = -1, st = 0;
+    switch (type) {
+        case 0: inst = 0; break;
+        case 1:
+            if (l1 <= 0.0 && l4 <= 0.0 && l5 <= 0.0) inst = 10;
+            else if (l1 >= 0.0 && l4 >= 0.0 && l5 >= 0.0) inst = 11;
+            else if (l1 >= 0.0 && l5 <= 0.0 && l4 >= 0.0) inst = 9;
+            else if (l1 <= 0.0 && l4 >= 0.0 && l5 <= 0.0) inst = 8;
+            else { inst = 1; st = 2; }
+            break;
+        case 2:
+            if (l1 <= 0.0 && l4 >= 0.0 && l5 <= 0.0) inst = 4;
+            else if (l1 <= 0.0 && l4 <= 0.0 && l5 <= 0.0) inst = 6;
+            else inst = fabs(l1) < O.c ? 4 : 6;
+            break;
+        case 3:
+            if (l1 >= 0.0 && l5 <= 0.0 && l4 >= 0.0) inst = 5;
+            else if (l1 >= 0.0 && l4 >= 0.0 && l5 >= 0.0) inst = 7;
+            else inst = fabs(l1) < O.c ? 5 : 7;
+            break;
+        default: inst = type; break;
+    }
+    double qi[5] = {I.rho, I.u, I.v, I.w, I.p}, qinf[5] = {inf[0], inf[1], inf[2], inf[3], inf[5]};
+    double B[5], X[5], xb[5] = {inf[0], inf[1], inf[2], inf[3], inf[5]};
+    double outp = p->outflow_p != 0.0 ? p->outflow_p : inf[5];
+    switch (inst) {
+        case 0: /* wall: four characteristics from inside, zero normal velocity */
+            lmul5(S.L, qi, B);
+            B[4] = 0.0;
+            S.L[4][0] = 0.0; S.L[4][1] = n[0]; S.L[4][2] = n[1]; S.L[4][3] = n[2]; S.L[4][4] = 0.0;
+            solve5(S.L, B, xb);
+            if (p->iteration < p->zpg_iteration && xb[4] + p->pinf < 0.0) {
+                xb[0] = I.rho; xb[4] = I.p;
+                xb[1] = I.u - n[0] * I.ubar; xb[2] = I.v - n[1] * I.ubar; xb[3] = I.w - n[2] * I.ubar;
+            }
+            if (xb[4] + p->pinf < 0.0) st = st ? st : 1;
+            break;
+        case 4: case 8: { /* subsonic inflow: the u.n + c characteristic from inside */
+            double qe[5] = {qinf[0], qinf[1], qinf[2], qinf[3], inst == 4 ? I.p : qinf[4]};
+            lmul5(S.L, qe, B);
+            lmul5(S.L, qi, X);
+            B[3] = X[3];
+            solve5(S.L, B, xb);
+        } break;
+        case 5: /* subsonic outflow: pressure imposed */
+            lmul5(S.L, qi, B);
+            for (int j = 0; j < 4; j++) S.L[4][j] = 0.0;
+            S.L[4][4] = 1.0;
+            B[4] = outp;
+            solve5(S.L, B, xb);
+            break;
+        case 9: /* far-field subsonic outflow: the u.n - c characteristic from outside */
+            lmul5(S.L, qi, B);
+            lmul5(S.L, qinf, X);
+            B[4] = X[4];
+            solve5(S.L, B, xb);
+            break;
+        case 7: case 11:
+            for (int k = 0; k < 5; k++) xb[k] = qi[k];
+            break;
+        default: break; /* 1, 6, 10: freestream */
+    }
+    double rb = xb[0], ub = xb[1], vb = xb[2], wb = xb[3], pb = xb[4];
+    double et = (pb + p->gamma * p->pinf) / ((p->gamma - 1.0) * rb) + 0.5 * (ub * ub + vb * vb + wb * wb);
+    qB[0] = rb; qB[1] = rb * ub; qB[2] = rb * vb; qB[3] = rb * wb; qB[4] = rb * et;
+    return st;
+}
+
 /* Characteristic BC ghost state (Compute_Characteristic_BoundaryCondition_New,
  * Euler3D/src/BC.cpp:381-677), conservative variables.  Returns nonzero where
  * the reference would abort. */
@@ -141,7 +447,8 @@ void orc_apply_bc(const orc_mesh *m, const orc_params *p, double *Q) {
         int L = m->bn[2 * b], R = m->bn[2 * b + 1];
         double qI[5], qG[5], qB[5];
         for (int k = 0; k < 5; k++) { qI[k] = Q[IDX(k, L, ld)]; qG[k] = Q[IDX(k, R, ld)]; }
-        bc_state(qI, qG, m->ba + 3 * (size_t)b, m->bt[b], p, inf, qB);
+        if (p->flux == 4) bc_state_pc(qI, qG, m->ba + 3 * (size_t)b, m->bt[b], p, inf, qB);
+        else bc_state(qI, qG, m->ba + 3 * (size_t)b, m->bt[b], p, inf, qB);
         for (int k = 0; k < 5; k++) Q[IDX(k, R, ld)] = qB[k];
     }
 }
@@ -338,7 +645,7 @@ void orc_residual(const orc_mesh *m, const orc_params *p, const double *Q, const
             if (p->flux == 1) lmax = hllc(qL, qR, n, area, p, fc, fd);
             else if (p->flux == 2) lmax = ausmp(qL, qR, n, area, p, fc, fd);
             else {
-                lmax = roe(qL, qR, n, area, p, fc, fd, lam);
+                lmax = p->flux == 4 ? roe_pc(qL, qR, n, area, p, fc, fd, lam) : roe(qL, qR, n, area, p, fc, fd, lam);
                 ext[0] = dmin(ext[0], lam[0]); ext[1] = dmax(ext[1], lam[0]);
                 ext[2] = dmin(ext[2], lam[1]); ext[3] = dmax(ext[3], lam[1]);
                 ext[4] = dmin(ext[4], lam[2]); ext[5] = dmax(ext[5], lam[2]);
@@ -492,7 +799,7 @@ void orc_limiter(const orc_mesh *m, const orc_params *p, const double *Q, const 
         }
         for (int v = 0; v < 5; v++) phi[IDX(v, i, nn)] = ph[v];
     }
-    if (p->flux != 0 && p->flux != 3) return;
+    if (p->flux != 0 && p->flux != 3 && p->flux != 4) return;
     for (int i = 0; i < nn; i++) {
         for (int k = m->ia[i]; k < m->ia[i + 1]; k++) {
             int j = m->ja[k];
@@ -613,7 +920,14 @@ void orc_jacobian(const orc_mesh *m, const orc_params *p, const double *Q, const
     for (int i = 0; i < nn; i++) {
         for (int k = 0; k < 5; k++)
             B[5 * (size_t)i + k] = -(conv[IDX(k, i, nn)] + (include_diss ? diss[IDX(k, i, nn)] : 0.0));
-        if (add_time)
+        if (add_time && p->flux == 4) {
+            /* pseudo-time term (V / dt) Cinv of the preconditioned system (Roe_Jacobian.cpp:241-264) */
+            double q[5], C[5][5];
+            for (int k = 0; k < 5; k++) q[k] = Q[IDX(k, i, ld)];
+            pc_node_cinv(q, p, C);
+            for (int a = 0; a < 5; a++)
+                for (int b = 0; b < 5; b++) A[25 * (size_t)IAU[i] + 5 * a + b] = m->vol[i] / dt[i] * C[a][b];
+        } else if (add_time)
             for (int k = 0; k < 5; k++) A[25 * (size_t)IAU[i] + 6 * k] = m->vol[i] / dt[i];
     }
     for (int pass = 0; pass < 2; pass++) {
@@ -627,7 +941,15 @@ void orc_jacobian(const orc_mesh *m, const orc_params *p, const double *Q, const
             for (int k = 0; k < 5; k++) { qL[k] = Q[IDX(k, L, ld)]; qR[k] = Q[IDX(k, R, ld)]; }
             flux_jac(qL, n, p->gamma, p->pinf, JL);
             flux_jac(qR, n, p->gamma, p->pinf, JR);
-            roe_absA(qL, qR, n, p, Ab);
+            if (p->flux == 4) {
+                face_t Lf, Rf;
+                pc_sys_t S;
+                double avg[4];
+                pc_edge(qL, qR, n, p, &Lf, &Rf, avg, &S);
+                pc_absA(&S, avg, p->gamma, Ab);
+            } else {
+                roe_absA(qL, qR, n, p, Ab);
+            }
             double *dL = A + 25 * (size_t)IAU[L];
             if (pass == 1) {
                 for (int a = 0; a < 5; a++)

@@ -18,6 +18,11 @@ typedef struct {
     int flux, order, limiter, limiter_order, limiter_smooth, entropy_fix;
     int global_time, ls_weight, gradient, iteration, zpg_iteration;
     double pinf; /* stiffened-gas constant (0: ideal gas) */
+    /* flux 4, preconditioned Roe (MPFLOW3D enum values): method 2 BTW, 3 Eriksson,
+     * 5 Turkel; type 0 local, 1 global, 2 unrestricted local; reference Mach;
+     * subsonic outflow pressure (0: freestream) */
+    int pc_method, pc_type;
+    double pc_mach, outflow_p;
 } orc_params;
 
 typedef struct {

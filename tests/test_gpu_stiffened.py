@@ -24,6 +24,8 @@ pytestmark = pytest.mark.gpu
 
 WATER = dict(gamma=4.4, pinf=6000.0, mach=0.0062, mach_min=0.0062)  # 1000 kg/m^3, 1 bar, pinf 6e8 Pa, ~10 m/s
 CHANNEL_BC = (2, 3, 0, 0, 0, 0)  # inflow at x = 0, outflow at x = lx, slip walls
+# MPFLOW3D's Turkel preconditioning, local beta with the freestream Mach as reference
+PRECOND = dict(flux_scheme=4, precond_method=5, precond_type=0, precond_mach=0.0062)
 
 
 def tol(cfg):
@@ -39,6 +41,12 @@ CASES = [
     ("lmfix2_water_channel", dict(CFG1, **WATER, flux_scheme=3, order=1, limiter=1, limiter_order=1,
                                   alpha_deg=0.0), CHANNEL_BC),
     ("roe2_water_channel", dict(CFG1, **WATER, order=1, gradient=1, limiter=1, alpha_deg=0.0), CHANNEL_BC),
+    ("turkel2_water_channel", dict(CFG1, **WATER, **PRECOND, order=1, limiter=1, alpha_deg=0.0), CHANNEL_BC),
+    ("turkel1_water_channel", dict(CFG1, **WATER, **PRECOND, alpha_deg=0.0), CHANNEL_BC),
+    ("eriksson2_far", dict(CFG1, gamma=4.4, pinf=3.0, flux_scheme=4, precond_method=3, precond_type=1,
+                           precond_mach=0.2, order=1, gradient=1, limiter=1, mach=0.1, mach_min=0.1), (1,) * 6),
+    ("btw1_far_urlocal", dict(CFG1, flux_scheme=4, precond_method=2, precond_type=2, mach=0.2, mach_min=0.2),
+     (1,) * 6),
 ]
 
 
@@ -60,9 +68,12 @@ def test_stiffened_residual_matches_restatement(gpu_available, name, cfg, face_b
     assert relerr(g["deltat"], o["deltat"]) <= 1e-12
 
 
-@pytest.mark.parametrize("flux", [0, 3])
+@pytest.mark.parametrize("flux", [0, 3, 4])
 def test_stiffened_jacobian_and_ghosts_match_restatement(gpu_available, flux):
-    cfg = dict(CFG1, **WATER, flux_scheme=flux, alpha_deg=0.0)
+    """Ghost states, approximate Jacobian (for flux 4 with the preconditioned
+    dissipation and pseudo-time term) and right-hand side on the water channel."""
+    cfg = dict(CFG1, **WATER, **PRECOND, alpha_deg=0.0)
+    cfg["flux_scheme"] = flux
     m = box_mesh((10, 5, 5), lengths=(2.0, 1.0, 1.0), jitter=0.1, seed=31, face_bc=CHANNEL_BC)
     _, cfg, Q = make_case(mesh=m, cfg=cfg, seed=31, noise=(0.0, 0.02, 0.0))
     o = restatement.first_order_step(m, cfg, Q, gs_sweeps=1)
@@ -78,18 +89,20 @@ def test_stiffened_jacobian_and_ghosts_match_restatement(gpu_available, flux):
         A, B, _ = s.get_system()
     # freestream of the stiffened gas: c^2 = gamma (p + pinf) / rho with rho = p = 1
     assert abs(farfield[6] - np.sqrt(4.4 * 6001.0)) <= 1e-13 * farfield[6]
-    assert relerr_rows(state, o["state"]) <= 1e-15
+    # ghost states carry the pressure difference through dp / c^2 and dp / (rho c)
+    assert relerr_rows(state, o["state"]) <= 1e-12
     assert relerr(A, o["A"]) <= 1e-12
     assert relerr(B, o["B"]) <= tol(cfg)
 
 
 def test_low_mach_water_channel_steady_solve(gpu_available):
-    """A small water channel (stiffened gas, low-Mach Roe, inflow/outflow and
-    slip walls, +-2 % velocity noise) converges to a 1e-8 residual drop with
-    the FP32 Jacobian/ILU(0) as with FP64, to the same state."""
+    """A small water channel (stiffened gas, Turkel-preconditioned Roe, second
+    order, inflow/outflow and slip walls, +-2 % velocity noise) reaches a 1e-8
+    residual drop with the FP32 Jacobian/ILU(0) as with FP64, to the same
+    state (both continued to the round-off floor of the stiffened EOS)."""
     from cfdsolutions_b200 import capi, default_params
-    cfg = dict(CFG1, **WATER, flux_scheme=3, order=1, gradient=1, limiter=1, venkat_k=5.0, alpha_deg=0.0,
-               cfl_min=10.0, cfl_max=1000.0, cfl_ramp=20)
+    cfg = dict(CFG1, **WATER, **PRECOND, order=1, limiter=1, venkat_k=5.0, alpha_deg=0.0,
+               cfl_min=10.0, cfl_max=1e4, cfl_ramp=20)
     m = box_mesh((16, 4, 4), lengths=(4.0, 1.0, 1.0), jitter=0.1, seed=7, face_bc=CHANNEL_BC, rcm=True)
     _, cfg, Q = make_case(mesh=m, cfg=cfg, seed=7, noise=(0.0, 0.02, 0.0))
     states = {}
@@ -97,10 +110,12 @@ def test_low_mach_water_channel_steady_solve(gpu_available):
         with Euler3DGPU(m, default_params(**cfg)) as s:
             s.set_state(Q)
             g = capi.GmresOpts(30, 30, 0.1, capi.PC_ILU0, prec, 1)
-            st = s.solve_steady(max_iterations=400, drop=1e-10, include_diss=1, linear_solver=1, gmres=g)
-            assert st.rms_last <= 1e-10 * st.rms_first, (name, st.iterations, st.rms_last / st.rms_first)
+            st = s.solve_steady(max_iterations=400, drop=1e-8, include_diss=1, linear_solver=1, gmres=g)
+            assert st.rms_last <= 1e-8 * st.rms_first, (name, st.iterations, st.rms_last / st.rms_first)
+            s.set_params(default_params(**dict(cfg, cfl_min=cfg["cfl_max"], cfl_ramp=0)))
+            s.solve_steady(max_iterations=60, drop=1e-3, include_diss=1, linear_solver=1, gmres=g)
             states[name] = s.get_state()[:, :m.nnode]
     a, b = states["fp32"], states["fp64"]
     for v in range(5):
         scale = np.abs(b[v]).max() if v in (0, 4) else np.abs(b[1:4]).max()
-        assert np.abs(a[v] - b[v]).max() <= 1e-8 * scale
+        assert np.abs(a[v] - b[v]).max() <= 1e-8 * scale, (v, np.abs(a[v] - b[v]).max() / scale)

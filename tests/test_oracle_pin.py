@@ -242,17 +242,19 @@ def test_stiffened_gas_fluxes_upwind_when_supersonic(flux, pinf):
 
 
 @pytest.mark.parametrize("face_bc,flux", [((1, 1, 1, 1, 1, 1), 0), ((1, 1, 1, 1, 1, 1), 1), ((1, 1, 1, 1, 1, 1), 2),
-                                          ((1, 1, 1, 1, 1, 1), 3), ((2, 3, 0, 0, 0, 0), 3)])
+                                          ((1, 1, 1, 1, 1, 1), 3), ((2, 3, 0, 0, 0, 0), 3),
+                                          ((1, 1, 1, 1, 1, 1), 4), ((2, 3, 0, 0, 0, 0), 4)])
 def test_stiffened_gas_freestream_preserved(face_bc, flux):
     """A uniform stiffened-gas freestream (gamma 4.4, pinf 6000, u ~ c/160)
     is a steady state: ghost states are the freestream and the residual
     vanishes to round-off of the energy flux scale.  The channel (inflow,
     outflow, slip walls) uses the low-Mach fix, whose outflow keeps the
-    freestream (without it the subsonic outflow imposes 0.935 p)."""
+    freestream (without it the subsonic outflow imposes 0.935 p), or the
+    preconditioned Roe, whose outflow imposes the freestream pressure."""
     from cfdsolutions_b200 import box_mesh
     m = box_mesh((8, 4, 4), lengths=(2.0, 1.0, 1.0), jitter=0.1, seed=5, face_bc=face_bc)
     cfg = dict(CFG1, flux_scheme=flux, gamma=4.4, pinf=6000.0, mach=0.0062, mach_min=0.0062,
-               alpha_deg=0.0 if face_bc[0] == 2 else 2.0)
+               alpha_deg=0.0 if face_bc[0] == 2 else 2.0, precond_method=5, precond_type=0, precond_mach=0.0062)
     _, cfg, Q0 = make_case(mesh=m, cfg=cfg, noise=0.0)
     s = restatement.Session(m, cfg)
     Qb = s.apply_bc(Q0)
@@ -263,3 +265,90 @@ def test_stiffened_gas_freestream_preserved(face_bc, flux):
         # each equation against its own flux scale: rho u, rho u^2 + p, (rho et + p) u
         fscale = np.abs(Qb[v]).max() * np.abs(Qb[1]).max() / Qb[0].min() + (1.0 if 1 <= v <= 3 else 0.0)
         assert np.abs(conv[v] + diss[v]).max() <= 1e-12 * fscale * amax * 20
+
+
+def _precond_expected(qa, qb, a, gamma, pinf, method, ptype, pmach):
+    """-1/2 |a| Mop Kinv |K A| Mpr (qb - qa) with |K A| from numpy's
+    eigendecomposition: the preconditioned Roe dissipation written from its
+    definition, independent of the closed-form eigenvectors under test."""
+    def prim(q):
+        rho, u = q[0], q[1:4] / q[0]
+        p = (gamma - 1.0) * (q[4] - 0.5 * rho * (u @ u)) - gamma * pinf
+        return rho, u, p, (q[4] + p) / rho, np.sqrt(gamma * (p + pinf) / rho)
+    rl, ul, _, hl, cl = prim(qa)
+    rr, ur, _, hr, cr = prim(qb)
+    rho = np.sqrt(rl * rr)
+    s = rho / (rl + rho)
+    u = ul + s * (ur - ul)
+    ht = hl + s * (hr - hl)
+    c = np.sqrt((gamma - 1.0) * (ht - 0.5 * u @ u))
+    n = a / np.linalg.norm(a)
+    mach, mmax = np.linalg.norm(u) / c, max(np.linalg.norm(ul) / cl, np.linalg.norm(ur) / cr)
+    if ptype == 0:
+        M, G = max(mach, mmax), pmach
+        b = (0.5 * M * M / (G * G) - M / G + 1.0) if M < G else 0.5
+        b = min(1.0, b * (np.sqrt(M * G) + M))
+    elif ptype == 2:
+        b = min(1.0, mach)
+    else:
+        b = min(1.0, pmach)
+    beta = b * b
+    alpha = 0.4 if method == 5 else 0.0
+    delta = 1.0 if method == 2 else beta
+    un = u @ n
+    A = np.zeros((5, 5))
+    A[0, 0] = A[1, 1] = A[2, 2] = A[3, 3] = A[4, 4] = un
+    A[0, 1:4] = rho * n
+    A[1:4, 4] = n / rho
+    A[4, 1:4] = rho * c * c * n
+    K = np.eye(5)
+    K[0, 4] = (delta - 1.0) / (c * c)
+    K[1:4, 4] = -alpha * u / (rho * c * c)
+    K[4, 4] = beta
+    lam, V = np.linalg.eig(K @ A)
+    absKA = (V @ np.diag(np.abs(lam.real)) @ np.linalg.inv(V)).real
+    q2 = u @ u
+    g1 = gamma - 1.0
+    Mpr = np.array([[1, 0, 0, 0, 0], [-u[0] / rho, 1 / rho, 0, 0, 0], [-u[1] / rho, 0, 1 / rho, 0, 0],
+                    [-u[2] / rho, 0, 0, 1 / rho, 0], [0.5 * g1 * q2, -g1 * u[0], -g1 * u[1], -g1 * u[2], g1]])
+    Mop = np.linalg.inv(Mpr)
+    return -0.5 * np.linalg.norm(a) * (Mop @ np.linalg.inv(K) @ absKA @ Mpr @ (qb - qa)), np.abs(lam.real).max()
+
+
+@pytest.mark.parametrize("method", [2, 3, 5])
+@pytest.mark.parametrize("ptype", [0, 1, 2])
+@pytest.mark.parametrize("pinf", [0.0, 6000.0])
+def test_preconditioned_roe_dissipation_matches_its_definition(method, ptype, pinf):
+    """Flux 4 (the Turkel-family preconditioned Roe of MPFLOW3D, restated;
+    the compiled reference is Euler3D, which lacks it): the closed-form
+    eigenvectors give Mop Kinv |K A| Mpr dQ, and the time-step eigenvalue is
+    the spectral radius of K A."""
+    gamma = 4.4
+    a = np.array([0.3, -0.2, 0.25])
+    c0 = np.sqrt(gamma * (1.0 + pinf))
+
+    def state(rho, p, vel):
+        return np.r_[rho, rho * vel, (p + gamma * pinf) / (gamma - 1.0) + 0.5 * rho * (vel @ vel)]
+
+    qa = state(1.0, 1.0, c0 * np.array([0.05, 0.01, -0.02]))
+    qb = state(1.02, 1.0 + 1e-3 * c0 * c0, c0 * np.array([0.045, 0.015, -0.01]))
+    cfg = dict(CFG1, flux_scheme=4, gamma=gamma, pinf=pinf, precond_method=method, precond_type=ptype,
+               precond_mach=0.1)
+    conv, diss, dts, _ = restatement.Session(_two_node_mesh(a), cfg).residual(np.stack([qa, qb], axis=1))
+    exp, lmax = _precond_expected(qa, qb, a, gamma, pinf, method, ptype, 0.1)
+    assert np.abs(diss[:, 0] - exp).max() <= 1e-9 * np.abs(exp).max(), (diss[:, 0], exp)
+    assert abs(dts[0] - np.linalg.norm(a) * lmax) <= 1e-12 * dts[0]
+
+
+def test_preconditioned_roe_without_preconditioning_is_roe():
+    """beta = 1 with BTW (K = I): flux 4 reduces to the Roe flux (on the same
+    ghost states; the two families have their own characteristic BCs)."""
+    m, cfg, Q = make_case(n=5, seed=12, noise=0.02)
+    s0 = restatement.Session(m, dict(cfg, flux_scheme=0))
+    s4 = restatement.Session(m, dict(cfg, flux_scheme=4, precond_method=2, precond_type=1, precond_mach=1.0))
+    Qb = s0.apply_bc(Q)
+    c0, d0, t0, _ = s0.residual(Qb)
+    c4, d4, t4, _ = s4.residual(Qb)
+    np.testing.assert_allclose(c4, c0, rtol=0, atol=1e-12 * np.abs(c0).max())
+    np.testing.assert_allclose(d4, d0, rtol=0, atol=1e-12 * np.abs(d0).max())
+    np.testing.assert_allclose(t4, t0, rtol=1e-13)
