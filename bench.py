@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--side-rcm", action="store_true", help="also time the plain node-level RCM numbering")
     ap.add_argument("--no-steady", action="store_true", help="skip the time-to-steady-state solves")
     ap.add_argument("--no-serve", action="store_true", help="skip the served batch")
+    ap.add_argument("--no-lowmach", action="store_true", help="skip the low-Mach liquid channel solves")
     ap.add_argument("--serve-requests", type=int, default=32)
     ap.add_argument("--serve-nmax", type=int, default=64, help="largest cube side of the served mix (config: 96)")
     ap.add_argument("--serve-rate", type=float, default=2.0, help="Poisson arrival rate, requests per second")
@@ -222,6 +223,108 @@ def steady_solves(mesh, Q, dev, stream, timed_once):
         out[name]["max_rel_err_vs_fp64"] = err  # converged fields (1e-11 drop), per-field scale
         out[name]["speedup_vs_fp64"] = out["fp64"]["seconds"] / out[name]["seconds"]
     return out
+
+
+# The low-Mach liquid channel: stiffened-gas water (gamma 4.4, pinf 6e8 Pa over
+# a 1 bar reference pressure, rho 1000 kg/m^3), u = 10 m/s (c = 1625 m/s,
+# M = 0.0062) with +-2 % seeded velocity noise, inflow / outflow / slip walls,
+# Turkel-preconditioned Roe (local beta, reference Mach = freestream Mach).
+LOWMACH_MESH = (192, 48, 48)
+LOWMACH = dict(flux_scheme=4, precond_method=5, precond_type=0, precond_mach=0.0062, order=1, gradient=0,
+               limiter=1, venkat_k=5.0, gamma=4.4, pinf=6000.0, mach=0.0062, mach_min=0.0062, alpha_deg=0.0,
+               cfl_min=10.0, cfl_max=1e4, cfl_ramp=20)
+
+
+def lowmach_case(size):
+    from cfdsolutions_b200 import box_mesh, perturbed_freestream
+    from cfdsolutions_b200.mesh import NUMBERING_PATCH_RCM
+    m = box_mesh(size, lengths=(4.0, 1.0, 1.0), jitter=0.1, seed=4242, rcm=NUMBERING_PATCH_RCM,
+                 face_bc=(2, 3, 0, 0, 0, 0))
+    Q = perturbed_freestream(m, LOWMACH["gamma"], LOWMACH["mach"], 0.0, noise=(0.0, 0.02, 0.0), seed=4243,
+                             pinf=LOWMACH["pinf"])
+    return m, Q
+
+
+def lowmach_config(m):
+    nx, ny, nz = LOWMACH_MESH
+    return {"workload": f"implicit steady solve to a {STEADY_DROP:g} L2 residual drop, 4x1x1 channel of {nx}x{ny}x{nz} "
+                        f"hexes split into tets ({m.nnode} nodes), jitter 0.1h, inflow / outflow / slip walls",
+            "physics": "stiffened-gas water: gamma 4.4, pinf 6e8 Pa (6000 over the 1 bar reference pressure), "
+                       "rho 1000 kg/m^3, u 10 m/s (c 1625 m/s, M 0.0062), +-2 % seeded velocity noise; "
+                       "Turkel-preconditioned Roe (MPFLOW3D PRECOND_METHOD_TURKEL, PRECOND_TYPE_LOCAL, reference "
+                       "Mach 0.0062), second order (LSQ gradient + Venkatakrishnan K=5), preconditioned "
+                       "characteristic BCs, CFL 10->1e4 over 20 iterations",
+            "linear": f"GMRES(30), inner rtol {STEADY_RTOL}, block-multicolour ILU(0) refactored every "
+                      f"{STEADY_PC_UPDATE} iterations",
+            "mixed": "fp32: Jacobian and ILU(0) stored in FP32 only, FP64 residual and Arnoldi"}
+
+
+def lowmach_solves(dev, stream, timed_once):
+    """Config of the low-Mach liquid channel: time to the residual drop, plain
+    FP64 and FP32 Jacobian/ILU(0); the converged states (continued untimed at
+    the final CFL to the round-off floor of the stiffened EOS) compared."""
+    from cfdsolutions_b200 import Euler3DGPU, capi, default_params
+
+    m, Q = lowmach_case(LOWMACH_MESH)
+    out, states = {"config": lowmach_config(m)}, {}
+    for name, prec in (("fp64", capi.PREC_FP64), ("fp32", capi.PREC_FP32 | capi.PREC_LOW_ONLY)):
+        with Euler3DGPU(m, default_params(**LOWMACH), device=dev, stream=stream.cuda_stream) as ss:
+            ss.set_state(Q)
+            capi.check(capi.lib.cfd_ilu_mc_order(ss.handle, None, None), "cfd_ilu_mc_order")
+            g = capi.GmresOpts(30, 30, STEADY_RTOL, capi.PC_ILU0_MC, prec, 1)
+            box = {}
+
+            def run():
+                box["st"] = ss.solve_steady(max_iterations=800, drop=STEADY_DROP, include_diss=1, linear_solver=1,
+                                            gmres=g, precond_update=STEADY_PC_UPDATE)
+
+            ms = timed_once(run)
+            st = box["st"]
+            out[name] = {"seconds": ms / 1e3, "newton_iterations": st.iterations,
+                         "gmres_iterations": st.linear_iterations, "rms_drop": st.rms_last / st.rms_first,
+                         "converged": bool(st.rms_last <= STEADY_DROP * st.rms_first)}
+            ss.set_params(default_params(**dict(LOWMACH, cfl_min=LOWMACH["cfl_max"], cfl_ramp=0)))
+            st2 = ss.solve_steady(max_iterations=100, drop=1e-4, include_diss=1, linear_solver=1, gmres=g,
+                                  precond_update=STEADY_PC_UPDATE)
+            out[name]["rms_drop_compared"] = st2.rms_last / st.rms_first
+            states[name] = ss.get_state()[:, :m.nnode]
+    ref = states["fp64"]
+    mom = float(np.abs(ref[1:4]).max())
+    err = 0.0
+    for v in range(5):
+        scale = max(float(np.abs(ref[v]).max()), mom if 1 <= v <= 3 else 0.0)
+        err = max(err, float(np.abs(states["fp32"][v] - ref[v]).max()) / scale)
+    out["fp32"]["max_rel_err_vs_fp64"] = err
+    out["fp32"]["speedup_vs_fp64"] = out["fp64"]["seconds"] / out["fp32"]["seconds"]
+    return m, out
+
+
+def lowmach_port_rate(size, iters):
+    """The oracle's restatement of the same implicit iteration (single
+    threaded) on a smaller channel: node-iterations per second."""
+    import time as _t
+    from oracle import restatement
+    m, Q = lowmach_case(size)
+    n = m.nnode
+    per = []
+    for it in range(iters + 1):
+        t0 = _t.perf_counter()
+        s = restatement.Session(m, LOWMACH, iteration=it)
+        Qb = s.apply_bc(Q)
+        gr = s.gradient(Qb, 0)
+        phi = s.limiter(Qb, gr)
+        conv, diss, dts, _ = s.residual(Qb, gr, phi)
+        dt, _ = s.deltat(dts)
+        A, B = s.jacobian(Qb, dt, conv, diss, include_diss=1)
+        X, _, _, _ = s.gmres(A, B, m=30, maxit=30, rtol=STEADY_RTOL, precond=2)
+        Q = Qb.copy()
+        Q[:, :n] += X.T
+        per.append(_t.perf_counter() - t0)
+    per_it = statistics.mean(per[1:])
+    sample = (f"{size[0]}x{size[1]}x{size[2]}-hex channel ({n} nodes), 1+{iters} implicit iterations of the "
+              "oracle's C restatement (BC, LSQ gradient, Venkatakrishnan, preconditioned Roe residual, dt, "
+              "preconditioned Jacobian, GMRES(30)+ILU(0) to rtol 0.1, update), one thread")
+    return n / per_it, per_it, sample
 
 
 def reference_implicit_rate(sample_n, procs, iters):
@@ -508,22 +611,22 @@ def main():
     s.close()
 
     # ---- time to the steady residual drop (plain FP64 and mixed precision)
+    def timed_once(fn):
+        barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        fn()
+        ev1.record(stream)
+        barrier()
+        ms = ev0.elapsed_time(ev1)
+        if world > 1:
+            t = torch.tensor([ms], device=f"cuda:{dev}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
     steady = None
     if not args.no_steady:
-        def timed_once(fn):
-            barrier()
-            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            ev0.record(stream)
-            fn()
-            ev1.record(stream)
-            barrier()
-            ms = ev0.elapsed_time(ev1)
-            if world > 1:
-                t = torch.tensor([ms], device=f"cuda:{dev}")
-                dist.all_reduce(t, op=dist.ReduceOp.MAX)
-                ms = float(t.item())
-            return ms
-
         steady = {"metric": "time to steady residual drop", "unit": "s", "higher_is_better": False,
                   "config": steady_config(args.n)}
         steady.update(steady_solves(mesh, Q, dev, stream, timed_once))
@@ -536,6 +639,17 @@ def main():
                 steady["cpu_baseline"] = {"value": rate, "unit": "node-iterations/s", "cores": procs,
                                           "kind": "reference", "sample": sample, "seconds_per_iteration": per_it,
                                           "gpu_fp64_value": gpu_rate}
+
+    # ---- the low-Mach liquid channel (stiffened gas, preconditioned Roe)
+    lowmach = None
+    if not args.no_lowmach:
+        lm_mesh, lowmach = lowmach_solves(dev, stream, timed_once)
+        lowmach.update({"metric": "time to steady residual drop", "unit": "s", "higher_is_better": False})
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            rate, per_it, sample = lowmach_port_rate((96, 24, 24), 3)
+            gpu_rate = lm_mesh.nnode * lowmach["fp64"]["newton_iterations"] / lowmach["fp64"]["seconds"]
+            lowmach["cpu_baseline"] = {"value": rate, "unit": "node-iterations/s", "cores": 1, "kind": "port",
+                                       "sample": sample, "seconds_per_iteration": per_it, "gpu_fp64_value": gpu_rate}
 
     # ---- served batch (continuous admission) vs sequential plain FP64 solves
     serve = None
@@ -578,7 +692,8 @@ def main():
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded tet-split cube, seeded +-1% state noise)",
             "config": workload_config(args.n, mesh), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": KERNELS_PER_STEP * args.steps, "clocks": clocks, "per_flux": per_flux,
-            "breakdown_ms": breakdown, "variants": side, "setup_s": setup_s, "steady": steady, "serve": serve,
+            "breakdown_ms": breakdown, "variants": side, "setup_s": setup_s, "steady": steady, "lowmach": lowmach,
+            "serve": serve,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
