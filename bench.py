@@ -61,6 +61,8 @@ def parse():
                     help="small linear-solve case for ncu captures (Jacobian + one GMRES(30) call per precision)")
     ap.add_argument("--profile", action="store_true",
                     help="profiling case for ncu: two residual steps per kernel variant, no timing, no output line")
+    ap.add_argument("--profile-lowmach", type=int, default=0, metavar="ITERS",
+                    help="ncu case: ITERS implicit iterations of the low-Mach channel (FP32 Jacobian), no output line")
     return ap.parse_args()
 
 
@@ -437,6 +439,20 @@ def profile_case(n):
             s.synchronize()
 
 
+def profile_lowmach_case(iters):
+    """`--profile-lowmach ITERS`: the low-Mach channel's first ITERS implicit
+    iterations with the FP32 low-precision-only system, for launch lists."""
+    from cfdsolutions_b200 import Euler3DGPU, capi, default_params
+    m, Q = lowmach_case(LOWMACH_MESH)
+    with Euler3DGPU(m, default_params(**LOWMACH)) as ss:
+        ss.set_state(Q)
+        capi.check(capi.lib.cfd_ilu_mc_order(ss.handle, None, None), "cfd_ilu_mc_order")
+        g = capi.GmresOpts(30, 30, STEADY_RTOL, capi.PC_ILU0_MC, capi.PREC_FP32 | capi.PREC_LOW_ONLY, 1)
+        ss.solve_steady(max_iterations=iters, drop=STEADY_DROP, include_diss=1, linear_solver=1, gmres=g,
+                        precond_update=STEADY_PC_UPDATE)
+        ss.synchronize()
+
+
 def profile_linear_case(n):
     """Small fixed case for ncu captures of the linear solver
     (`--profile-linear --n 64`): the steady workload's Jacobian at CFL 1000 on
@@ -478,6 +494,9 @@ def main():
         return
     if args.profile:
         profile_case(args.n)
+        return
+    if args.profile_lowmach:
+        profile_lowmach_case(args.profile_lowmach)
         return
     if args.profile_linear:
         profile_linear_case(args.n)

@@ -213,6 +213,15 @@ __global__ void k_mc_factor(const int *__restrict__ patches, int npatch, int n, 
     }
 }
 
+// Programmatic dependent launch (sm_90+): the solve of one colour lets the
+// next colour's launch begin as soon as all of its own CTAs are resident
+// (launch_dependents), and that launch stages its constant factor blocks
+// before waiting (wait) for the vectors the earlier launches write.  Every
+// CTA of the earlier grid is resident before a dependent CTA can start, so
+// the earlier grid always completes.  Both are no-ops in a plain launch.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Blocks of a row inside its own patch staged in shared memory before the
 // level loop of a triangular solve (more go through the load path).
 template <typename TM>
@@ -244,10 +253,12 @@ __global__ void __launch_bounds__(5 * kMcRows, 6) k_mc_fwd(const int *__restrict
     const bool act = q < nr;
     const int i = p0 + q;
     double s = 0.0;
-    int lev = -1, ui = 0, ue = 0;
+    int lev = -1, ui = 0, ue = 0, base = 0;
+    // the next colour's launch may start staging its constant factors now
+    pdl_trigger();
     if (act) {
         const int4 mt = meta[i];
-        const int base = IA[i];
+        base = IA[i];
         lev = mt.w & 0xffff;
         ui = base + mt.x;
         ue = base + mt.y;
@@ -259,6 +270,9 @@ __global__ void __launch_bounds__(5 * kMcRows, 6) k_mc_fwd(const int *__restrict
 #pragma unroll
                 for (int c = 0; c < 5; c++) pa[t * 5 + c][tid] = am[c];
             }
+    }
+    pdl_wait();  // r and the earlier colours' y are complete from here on
+    if (act) {
         s = r[(int64_t)i * 5 + m];
 #pragma unroll 4
         for (int u = base; u < ui; u++) {
@@ -311,15 +325,16 @@ __global__ void __launch_bounds__(5 * kMcRows, 6) k_mc_bwd(const int *__restrict
     const bool act = q < nr;
     const int i = p0 + q;
     double s = 0.0;
-    int lev = -1, u0 = 0, u1 = 0;
+    int lev = -1, u0 = 0, u1 = 0, end = 0;
     TM dg[5];
+    pdl_trigger();
     if (act) {
         const int4 mt = meta[i];
         const int base = IA[i];
         lev = mt.w >> 16;
         u0 = base + mt.y + 1;  // first upper entry
         u1 = u0 + mt.z;        // first upper entry outside the patch
-        const int end = IA[i + 1];
+        end = IA[i + 1];
 #pragma unroll
         for (int t = 0; t < K; t++)
             if (u0 + t < u1) {
@@ -331,6 +346,9 @@ __global__ void __launch_bounds__(5 * kMcRows, 6) k_mc_bwd(const int *__restrict
         const TM *d = M + (int64_t)(u0 - 1) * 25 + m * 5;
 #pragma unroll
         for (int c = 0; c < 5; c++) dg[c] = d[c];
+    }
+    pdl_wait();  // y and the later colours' z are complete from here on
+    if (act) {
         s = y[(int64_t)i * 5 + m];
 #pragma unroll 4
         for (int u = u1; u < end; u++) {
@@ -542,15 +560,26 @@ int mc_factor(cfd_ctx *c, const TA *A, TM *M) {
 template <typename TM>
 static int mc_apply_launch(cfd_ctx *c, const TM *M, const double *r, double *tmp, double *z) {
     Abmc &mc = c->mc;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t lc = {};
+    lc.blockDim = dim3(5 * kMcRows);
+    lc.dynamicSmemBytes = 0;
+    lc.stream = c->stream;
+    lc.attrs = at;
+    lc.numAttrs = 1;
     for (int k = 0; k < mc.ncolor; k++) {
-        const int cnt = mc.cptr[k + 1] - mc.cptr[k];
-        k_mc_fwd<TM><<<cnt, 5 * kMcRows, 0, c->stream>>>(mc.patches.p + mc.cptr[k], c->nnode, c->IA.p, mc.scol.p,
-                                                           mc.meta.p, mc.plev.p, M, r, tmp);
+        lc.gridDim = dim3(mc.cptr[k + 1] - mc.cptr[k]);
+        CFD_CUDA(cudaLaunchKernelEx(&lc, k_mc_fwd<TM>, (const int *)(mc.patches.p + mc.cptr[k]), c->nnode,
+                                    (const int *)c->IA.p, (const int *)mc.scol.p, (const int4 *)mc.meta.p,
+                                    (const int2 *)mc.plev.p, M, r, tmp));
     }
     for (int k = mc.ncolor - 1; k >= 0; k--) {
-        const int cnt = mc.cptr[k + 1] - mc.cptr[k];
-        k_mc_bwd<TM><<<cnt, 5 * kMcRows, 0, c->stream>>>(mc.patches.p + mc.cptr[k], c->nnode, c->IA.p, mc.scol.p,
-                                                           mc.meta.p, mc.plev.p, M, tmp, z);
+        lc.gridDim = dim3(mc.cptr[k + 1] - mc.cptr[k]);
+        CFD_CUDA(cudaLaunchKernelEx(&lc, k_mc_bwd<TM>, (const int *)(mc.patches.p + mc.cptr[k]), c->nnode,
+                                    (const int *)c->IA.p, (const int *)mc.scol.p, (const int4 *)mc.meta.p,
+                                    (const int2 *)mc.plev.p, M, (const double *)tmp, z));
     }
     CFD_LAUNCH_CHECK();
     return CFD_OK;
