@@ -468,7 +468,8 @@ __global__ void k_add_diss(int64_t n, const double *__restrict__ a, const double
 //   A[L,R] = dFdR = 0.5 (J(Q_R) - |A|) area,  A[R,L] = -dFdL = -0.5 (J(Q_L) + |A|) area.
 // Every off-diagonal slot belongs to exactly one edge, so no zeroing and no
 // accumulation is needed.
-template <typename TA, bool PC>
+// MODE: 0 Roe, 1 preconditioned Roe (CFD_FLUX_ROE_PRECOND), 2 Thornber (|A| of the modified states)
+template <typename TA, int MODE>
 __global__ void __launch_bounds__(128) k_jac_edges(int nedge, int64_t ldq, const double *__restrict__ Q,
                                                    const int2 *__restrict__ en, const double4 *__restrict__ eg,
                                                    const int2 *__restrict__ eslot, Flow f, double *__restrict__ A64,
@@ -484,8 +485,15 @@ __global__ void __launch_bounds__(128) k_jac_edges(int nedge, int64_t ldq, const
         qR[v] = Q[v * ldq + nd.y];
     }
     double Ab[25], J[25];
-    if (PC) pc_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
-    else roe_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
+    if (MODE == 1) {
+        pc_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
+    } else if (MODE == 2) {
+        double mL[5], mR[5];
+        thornber_states(qL, qR, f, mL, mR);
+        roe_abs_jacobian(mL, mR, g.x, g.y, g.z, f, Ab);
+    } else {
+        roe_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
+    }
     const int2 sl = eslot[e];
     const double ha = 0.5 * g.w;
     euler_flux_jacobian(qR, g.x, g.y, g.z, f.gamma, f.gpinf, J);
@@ -507,7 +515,7 @@ __global__ void __launch_bounds__(128) k_jac_edges(int nedge, int64_t ldq, const
 // Diagonal blocks and right-hand side, one thread per row:
 //   A[i,i] = V_i/dt_i I - sum_j A[j,i] + sum_b 0.5 (J(Q_i) + |A|)_b area_b
 //   B_i    = -(Res_i [+ Res_Diss_i])
-template <typename TA, bool PC>
+template <typename TA, int MODE>
 __global__ void __launch_bounds__(128) k_jac_rows(
     int nnode, int64_t ldq, const double *__restrict__ Q, const int *__restrict__ IA, const int *__restrict__ IAU,
     const int *__restrict__ tslot, const int *__restrict__ n2b_ptr, const int *__restrict__ n2b,
@@ -519,7 +527,7 @@ __global__ void __launch_bounds__(128) k_jac_rows(
     if (i >= nnode) return;
     double D[25];
     const double vd = add_time ? vol[i] / dt[i] : 0.0;
-    if (PC && add_time) {
+    if (MODE == 1 && add_time) {
         // preconditioned pseudo-time term (V/dt) Cinv (Roe_Jacobian.cpp:241-264)
         double qi[5];
 #pragma unroll
@@ -554,8 +562,15 @@ __global__ void __launch_bounds__(128) k_jac_rows(
             qL[v] = Q[v * ldq + nd.x];
             qR[v] = Q[v * ldq + nd.y];
         }
-        if (PC) pc_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
-        else roe_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
+        if (MODE == 1) {
+            pc_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
+        } else if (MODE == 2) {
+            double mL[5], mR[5];
+            thornber_states(qL, qR, f, mL, mR);
+            roe_abs_jacobian(mL, mR, g.x, g.y, g.z, f, Ab);
+        } else {
+            roe_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
+        }
         euler_flux_jacobian(qL, g.x, g.y, g.z, f.gamma, f.gpinf, J);
         const double ha = 0.5 * g.w;
 #pragma unroll
@@ -575,17 +590,24 @@ __global__ void __launch_bounds__(128) k_jac_rows(
 }
 
 // Edge blocks then diagonal blocks and right-hand side of the approximate
-// Roe Jacobian (PC: the preconditioned Roe's dissipation and pseudo-time term).
-template <typename TA, bool PC>
+// Roe Jacobian (MODE as k_jac_edges).
+template <typename TA, int MODE>
 static void launch_jacobian(cfd_ctx *c, int add_time, int include_diss, double *A64, TA *Alow) {
     const int ge = grid_for(c->nedge, 128), gr = grid_for(c->nnode, 128);
     if (c->nedge)
-        k_jac_edges<TA, PC><<<ge, 128, 0, c->stream>>>(c->nedge, c->ldq, c->Q.p, c->edge_nodes.p, c->edge_geo.p,
+        k_jac_edges<TA, MODE><<<ge, 128, 0, c->stream>>>(c->nedge, c->ldq, c->Q.p, c->edge_nodes.p, c->edge_geo.p,
                                                        c->eslot.p, c->flow, A64, Alow);
-    k_jac_rows<TA, PC><<<gr, 128, 0, c->stream>>>(c->nnode, c->ldq, c->Q.p, c->IA.p, c->IAU.p, c->tslot.p,
+    k_jac_rows<TA, MODE><<<gr, 128, 0, c->stream>>>(c->nnode, c->ldq, c->Q.p, c->IA.p, c->IAU.p, c->tslot.p,
                                                   c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p,
                                                   c->cvol.p, c->dt.p, c->res.p, c->resd.p, add_time, include_diss,
                                                   c->flow, A64, Alow, c->B.p);
+}
+
+template <typename TA>
+static void dispatch_jacobian(int mode, cfd_ctx *c, int add_time, int include_diss, double *A64, TA *Alow) {
+    if (mode == 1) launch_jacobian<TA, 1>(c, add_time, include_diss, A64, Alow);
+    else if (mode == 2) launch_jacobian<TA, 2>(c, add_time, include_diss, A64, Alow);
+    else launch_jacobian<TA, 0>(c, add_time, include_diss, A64, Alow);
 }
 
 // ---- block Gauss-Seidel (MC_Iterative_Block_LU_Jacobi_CRS,
@@ -1032,7 +1054,7 @@ int cfd_set_stream(cfd_ctx *c, void *stream) {
 
 int cfd_set_params(cfd_ctx *c, const cfd_params *p) {
     if (!c || !p) { set_error("cfd_set_params: NULL"); return CFD_ERR_ARG; }
-    if (p->flux_scheme < CFD_FLUX_ROE || p->flux_scheme > CFD_FLUX_ROE_PRECOND) {
+    if (p->flux_scheme < CFD_FLUX_ROE || p->flux_scheme > CFD_FLUX_ROE_THORNBER) {
         set_error("cfd_set_params: invalid flux scheme %d", p->flux_scheme);
         return CFD_ERR_ARG;
     }
@@ -1461,6 +1483,8 @@ int cfd_residual(cfd_ctx *c, int add_time) {
         case 7: return residual_with_fix<CFD_FLUX_ROE_LMFIX, true>(c, add_time);
         case 8: return residual_with_fix<CFD_FLUX_ROE_PRECOND, false>(c, add_time);
         case 9: return residual_with_fix<CFD_FLUX_ROE_PRECOND, true>(c, add_time);
+        case 10: return residual_with_fix<CFD_FLUX_ROE_THORNBER, false>(c, add_time);
+        case 11: return residual_with_fix<CFD_FLUX_ROE_THORNBER, true>(c, add_time);
         default: set_error("cfd_residual: bad flux scheme"); return CFD_ERR_ARG;
     }
 }
@@ -1512,18 +1536,16 @@ int cfd_jacobian(cfd_ctx *c, int add_time, int include_diss, int precision) {
     c->a_precision = precision;
     c->a64_valid = !low_only;
     double *A64 = low_only ? nullptr : c->A64.p;
-    const bool pc = c->params.flux_scheme == CFD_FLUX_ROE_PRECOND;
+    const int mode = c->params.flux_scheme == CFD_FLUX_ROE_PRECOND ? 1
+                     : (c->params.flux_scheme == CFD_FLUX_ROE_THORNBER ? 2 : 0);
     if (precision == CFD_PREC_FP32) {
         CFD_CUDA(c->A32.alloc((size_t)c->nnzb * 25));
-        if (pc) launch_jacobian<float, true>(c, add_time, include_diss, A64, c->A32.p);
-        else launch_jacobian<float, false>(c, add_time, include_diss, A64, c->A32.p);
+        dispatch_jacobian<float>(mode, c, add_time, include_diss, A64, c->A32.p);
     } else if (precision == CFD_PREC_BF16) {
         CFD_CUDA(c->A16.alloc((size_t)c->nnzb * 25));
-        if (pc) launch_jacobian<uint16_t, true>(c, add_time, include_diss, A64, c->A16.p);
-        else launch_jacobian<uint16_t, false>(c, add_time, include_diss, A64, c->A16.p);
+        dispatch_jacobian<uint16_t>(mode, c, add_time, include_diss, A64, c->A16.p);
     } else {
-        if (pc) launch_jacobian<float, true>(c, add_time, include_diss, A64, (float *)nullptr);
-        else launch_jacobian<float, false>(c, add_time, include_diss, A64, (float *)nullptr);
+        dispatch_jacobian<float>(mode, c, add_time, include_diss, A64, (float *)nullptr);
     }
     CFD_LAUNCH_CHECK();
     c->has_system = true;

@@ -63,8 +63,8 @@ __device__ void mat5_mul(const double *A, const double *B, double *Out) {
         }
 }
 
-// Matrix-form Roe flux of two first-order states (Compute_RoeFlux without
-// low-Mach preconditioning): conv = 1/2 (F_L + F_R) area,
+// Matrix-form Roe flux of two first-order states (Compute_RoeFlux, with its
+// low-Mach-fix branch for CFD_FLUX_ROE_LMFIX): conv = 1/2 (F_L + F_R) area,
 // diss = -1/2 (M P |Lambda| Pinv Minv) (Q_R - Q_L) area.
 __device__ void ref_roe_flux(const double qL[5], const double qR[5], double nx, double ny, double nz, double area,
                              const Flow &f, double conv[5], double diss[5]) {
@@ -129,6 +129,53 @@ __device__ void ref_roe_flux(const double qL[5], const double qR[5], double nx, 
     } else {
         E[18] = fabs(ubar + c);
         E[24] = fabs(ubar - c);
+    }
+    if (f.lmfix) {
+        // PRECOND_METHOD_ROE_LMFIX branch of Compute_RoeFlux (Roe_Fluxes.cpp:641-685, :820-848):
+        // fix = min(1, (|u.n| + |u.t1| + |u.t2|) / c) at the Roe average; |A| acts on the
+        // density and pressure jumps, and the velocity jump enters through fix * (du.n)
+        double nmax = fabs(nx);
+        int mc = 1;
+        if (nmax < fabs(ny)) { nmax = fabs(ny); mc = 2; }
+        if (nmax < fabs(nz)) { nmax = fabs(nz); mc = 3; }
+        double t1[3] = {1.0, 1.0, 1.0};
+        if (mc == 1) t1[0] = -(ny + nz) / nx;
+        else if (mc == 2) t1[1] = -(nx + nz) / ny;
+        else t1[2] = -(nx + ny) / nz;
+        double mg = sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+        if (mg > 1.0e-20) { t1[0] = t1[0] / mg; t1[1] = t1[1] / mg; t1[2] = t1[2] / mg; }
+        const double ub1 = u * t1[0] + v * t1[1] + w * t1[2];
+        double t2[3] = {+t1[1] * nz - t1[2] * ny, -t1[0] * nz + t1[2] * nx, +t1[0] * ny - t1[1] * nx};
+        mg = sqrt(t2[0] * t2[0] + t2[1] * t2[1] + t2[2] * t2[2]);
+        if (mg > 1.0e-20) { t2[0] = t2[0] / mg; t2[1] = t2[1] / mg; t2[2] = t2[2] / mg; }
+        const double ub2 = u * t2[0] + v * t2[1] + w * t2[2];
+        double mach = fabs(ubar) + fabs(ub1) + fabs(ub2);
+        mach = mach / c;
+        const double fix = mach < 1.0 ? mach : 1.0;
+        mat5_mul(E, Pinv, Tinv);
+        mat5_mul(T, Tinv, A);  // M P |Lambda| Pinv
+        const double d1[5] = {R.rho - L.rho, 0.0, 0.0, 0.0, R.p - L.p};
+        double fa[5], dw[5], md[5];
+        for (int i = 0; i < 5; i++) {
+            fa[i] = 0.0;
+            for (int k = 0; k < 5; k++) fa[i] += A[i * 5 + k] * d1[k];
+        }
+        const double fixUn = fix * ((R.u - L.u) * nx + (R.v - L.v) * ny + (R.w - L.w) * nz);
+        const double ap = fabs(ubar + c), am = fabs(ubar - c);
+        dw[0] = (0.5 * rho * fixUn * (ap - am)) / c;
+        dw[1] = fabs(ubar) * ((R.u - L.u) - fixUn * nx) + 0.5 * nx * fixUn * (ap + am);
+        dw[2] = fabs(ubar) * ((R.v - L.v) - fixUn * ny) + 0.5 * ny * fixUn * (ap + am);
+        dw[3] = fabs(ubar) * ((R.w - L.w) - fixUn * nz) + 0.5 * nz * fixUn * (ap + am);
+        dw[4] = 0.5 * rho * c * fixUn * (ap - am);
+        for (int i = 0; i < 5; i++) {
+            md[i] = 0.0;
+            for (int k = 0; k < 5; k++) md[i] += M[i * 5 + k] * dw[k];
+        }
+        for (int i = 0; i < 5; i++) {
+            conv[i] = 0.5 * (fl[i] + fr[i]) * area;
+            diss[i] = -0.5 * (fa[i] + md[i]) * area;
+        }
+        return;
     }
     mat5_mul(Pinv, Minv, Tinv);
     mat5_mul(E, Tinv, A);
@@ -346,6 +393,12 @@ extern "C" int cfd_jacobian_fd(cfd_ctx *c, int add_time, int include_diss, int m
     if (method < CFD_JAC_CENTRAL || method > CFD_JAC_ALTERNATE) {
         set_error("cfd_jacobian_fd: method must be CFD_JAC_CENTRAL, _FORWARD, _BACKWARD or _ALTERNATE");
         return CFD_ERR_ARG;
+    }
+    if (c->params.flux_scheme != CFD_FLUX_ROE && c->params.flux_scheme != CFD_FLUX_ROE_LMFIX) {
+        // Compute_Jacobian_FiniteDifference_Roe differences the Roe flux (Roe_Jacobian.cpp:236)
+        set_error("cfd_jacobian_fd: the finite-difference Jacobian is defined for the Roe flux (with or "
+                  "without the low-Mach fix)");
+        return CFD_ERR_UNSUPPORTED;
     }
     CFD_CUDA(cudaSetDevice(c->device));
     if (method == CFD_JAC_ALTERNATE)  // Roe_Jacobian.cpp:282-287

@@ -139,12 +139,18 @@ __device__ __forceinline__ double edge_flux(const double qL[5], const double qR[
     if (FLUX == CFD_FLUX_HLLC) return hllc_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
     if (FLUX == CFD_FLUX_AUSM) return ausmp_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
     if (FLUX == CFD_FLUX_ROE_PRECOND) return roe_precond_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
+    if (FLUX == CFD_FLUX_ROE_THORNBER) {
+        double mL[5], mR[5];
+        thornber_states(qL, qR, f, mL, mR);
+        return roe_flux<false>(mL, mR, nx, ny, nz, area, f, conv, diss, lam);
+    }
     return roe_flux<FLUX == CFD_FLUX_ROE_LMFIX>(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
 }
 
 // The Roe family (plain, low-Mach fix, preconditioned): the limiter pressure fix applies.
 __host__ __device__ constexpr bool is_roe_flux(int flux) {
-    return flux == CFD_FLUX_ROE || flux == CFD_FLUX_ROE_LMFIX || flux == CFD_FLUX_ROE_PRECOND;
+    return flux == CFD_FLUX_ROE || flux == CFD_FLUX_ROE_LMFIX || flux == CFD_FLUX_ROE_PRECOND ||
+           flux == CFD_FLUX_ROE_THORNBER;
 }
 
 // Pressure of the Roe-averaged state of two reconstructed face states

@@ -339,6 +339,31 @@ __device__ __forceinline__ void roe_abs_jacobian(const double qL[5], const doubl
     }
 }
 
+// Thornber's low-Mach modification (Compute_Flux_Roe_Thornber,
+// MPFLOW3D/src/Roe_Fluxes.cpp:1141-1165): with z = min(1, max(M_L, M_R)) the
+// face velocities become u_L' = ((1+z) u_L + (1-z) u_R)/2 and symmetrically
+// u_R'; density and total energy stay, so the pressure follows the changed
+// kinetic energy.  The Roe flux is then formed from the modified states.
+__device__ __forceinline__ void thornber_states(const double qL[5], const double qR[5], const Flow &f,
+                                                double mL[5], double mR[5]) {
+    Face L, R;
+    eos_face(qL, 1.0, 0.0, 0.0, f, true, L);
+    eos_face(qR, 1.0, 0.0, 0.0, f, true, R);
+    const double ml = sqrt(L.u * L.u + L.v * L.v + L.w * L.w) / L.c;
+    const double mr = sqrt(R.u * R.u + R.v * R.v + R.w * R.w) / R.c;
+    const double z = fmin(1.0, fmax(ml, mr));
+    mL[0] = qL[0];
+    mR[0] = qR[0];
+#pragma unroll
+    for (int i = 1; i < 4; i++) {
+        const double ul = qL[i] / qL[0], ur = qR[i] / qR[0];
+        mL[i] = qL[0] * (0.5 * ((1.0 + z) * ul + (1.0 - z) * ur));
+        mR[i] = qR[0] * (0.5 * ((1.0 + z) * ur + (1.0 - z) * ul));
+    }
+    mL[4] = qL[4];
+    mR[4] = qR[4];
+}
+
 // ---------------------------------------------------------------------------
 // Low-Mach preconditioned Roe of the Turkel family (MPFLOW3D:
 // Compute_Flux_Roe_Precondition_Turkel, MPFLOW3D/src/Roe_Fluxes.cpp:2043-2526;

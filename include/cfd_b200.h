@@ -64,6 +64,10 @@ extern "C" {
                                 MPFLOW3D/src/Roe_Fluxes.cpp:2043), its eigenvalues in the time step,
                                 the preconditioned pseudo-time term of the Jacobian (Roe_Jacobian.cpp:241)
                                 and the preconditioned characteristic BC (MPFLOW3D/src/BC.cpp:113) */
+#define CFD_FLUX_ROE_THORNBER 5 /* FLUX_SCHEME_ROE with MPFLOW3D's PRECOND_METHOD_THORNBER: the face velocities
+                                blended toward each other by min(1, max Mach) before the Roe flux
+                                (Compute_Flux_Roe_Thornber, MPFLOW3D/src/Roe_Fluxes.cpp:1081), plain
+                                characteristic BCs */
 /* cfd_params.precond_method (MPFLOW3D PRECOND_METHOD values) */
 #define CFD_PRECOND_BTW      2  /* Briley-Taylor-Whitfield: alpha 0, delta 1    */
 #define CFD_PRECOND_ERIKSSON 3  /* Eriksson: alpha 0, delta beta                */

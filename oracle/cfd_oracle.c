@@ -464,6 +464,24 @@ static void entropy_fix(double ubL, double cL, double ubR, double cR, double ub,
     E[2] = fabs(l) < eps ? (l * l + eps * eps) / (2.0 * eps) : fabs(l);
 }
 
+/* Thornber modification (Compute_Flux_Roe_Thornber, MPFLOW3D/src/Roe_Fluxes.cpp:1141-1165,
+ * conservative variables): z = min(1, max(M_L, M_R)); u_L' = ((1+z) u_L + (1-z) u_R)/2,
+ * u_R' symmetric; density and total energy unchanged. */
+static void thornber(const double *qL, const double *qR, const orc_params *p, double *mL, double *mR) {
+    face_t L, R;
+    eos_face(qL, 1.0, 0.0, 0.0, p->gamma, p->pinf, &L);
+    eos_face(qR, 1.0, 0.0, 0.0, p->gamma, p->pinf, &R);
+    double z = dmin(1.0, dmax(sqrt(L.u * L.u + L.v * L.v + L.w * L.w) / L.c,
+                              sqrt(R.u * R.u + R.v * R.v + R.w * R.w) / R.c));
+    mL[0] = qL[0]; mR[0] = qR[0]; mL[4] = qL[4]; mR[4] = qR[4];
+    for (int i = 1; i < 4; i++) {
+        double t1 = 0.5 * ((1.0 + z) * qL[i] / qL[0] + (1.0 - z) * qR[i] / qR[0]);
+        double t2 = 0.5 * ((1.0 + z) * qR[i] / qR[0] + (1.0 - z) * qL[i] / qL[0]);
+        mL[i] = qL[0] * t1;
+        mR[i] = qR[0] * t2;
+    }
+}
+
 /* Compute_Flux_Roe_Optimized (Euler3D/src/FluxTest.cpp:3026-3200). */
 static double roe(const double *qL, const double *qR, const double *n, double area, const orc_params *p,
                   double *conv, double *diss, double lam[3]) {
@@ -645,7 +663,13 @@ void orc_residual(const orc_mesh *m, const orc_params *p, const double *Q, const
             if (p->flux == 1) lmax = hllc(qL, qR, n, area, p, fc, fd);
             else if (p->flux == 2) lmax = ausmp(qL, qR, n, area, p, fc, fd);
             else {
-                lmax = p->flux == 4 ? roe_pc(qL, qR, n, area, p, fc, fd, lam) : roe(qL, qR, n, area, p, fc, fd, lam);
+                if (p->flux == 5) {
+                    double mL[5], mR[5];
+                    thornber(qL, qR, p, mL, mR);
+                    lmax = roe(mL, mR, n, area, p, fc, fd, lam);
+                } else {
+                    lmax = p->flux == 4 ? roe_pc(qL, qR, n, area, p, fc, fd, lam) : roe(qL, qR, n, area, p, fc, fd, lam);
+                }
                 ext[0] = dmin(ext[0], lam[0]); ext[1] = dmax(ext[1], lam[0]);
                 ext[2] = dmin(ext[2], lam[1]); ext[3] = dmax(ext[3], lam[1]);
                 ext[4] = dmin(ext[4], lam[2]); ext[5] = dmax(ext[5], lam[2]);
@@ -799,7 +823,7 @@ void orc_limiter(const orc_mesh *m, const orc_params *p, const double *Q, const 
         }
         for (int v = 0; v < 5; v++) phi[IDX(v, i, nn)] = ph[v];
     }
-    if (p->flux != 0 && p->flux != 3 && p->flux != 4) return;
+    if (p->flux != 0 && p->flux != 3 && p->flux != 4 && p->flux != 5) return;
     for (int i = 0; i < nn; i++) {
         for (int k = m->ia[i]; k < m->ia[i + 1]; k++) {
             int j = m->ja[k];
@@ -947,6 +971,10 @@ void orc_jacobian(const orc_mesh *m, const orc_params *p, const double *Q, const
                 double avg[4];
                 pc_edge(qL, qR, n, p, &Lf, &Rf, avg, &S);
                 pc_absA(&S, avg, p->gamma, Ab);
+            } else if (p->flux == 5) {
+                double mL[5], mR[5];
+                thornber(qL, qR, p, mL, mR);
+                roe_absA(mL, mR, n, p, Ab);
             } else {
                 roe_absA(qL, qR, n, p, Ab);
             }

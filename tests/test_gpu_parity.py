@@ -185,8 +185,8 @@ def test_block_lusgs_bit_exact(gpu_available, ref_available, iters):
     assert rms == ref["lusgs_rms"][0]
 
 
-@pytest.mark.parametrize("method,iteration", [(0, 0), (1, 0), (2, 0), (3, 1)])
-def test_finite_difference_jacobian_matches_reference(gpu_available, ref_available, method, iteration):
+@pytest.mark.parametrize("method,iteration,flux", [(0, 0, 0), (1, 0, 0), (2, 0, 0), (3, 1, 0), (0, 0, 3), (3, 1, 3)])
+def test_finite_difference_jacobian_matches_reference(gpu_available, ref_available, method, iteration, flux):
     """Finite-difference Roe Jacobian (JACOBIAN_METHOD_CENTRAL / FORWARD /
     BACKWARD / ALTERNATE) from the reference's own state after its boundary
     update: the off-diagonal blocks (interior-edge difference quotients of
@@ -194,8 +194,10 @@ def test_finite_difference_jacobian_matches_reference(gpu_available, ref_availab
     blocks, summed per row in another order, to 1e-13 of the row scale.
     Through this library's own boundary update the ghost states differ from
     the reference's in the last bits, which the 1e-8 difference quotient of
-    the boundary blocks amplifies by up to 1e8: the diagonal agrees to 1e-8."""
-    m, cfg, Q = make_case(n=5, seed=4)
+    the boundary blocks amplifies by up to 1e8: the diagonal agrees to 1e-8.
+    Flux 3 differences Compute_RoeFlux's low-Mach-fix branch (M 0.1)."""
+    m, cfg, Q = make_case(n=5, seed=4, cfg=dict(CFG1, flux_scheme=flux, mach=0.1 if flux == 3 else 0.5,
+                                                mach_min=0.1 if flux == 3 else 0.5))
     cfg = dict(cfg, jacobian_method=method)
     ref = refharness.run(m, cfg, Q, [("begin", iteration), ("bc", iteration), ("get", "state"), ("residual", 1),
                                      ("deltat", iteration), ("jacobian", 1, iteration), ("get", "matrix"),

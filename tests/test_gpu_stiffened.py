@@ -48,6 +48,8 @@ CASES = [
                            precond_mach=0.2, order=1, gradient=1, limiter=1, mach=0.1, mach_min=0.1), (1,) * 6),
     ("btw1_far_urlocal", dict(CFG1, flux_scheme=4, precond_method=2, precond_type=2, mach=0.2, mach_min=0.2),
      (1,) * 6),
+    ("thornber2_far", dict(CFG1, flux_scheme=5, order=1, gradient=1, limiter=1, mach=0.2, mach_min=0.2), (1,) * 6),
+    ("thornber1_water_channel", dict(CFG1, **WATER, flux_scheme=5, alpha_deg=1.0, beta_deg=1.0), CHANNEL_BC),
 ]
 
 
@@ -69,7 +71,7 @@ def test_stiffened_residual_matches_restatement(gpu_available, name, cfg, face_b
     assert relerr(g["deltat"], o["deltat"]) <= 1e-12
 
 
-@pytest.mark.parametrize("flux", [0, 3, 4])
+@pytest.mark.parametrize("flux", [0, 3, 4, 5])
 def test_stiffened_jacobian_and_ghosts_match_restatement(gpu_available, flux):
     """Ghost states, approximate Jacobian (for flux 4 with the preconditioned
     dissipation and pseudo-time term) and right-hand side on the water channel."""

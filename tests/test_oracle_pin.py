@@ -352,3 +352,30 @@ def test_preconditioned_roe_without_preconditioning_is_roe():
     np.testing.assert_allclose(c4, c0, rtol=0, atol=1e-12 * np.abs(c0).max())
     np.testing.assert_allclose(d4, d0, rtol=0, atol=1e-12 * np.abs(d0).max())
     np.testing.assert_allclose(t4, t0, rtol=1e-13)
+
+
+def test_thornber_is_roe_above_mach_one_and_blends_velocities_below():
+    """Flux 5 (MPFLOW3D's Thornber modification, restated): at max(M_L, M_R)
+    >= 1 it is the Roe flux; below, the Roe flux of states whose velocities are
+    blended toward each other by (1 - z)/2, density and energy kept."""
+    a = np.array([0.3, -0.2, 0.25])
+    g = 1.4
+
+    def state(rho, p, vel):
+        return np.r_[rho, rho * vel, p / (g - 1.0) + 0.5 * rho * (vel @ vel)]
+
+    def flux(qa, qb, f):
+        conv, diss, _, _ = restatement.Session(_two_node_mesh(a), dict(CFG1, flux_scheme=f)).residual(
+            np.stack([qa, qb], axis=1))
+        return conv[:, 0] + diss[:, 0]
+
+    c = np.sqrt(g)
+    qa, qb = state(1.0, 1.0, c * np.array([1.2, 0.1, 0.0])), state(1.1, 1.2, c * np.array([0.9, -0.1, 0.2]))
+    np.testing.assert_allclose(flux(qa, qb, 5), flux(qa, qb, 0), rtol=0, atol=1e-14)
+    va, vb = c * np.array([0.1, 0.02, -0.01]), c * np.array([0.08, -0.03, 0.02])
+    qa, qb = state(1.0, 1.0, va), state(1.02, 1.01, vb)
+    z = max(np.linalg.norm(va) / np.sqrt(g * 1.0 / 1.0), np.linalg.norm(vb) / np.sqrt(g * 1.01 / 1.02))
+    ma, mb = qa.copy(), qb.copy()
+    ma[1:4] = qa[0] * 0.5 * ((1 + z) * va + (1 - z) * vb)
+    mb[1:4] = qb[0] * 0.5 * ((1 + z) * vb + (1 - z) * va)
+    np.testing.assert_allclose(flux(qa, qb, 5), flux(ma, mb, 0), rtol=1e-13, atol=1e-15)
