@@ -394,7 +394,6 @@ __device__ __forceinline__ double pc_beta(const Flow &f, double mach, double mac
 }
 
 struct PcSys {
-    double L[25];                 // left eigenvectors of K A (rows)
     double rho, u, v, w, c, beta, alpha, delta, zp, zm, ubar, ubp, cp;
     double lam0, lam3, lam4;      // |u.n|, |ubp + cp|, |ubp - cp|
 };
@@ -403,39 +402,55 @@ __device__ __forceinline__ void pc_system(double rho, double u, double v, double
                                           double nz, double beta, const Flow &f, PcSys &S) {
     const double alpha = f.pc_method == CFD_PRECOND_TURKEL ? 0.4 : 0.0;
     const double delta = f.pc_method == CFD_PRECOND_BTW ? 1.0 : beta;
-    const double ubar = u * nx + v * ny + w * nz, c2 = c * c, bc2 = beta * c2;
+    const double ubar = u * nx + v * ny + w * nz;
     const double zp = 0.5 * (1.0 + beta - alpha), zm = 0.5 * (1.0 - beta + alpha);
-    const double ubp = zp * ubar, cp = sqrt(beta * (c2 - ubar * ubar) + zp * zp * ubar * ubar);
-    const double pv1 = rho * (beta - delta), pv2 = pv1 * ubar, pv3 = bc2 - alpha * ubar * ubar;
-    const double ipv3 = 1.0 / pv3, irc = 1.0 / (rho * c2 * pv3);
-    const double pv4 = (bc2 * (cp + ubar * zm)) / (2.0 * cp * pv3), pv5 = (bc2 * (cp - ubar * zm)) / (2.0 * cp * pv3);
-    const double aub = alpha * ubar, aub2r = alpha * rho * ubar * ubar, rdc = rho * delta * c2;
+    const double ubp = zp * ubar, cp = sqrt(beta * (c * c - ubar * ubar) + zp * zp * ubar * ubar);
     S.rho = rho; S.u = u; S.v = v; S.w = w; S.c = c;
     S.beta = beta; S.alpha = alpha; S.delta = delta; S.zp = zp; S.zm = zm;
     S.ubar = ubar; S.ubp = ubp; S.cp = cp;
     S.lam0 = fabs(ubar);
     S.lam3 = fabs(ubp + cp);
     S.lam4 = fabs(ubp - cp);
-    double *L = S.L;
-    L[0] = nx;
-    L[1] = nx * ubar * (alpha * (v * nz - w * ny) + pv1 * nx) * ipv3;
-    L[2] = (bc2 * nz - aub * (w * ny * ny + u * nx * nz + w * nz * nz) + pv2 * nx * ny) * ipv3;
-    L[3] = (-bc2 * ny + aub * (v * ny * ny + u * nx * ny + v * nz * nz) + pv2 * nx * nz) * ipv3;
-    L[4] = (-rdc * nx + alpha * c2 * (v * nz - w * ny) + aub2r * nx) * irc;
-    L[5] = ny;
-    L[6] = (-bc2 * nz + aub * (w * nx * nx + v * ny * nz + w * nz * nz) + pv2 * nx * ny) * ipv3;
-    L[7] = ny * ubar * (alpha * (w * nx - u * nz) + pv1 * ny) * ipv3;
-    L[8] = (bc2 * nx - aub * (u * nx * nx + v * nx * ny + u * nz * nz) + pv2 * ny * nz) * ipv3;
-    L[9] = (-rdc * ny + alpha * c2 * (w * nx - u * nz) + aub2r * ny) * irc;
-    L[10] = nz;
-    L[11] = (bc2 * ny - aub * (v * nx * nx + w * ny * nz + v * ny * ny) + pv2 * nx * nz) * ipv3;
-    L[12] = (-bc2 * nx + aub * (u * nx * nx + w * nx * nz + u * ny * ny) + pv2 * ny * nz) * ipv3;
-    L[13] = nz * ubar * (alpha * (u * ny - v * nx) + pv1 * nz) * ipv3;
-    L[14] = (-rdc * nz + alpha * c2 * (u * ny - v * nx) + aub2r * nz) * irc;
-    L[15] = 0.0; L[16] = pv4 * nx; L[17] = pv4 * ny; L[18] = pv4 * nz;
-    L[19] = (bc2 + aub * (cp - ubar * zp)) / (2.0 * rho * cp * pv3);
-    L[20] = 0.0; L[21] = -pv5 * nx; L[22] = -pv5 * ny; L[23] = -pv5 * nz;
-    L[24] = (bc2 - aub * (cp + ubar * zp)) / (2.0 * rho * cp * pv3);
+}
+
+// Row k of the left eigenvectors of K A (rows of the reference's right-
+// eigenvector array, Roe_Fluxes.cpp:2353-2387; BC.cpp:279-305).  Called with
+// a constant k so each row is formed where it is consumed.
+__device__ __forceinline__ void pc_left_row(int k, const PcSys &S, double nx, double ny, double nz, double L[5]) {
+    const double rho = S.rho, u = S.u, v = S.v, w = S.w, ubar = S.ubar, c2 = S.c * S.c;
+    const double beta = S.beta, alpha = S.alpha, delta = S.delta, zp = S.zp, zm = S.zm, cp = S.cp;
+    const double bc2 = beta * c2, pv1 = rho * (beta - delta), pv2 = pv1 * ubar, pv3 = bc2 - alpha * ubar * ubar;
+    const double ipv3 = 1.0 / pv3, aub = alpha * ubar;
+    if (k < 3) {
+        const double irc = 1.0 / (rho * c2 * pv3), aub2r = alpha * rho * ubar * ubar, rdc = rho * delta * c2;
+        if (k == 0) {
+            L[0] = nx;
+            L[1] = nx * ubar * (alpha * (v * nz - w * ny) + pv1 * nx) * ipv3;
+            L[2] = (bc2 * nz - aub * (w * ny * ny + u * nx * nz + w * nz * nz) + pv2 * nx * ny) * ipv3;
+            L[3] = (-bc2 * ny + aub * (v * ny * ny + u * nx * ny + v * nz * nz) + pv2 * nx * nz) * ipv3;
+            L[4] = (-rdc * nx + alpha * c2 * (v * nz - w * ny) + aub2r * nx) * irc;
+        } else if (k == 1) {
+            L[0] = ny;
+            L[1] = (-bc2 * nz + aub * (w * nx * nx + v * ny * nz + w * nz * nz) + pv2 * nx * ny) * ipv3;
+            L[2] = ny * ubar * (alpha * (w * nx - u * nz) + pv1 * ny) * ipv3;
+            L[3] = (bc2 * nx - aub * (u * nx * nx + v * nx * ny + u * nz * nz) + pv2 * ny * nz) * ipv3;
+            L[4] = (-rdc * ny + alpha * c2 * (w * nx - u * nz) + aub2r * ny) * irc;
+        } else {
+            L[0] = nz;
+            L[1] = (bc2 * ny - aub * (v * nx * nx + w * ny * nz + v * ny * ny) + pv2 * nx * nz) * ipv3;
+            L[2] = (-bc2 * nx + aub * (u * nx * nx + w * nx * nz + u * ny * ny) + pv2 * ny * nz) * ipv3;
+            L[3] = nz * ubar * (alpha * (u * ny - v * nx) + pv1 * nz) * ipv3;
+            L[4] = (-rdc * nz + alpha * c2 * (u * ny - v * nx) + aub2r * nz) * irc;
+        }
+    } else if (k == 3) {
+        const double pv4 = (bc2 * (cp + ubar * zm)) / (2.0 * cp * pv3);
+        L[0] = 0.0; L[1] = pv4 * nx; L[2] = pv4 * ny; L[3] = pv4 * nz;
+        L[4] = (bc2 + aub * (cp - ubar * zp)) / (2.0 * rho * cp * pv3);
+    } else {
+        const double pv5 = (bc2 * (cp - ubar * zm)) / (2.0 * cp * pv3);
+        L[0] = 0.0; L[1] = -pv5 * nx; L[2] = -pv5 * ny; L[3] = -pv5 * nz;
+        L[4] = (bc2 - aub * (cp + ubar * zp)) / (2.0 * rho * cp * pv3);
+    }
 }
 
 // out = Mop Kinv R |Lambda| L Mpr dQ at the system's averaged state, with
@@ -452,9 +467,11 @@ __device__ __forceinline__ void pc_dissipation(const PcSys &S, double nx, double
     dq[4] = f.gm1 * (0.5 * q2 * dQ[0] - u * dQ[1] - v * dQ[2] - w * dQ[3] + dQ[4]);
     double a[5];
 #pragma unroll
-    for (int k = 0; k < 5; k++)
-        a[k] = S.L[5 * k] * dq[0] + S.L[5 * k + 1] * dq[1] + S.L[5 * k + 2] * dq[2] + S.L[5 * k + 3] * dq[3] +
-               S.L[5 * k + 4] * dq[4];
+    for (int k = 0; k < 5; k++) {
+        double l[5];
+        pc_left_row(k, S, nx, ny, nz, l);
+        a[k] = l[0] * dq[0] + l[1] * dq[1] + l[2] * dq[2] + l[3] * dq[3] + l[4] * dq[4];
+    }
     a[0] *= S.lam0; a[1] *= S.lam0; a[2] *= S.lam0; a[3] *= S.lam3; a[4] *= S.lam4;
     // right eigenvectors
     const double bc2 = S.beta * S.c * S.c, ibc2 = 1.0 / bc2, zp = S.zp, zm = S.zm, ub = S.ubar, cp = S.cp;
@@ -537,10 +554,12 @@ __device__ __forceinline__ void pc_abs_jacobian(const double qL[5], const double
     eos_face(qR, nx, ny, nz, f, true, R);
     PcSys S;
     pc_edge_system(L, R, nx, ny, nz, f, S);
-#pragma unroll 1
+    // fully unrolled so that every index is a constant (no local-memory arrays)
+#pragma unroll
     for (int j = 0; j < 5; j++) {
-        double e[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, col[5];
-        e[j] = 1.0;
+        double e[5], col[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) e[k] = k == j ? 1.0 : 0.0;
         pc_dissipation(S, nx, ny, nz, f, e, col);
 #pragma unroll
         for (int i = 0; i < 5; i++) A[5 * i + j] = col[i];
@@ -637,6 +656,9 @@ __device__ __forceinline__ int precond_characteristic_bc(const double qI[5], con
     const double mG = sqrt(G.u * G.u + G.v * G.v + G.w * G.w) / G.c;
     PcSys S;
     pc_system(O.rho, O.u, O.v, O.w, O.c, nx, ny, nz, pc_beta(f, mach, fmax(mI, mG)), f, S);
+    double Lm[25];
+#pragma unroll
+    for (int k = 0; k < 5; k++) pc_left_row(k, S, nx, ny, nz, Lm + 5 * k);
     const double l1 = S.ubar, l4 = S.ubp + S.cp, l5 = S.ubp - S.cp;
     int inst, status = 0;
     switch (bc_type) {
@@ -665,8 +687,8 @@ __device__ __forceinline__ int precond_characteristic_bc(const double qI[5], con
     const double qf[5] = {f.inf_rho, f.inf_u, f.inf_v, f.inf_w, f.inf_p};
     double xb[5] = {f.inf_rho, f.inf_u, f.inf_v, f.inf_w, f.inf_p};
     auto lrow = [&](int k, const double q[5]) {
-        return S.L[5 * k] * q[0] + S.L[5 * k + 1] * q[1] + S.L[5 * k + 2] * q[2] + S.L[5 * k + 3] * q[3] +
-               S.L[5 * k + 4] * q[4];
+        return Lm[5 * k] * q[0] + Lm[5 * k + 1] * q[1] + Lm[5 * k + 2] * q[2] + Lm[5 * k + 3] * q[3] +
+               Lm[5 * k + 4] * q[4];
     };
     double B[5];
     switch (inst) {
@@ -674,8 +696,8 @@ __device__ __forceinline__ int precond_characteristic_bc(const double qI[5], con
 #pragma unroll
             for (int k = 0; k < 4; k++) B[k] = lrow(k, qi);
             B[4] = 0.0;
-            S.L[20] = 0.0; S.L[21] = nx; S.L[22] = ny; S.L[23] = nz; S.L[24] = 0.0;
-            solve5_pivot(S.L, B, xb);
+            Lm[20] = 0.0; Lm[21] = nx; Lm[22] = ny; Lm[23] = nz; Lm[24] = 0.0;
+            solve5_pivot(Lm, B, xb);
             if (f.iteration < f.zpg_iteration && xb[4] + f.pinf < 0.0) {
                 xb[0] = I.rho; xb[4] = I.p;
                 xb[1] = I.u - nx * I.ubar; xb[2] = I.v - ny * I.ubar; xb[3] = I.w - nz * I.ubar;
@@ -686,19 +708,19 @@ __device__ __forceinline__ int precond_characteristic_bc(const double qI[5], con
             const double qe[5] = {qf[0], qf[1], qf[2], qf[3], inst == 4 ? I.p : qf[4]};
 #pragma unroll
             for (int k = 0; k < 5; k++) B[k] = k == 3 ? lrow(3, qi) : lrow(k, qe);
-            solve5_pivot(S.L, B, xb);
+            solve5_pivot(Lm, B, xb);
         } break;
         case 5:
 #pragma unroll
             for (int k = 0; k < 4; k++) B[k] = lrow(k, qi);
             B[4] = f.pc_outflow_p;
-            S.L[20] = 0.0; S.L[21] = 0.0; S.L[22] = 0.0; S.L[23] = 0.0; S.L[24] = 1.0;
-            solve5_pivot(S.L, B, xb);
+            Lm[20] = 0.0; Lm[21] = 0.0; Lm[22] = 0.0; Lm[23] = 0.0; Lm[24] = 1.0;
+            solve5_pivot(Lm, B, xb);
             break;
         case 9:
 #pragma unroll
             for (int k = 0; k < 5; k++) B[k] = k == 4 ? lrow(4, qf) : lrow(k, qi);
-            solve5_pivot(S.L, B, xb);
+            solve5_pivot(Lm, B, xb);
             break;
         case 7: case 11:
 #pragma unroll
