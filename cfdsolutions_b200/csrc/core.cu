@@ -736,14 +736,14 @@ int reduce_sum_sq(cfd_ctx *c, const double *x, int64_t n, int64_t stride, int nv
     k_sum_final<<<1, bs, bs * sizeof(double), c->stream>>>(c->red.p, nblk, nvec, c->red_out.p);
     CFD_LAUNCH_CHECK();
     CFD_CUDA(cudaMemcpyAsync(out_host, c->red_out.p, nvec * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    CFD_CUDA(stream_wait(c->stream));
     return CFD_OK;
 }
 
 int check_device_error(cfd_ctx *c) {
     int h = 0;
     CFD_CUDA(cudaMemcpyAsync(&h, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    CFD_CUDA(stream_wait(c->stream));
     if (h) {
         CFD_CUDA(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
         set_error("device reported numerical failure (flags 0x%x)", h);
@@ -1041,7 +1041,7 @@ int cfd_create(int device, cfd_ctx **out) {
 int cfd_destroy(cfd_ctx *c) {
     if (!c) return CFD_OK;
     cudaSetDevice(c->device);
-    cudaStreamSynchronize(c->stream);
+    stream_wait(c->stream);
     delete c;
     return CFD_OK;
 }
@@ -1089,7 +1089,7 @@ int cfd_set_params(cfd_ctx *c, const cfd_params *p) {
 int cfd_synchronize(cfd_ctx *c) {
     if (!c) return CFD_ERR_ARG;
     CFD_CUDA(cudaSetDevice(c->device));
-    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    CFD_CUDA(stream_wait(c->stream));
     return CFD_OK;
 }
 
@@ -1180,7 +1180,7 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         CFD_CUDA(c->bedge_geo.upload(bgv.data(), nbedge, s));
         CFD_CUDA(c->bedge_sv.upload(bsv.data(), nbedge, s));
         CFD_CUDA(c->bedge_type.upload(bedge_type, nbedge, s));
-        CFD_CUDA(cudaStreamSynchronize(s));
+        CFD_CUDA(stream_wait(s));
     }
     CFD_CUDA(c->cvol.upload(cvol, nnode, s));
     {
@@ -1188,7 +1188,7 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         for (int i = 0; i < nnode; i++)
             for (int d = 0; d < 3; d++) x[(size_t)d * nnode + i] = coords[3 * (size_t)i + d];
         CFD_CUDA(c->xyz.upload(x.data(), x.size(), s));
-        CFD_CUDA(cudaStreamSynchronize(s));
+        CFD_CUDA(stream_wait(s));
     }
     // physical graph, rows sorted (the reference's list order is insertion order;
     // gradients and limiters are order-insensitive to round-off)
@@ -1221,7 +1221,7 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         }
         CFD_CUDA(c->n2e_ptr.upload(ptr.data(), ptr.size(), s));
         CFD_CUDA(c->n2e.upload(lst.data(), lst.size(), s));
-        CFD_CUDA(cudaStreamSynchronize(s));
+        CFD_CUDA(stream_wait(s));
     }
     // ---- sliced-ELL incidence of the node-gather kernel (slices of 32 nodes)
     {
@@ -1249,7 +1249,7 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         CFD_CUDA(c->sell_nbr.upload(sn.data(), sn.size(), s));
         CFD_CUDA(c->sell_geo.upload(sg.data(), sg.size(), s));
         CFD_CUDA(c->deg.upload(dg.data(), dg.size(), s));
-        CFD_CUDA(cudaStreamSynchronize(s));
+        CFD_CUDA(stream_wait(s));
     }
     // ---- patch layout of the residual kernel: node ranges of CFD_PATCH_NODES
     // nodes; per patch its halo (neighbours outside the range, sorted), every
@@ -1319,7 +1319,7 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
             CFD_CUDA(c->halo.upload(halo.data(), halo.size(), s));
             CFD_CUDA(c->inc_ptr.upload(iptr.data(), iptr.size(), s));
             CFD_CUDA(c->inc.upload(ilist.data(), ilist.size(), s));
-            CFD_CUDA(cudaStreamSynchronize(s));
+            CFD_CUDA(stream_wait(s));
         }
     }
     CFD_CUDA(c->roeflag.alloc(nnode));
@@ -1335,7 +1335,7 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         for (int e = 0; e < nbedge; e++) lst[fill[bedge_nodes[2 * e]]++] = e;
         CFD_CUDA(c->n2b_ptr.upload(ptr.data(), ptr.size(), s));
         CFD_CUDA(c->n2b.upload(lst.data(), lst.size(), s));
-        CFD_CUDA(cudaStreamSynchronize(s));
+        CFD_CUDA(stream_wait(s));
     }
     // ---- block CRS pattern (Create_CRS_SolverBlockMatrix, Euler3D/src/Solver.cpp:612-672)
     {
@@ -1378,7 +1378,7 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         build_levels(c->h_IA, c->h_JA, nnode, true, c->lv_fwd, s, e1);
         build_levels(c->h_IA, c->h_JA, nnode, false, c->lv_bwd, s, e2);
         if (e1 || e2) { set_error("cfd_set_mesh: level upload failed"); return CFD_ERR_CUDA; }
-        CFD_CUDA(cudaStreamSynchronize(s));
+        CFD_CUDA(stream_wait(s));
     }
     // ---- state and work arrays
     CFD_CUDA(c->Q.alloc((size_t)5 * c->ldq));
@@ -1389,7 +1389,7 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
     CFD_CUDA(cudaMemsetAsync(c->res.p, 0, sizeof(double) * 5 * nnode, s));
     CFD_CUDA(cudaMemsetAsync(c->resd.p, 0, sizeof(double) * 5 * nnode, s));
     CFD_CUDA(cudaMemsetAsync(c->dt.p, 0, sizeof(double) * nnode, s));
-    CFD_CUDA(cudaStreamSynchronize(s));
+    CFD_CUDA(stream_wait(s));
     c->has_mesh = true;
     return cfd_set_freestream(c);
 }
@@ -1423,7 +1423,7 @@ int cfd_get_state(cfd_ctx *c, double *Q) {
     const int64_t n = (int64_t)c->nnode + c->nghost;
     CFD_CUDA(cudaMemcpy2DAsync(Q, n * sizeof(double), c->Q.p, c->ldq * sizeof(double), n * sizeof(double), 5,
                                cudaMemcpyDeviceToHost, c->stream));
-    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    CFD_CUDA(stream_wait(c->stream));
     return CFD_OK;
 }
 
@@ -1625,7 +1625,7 @@ int cfd_block_lusgs(cfd_ctx *c, int iterations, double *rms) {
     CFD_CUDA(cudaMemcpyAsync(blk.data(), c->A64.p + 5 * 25, sizeof(double) * 25, cudaMemcpyDeviceToHost, c->stream));
     CFD_CUDA(cudaMemcpyAsync(xj.data(), c->X.p + (int64_t)c->h_JA[5] * 5, sizeof(double) * 5,
                              cudaMemcpyDeviceToHost, c->stream));
-    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    CFD_CUDA(stream_wait(c->stream));
     double tv[5];
     for (int ii = 0; ii < 5; ii++) {
         tv[ii] = 0.0;
@@ -1657,7 +1657,7 @@ int cfd_get_residual(cfd_ctx *c, double *conv, double *diss) {
     const size_t bytes = sizeof(double) * 5 * c->nnode;
     if (conv) CFD_CUDA(cudaMemcpyAsync(conv, c->res.p, bytes, cudaMemcpyDeviceToHost, c->stream));
     if (diss) CFD_CUDA(cudaMemcpyAsync(diss, c->resd.p, bytes, cudaMemcpyDeviceToHost, c->stream));
-    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    CFD_CUDA(stream_wait(c->stream));
     return check_device_error(c);
 }
 
@@ -1665,7 +1665,7 @@ int cfd_get_deltat(cfd_ctx *c, double *dt) {
     NEED_MESH("cfd_get_deltat");
     if (!dt) return CFD_ERR_ARG;
     CFD_CUDA(cudaMemcpyAsync(dt, c->dt.p, sizeof(double) * c->nnode, cudaMemcpyDeviceToHost, c->stream));
-    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    CFD_CUDA(stream_wait(c->stream));
     return CFD_OK;
 }
 
@@ -1673,7 +1673,7 @@ int cfd_get_extrema(cfd_ctx *c, double out[8]) {
     NEED_MESH("cfd_get_extrema");
     unsigned long long h[8];
     CFD_CUDA(cudaMemcpyAsync(h, c->ext.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
-    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    CFD_CUDA(stream_wait(c->stream));
     for (int k = 0; k < 8; k++) out[k] = bitsd(h[k]);
     return CFD_OK;
 }
@@ -1704,12 +1704,12 @@ int cfd_get_system(cfd_ctx *c, double *A, double *B, double *X) {
         if (c->a_precision == CFD_PREC_FP32) {
             std::vector<float> h(nz);
             CFD_CUDA(cudaMemcpyAsync(h.data(), c->A32.p, sizeof(float) * nz, cudaMemcpyDeviceToHost, c->stream));
-            CFD_CUDA(cudaStreamSynchronize(c->stream));
+            CFD_CUDA(stream_wait(c->stream));
             for (size_t k = 0; k < nz; k++) A[k] = h[k];
         } else {
             std::vector<uint16_t> h(nz);
             CFD_CUDA(cudaMemcpyAsync(h.data(), c->A16.p, sizeof(uint16_t) * nz, cudaMemcpyDeviceToHost, c->stream));
-            CFD_CUDA(cudaStreamSynchronize(c->stream));
+            CFD_CUDA(stream_wait(c->stream));
             for (size_t k = 0; k < nz; k++) {
                 const uint32_t bits = (uint32_t)h[k] << 16;
                 float f;
@@ -1720,7 +1720,7 @@ int cfd_get_system(cfd_ctx *c, double *A, double *B, double *X) {
     }
     if (B) CFD_CUDA(cudaMemcpyAsync(B, c->B.p, sizeof(double) * 5 * c->nnode, cudaMemcpyDeviceToHost, c->stream));
     if (X) CFD_CUDA(cudaMemcpyAsync(X, c->X.p, sizeof(double) * 5 * c->nnode, cudaMemcpyDeviceToHost, c->stream));
-    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    CFD_CUDA(stream_wait(c->stream));
     return CFD_OK;
 }
 
@@ -1731,7 +1731,7 @@ int cfd_set_system(cfd_ctx *c, const double *A, const double *B) {
     CFD_CUDA(c->B.upload(B, (size_t)c->nnode * 5, c->stream));
     CFD_CUDA(c->X.alloc((size_t)c->nnode * 5));
     CFD_CUDA(cudaMemsetAsync(c->X.p, 0, sizeof(double) * 5 * c->nnode, c->stream));
-    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    CFD_CUDA(stream_wait(c->stream));
     c->a_precision = CFD_PREC_FP64;
     c->a64_valid = true;
     c->has_system = true;

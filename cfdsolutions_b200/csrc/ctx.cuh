@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <thread>
 #include <vector>
 
 #include "cfd_internal.h"
@@ -19,6 +20,19 @@ namespace cfd {
 // (cudaFree waits for all streams).  Off (plain cudaMalloc/cudaFree) otherwise.
 inline thread_local bool g_alloc_async = false;
 inline thread_local cudaStream_t g_alloc_stream = nullptr;
+
+// Waits for the work queued on s.  On a serving worker it polls the stream and
+// yields the core between polls instead of blocking in the driver's spin
+// wait, so a dozen concurrent solves leave the host cores to the threads that
+// issue the launches; elsewhere it is cudaStreamSynchronize.
+inline cudaError_t stream_wait(cudaStream_t s) {
+    if (!g_alloc_async) return cudaStreamSynchronize(s);
+    for (;;) {
+        const cudaError_t e = cudaStreamQuery(s);
+        if (e != cudaErrorNotReady) return e;
+        std::this_thread::yield();
+    }
+}
 
 template <typename T>
 struct DevBuf {

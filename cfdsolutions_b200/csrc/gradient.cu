@@ -377,7 +377,7 @@ extern "C" {
 int cfd_get_gradients(cfd_ctx *c, double *g) {
     if (!c || !g || !c->has_grad) return CFD_ERR_STATE;
     CFD_CUDA(cudaMemcpyAsync(g, c->grad.p, sizeof(double) * 15 * c->nnode, cudaMemcpyDeviceToHost, c->stream));
-    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    CFD_CUDA(stream_wait(c->stream));
     return CFD_OK;
 }
 
@@ -386,7 +386,7 @@ int cfd_get_limiters(cfd_ctx *c, double *phi) {
     int st = roe_fix_standalone(c);
     if (st) return st;
     CFD_CUDA(cudaMemcpyAsync(phi, c->phi.p, sizeof(double) * 5 * c->nnode, cudaMemcpyDeviceToHost, c->stream));
-    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    CFD_CUDA(stream_wait(c->stream));
     return CFD_OK;
 }
 

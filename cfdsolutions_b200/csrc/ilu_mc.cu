@@ -521,7 +521,7 @@ int mc_build(cfd_ctx *c) {
     CFD_CUDA(mc.hdr.upload(hdr.data(), hdr.size(), c->stream));
     CFD_CUDA(mc.pair_ptr.upload(pair_ptr.data(), pair_ptr.size(), c->stream));
     CFD_CUDA(mc.pairs.upload(pairs.data(), pairs.size(), c->stream));
-    CFD_CUDA(cudaStreamSynchronize(c->stream));  // host vectors go out of scope
+    CFD_CUDA(stream_wait(c->stream));  // host vectors go out of scope
     mc.built = true;
     return CFD_OK;
 }

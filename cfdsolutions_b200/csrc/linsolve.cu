@@ -62,7 +62,7 @@ int reduce_sum_plain(cfd_ctx *c, const double *x, int64_t n, double *out_host) {
     k_sum_one<<<1, 256, 0, c->stream>>>(c->red.p, nblk, c->red_out.p);
     CFD_LAUNCH_CHECK();
     CFD_CUDA(cudaMemcpyAsync(out_host, c->red_out.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    CFD_CUDA(stream_wait(c->stream));
     return CFD_OK;
 }
 
@@ -195,7 +195,7 @@ static int mdot(cfd_ctx *c, const double *V, int64_t ld, int k, const double *w,
     int st = dot_buffers(c);
     if (st || (st = mdot_dev(c, V, ld, k, w, n, c->dots.p))) return st;
     CFD_CUDA(cudaMemcpyAsync(out_host, c->dots.p, sizeof(double) * k, cudaMemcpyDeviceToHost, c->stream));
-    CFD_CUDA(cudaStreamSynchronize(c->stream));
+    CFD_CUDA(stream_wait(c->stream));
     return CFD_OK;
 }
 
@@ -655,7 +655,7 @@ static int gmres_inner(cfd_ctx *c, int aprec, const Precond &pc, int m, int max_
             CFD_LAUNCH_CHECK();
             CFD_CUDA(cudaMemcpyAsync(h.data(), dd + DOT_COL, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost,
                                      c->stream));
-            CFD_CUDA(cudaStreamSynchronize(c->stream));
+            CFD_CUDA(stream_wait(c->stream));
             const double hn = h[j + 1];
             if (!std::isfinite(hn)) { set_error("gmres: breakdown (non-finite)"); return CFD_ERR_NUMERIC; }
             // apply previous rotations, form a new one
