@@ -53,10 +53,10 @@ def parse():
     ap.add_argument("--no-steady", action="store_true", help="skip the time-to-steady-state solves")
     ap.add_argument("--no-serve", action="store_true", help="skip the served batch")
     ap.add_argument("--no-lowmach", action="store_true", help="skip the low-Mach liquid channel solves")
-    ap.add_argument("--serve-requests", type=int, default=32)
+    ap.add_argument("--serve-requests", type=int, default=64)
     ap.add_argument("--serve-nmax", type=int, default=64, help="largest cube side of the served mix (config: 96)")
     ap.add_argument("--serve-rate", type=float, default=2.0, help="Poisson arrival rate, requests per second")
-    ap.add_argument("--serve-workers", type=int, default=8)
+    ap.add_argument("--serve-workers", type=int, default=12)
     ap.add_argument("--profile-linear", action="store_true",
                     help="small linear-solve case for ncu captures (Jacobian + one GMRES(30) call per precision)")
     ap.add_argument("--profile", action="store_true",
