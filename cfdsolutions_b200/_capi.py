@@ -72,6 +72,17 @@ class SolveStats(C.Structure):
                 ("linear_iterations", C.c_int), ("status", C.c_int)]
 
 
+class UnsteadyOpts(C.Structure):
+    _fields_ = [("dt", C.c_double), ("steps", C.c_int), ("inner_iterations", C.c_int), ("bdf2", C.c_int),
+                ("include_diss", C.c_int), ("linear_solver", C.c_int), ("linear_iters", C.c_int),
+                ("relax", C.c_double), ("gmres", GmresOpts)]
+
+
+class UnsteadyStats(C.Structure):
+    _fields_ = [("steps", C.c_int), ("inner_iterations", C.c_int), ("rms_last", C.c_double),
+                ("linear_iterations", C.c_int), ("status", C.c_int)]
+
+
 class ServeRequest(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("lx", C.c_double), ("ly", C.c_double),
                 ("lz", C.c_double), ("jitter", C.c_double), ("mesh_seed", C.c_uint64), ("numbering", C.c_int),
@@ -135,6 +146,7 @@ SIGNATURES = {
     "cfd_set_system": (I, [P, P, P]),
     "cfd_residual_step": (I, [P, I, P, P, P]),
     "cfd_solve_steady": (I, [P, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
+    "cfd_solve_unsteady": (I, [P, C.POINTER(UnsteadyOpts), C.POINTER(UnsteadyStats)]),
     "cfd_mesh_box": (I, [I, I, I, D, D, D, D, C.c_uint64, I, P, C.POINTER(P)]),
     "cfd_mesh_from_cells": (I, [I, P, I64, P, I64, P, P, C.POINTER(P)]),
     "cfd_mesh_sizes": (I, [P, P]),

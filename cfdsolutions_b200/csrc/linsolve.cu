@@ -705,6 +705,43 @@ static int gmres_inner(cfd_ctx *c, int aprec, const Precond &pc, int m, int max_
 
 using namespace cfd;
 
+// Physical-time terms of one inner iteration (Solver_Unsteady_Implicit.cpp:
+// 181-216), one thread per node: s = V/dt ((1+theta)(Q - Q^n) - theta (Q^n -
+// Q^n-1)) is subtracted from B and added to the convective residual (for
+// the RMS), and (1+theta) V/dt joins the diagonal block of every stored
+// precision.  qn / qn1 are [5][n] copies of the physical nodes.
+template <typename TA>
+__global__ void k_unsteady_terms(int n, int64_t ldq, const double *__restrict__ Q, const double *__restrict__ qn,
+                                 const double *__restrict__ qn1, const double *__restrict__ vol, double dt,
+                                 double theta, const int *__restrict__ IAU, double *__restrict__ B,
+                                 double *__restrict__ res, double *__restrict__ A64, TA *__restrict__ Alow) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double eta = vol[i] / dt;
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        const double q = Q[v * ldq + i], a = qn[v * (int64_t)n + i], b = qn1[v * (int64_t)n + i];
+        const double src = eta * ((1.0 + theta) * (q - a) - theta * (a - b));
+        B[(int64_t)i * 5 + v] -= src;
+        res[v * (int64_t)n + i] += src;
+    }
+    const double d = (1.0 + theta) * eta;
+    const int64_t dg = (int64_t)IAU[i] * 25;
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        if (A64) A64[dg + 6 * k] += d;
+        if (Alow) store_low(Alow + dg + 6 * k, load_low(Alow + dg + 6 * k) + d);
+    }
+}
+
+// Copies the physical part of Q ([5][ldq]) to a [5][n] history array.
+__global__ void k_copy_state(int n, int64_t ldq, const double *__restrict__ Q, double *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int v = 0; v < 5; v++) out[v * (int64_t)n + i] = Q[v * ldq + i];
+}
+
 extern "C" {
 
 void cfd_gmres_default(cfd_gmres_opts *o) {
@@ -798,6 +835,76 @@ int cfd_gmres(cfd_ctx *c, const cfd_gmres_opts *o, cfd_gmres_stats *stats) {
     if (stats) *stats = s;
     if (!std::isfinite(s.rel_residual)) return CFD_ERR_NUMERIC;
     return s.rel_residual <= opt.rtol * 1.0000001 ? CFD_OK : CFD_ERR_NOT_CONVERGED;
+}
+
+int cfd_solve_unsteady(cfd_ctx *c, const cfd_unsteady_opts *o, cfd_unsteady_stats *stats) {
+    if (!c || !c->has_mesh || !o) { set_error("cfd_solve_unsteady: no mesh / options"); return CFD_ERR_STATE; }
+    if (!(o->dt > 0.0) || o->steps < 0 || o->inner_iterations < 1) {
+        set_error("cfd_solve_unsteady: dt > 0, steps >= 0 and inner_iterations >= 1");
+        return CFD_ERR_ARG;
+    }
+    const int n = c->nnode;
+    DevBuf<double> qn, qn1;
+    CFD_CUDA(qn.alloc((size_t)5 * n));
+    CFD_CUDA(qn1.alloc((size_t)5 * n));
+    const int g = grid_for(n, 256);
+    cfd_unsteady_stats s{};
+    int st = CFD_OK;
+    const int prec = o->linear_solver == 1 ? o->gmres.precision : CFD_PREC_FP64;
+    for (int t = 0; t < o->steps && !st; t++) {
+        const double theta = (o->bdf2 && t > 0) ? 0.5 : 0.0;
+        if (o->bdf2) CFD_CUDA(cudaMemcpyAsync(qn1.p, qn.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToDevice, c->stream));
+        k_copy_state<<<g, 256, 0, c->stream>>>(n, c->ldq, c->Q.p, qn.p);
+        CFD_LAUNCH_CHECK();
+        if (t == 0) CFD_CUDA(cudaMemcpyAsync(qn1.p, qn.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToDevice, c->stream));
+        for (int it = 0; it < o->inner_iterations; it++) {
+            if ((st = cfd_begin_iteration(c, it))) break;
+            if (c->params.order == CFD_ORDER_SECOND) {
+                if ((st = cfd_gradient(c))) break;
+                if (c->params.limiter != CFD_LIMITER_NONE && (st = cfd_limiter(c))) break;
+            }
+            if ((st = cfd_apply_bc(c, it))) break;
+            if ((st = cfd_residual(c, 0))) break;
+            if ((st = cfd_jacobian(c, 0, o->include_diss, prec))) break;
+            double *A64 = c->a64_valid ? c->A64.p : nullptr;
+            if (c->a_precision == CFD_PREC_FP32)
+                k_unsteady_terms<float><<<g, 256, 0, c->stream>>>(n, c->ldq, c->Q.p, qn.p, qn1.p, c->cvol.p, o->dt,
+                                                                 theta, c->IAU.p, c->B.p, c->res.p, A64, c->A32.p);
+            else if (c->a_precision == CFD_PREC_BF16)
+                k_unsteady_terms<uint16_t><<<g, 256, 0, c->stream>>>(n, c->ldq, c->Q.p, qn.p, qn1.p, c->cvol.p,
+                                                                    o->dt, theta, c->IAU.p, c->B.p, c->res.p, A64,
+                                                                    c->A16.p);
+            else
+                k_unsteady_terms<float><<<g, 256, 0, c->stream>>>(n, c->ldq, c->Q.p, qn.p, qn1.p, c->cvol.p, o->dt,
+                                                                 theta, c->IAU.p, c->B.p, c->res.p, A64,
+                                                                 (float *)nullptr);
+            CFD_LAUNCH_CHECK();
+            double rms[6];
+            if ((st = cfd_residual_rms(c, o->include_diss, rms))) break;
+            if ((st = check_device_error(c))) break;
+            s.rms_last = rms[5];
+            s.inner_iterations++;
+            if (!std::isfinite(rms[5])) { set_error("cfd_solve_unsteady: non-finite residual"); st = CFD_ERR_NUMERIC; break; }
+            if (o->linear_solver == 1) {
+                cfd_gmres_stats gs{};
+                cfd_gmres_opts go = o->gmres;
+                go.reuse_precond = 0;
+                st = cfd_gmres(c, &go, &gs);
+                s.linear_iterations += gs.iterations;
+                if (st == CFD_ERR_NOT_CONVERGED) st = CFD_OK;
+                if (st) break;
+            } else {
+                double lr;
+                if ((st = cfd_block_gs(c, o->linear_iters, 0, &lr))) break;
+                s.linear_iterations += o->linear_iters;
+            }
+            if ((st = cfd_update(c, o->relax))) break;
+        }
+        if (!st) s.steps = t + 1;
+    }
+    s.status = st;
+    if (stats) *stats = s;
+    return st;
 }
 
 int cfd_solve_steady(cfd_ctx *c, const cfd_solve_opts *o, cfd_solve_stats *stats) {

@@ -185,6 +185,16 @@ class Euler3DGPU:
         capi.check(capi.lib.cfd_solve_steady(self._h, C.byref(o), C.byref(st)), "cfd_solve_steady")
         return st
 
+    def solve_unsteady(self, dt, steps, inner_iterations=10, bdf2=True, include_diss=1, linear_solver=1,
+                       linear_iters=10, relax=1.0, gmres: capi.GmresOpts | None = None) -> capi.UnsteadyStats:
+        """Solver_Unsteady_Implicit (MPFLOW3D/src/Solver_Unsteady_Implicit.cpp:36-305)."""
+        g = gmres if gmres is not None else capi.GmresOpts(30, 300, 1e-6, capi.PC_ILU0, capi.PREC_FP64, 1)
+        o = capi.UnsteadyOpts(float(dt), int(steps), int(inner_iterations), int(bool(bdf2)), include_diss,
+                              linear_solver, linear_iters, relax, g)
+        st = capi.UnsteadyStats()
+        capi.check(capi.lib.cfd_solve_unsteady(self._h, C.byref(o), C.byref(st)), "cfd_solve_unsteady")
+        return st
+
     # ------------------------------------------------------------ readback
     def get_residual(self):
         conv = np.empty((5, self.mesh.nnode))

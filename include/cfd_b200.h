@@ -369,6 +369,35 @@ typedef struct cfd_solve_stats {
  * Solver_Steady_Implicit.cpp:35-184) entirely on the device. */
 int  cfd_solve_steady(cfd_ctx *ctx, const cfd_solve_opts *o, cfd_solve_stats *st);
 
+/* Physical-time implicit solve (Solver_Unsteady_Implicit,
+ * MPFLOW3D/src/Solver_Unsteady_Implicit.cpp:36-305): `steps` physical steps of
+ * `dt`, each converged by `inner_iterations` Newton iterations of
+ *   (J + (1+theta) V/dt I) dQ = -(Res + Res_Diss + V/dt ((1+theta)(Q - Q^n) - theta (Q^n - Q^n-1)))
+ * with J the approximate Jacobian without a pseudo-time term (AddTime FALSE);
+ * theta = 0 (TIME_INTEGRATION_METHOD_IMPLICIT_EULER_EULER) or, with bdf2,
+ * 0.5 from the second step on (TIME_INTEGRATION_METHOD_IMPLICIT_EULER_BDF). */
+typedef struct cfd_unsteady_opts {
+    double dt;               /* PHYSICAL_DELTA_TIME (non-dimensional)       */
+    int    steps;            /* physical time steps                          */
+    int    inner_iterations; /* INNER_NITERATION                             */
+    int    bdf2;             /* 1: second-order backward difference          */
+    int    include_diss;     /* as cfd_solve_opts                            */
+    int    linear_solver;    /* 0 block GS sweeps (the reference's), 1 GMRES */
+    int    linear_iters;     /* LINEAR_SOLVER_NITERATION                     */
+    double relax;            /* SOLVER_RELAXATION                            */
+    cfd_gmres_opts gmres;
+} cfd_unsteady_opts;
+
+typedef struct cfd_unsteady_stats {
+    int    steps;              /* physical steps completed                   */
+    int    inner_iterations;   /* summed                                    */
+    double rms_last;           /* RMS of the last inner iteration           */
+    int    linear_iterations;  /* summed                                    */
+    int    status;
+} cfd_unsteady_stats;
+
+int  cfd_solve_unsteady(cfd_ctx *ctx, const cfd_unsteady_opts *o, cfd_unsteady_stats *st);
+
 /* ----------------------------------------------------- host mesh builder */
 typedef struct cfd_mesh cfd_mesh;
 

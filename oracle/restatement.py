@@ -183,3 +183,39 @@ def residual_pass(mesh, cfg: dict, Q: np.ndarray) -> dict:
     conv, diss, dts, ext = s.residual(Qb, grad, phi)
     dt, ext2 = s.deltat(dts)
     return dict(state=Qb, grad=grad, phi=phi, conv=conv, diss=diss, deltat=dt, extrema=np.r_[ext, ext2])
+
+
+def unsteady(mesh, cfg: dict, Q: np.ndarray, dt: float, steps: int, inner: int, bdf2: bool = True,
+             include_diss: int = 1, rtol: float = 1e-13) -> np.ndarray:
+    """Solver_Unsteady_Implicit (MPFLOW3D/src/Solver_Unsteady_Implicit.cpp:36-305) on the
+    restatement: per inner iteration gradient/limiter, BC, residual, Jacobian without the
+    pseudo-time term, the physical-time source and diagonal, a GMRES(30)+ILU(0) solve
+    (tolerance rtol) and the update.  Returns the state [5, nnode+nghost]."""
+    Q = np.array(Q, dtype=np.float64, copy=True)
+    n = mesh.nnode
+    qn = Q[:, :n].copy()
+    qn1 = qn.copy()
+    for t in range(steps):
+        theta = 0.5 if (bdf2 and t > 0) else 0.0
+        if bdf2:
+            qn1 = qn.copy()
+        qn = Q[:, :n].copy()
+        if t == 0:
+            qn1 = qn.copy()
+        for it in range(inner):
+            s = Session(mesh, cfg, iteration=it)
+            g = phi = None
+            if cfg.get("order", 0) == 1:
+                g = s.gradient(Q, cfg.get("gradient", 0))
+                if cfg.get("limiter", -1) != -1:
+                    phi = s.limiter(Q, g)
+            Q = s.apply_bc(Q)
+            conv, diss, _, _ = s.residual(Q, g, phi)
+            A, B = s.jacobian(Q, np.zeros(n), conv, diss, add_time=0, include_diss=include_diss)
+            eta = mesh.cvol / dt
+            src = eta * ((1.0 + theta) * (Q[:, :n] - qn) - theta * (qn - qn1))
+            B -= src.T
+            A[s.IAU] += (1.0 + theta) * eta[:, None, None] * np.eye(5)
+            X, _, _, _ = s.gmres(A, B, m=30, maxit=3000, rtol=rtol, precond=2)
+            Q[:, :n] += X.T
+    return Q
