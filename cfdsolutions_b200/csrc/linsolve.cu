@@ -833,7 +833,10 @@ int cfd_gmres(cfd_ctx *c, const cfd_gmres_opts *o, cfd_gmres_stats *stats) {
     if ((st = vnorm(c, r, n5, &rn))) return st;
     s.rel_residual = rn / bnorm;
     if (stats) *stats = s;
-    if (!std::isfinite(s.rel_residual)) return CFD_ERR_NUMERIC;
+    if (!std::isfinite(s.rel_residual)) {
+        set_error("gmres: non-finite final residual (right-hand side norm %g)", bnorm);
+        return CFD_ERR_NUMERIC;
+    }
     return s.rel_residual <= opt.rtol * 1.0000001 ? CFD_OK : CFD_ERR_NOT_CONVERGED;
 }
 
@@ -926,7 +929,11 @@ int cfd_solve_steady(cfd_ctx *c, const cfd_solve_opts *o, cfd_solve_stats *stats
         if (iter == 0) s.rms_first = rms[5];
         s.rms_last = rms[5];
         s.iterations = iter + 1;
-        if (!std::isfinite(rms[5])) { st = CFD_ERR_NUMERIC; break; }
+        if (!std::isfinite(rms[5])) {
+            set_error("cfd_solve_steady: non-finite residual at implicit iteration %d", iter);
+            st = CFD_ERR_NUMERIC;
+            break;
+        }
         if (rms[5] <= o->drop * s.rms_first && iter > 0) break;
         if (rms[5] < 10.0 * DBL_EPSILON) break;  // Solver_Steady_Implicit.cpp:176
         const int prec = o->linear_solver == 1 ? o->gmres.precision : CFD_PREC_FP64;
