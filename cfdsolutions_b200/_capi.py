@@ -147,6 +147,7 @@ SIGNATURES = {
     "cfd_residual_step": (I, [P, I, P, P, P]),
     "cfd_solve_steady": (I, [P, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
     "cfd_solve_unsteady": (I, [P, C.POINTER(UnsteadyOpts), C.POINTER(UnsteadyStats)]),
+    "cfd_vtk_write": (I, [C.c_char_p, I, P, C.c_int64, P, P, C.c_int64, P, C.POINTER(Params), P, C.c_int64]),
     "cfd_mesh_box": (I, [I, I, I, D, D, D, D, C.c_uint64, I, P, C.POINTER(P)]),
     "cfd_mesh_from_cells": (I, [I, P, I64, P, I64, P, P, C.POINTER(P)]),
     "cfd_mesh_sizes": (I, [P, P]),

@@ -134,3 +134,18 @@ def perturbed_freestream(mesh: Mesh, gamma: float, mach: float, alpha_deg: float
     Q[1:4] = rho * vel
     Q[4] = rho * et
     return Q
+
+
+def write_vtk(mesh: Mesh, path: str, params, Q: np.ndarray, tri_tag: np.ndarray | None = None) -> None:
+    """VTK legacy solution file of the reference's VTK_Writer (Euler3D/src/MeshIO.cpp:219)
+    for a mesh built with its cells (``with_cells=True``) and a state Q [5, nnode+nghost]."""
+    if mesh.tets is None or mesh.tris is None:
+        raise ValueError("write_vtk needs the mesh's cells (build it with with_cells=True)")
+    Q = np.ascontiguousarray(Q, np.float64)
+    coords = np.ascontiguousarray(mesh.coords, np.float64)
+    tris = np.ascontiguousarray(mesh.tris, np.int32)
+    tets = np.ascontiguousarray(mesh.tets, np.int32)
+    tag = None if tri_tag is None else np.ascontiguousarray(tri_tag, np.int32)
+    capi.check(capi.lib.cfd_vtk_write(str(path).encode(), mesh.nnode, capi.ptr(coords), tris.shape[0], capi.ptr(tris),
+                                      None if tag is None else capi.ptr(tag), tets.shape[0], capi.ptr(tets),
+                                      C.byref(params), capi.ptr(Q), Q.shape[1]), "cfd_vtk_write")

@@ -501,6 +501,19 @@ int  cfd_server_stats(cfd_server *srv, double out[5]);
 /* Running requests finish; queued ones are dropped. */
 int  cfd_server_destroy(cfd_server *srv);
 
+/* ------------------------------------------------------ VTK solution file
+ * VTK_Writer (Euler3D/src/MeshIO.cpp:219-372), conservative variables: the
+ * legacy ASCII file the reference writes at the end of a run (points,
+ * surface triangles then tetrahedra with 0-based node indices, cell types,
+ * boundary ids = tri_tag or 1 when NULL, density, velocity components,
+ * pressure, temperature, Mach number, velocity vector of the nnode physical
+ * nodes of Q, SoA [5][ld]).  Byte-identical to the reference's file for the
+ * same mesh and state with pinf = 0 (derived fields in its operation order);
+ * with pinf > 0 pressure, temperature and Mach follow the stiffened gas. */
+int  cfd_vtk_write(const char *path, int nnode, const double *coords, int64_t ntri, const int *tris,
+                   const int *tri_tag, int64_t ntet, const int *tets, const cfd_params *p, const double *Q,
+                   int64_t ld);
+
 /* ------------------------------------------------- restart file (binary)
  * Byte-compatible with Restart_Writer / Restart_Reader
  * (Euler3D/src/RestartIO.cpp:45-179): int32 {iteration, nNode, nBNode, 5}
