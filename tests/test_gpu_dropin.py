@@ -70,6 +70,30 @@ def test_euler3d_executable_with_gpu_hot_path(gpu_available, ref_available, tmp_
     assert np.abs(qg - qc).max() <= 1e-10 * np.abs(qc).max()
 
 
+@pytest.mark.parametrize("method", ["TIME_INTEGRATION_METHOD_EXPLICIT_EULER", "TIME_INTEGRATION_METHOD_EXPLICIT_RK4"])
+def test_euler3d_explicit_executable_with_gpu_hot_path(gpu_available, ref_available, tmp_path, method):
+    """The reference's explicit drivers (Solver_Steady_Explicit_Euler / _RK4,
+    Euler3D/src/Solver_Steady_Explicit.cpp:25, :202) over the GPU residual,
+    gradient, limiter, boundary and time-step functions."""
+    if not EXE_GPU.exists():
+        pytest.skip("drop-in executable not built (make -C oracle gpu)")
+    iters = 5
+    write_case(tmp_path, 8, 1, iters)
+    text = (tmp_path / "param.txt").read_text()
+    text = text.replace("SOLVER_SCHEME=SOLVER_SCHEME_IMPLICIT", "SOLVER_SCHEME=SOLVER_SCHEME_EXPLICIT")
+    text = text.replace("TIME_INTEGRATION_METHOD=TIME_INTEGRATION_METHOD_IMPLICIT_EULER", f"TIME_INTEGRATION_METHOD={method}")
+    text = text.replace("CFL_MIN=10.0", "CFL_MIN=1.0").replace("CFL_MAX=10.0", "CFL_MAX=1.0")  # explicit stability
+    assert "SOLVER_SCHEME_EXPLICIT" in text and method in text
+    (tmp_path / "param.txt").write_text(text)
+    res_cpu, rst_cpu = run(EXE_CPU, tmp_path / "cpu", tmp_path / "param.txt")
+    res_gpu, rst_gpu = run(EXE_GPU, tmp_path / "gpu", tmp_path / "param.txt")
+    assert res_cpu.shape == res_gpu.shape and res_cpu.shape[0] == iters
+    np.testing.assert_allclose(res_gpu, res_cpu, rtol=2e-5, atol=0)
+    qc = np.frombuffer(rst_cpu[16:], np.float64)
+    qg = np.frombuffer(rst_gpu[16:], np.float64)
+    assert np.abs(qg - qc).max() <= 1e-10 * np.abs(qc).max()
+
+
 def test_euler3d_executable_gmres_converges(gpu_available, ref_available, tmp_path):
     """Same executable with the block sweeps replaced by mixed-precision
     GMRES(30)+ILU(0) (CFD_B200_LINEAR=gmres): the residual still drops.
