@@ -71,6 +71,8 @@ extern int TimeIntegrationType, CFL_Ramp, Mach_Ramp, ZPGIteration, JacobianUpdat
 extern int JacobianMethod;
 extern double CFL_MIN, CFL_MAX, Mach_MIN, Mach_MAX, Gamma, Ref_Alpha, Ref_Beta, Venkat_KThreshold;
 extern double Inf_Rho, Inf_U, Inf_V, Inf_W, Inf_Et, Inf_Pressure, Inf_SpeedSound, Inf_Mach;
+extern int SolverMethod;           // SOLVER_METHOD_STEADY (0) / SOLVER_METHOD_UNSTEADY (1)
+extern MC_CRS SolverBlockMatrix;   // Solver.cpp:612-704
 
 namespace {
 
@@ -236,24 +238,61 @@ void Compute_DeltaT(int Iteration) {
     MaxDeltaT = ext[7];
 }
 
+namespace {
+
+// The unsteady drivers add the physical-time terms to the host block system
+// between Compute_Jacobian and the linear solve (Solver_Unsteady_Implicit.cpp:
+// 100-121): with them the system is mirrored to SolverBlockMatrix after
+// assembly and taken back from it before the solve.
+bool mirror_system() { return SolverMethod == 1; }
+
+void download_system() {
+    const size_t nnzb = (size_t)SolverBlockMatrix.IA[g.nnode];
+    g.buf.resize(25 * nnzb + 5 * (size_t)g.nnode);
+    double *A = g.buf.data(), *B = A + 25 * nnzb;
+    CHECK(cfd_get_system(g.ctx, A, B, nullptr));
+    for (size_t k = 0; k < nnzb; k++)
+        for (int r = 0; r < 5; r++)
+            for (int c = 0; c < 5; c++) SolverBlockMatrix.A[k][r][c] = A[25 * k + 5 * r + c];
+    for (int i = 0; i < g.nnode; i++)
+        for (int v = 0; v < 5; v++) SolverBlockMatrix.B[i][v] = B[5 * (size_t)i + v];
+}
+
+void upload_system() {
+    const size_t nnzb = (size_t)SolverBlockMatrix.IA[g.nnode];
+    g.buf.resize(25 * nnzb + 5 * (size_t)g.nnode);
+    double *A = g.buf.data(), *B = A + 25 * nnzb;
+    for (size_t k = 0; k < nnzb; k++)
+        for (int r = 0; r < 5; r++)
+            for (int c = 0; c < 5; c++) A[25 * k + 5 * r + c] = SolverBlockMatrix.A[k][r][c];
+    for (int i = 0; i < g.nnode; i++)
+        for (int v = 0; v < 5; v++) B[5 * (size_t)i + v] = SolverBlockMatrix.B[i][v];
+    CHECK(cfd_set_system(g.ctx, A, B));
+}
+
+}  // namespace
+
 void Compute_Jacobian(int AddTime, int Iteration) {
     ensure_init();
     if (Iteration % JacobianUpdate != 0) return;  // Jacobian.cpp:26-28
     // Euler3D's right-hand side is B = -Res (its Res_Diss is never added, FluxTest.cpp:8143-8150)
+    const bool mirror = mirror_system();
     if (JacobianMethod >= CFD_JAC_CENTRAL && JacobianMethod <= CFD_JAC_ALTERNATE)  // Roe_Jacobian.cpp:780-793
         CHECK(cfd_jacobian_fd(g.ctx, AddTime, 0, JacobianMethod, Iteration));
     else
-        CHECK(cfd_jacobian(g.ctx, AddTime, 0, g.gmres ? CFD_PREC_FP32 : CFD_PREC_FP64));
+        CHECK(cfd_jacobian(g.ctx, AddTime, 0, (g.gmres && !mirror) ? CFD_PREC_FP32 : CFD_PREC_FP64));
+    if (mirror) download_system();
 }
 
 extern "C" double MC_Iterative_Block_LU_Jacobi_CRS(int Iteration, int Direction, MC_CRS Object) {
     ensure_init();
+    if (mirror_system()) upload_system();
     double rms = 0.0;
     if (g.gmres) {
         cfd_gmres_opts o;
         cfd_gmres_default(&o);
         o.max_iters = Iteration > 0 ? Iteration : o.max_iters;
-        o.precision = CFD_PREC_FP32;
+        o.precision = mirror_system() ? CFD_PREC_FP64 : CFD_PREC_FP32;
         o.refine = 4;
         cfd_gmres_stats st;
         const int rc = cfd_gmres(g.ctx, &o, &st);
@@ -273,6 +312,7 @@ extern "C" double MC_Iterative_Block_LU_Jacobi_CRS(int Iteration, int Direction,
 
 extern "C" double MC_Iterative_Block_LUSGS_CRS(int Iteration, MC_CRS Object) {
     ensure_init();
+    if (mirror_system()) upload_system();
     double rms = 0.0;
     const int rc = cfd_block_lusgs(g.ctx, Iteration, &rms);
     if (rc == CFD_ERR_NUMERIC) return NAN;

@@ -94,6 +94,29 @@ def test_euler3d_explicit_executable_with_gpu_hot_path(gpu_available, ref_availa
     assert np.abs(qg - qc).max() <= 1e-10 * np.abs(qc).max()
 
 
+def test_euler3d_unsteady_executable_with_gpu_hot_path(gpu_available, ref_available, tmp_path):
+    """The reference's physical-time driver (Solver_Unsteady_Implicit,
+    Euler3D/src/Solver_Unsteady_Implicit.cpp:41, BDF2, 3 steps x 3 inner
+    iterations) edits the host block system between Compute_Jacobian and the
+    block sweeps; the shim mirrors the system to the host and back for it."""
+    if not EXE_GPU.exists():
+        pytest.skip("drop-in executable not built (make -C oracle gpu)")
+    write_case(tmp_path, 6, 0, 3)
+    text = (tmp_path / "param.txt").read_text()
+    text = text.replace("SOLVER_METHOD=SOLVER_METHOD_STEADY", "SOLVER_METHOD=SOLVER_METHOD_UNSTEADY")
+    text = text.replace("TIME_INTEGRATION_METHOD=TIME_INTEGRATION_METHOD_IMPLICIT_EULER",
+                        "TIME_INTEGRATION_METHOD=TIME_INTEGRATION_METHOD_IMPLICIT_EULER_BDF")
+    text += "\nPHYSICAL_DELTA_TIME=0.05\nSOLVER_INNER_NITERATION=3\n"
+    (tmp_path / "param.txt").write_text(text)
+    res_cpu, rst_cpu = run(EXE_CPU, tmp_path / "cpu", tmp_path / "param.txt")
+    res_gpu, rst_gpu = run(EXE_GPU, tmp_path / "gpu", tmp_path / "param.txt")
+    assert res_cpu.shape == res_gpu.shape and res_cpu.shape[0] == 9
+    np.testing.assert_allclose(res_gpu, res_cpu, rtol=2e-5, atol=0)
+    qc = np.frombuffer(rst_cpu[16:], np.float64)
+    qg = np.frombuffer(rst_gpu[16:], np.float64)
+    assert np.abs(qg - qc).max() <= 1e-10 * np.abs(qc).max()
+
+
 def test_euler3d_executable_gmres_converges(gpu_available, ref_available, tmp_path):
     """Same executable with the block sweeps replaced by mixed-precision
     GMRES(30)+ILU(0) (CFD_B200_LINEAR=gmres): the residual still drops.
