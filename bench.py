@@ -406,6 +406,24 @@ def cpu_count():
         return os.cpu_count() or 1
 
 
+def max_over_ranks(x, world, device=None):
+    """The largest value of x over all ranks of the process group (x itself
+    on one rank): every multi-GPU time here is the slowest rank's."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(units_per_rank, seconds, world):
+    """Whole-job throughput of `world` replicas that each processed
+    units_per_rank in at most `seconds` (the max over ranks)."""
+    return units_per_rank * world / seconds
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -538,19 +556,14 @@ def main():
             fn(w + i)
         ev1.record(stream)
         barrier()
-        ms = ev0.elapsed_time(ev1)
-        if world > 1:
-            t = torch.tensor([ms], device=f"cuda:{dev}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(ev0.elapsed_time(ev1), world, f"cuda:{dev}")
 
     # ---- headline: resident residual steps (Roe)
     with Clocks(dev) as clk:
         ms = timed(lambda i: s.residual_step(i), args.steps, args.warmup)
     clocks = clk.summary()
     ms_step = ms / args.steps
-    value = units * args.steps * world / (ms / 1e3) / 1e9
+    value = aggregate_rate(units * args.steps, ms / 1e3, world) / 1e9
 
     # ---- per-kernel breakdown of one step (events between calls)
     names = ["begin", "bc", "gradient", "limiter", "residual", "deltat"]
@@ -637,12 +650,7 @@ def main():
         fn()
         ev1.record(stream)
         barrier()
-        ms = ev0.elapsed_time(ev1)
-        if world > 1:
-            t = torch.tensor([ms], device=f"cuda:{dev}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(ev0.elapsed_time(ev1), world, f"cuda:{dev}")
 
     steady = None
     if not args.no_steady:
@@ -682,6 +690,8 @@ def main():
         sat, sat_wall, sat_peak = serve_run(ns, machs, alphas, np.zeros(len(ns)), args.serve_workers, mixed, dev)
         barrier()
         seq, seq_wall, _ = serve_run(ns, machs, alphas, None, 1, capi.PREC_FP64, dev)
+        # host wall clocks of the replicas' servers: the slowest rank sets each rate
+        wall, sat_wall, seq_wall = (max_over_ranks(w, world, f"cuda:{dev}") for w in (wall, sat_wall, seq_wall))
         lat = np.array([r.latency for r in res])
         sat_lat = np.array([r.latency for r in sat])
         conv = lambda rs: sum(r.status == 0 and r.rms_last <= STEADY_DROP * r.rms_first for r in rs)  # noqa: E731
@@ -694,12 +704,12 @@ def main():
                        "served_precision": "fp32 low-precision-only Jacobian + ILU(0)",
                        "sequential": "plain fp64 solves one at a time through the same server (1 worker)"},
             # capacity: all requests submitted at once; latency: at the stated arrival rate
-            "value": len(sat) / sat_wall * world, "wall_s": sat_wall,
+            "value": aggregate_rate(len(sat), sat_wall, world), "wall_s": sat_wall,
             "saturated_p50_s": float(np.percentile(sat_lat, 50)), "saturated_p99_s": float(np.percentile(sat_lat, 99)),
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-            "at_rate_solves_per_s": len(res) / wall * world, "converged": ok, "requests_run": len(res) + len(sat),
+            "at_rate_solves_per_s": aggregate_rate(len(res), wall, world), "converged": ok, "requests_run": len(res) + len(sat),
             "peak_reserved_gb": max(peak, sat_peak) / 1e9,
-            "sequential_fp64": {"value": len(seq) / seq_wall * world, "wall_s": seq_wall, "converged": ok_seq,
+            "sequential_fp64": {"value": aggregate_rate(len(seq), seq_wall, world), "wall_s": seq_wall, "converged": ok_seq,
                                 "p50_solve_s": float(np.percentile([r.t_done - r.t_admit for r in seq], 50))},
         }
         serve["speedup_vs_sequential_fp64"] = serve["value"] / serve["sequential_fp64"]["value"]
