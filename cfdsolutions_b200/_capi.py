@@ -18,7 +18,7 @@ ERRORS = {
     -1: "CFD_ERR_ARG", -2: "CFD_ERR_MESH", -3: "CFD_ERR_CUDA", -4: "CFD_ERR_IO", -5: "CFD_ERR_STATE",
     -6: "CFD_ERR_NUMERIC", -7: "CFD_ERR_NOT_CONVERGED", -8: "CFD_ERR_UNSUPPORTED", -9: "CFD_ERR_RANGE",
 }
-FLUX_ROE, FLUX_HLLC, FLUX_AUSM, FLUX_ROE_LMFIX, FLUX_ROE_PRECOND, FLUX_ROE_THORNBER = 0, 1, 2, 3, 4, 5
+FLUX_ROE, FLUX_HLLC, FLUX_AUSM, FLUX_ROE_LMFIX, FLUX_ROE_PRECOND, FLUX_ROE_THORNBER, FLUX_VANLEER = 0, 1, 2, 3, 4, 5, 6
 PRECOND_BTW, PRECOND_ERIKSSON, PRECOND_TURKEL = 2, 3, 5
 PRECOND_LOCAL, PRECOND_GLOBAL, PRECOND_URLOCAL = 0, 1, 2
 ORDER_FIRST, ORDER_SECOND = 0, 1

@@ -1054,7 +1054,7 @@ int cfd_set_stream(cfd_ctx *c, void *stream) {
 
 int cfd_set_params(cfd_ctx *c, const cfd_params *p) {
     if (!c || !p) { set_error("cfd_set_params: NULL"); return CFD_ERR_ARG; }
-    if (p->flux_scheme < CFD_FLUX_ROE || p->flux_scheme > CFD_FLUX_ROE_THORNBER) {
+    if (p->flux_scheme < CFD_FLUX_ROE || p->flux_scheme > CFD_FLUX_VANLEER) {
         set_error("cfd_set_params: invalid flux scheme %d", p->flux_scheme);
         return CFD_ERR_ARG;
     }
@@ -1068,6 +1068,10 @@ int cfd_set_params(cfd_ctx *c, const cfd_params *p) {
                       "precond_type LOCAL/GLOBAL/URLOCAL and precond_mach > 0");
             return CFD_ERR_ARG;
         }
+    }
+    if (p->flux_scheme == CFD_FLUX_VANLEER && p->pinf != 0.0) {
+        set_error("cfd_set_params: the Van Leer splitting is written for the ideal gas (pinf = 0)");
+        return CFD_ERR_ARG;
     }
     if (!(p->pinf >= 0.0 && p->pinf < 1.0e300)) {
         set_error("cfd_set_params: pinf must be finite and >= 0");
@@ -1485,6 +1489,8 @@ int cfd_residual(cfd_ctx *c, int add_time) {
         case 9: return residual_with_fix<CFD_FLUX_ROE_PRECOND, true>(c, add_time);
         case 10: return residual_with_fix<CFD_FLUX_ROE_THORNBER, false>(c, add_time);
         case 11: return residual_with_fix<CFD_FLUX_ROE_THORNBER, true>(c, add_time);
+        case 12: return residual_with_fix<CFD_FLUX_VANLEER, false>(c, add_time);
+        case 13: return residual_with_fix<CFD_FLUX_VANLEER, true>(c, add_time);
         default: set_error("cfd_residual: bad flux scheme"); return CFD_ERR_ARG;
     }
 }

@@ -97,13 +97,15 @@ void die(const char *where, int code) {
 void sync_params() {
     cfd_params p;
     cfd_params_default(&p);
-    // PRECOND_METHOD_NONE (-1) or PRECOND_METHOD_ROE_LMFIX (0) with the Roe flux
-    if (VariableType != 0 || !(PrecondMethod == -1 || (PrecondMethod == 0 && FluxScheme == CFD_FLUX_ROE))) {
-        std::fprintf(stderr, "cfd_b200 shim: only VARIABLE_CONSERVATIVE without preconditioning or with the Roe "
-                             "low-Mach fix is supported\n");
+    // PRECOND_METHOD_NONE (-1) or PRECOND_METHOD_ROE_LMFIX (0) with the Roe flux; FLUX_SCHEME_ROE,
+    // _HLLC, _AUSM or _VANLEER (SolverParameters.h:109-117; the other families are empty stubs there)
+    if (VariableType != 0 || !(PrecondMethod == -1 || (PrecondMethod == 0 && FluxScheme == CFD_FLUX_ROE)) ||
+        FluxScheme < 0 || FluxScheme > 3) {
+        std::fprintf(stderr, "cfd_b200 shim: only VARIABLE_CONSERVATIVE with the Roe (optionally with its low-Mach "
+                             "fix), HLLC, AUSM or Van Leer flux is supported\n");
         std::exit(EXIT_FAILURE);
     }
-    p.flux_scheme = PrecondMethod == 0 ? CFD_FLUX_ROE_LMFIX : FluxScheme;
+    p.flux_scheme = PrecondMethod == 0 ? CFD_FLUX_ROE_LMFIX : (FluxScheme == 3 ? CFD_FLUX_VANLEER : FluxScheme);
     p.order = SolverOrder;
     p.limiter = LimiterMethod;
     p.limiter_order = LimiterOrder;

@@ -132,12 +132,79 @@ __device__ __forceinline__ double ausmp_flux(const double qL[5], const double qR
     return fabs(u * nx + v * ny + w * nz) + c;
 }
 
+// Van Leer flux-vector splitting (Compute_VanLeerFlux, Euler3D/src/VanLeer_Fluxes.cpp:143-305):
+// F+ of the left state and F- of the right state by the face-normal Mach
+// number, the full flux beyond |M| = 1; no dissipative part; the time-step
+// eigenvalue from the arithmetic means (c of the mean rho and p).  Ideal gas.
+__device__ __forceinline__ double vanleer_flux(const double qL[5], const double qR[5], double nx, double ny,
+                                               double nz, double area, const Flow &f, double conv[5],
+                                               double diss[5], double lam[3]) {
+    Face L, R;
+    eos_face(qL, nx, ny, nz, f, true, L);
+    eos_face(qR, nx, ny, nz, f, true, R);
+    const double g = f.gamma, gg = g * g - 1.0;
+    const double rho_a = 0.5 * (L.rho + R.rho);
+    const double ub_a = 0.5 * ((L.u + R.u) * nx + (L.v + R.v) * ny + (L.w + R.w) * nz);
+    const double p_a = 0.5 * (L.p + R.p);
+    const double c_a = sqrt(g * p_a / rho_a);
+    double fp[5], fm[5];
+    {
+        const double M = L.ubar / L.c, q2 = L.u * L.u + L.v * L.v + L.w * L.w;
+        if (fabs(M) < 1.0) {
+            const double b = -L.ubar + 2.0 * L.c;
+            fp[0] = 0.25 * L.rho * L.c * (M + 1.0) * (M + 1.0);
+            fp[1] = fp[0] * (nx * b / g + L.u);
+            fp[2] = fp[0] * (ny * b / g + L.v);
+            fp[3] = fp[0] * (nz * b / g + L.w);
+            fp[4] = fp[0] * ((-(g - 1.0) * L.ubar * L.ubar + 2.0 * (g - 1.0) * L.ubar * L.c + 2.0 * L.c * L.c) / gg +
+                             0.5 * q2);
+        } else if (M >= 1.0) {
+            fp[0] = L.rho * L.ubar;
+            fp[1] = L.rho * L.u * L.ubar + nx * L.p;
+            fp[2] = L.rho * L.v * L.ubar + ny * L.p;
+            fp[3] = L.rho * L.w * L.ubar + nz * L.p;
+            fp[4] = (qL[4] + L.p) * L.ubar;
+        } else {
+            fp[0] = fp[1] = fp[2] = fp[3] = fp[4] = 0.0;
+        }
+    }
+    {
+        const double M = R.ubar / R.c, q2 = R.u * R.u + R.v * R.v + R.w * R.w;
+        if (fabs(M) < 1.0) {
+            const double b = -R.ubar - 2.0 * R.c;
+            fm[0] = -0.25 * R.rho * R.c * (M - 1.0) * (M - 1.0);
+            fm[1] = fm[0] * (nx * b / g + R.u);
+            fm[2] = fm[0] * (ny * b / g + R.v);
+            fm[3] = fm[0] * (nz * b / g + R.w);
+            fm[4] = fm[0] * ((-(g - 1.0) * R.ubar * R.ubar - 2.0 * (g - 1.0) * R.ubar * R.c + 2.0 * R.c * R.c) / gg +
+                             0.5 * q2);
+        } else if (M <= -1.0) {
+            fm[0] = R.rho * R.ubar;
+            fm[1] = R.rho * R.u * R.ubar + nx * R.p;
+            fm[2] = R.rho * R.v * R.ubar + ny * R.p;
+            fm[3] = R.rho * R.w * R.ubar + nz * R.p;
+            fm[4] = (qR[4] + R.p) * R.ubar;
+        } else {
+            fm[0] = fm[1] = fm[2] = fm[3] = fm[4] = 0.0;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        conv[k] = (fp[k] + fm[k]) * area;
+        diss[k] = 0.0;
+    }
+    // the reference leaves the eigenvalue extrema untouched for this flux
+    lam[0] = lam[1] = lam[2] = __longlong_as_double(0x7ff8000000000000LL);
+    return fmax(fabs(ub_a), fmax(fabs(ub_a + c_a), fabs(ub_a - c_a)));
+}
+
 template <int FLUX>
 __device__ __forceinline__ double edge_flux(const double qL[5], const double qR[5], double nx, double ny, double nz,
                                             double area, const Flow &f, double conv[5], double diss[5],
                                             double lam[3]) {
     if (FLUX == CFD_FLUX_HLLC) return hllc_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
     if (FLUX == CFD_FLUX_AUSM) return ausmp_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
+    if (FLUX == CFD_FLUX_VANLEER) return vanleer_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
     if (FLUX == CFD_FLUX_ROE_PRECOND) return roe_precond_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
     if (FLUX == CFD_FLUX_ROE_THORNBER) {
         double mL[5], mR[5];

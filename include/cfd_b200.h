@@ -68,6 +68,9 @@ extern "C" {
                                 blended toward each other by min(1, max Mach) before the Roe flux
                                 (Compute_Flux_Roe_Thornber, MPFLOW3D/src/Roe_Fluxes.cpp:1081), plain
                                 characteristic BCs */
+#define CFD_FLUX_VANLEER 6    /* FLUX_SCHEME_VANLEER (SolverParameters.h:114): Van Leer flux-vector splitting
+                                (Compute_VanLeerFlux, Euler3D/src/VanLeer_Fluxes.cpp:143), ideal gas only;
+                                implicit steps use the approximate Roe Jacobian */
 /* cfd_params.precond_method (MPFLOW3D PRECOND_METHOD values) */
 #define CFD_PRECOND_BTW      2  /* Briley-Taylor-Whitfield: alpha 0, delta 1    */
 #define CFD_PRECOND_ERIKSSON 3  /* Eriksson: alpha 0, delta beta                */

@@ -581,6 +581,54 @@ static double hllc(const double *qL, const double *qR, const double *n, double a
     return lmax;
 }
 
+/* Compute_VanLeerFlux (Euler3D/src/VanLeer_Fluxes.cpp:143-305): Van Leer flux-vector
+ * splitting, F+ of the left and F- of the right face state by the normal Mach number;
+ * the time step takes the eigenvalues of the arithmetic mean state. */
+static double vanleer(const double *qL, const double *qR, const double *n, double area, const orc_params *p,
+                      double *conv, double *diss) {
+    face_t L, R;
+    double g = p->gamma, nx = n[0], ny = n[1], nz = n[2];
+    eos_face(qL, nx, ny, nz, g, p->pinf, &L);
+    eos_face(qR, nx, ny, nz, g, p->pinf, &R);
+    double rho_a = 0.5 * (L.rho + R.rho), ub_a = 0.5 * ((L.u + R.u) * nx + (L.v + R.v) * ny + (L.w + R.w) * nz);
+    double p_a = 0.5 * (L.p + R.p), c_a = sqrt(g * p_a / rho_a);
+    double lmax = dmax(fabs(ub_a), dmax(fabs(ub_a + c_a), fabs(ub_a - c_a)));
+    double fp[5] = {0, 0, 0, 0, 0}, fm[5] = {0, 0, 0, 0, 0};
+    double M = L.ubar / L.c, q2 = L.u * L.u + L.v * L.v + L.w * L.w;
+    if (fabs(M) < 1.0) {
+        double b = -L.ubar + 2.0 * L.c;
+        fp[0] = 0.25 * L.rho * L.c * (M + 1.0) * (M + 1.0);
+        fp[1] = fp[0] * (nx * b / g + L.u);
+        fp[2] = fp[0] * (ny * b / g + L.v);
+        fp[3] = fp[0] * (nz * b / g + L.w);
+        fp[4] = fp[0] * ((-(g - 1.0) * L.ubar * L.ubar + 2.0 * (g - 1.0) * L.ubar * L.c + 2.0 * L.c * L.c) / (g * g - 1.0) + 0.5 * q2);
+    } else if (M >= 1.0) {
+        fp[0] = L.rho * L.ubar;
+        fp[1] = L.rho * L.u * L.ubar + nx * L.p;
+        fp[2] = L.rho * L.v * L.ubar + ny * L.p;
+        fp[3] = L.rho * L.w * L.ubar + nz * L.p;
+        fp[4] = (L.rho * L.et + L.p) * L.ubar;
+    }
+    M = R.ubar / R.c;
+    q2 = R.u * R.u + R.v * R.v + R.w * R.w;
+    if (fabs(M) < 1.0) {
+        double b = -R.ubar - 2.0 * R.c;
+        fm[0] = -0.25 * R.rho * R.c * (M - 1.0) * (M - 1.0);
+        fm[1] = fm[0] * (nx * b / g + R.u);
+        fm[2] = fm[0] * (ny * b / g + R.v);
+        fm[3] = fm[0] * (nz * b / g + R.w);
+        fm[4] = fm[0] * ((-(g - 1.0) * R.ubar * R.ubar - 2.0 * (g - 1.0) * R.ubar * R.c + 2.0 * R.c * R.c) / (g * g - 1.0) + 0.5 * q2);
+    } else if (M <= -1.0) {
+        fm[0] = R.rho * R.ubar;
+        fm[1] = R.rho * R.u * R.ubar + nx * R.p;
+        fm[2] = R.rho * R.v * R.ubar + ny * R.p;
+        fm[3] = R.rho * R.w * R.ubar + nz * R.p;
+        fm[4] = (R.rho * R.et + R.p) * R.ubar;
+    }
+    for (int k = 0; k < 5; k++) { conv[k] = (fp[k] + fm[k]) * area; diss[k] = 0.0; }
+    return lmax;
+}
+
 /* AUSM+ restated from Liou, J. Comput. Phys. 129 (1996) 364-382: c_1/2 =
  * min(c^_L, c^_R), c^ = c*^2/max(c*, |u|), c*^2 = 2(g-1)/(g+1) H; M+-(M)
  * degree-4 polynomials with beta = 1/8, P+-(M) degree-5 with alpha = 3/16.
@@ -662,6 +710,7 @@ void orc_residual(const orc_mesh *m, const orc_params *p, const double *Q, const
             }
             if (p->flux == 1) lmax = hllc(qL, qR, n, area, p, fc, fd);
             else if (p->flux == 2) lmax = ausmp(qL, qR, n, area, p, fc, fd);
+            else if (p->flux == 6) lmax = vanleer(qL, qR, n, area, p, fc, fd);
             else {
                 if (p->flux == 5) {
                     double mL[5], mR[5];

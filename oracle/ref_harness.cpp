@@ -23,6 +23,7 @@
 
 void Roe_Init_New(void);
 void HLLC_Init(void);
+void VanLeer_Init(void);
 
 static Edge3D *alloc_edges(int n) {
     Edge3D *e = (Edge3D *)malloc((size_t)(n > 0 ? n : 1) * sizeof(Edge3D));
@@ -92,6 +93,7 @@ void ref_setup_mesh(int nnode, int nghost, int nedge, const int *edge_nodes,
     switch (FluxScheme) {
         case FLUX_SCHEME_ROE: Roe_Init_New(); break;
         case FLUX_SCHEME_HLLC: HLLC_Init(); break;
+        case FLUX_SCHEME_VANLEER: VanLeer_Init(); break;
         default: break;
     }
 }

@@ -24,7 +24,7 @@ HERE = Path(__file__).resolve().parent
 REF_LIB = HERE / "_ref" / "libeuler3d_ref.so"
 REF_EXE = HERE / "_ref" / "euler3d"
 
-FLUX = {0: "FLUX_SCHEME_ROE", 1: "FLUX_SCHEME_HLLC", 2: "FLUX_SCHEME_AUSM", 3: "FLUX_SCHEME_ROE"}
+FLUX = {0: "FLUX_SCHEME_ROE", 1: "FLUX_SCHEME_HLLC", 2: "FLUX_SCHEME_AUSM", 3: "FLUX_SCHEME_ROE", 6: "FLUX_SCHEME_VANLEER"}
 LIMITER = {-1: "LIMITER_METHOD_NONE", 0: "LIMITER_METHOD_BERTH_JESPERSEN", 1: "LIMITER_METHOD_VENKATAKRISHNAN"}
 
 

@@ -70,15 +70,18 @@ def test_euler3d_executable_with_gpu_hot_path(gpu_available, ref_available, tmp_
     assert np.abs(qg - qc).max() <= 1e-10 * np.abs(qc).max()
 
 
-@pytest.mark.parametrize("method", ["TIME_INTEGRATION_METHOD_EXPLICIT_EULER", "TIME_INTEGRATION_METHOD_EXPLICIT_RK4"])
-def test_euler3d_explicit_executable_with_gpu_hot_path(gpu_available, ref_available, tmp_path, method):
+@pytest.mark.parametrize("method,flux", [("TIME_INTEGRATION_METHOD_EXPLICIT_EULER", 0),
+                                         ("TIME_INTEGRATION_METHOD_EXPLICIT_RK4", 0),
+                                         ("TIME_INTEGRATION_METHOD_EXPLICIT_RK4", 6)])
+def test_euler3d_explicit_executable_with_gpu_hot_path(gpu_available, ref_available, tmp_path, method, flux):
     """The reference's explicit drivers (Solver_Steady_Explicit_Euler / _RK4,
     Euler3D/src/Solver_Steady_Explicit.cpp:25, :202) over the GPU residual,
-    gradient, limiter, boundary and time-step functions."""
+    gradient, limiter, boundary and time-step functions; flux 6 is
+    FLUX_SCHEME_VANLEER, which the reference runs with its explicit drivers only."""
     if not EXE_GPU.exists():
         pytest.skip("drop-in executable not built (make -C oracle gpu)")
     iters = 5
-    write_case(tmp_path, 8, 1, iters)
+    write_case(tmp_path, 8, 1, iters, flux=flux)
     text = (tmp_path / "param.txt").read_text()
     text = text.replace("SOLVER_SCHEME=SOLVER_SCHEME_IMPLICIT", "SOLVER_SCHEME=SOLVER_SCHEME_EXPLICIT")
     text = text.replace("TIME_INTEGRATION_METHOD=TIME_INTEGRATION_METHOD_IMPLICIT_EULER", f"TIME_INTEGRATION_METHOD={method}")

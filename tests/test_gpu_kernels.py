@@ -45,6 +45,8 @@ CASES = [
     dict(CFG1, order=1, gradient=1, limiter=1, flux_scheme=2, mach=0.8, mach_min=0.8, alpha_deg=1.25),
     dict(CFG1, order=1, gradient=0, limiter=0, limiter_order=1, mach=0.8, mach_min=0.8, alpha_deg=1.25),
     dict(CFG1, order=1, gradient=1, limiter=-1, entropy_fix=1),
+    dict(CFG1, flux_scheme=6),
+    dict(CFG1, order=1, gradient=0, limiter=1, flux_scheme=6, mach=0.8, mach_min=0.8, alpha_deg=1.25),
 ]
 
 

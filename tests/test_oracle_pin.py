@@ -379,3 +379,27 @@ def test_thornber_is_roe_above_mach_one_and_blends_velocities_below():
     ma[1:4] = qa[0] * 0.5 * ((1 + z) * va + (1 - z) * vb)
     mb[1:4] = qb[0] * 0.5 * ((1 + z) * vb + (1 - z) * va)
     np.testing.assert_allclose(flux(qa, qb, 5), flux(ma, mb, 0), rtol=1e-13, atol=1e-15)
+
+
+@pytest.mark.parametrize("order", [0, 1])
+def test_vanleer_matches_reference(ref_available, order):
+    """Flux 6 (FLUX_SCHEME_VANLEER, Compute_VanLeerFlux) of the restatement
+    against the compiled reference: residual and time step, first and second
+    order (LSQ + Venkatakrishnan)."""
+    cfg = dict(CFG1, flux_scheme=6, order=order, limiter=1 if order else -1, venkat_k=5.0, mach=0.8, mach_min=0.8,
+               alpha_deg=1.25)
+    m, cfg, Q = make_case(n=7, seed=21, cfg=cfg, noise=0.02)
+    steps = [("begin", 0)] + ([("gradient", 0), ("limiter",)] if order else [])
+    steps += [("bc", 0), ("residual", 1), ("get", "residual"), ("deltat", 0), ("get", "deltat")]
+    ref = refharness.run(m, cfg, Q, steps)
+    s = restatement.Session(m, cfg)
+    g = phi = None
+    if order:
+        g = s.gradient(Q)
+        phi = s.limiter(Q, g)
+    Qb = s.apply_bc(Q)
+    conv, diss, dts, _ = s.residual(Qb, g, phi)
+    dt, _ = s.deltat(dts)
+    assert relerr_rows(conv, ref["conv"]) <= TOL
+    assert np.abs(diss).max() == 0.0 and np.abs(ref["diss"]).max() == 0.0
+    assert relerr(dt, ref["deltat"]) <= TOL
