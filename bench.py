@@ -82,6 +82,18 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
+def profile_figure(key):
+    """A `key: value` figure of the committed ncu summary of the residual kernel
+    (None if not captured)."""
+    p = ROOT / "profiles" / "residual_roe2_128.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith(key + ":"):
+            return float(line.split(":")[1])
+    return None
+
+
 def traffic_from_profile():
     """DRAM bytes per residual launch from the committed ncu summary, scaled
     per edge (None if not captured)."""
@@ -591,7 +603,10 @@ def main():
     roofline = {"bound": "hbm", "kernel": "k_residual_gather<ROE,SECOND>", "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                 "algorithmic_bytes_per_launch": abytes, "launch_ms": ms_res,
-                "traffic": (tpe * units) if tpe else None}
+                "traffic": (tpe * units) if tpe else None,
+                # the kernel is bound by FP64 issue, not HBM (ncu, profiles/residual_roe2_128.md)
+                "fp64_pipe_active_pct": profile_figure("fp64_pipe_active_pct"),
+                "issue_active_pct": profile_figure("issue_active_pct")}
 
     # ---- other flux families (HLLC, AUSM+)
     per_flux = {"roe": {"gedges_per_s": value / world, "ms_per_step": ms_step}}
