@@ -598,7 +598,9 @@ __device__ __forceinline__ void pc_node_cinv(const double q[5], const Flow &f, d
 
 // x = A^-1 b for a 5x5 system by Gaussian elimination with partial pivoting
 // (the pivoted LU the preconditioned BC solves with); A is overwritten.
-__device__ __forceinline__ void solve5_pivot(double A[25], double b[5], double x[5]) {
+// Returns false (x then undefined) when a pivot is zero.
+__device__ __forceinline__ bool solve5_pivot(double A[25], double b[5], double x[5]) {
+    bool ok = true;
 #pragma unroll
     for (int c = 0; c < 5; c++) {
         int p = c;
@@ -616,6 +618,7 @@ __device__ __forceinline__ void solve5_pivot(double A[25], double b[5], double x
             b[c] = b[p];
             b[p] = t;
         }
+        if (A[5 * c + c] == 0.0) ok = false;
 #pragma unroll
         for (int i = c + 1; i < 5; i++) {
             const double m = A[5 * i + c] / A[5 * c + c];
@@ -631,6 +634,7 @@ __device__ __forceinline__ void solve5_pivot(double A[25], double b[5], double x
         for (int j = i + 1; j < 5; j++) t -= A[5 * i + j] * x[j];
         x[i] = t / A[5 * i + i];
     }
+    return ok;
 }
 
 // Ghost state of the preconditioned characteristic BC
@@ -640,7 +644,8 @@ __device__ __forceinline__ void solve5_pivot(double A[25], double b[5], double x
 // wall = four outgoing characteristics and zero normal velocity; subsonic
 // inflow = freestream (rho, u, v, w) with the interior's p and the u.n + c'
 // characteristic from inside; subsonic outflow = four characteristics from
-// inside and the outflow pressure.  Returns as characteristic_bc.
+// inside and the outflow pressure.  Returns as characteristic_bc (2 also for
+// a singular characteristic system).
 __device__ __forceinline__ int precond_characteristic_bc(const double qI[5], const double qG[5], double nx,
                                                          double ny, double nz, int bc_type, const Flow &f,
                                                          double qB[5]) {
@@ -697,7 +702,7 @@ __device__ __forceinline__ int precond_characteristic_bc(const double qI[5], con
             for (int k = 0; k < 4; k++) B[k] = lrow(k, qi);
             B[4] = 0.0;
             Lm[20] = 0.0; Lm[21] = nx; Lm[22] = ny; Lm[23] = nz; Lm[24] = 0.0;
-            solve5_pivot(Lm, B, xb);
+            if (!solve5_pivot(Lm, B, xb)) status = status ? status : 2;
             if (f.iteration < f.zpg_iteration && xb[4] + f.pinf < 0.0) {
                 xb[0] = I.rho; xb[4] = I.p;
                 xb[1] = I.u - nx * I.ubar; xb[2] = I.v - ny * I.ubar; xb[3] = I.w - nz * I.ubar;
@@ -708,19 +713,19 @@ __device__ __forceinline__ int precond_characteristic_bc(const double qI[5], con
             const double qe[5] = {qf[0], qf[1], qf[2], qf[3], inst == 4 ? I.p : qf[4]};
 #pragma unroll
             for (int k = 0; k < 5; k++) B[k] = k == 3 ? lrow(3, qi) : lrow(k, qe);
-            solve5_pivot(Lm, B, xb);
+            if (!solve5_pivot(Lm, B, xb)) status = status ? status : 2;
         } break;
         case 5:
 #pragma unroll
             for (int k = 0; k < 4; k++) B[k] = lrow(k, qi);
             B[4] = f.pc_outflow_p;
             Lm[20] = 0.0; Lm[21] = 0.0; Lm[22] = 0.0; Lm[23] = 0.0; Lm[24] = 1.0;
-            solve5_pivot(Lm, B, xb);
+            if (!solve5_pivot(Lm, B, xb)) status = status ? status : 2;
             break;
         case 9:
 #pragma unroll
             for (int k = 0; k < 5; k++) B[k] = k == 4 ? lrow(4, qf) : lrow(k, qi);
-            solve5_pivot(Lm, B, xb);
+            if (!solve5_pivot(Lm, B, xb)) status = status ? status : 2;
             break;
         case 7: case 11:
 #pragma unroll
