@@ -124,10 +124,10 @@ __global__ void __launch_bounds__(128, 3) k_residual_gather(
     const double *__restrict__ phi, const double *__restrict__ xyz, const int64_t *__restrict__ sell_ptr,
     const int *__restrict__ sell_nbr, const double4 *__restrict__ sell_geo, const int *__restrict__ deg,
     const int *__restrict__ n2b_ptr, const int *__restrict__ n2b, const int2 *__restrict__ bn,
-    const double4 *__restrict__ bg, Flow f, int add_time, int check_roe, int *__restrict__ roeflag,
-    int *__restrict__ roecount, const int *__restrict__ gate, double *__restrict__ res, double *__restrict__ resd,
+    const double4 *__restrict__ bg, Flow f, int add_time, int checks, int *__restrict__ roeflag,
+    int *__restrict__ fixcount, const int *__restrict__ gate, double *__restrict__ res, double *__restrict__ resd,
     double *__restrict__ dtsum, unsigned long long *__restrict__ ext) {
-    if (gate && *gate == 0) return;
+    if (gate && gate[0] == 0 && gate[1] == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
     if (i < nnode) {
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(128, 3) k_residual_gather(
             for (int d = 0; d < 3; d++) xo[d] = xyz[d * (int64_t)nnode + i];
         }
         double ac[5] = {0, 0, 0, 0, 0}, ad[5] = {0, 0, 0, 0, 0}, adt = 0.0;
-        bool roe_bad = false;
+        int bad = 0;  // bit 0: Roe-average pressure < 0, bit 1: own reconstructed pressure < 0
         const int64_t base = sell_ptr[i >> 5] + (i & 31);
         const int d = deg[i];
         for (int k = 0; k < d; k++) {
@@ -169,6 +169,9 @@ __global__ void __launch_bounds__(128, 3) k_residual_gather(
                     fo[v] = qo[v] + po[v] * (f.frac * (qn[v] - qo[v]) + (1.0 - f.frac) * gno);
                     fn[v] = qn[v] + pn * (f.frac * (qo[v] - qn[v]) + (1.0 - f.frac) * gnn);
                 }
+                // the limiter's reconstructed-pressure correction (Limiters.cpp:273-304)
+                // tests exactly this node's own face states
+                if ((checks & 2) && recon_pressure_negative(fo, f)) bad |= 2;
             } else {
 #pragma unroll
                 for (int v = 0; v < 5; v++) { fo[v] = qo[v]; fn[v] = qn[v]; }
@@ -179,7 +182,7 @@ __global__ void __launch_bounds__(128, 3) k_residual_gather(
                 qL[v] = own_is_L ? fo[v] : fn[v];
                 qR[v] = own_is_L ? fn[v] : fo[v];
             }
-            if (SECOND && check_roe && roe_avg_pressure(qL, qR, f.gamma, f.gpinf) < 0.0) roe_bad = true;
+            if (SECOND && (checks & 1) && roe_avg_pressure(qL, qR, f.gamma, f.gpinf) < 0.0) bad |= 1;
             double cf[5], df[5], lam[3];
             const double lmax = edge_flux<FLUX>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam);
             const double sg = own_is_L ? 1.0 : -1.0;
@@ -192,9 +195,10 @@ __global__ void __launch_bounds__(128, 3) k_residual_gather(
 #pragma unroll
             for (int m = 0; m < 3; m++) { mn[m] = fmin(mn[m], lam[m]); mx[m] = fmax(mx[m], lam[m]); }
         }
-        if (roe_bad) {
-            roeflag[i] = 1;
-            atomicAdd(roecount, 1);
+        if (bad) {
+            roeflag[i] = bad;
+            if (bad & 1) atomicAdd(&fixcount[0], 1);
+            if (bad & 2) atomicAdd(&fixcount[1], 1);
         }
         // boundary edges: first order, flux into node_L only (FluxTest.cpp:8044-8098)
         for (int k = n2b_ptr[i]; k < n2b_ptr[i + 1]; k++) {
@@ -236,8 +240,8 @@ __global__ void __launch_bounds__(128, 3) k_residual_gather(
 // atomics on the residual, deterministic summation order, one flux evaluation
 // per edge per patch instead of one per edge end, and the L1 cache stays free
 // for the few global loads left (ghost states of boundary edges).
-// `gate`: when non-null and *gate == 0 the launch does nothing (conditional
-// re-evaluation after the limiter's pressure fix).
+// `gate`: when non-null and both fix counters are zero the launch does nothing
+// (conditional re-evaluation after the limiter's pressure fixes).
 template <int FLUX, bool SECOND>
 __global__ void __launch_bounds__(PATCH_CHUNK, 2) k_residual_patch(
     int nnode, int64_t ldq, const double *__restrict__ Q, const double *__restrict__ grad,
@@ -246,9 +250,9 @@ __global__ void __launch_bounds__(PATCH_CHUNK, 2) k_residual_patch(
     const int *__restrict__ halo, const int *__restrict__ inc_ptr, const int *__restrict__ inc,
     const int *__restrict__ n2b_ptr, const int *__restrict__ n2b, const int2 *__restrict__ bn,
     const double4 *__restrict__ bg, Flow f, int add_time, int nlm, int check_roe, int *__restrict__ roeflag,
-    int *__restrict__ roecount, const int *__restrict__ gate, double *__restrict__ res, double *__restrict__ resd,
+    int *__restrict__ fixcount, const int *__restrict__ gate, double *__restrict__ res, double *__restrict__ resd,
     double *__restrict__ dtsum, unsigned long long *__restrict__ ext) {
-    if (gate && *gate == 0) return;
+    if (gate && gate[0] == 0 && gate[1] == 0) return;
     constexpr int NV = SECOND ? PATCH_NV2 : 5;
     extern __shared__ double sm[];
     double *nv = sm;                       // [NV][nlm]: Q 0-4 | grad 5-19 | phi 20-24 | xyz 25-27
@@ -312,7 +316,7 @@ __global__ void __launch_bounds__(PATCH_CHUNK, 2) k_residual_patch(
                 if (check_roe && roe_avg_pressure(qL, qR, f.gamma, f.gpinf) < 0.0) {
                     roeflag[a < nown ? n0 + a : halo[h0 + a - nown]] = 1;
                     roeflag[b < nown ? n0 + b : halo[h0 + b - nown]] = 1;
-                    atomicAdd(roecount, 1);
+                    atomicAdd(&fixcount[0], 1);
                 }
             }
             double cf[5], df[5], lam[3];
@@ -376,15 +380,33 @@ __global__ void __launch_bounds__(PATCH_CHUNK, 2) k_residual_patch(
     if (add_time) block_extrema3(mn, mx, ext);
 }
 
-// Limiter pressure fix selected by the residual's check: zero the limiters of
-// flagged nodes; no-op unless some edge failed (*count == 0).
-__global__ void k_roe_fix_apply(int nnode, const int *__restrict__ count, const int *__restrict__ flag,
-                                double *__restrict__ phi) {
-    if (*count == 0) return;
+// Limiter fixes selected by the residual's checks (count = fixcount, flag =
+// per-node bits).  When no reconstructed pressure failed (count[1] == 0) the
+// Roe check saw the final limiters and its flagged nodes (bit 0) drop to
+// first order.  Otherwise the correction (bit 1) is applied first, as the
+// reference orders the two (Limiters.cpp:61-110 after :273-304), and, when
+// `redo_roe`, the corrected limiters are also copied to `work` for a full
+// k_roe_pressure_fix pass.  No-op when both counts are zero.
+__global__ void k_limiter_fix_apply(int nnode, const int *__restrict__ count, const int *__restrict__ flag,
+                                    int redo_roe, double *__restrict__ phi, double *__restrict__ work) {
+    const int nroe = count[0], npc = count[1];
+    if (nroe == 0 && npc == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nnode || !flag[i]) return;
+    if (i >= nnode) return;
+    const int fl = flag[i];
+    if (npc == 0) {
+        if (fl & 1) {
 #pragma unroll
-    for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = 0.0;
+            for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = 0.0;
+        }
+        return;
+    }
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        const double ph = (fl & 2) ? 0.0 : phi[v * (int64_t)nnode + i];
+        if (fl & 2) phi[v * (int64_t)nnode + i] = 0.0;
+        if (redo_roe) work[v * (int64_t)nnode + i] = ph;
+    }
 }
 
 // dt_i = V_i * CFL / sum_i (Compute_DeltaT, Euler3D/src/Time_Step.cpp:23-51).
@@ -806,10 +828,9 @@ static void compute_flow(cfd_ctx *c, int iteration) {
         c->cfl = p.cfl_max;
 }
 
-static bool patch_kernel(const cfd_ctx *c) { return c->use_patch && c->params.residual_kernel == 1; }
 
 template <int FLUX, bool SECOND>
-static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, const int *gate) {
+static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, bool check_pc, const int *gate) {
     if (patch_kernel(c)) {
         const size_t smem = patch_smem_bytes(c->patch_nlocmax, SECOND);
         if (smem > 48 * 1024) {
@@ -823,13 +844,14 @@ static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, const int *
         k_residual_patch<FLUX, SECOND><<<c->npatch, PATCH_CHUNK, smem, c->stream>>>(
             c->nnode, c->ldq, c->Q.p, c->grad.p, c->phi.p, c->xyz.p, c->pe_ptr.p, c->pe_loc.p, c->pe_geo.p,
             c->ph_ptr.p, c->halo.p, c->inc_ptr.p, c->inc.p, c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p,
-            c->flow, add_time, c->patch_nlocmax, check_roe ? 1 : 0, c->roeflag.p, c->roecount.p, gate, c->res.p,
+            c->flow, add_time, c->patch_nlocmax, check_roe ? 1 : 0, c->roeflag.p, c->fixcount.p, gate, c->res.p,
             c->resd.p, c->dt.p, c->ext.p);
     } else {
         k_residual_gather<FLUX, SECOND><<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(
             c->nnode, c->ldq, c->Q.p, c->grad.p, c->phi.p, c->xyz.p, c->sell_ptr.p, c->sell_nbr.p, c->sell_geo.p,
             c->deg.p, c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p, c->flow, add_time,
-            check_roe ? 1 : 0, c->roeflag.p, c->roecount.p, gate, c->res.p, c->resd.p, c->dt.p, c->ext.p);
+            (check_roe ? 1 : 0) | (check_pc ? 2 : 0), c->roeflag.p, c->fixcount.p, gate, c->res.p, c->resd.p,
+            c->dt.p, c->ext.p);
     }
     CFD_LAUNCH_CHECK();
     return CFD_OK;
@@ -934,16 +956,35 @@ __global__ void __launch_bounds__(128) k_lusgs_level(int nrows, const int *__res
 
 template <int FLUX, bool SECOND>
 static int residual_with_fix(cfd_ctx *c, int add_time) {
-    // Roe flux + limiter: the limiter's Roe-average pressure fix is decided by
-    // the residual's own reconstruction (same states) and applied, followed by
-    // a gated re-evaluation, only when some edge failed the check.
-    const bool fused = SECOND && is_roe_flux(FLUX) && c->roe_fix_pending;
-    int st = launch_residual<FLUX, SECOND>(c, add_time, fused, nullptr);
-    if (st || !fused) return st;
-    k_roe_fix_apply<<<grid_for(c->nnode, 256), 256, 0, c->stream>>>(c->nnode, c->roecount.p, c->roeflag.p, c->phi.p);
+    // Second order with a limiter: the limiter's pressure fixes are decided by
+    // the residual's own reconstruction (the same face states) and applied,
+    // followed by a gated re-evaluation, only when some node failed a check;
+    // nothing is read back to the host.  The patch kernel carries only the
+    // Roe check, so a pending reconstructed-pressure correction runs first.
+    if (!SECOND) return launch_residual<FLUX, SECOND>(c, add_time, false, false, nullptr);
+    if (c->pc_fix_pending && patch_kernel(c)) {
+        const bool roe = c->roe_fix_pending;
+        c->roe_fix_pending = false;
+        int st = limiter_fix_standalone(c);
+        c->roe_fix_pending = roe;
+        if (st) return st;
+    }
+    const bool check_roe = is_roe_flux(FLUX) && c->roe_fix_pending;
+    const bool check_pc = c->pc_fix_pending;
+    int st = launch_residual<FLUX, SECOND>(c, add_time, check_roe, check_pc, nullptr);
+    if (st || !(check_roe || check_pc)) return st;
+    const bool redo_roe = check_roe && check_pc;
+    if (redo_roe) CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)5 * c->nnode)));
+    k_limiter_fix_apply<<<grid_for(c->nnode, 256), 256, 0, c->stream>>>(c->nnode, c->fixcount.p, c->roeflag.p,
+                                                                         redo_roe ? 1 : 0, c->phi.p, c->work.p);
     CFD_LAUNCH_CHECK();
+    if (redo_roe) {
+        st = launch_roe_pressure_fix(c, c->fixcount.p);
+        if (st) return st;
+    }
     c->roe_fix_pending = false;
-    return launch_residual<FLUX, SECOND>(c, add_time, false, c->roecount.p);
+    c->pc_fix_pending = false;
+    return launch_residual<FLUX, SECOND>(c, add_time, false, false, c->fixcount.p);
 }
 
 static Levels *build_levels(const std::vector<int> &IA, const std::vector<int> &JA, int n, bool forward,
@@ -1327,10 +1368,11 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         }
     }
     CFD_CUDA(c->roeflag.alloc(nnode));
-    CFD_CUDA(c->roecount.alloc(1));
+    CFD_CUDA(c->fixcount.alloc(2));
     CFD_CUDA(cudaMemsetAsync(c->roeflag.p, 0, sizeof(int) * nnode, s));
-    CFD_CUDA(cudaMemsetAsync(c->roecount.p, 0, sizeof(int), s));
+    CFD_CUDA(cudaMemsetAsync(c->fixcount.p, 0, 2 * sizeof(int), s));
     c->roe_fix_pending = false;
+    c->pc_fix_pending = false;
     {
         std::vector<int> ptr(nnode + 1, 0);
         for (int e = 0; e < nbedge; e++) ptr[bedge_nodes[2 * e] + 1]++;

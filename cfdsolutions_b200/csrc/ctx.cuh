@@ -152,10 +152,13 @@ struct cfd_ctx {
     cfd::DevBuf<int> inc_ptr, inc;    // per node: (patch-local edge << 1) | (node is R), increasing
     int npatch = 0, patch_nlocmax = 0;
     bool use_patch = false;
-    // Roe-average pressure positivity fix of the limiter (see cfd_limiter)
+    // limiter fixes decided by the residual (see cfd_limiter): per node bit 0 =
+    // Roe-average pressure fix, bit 1 = reconstructed-pressure correction;
+    // fixcount = [nodes failing the Roe check, nodes failing the pressure check]
     cfd::DevBuf<int> roeflag;         // [nnode]
-    cfd::DevBuf<int> roecount;        // [1]
+    cfd::DevBuf<int> fixcount;        // [2]
     bool roe_fix_pending = false;
+    bool pc_fix_pending = false;
 
     // state and residual
     cfd::DevBuf<double> Q;      // [5][ldq]

@@ -134,10 +134,24 @@ __global__ void __launch_bounds__(128) k_gg_grad(int nnode, int64_t ldq, const d
     }
 }
 
+// Reconstructed increment of node i towards neighbour j (Compute_SecondOrderReconstructQ,
+// MPFLOW3D/src/HigherOrderReconstructQ.cpp:56-60, without phi):
+// frac (Q_j - Q_i) + (1 - frac) grad_i . r.  KAPPA0 is the frac = 0 case (the
+// default LIMITER_ORDER): frac (Q_j - Q_i) is then a signed zero and
+// (1 - frac) g.r is g.r exactly, so the neighbour's state is not loaded and
+// every sum below rounds as in the general form (up to the sign of an exact zero).
+template <bool KAPPA0>
+__device__ __forceinline__ double recon_incr(double qj, double qi, double gr, double frac) {
+    return KAPPA0 ? gr : frac * (qj - qi) + (1.0 - frac) * gr;
+}
+
 // Venkatakrishnan limiter per node (Compute_Limiter_Venkatakrishnan,
-// Euler3D/src/Limiters.cpp:185-267), optional variable smoothing (:50-58) and
-// the reconstructed-pressure correction (Compute_Limiter_PressureCorrection,
-// :273-304).
+// Euler3D/src/Limiters.cpp:185-267), optional variable smoothing (:50-58) and,
+// when PC, the reconstructed-pressure correction (Compute_Limiter_PressureCorrection,
+// :273-304).  Without PC the correction is left to the residual, whose
+// gather kernel forms the same reconstructed states (k_residual_gather,
+// check_pc), or to k_venkat_pc.
+template <bool KAPPA0, bool PC>
 __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const double *__restrict__ Q,
                                                 const int64_t *__restrict__ sell_ptr, const int *__restrict__ sell_nbr,
                             const int *__restrict__ deg,
@@ -185,7 +199,8 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
             const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
 #pragma unroll
             for (int v = 0; v < 5; v++) {
-                const double q = qc[v] + frac * (Q[v * ldq + j] - qc[v]) + (1.0 - frac) * (gx[v] * rx + gy[v] * ry + gz[v] * rz);
+                const double qj = KAPPA0 ? 0.0 : Q[v * ldq + j];
+                const double q = qc[v] + recon_incr<KAPPA0>(qj, qc[v], gx[v] * rx + gy[v] * ry + gz[v] * rz, frac);
                 const double dm = q - qc[v];
                 if (dm != 0.0) {
                     const double dp = (dm > 0.0 ? qmax[v] : qmin[v]) - qc[v];
@@ -204,7 +219,8 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
             const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
 #pragma unroll
             for (int v = 0; v < 5; v++) {
-                const double q = qc[v] + frac * (Q[v * ldq + j] - qc[v]) + (1.0 - frac) * (gx[v] * rx + gy[v] * ry + gz[v] * rz);
+                const double qj = KAPPA0 ? 0.0 : Q[v * ldq + j];
+                const double q = qc[v] + recon_incr<KAPPA0>(qj, qc[v], gx[v] * rx + gy[v] * ry + gz[v] * rz, frac);
                 const double dm = q - qc[v];
                 double t = 1.0;
                 if (dm > 0.0) t = fmin(1.0, (qmax[v] - qc[v]) / dm);
@@ -221,28 +237,71 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
         for (int v = 0; v < 5; v++) ph[v] = m;
     }
     // pressure correction: any negative reconstructed pressure -> first order
+    if (PC) {
+        bool neg = false;
+        for (int k = 0; k < dgi; k++) {
+            int j = sell_nbr[sb + 32 * k];
+            j = j >= 0 ? j : ~j;
+            const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
+            double q[5];
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                const double qj = KAPPA0 ? 0.0 : Q[v * ldq + j];
+                q[v] = qc[v] + ph[v] * recon_incr<KAPPA0>(qj, qc[v], gx[v] * rx + gy[v] * ry + gz[v] * rz, frac);
+            }
+            if (recon_pressure_negative(q, f)) neg = true;
+        }
+        if (neg) {
+#pragma unroll
+            for (int v = 0; v < 5; v++) ph[v] = 0.0;
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = ph[v];
+}
+
+// The reconstructed-pressure correction alone (Compute_Limiter_PressureCorrection,
+// Euler3D/src/Limiters.cpp:273-304), in place: node i reads only its own
+// limiters.  Resolves a correction that k_venkat<.., false> left to the residual
+// when the limiters are needed before (or without) a gather residual.
+template <bool KAPPA0>
+__global__ void __launch_bounds__(128) k_venkat_pc(int nnode, int64_t ldq, const double *__restrict__ Q,
+                                                   const int64_t *__restrict__ sell_ptr,
+                                                   const int *__restrict__ sell_nbr, const int *__restrict__ deg,
+                                                   const double *__restrict__ xyz, const double *__restrict__ g,
+                                                   Flow f, double *__restrict__ phi) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nnode) return;
+    const int64_t sb = sell_ptr[i >> 5] + (i & 31);
+    const int dgi = deg[i];
+    const double frac = f.frac;
+    double qc[5], ph[5], gx[5], gy[5], gz[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        qc[v] = Q[v * ldq + i];
+        ph[v] = phi[v * (int64_t)nnode + i];
+        gx[v] = g[(3 * v) * (int64_t)nnode + i];
+        gy[v] = g[(3 * v + 1) * (int64_t)nnode + i];
+        gz[v] = g[(3 * v + 2) * (int64_t)nnode + i];
+    }
+    const double xi = xyz[i], yi = xyz[nnode + i], zi = xyz[2 * nnode + i];
     bool neg = false;
-    for (int k = 0; k < dgi; k++) {
+    for (int k = 0; k < dgi && !neg; k++) {
         int j = sell_nbr[sb + 32 * k];
         j = j >= 0 ? j : ~j;
         const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
         double q[5];
 #pragma unroll
-        for (int v = 0; v < 5; v++)
-            q[v] = qc[v] + ph[v] * (frac * (Q[v * ldq + j] - qc[v]) + (1.0 - frac) * (gx[v] * rx + gy[v] * ry + gz[v] * rz));
-        // p < 0 of (Limiters.cpp:296-301) without the division when rho > 0 (p + pinf < 0
-        // for the stiffened gas)
-        const double m2 = q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
-        const bool pneg = q[0] > 0.0 ? (2.0 * q[0] * (q[4] - f.pinf) < m2)
-                                     : (f.gm1 * ((q[4] - f.pinf) - (0.5 / q[0]) * m2) < 0.0);
-        if (pneg) neg = true;
+        for (int v = 0; v < 5; v++) {
+            const double qj = KAPPA0 ? 0.0 : Q[v * ldq + j];
+            q[v] = qc[v] + ph[v] * recon_incr<KAPPA0>(qj, qc[v], gx[v] * rx + gy[v] * ry + gz[v] * rz, frac);
+        }
+        neg = recon_pressure_negative(q, f);
     }
     if (neg) {
 #pragma unroll
-        for (int v = 0; v < 5; v++) ph[v] = 0.0;
+        for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = 0.0;
     }
-#pragma unroll
-    for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = ph[v];
 }
 
 // Roe-average pressure correction (Compute_Limiter_RoePressureCorrection,
@@ -256,7 +315,11 @@ __global__ void __launch_bounds__(128) k_roe_pressure_fix(int nnode, int64_t ldq
                             const int *__restrict__ deg,
                                                           const double *__restrict__ xyz,
                                                           const double *__restrict__ g, Flow f,
+                                                          const int *__restrict__ gate,
                                                           const double *__restrict__ phi_in, double *__restrict__ phi) {
+    // gate: the residual's fix counters; this full pass is needed only when the
+    // reconstructed-pressure correction changed some limiter (gate[1] > 0)
+    if (gate && gate[1] == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnode) return;
     const int64_t sb = sell_ptr[i >> 5] + (i & 31);
@@ -298,6 +361,13 @@ __global__ void __launch_bounds__(128) k_roe_pressure_fix(int nnode, int64_t ldq
     }
 #pragma unroll
     for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = neg ? 0.0 : phi_in[v * (int64_t)nnode + i];
+}
+
+template <bool KAPPA0, bool PC>
+static void launch_venkat(cfd_ctx *c) {
+    k_venkat<KAPPA0, PC><<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(
+        c->nnode, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p, c->deg.p, c->xyz.p, c->grad.p, c->cvol.p, c->flow,
+        c->phi.p, c->roeflag.p);
 }
 
 }  // namespace cfd
@@ -342,31 +412,58 @@ int cfd_limiter(cfd_ctx *c) {
         CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)5 * n)));
         return CFD_OK;
     }
-    k_venkat<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p, c->deg.p, c->xyz.p, c->grad.p,
-                                                        c->cvol.p, c->flow, c->phi.p, c->roeflag.p);
-    CFD_LAUNCH_CHECK();
-    if (is_roe_flux(c->params.flux_scheme)) {
-        // The Roe-average pressure fix (Limiters.cpp:61-110) needs the
-        // reconstructed face states the residual forms anyway: it is done by
-        // the next cfd_residual (or by roe_fix_standalone when the limiters
-        // are read back first).
-        CFD_CUDA(cudaMemsetAsync(c->roecount.p, 0, sizeof(int), c->stream));
-        c->roe_fix_pending = true;
+    // The reconstructed-pressure correction (Limiters.cpp:273-304) and, for
+    // the Roe fluxes, the Roe-average pressure fix (:61-110) test the face
+    // states the second-order residual forms anyway: both are left to the
+    // next cfd_residual (k_residual_gather flags the nodes that fail and a
+    // gated pass applies the fixes), or to limiter_fix_standalone when the
+    // limiters are read back or consumed by another kernel first.
+    const bool kappa0 = c->flow.frac == 0.0;
+    const bool defer_pc = !patch_kernel(c);
+    if (kappa0) {
+        if (defer_pc) launch_venkat<true, false>(c);
+        else launch_venkat<true, true>(c);
+    } else {
+        if (defer_pc) launch_venkat<false, false>(c);
+        else launch_venkat<false, true>(c);
     }
+    CFD_LAUNCH_CHECK();
+    c->pc_fix_pending = defer_pc;
+    c->roe_fix_pending = is_roe_flux(c->params.flux_scheme);
+    if (c->pc_fix_pending || c->roe_fix_pending)
+        CFD_CUDA(cudaMemsetAsync(c->fixcount.p, 0, 2 * sizeof(int), c->stream));
     return CFD_OK;
 }
 
 }  // extern "C"
 
 namespace cfd {
-int roe_fix_standalone(cfd_ctx *c) {
-    if (!c->roe_fix_pending) return CFD_OK;
+int launch_roe_pressure_fix(cfd_ctx *c, const int *gate) {
     const int n = c->nnode;
+    k_roe_pressure_fix<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p,
+                                                                  c->deg.p, c->xyz.p, c->grad.p, c->flow, gate,
+                                                                  c->work.p, c->phi.p);
+    CFD_LAUNCH_CHECK();
+    return CFD_OK;
+}
+
+int limiter_fix_standalone(cfd_ctx *c) {
+    const int n = c->nnode;
+    if (c->pc_fix_pending) {
+        if (c->flow.frac == 0.0)
+            k_venkat_pc<true><<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p,
+                                                                         c->deg.p, c->xyz.p, c->grad.p, c->flow, c->phi.p);
+        else
+            k_venkat_pc<false><<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p,
+                                                                          c->deg.p, c->xyz.p, c->grad.p, c->flow, c->phi.p);
+        CFD_LAUNCH_CHECK();
+        c->pc_fix_pending = false;
+    }
+    if (!c->roe_fix_pending) return CFD_OK;
     CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)5 * n)));
     CFD_CUDA(cudaMemcpyAsync(c->work.p, c->phi.p, sizeof(double) * 5 * n, cudaMemcpyDeviceToDevice, c->stream));
-    k_roe_pressure_fix<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p, c->deg.p, c->xyz.p,
-                                                                  c->grad.p, c->flow, c->work.p, c->phi.p);
-    CFD_LAUNCH_CHECK();
+    int st = launch_roe_pressure_fix(c, nullptr);
+    if (st) return st;
     c->roe_fix_pending = false;
     return CFD_OK;
 }
@@ -383,7 +480,7 @@ int cfd_get_gradients(cfd_ctx *c, double *g) {
 
 int cfd_get_limiters(cfd_ctx *c, double *phi) {
     if (!c || !phi || !c->phi.p) return CFD_ERR_STATE;
-    int st = roe_fix_standalone(c);
+    int st = limiter_fix_standalone(c);
     if (st) return st;
     CFD_CUDA(cudaMemcpyAsync(phi, c->phi.p, sizeof(double) * 5 * c->nnode, cudaMemcpyDeviceToHost, c->stream));
     CFD_CUDA(stream_wait(c->stream));

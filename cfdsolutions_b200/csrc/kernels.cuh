@@ -241,6 +241,14 @@ __device__ __forceinline__ double roe_avg_pressure(const double qa[5], const dou
     return (g - 1.0) * (e - 0.5 * rho * q2);
 }
 
+// Reconstructed-pressure test of Compute_Limiter_PressureCorrection
+// (Euler3D/src/Limiters.cpp:296-301): p < 0, without the division when rho > 0
+// (p + pinf < 0 for the stiffened gas).
+__device__ __forceinline__ bool recon_pressure_negative(const double q[5], const Flow &f) {
+    const double m2 = q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+    return q[0] > 0.0 ? (2.0 * q[0] * (q[4] - f.pinf) < m2) : (f.gm1 * ((q[4] - f.pinf) - (0.5 / q[0]) * m2) < 0.0);
+}
+
 __device__ __forceinline__ void store_low(float *p, double v) { *p = (float)v; }
 __device__ __forceinline__ void store_low(uint16_t *p, double v) {
     __nv_bfloat16 b = __double2bfloat16(v);
@@ -277,8 +285,14 @@ inline size_t patch_smem_bytes(int nlocmax, bool second) {
     return ((size_t)(second ? PATCH_NV2 : 5) * nlocmax + 11 * PATCH_CHUNK) * sizeof(double);
 }
 
-// The limiter's Roe-average pressure fix as its own pass over the node graph
-// (gradient.cu); used when the fused check in the residual cannot run.
-int roe_fix_standalone(cfd_ctx *c);
+// The limiter fixes left to the residual (reconstructed-pressure correction,
+// Roe-average pressure fix) as their own passes over the node graph
+// (gradient.cu); used when the limiters are needed before a gather residual.
+int limiter_fix_standalone(cfd_ctx *c);
+// k_roe_pressure_fix from c->work into c->phi; gate as in the kernel
+int launch_roe_pressure_fix(cfd_ctx *c, const int *gate);
+
+// The patch residual kernel is selected (it carries no reconstructed-pressure check).
+inline bool patch_kernel(const cfd_ctx *c) { return c->use_patch && c->params.residual_kernel == 1; }
 
 }  // namespace cfd

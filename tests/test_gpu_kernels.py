@@ -69,6 +69,73 @@ def test_residual_matches_restatement(gpu_available, cfg, numbering):
     assert relerr(g["deltat"], o["deltat"]) <= TOL
 
 
+def low_pressure_spots(Q, nnode, gamma, scale=0.02, seed=5, share=0.03):
+    """Q with the pressure of a seeded 3 % of the nodes scaled by `scale`
+    (momentum kept): the reconstructed pressure of those nodes' neighbours goes
+    negative, so the limiter's pressure correction fires."""
+    rng = np.random.default_rng(seed)
+    Q = Q.copy()
+    idx = rng.choice(nnode, size=max(1, int(share * nnode)), replace=False)
+    ke = 0.5 * (Q[1:4, idx] ** 2).sum(0) / Q[0, idx]
+    Q[4, idx] = scale * (Q[4, idx] - ke) + ke
+    return Q
+
+
+FIX_CASES = [(flux, lo, g) for flux in (1, 0) for lo in (0, 1) for g in (0, 1)]
+
+
+@pytest.mark.parametrize("flux,limiter_order,gradient", FIX_CASES,
+                         ids=[f"f{a}lo{b}g{c}" for a, b, c in FIX_CASES])
+@pytest.mark.parametrize("kernel", [0, 1])
+def test_limiter_pressure_correction_matches_restatement(gpu_available, flux, limiter_order, gradient, kernel):
+    """The reconstructed-pressure correction (Limiters.cpp:273-304), decided
+    inside the gather residual (kernel 0) or by its own pass before the patch
+    residual (kernel 1), zeroes the same limiters as the reference's per-node
+    sweep, and the residual is the one of the corrected limiters.  HLLC has no
+    Roe-average fix; for Roe the corrected limiters go through it again."""
+    cfg = dict(CFG1, order=1, gradient=gradient, limiter=1, limiter_order=limiter_order, flux_scheme=flux,
+               mach=0.8, mach_min=0.8, alpha_deg=1.25)
+    m = box_mesh(10, jitter=0.15, seed=3)
+    _, cfg, Q = make_case(mesh=m, cfg=cfg, seed=3, noise=0.02)
+    Q = low_pressure_spots(Q, m.nnode, cfg["gamma"])
+    o = restatement.residual_pass(m, cfg, Q)
+    assert (o["phi"] == 0).all(axis=0).sum() >= 5  # the correction fired
+    g = gpu_pass(m, cfg, Q, kernel=kernel)
+    np.testing.assert_array_equal(g["phi"] == 0, o["phi"] == 0)
+    assert np.abs(g["phi"] - o["phi"]).max() <= 1e-12
+    assert relerr_rows(g["conv"], o["conv"]) <= TOL
+    if np.abs(o["diss"]).max() > 0:
+        assert relerr_rows(g["diss"], o["diss"]) <= TOL
+
+
+@pytest.mark.parametrize("flux", [0, 1])
+def test_limiter_fixes_fused_equal_standalone(gpu_available, flux):
+    """The limiter fixes left to the residual give bit for bit the limiters and
+    residual of the standalone passes (limiters read back before the residual)."""
+    cfg = dict(CFG1, order=1, gradient=1, limiter=1, flux_scheme=flux, mach=0.8, mach_min=0.8, alpha_deg=1.25)
+    m = box_mesh(12, jitter=0.15, seed=9, rcm=2)
+    _, cfg, Q = make_case(mesh=m, cfg=cfg, seed=9, noise=0.02)
+    Q = low_pressure_spots(Q, m.nnode, cfg["gamma"], seed=9)
+    out = []
+    for read_first in (False, True):
+        with Euler3DGPU(m, params_from(cfg)) as s:
+            s.set_state(Q)
+            s.begin_iteration(0)
+            s.Apply_Boundary_Condition(0)
+            s.Compute_Gradient()
+            s.Compute_Limiter()
+            phi0 = s.get_limiters() if read_first else None
+            s.Compute_Residual(1)
+            conv, diss = s.get_residual()
+            phi = s.get_limiters()
+            if read_first:
+                np.testing.assert_array_equal(phi0, phi)
+            out.append((phi, conv, diss))
+    assert (out[0][0] == 0).all(axis=0).sum() >= 5
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a, b)
+
+
 @pytest.mark.parametrize("cfg", [CASES[0], CASES[3], CASES[4]], ids=["roe1", "roe2", "hllc2"])
 def test_patch_and_gather_kernels_agree_and_are_deterministic(gpu_available, cfg):
     m, cfg, Q = make_case(n=16, seed=5, rcm=2, cfg=cfg, noise=0.02)
