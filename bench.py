@@ -36,7 +36,9 @@ UNIT = "GEdges/s"
 CFG = dict(flux_scheme=0, order=1, limiter=1, limiter_order=0, gradient=1, venkat_k=5.0, gamma=1.4, mach=0.8,
            mach_min=0.8, alpha_deg=1.25, cfl_min=10.0, cfl_max=10.0)
 FLUX_NAMES = {0: "roe", 1: "hllc", 2: "ausm+"}
-KERNELS_PER_STEP = 8  # begin, bc, gradient, limiter, residual, pressure-fix apply, gated residual, dt
+# begin, bc, Green-Gauss + limiter, residual (interior + boundary edges), limiter-fix apply, gated Roe-fix
+# pass, gated residual (interior + boundary), dt
+KERNELS_PER_STEP = 10
 
 
 def parse():

@@ -118,13 +118,15 @@ __device__ __forceinline__ void reconstruct(const double qs[5], const double qo[
 // lanes contiguous): neighbour id (~id when the node is node_R) and the edge's
 // unit normal + area per slot, so the per-edge loads of a warp are coalesced;
 // the node's own state, gradients, limiters and coordinates stay in registers.
-template <int FLUX, bool SECOND>
+// KAPPA0: second order with frac = 0 (the default LIMITER_ORDER), where the
+// reconstruction frac (Q_o - Q_s) + (1 - frac) grad_s.r rounds to grad_s.r
+// exactly (up to the sign of an exact zero), so those terms are not formed.
+template <int FLUX, bool SECOND, bool KAPPA0 = false>
 __global__ void __launch_bounds__(128, 3) k_residual_gather(
     int nnode, int64_t ldq, const double *__restrict__ Q, const double *__restrict__ grad,
     const double *__restrict__ phi, const double *__restrict__ xyz, const int64_t *__restrict__ sell_ptr,
     const int *__restrict__ sell_nbr, const double4 *__restrict__ sell_geo, const int *__restrict__ deg,
-    const int *__restrict__ n2b_ptr, const int *__restrict__ n2b, const int2 *__restrict__ bn,
-    const double4 *__restrict__ bg, Flow f, int add_time, int checks, int *__restrict__ roeflag,
+    Flow f, int add_time, int checks, int *__restrict__ roeflag,
     int *__restrict__ fixcount, const int *__restrict__ gate, double *__restrict__ res, double *__restrict__ resd,
     double *__restrict__ dtsum, unsigned long long *__restrict__ ext) {
     if (gate && gate[0] == 0 && gate[1] == 0) return;
@@ -166,8 +168,13 @@ __global__ void __launch_bounds__(128, 3) k_residual_gather(
                                          grad[(3 * v + 1) * (int64_t)nnode + j] * ry +
                                          grad[(3 * v + 2) * (int64_t)nnode + j] * rz);
                     const double pn = limited ? phi[v * (int64_t)nnode + j] : 1.0;
-                    fo[v] = qo[v] + po[v] * (f.frac * (qn[v] - qo[v]) + (1.0 - f.frac) * gno);
-                    fn[v] = qn[v] + pn * (f.frac * (qo[v] - qn[v]) + (1.0 - f.frac) * gnn);
+                    if (KAPPA0) {
+                        fo[v] = qo[v] + po[v] * gno;
+                        fn[v] = qn[v] + pn * gnn;
+                    } else {
+                        fo[v] = qo[v] + po[v] * (f.frac * (qn[v] - qo[v]) + (1.0 - f.frac) * gno);
+                        fn[v] = qn[v] + pn * (f.frac * (qo[v] - qn[v]) + (1.0 - f.frac) * gnn);
+                    }
                 }
                 // the limiter's reconstructed-pressure correction (Limiters.cpp:273-304)
                 // tests exactly this node's own face states
@@ -200,7 +207,43 @@ __global__ void __launch_bounds__(128, 3) k_residual_gather(
             if (bad & 1) atomicAdd(&fixcount[0], 1);
             if (bad & 2) atomicAdd(&fixcount[1], 1);
         }
-        // boundary edges: first order, flux into node_L only (FluxTest.cpp:8044-8098)
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            res[v * (int64_t)nnode + i] = ac[v];
+            resd[v * (int64_t)nnode + i] = ad[v];
+        }
+        if (add_time) dtsum[i] = adt;
+    }
+    if (add_time) block_extrema3(mn, mx, ext);
+}
+
+// Boundary edges of the gather residual: first order, flux into node_L only
+// (FluxTest.cpp:8044-8098).  One thread per node that has boundary edges
+// (`bnode`, increasing), launched after k_residual_gather: it continues the
+// node's interior sums with its boundary edges in increasing order, the
+// order one loop over both would take, so every sum is the same bit for bit.
+// Kept out of the interior kernel because the ~5 % of nodes that carry
+// boundary edges sit in ~20 % of its warps, whose other lanes would idle
+// through them.
+template <int FLUX>
+__global__ void __launch_bounds__(128) k_residual_bnd(
+    int nbnode, const int *__restrict__ bnode, int nnode, int64_t ldq, const double *__restrict__ Q,
+    const int *__restrict__ n2b_ptr, const int *__restrict__ n2b, const int2 *__restrict__ bn,
+    const double4 *__restrict__ bg, Flow f, int add_time, const int *__restrict__ gate, double *__restrict__ res,
+    double *__restrict__ resd, double *__restrict__ dtsum, unsigned long long *__restrict__ ext) {
+    if (gate && gate[0] == 0 && gate[1] == 0) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
+    if (t < nbnode) {
+        const int i = bnode[t];
+        double qo[5], ac[5], ad[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            qo[v] = Q[v * ldq + i];
+            ac[v] = res[v * (int64_t)nnode + i];
+            ad[v] = resd[v * (int64_t)nnode + i];
+        }
+        double adt = add_time ? dtsum[i] : 0.0;
         for (int k = n2b_ptr[i]; k < n2b_ptr[i + 1]; k++) {
             const int b = n2b[k];
             const int2 nd = bn[b];
@@ -847,11 +890,18 @@ static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, bool check_
             c->flow, add_time, c->patch_nlocmax, check_roe ? 1 : 0, c->roeflag.p, c->fixcount.p, gate, c->res.p,
             c->resd.p, c->dt.p, c->ext.p);
     } else {
-        k_residual_gather<FLUX, SECOND><<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(
+        auto kern = SECOND && c->flow.frac == 0.0 ? k_residual_gather<FLUX, SECOND, SECOND>
+                                                  : k_residual_gather<FLUX, SECOND, false>;
+        kern<<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(
             c->nnode, c->ldq, c->Q.p, c->grad.p, c->phi.p, c->xyz.p, c->sell_ptr.p, c->sell_nbr.p, c->sell_geo.p,
-            c->deg.p, c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p, c->flow, add_time,
-            (check_roe ? 1 : 0) | (check_pc ? 2 : 0), c->roeflag.p, c->fixcount.p, gate, c->res.p, c->resd.p,
-            c->dt.p, c->ext.p);
+            c->deg.p, c->flow, add_time, (check_roe ? 1 : 0) | (check_pc ? 2 : 0), c->roeflag.p, c->fixcount.p, gate,
+            c->res.p, c->resd.p, c->dt.p, c->ext.p);
+        if (c->nbnode > 0) {
+            CFD_LAUNCH_CHECK();
+            k_residual_bnd<FLUX><<<grid_for(c->nbnode, 128), 128, 0, c->stream>>>(
+                c->nbnode, c->bnode.p, c->nnode, c->ldq, c->Q.p, c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p,
+                c->bedge_geo.p, c->flow, add_time, gate, c->res.p, c->resd.p, c->dt.p, c->ext.p);
+        }
     }
     CFD_LAUNCH_CHECK();
     return CFD_OK;
@@ -1095,6 +1145,7 @@ int cfd_set_stream(cfd_ctx *c, void *stream) {
 
 int cfd_set_params(cfd_ctx *c, const cfd_params *p) {
     if (!c || !p) { set_error("cfd_set_params: NULL"); return CFD_ERR_ARG; }
+    c->phi_next_valid = false;
     if (p->flux_scheme < CFD_FLUX_ROE || p->flux_scheme > CFD_FLUX_VANLEER) {
         set_error("cfd_set_params: invalid flux scheme %d", p->flux_scheme);
         return CFD_ERR_ARG;
@@ -1189,6 +1240,7 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
     c->has_mesh = false;
     c->has_system = false;
     c->has_grad = false;
+    c->phi_next_valid = false;
     c->lsq_weight = -1;
     c->nnode = nnode;
     c->nghost = nghost;
@@ -1381,6 +1433,12 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         for (int e = 0; e < nbedge; e++) lst[fill[bedge_nodes[2 * e]]++] = e;
         CFD_CUDA(c->n2b_ptr.upload(ptr.data(), ptr.size(), s));
         CFD_CUDA(c->n2b.upload(lst.data(), lst.size(), s));
+        std::vector<int> bnode;
+        for (int i = 0; i < nnode; i++)
+            if (ptr[i + 1] > ptr[i]) bnode.push_back(i);
+        c->nbnode = (int)bnode.size();
+        if (bnode.empty()) bnode.push_back(0);
+        CFD_CUDA(c->bnode.upload(bnode.data(), bnode.size(), s));
         CFD_CUDA(stream_wait(s));
     }
     // ---- block CRS pattern (Create_CRS_SolverBlockMatrix, Euler3D/src/Solver.cpp:612-672)
@@ -1457,6 +1515,7 @@ int cfd_get_block_pattern(cfd_ctx *c, int64_t *nnzb, int *IA, int *JA, int *IAU)
 int cfd_set_state(cfd_ctx *c, const double *Q) {
     NEED_MESH("cfd_set_state");
     if (!Q) return CFD_ERR_ARG;
+    c->phi_next_valid = false;
     const int64_t n = (int64_t)c->nnode + c->nghost;
     CFD_CUDA(cudaMemcpy2DAsync(c->Q.p, c->ldq * sizeof(double), Q, n * sizeof(double), n * sizeof(double), 5,
                                cudaMemcpyHostToDevice, c->stream));
@@ -1475,6 +1534,7 @@ int cfd_get_state(cfd_ctx *c, double *Q) {
 
 int cfd_state_device_ptr(cfd_ctx *c, double **dQ, int64_t *ld) {
     NEED_MESH("cfd_state_device_ptr");
+    c->phi_next_valid = false;  // the caller may write the state
     if (dQ) *dQ = c->Q.p;
     if (ld) *ld = c->ldq;
     return CFD_OK;
@@ -1482,6 +1542,7 @@ int cfd_state_device_ptr(cfd_ctx *c, double **dQ, int64_t *ld) {
 
 int cfd_set_freestream(cfd_ctx *c) {
     NEED_MESH("cfd_set_freestream");
+    c->phi_next_valid = false;
     compute_flow(c, 0);
     const int n = c->nnode + c->nghost;
     k_freestream<<<grid_for(n, 256), 256, 0, c->stream>>>(n, c->ldq, c->flow, c->Q.p);
@@ -1695,6 +1756,7 @@ int cfd_block_lusgs(cfd_ctx *c, int iterations, double *rms) {
 int cfd_update(cfd_ctx *c, double relax) {
     NEED_MESH("cfd_update");
     if (!c->X.p) { set_error("cfd_update: no solution vector"); return CFD_ERR_STATE; }
+    c->phi_next_valid = false;
     k_update<<<grid_for(c->nnode, 256), 256, 0, c->stream>>>(c->nnode, c->ldq, relax, c->X.p, c->Q.p);
     CFD_LAUNCH_CHECK();
     return CFD_OK;

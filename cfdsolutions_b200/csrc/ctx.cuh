@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <thread>
+#include <utility>
 #include <vector>
 
 #include "cfd_internal.h"
@@ -59,6 +60,10 @@ struct DevBuf {
         if (e == cudaSuccess) n = count;
         else p = nullptr;
         return e;
+    }
+    void swap(DevBuf &o) {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
     }
     cudaError_t upload(const T *h, size_t count, cudaStream_t s) {
         cudaError_t e = alloc(count);
@@ -133,6 +138,8 @@ struct cfd_ctx {
     cfd::DevBuf<int> n2n_ia, n2n_ja;  // physical node graph (no diagonal)
     cfd::DevBuf<int> n2e_ptr, n2e;    // incident interior edges, ~e when the node is node_R
     cfd::DevBuf<int> n2b_ptr, n2b;    // incident boundary edges
+    cfd::DevBuf<int> bnode;           // nodes with boundary edges, increasing
+    int nbnode = 0;
     // block CRS (Create_CRS_SolverBlockMatrix layout)
     std::vector<int> h_IA, h_JA, h_IAU;
     cfd::DevBuf<int> IA, JA, IAU, tslot;  // tslot[k] = slot of (JA[k], row)
@@ -159,6 +166,12 @@ struct cfd_ctx {
     cfd::DevBuf<int> fixcount;        // [2]
     bool roe_fix_pending = false;
     bool pc_fix_pending = false;
+    // limiters formed by cfd_gradient's fused Green-Gauss + limiter pass for
+    // the next cfd_limiter; cleared by anything that changes the state or the
+    // parameters in between
+    cfd::DevBuf<double> phi_next;     // [5][nnode]
+    bool phi_next_valid = false;
+    bool phi_next_defers_pc = false;
 
     // state and residual
     cfd::DevBuf<double> Q;      // [5][ldq]

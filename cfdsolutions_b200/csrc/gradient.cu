@@ -145,47 +145,22 @@ __device__ __forceinline__ double recon_incr(double qj, double qi, double gr, do
     return KAPPA0 ? gr : frac * (qj - qi) + (1.0 - frac) * gr;
 }
 
-// Venkatakrishnan limiter per node (Compute_Limiter_Venkatakrishnan,
-// Euler3D/src/Limiters.cpp:185-267), optional variable smoothing (:50-58) and,
-// when PC, the reconstructed-pressure correction (Compute_Limiter_PressureCorrection,
-// :273-304).  Without PC the correction is left to the residual, whose
-// gather kernel forms the same reconstructed states (k_residual_gather,
-// check_pc), or to k_venkat_pc.
+// Limiter of node i from its state qc, gradient (gx, gy, gz) and the extremes
+// of its neighbours' states, as differences dmax = max_j Q_j - qc >= 0 and
+// dmin = min_j Q_j - qc <= 0: Venkatakrishnan (Compute_Limiter_Venkatakrishnan,
+// Euler3D/src/Limiters.cpp:185-267) or Barth-Jespersen (:117-178), the
+// optional variable smoothing (:50-58) and, when PC, the reconstructed-
+// pressure correction (Compute_Limiter_PressureCorrection, :273-304).
 template <bool KAPPA0, bool PC>
-__global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const double *__restrict__ Q,
-                                                const int64_t *__restrict__ sell_ptr, const int *__restrict__ sell_nbr,
-                            const int *__restrict__ deg,
-                                                const double *__restrict__ xyz, const double *__restrict__ g,
-                                                const double *__restrict__ vol, Flow f, double *__restrict__ phi,
-                                                int *__restrict__ roeflag) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nnode) return;
-    const int64_t sb = sell_ptr[i >> 5] + (i & 31);
-    const int dgi = deg[i];
-    roeflag[i] = 0;
+__device__ __forceinline__ void limit_node(int i, int nnode, int64_t ldq, const double *__restrict__ Q, int64_t sb,
+                                           int dgi, const int *__restrict__ sell_nbr, const double *__restrict__ xyz,
+                                           const Flow &f, const double qc[5], const double dmin[5],
+                                           const double dmax[5], const double gx[5], const double gy[5],
+                                           const double gz[5], double eps2, double ph[5]) {
     const double frac = f.frac;
-    double qc[5], qmin[5], qmax[5], ph[5], gx[5], gy[5], gz[5];
-#pragma unroll
-    for (int v = 0; v < 5; v++) {
-        qc[v] = Q[v * ldq + i];
-        qmin[v] = qmax[v] = qc[v];
-        ph[v] = 1.0;
-        gx[v] = g[(3 * v) * (int64_t)nnode + i];
-        gy[v] = g[(3 * v + 1) * (int64_t)nnode + i];
-        gz[v] = g[(3 * v + 2) * (int64_t)nnode + i];
-    }
-    const double eps2 = 6.0 * f.venkat_eps_k3 * vol[i] / M_PI;
-    for (int k = 0; k < dgi; k++) {
-        int j = sell_nbr[sb + 32 * k];
-        j = j >= 0 ? j : ~j;
-#pragma unroll
-        for (int v = 0; v < 5; v++) {
-            const double q = Q[v * ldq + j];
-            qmin[v] = fmin(qmin[v], q);
-            qmax[v] = fmax(qmax[v], q);
-        }
-    }
     const double xi = xyz[i], yi = xyz[nnode + i], zi = xyz[2 * nnode + i];
+#pragma unroll
+    for (int v = 0; v < 5; v++) ph[v] = 1.0;
     if (f.limiter == CFD_LIMITER_VENKAT) {
         // phi = min(1, min_edges num/den) with num, den >= 0 (dm and dp share
         // their sign).  The running minimum is kept as a fraction and compared
@@ -203,7 +178,7 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
                 const double q = qc[v] + recon_incr<KAPPA0>(qj, qc[v], gx[v] * rx + gy[v] * ry + gz[v] * rz, frac);
                 const double dm = q - qc[v];
                 if (dm != 0.0) {
-                    const double dp = (dm > 0.0 ? qmax[v] : qmin[v]) - qc[v];
+                    const double dp = dm > 0.0 ? dmax[v] : dmin[v];
                     const double num = (dp * dp + eps2) + 2.0 * (dm * dp);
                     const double den = dp * dp + 2.0 * dm * dm + dm * dp + eps2;
                     if (num * bd[v] < bn[v] * den) { bn[v] = num; bd[v] = den; }
@@ -212,7 +187,7 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
         }
 #pragma unroll
         for (int v = 0; v < 5; v++) ph[v] = fmax(0.0, bn[v] == bd[v] ? 1.0 : bn[v] / bd[v]);
-    } else {  // Barth-Jespersen (Compute_Limiter_Barth_Jespersen, Limiters.cpp:117-178)
+    } else {  // Barth-Jespersen
         for (int k = 0; k < dgi; k++) {
             int j = sell_nbr[sb + 32 * k];
             j = j >= 0 ? j : ~j;
@@ -223,8 +198,8 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
                 const double q = qc[v] + recon_incr<KAPPA0>(qj, qc[v], gx[v] * rx + gy[v] * ry + gz[v] * rz, frac);
                 const double dm = q - qc[v];
                 double t = 1.0;
-                if (dm > 0.0) t = fmin(1.0, (qmax[v] - qc[v]) / dm);
-                else if (dm < 0.0) t = fmin(1.0, (qmin[v] - qc[v]) / dm);
+                if (dm > 0.0) t = fmin(1.0, dmax[v] / dm);
+                else if (dm < 0.0) t = fmin(1.0, dmin[v] / dm);
                 ph[v] = fmax(0.0, fmin(ph[v], t));
             }
         }
@@ -256,6 +231,105 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
             for (int v = 0; v < 5; v++) ph[v] = 0.0;
         }
     }
+}
+
+// Limiter pass over stored gradients (any gradient method).  Without PC the
+// pressure correction is left to the residual, whose gather kernel forms the
+// same reconstructed states (k_residual_gather, check bit 1), or to k_venkat_pc.
+template <bool KAPPA0, bool PC>
+__global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const double *__restrict__ Q,
+                                                const int64_t *__restrict__ sell_ptr, const int *__restrict__ sell_nbr,
+                                                const int *__restrict__ deg, const double *__restrict__ xyz,
+                                                const double *__restrict__ g, const double *__restrict__ vol, Flow f,
+                                                double *__restrict__ phi, int *__restrict__ roeflag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nnode) return;
+    const int64_t sb = sell_ptr[i >> 5] + (i & 31);
+    const int dgi = deg[i];
+    roeflag[i] = 0;
+    double qc[5], qmin[5], qmax[5], ph[5], gx[5], gy[5], gz[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        qc[v] = Q[v * ldq + i];
+        qmin[v] = qmax[v] = qc[v];
+        gx[v] = g[(3 * v) * (int64_t)nnode + i];
+        gy[v] = g[(3 * v + 1) * (int64_t)nnode + i];
+        gz[v] = g[(3 * v + 2) * (int64_t)nnode + i];
+    }
+    const double eps2 = 6.0 * f.venkat_eps_k3 * vol[i] / M_PI;
+    for (int k = 0; k < dgi; k++) {
+        int j = sell_nbr[sb + 32 * k];
+        j = j >= 0 ? j : ~j;
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            const double q = Q[v * ldq + j];
+            qmin[v] = fmin(qmin[v], q);
+            qmax[v] = fmax(qmax[v], q);
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        qmin[v] -= qc[v];
+        qmax[v] -= qc[v];
+    }
+    limit_node<KAPPA0, PC>(i, nnode, ldq, Q, sb, dgi, sell_nbr, xyz, f, qc, qmin, qmax, gx, gy, gz, eps2, ph);
+#pragma unroll
+    for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = ph[v];
+}
+
+// Green-Gauss gradient and limiter in one pass over the node graph: the
+// gradient loop of k_gg_grad (same sums, same order, so the same gradients
+// bit for bit) also takes the neighbours' extremes, and the limiter then
+// reads the gradient from registers.  Saves the limiter's own neighbour pass
+// and its re-read of the 15 gradient components.
+template <bool KAPPA0, bool PC>
+__global__ void __launch_bounds__(128) k_gg_limiter(int nnode, int64_t ldq, const double *__restrict__ Q,
+                                                    const int64_t *__restrict__ sell_ptr,
+                                                    const int *__restrict__ sell_nbr, const int *__restrict__ deg,
+                                                    const double4 *__restrict__ sell_geo,
+                                                    const double *__restrict__ xyz, const double *__restrict__ vol,
+                                                    Flow f, double *__restrict__ g, double *__restrict__ phi,
+                                                    int *__restrict__ roeflag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nnode) return;
+    const int64_t sb = sell_ptr[i >> 5] + (i & 31);
+    const int dgi = deg[i];
+    roeflag[i] = 0;
+    double qi[5], qmin[5], qmax[5], gx[5] = {0, 0, 0, 0, 0}, gy[5] = {0, 0, 0, 0, 0}, gz[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+    for (int v = 0; v < 5; v++) qmin[v] = qmax[v] = qi[v] = Q[v * ldq + i];
+    for (int k = 0; k < dgi; k++) {
+        const int sn = sell_nbr[sb + 32 * k];
+        const int j = sn >= 0 ? sn : ~sn;
+        const double4 S = sell_geo[sb + 32 * k];
+        const double sg = sn >= 0 ? 0.5 * S.w : -0.5 * S.w;
+        const double sx = sg * S.x, sy = sg * S.y, sz = sg * S.z;
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            const double qj = Q[v * ldq + j];
+            const double d = qj - qi[v];
+            gx[v] += d * sx;
+            gy[v] += d * sy;
+            gz[v] += d * sz;
+            qmin[v] = fmin(qmin[v], qj);
+            qmax[v] = fmax(qmax[v], qj);
+        }
+    }
+    const double vinv = 1.0 / vol[i];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        gx[v] *= vinv;
+        gy[v] *= vinv;
+        gz[v] *= vinv;
+        g[(3 * v) * (int64_t)nnode + i] = gx[v];
+        g[(3 * v + 1) * (int64_t)nnode + i] = gy[v];
+        g[(3 * v + 2) * (int64_t)nnode + i] = gz[v];
+        qmin[v] -= qi[v];
+        qmax[v] -= qi[v];
+    }
+    const double eps2 = 6.0 * f.venkat_eps_k3 * vol[i] / M_PI;
+    double ph[5];
+    limit_node<KAPPA0, PC>(i, nnode, ldq, Q, sb, dgi, sell_nbr, xyz, f, qi, qmin, qmax, gx, gy, gz, eps2, ph);
 #pragma unroll
     for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = ph[v];
 }
@@ -370,6 +444,17 @@ static void launch_venkat(cfd_ctx *c) {
         c->phi.p, c->roeflag.p);
 }
 
+template <bool KAPPA0, bool PC>
+static void launch_gg_limiter(cfd_ctx *c) {
+    k_gg_limiter<KAPPA0, PC><<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(
+        c->nnode, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p, c->deg.p, c->sell_geo.p, c->xyz.p, c->cvol.p, c->flow,
+        c->grad.p, c->phi_next.p, c->roeflag.p);
+}
+
+// Whether the next limiter leaves its reconstructed-pressure correction to
+// the residual: only the gather residual kernel carries that check.
+static bool limiter_defers_pc(const cfd_ctx *c) { return !patch_kernel(c); }
+
 }  // namespace cfd
 
 using namespace cfd;
@@ -381,7 +466,25 @@ int cfd_gradient(cfd_ctx *c) {
     CFD_CUDA(cudaSetDevice(c->device));
     const int n = c->nnode;
     CFD_CUDA(c->grad.alloc((size_t)15 * n));
-    if (c->params.gradient == CFD_GRAD_GG) {
+    c->phi_next_valid = false;
+    const bool with_limiter = c->params.order == CFD_ORDER_SECOND && c->params.limiter != CFD_LIMITER_NONE;
+    if (c->params.gradient == CFD_GRAD_GG && with_limiter) {
+        // second order with a limiter: the limiter of this state is formed in
+        // the same pass and taken by the next cfd_limiter unless the state or
+        // the parameters change before it (phi_next_valid)
+        CFD_CUDA(c->phi_next.alloc((size_t)5 * n));
+        const bool kappa0 = c->flow.frac == 0.0, defer = limiter_defers_pc(c);
+        if (kappa0) {
+            if (defer) launch_gg_limiter<true, false>(c);
+            else launch_gg_limiter<true, true>(c);
+        } else {
+            if (defer) launch_gg_limiter<false, false>(c);
+            else launch_gg_limiter<false, true>(c);
+        }
+        CFD_LAUNCH_CHECK();
+        c->phi_next_valid = true;
+        c->phi_next_defers_pc = defer;
+    } else if (c->params.gradient == CFD_GRAD_GG) {
         k_gg_grad<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p, c->deg.p,
                                                              c->sell_geo.p, c->cvol.p, c->grad.p);
     } else {
@@ -418,16 +521,24 @@ int cfd_limiter(cfd_ctx *c) {
     // next cfd_residual (k_residual_gather flags the nodes that fail and a
     // gated pass applies the fixes), or to limiter_fix_standalone when the
     // limiters are read back or consumed by another kernel first.
-    const bool kappa0 = c->flow.frac == 0.0;
-    const bool defer_pc = !patch_kernel(c);
-    if (kappa0) {
-        if (defer_pc) launch_venkat<true, false>(c);
-        else launch_venkat<true, true>(c);
+    bool defer_pc;
+    if (c->phi_next_valid) {
+        // formed by cfd_gradient together with the gradient of this state
+        c->phi.swap(c->phi_next);
+        c->phi_next_valid = false;
+        defer_pc = c->phi_next_defers_pc;
     } else {
-        if (defer_pc) launch_venkat<false, false>(c);
-        else launch_venkat<false, true>(c);
+        const bool kappa0 = c->flow.frac == 0.0;
+        defer_pc = limiter_defers_pc(c);
+        if (kappa0) {
+            if (defer_pc) launch_venkat<true, false>(c);
+            else launch_venkat<true, true>(c);
+        } else {
+            if (defer_pc) launch_venkat<false, false>(c);
+            else launch_venkat<false, true>(c);
+        }
+        CFD_LAUNCH_CHECK();
     }
-    CFD_LAUNCH_CHECK();
     c->pc_fix_pending = defer_pc;
     c->roe_fix_pending = is_roe_flux(c->params.flux_scheme);
     if (c->pc_fix_pending || c->roe_fix_pending)

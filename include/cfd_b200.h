@@ -192,7 +192,8 @@ int  cfd_get_block_pattern(cfd_ctx *ctx, int64_t *nnzb, int *IA, int *JA, int *I
 int  cfd_set_state(cfd_ctx *ctx, const double *Q);
 int  cfd_get_state(cfd_ctx *ctx, double *Q);
 /* Device pointer of the resident state (SoA, leading dimension *ld >=
- * nnode+nghost) for zero-copy callers. */
+ * nnode+nghost) for zero-copy callers.  A state written through it after
+ * cfd_gradient needs cfd_gradient again before cfd_limiter. */
 int  cfd_state_device_ptr(cfd_ctx *ctx, double **dQ, int64_t *ld);
 /* Freestream state per node (Solver_Set_Initial_Conditions,
  * Euler3D/src/Solver.cpp:339-393) on the device. */
@@ -209,9 +210,14 @@ int  cfd_begin_iteration(cfd_ctx *ctx, int iteration);
  * Euler3D/src/BC.cpp:1440-1487, 381-677). */
 int  cfd_apply_bc(cfd_ctx *ctx, int iteration);
 /* Node gradients of Q1..Q5 (Compute_Least_Square_Gradient,
- * Euler3D/src/Gradient.cpp:232-296, or Green-Gauss). */
+ * Euler3D/src/Gradient.cpp:232-296, or Green-Gauss).  With Green-Gauss,
+ * second order and a limiter, the limiters of the same state are formed in
+ * the same pass and taken by the next cfd_limiter. */
 int  cfd_gradient(cfd_ctx *ctx);
-/* Limiter (Compute_Limiter, Euler3D/src/Limiters.cpp:20-111). */
+/* Limiter (Compute_Limiter, Euler3D/src/Limiters.cpp:20-111) of the state
+ * and gradients of the last cfd_gradient.  Its pressure fixes (:61-110,
+ * :273-304) are completed by the next second-order cfd_residual, or by
+ * cfd_get_limiters. */
 int  cfd_limiter(cfd_ctx *ctx);
 /* Flux residual (Compute_Residual, Euler3D/src/Residual.cpp:18 ->
  * FluxTest.cpp:7968 Roe / HLLC_Fluxes.cpp:519 HLLC / AUSM+).  Writes the

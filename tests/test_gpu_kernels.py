@@ -44,6 +44,9 @@ CASES = [
     dict(CFG1, order=1, gradient=1, limiter=1, flux_scheme=1, mach=0.8, mach_min=0.8, alpha_deg=1.25),
     dict(CFG1, order=1, gradient=1, limiter=1, flux_scheme=2, mach=0.8, mach_min=0.8, alpha_deg=1.25),
     dict(CFG1, order=1, gradient=0, limiter=0, limiter_order=1, mach=0.8, mach_min=0.8, alpha_deg=1.25),
+    dict(CFG1, order=1, gradient=1, limiter=0, limiter_smooth=1, mach=0.8, mach_min=0.8, alpha_deg=1.25),
+    dict(CFG1, order=1, gradient=1, limiter=1, limiter_order=1, limiter_smooth=1, flux_scheme=1, mach=0.8,
+         mach_min=0.8, alpha_deg=1.25),
     dict(CFG1, order=1, gradient=1, limiter=-1, entropy_fix=1),
     dict(CFG1, flux_scheme=6),
     dict(CFG1, order=1, gradient=0, limiter=1, flux_scheme=6, mach=0.8, mach_min=0.8, alpha_deg=1.25),
@@ -51,7 +54,8 @@ CASES = [
 
 
 @pytest.mark.parametrize("cfg", CASES, ids=lambda c: f"f{c['flux_scheme']}o{c['order']}g{c.get('gradient', 0)}"
-                                                     f"l{c.get('limiter', -1)}e{c.get('entropy_fix', 0)}")
+                                                     f"l{c.get('limiter', -1)}e{c.get('entropy_fix', 0)}"
+                                                     f"k{c.get('limiter_order', 0)}s{c.get('limiter_smooth', 0)}")
 @pytest.mark.parametrize("numbering", [0, 2])
 def test_residual_matches_restatement(gpu_available, cfg, numbering):
     m, cfg, Q = make_case(n=12, seed=17, rcm=numbering, cfg=cfg, noise=0.02)
@@ -134,6 +138,32 @@ def test_limiter_fixes_fused_equal_standalone(gpu_available, flux):
     assert (out[0][0] == 0).all(axis=0).sum() >= 5
     for a, b in zip(out[0], out[1]):
         np.testing.assert_array_equal(a, b)
+
+
+def test_limiter_follows_state_changed_after_gradient(gpu_available):
+    """cfd_gradient forms the limiters of its state in the same pass (Green-
+    Gauss); a state set between it and cfd_limiter is the one limited, as with
+    the separate limiter pass (gradients of the earlier state)."""
+    cfg = dict(CASES[3])
+    m, cfg, Q = make_case(n=10, seed=21, cfg=cfg, noise=0.02)
+    _, _, Q2 = make_case(mesh=m, cfg=cfg, seed=22, noise=0.02)
+    with Euler3DGPU(m, params_from(cfg)) as s:
+        s.set_state(Q)
+        s.begin_iteration(0)
+        s.Apply_Boundary_Condition(0)
+        s.Compute_Gradient()
+        s.set_state(Q2)
+        s.Compute_Limiter()
+        phi_changed = s.get_limiters()
+        s.set_state(Q)
+        s.Compute_Gradient()
+        s.Compute_Limiter()
+        phi_fused = s.get_limiters()
+        grad = s.get_gradients()
+    o = restatement.residual_pass(m, cfg, Q)
+    assert np.abs(phi_fused - o["phi"]).max() <= 1e-12
+    assert relerr_rows(grad, o["grad"]) <= TOL
+    assert np.abs(phi_changed - phi_fused).max() > 1e-3  # Q2 was limited, not Q
 
 
 @pytest.mark.parametrize("cfg", [CASES[0], CASES[3], CASES[4]], ids=["roe1", "roe2", "hllc2"])
