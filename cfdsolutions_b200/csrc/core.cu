@@ -121,18 +121,18 @@ __device__ __forceinline__ void reconstruct(const double qs[5], const double qo[
 // KAPPA0: second order with frac = 0 (the default LIMITER_ORDER), where the
 // reconstruction frac (Q_o - Q_s) + (1 - frac) grad_s.r rounds to grad_s.r
 // exactly (up to the sign of an exact zero), so those terms are not formed.
-template <int FLUX, bool SECOND, bool KAPPA0 = false>
-__global__ void __launch_bounds__(128, 3) k_residual_gather(
-    int nnode, int64_t ldq, const double *__restrict__ Q, const double *__restrict__ grad,
-    const double *__restrict__ phi, const double *__restrict__ xyz, const int64_t *__restrict__ sell_ptr,
-    const int *__restrict__ sell_nbr, const double4 *__restrict__ sell_geo, const int *__restrict__ deg,
-    Flow f, int add_time, int checks, int *__restrict__ roeflag,
-    int *__restrict__ fixcount, const int *__restrict__ gate, double *__restrict__ res, double *__restrict__ resd,
-    double *__restrict__ dtsum, unsigned long long *__restrict__ ext) {
-    if (gate && gate[0] == 0 && gate[1] == 0) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
-    if (i < nnode) {
+#define GATHER_PARAMS                                                                                        \
+    int nnode, int64_t ldq, const double *__restrict__ Q, const double *__restrict__ grad,                    \
+        const double *__restrict__ phi, const double *__restrict__ xyz, const int64_t *__restrict__ sell_ptr, \
+        const int *__restrict__ sell_nbr, const double4 *__restrict__ sell_geo, const int *__restrict__ deg,   \
+        Flow f, int add_time, int checks, int *__restrict__ roeflag, int *__restrict__ fixcount,                 \
+        double *__restrict__ res, double *__restrict__ resd, double *__restrict__ dtsum
+#define GATHER_ARGS \
+    nnode, ldq, Q, grad, phi, xyz, sell_ptr, sell_nbr, sell_geo, deg, f, add_time, checks, roeflag, fixcount, res, resd, dtsum
+
+template <int FLUX, bool SECOND, bool KAPPA0>
+__device__ __forceinline__ void residual_gather_node(int i, GATHER_PARAMS, double mn[3], double mx[3]) {
+    {
         const bool limited = f.limiter != CFD_LIMITER_NONE;
         double qo[5], go[15], po[5], xo[3];
 #pragma unroll
@@ -149,8 +149,12 @@ __global__ void __launch_bounds__(128, 3) k_residual_gather(
         int bad = 0;  // bit 0: Roe-average pressure < 0, bit 1: own reconstructed pressure < 0
         const int64_t base = sell_ptr[i >> 5] + (i & 31);
         const int d = deg[i];
+        // the next slot's neighbour id is loaded one edge ahead, so the
+        // neighbour gathers of an edge do not wait for their index load
+        int sn_next = d > 0 ? sell_nbr[base] : 0;
         for (int k = 0; k < d; k++) {
-            const int sn = sell_nbr[base + 32 * k];
+            const int sn = sn_next;
+            if (k + 1 < d) sn_next = sell_nbr[base + 32 * (k + 1)];
             const double4 g = sell_geo[base + 32 * k];
             const bool own_is_L = sn >= 0;
             const int j = own_is_L ? sn : ~sn;
@@ -189,9 +193,12 @@ __global__ void __launch_bounds__(128, 3) k_residual_gather(
                 qL[v] = own_is_L ? fo[v] : fn[v];
                 qR[v] = own_is_L ? fn[v] : fo[v];
             }
-            if (SECOND && (checks & 1) && roe_avg_pressure(qL, qR, f.gamma, f.gpinf) < 0.0) bad |= 1;
-            double cf[5], df[5], lam[3];
-            const double lmax = edge_flux<FLUX>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam);
+            if (SECOND && !roe_c2_of<FLUX>() && (checks & 1) && roe_avg_pressure(qL, qR, f.gamma, f.gpinf) < 0.0)
+                bad |= 1;
+            double cf[5], df[5], lam[3], c2 = 1.0;
+            const double lmax = edge_flux<FLUX>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam,
+                                                SECOND && roe_c2_of<FLUX>() ? &c2 : nullptr);
+            if (SECOND && roe_c2_of<FLUX>() && (checks & 1) && c2 < 0.0) bad |= 1;
             const double sg = own_is_L ? 1.0 : -1.0;
 #pragma unroll
             for (int v = 0; v < 5; v++) {
@@ -213,6 +220,28 @@ __global__ void __launch_bounds__(128, 3) k_residual_gather(
             resd[v * (int64_t)nnode + i] = ad[v];
         }
         if (add_time) dtsum[i] = adt;
+    }
+}
+
+template <int FLUX, bool SECOND, bool KAPPA0 = false>
+__global__ void __launch_bounds__(128, 3) k_residual_gather(GATHER_PARAMS, unsigned long long *__restrict__ ext) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
+    if (i < nnode) residual_gather_node<FLUX, SECOND, KAPPA0>(i, GATHER_ARGS, mn, mx);
+    if (add_time) block_extrema3(mn, mx, ext);
+}
+
+// The gated re-evaluation after a limiter fix (gate = the fix counters): a
+// grid of a few CTAs per SM strides over the nodes, so that the usual case,
+// no node failed, costs one short wave instead of the full grid's.
+template <int FLUX, bool SECOND, bool KAPPA0 = false>
+__global__ void __launch_bounds__(128, 3) k_residual_gather_rerun(GATHER_PARAMS, const int *__restrict__ gate,
+                                                                  unsigned long long *__restrict__ ext) {
+    if (gate[0] == 0 && gate[1] == 0) return;
+    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
+    for (int b = blockIdx.x * blockDim.x; b < nnode; b += gridDim.x * blockDim.x) {
+        const int i = b + threadIdx.x;
+        if (i < nnode) residual_gather_node<FLUX, SECOND, KAPPA0>(i, GATHER_ARGS, mn, mx);
     }
     if (add_time) block_extrema3(mn, mx, ext);
 }
@@ -434,21 +463,21 @@ __global__ void k_limiter_fix_apply(int nnode, const int *__restrict__ count, co
                                     int redo_roe, double *__restrict__ phi, double *__restrict__ work) {
     const int nroe = count[0], npc = count[1];
     if (nroe == 0 && npc == 0) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nnode) return;
-    const int fl = flag[i];
-    if (npc == 0) {
-        if (fl & 1) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nnode; i += gridDim.x * blockDim.x) {
+        const int fl = flag[i];
+        if (npc == 0) {
+            if (fl & 1) {
 #pragma unroll
-            for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = 0.0;
+                for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = 0.0;
+            }
+            continue;
         }
-        return;
-    }
 #pragma unroll
-    for (int v = 0; v < 5; v++) {
-        const double ph = (fl & 2) ? 0.0 : phi[v * (int64_t)nnode + i];
-        if (fl & 2) phi[v * (int64_t)nnode + i] = 0.0;
-        if (redo_roe) work[v * (int64_t)nnode + i] = ph;
+        for (int v = 0; v < 5; v++) {
+            const double ph = (fl & 2) ? 0.0 : phi[v * (int64_t)nnode + i];
+            if (fl & 2) phi[v * (int64_t)nnode + i] = 0.0;
+            if (redo_roe) work[v * (int64_t)nnode + i] = ph;
+        }
     }
 }
 
@@ -890,12 +919,20 @@ static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, bool check_
             c->flow, add_time, c->patch_nlocmax, check_roe ? 1 : 0, c->roeflag.p, c->fixcount.p, gate, c->res.p,
             c->resd.p, c->dt.p, c->ext.p);
     } else {
-        auto kern = SECOND && c->flow.frac == 0.0 ? k_residual_gather<FLUX, SECOND, SECOND>
-                                                  : k_residual_gather<FLUX, SECOND, false>;
-        kern<<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(
-            c->nnode, c->ldq, c->Q.p, c->grad.p, c->phi.p, c->xyz.p, c->sell_ptr.p, c->sell_nbr.p, c->sell_geo.p,
-            c->deg.p, c->flow, add_time, (check_roe ? 1 : 0) | (check_pc ? 2 : 0), c->roeflag.p, c->fixcount.p, gate,
-            c->res.p, c->resd.p, c->dt.p, c->ext.p);
+        const bool k0 = SECOND && c->flow.frac == 0.0;
+        const int checks = (check_roe ? 1 : 0) | (check_pc ? 2 : 0);
+#define GATHER_LAUNCH_ARGS                                                                                          \
+    c->nnode, c->ldq, c->Q.p, c->grad.p, c->phi.p, c->xyz.p, c->sell_ptr.p, c->sell_nbr.p, c->sell_geo.p, c->deg.p, \
+        c->flow, add_time, checks, c->roeflag.p, c->fixcount.p, c->res.p, c->resd.p, c->dt.p
+        if (gate) {
+            auto kern = k0 ? k_residual_gather_rerun<FLUX, SECOND, SECOND> : k_residual_gather_rerun<FLUX, SECOND, false>;
+            const int grid = std::min(grid_for(c->nnode, 128), 3 * c->nsm);
+            kern<<<grid, 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, gate, c->ext.p);
+        } else {
+            auto kern = k0 ? k_residual_gather<FLUX, SECOND, SECOND> : k_residual_gather<FLUX, SECOND, false>;
+            kern<<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, c->ext.p);
+        }
+#undef GATHER_LAUNCH_ARGS
         if (c->nbnode > 0) {
             CFD_LAUNCH_CHECK();
             k_residual_bnd<FLUX><<<grid_for(c->nbnode, 128), 128, 0, c->stream>>>(
@@ -1025,8 +1062,8 @@ static int residual_with_fix(cfd_ctx *c, int add_time) {
     if (st || !(check_roe || check_pc)) return st;
     const bool redo_roe = check_roe && check_pc;
     if (redo_roe) CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)5 * c->nnode)));
-    k_limiter_fix_apply<<<grid_for(c->nnode, 256), 256, 0, c->stream>>>(c->nnode, c->fixcount.p, c->roeflag.p,
-                                                                         redo_roe ? 1 : 0, c->phi.p, c->work.p);
+    k_limiter_fix_apply<<<std::min(grid_for(c->nnode, 256), 4 * c->nsm), 256, 0, c->stream>>>(
+        c->nnode, c->fixcount.p, c->roeflag.p, redo_roe ? 1 : 0, c->phi.p, c->work.p);
     CFD_LAUNCH_CHECK();
     if (redo_roe) {
         st = launch_roe_pressure_fix(c, c->fixcount.p);
@@ -1113,8 +1150,11 @@ int cfd_create(int device, cfd_ctx **out) {
     CFD_CUDA(cudaGetDeviceCount(&ndev));
     if (device < 0 || device >= ndev) { set_error("cfd_create: device %d of %d", device, ndev); return CFD_ERR_ARG; }
     CFD_CUDA(cudaSetDevice(device));
+    int nsm = 0;
+    CFD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     cfd_ctx *c = new cfd_ctx();
     c->device = device;
+    c->nsm = nsm;
     if (g_alloc_async) c->stream = g_alloc_stream;  // serving worker: its own stream from the start
     cfd_params_default(&c->params);
     if (c->err.alloc(1) != cudaSuccess || c->ext.alloc(8) != cudaSuccess) {

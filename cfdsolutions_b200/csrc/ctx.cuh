@@ -115,6 +115,7 @@ struct Abmc {
 
 struct cfd_ctx {
     int device = 0;
+    int nsm = 148;  // SMs of the device (grids of the gated, usually empty passes)
     cudaStream_t stream = nullptr;
     cfd_params params{};
     cfd::Flow flow{};

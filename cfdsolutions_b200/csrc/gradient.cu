@@ -168,8 +168,10 @@ __device__ __forceinline__ void limit_node(int i, int nnode, int64_t ldq, const 
         // per edge; the result is the same rounded quotient the reference's
         // per-edge divisions select, except for ties closer than an ulp.
         double bn[5] = {1, 1, 1, 1, 1}, bd[5] = {1, 1, 1, 1, 1};
+        int sn_next = dgi > 0 ? sell_nbr[sb] : 0;
         for (int k = 0; k < dgi; k++) {
-            int j = sell_nbr[sb + 32 * k];
+            int j = sn_next;
+            if (k + 1 < dgi) sn_next = sell_nbr[sb + 32 * (k + 1)];
             j = j >= 0 ? j : ~j;
             const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
 #pragma unroll
@@ -298,10 +300,17 @@ __global__ void __launch_bounds__(128) k_gg_limiter(int nnode, int64_t ldq, cons
     double qi[5], qmin[5], qmax[5], gx[5] = {0, 0, 0, 0, 0}, gy[5] = {0, 0, 0, 0, 0}, gz[5] = {0, 0, 0, 0, 0};
 #pragma unroll
     for (int v = 0; v < 5; v++) qmin[v] = qmax[v] = qi[v] = Q[v * ldq + i];
+    // slot k+1's neighbour id and face are loaded while slot k is summed
+    int sn_next = dgi > 0 ? sell_nbr[sb] : 0;
+    double4 S_next = dgi > 0 ? sell_geo[sb] : make_double4(0, 0, 0, 0);
     for (int k = 0; k < dgi; k++) {
-        const int sn = sell_nbr[sb + 32 * k];
+        const int sn = sn_next;
+        const double4 S = S_next;
+        if (k + 1 < dgi) {
+            sn_next = sell_nbr[sb + 32 * (k + 1)];
+            S_next = sell_geo[sb + 32 * (k + 1)];
+        }
         const int j = sn >= 0 ? sn : ~sn;
-        const double4 S = sell_geo[sb + 32 * k];
         const double sg = sn >= 0 ? 0.5 * S.w : -0.5 * S.w;
         const double sx = sg * S.x, sy = sg * S.y, sz = sg * S.z;
 #pragma unroll
@@ -394,47 +403,47 @@ __global__ void __launch_bounds__(128) k_roe_pressure_fix(int nnode, int64_t ldq
     // gate: the residual's fix counters; this full pass is needed only when the
     // reconstructed-pressure correction changed some limiter (gate[1] > 0)
     if (gate && gate[1] == 0) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nnode) return;
-    const int64_t sb = sell_ptr[i >> 5] + (i & 31);
-    const int dgi = deg[i];
-    const double frac = f.frac;
-    bool neg = false;
-    const double xi = xyz[i], yi = xyz[nnode + i], zi = xyz[2 * nnode + i];
-    for (int k = 0; k < dgi && !neg; k++) {
-        int j = sell_nbr[sb + 32 * k];
-        j = j >= 0 ? j : ~j;
-        const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
-        double qa[5], qb[5];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nnode; i += gridDim.x * blockDim.x) {
+        const int64_t sb = sell_ptr[i >> 5] + (i & 31);
+        const int dgi = deg[i];
+        const double frac = f.frac;
+        bool neg = false;
+        const double xi = xyz[i], yi = xyz[nnode + i], zi = xyz[2 * nnode + i];
+        for (int k = 0; k < dgi && !neg; k++) {
+            int j = sell_nbr[sb + 32 * k];
+            j = j >= 0 ? j : ~j;
+            const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
+            double qa[5], qb[5];
 #pragma unroll
-        for (int v = 0; v < 5; v++) {
-            const double ci = Q[v * ldq + i], cj = Q[v * ldq + j];
-            const double pi_ = phi_in[v * (int64_t)nnode + i], pj = phi_in[v * (int64_t)nnode + j];
-            qa[v] = ci + pi_ * (frac * (cj - ci) + (1.0 - frac) * (g[(3 * v) * (int64_t)nnode + i] * rx +
-                                                                  g[(3 * v + 1) * (int64_t)nnode + i] * ry +
-                                                                  g[(3 * v + 2) * (int64_t)nnode + i] * rz));
-            qb[v] = cj + pj * (frac * (ci - cj) - (1.0 - frac) * (g[(3 * v) * (int64_t)nnode + j] * rx +
-                                                                 g[(3 * v + 1) * (int64_t)nnode + j] * ry +
-                                                                 g[(3 * v + 2) * (int64_t)nnode + j] * rz));
+            for (int v = 0; v < 5; v++) {
+                const double ci = Q[v * ldq + i], cj = Q[v * ldq + j];
+                const double pi_ = phi_in[v * (int64_t)nnode + i], pj = phi_in[v * (int64_t)nnode + j];
+                qa[v] = ci + pi_ * (frac * (cj - ci) + (1.0 - frac) * (g[(3 * v) * (int64_t)nnode + i] * rx +
+                                                                      g[(3 * v + 1) * (int64_t)nnode + i] * ry +
+                                                                      g[(3 * v + 2) * (int64_t)nnode + i] * rz));
+                qb[v] = cj + pj * (frac * (ci - cj) - (1.0 - frac) * (g[(3 * v) * (int64_t)nnode + j] * rx +
+                                                                     g[(3 * v + 1) * (int64_t)nnode + j] * ry +
+                                                                     g[(3 * v + 2) * (int64_t)nnode + j] * rz));
+            }
+            // Compute_RoeVariables (Roe_Fluxes.cpp:3609-3633)
+            const double ra = qa[0], rb = qb[0];
+            const double ua = qa[1] / ra, va = qa[2] / ra, wa = qa[3] / ra;
+            const double ub = qb[1] / rb, vb = qb[2] / rb, wb = qb[3] / rb;
+            const double pa = f.gm1 * (qa[4] - 0.5 * ra * (ua * ua + va * va + wa * wa)) - f.gpinf;
+            const double pb = f.gm1 * (qb[4] - 0.5 * rb * (ub * ub + vb * vb + wb * wb)) - f.gpinf;
+            const double ha = (qa[4] + pa) / ra, hb = (qb[4] + pb) / rb;
+            const double rho = sqrt(ra * rb), sg = rho / (ra + rho);
+            const double u = ua + sg * (ub - ua), v = va + sg * (vb - va), w = wa + sg * (wb - wa);
+            const double ht = ha + sg * (hb - ha);
+            double qr[5];
+            qr[0] = rho; qr[1] = rho * u; qr[2] = rho * v; qr[3] = rho * w;
+            qr[4] = (rho / f.gamma) * (ht + 0.5 * f.gm1 * (u * u + v * v + w * w));
+            const double p = f.gm1 * (qr[4] - (0.5 / qr[0]) * (qr[1] * qr[1] + qr[2] * qr[2] + qr[3] * qr[3]));
+            if (p < 0.0) neg = true;
         }
-        // Compute_RoeVariables (Roe_Fluxes.cpp:3609-3633)
-        const double ra = qa[0], rb = qb[0];
-        const double ua = qa[1] / ra, va = qa[2] / ra, wa = qa[3] / ra;
-        const double ub = qb[1] / rb, vb = qb[2] / rb, wb = qb[3] / rb;
-        const double pa = f.gm1 * (qa[4] - 0.5 * ra * (ua * ua + va * va + wa * wa)) - f.gpinf;
-        const double pb = f.gm1 * (qb[4] - 0.5 * rb * (ub * ub + vb * vb + wb * wb)) - f.gpinf;
-        const double ha = (qa[4] + pa) / ra, hb = (qb[4] + pb) / rb;
-        const double rho = sqrt(ra * rb), sg = rho / (ra + rho);
-        const double u = ua + sg * (ub - ua), v = va + sg * (vb - va), w = wa + sg * (wb - wa);
-        const double ht = ha + sg * (hb - ha);
-        double qr[5];
-        qr[0] = rho; qr[1] = rho * u; qr[2] = rho * v; qr[3] = rho * w;
-        qr[4] = (rho / f.gamma) * (ht + 0.5 * f.gm1 * (u * u + v * v + w * w));
-        const double p = f.gm1 * (qr[4] - (0.5 / qr[0]) * (qr[1] * qr[1] + qr[2] * qr[2] + qr[3] * qr[3]));
-        if (p < 0.0) neg = true;
-    }
 #pragma unroll
-    for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = neg ? 0.0 : phi_in[v * (int64_t)nnode + i];
+        for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = neg ? 0.0 : phi_in[v * (int64_t)nnode + i];
+    }
 }
 
 template <bool KAPPA0, bool PC>
@@ -551,7 +560,9 @@ int cfd_limiter(cfd_ctx *c) {
 namespace cfd {
 int launch_roe_pressure_fix(cfd_ctx *c, const int *gate) {
     const int n = c->nnode;
-    k_roe_pressure_fix<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p,
+    // gated: usually a no-op, so a short grid that strides when it runs
+    const int grid = gate ? std::min(grid_for(n, 128), 4 * c->nsm) : grid_for(n, 128);
+    k_roe_pressure_fix<<<grid, 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p,
                                                                   c->deg.p, c->xyz.p, c->grad.p, c->flow, gate,
                                                                   c->work.p, c->phi.p);
     CFD_LAUNCH_CHECK();

@@ -198,10 +198,20 @@ __device__ __forceinline__ double vanleer_flux(const double qL[5], const double 
     return fmax(fabs(ub_a), fmax(fabs(ub_a + c_a), fabs(ub_a - c_a)));
 }
 
+// roe_c2, when not null and FLUX is the plain or low-Mach-fix Roe flux (the
+// fluxes that average qL and qR themselves, roe_c2_of), receives the c^2 of
+// their Roe average: (gamma - 1)(h - q^2/2), of the sign of the Roe state's
+// pressure (Compute_Limiter_RoePressureCorrection, Limiters.cpp:311-356, forms
+// p = (rho/gamma)(gamma - 1)(h - q^2/2) from the same averages, or p + pinf for
+// the stiffened gas), so the limiter's Roe-average pressure check costs no
+// second average.  The two agree in sign except within rounding of zero.
+template <int FLUX>
+__host__ __device__ constexpr bool roe_c2_of() { return FLUX == CFD_FLUX_ROE || FLUX == CFD_FLUX_ROE_LMFIX; }
+
 template <int FLUX>
 __device__ __forceinline__ double edge_flux(const double qL[5], const double qR[5], double nx, double ny, double nz,
                                             double area, const Flow &f, double conv[5], double diss[5],
-                                            double lam[3]) {
+                                            double lam[3], double *roe_c2 = nullptr) {
     if (FLUX == CFD_FLUX_HLLC) return hllc_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
     if (FLUX == CFD_FLUX_AUSM) return ausmp_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
     if (FLUX == CFD_FLUX_VANLEER) return vanleer_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
@@ -211,7 +221,7 @@ __device__ __forceinline__ double edge_flux(const double qL[5], const double qR[
         thornber_states(qL, qR, f, mL, mR);
         return roe_flux<false>(mL, mR, nx, ny, nz, area, f, conv, diss, lam);
     }
-    return roe_flux<FLUX == CFD_FLUX_ROE_LMFIX>(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
+    return roe_flux<FLUX == CFD_FLUX_ROE_LMFIX>(qL, qR, nx, ny, nz, area, f, conv, diss, lam, roe_c2);
 }
 
 // The Roe family (plain, low-Mach fix, preconditioned): the limiter pressure fix applies.

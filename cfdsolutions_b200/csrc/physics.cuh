@@ -79,10 +79,11 @@ __device__ __forceinline__ void roe_entropy_fix(double ubar_L, double c_L, doubl
 // |A| dQ = M_{cons<-RUP} * dw, dw in closed form (FluxTest.cpp:3180-3190).
 // Returns the largest |eigenvalue| (for the time step) and the three
 // eigenvalue magnitudes |ubar|, |ubar+c|, |ubar-c| in lam[3].
+// c2_out, when not null, receives the Roe-averaged c^2 (see edge_flux).
 template <bool LMFIX>
 __device__ __forceinline__ double roe_flux(const double qL[5], const double qR[5], double nx, double ny,
                                            double nz, double area, const Flow &f, double conv[5],
-                                           double diss[5], double lam[3]) {
+                                           double diss[5], double lam[3], double *c2_out = nullptr) {
     Face L, R;
     const bool want_c = f.entropy_fix != 0;
     eos_face(qL, nx, ny, nz, f, want_c, L);
@@ -109,6 +110,7 @@ __device__ __forceinline__ double roe_flux(const double qL[5], const double qR[5
     const double q2 = u * u + v * v + w * w;
     // Get_SpeedSound(u,v,w,ht), generic non-dimensionalisation (Material.cpp:939-960)
     const double c2 = f.gm1 * ht - 0.5 * f.gm1 * q2;
+    if (c2_out) *c2_out = c2;
     const double ci = rsqrt(c2);
     const double c = c2 * ci;
     const double ubar = u * nx + v * ny + w * nz;
