@@ -602,7 +602,9 @@ def main():
     abytes = algorithmic_bytes(mesh.nnode, mesh.nedge, mesh.nghost)
     achieved = abytes / (ms_res / 1e3) / 1e9
     tpe = traffic_from_profile()
-    roofline = {"bound": "hbm", "kernel": "k_residual_gather<ROE,SECOND>", "achieved": achieved, "peak": peak,
+    # one cfd_residual: k_residual_gather<ROE,SECOND> (interior edges) + k_residual_bnd<ROE> (boundary edges)
+    roofline = {"bound": "hbm", "kernel": "k_residual_gather<ROE,SECOND> + k_residual_bnd<ROE>", "achieved": achieved,
+                "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                 "algorithmic_bytes_per_launch": abytes, "launch_ms": ms_res,
                 "traffic": (tpe * units) if tpe else None,

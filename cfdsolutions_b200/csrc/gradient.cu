@@ -168,12 +168,25 @@ __device__ __forceinline__ void limit_node(int i, int nnode, int64_t ldq, const 
         // per edge; the result is the same rounded quotient the reference's
         // per-edge divisions select, except for ties closer than an ulp.
         double bn[5] = {1, 1, 1, 1, 1}, bd[5] = {1, 1, 1, 1, 1};
-        int sn_next = dgi > 0 ? sell_nbr[sb] : 0;
+        // neighbour ids two slots ahead, coordinates one slot ahead
+        int sn1 = 0, sn2 = 0;
+        double xn = 0.0, yn = 0.0, zn = 0.0;
+        if (dgi > 0) {
+            sn1 = sell_nbr[sb];
+            const int j0 = sn1 >= 0 ? sn1 : ~sn1;
+            xn = xyz[j0]; yn = xyz[nnode + j0]; zn = xyz[2 * nnode + j0];
+        }
+        if (dgi > 1) sn2 = sell_nbr[sb + 32];
         for (int k = 0; k < dgi; k++) {
-            int j = sn_next;
-            if (k + 1 < dgi) sn_next = sell_nbr[sb + 32 * (k + 1)];
+            const double rx = 0.5 * (xn - xi), ry = 0.5 * (yn - yi), rz = 0.5 * (zn - zi);
+            int j = sn1;
+            if (k + 1 < dgi) {
+                sn1 = sn2;
+                const int j1 = sn1 >= 0 ? sn1 : ~sn1;
+                xn = xyz[j1]; yn = xyz[nnode + j1]; zn = xyz[2 * nnode + j1];
+                if (k + 2 < dgi) sn2 = sell_nbr[sb + 32 * (k + 2)];
+            }
             j = j >= 0 ? j : ~j;
-            const double rx = 0.5 * (xyz[j] - xi), ry = 0.5 * (xyz[nnode + j] - yi), rz = 0.5 * (xyz[2 * nnode + j] - zi);
 #pragma unroll
             for (int v = 0; v < 5; v++) {
                 const double qj = KAPPA0 ? 0.0 : Q[v * ldq + j];
@@ -301,21 +314,33 @@ __global__ void __launch_bounds__(128) k_gg_limiter(int nnode, int64_t ldq, cons
 #pragma unroll
     for (int v = 0; v < 5; v++) qmin[v] = qmax[v] = qi[v] = Q[v * ldq + i];
     // slot k+1's neighbour id and face are loaded while slot k is summed
-    int sn_next = dgi > 0 ? sell_nbr[sb] : 0;
+    int sn_next = dgi > 0 ? sell_nbr[sb] : 0, sn_far = dgi > 1 ? sell_nbr[sb + 32] : 0;
     double4 S_next = dgi > 0 ? sell_geo[sb] : make_double4(0, 0, 0, 0);
+    double qn[5] = {0, 0, 0, 0, 0};
+    if (dgi > 0) {
+        const int j0 = sn_next >= 0 ? sn_next : ~sn_next;
+#pragma unroll
+        for (int v = 0; v < 5; v++) qn[v] = Q[v * ldq + j0];
+    }
     for (int k = 0; k < dgi; k++) {
         const int sn = sn_next;
         const double4 S = S_next;
+        double qcur[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) qcur[v] = qn[v];
         if (k + 1 < dgi) {
-            sn_next = sell_nbr[sb + 32 * (k + 1)];
+            sn_next = sn_far;
             S_next = sell_geo[sb + 32 * (k + 1)];
+            const int j1 = sn_next >= 0 ? sn_next : ~sn_next;
+#pragma unroll
+            for (int v = 0; v < 5; v++) qn[v] = Q[v * ldq + j1];
+            if (k + 2 < dgi) sn_far = sell_nbr[sb + 32 * (k + 2)];
         }
-        const int j = sn >= 0 ? sn : ~sn;
         const double sg = sn >= 0 ? 0.5 * S.w : -0.5 * S.w;
         const double sx = sg * S.x, sy = sg * S.y, sz = sg * S.z;
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-            const double qj = Q[v * ldq + j];
+            const double qj = qcur[v];
             const double d = qj - qi[v];
             gx[v] += d * sx;
             gy[v] += d * sy;
