@@ -32,3 +32,15 @@ def relerr(a, b):
 def relerr_rows(a, b):
     """max over components of normwise relative error (rows = equations)."""
     return max(relerr(x, y) for x, y in zip(a, b))
+
+
+def low_pressure_spots(Q, nnode, gamma, scale=0.02, seed=5, share=0.03):
+    """Q with the pressure of a seeded 3 % of the nodes scaled by `scale`
+    (momentum kept): the reconstructed pressure of those nodes' neighbours goes
+    negative, so the limiter's pressure correction fires."""
+    rng = np.random.default_rng(seed)
+    Q = Q.copy()
+    idx = rng.choice(nnode, size=max(1, int(share * nnode)), replace=False)
+    ke = 0.5 * (Q[1:4, idx] ** 2).sum(0) / Q[0, idx]
+    Q[4, idx] = scale * (Q[4, idx] - ke) + ke
+    return Q

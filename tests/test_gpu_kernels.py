@@ -8,7 +8,7 @@ import pytest
 
 from cfdsolutions_b200 import Euler3DGPU, box_mesh
 from oracle import restatement
-from tests._util import CFG1, make_case, params_from, relerr, relerr_rows
+from tests._util import CFG1, low_pressure_spots, make_case, params_from, relerr, relerr_rows
 
 pytestmark = pytest.mark.gpu
 
@@ -71,18 +71,6 @@ def test_residual_matches_restatement(gpu_available, cfg, numbering):
     else:
         assert np.abs(g["diss"]).max() == 0.0
     assert relerr(g["deltat"], o["deltat"]) <= TOL
-
-
-def low_pressure_spots(Q, nnode, gamma, scale=0.02, seed=5, share=0.03):
-    """Q with the pressure of a seeded 3 % of the nodes scaled by `scale`
-    (momentum kept): the reconstructed pressure of those nodes' neighbours goes
-    negative, so the limiter's pressure correction fires."""
-    rng = np.random.default_rng(seed)
-    Q = Q.copy()
-    idx = rng.choice(nnode, size=max(1, int(share * nnode)), replace=False)
-    ke = 0.5 * (Q[1:4, idx] ** 2).sum(0) / Q[0, idx]
-    Q[4, idx] = scale * (Q[4, idx] - ke) + ke
-    return Q
 
 
 FIX_CASES = [(flux, lo, g) for flux in (1, 0) for lo in (0, 1) for g in (0, 1)]

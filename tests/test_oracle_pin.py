@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from oracle import refharness, restatement
-from tests._util import CFG1, make_case, relerr, relerr_rows
+from tests._util import CFG1, low_pressure_spots, make_case, relerr, relerr_rows
 
 TOL = 1e-13
 
@@ -60,6 +60,29 @@ def test_second_order_matches_reference(ref_available, flux, limiter, lorder, sm
     assert relerr_rows(conv, ref["conv"]) <= TOL
     assert np.abs(diss - ref["diss"]).max() <= TOL * max(np.abs(ref["diss"]).max(), 1.0)
     assert relerr(dt, ref["deltat"]) <= TOL
+
+
+@pytest.mark.parametrize("flux,limiter,lorder", [(0, 1, 0), (1, 1, 1), (0, 1, 1), (1, 1, 0)])
+def test_limiter_pressure_corrections_match_reference(ref_available, flux, limiter, lorder):
+    """States with low-pressure spots, where the limiter's reconstructed-pressure
+    correction (Limiters.cpp:273-304) and, for Roe, the sequential Roe-average
+    fix (:61-110) fire: the restatement zeroes the reference's limiters and
+    gives its residual."""
+    cfg = dict(CFG1, flux_scheme=flux, order=1, limiter=limiter, limiter_order=lorder, venkat_k=5.0, mach=0.8,
+               mach_min=0.8, alpha_deg=1.25)
+    m, cfg, Q = make_case(n=8, seed=9, cfg=cfg, noise=0.02)
+    Q = low_pressure_spots(Q, m.nnode, cfg["gamma"], seed=9)
+    ref = refharness.run(m, cfg, Q, [("begin", 0), ("gradient", 0), ("limiter",), ("bc", 0), ("residual", 1),
+                                     ("get", "residual"), ("get", "limiters")])
+    s = restatement.Session(m, cfg)
+    g = s.gradient(Q)
+    phi = s.limiter(Q, g)
+    conv, diss, _, _ = s.residual(s.apply_bc(Q), g, phi)
+    assert (ref["limiters"] == 0).all(axis=0).sum() >= 3  # the corrections fired
+    np.testing.assert_array_equal(phi == 0, ref["limiters"] == 0)
+    assert np.abs(phi - ref["limiters"]).max() <= 1e-13
+    assert relerr_rows(conv, ref["conv"]) <= TOL
+    assert np.abs(diss - ref["diss"]).max() <= TOL * max(np.abs(ref["diss"]).max(), 1.0)
 
 
 def test_entropy_fix_and_global_time_match_reference(ref_available):
