@@ -23,6 +23,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -112,7 +113,7 @@ class Clocks:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+        self.path = Path(tempfile.gettempdir()) / f"cfd_b200_clocks_{os.getpid()}.csv"
 
     def __enter__(self):
         try:

@@ -1,7 +1,7 @@
 """Parity of the CUDA path with the reference's own functions (the Euler3D
 objects compiled into oracle/_ref, run on the same mesh arrays and state).
 
-Tolerances (north star): residuals within 1e-12 relative in FP64 (normwise
+Tolerances: residuals within 1e-12 relative in FP64 (normwise
 per equation, max |gpu - ref| / max |ref|); the same bound for ghost states,
 time steps, gradients, limiters and Jacobian blocks.  Block Gauss-Seidel on an
 identical system is bit-exact (level scheduling preserves the sequential
