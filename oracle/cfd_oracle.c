@@ -175,11 +175,20 @@ static double pc_edge(const double *qL, const double *qR, const double *n, const
     double g = p->gamma;
     eos_face(qL, n[0], n[1], n[2], g, p->pinf, Lf);
     eos_face(qR, n[0], n[1], n[2], g, p->pinf, Rf);
-    double rho = sqrt(Rf->rho * Lf->rho), sigma = rho / (Lf->rho + rho);
-    double u = Lf->u + sigma * (Rf->u - Lf->u), v = Lf->v + sigma * (Rf->v - Lf->v), w = Lf->w + sigma * (Rf->w - Lf->w);
-    double ht = Lf->ht + sigma * (Rf->ht - Lf->ht);
-    double q2 = u * u + v * v + w * w, h = ht - 0.5 * q2;
-    double c = sqrt((g - 1.0) * h); /* Material_Get_DH_SpeedSound: c^2 = (g - 1) h for either gas */
+    double rho, u, v, w, ht, c;
+    if (p->pc_avg == 1) { /* simple mean, |c^2| (Euler3D FluxTest.cpp:3927-3940) */
+        rho = 0.5 * (Rf->rho + Lf->rho);
+        u = 0.5 * (Rf->u + Lf->u); v = 0.5 * (Rf->v + Lf->v); w = 0.5 * (Rf->w + Lf->w);
+        ht = 0.5 * (Rf->ht + Lf->ht);
+        c = sqrt(fabs((g - 1.0) * (ht - 0.5 * (u * u + v * v + w * w))));
+    } else {
+        double sigma;
+        rho = sqrt(Rf->rho * Lf->rho), sigma = rho / (Lf->rho + rho);
+        u = Lf->u + sigma * (Rf->u - Lf->u), v = Lf->v + sigma * (Rf->v - Lf->v), w = Lf->w + sigma * (Rf->w - Lf->w);
+        ht = Lf->ht + sigma * (Rf->ht - Lf->ht);
+        c = sqrt((g - 1.0) * (ht - 0.5 * (u * u + v * v + w * w))); /* Material_Get_DH_SpeedSound: c^2 = (g - 1) h */
+    }
+    double q2 = u * u + v * v + w * w;
     double mach = sqrt(q2) / c;
     double mL = sqrt(Lf->u * Lf->u + Lf->v * Lf->v + Lf->w * Lf->w) / Lf->c;
     double mR = sqrt(Rf->u * Rf->u + Rf->v * Rf->v + Rf->w * Rf->w) / Rf->c;

@@ -23,6 +23,10 @@ typedef struct {
      * subsonic outflow pressure (0: freestream) */
     int pc_method, pc_type;
     double pc_mach, outflow_p;
+    /* face average of the preconditioned Roe: 0 Roe (MPFLOW3D AVERAGE_TYPE_ROE), 1 simple
+     * arithmetic mean of rho, u, v, w, h (Euler3D's Compute_Flux_Roe_Precondition_BTW,
+     * FluxTest.cpp:3917-3940) */
+    int pc_avg;
 } orc_params;
 
 typedef struct {

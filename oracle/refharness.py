@@ -70,6 +70,13 @@ def param_text(cfg: dict) -> str:
         "MACH_MIN": repr(float(g("mach_min", mach))), "MACH_MAX": repr(float(mach)),
         "RESTART_INPUT": "NO", "RESTART_OUTPUT": "NO",
     }
+    if "e3d_precond" in cfg:
+        # Euler3D's own preconditioned Roe (FluxTest.cpp: Compute_Flux_Roe_Precondition_*),
+        # e.g. "PRECOND_METHOD_ROE_BTW" with "PRECOND_TYPE_GLOBAL"
+        lines["FLUX_SCHEME"] = "FLUX_SCHEME_ROE"
+        lines["PRECOND_METHOD"] = cfg["e3d_precond"]
+        lines["PRECOND_TYPE"] = cfg.get("e3d_precond_type", "PRECOND_TYPE_GLOBAL")
+        lines["PRECOND_SMOOTH"] = "NO"
     return "".join(f"{k}={v}\n" for k, v in lines.items())
 
 
