@@ -85,14 +85,17 @@ def test_limiter_pressure_corrections_match_reference(ref_available, flux, limit
     assert np.abs(diss - ref["diss"]).max() <= TOL * max(np.abs(ref["diss"]).max(), 1.0)
 
 
-@pytest.mark.parametrize("method,e3d,average", [(2, "PRECOND_METHOD_ROE_BTW", 1), (3, "PRECOND_METHOD_ROE_ERIKSSON", 0)],
-                         ids=["btw", "eriksson"])
+@pytest.mark.parametrize("method,e3d,average,ptype", [(2, "PRECOND_METHOD_ROE_BTW", 1, 1),
+                                                       (3, "PRECOND_METHOD_ROE_ERIKSSON", 0, 1),
+                                                       (3, "PRECOND_METHOD_ROE_ERIKSSON", 0, 0)],
+                         ids=["btw-global", "eriksson-global", "eriksson-local"])
 @pytest.mark.parametrize("order", [0, 1])
-def test_preconditioned_roe_matches_euler3d(ref_available, method, e3d, average, order):
+def test_preconditioned_roe_matches_euler3d(ref_available, method, e3d, average, ptype, order):
     """The restatement's preconditioned Roe (flux 4, written after MPFLOW3D with
     closed-form eigenvectors of K A) against Euler3D's own BTW and Eriksson
     fluxes (FluxTest.cpp:3842-4238, 4238-4628), compiled from the reference,
-    with the global beta = min(1, M_ref)^2.  Euler3D's BTW takes the simple mean
+    with the global beta = min(1, M_ref)^2 and, for Eriksson, the local beta of
+    the face and its two ends (FluxTest.cpp:4405-4412, no smoothing).  Euler3D's BTW takes the simple mean
     of the face states (FluxTest.cpp:3917-3940, precond_average 1), its
     Eriksson the Roe average.  Compared at the nodes without boundary edges:
     the reference's preconditioned boundary condition is not on this path, so
@@ -100,12 +103,14 @@ def test_preconditioned_roe_matches_euler3d(ref_available, method, e3d, average,
     mach = 0.1
     base = dict(CFG1, order=order, gradient=0, limiter=1 if order else -1, venkat_k=5.0, mach=mach, mach_min=mach,
                 alpha_deg=1.25)
-    cfg = dict(base, flux_scheme=4, precond_method=method, precond_type=1, precond_mach=mach,
+    cfg = dict(base, flux_scheme=4, precond_method=method, precond_type=ptype, precond_mach=mach,
                precond_average=average)
     m, cfg, Q = make_case(n=8, seed=41, cfg=cfg, noise=0.02)
     steps = [("begin", 0)] + ([("gradient", 0), ("limiter",)] if order else []) + \
             [("residual", 1), ("get", "residual"), ("deltat", 0), ("get", "deltat")]
-    ref = refharness.run(m, dict(base, flux_scheme=0, e3d_precond=e3d), Q, steps)
+    ref = refharness.run(m, dict(base, flux_scheme=0, e3d_precond=e3d,
+                                 e3d_precond_type="PRECOND_TYPE_GLOBAL" if ptype == 1 else "PRECOND_TYPE_LOCAL"),
+                         Q, steps)
     s = restatement.Session(m, cfg)
     g = s.gradient(Q) if order else None
     phi = s.limiter(Q, g) if order else None
