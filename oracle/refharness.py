@@ -37,7 +37,11 @@ JACOBIAN = {0: "JACOBIAN_METHOD_CENTRAL", 1: "JACOBIAN_METHOD_FORWARD", 2: "JACO
 
 
 def param_text(cfg: dict) -> str:
-    """Reference parameter file for the options in ``cfg`` (same keys as cfd_params)."""
+    """Reference parameter file for the options in ``cfg`` (same keys as cfd_params).
+
+    Two keys only the reference has: ``e3d_precond`` selects one of Euler3D's own
+    preconditioned Roe fluxes by its PRECOND_METHOD name, with ``e3d_precond_type``
+    (PRECOND_TYPE_GLOBAL by default)."""
     g = lambda k, d: cfg.get(k, d)  # noqa: E731
     mach = g("mach", 0.5)
     lines = {
