@@ -21,7 +21,13 @@
 //     at zero (the solution) is cleared by each call.
 // The device address of the array is looked up once per device, with that
 // device current, on the first call made on it; make that first call before
-// any stream capture begins.
+// any stream capture begins.  The address stays cached for the life of the
+// process, so do not call cudaDeviceReset (or otherwise destroy the device's
+// primary context) while this entry point is still in use.
+//
+// Host cost per call: the pattern (IA, IAU, then JA) is copied to the host
+// with two synchronising copies and checked, both level schedules are rebuilt
+// on the host (O(nnz)), and each sweep synchronises once to read its RMS.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -117,23 +123,39 @@ extern "C" int cfd_block_gs_static(int nrow, const int *dIA, const int *dJA, con
     double *part = scr + (int64_t)CFD_GS_STATIC_MAX_ROWS * 26 + CFD_GS_STATIC_MAX_ROWS;
     double *total = part + 296;
 
-    // pattern to the host for the level schedules (host memory only)
-    std::vector<int> IA(nrow + 1);
+    // Pattern to the host for the level schedules (host memory only).  The
+    // pattern comes from the caller, so it is checked in full before any
+    // kernel reads A, JA or IAU through it: IA must be an increasing row
+    // pointer starting at 0 (its last entry is the length of JA and A), every
+    // column in range, and every IAU[r] the slot of row r's diagonal block.
+    std::vector<int> IA(nrow + 1), IAU(nrow);
     CFD_CUDA(cudaMemcpyAsync(IA.data(), dIA, sizeof(int) * (nrow + 1), cudaMemcpyDeviceToHost, s));
+    CFD_CUDA(cudaMemcpyAsync(IAU.data(), dIAU, sizeof(int) * nrow, cudaMemcpyDeviceToHost, s));
     CFD_CUDA(cudaStreamSynchronize(s));
     if (IA[0] != 0 || IA[nrow] < nrow) {
-        set_error("cfd_block_gs_static: IA is not a block-CRS row pointer");
+        set_error("cfd_block_gs_static: IA is not a block-CRS row pointer (IA[0] = %d, IA[nrow] = %d)", IA[0],
+                  IA[nrow]);
         return CFD_ERR_ARG;
     }
+    for (int i = 0; i < nrow; i++)
+        if (IA[i + 1] <= IA[i]) {  // every row holds at least its diagonal block
+            set_error("cfd_block_gs_static: IA is not increasing at row %d (IA[%d] = %d, IA[%d] = %d)", i, i,
+                      IA[i], i + 1, IA[i + 1]);
+            return CFD_ERR_ARG;
+        }
     std::vector<int> JA(IA[nrow]);
     CFD_CUDA(cudaMemcpyAsync(JA.data(), dJA, sizeof(int) * IA[nrow], cudaMemcpyDeviceToHost, s));
     CFD_CUDA(cudaStreamSynchronize(s));
-    for (int i = 0; i < nrow; i++)
-        for (int k = IA[i]; k < IA[i + 1]; k++)
-            if (JA[k] < 0 || JA[k] >= nrow) {
-                set_error("cfd_block_gs_static: JA[%d] = %d out of range", k, JA[k]);
-                return CFD_ERR_ARG;
-            }
+    for (int k = 0; k < IA[nrow]; k++)
+        if (JA[k] < 0 || JA[k] >= nrow) {
+            set_error("cfd_block_gs_static: JA[%d] = %d out of range", k, JA[k]);
+            return CFD_ERR_ARG;
+        }
+    for (int r = 0; r < nrow; r++)
+        if (IAU[r] < IA[r] || IAU[r] >= IA[r + 1] || JA[IAU[r]] != r) {
+            set_error("cfd_block_gs_static: IAU[%d] = %d is not the diagonal slot of row %d", r, IAU[r], r);
+            return CFD_ERR_ARG;
+        }
     std::vector<int> fptr, frows, bptr, brows;
     levels_host(IA, JA, nrow, true, fptr, frows);
     levels_host(IA, JA, nrow, false, bptr, brows);

@@ -317,7 +317,13 @@ int  cfd_ilu_mc_order(cfd_ctx *ctx, int *order, int *ncolor);
  * larger systems return CFD_ERR_RANGE.  The array is shared: calls that
  * overlap on the GPU race, so keep them on one stream.  The first call on a
  * device looks up the array's device address (make it before any stream
- * capture).  Work runs on `stream` (a cudaStream_t, NULL = legacy stream). */
+ * capture) and keeps it until exit: do not cudaDeviceReset the device while
+ * the library is in use.  The caller's pattern is checked on the host before
+ * any launch (IA increasing from 0, JA in range, JA[IAU[r]] == r with IAU[r] in
+ * row r), CFD_ERR_ARG otherwise.  Each call copies the pattern to the host
+ * (two synchronising copies), rebuilds its level schedules there (O(nnz)) and
+ * synchronises once per sweep.  Work runs on `stream` (a cudaStream_t, NULL =
+ * legacy stream). */
 #define CFD_GS_STATIC_MAX_ROWS 16384
 int  cfd_block_gs_static(int nrow, const int *IA, const int *JA, const int *IAU, const double *A,
                          const double *B, double *X, int iterations, int direction, void *stream,

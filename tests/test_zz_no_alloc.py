@@ -81,3 +81,83 @@ def test_static_block_gs_rejects_too_many_rows(gpu_available):
                                         buf.data_ptr(), buf.data_ptr(), 1, 0, None, C.byref(rms))
     assert code == -9  # CFD_ERR_RANGE
     assert b"static scratch capacity" in capi.lib.cfd_last_error()
+
+
+def _call_raw(torch, n, IA, JA, IAU, nnzb):
+    """Call cfd_block_gs_static on a caller-built pattern (host lists) with
+    device buffers sized for it; returns the status code."""
+    dev = torch.device("cuda:0")
+    t = lambda a: torch.tensor(a, dtype=torch.int32, device=dev)  # noqa: E731
+    dIA, dJA, dIAU = t(IA), t(JA), t(IAU)
+    A = torch.zeros((max(nnzb, 1), 5, 5), dtype=torch.float64)
+    for r, k in enumerate(IAU):
+        if 0 <= k < nnzb:
+            A[k] = torch.eye(5, dtype=torch.float64)  # identity diagonal blocks: a solvable system
+    A = A.to(dev)
+    B = torch.zeros(n * 5, dtype=torch.float64, device=dev)
+    X = torch.zeros(n * 5, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    rms = C.c_double()
+    return capi.lib.cfd_block_gs_static(n, dIA.data_ptr(), dJA.data_ptr(), dIAU.data_ptr(), A.data_ptr(),
+                                        B.data_ptr(), X.data_ptr(), 1, 0, None, C.byref(rms))
+
+
+def test_static_block_gs_rejects_bad_patterns_before_any_launch(gpu_available):
+    """The caller's pattern is validated on the host, so each malformed one
+    below returns CFD_ERR_ARG without a kernel ever indexing through it.  Every
+    device buffer is allocated at the size the (bad) pattern itself claims, so
+    the host-side copies stay inside them."""
+    import torch
+
+    # a valid 3-row tridiagonal pattern: rows {0,1}, {0,1,2}, {1,2}
+    IA = [0, 2, 5, 7]
+    JA = [0, 1, 0, 1, 2, 1, 2]
+    IAU = [0, 3, 6]
+    assert _call_raw(torch, 3, IA, JA, IAU, 7) == 0
+    cases = {
+        "IA not starting at 0": ([1, 2, 5, 7], JA, IAU),
+        "IA decreasing": ([0, 5, 2, 7], JA, IAU),
+        "empty row": ([0, 2, 2, 7], JA, IAU),
+        "JA out of range": (IA, [0, 1, 0, 1, 3, 1, 2], IAU),
+        "negative JA": (IA, [0, -1, 0, 1, 2, 1, 2], IAU),
+        "IAU outside its row": (IA, JA, [0, 5, 6]),
+        "IAU past the pattern": (IA, JA, [0, 3, 9]),
+        "IAU not on the diagonal": (IA, JA, [1, 3, 6]),
+    }
+    for what, (ia, ja, iau) in cases.items():
+        code = _call_raw(torch, 3, ia, ja, iau, len(ja))
+        assert code == -1, what  # CFD_ERR_ARG
+    # after the rejections the entry point still solves a real system
+    sysd = _system(6, 3)
+    (x_ref, rms_ref) = sysd["expect"][(6, 0)]
+    x, rms = _static_gs(torch, sysd, 6, 0)
+    np.testing.assert_array_equal(x, x_ref)
+
+
+def test_static_block_gs_allocates_no_device_memory(gpu_available):
+    """After the first call on the device, further calls leave the device's
+    free memory exactly unchanged: the entry point reaches no allocator (all
+    buffers of this test are created before the measured calls)."""
+    import torch
+
+    sysd = _system(12, 5)
+    dev = torch.device("cuda:0")
+    t = {k: torch.from_numpy(np.ascontiguousarray(sysd[k])).to(dev) for k in ("IA", "JA", "IAU", "A", "B")}
+    X = torch.empty((sysd["n"], 5), dtype=torch.float64, device=dev)
+    rms = C.c_double()
+
+    def call():
+        code = capi.lib.cfd_block_gs_static(sysd["n"], t["IA"].data_ptr(), t["JA"].data_ptr(),
+                                            t["IAU"].data_ptr(), t["A"].data_ptr(), t["B"].data_ptr(),
+                                            X.data_ptr(), 6, 0, None, C.byref(rms))
+        capi.check(code, "cfd_block_gs_static")
+
+    call()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(4):
+        call()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    np.testing.assert_array_equal(X.cpu().numpy(), sysd["expect"][(6, 0)][0])
