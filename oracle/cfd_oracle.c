@@ -538,6 +538,34 @@ static double roe(const double *qL, const double *qR, const double *n, double ar
         double mach = (fabs(ub) + fabs(u * t1[0] + v * t1[1] + w * t1[2]) + fabs(u * t2[0] + v * t2[1] + w * t2[2])) / c;
         dU = dmin(mach, 1.0) * dU;
     }
+    if (p->mpf_form) {
+        /* MPFLOW3D's matrix form (Roe_Fluxes.cpp:1598-1683, VARIABLE_RUP): |A| dQ =
+         * (Mop P) dW with P = |A| in (rho, u, v, w, p), Mop at the Roe state and dW the
+         * jump of (rho, u, v, w, p); E4 = |u.n + c|, E5 = |u.n - c| */
+        double Em = E1 - E2, Ep = E1 + E2, c2 = c * c, P[5][5], T[5][5];
+        double dd = p->mpf_form == 1 ? n[1] * n[1] : n[2] * n[2];
+        P[0][0] = E0; P[0][1] = 0.5 * Em * rho * n[0] / c; P[0][2] = 0.5 * Em * rho * n[1] / c;
+        P[0][3] = 0.5 * Em * rho * n[2] / c; P[0][4] = -E0 / c2 + 0.5 * Ep / c2;
+        P[1][0] = 0.0; P[1][1] = E0 * (1.0 - n[0] * n[0]) + 0.5 * Ep * n[0] * n[0];
+        P[1][2] = -E0 * n[0] * n[1] + 0.5 * Ep * n[0] * n[1]; P[1][3] = -E0 * n[0] * n[2] + 0.5 * Ep * n[0] * n[2];
+        P[1][4] = 0.5 * Em * n[0] / (rho * c);
+        P[2][0] = 0.0; P[2][1] = -E0 * n[0] * n[1] + 0.5 * Ep * n[1] * n[0];
+        P[2][2] = E0 * (1.0 - n[1] * n[1]) + 0.5 * Ep * n[1] * n[1];
+        P[2][3] = -E0 * n[1] * n[2] + 0.5 * Ep * n[1] * n[2]; P[2][4] = 0.5 * Em * n[1] / (rho * c);
+        P[3][0] = 0.0; P[3][1] = -E0 * n[0] * n[2] + 0.5 * Ep * n[2] * n[0];
+        P[3][2] = -E0 * n[1] * n[2] + 0.5 * Ep * n[2] * n[1];
+        P[3][3] = E0 * (1.0 - dd) + 0.5 * Ep * n[2] * n[2]; P[3][4] = 0.5 * Em * n[2] / (rho * c);
+        P[4][0] = 0.0; P[4][1] = 0.5 * Em * c * rho * n[0]; P[4][2] = 0.5 * Em * c * rho * n[1];
+        P[4][3] = 0.5 * Em * c * rho * n[2]; P[4][4] = 0.0 + 0.5 * Ep;
+        mm5g(M, P, T);
+        for (int i = 0; i < 5; i++) {
+            double fa = 0.0;
+            for (int j = 0; j < 5; j++) fa += T[i][j] * dQ[j];
+            conv[i] = 0.5 * (FL[i] + FR[i]) * area;
+            diss[i] = -0.5 * fa * area;
+        }
+        return dmax(E0, dmax(E1, E2));
+    }
     double dw[5];
     dw[0] = E0 * dQ[0] + (E1 + E2 - 2.0 * E0) * dQ[4] / (2.0 * c * c) + rho * (E1 - E2) * dU / (2.0 * c);
     for (int k = 1; k < 4; k++)

@@ -27,6 +27,12 @@ typedef struct {
      * arithmetic mean of rho, u, v, w, h (Euler3D's Compute_Flux_Roe_Precondition_BTW,
      * FluxTest.cpp:3917-3940) */
     int pc_avg;
+    /* Roe dissipation form (test pins only): 0 the closed form of Euler3D's
+     * Compute_Flux_Roe_Optimized (FluxTest.cpp:3143-3200, the library's form);
+     * 1 MPFLOW3D's matrix form Mop P dW (MPFLOW3D/src/Roe_Fluxes.cpp:1605-1683)
+     * exactly as written, whose w-momentum diagonal reads E1 (1 - ny^2); 2 the
+     * same matrix form with E1 (1 - nz^2) */
+    int mpf_form;
 } orc_params;
 
 typedef struct {

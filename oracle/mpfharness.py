@@ -78,7 +78,7 @@ def param_text(cfg: dict) -> str:
         "PRECOND_METHOD": PRECOND[precond_of(cfg)],
         "PRECOND_TYPE": PRECOND_TYPE[g("precond_type", 1)], "PRECOND_SMOOTH": "NO",
         "BC_METHOD": "BC_METHOD_CHARCTERISTIC", "ZPG_ITERATION": str(g("zpg_iteration", 0)),
-        "VARIABLE_TYPE": "VARIABLE_RUP", "ENTROPY_FIX": "YES" if g("entropy_fix", 0) else "NO",
+        "VARIABLE_TYPE": "VARIABLE_CON" if g("mpf_variable", "rup") == "con" else "VARIABLE_RUP", "ENTROPY_FIX": "YES" if g("entropy_fix", 0) else "NO",
         "JACOBIAN_METHOD": "JACOBIAN_METHOD_APPROX", "JACOBIAN_UPDATE": "1", "FIRST_ORDER_NITERATION": "0",
         "PHYSICAL_DELTA_TIME": "0.0", "SOLVER_RELAXATION": "1.0", "AVERAGE_TYPE": "AVERAGE_TYPE_ROE",
         "SOLUTION_SMOOTH": "NO", "SOLUTION_SMOOTH_NITERATION": "0", "SOLUTION_SMOOTH_RELAXATION": "0.5",
@@ -241,16 +241,20 @@ def _session(mesh_arrays: dict, cfg: dict, R: np.ndarray | None, steps: list, qu
 
 def run(mesh, cfg: dict, Q: np.ndarray | None, steps: list, quiet: bool = True, timeout: float = 600.0) -> dict:
     """Run ``steps`` on MPFLOW3D in a fresh spawned process.  ``Q`` is the
-    library's conservative state [5][nnode+nghost]; it is handed to MPFLOW3D
-    as RUP.  A returned ``state`` is converted back to conservative variables
+    library's conservative state [5][nnode+nghost].  With ``cfg["mpf_variable"]
+    == "con"`` MPFLOW3D runs in conservative variables (VARIABLE_CON; its
+    residual, BC and time step, not its implicit Jacobian, which needs RUP) and
+    the state passes unchanged; otherwise it is handed to MPFLOW3D as RUP and a
+    returned ``state`` is converted back to conservative variables
     (``state_rup`` keeps MPFLOW3D's own)."""
     if not available():
         raise FileNotFoundError(f"{MPF_LIB} not built (make -C oracle ref)")
-    R = None if Q is None else cons_to_rup(np.asarray(Q, np.float64))
+    con = cfg.get("mpf_variable", "rup") == "con"
+    R = None if Q is None else (np.asarray(Q, np.float64) if con else cons_to_rup(np.asarray(Q, np.float64)))
     ctx = mp.get_context("spawn")
     with ctx.Pool(1) as pool:
         out = pool.apply_async(_session, (_mesh_dict(mesh), cfg, R, steps, quiet)).get(timeout)
-    if "state" in out:
+    if "state" in out and not con:
         out["state_rup"] = out["state"]
         out["state"] = rup_to_cons(out["state"])
     return out
