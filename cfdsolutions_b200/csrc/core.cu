@@ -126,11 +126,12 @@ __device__ __forceinline__ void reconstruct(const double qs[5], const double qo[
         const double *__restrict__ phi, const double *__restrict__ xyz, const int64_t *__restrict__ sell_ptr, \
         const int *__restrict__ sell_nbr, const double4 *__restrict__ sell_geo, const int *__restrict__ deg,   \
         Flow f, int add_time, int checks, int *__restrict__ roeflag, int *__restrict__ fixcount,                 \
-        double *__restrict__ res, double *__restrict__ resd, double *__restrict__ dtsum
+        double *__restrict__ res, double *__restrict__ resd, double *__restrict__ dtsum, const double *__restrict__ lgrad
 #define GATHER_ARGS \
-    nnode, ldq, Q, grad, phi, xyz, sell_ptr, sell_nbr, sell_geo, deg, f, add_time, checks, roeflag, fixcount, res, resd, dtsum
+    nnode, ldq, Q, grad, phi, xyz, sell_ptr, sell_nbr, sell_geo, deg, f, add_time, checks, roeflag, fixcount, res, resd, \
+        dtsum, lgrad
 
-template <int FLUX, bool SECOND, bool KAPPA0>
+template <int FLUX, bool SECOND, bool KAPPA0, bool LG = false>
 __device__ __forceinline__ void residual_gather_node(int i, GATHER_PARAMS, double mn[3], double mx[3]) {
     {
         const bool limited = f.limiter != CFD_LIMITER_NONE;
@@ -139,7 +140,7 @@ __device__ __forceinline__ void residual_gather_node(int i, GATHER_PARAMS, doubl
         for (int v = 0; v < 5; v++) qo[v] = Q[v * ldq + i];
         if (SECOND) {
 #pragma unroll
-            for (int k = 0; k < 15; k++) go[k] = grad[k * (int64_t)nnode + i];
+            for (int k = 0; k < 15; k++) go[k] = LG ? lgrad[k * (int64_t)nnode + i] : grad[k * (int64_t)nnode + i];
 #pragma unroll
             for (int v = 0; v < 5; v++) po[v] = limited ? phi[v * (int64_t)nnode + i] : 1.0;
 #pragma unroll
@@ -168,6 +169,14 @@ __device__ __forceinline__ void residual_gather_node(int i, GATHER_PARAMS, doubl
 #pragma unroll
                 for (int v = 0; v < 5; v++) {
                     const double gno = go[3 * v] * rx + go[3 * v + 1] * ry + go[3 * v + 2] * rz;
+                    if (LG) {
+                        const double gnn = -(lgrad[(3 * v) * (int64_t)nnode + j] * rx +
+                                             lgrad[(3 * v + 1) * (int64_t)nnode + j] * ry +
+                                             lgrad[(3 * v + 2) * (int64_t)nnode + j] * rz);
+                        fo[v] = qo[v] + gno;
+                        fn[v] = qn[v] + gnn;
+                        continue;
+                    }
                     const double gnn = -(grad[(3 * v) * (int64_t)nnode + j] * rx +
                                          grad[(3 * v + 1) * (int64_t)nnode + j] * ry +
                                          grad[(3 * v + 2) * (int64_t)nnode + j] * rz);
@@ -223,11 +232,11 @@ __device__ __forceinline__ void residual_gather_node(int i, GATHER_PARAMS, doubl
     }
 }
 
-template <int FLUX, bool SECOND, bool KAPPA0 = false>
+template <int FLUX, bool SECOND, bool KAPPA0 = false, bool LG = false>
 __global__ void __launch_bounds__(128, 3) k_residual_gather(GATHER_PARAMS, unsigned long long *__restrict__ ext) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
-    if (i < nnode) residual_gather_node<FLUX, SECOND, KAPPA0>(i, GATHER_ARGS, mn, mx);
+    if (i < nnode) residual_gather_node<FLUX, SECOND, KAPPA0, LG>(i, GATHER_ARGS, mn, mx);
     if (add_time) block_extrema3(mn, mx, ext);
 }
 
@@ -921,10 +930,17 @@ static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, bool check_
     } else {
         const bool k0 = SECOND && c->flow.frac == 0.0;
         const int checks = (check_roe ? 1 : 0) | (check_pc ? 2 : 0);
+        // limited gradients phi * grad formed with these limiters by the fused
+        // Green-Gauss + limiter pass (first pass only: a gated re-evaluation
+        // follows limiter fixes, which change phi)
+        const bool lgk = k0 && !gate && c->lgrad_valid && c->params.limiter != CFD_LIMITER_NONE;
 #define GATHER_LAUNCH_ARGS                                                                                          \
     c->nnode, c->ldq, c->Q.p, c->grad.p, c->phi.p, c->xyz.p, c->sell_ptr.p, c->sell_nbr.p, c->sell_geo.p, c->deg.p, \
-        c->flow, add_time, checks, c->roeflag.p, c->fixcount.p, c->res.p, c->resd.p, c->dt.p
-        if (gate) {
+        c->flow, add_time, checks, c->roeflag.p, c->fixcount.p, c->res.p, c->resd.p, c->dt.p, c->lgrad.p
+        if (lgk) {
+            k_residual_gather<FLUX, SECOND, SECOND, true>
+                <<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, c->ext.p);
+        } else if (gate) {
             auto kern = k0 ? k_residual_gather_rerun<FLUX, SECOND, SECOND> : k_residual_gather_rerun<FLUX, SECOND, false>;
             const int grid = std::min(grid_for(c->nnode, 128), 3 * c->nsm);
             kern<<<grid, 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, gate, c->ext.p);
@@ -1065,6 +1081,7 @@ static int residual_with_fix(cfd_ctx *c, int add_time) {
     k_limiter_fix_apply<<<std::min(grid_for(c->nnode, 256), 4 * c->nsm), 256, 0, c->stream>>>(
         c->nnode, c->fixcount.p, c->roeflag.p, redo_roe ? 1 : 0, c->phi.p, c->work.p);
     CFD_LAUNCH_CHECK();
+    c->lgrad_valid = false;  // the fixes may have changed phi
     if (redo_roe) {
         st = launch_roe_pressure_fix(c, c->fixcount.p);
         if (st) return st;
@@ -1186,6 +1203,7 @@ int cfd_set_stream(cfd_ctx *c, void *stream) {
 int cfd_set_params(cfd_ctx *c, const cfd_params *p) {
     if (!c || !p) { set_error("cfd_set_params: NULL"); return CFD_ERR_ARG; }
     c->phi_next_valid = false;
+    c->lgrad_valid = c->lgrad_pending = false;
     if (p->flux_scheme < CFD_FLUX_ROE || p->flux_scheme > CFD_FLUX_VANLEER) {
         set_error("cfd_set_params: invalid flux scheme %d", p->flux_scheme);
         return CFD_ERR_ARG;
@@ -1281,6 +1299,7 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
     c->has_system = false;
     c->has_grad = false;
     c->phi_next_valid = false;
+    c->lgrad_valid = c->lgrad_pending = false;
     c->lsq_weight = -1;
     c->nnode = nnode;
     c->nghost = nghost;
@@ -1556,6 +1575,7 @@ int cfd_set_state(cfd_ctx *c, const double *Q) {
     NEED_MESH("cfd_set_state");
     if (!Q) return CFD_ERR_ARG;
     c->phi_next_valid = false;
+    c->lgrad_valid = c->lgrad_pending = false;
     const int64_t n = (int64_t)c->nnode + c->nghost;
     CFD_CUDA(cudaMemcpy2DAsync(c->Q.p, c->ldq * sizeof(double), Q, n * sizeof(double), n * sizeof(double), 5,
                                cudaMemcpyHostToDevice, c->stream));
@@ -1575,6 +1595,7 @@ int cfd_get_state(cfd_ctx *c, double *Q) {
 int cfd_state_device_ptr(cfd_ctx *c, double **dQ, int64_t *ld) {
     NEED_MESH("cfd_state_device_ptr");
     c->phi_next_valid = false;  // the caller may write the state
+    c->lgrad_valid = c->lgrad_pending = false;
     if (dQ) *dQ = c->Q.p;
     if (ld) *ld = c->ldq;
     return CFD_OK;
@@ -1583,6 +1604,7 @@ int cfd_state_device_ptr(cfd_ctx *c, double **dQ, int64_t *ld) {
 int cfd_set_freestream(cfd_ctx *c) {
     NEED_MESH("cfd_set_freestream");
     c->phi_next_valid = false;
+    c->lgrad_valid = c->lgrad_pending = false;
     compute_flow(c, 0);
     const int n = c->nnode + c->nghost;
     k_freestream<<<grid_for(n, 256), 256, 0, c->stream>>>(n, c->ldq, c->flow, c->Q.p);
@@ -1797,6 +1819,7 @@ int cfd_update(cfd_ctx *c, double relax) {
     NEED_MESH("cfd_update");
     if (!c->X.p) { set_error("cfd_update: no solution vector"); return CFD_ERR_STATE; }
     c->phi_next_valid = false;
+    c->lgrad_valid = c->lgrad_pending = false;
     k_update<<<grid_for(c->nnode, 256), 256, 0, c->stream>>>(c->nnode, c->ldq, relax, c->X.p, c->Q.p);
     CFD_LAUNCH_CHECK();
     return CFD_OK;

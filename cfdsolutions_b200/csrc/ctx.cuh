@@ -149,6 +149,12 @@ struct cfd_ctx {
     // sliced-ELL incidence of the node-gather residual kernel
     cfd::DevBuf<int64_t> sell_ptr;    // [nslice+1] slot offset of each 32-node slice
     cfd::DevBuf<int> sell_nbr;        // [slots] neighbour id, ~id when the node is node_R
+    // limited gradients phi * grad of the fused Green-Gauss + limiter pass
+    // (frac = 0 only), read for the neighbours by the first residual pass;
+    // valid while grad and phi are the ones they were formed from
+    cfd::DevBuf<double> lgrad;        // [15][nnode]
+    bool lgrad_pending = false;       // lgrad matches phi_next
+    bool lgrad_valid = false;         // lgrad matches phi
     cfd::DevBuf<double4> sell_geo;    // [slots] edge unit normal (L->R) + |S|
     cfd::DevBuf<int> deg;             // [nnode] interior edges per node
     // patch layout of the residual kernel: patches are contiguous ranges of

@@ -298,13 +298,13 @@ __global__ void __launch_bounds__(128) k_venkat(int nnode, int64_t ldq, const do
 // reads the gradient from registers.  Saves the limiter's own neighbour pass
 // and its re-read of the 15 gradient components.
 template <bool KAPPA0, bool PC>
-__global__ void __launch_bounds__(128) k_gg_limiter(int nnode, int64_t ldq, const double *__restrict__ Q,
+__global__ void __launch_bounds__(128, 4) k_gg_limiter(int nnode, int64_t ldq, const double *__restrict__ Q,
                                                     const int64_t *__restrict__ sell_ptr,
                                                     const int *__restrict__ sell_nbr, const int *__restrict__ deg,
                                                     const double4 *__restrict__ sell_geo,
                                                     const double *__restrict__ xyz, const double *__restrict__ vol,
                                                     Flow f, double *__restrict__ g, double *__restrict__ phi,
-                                                    int *__restrict__ roeflag) {
+                                                    int *__restrict__ roeflag, double *__restrict__ lg) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnode) return;
     const int64_t sb = sell_ptr[i >> 5] + (i & 31);
@@ -366,6 +366,17 @@ __global__ void __launch_bounds__(128) k_gg_limiter(int nnode, int64_t ldq, cons
     limit_node<KAPPA0, PC>(i, nnode, ldq, Q, sb, dgi, sell_nbr, xyz, f, qi, qmin, qmax, gx, gy, gz, eps2, ph);
 #pragma unroll
     for (int v = 0; v < 5; v++) phi[v * (int64_t)nnode + i] = ph[v];
+    if (KAPPA0 && lg) {
+        // limited gradients for the residual's neighbour gathers: with frac = 0
+        // the face state is Q + phi grad.r, and a neighbour's (phi grad) is 15
+        // loads where grad and phi are 20
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            lg[(3 * v) * (int64_t)nnode + i] = ph[v] * gx[v];
+            lg[(3 * v + 1) * (int64_t)nnode + i] = ph[v] * gy[v];
+            lg[(3 * v + 2) * (int64_t)nnode + i] = ph[v] * gz[v];
+        }
+    }
 }
 
 // The reconstructed-pressure correction alone (Compute_Limiter_PressureCorrection,
@@ -479,10 +490,10 @@ static void launch_venkat(cfd_ctx *c) {
 }
 
 template <bool KAPPA0, bool PC>
-static void launch_gg_limiter(cfd_ctx *c) {
+static void launch_gg_limiter(cfd_ctx *c, double *lg) {
     k_gg_limiter<KAPPA0, PC><<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(
         c->nnode, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p, c->deg.p, c->sell_geo.p, c->xyz.p, c->cvol.p, c->flow,
-        c->grad.p, c->phi_next.p, c->roeflag.p);
+        c->grad.p, c->phi_next.p, c->roeflag.p, lg);
 }
 
 // Whether the next limiter leaves its reconstructed-pressure correction to
@@ -501,6 +512,7 @@ int cfd_gradient(cfd_ctx *c) {
     const int n = c->nnode;
     CFD_CUDA(c->grad.alloc((size_t)15 * n));
     c->phi_next_valid = false;
+    c->lgrad_valid = c->lgrad_pending = false;  // grad changes
     const bool with_limiter = c->params.order == CFD_ORDER_SECOND && c->params.limiter != CFD_LIMITER_NONE;
     if (c->params.gradient == CFD_GRAD_GG && with_limiter) {
         // second order with a limiter: the limiter of this state is formed in
@@ -508,16 +520,23 @@ int cfd_gradient(cfd_ctx *c) {
         // the parameters change before it (phi_next_valid)
         CFD_CUDA(c->phi_next.alloc((size_t)5 * n));
         const bool kappa0 = c->flow.frac == 0.0, defer = limiter_defers_pc(c);
+        // the gather residual reads the limited gradients (frac = 0)
+        double *lg = nullptr;
+        if (kappa0 && !patch_kernel(c)) {
+            CFD_CUDA(c->lgrad.alloc((size_t)15 * n));
+            lg = c->lgrad.p;
+        }
         if (kappa0) {
-            if (defer) launch_gg_limiter<true, false>(c);
-            else launch_gg_limiter<true, true>(c);
+            if (defer) launch_gg_limiter<true, false>(c, lg);
+            else launch_gg_limiter<true, true>(c, lg);
         } else {
-            if (defer) launch_gg_limiter<false, false>(c);
-            else launch_gg_limiter<false, true>(c);
+            if (defer) launch_gg_limiter<false, false>(c, lg);
+            else launch_gg_limiter<false, true>(c, lg);
         }
         CFD_LAUNCH_CHECK();
         c->phi_next_valid = true;
         c->phi_next_defers_pc = defer;
+        c->lgrad_pending = lg != nullptr;
     } else if (c->params.gradient == CFD_GRAD_GG) {
         k_gg_grad<<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p, c->deg.p,
                                                              c->sell_geo.p, c->cvol.p, c->grad.p);
@@ -556,11 +575,13 @@ int cfd_limiter(cfd_ctx *c) {
     // gated pass applies the fixes), or to limiter_fix_standalone when the
     // limiters are read back or consumed by another kernel first.
     bool defer_pc;
+    c->lgrad_valid = false;
     if (c->phi_next_valid) {
         // formed by cfd_gradient together with the gradient of this state
         c->phi.swap(c->phi_next);
         c->phi_next_valid = false;
         defer_pc = c->phi_next_defers_pc;
+        c->lgrad_valid = c->lgrad_pending;
     } else {
         const bool kappa0 = c->flow.frac == 0.0;
         defer_pc = limiter_defers_pc(c);
@@ -596,6 +617,7 @@ int launch_roe_pressure_fix(cfd_ctx *c, const int *gate) {
 
 int limiter_fix_standalone(cfd_ctx *c) {
     const int n = c->nnode;
+    c->lgrad_valid = false;  // the fixes may change phi
     if (c->pc_fix_pending) {
         if (c->flow.frac == 0.0)
             k_venkat_pc<true><<<grid_for(n, 128), 128, 0, c->stream>>>(n, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p,
