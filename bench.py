@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--no-steady", action="store_true", help="skip the time-to-steady-state solves")
     ap.add_argument("--no-serve", action="store_true", help="skip the served batch")
     ap.add_argument("--no-lowmach", action="store_true", help="skip the low-Mach liquid channel solves")
+    ap.add_argument("--no-linear", action="store_true", help="skip the linear-algebra kernel rooflines")
     ap.add_argument("--serve-requests", type=int, default=64)
     ap.add_argument("--serve-nmax", type=int, default=64, help="largest cube side of the served mix (config: 96)")
     ap.add_argument("--serve-rate", type=float, default=2.0, help="Poisson arrival rate, requests per second")
@@ -160,11 +161,12 @@ def reference_throughput(sample_n, procs, warmup, steps):
     """Reference CPU residual passes (LSQ gradient + Venkatakrishnan + Roe
     residual + dt, its own second-order path) on a sample_n^3 cube, one
     single-threaded reference process per core; returns (GEdges/s, details)."""
-    from cfdsolutions_b200 import box_mesh, perturbed_freestream
-    from oracle import refharness
+    # the sample mesh comes from the oracle's numpy builder, so this leg maps
+    # no library of this repository: only the reference's own objects run
+    from oracle import boxmesh, refharness
 
-    m = box_mesh(sample_n, jitter=0.15, seed=1234, rcm=True)
-    Q = perturbed_freestream(m, CFG["gamma"], CFG["mach"], CFG["alpha_deg"], noise=0.01, seed=1235)
+    m = boxmesh.box_mesh(sample_n, jitter=0.15, seed=1234, rcm=True)
+    Q = boxmesh.perturbed_freestream(m, CFG["gamma"], CFG["mach"], CFG["alpha_deg"], noise=0.01, seed=1235)
     cfg = dict(CFG, gradient=0, scheme="explicit")
     one = [("begin", 0), ("gradient", 0), ("limiter",), ("bc", 0), ("residual", 1), ("deltat", 0)]
     steps_all = one * (warmup + steps)
@@ -439,6 +441,17 @@ def aggregate_rate(units_per_rank, seconds, world):
     return units_per_rank * world / seconds
 
 
+def reference_sample_config(sample_n):
+    """The workload the reference arm times: the headline's flow and limiter on
+    a sample_n^3 cube with the reference's own gradient (least squares; the
+    reference has no Green-Gauss) and plain RCM numbering."""
+    return {"workload": f"second-order residual evaluation, {sample_n}^3-hex tet cube (6 tets/hex), RCM, jitter "
+                        "0.15h, least-squares gradient + Venkatakrishnan K=5 + Roe, M=0.8, alpha=1.25, +-1% noise",
+            "sample_of": "the headline workload at 128^3 (Green-Gauss), which the reference cannot run",
+            "numbering": "reverse Cuthill-McKee", "flux": "roe", "gradient": "least-squares",
+            "limiter": "venkatakrishnan", "venkat_k": 5.0, "mach": 0.8, "alpha_deg": 1.25, "precision": "fp64"}
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -448,11 +461,54 @@ def run_reference_arm(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": d["per_pass_s"] * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": workload_config(args.n),
+        "data": "synthetic", "config": reference_sample_config(args.cpu_sample_n),
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": procs, "kind": "reference", "sample": d["sample"]},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def linear_rooflines(s, mesh, stream, timed, args, peak):
+    """Jacobian assembly (FP32 blocks, low-precision-only system, the steady
+    solve's form), block SpMV with the FP32 matrix and one block-multicolour
+    ILU(0) apply with FP32 factors, each timed alone with CUDA events over
+    repeated calls on the library's stream, against the measured HBM copy
+    bandwidth.  Algorithmic bytes (compulsory traffic per call):
+      SpMV:     100 nnzb (FP32 blocks) + 4 nnzb (JA) + 4 (N+1) (IA) + 40 N (x) + 40 N (y)
+      ILU apply: the same on the L+U factors (forward and backward solve together)
+      Jacobian: 100 nnzb + 4 nnzb + 4 (N+1), plus Q (40 (N+G)), dt (8 N), residuals
+                (80 N) read and B (40 N) written."""
+    import torch
+    from cfdsolutions_b200 import capi
+
+    n, g = mesh.nnode, mesh.nghost
+    for i in range(2):
+        s.residual_step(i)
+    prec = capi.PREC_FP32 | capi.PREC_LOW_ONLY
+    jac = lambda i: s.Compute_Jacobian(1, 0, include_diss=1, precision=prec)  # noqa: E731
+    k = max(5, args.steps // 30)
+    ms_jac = timed(jac, k, 2) / k
+    nnzb = s.nnzb
+    capi.check(capi.lib.cfd_ilu_mc_order(s.handle, None, None), "cfd_ilu_mc_order")
+    s.solve_gmres(restart=30, max_iters=2, rtol=1e-12, precond=capi.PC_ILU0_MC, precision=prec,
+                  allow_not_converged=True)
+    dev = torch.cuda.current_device()
+    x = torch.randn((n, 5), dtype=torch.float64, device=dev)
+    y = torch.empty_like(x)
+    torch.cuda.synchronize()
+    k2 = max(10, args.steps // 6)
+    ms_spmv = timed(lambda i: s.spmv_device(x.data_ptr(), y.data_ptr(), capi.PREC_FP32), k2, 3) / k2
+    ms_ilu = timed(lambda i: s.precond_apply_device(x.data_ptr(), y.data_ptr()), k, 2) / k
+    b_mat = 100 * nnzb + 4 * nnzb + 4 * (n + 1)
+    out = {"system": f"128^3 tet cube: {n} block rows, {nnzb} blocks; FP32 blocks (low-precision-only system)"}
+    for name, ms, b, kern in (
+            ("spmv", ms_spmv, b_mat + 80 * n, "k_bspmv<float> (one warp per block row)"),
+            ("ilu_apply", ms_ilu, b_mat + 80 * n, "k_mc_fwd + k_mc_bwd (block-multicolour ILU(0), FP32 factors)"),
+            ("jacobian", ms_jac, b_mat + 40 * (n + g) + 128 * n, "k_jac_edges + k_jac_rows (FP32 blocks)")):
+        ach = b / (ms / 1e3) / 1e9
+        out[name] = {"bound": "hbm", "kernel": kern, "ms": ms, "algorithmic_bytes": b, "achieved": ach,
+                     "peak": peak, "unit": "GB/s", "frac": ach / peak}
+    return out
 
 
 def profile_case(n):
@@ -631,6 +687,23 @@ def main():
     msg = timed(lambda i: s.residual_step(i), args.steps, args.warmup)
     side["patch_kernel_gedges_per_s"] = units * args.steps / (msg / 1e3) / 1e9
     s.set_params(default_params(**CFG))
+    # the headline mesh with the reference's least-squares gradient
+    s.set_params(default_params(**dict(CFG, gradient=0)))
+    msg = timed(lambda i: s.residual_step(i), args.steps, args.warmup)
+    side["lsq_gradient_gedges_per_s"] = units * args.steps / (msg / 1e3) / 1e9
+    s.set_params(default_params(**CFG))
+    # the reference arm's own sample (same mesh builder, numbering and options),
+    # for a like-for-like ratio beside the headline
+    ms_ = args.cpu_sample_n
+    m3 = box_mesh(ms_, jitter=0.15, seed=1234, rcm=NUMBERING_RCM)
+    q3 = perturbed_freestream(m3, CFG["gamma"], CFG["mach"], CFG["alpha_deg"], noise=0.01, seed=1235)
+    with Euler3DGPU(m3, default_params(**dict(CFG, gradient=0)), device=dev, stream=stream.cuda_stream) as s3:
+        s3.set_state(q3)
+        ms3 = timed(lambda i: s3.residual_step(i), args.steps, args.warmup)
+    side["reference_sample_on_gpu"] = {"config": reference_sample_config(ms_),
+                                       "gedges_per_s": (m3.nedge + m3.nbedge) * args.steps / (ms3 / 1e3) / 1e9,
+                                       "ms_per_step": ms3 / args.steps}
+    del m3, q3
     if args.side_rcm:
         m2 = box_mesh(args.n, jitter=0.15, seed=1234, rcm=NUMBERING_RCM)
         q2 = perturbed_freestream(m2, CFG["gamma"], CFG["mach"], CFG["alpha_deg"], noise=0.01, seed=1235)
@@ -663,6 +736,8 @@ def main():
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                    "sample": "reference oracle library not built"}
 
+    # ---- the implicit step's linear-algebra kernels on the same 128^3 system
+    linear = None if args.no_linear else linear_rooflines(s, mesh, stream, timed, args, peak)
     s.close()
 
     # ---- time to the steady residual drop (plain FP64 and mixed precision)
@@ -744,7 +819,8 @@ def main():
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded tet-split cube, seeded +-1% state noise)",
             "config": workload_config(args.n, mesh), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": KERNELS_PER_STEP * args.steps, "clocks": clocks, "per_flux": per_flux,
-            "breakdown_ms": breakdown, "variants": side, "setup_s": setup_s, "steady": steady, "lowmach": lowmach,
+            "breakdown_ms": breakdown, "variants": side, "setup_s": setup_s, "linear": linear, "steady": steady,
+            "lowmach": lowmach,
             "serve": serve,
         }
         print(json.dumps(line), flush=True)

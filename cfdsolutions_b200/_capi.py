@@ -134,6 +134,8 @@ SIGNATURES = {
     "cfd_ilu_mc_order": (I, [P, P, C.POINTER(I)]),
     "cfd_gmres_default": (None, [C.POINTER(GmresOpts)]),
     "cfd_gmres": (I, [P, C.POINTER(GmresOpts), C.POINTER(GmresStats)]),
+    "cfd_spmv": (I, [P, I, P, P]),
+    "cfd_precond_apply": (I, [P, P, P]),
     "cfd_update": (I, [P, D]),
     "cfd_get_residual": (I, [P, P, P]),
     "cfd_get_deltat": (I, [P, P]),

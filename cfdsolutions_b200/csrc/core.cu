@@ -572,15 +572,24 @@ __global__ void k_add_diss(int64_t n, const double *__restrict__ a, const double
 // Every off-diagonal slot belongs to exactly one edge, so no zeroing and no
 // accumulation is needed.
 // MODE: 0 Roe, 1 preconditioned Roe (CFD_FLUX_ROE_PRECOND), 2 Thornber (|A| of the modified states)
+constexpr int JAC_WARPS = 4;  // warps per CTA of k_jac_edges / k_jac_rows_warp
+
 template <typename TA, int MODE>
 __global__ void __launch_bounds__(128) k_jac_edges(int nedge, int64_t ldq, const double *__restrict__ Q,
                                                    const int2 *__restrict__ en, const double4 *__restrict__ eg,
                                                    const int2 *__restrict__ eslot, Flow f, double *__restrict__ A64,
                                                    TA *__restrict__ Alow) {
+    // Each block is stored by the warp together: the lanes put their blocks in
+    // shared memory and the warp then writes them one after the other, lane m
+    // element m, so every block leaves as one contiguous 100/200-byte store
+    // instead of 25 scalar stores scattered over 32 slots.
+    __shared__ double stage[JAC_WARPS][32][26];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nedge) return;
-    const int2 nd = en[e];
-    const double4 g = eg[e];
+    if (e - lane >= nedge) return;  // whole warps past the end
+    const bool live = e < nedge;
+    const int2 nd = en[live ? e : nedge - 1];
+    const double4 g = eg[live ? e : nedge - 1];
     double qL[5], qR[5];
 #pragma unroll
     for (int v = 0; v < 5; v++) {
@@ -597,37 +606,86 @@ __global__ void __launch_bounds__(128) k_jac_edges(int nedge, int64_t ldq, const
     } else {
         roe_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
     }
-    const int2 sl = eslot[e];
+    const int2 sl = eslot[live ? e : nedge - 1];
     const double ha = 0.5 * g.w;
-    euler_flux_jacobian(qR, g.x, g.y, g.z, f.gamma, f.gpinf, J);
+    const unsigned act = __ballot_sync(0xffffffffu, live);
+    for (int half = 0; half < 2; half++) {
+        euler_flux_jacobian(half == 0 ? qR : qL, g.x, g.y, g.z, f.gamma, f.gpinf, J);
 #pragma unroll
-    for (int k = 0; k < 25; k++) {
-        const double val = ha * (J[k] - Ab[k]);
-        if (A64) A64[(int64_t)sl.x * 25 + k] = val;
-        if (Alow) store_low(Alow + (int64_t)sl.x * 25 + k, val);
-    }
-    euler_flux_jacobian(qL, g.x, g.y, g.z, f.gamma, f.gpinf, J);
-#pragma unroll
-    for (int k = 0; k < 25; k++) {
-        const double val = -ha * (J[k] + Ab[k]);
-        if (A64) A64[(int64_t)sl.y * 25 + k] = val;
-        if (Alow) store_low(Alow + (int64_t)sl.y * 25 + k, val);
+        for (int k = 0; k < 25; k++) stage[w][lane][k] = half == 0 ? ha * (J[k] - Ab[k]) : -ha * (J[k] + Ab[k]);
+        __syncwarp();
+        const int myslot = half == 0 ? sl.x : sl.y;
+        for (int b = 0; b < 32; b++) {
+            const int slot = __shfl_sync(0xffffffffu, myslot, b);
+            if (!((act >> b) & 1u) || lane >= 25) continue;
+            const double val = stage[w][b][lane];
+            if (A64) A64[(int64_t)slot * 25 + lane] = val;
+            if (Alow) store_low(Alow + (int64_t)slot * 25 + lane, val);
+        }
+        __syncwarp();
     }
 }
 
 // Diagonal blocks and right-hand side, one thread per row:
 //   A[i,i] = V_i/dt_i I - sum_j A[j,i] + sum_b 0.5 (J(Q_i) + |A|)_b area_b
 //   B_i    = -(Res_i [+ Res_Diss_i])
+// One warp per row without boundary edges (the rows with boundary edges go to
+// k_jac_rows, one thread per row): lane m < 25 owns element m of the diagonal
+// block, so each transposed off-diagonal block is one contiguous read of the
+// warp; lanes 0-4 form B.  Same terms in the same order as k_jac_rows.
+template <typename TA, int MODE>
+__global__ void __launch_bounds__(32 * JAC_WARPS) k_jac_rows_warp(
+    int nnode, int64_t ldq, const double *__restrict__ Q, const int *__restrict__ IA, const int *__restrict__ IAU,
+    const int *__restrict__ tslot, const int *__restrict__ n2b_ptr, const double *__restrict__ vol,
+    const double *__restrict__ dt, const double *__restrict__ res, const double *__restrict__ resd, int add_time,
+    int include_diss, Flow f, double *__restrict__ A64, TA *__restrict__ Alow, double *__restrict__ B) {
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * JAC_WARPS + (threadIdx.x >> 5);
+    if (i >= nnode || n2b_ptr[i + 1] > n2b_ptr[i]) return;  // whole warps
+    const int m = lane < 25 ? lane : 24;
+    const double vd = add_time ? vol[i] / dt[i] : 0.0;
+    double d;
+    if (MODE == 1 && add_time) {
+        double qi[5], C[25];
+#pragma unroll
+        for (int v = 0; v < 5; v++) qi[v] = Q[v * ldq + i];
+        pc_node_cinv(qi, f, C);
+        double cm = C[0];
+#pragma unroll
+        for (int k = 1; k < 25; k++)
+            if (k == m) cm = C[k];
+        d = cm * vd;
+    } else {
+        d = (m % 6 == 0) ? vd : 0.0;
+    }
+    const int dg = IAU[i];
+    for (int k = IA[i]; k < IA[i + 1]; k++) {
+        if (k == dg) continue;
+        const int64_t b = (int64_t)tslot[k] * 25 + m;
+        d -= A64 ? A64[b] : load_low(Alow + b);
+    }
+    if (lane < 25) {
+        if (A64) A64[(int64_t)dg * 25 + lane] = d;
+        if (Alow) store_low(Alow + (int64_t)dg * 25 + lane, d);
+    }
+    if (lane < 5) {
+        double r = res[lane * (int64_t)nnode + i];
+        if (include_diss) r += resd[lane * (int64_t)nnode + i];
+        B[(int64_t)i * 5 + lane] = -r;
+    }
+}
+
 template <typename TA, int MODE>
 __global__ void __launch_bounds__(128) k_jac_rows(
-    int nnode, int64_t ldq, const double *__restrict__ Q, const int *__restrict__ IA, const int *__restrict__ IAU,
-    const int *__restrict__ tslot, const int *__restrict__ n2b_ptr, const int *__restrict__ n2b,
-    const int2 *__restrict__ bn, const double4 *__restrict__ bg, const double *__restrict__ vol,
-    const double *__restrict__ dt, const double *__restrict__ res, const double *__restrict__ resd,
-    int add_time, int include_diss, Flow f, double *__restrict__ A64, TA *__restrict__ Alow,
-    double *__restrict__ B) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nnode) return;
+    int nrows, const int *__restrict__ rows, int64_t ldq, const double *__restrict__ Q, const int *__restrict__ IA,
+    const int *__restrict__ IAU, const int *__restrict__ tslot, const int *__restrict__ n2b_ptr,
+    const int *__restrict__ n2b, const int2 *__restrict__ bn, const double4 *__restrict__ bg,
+    const double *__restrict__ vol, const double *__restrict__ dt, const double *__restrict__ res,
+    const double *__restrict__ resd, int add_time, int include_diss, Flow f, int nnode, double *__restrict__ A64,
+    TA *__restrict__ Alow, double *__restrict__ B) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nrows) return;
+    const int i = rows[t];
     double D[25];
     const double vd = add_time ? vol[i] / dt[i] : 0.0;
     if (MODE == 1 && add_time) {
@@ -696,14 +754,18 @@ __global__ void __launch_bounds__(128) k_jac_rows(
 // Roe Jacobian (MODE as k_jac_edges).
 template <typename TA, int MODE>
 static void launch_jacobian(cfd_ctx *c, int add_time, int include_diss, double *A64, TA *Alow) {
-    const int ge = grid_for(c->nedge, 128), gr = grid_for(c->nnode, 128);
+    const int ge = grid_for(c->nedge, 32 * JAC_WARPS);
     if (c->nedge)
-        k_jac_edges<TA, MODE><<<ge, 128, 0, c->stream>>>(c->nedge, c->ldq, c->Q.p, c->edge_nodes.p, c->edge_geo.p,
-                                                       c->eslot.p, c->flow, A64, Alow);
-    k_jac_rows<TA, MODE><<<gr, 128, 0, c->stream>>>(c->nnode, c->ldq, c->Q.p, c->IA.p, c->IAU.p, c->tslot.p,
-                                                  c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p,
-                                                  c->cvol.p, c->dt.p, c->res.p, c->resd.p, add_time, include_diss,
-                                                  c->flow, A64, Alow, c->B.p);
+        k_jac_edges<TA, MODE><<<ge, 32 * JAC_WARPS, 0, c->stream>>>(c->nedge, c->ldq, c->Q.p, c->edge_nodes.p,
+                                                                  c->edge_geo.p, c->eslot.p, c->flow, A64, Alow);
+    k_jac_rows_warp<TA, MODE><<<grid_for(c->nnode, JAC_WARPS), 32 * JAC_WARPS, 0, c->stream>>>(
+        c->nnode, c->ldq, c->Q.p, c->IA.p, c->IAU.p, c->tslot.p, c->n2b_ptr.p, c->cvol.p, c->dt.p, c->res.p,
+        c->resd.p, add_time, include_diss, c->flow, A64, Alow, c->B.p);
+    if (c->nbnode > 0)
+        k_jac_rows<TA, MODE><<<grid_for(c->nbnode, 128), 128, 0, c->stream>>>(
+            c->nbnode, c->bnode.p, c->ldq, c->Q.p, c->IA.p, c->IAU.p, c->tslot.p, c->n2b_ptr.p, c->n2b.p,
+            c->bedge_nodes.p, c->bedge_geo.p, c->cvol.p, c->dt.p, c->res.p, c->resd.p, add_time, include_diss,
+            c->flow, c->nnode, A64, Alow, c->B.p);
 }
 
 template <typename TA>

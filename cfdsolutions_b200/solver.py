@@ -153,6 +153,14 @@ class Euler3DGPU:
             capi.check(code, "cfd_gmres")
         return st
 
+    def spmv_device(self, x_ptr: int, y_ptr: int, precision: int = capi.PREC_FP64):
+        """y = A x on device vectors [nnode][5] (raw device addresses)."""
+        capi.check(capi.lib.cfd_spmv(self._h, int(precision), C.c_void_p(x_ptr), C.c_void_p(y_ptr)), "cfd_spmv")
+
+    def precond_apply_device(self, r_ptr: int, z_ptr: int):
+        """z = M^-1 r with the last cfd_gmres preconditioner, on device vectors."""
+        capi.check(capi.lib.cfd_precond_apply(self._h, C.c_void_p(r_ptr), C.c_void_p(z_ptr)), "cfd_precond_apply")
+
     def update(self, relax: float = 1.0):
         capi.check(capi.lib.cfd_update(self._h, float(relax)), "cfd_update")
 

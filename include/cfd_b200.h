@@ -299,6 +299,18 @@ void cfd_gmres_default(cfd_gmres_opts *o);
  * the implicit drivers call in its place. */
 int  cfd_gmres(cfd_ctx *ctx, const cfd_gmres_opts *o, cfd_gmres_stats *st);
 
+/* The two operators of a Krylov iteration on their own, on DEVICE vectors of
+ * the context's device ([nnode][5] FP64, stream-ordered on the context's
+ * stream): cfd_spmv forms y = A x with the stored copy of the system of the
+ * given CFD_PREC_* (the FP64 copy when that copy is not stored; the stored
+ * low-precision copy when only that one exists); cfd_precond_apply forms
+ * z = M^-1 r with the preconditioner factored by the last cfd_gmres
+ * (CFD_ERR_STATE when there is none).  The reference's block products are
+ * inside its Gauss-Seidel sweeps (MATH/src/MC_Iterative_Jacobi.c:346-535);
+ * these give the GPU solver's products to a caller's own Krylov loop. */
+int  cfd_spmv(cfd_ctx *ctx, int precision, const double *x, double *y);
+int  cfd_precond_apply(cfd_ctx *ctx, const double *r, double *z);
+
 /* Factorisation order of CFD_PC_ILU0_MC: order[k] = row at position k
  * (nnode entries; colours in increasing order, rows of a colour in increasing
  * index) and the number of colours.  Either pointer may be NULL. */

@@ -1314,6 +1314,12 @@ static void ilu_apply(int n, const int *IA, const int *JA, const int *IAU, const
     free(y);
 }
 
+/* z = (LU)^-1 r with the factors of orc_ilu0 (the apply of orc_gmres' ILU(0)). */
+void orc_ilu0_apply(int n, const int *IA, const int *JA, const int *IAU, const double *F, const double *r,
+                    double *z) {
+    ilu_apply(n, IA, JA, IAU, F, r, z);
+}
+
 static double dot(const double *a, const double *b, size_t n) {
     double s = 0.0;
     for (size_t i = 0; i < n; i++) s += a[i] * b[i];

@@ -66,6 +66,8 @@ void orc_jacobian(const orc_mesh *m, const orc_params *p, const double *Q, const
 double orc_block_gs(int n, const int *IA, const int *JA, const int *IAU, const double *A, const double *B, double *X,
                     int iters, int direction);
 int orc_ilu0(int n, const int *IA, const int *JA, const int *IAU, const double *A, double *F);
+void orc_ilu0_apply(int n, const int *IA, const int *JA, const int *IAU, const double *F, const double *r,
+                    double *z);
 int orc_gmres(int n, const int *IA, const int *JA, const int *IAU, const double *A, const double *B, double *X,
               int m, int maxit, double rtol, int precond, int *iters, double *relres);
 double orc_block_lusgs(int n, const int *IA, const int *JA, const int *IAU, const double *A, const double *B,

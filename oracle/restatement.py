@@ -51,6 +51,7 @@ def _lib():
         "orc_gmres": (C.c_int, [C.c_int, P, P, P, P, P, P, C.c_int, C.c_int, C.c_double, C.c_int,
                                 C.POINTER(C.c_int), C.POINTER(C.c_double)]),
         "orc_bspmv": (None, [C.c_int, P, P, P, P, P]),
+        "orc_ilu0_apply": (None, [C.c_int, P, P, P, P, P, P]),
     }
     for k, (r, a) in sig.items():
         f = getattr(lib, k)
@@ -138,6 +139,20 @@ class Session:
         rc = lib.orc_gmres(self.n, _p(self.IA), _p(self.JA), _p(self.IAU), _p(np.ascontiguousarray(A)),
                            _p(np.ascontiguousarray(B)), _p(X), m, maxit, rtol, precond, C.byref(it), C.byref(rr))
         return X, rc, it.value, rr.value
+
+    def ilu0(self, A):
+        """ILU(0) factors in the block pattern (L unit-lower, U with inverted diagonal blocks)."""
+        F = np.zeros((len(self.JA), 5, 5))
+        rc = lib.orc_ilu0(self.n, _p(self.IA), _p(self.JA), _p(self.IAU), _p(np.ascontiguousarray(A)), _p(F))
+        if rc:
+            raise ArithmeticError("orc_ilu0: singular diagonal block")
+        return F
+
+    def ilu0_apply(self, F, r):
+        z = np.zeros((self.n, 5))
+        lib.orc_ilu0_apply(self.n, _p(self.IA), _p(self.JA), _p(self.IAU), _p(np.ascontiguousarray(F)),
+                           _p(np.ascontiguousarray(r, np.float64)), _p(z))
+        return z
 
     def spmv(self, A, x):
         y = np.zeros((self.n, 5))
