@@ -502,7 +502,7 @@ def linear_rooflines(s, mesh, stream, timed, args, peak):
     b_mat = 100 * nnzb + 4 * nnzb + 4 * (n + 1)
     out = {"system": f"128^3 tet cube: {n} block rows, {nnzb} blocks; FP32 blocks (low-precision-only system)"}
     for name, ms, b, kern in (
-            ("spmv", ms_spmv, b_mat + 80 * n, "k_bspmv<float> (one warp per block row)"),
+            ("spmv", ms_spmv, b_mat + 80 * n, "k_bspmv<float> (five lanes per block row, two blocks in flight)"),
             ("ilu_apply", ms_ilu, b_mat + 80 * n, "k_mc_fwd + k_mc_bwd (block-multicolour ILU(0), FP32 factors)"),
             ("jacobian", ms_jac, b_mat + 40 * (n + g) + 128 * n, "k_jac_edges + k_jac_rows (FP32 blocks)")):
         ach = b / (ms / 1e3) / 1e9
