@@ -244,6 +244,49 @@ def steady_solves(mesh, Q, dev, stream, timed_once):
     return out
 
 
+def reference_converged_errors(dev, stream, n=12, iterations=120):
+    """Converged fields against the reference's own converged solve, on an
+    n^3 sample of the steady workload with the reference's least-squares
+    gradient: the reference's implicit loop (compiled Euler3D: BCs, LSQ +
+    Venkatakrishnan, Roe residual, dt with the CFL ramp, approximate Jacobian,
+    10 block Gauss-Seidel sweeps, update) with B = -(Res + Res_Diss), run to
+    its round-off floor on the host; the GPU's FP64 / FP32 / BF16 steady
+    solves of the same problem to a 1e-11 drop.  Returns the per-field
+    relative error of each GPU state (max over rho, momentum, energy of
+    max |diff| / max |reference field|)."""
+    from cfdsolutions_b200 import Euler3DGPU, box_mesh, capi, default_params, perturbed_freestream
+    from oracle import refharness
+
+    cfg = dict(STEADY, gradient=0)
+    m = box_mesh(n, jitter=0.15, seed=1234, rcm=True)
+    Q = perturbed_freestream(m, cfg["gamma"], cfg["mach"], cfg["alpha_deg"], noise=0.01, seed=1235)
+    steps = []
+    for it in range(iterations):
+        steps += [("begin", it), ("gradient", 0), ("limiter",), ("bc", it), ("residual", 1), ("deltat", it),
+                  ("jacobian", 1, it), ("rhs_full",), ("gs", 10, 0), ("update", 1.0)]
+    steps.append(("get", "state"))
+    ref = refharness.run(m, cfg, Q, steps)
+    Qr = ref["state"][:, :m.nnode]
+    mom = float(np.abs(Qr[1:4]).max())
+    out = {"sample": f"{n}^3-hex tet cube ({m.nnode} nodes), LSQ gradient; reference: {iterations} implicit "
+                     f"iterations of compiled Euler3D with B = -(Res + Res_Diss), residual drop "
+                     f"{ref['rms_full'][-1] / ref['rms_full'][0]:.2e}; GPU: GMRES(30) + multicolour ILU(0) "
+                     f"to a 1e-11 drop"}
+    for name, prec in (("fp64", capi.PREC_FP64), ("fp32", capi.PREC_FP32 | capi.PREC_LOW_ONLY),
+                       ("bf16", capi.PREC_BF16 | capi.PREC_LOW_ONLY)):
+        with Euler3DGPU(m, default_params(**cfg), device=dev, stream=stream.cuda_stream) as ss:
+            ss.set_state(Q)
+            capi.check(capi.lib.cfd_ilu_mc_order(ss.handle, None, None), "cfd_ilu_mc_order")
+            g = capi.GmresOpts(30, 60, 1e-3, capi.PC_ILU0_MC, prec, 1)
+            ss.solve_steady(max_iterations=200, drop=1e-11, include_diss=1, linear_solver=1, gmres=g)
+            Qg = ss.get_state()[:, :m.nnode]
+        errs = [float(np.abs(Qg[0] - Qr[0]).max() / np.abs(Qr[0]).max()),
+                float(np.abs(Qg[1:4] - Qr[1:4]).max() / mom),
+                float(np.abs(Qg[4] - Qr[4]).max() / np.abs(Qr[4]).max())]
+        out[name] = max(errs)
+    return out
+
+
 # The low-Mach liquid channel: stiffened-gas water (gamma 4.4, pinf 6e8 Pa over
 # a 1 bar reference pressure, rho 1000 kg/m^3), u = 10 m/s (c = 1625 m/s,
 # M = 0.0062) with +-2 % seeded velocity noise, inflow / outflow / slip walls,
@@ -764,6 +807,10 @@ def main():
                 steady["cpu_baseline"] = {"value": rate, "unit": "node-iterations/s", "cores": procs,
                                           "kind": "reference", "sample": sample, "seconds_per_iteration": per_it,
                                           "gpu_fp64_value": gpu_rate}
+                errs = reference_converged_errors(dev, stream)
+                steady["vs_reference_cpu_solve"] = errs
+                for name in ("fp64", "fp32", "bf16"):
+                    steady[name]["max_rel_err_vs_reference_cpu_solve"] = errs[name]
 
     # ---- the low-Mach liquid channel (stiffened gas, preconditioned Roe)
     lowmach = None

@@ -866,6 +866,23 @@ __global__ void __launch_bounds__(128) k_gs_level(int nrows, const int *__restri
 
 // Per-iteration reset: sum(area*lambda) = 0, extrema = (DBL_MAX, DBL_MIN)
 // (Solver_Steady_Implicit.cpp:45-79).
+// Eigenvalue extrema of a residual pass that a limiter fix may supersede:
+// reset to the empty minimum / maximum, and merged into the call's extrema
+// only when no node failed a check (gate = the fix counters).
+__global__ void k_ext_reset(unsigned long long *__restrict__ e) {
+    const int i = threadIdx.x;
+    if (i < 6) e[i] = (i & 1) ? (unsigned long long)__double_as_longlong(DBL_MIN)
+                              : (unsigned long long)__double_as_longlong(DBL_MAX);
+}
+
+__global__ void k_ext_merge(const int *__restrict__ gate, const unsigned long long *__restrict__ e,
+                            unsigned long long *__restrict__ ext) {
+    const int i = threadIdx.x;
+    if (i >= 6 || gate[0] != 0 || gate[1] != 0) return;
+    if (i & 1) atomicMax(&ext[i], e[i]);
+    else atomicMin(&ext[i], e[i]);
+}
+
 __global__ void k_begin_iteration(int nnode, double *__restrict__ dt, unsigned long long *__restrict__ ext) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < nnode) dt[i] = 0.0;
@@ -973,7 +990,8 @@ static void compute_flow(cfd_ctx *c, int iteration) {
 
 
 template <int FLUX, bool SECOND>
-static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, bool check_pc, const int *gate) {
+static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, bool check_pc, const int *gate,
+                           unsigned long long *ext) {
     if (patch_kernel(c)) {
         const size_t smem = patch_smem_bytes(c->patch_nlocmax, SECOND);
         if (smem > 48 * 1024) {
@@ -988,7 +1006,7 @@ static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, bool check_
             c->nnode, c->ldq, c->Q.p, c->grad.p, c->phi.p, c->xyz.p, c->pe_ptr.p, c->pe_loc.p, c->pe_geo.p,
             c->ph_ptr.p, c->halo.p, c->inc_ptr.p, c->inc.p, c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p, c->bedge_geo.p,
             c->flow, add_time, c->patch_nlocmax, check_roe ? 1 : 0, c->roeflag.p, c->fixcount.p, gate, c->res.p,
-            c->resd.p, c->dt.p, c->ext.p);
+            c->resd.p, c->dt.p, ext);
     } else {
         const bool k0 = SECOND && c->flow.frac == 0.0;
         const int checks = (check_roe ? 1 : 0) | (check_pc ? 2 : 0);
@@ -1001,21 +1019,21 @@ static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, bool check_
         c->flow, add_time, checks, c->roeflag.p, c->fixcount.p, c->res.p, c->resd.p, c->dt.p, c->lgrad.p
         if (lgk) {
             k_residual_gather<FLUX, SECOND, SECOND, true>
-                <<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, c->ext.p);
+                <<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, ext);
         } else if (gate) {
             auto kern = k0 ? k_residual_gather_rerun<FLUX, SECOND, SECOND> : k_residual_gather_rerun<FLUX, SECOND, false>;
             const int grid = std::min(grid_for(c->nnode, 128), 3 * c->nsm);
-            kern<<<grid, 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, gate, c->ext.p);
+            kern<<<grid, 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, gate, ext);
         } else {
             auto kern = k0 ? k_residual_gather<FLUX, SECOND, SECOND> : k_residual_gather<FLUX, SECOND, false>;
-            kern<<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, c->ext.p);
+            kern<<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, ext);
         }
 #undef GATHER_LAUNCH_ARGS
         if (c->nbnode > 0) {
             CFD_LAUNCH_CHECK();
             k_residual_bnd<FLUX><<<grid_for(c->nbnode, 128), 128, 0, c->stream>>>(
                 c->nbnode, c->bnode.p, c->nnode, c->ldq, c->Q.p, c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p,
-                c->bedge_geo.p, c->flow, add_time, gate, c->res.p, c->resd.p, c->dt.p, c->ext.p);
+                c->bedge_geo.p, c->flow, add_time, gate, c->res.p, c->resd.p, c->dt.p, ext);
         }
     }
     CFD_LAUNCH_CHECK();
@@ -1126,7 +1144,7 @@ static int residual_with_fix(cfd_ctx *c, int add_time) {
     // followed by a gated re-evaluation, only when some node failed a check;
     // nothing is read back to the host.  The patch kernel carries only the
     // Roe check, so a pending reconstructed-pressure correction runs first.
-    if (!SECOND) return launch_residual<FLUX, SECOND>(c, add_time, false, false, nullptr);
+    if (!SECOND) return launch_residual<FLUX, SECOND>(c, add_time, false, false, nullptr, c->ext.p);
     if (c->pc_fix_pending && patch_kernel(c)) {
         const bool roe = c->roe_fix_pending;
         c->roe_fix_pending = false;
@@ -1136,8 +1154,14 @@ static int residual_with_fix(cfd_ctx *c, int add_time) {
     }
     const bool check_roe = is_roe_flux(FLUX) && c->roe_fix_pending;
     const bool check_pc = c->pc_fix_pending;
-    int st = launch_residual<FLUX, SECOND>(c, add_time, check_roe, check_pc, nullptr);
-    if (st || !(check_roe || check_pc)) return st;
+    if (!(check_roe || check_pc)) return launch_residual<FLUX, SECOND>(c, add_time, false, false, nullptr, c->ext.p);
+    // The first pass's eigenvalue extrema go to a scratch copy: they count only
+    // when no node fails a check (Compute_Residual sees the fixed limiters
+    // alone); otherwise the gated re-evaluation records them.
+    if (!c->ext_scratch.p) CFD_CUDA(c->ext_scratch.alloc(8));
+    k_ext_reset<<<1, 32, 0, c->stream>>>(c->ext_scratch.p);
+    int st = launch_residual<FLUX, SECOND>(c, add_time, check_roe, check_pc, nullptr, c->ext_scratch.p);
+    if (st) return st;
     const bool redo_roe = check_roe && check_pc;
     if (redo_roe) CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)5 * c->nnode)));
     k_limiter_fix_apply<<<std::min(grid_for(c->nnode, 256), 4 * c->nsm), 256, 0, c->stream>>>(
@@ -1150,7 +1174,9 @@ static int residual_with_fix(cfd_ctx *c, int add_time) {
     }
     c->roe_fix_pending = false;
     c->pc_fix_pending = false;
-    return launch_residual<FLUX, SECOND>(c, add_time, false, false, c->fixcount.p);
+    k_ext_merge<<<1, 32, 0, c->stream>>>(c->fixcount.p, c->ext_scratch.p, c->ext.p);
+    CFD_LAUNCH_CHECK();
+    return launch_residual<FLUX, SECOND>(c, add_time, false, false, c->fixcount.p, c->ext.p);
 }
 
 static Levels *build_levels(const std::vector<int> &IA, const std::vector<int> &JA, int n, bool forward,

@@ -190,6 +190,7 @@ struct cfd_ctx {
     cfd::DevBuf<double> ggw;    // least-squares per-node coefficients [nnode][8]
     int lsq_weight = -1;        // weight the coefficients in ggw were built for
     cfd::DevBuf<unsigned long long> ext;  // 8 extrema as ordered bit patterns
+    cfd::DevBuf<unsigned long long> ext_scratch;  // extrema of a residual pass a limiter fix may redo
     cfd::DevBuf<int> err;       // device error word
     cfd::DevBuf<double> red;    // reduction partials
     cfd::DevBuf<double> red_out;

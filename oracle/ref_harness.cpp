@@ -147,6 +147,25 @@ void ref_update(double relax) {
     }
 }
 
+/* B = -(Res + Res_Diss), the right-hand side of MPFLOW3D's implicit driver
+ * (MPFLOW3D/src/Roe_Jacobian.cpp:237-241), put into Euler3D's block system
+ * after its Compute_Jacobian (which sets B = -Res, Euler3D/src/Roe_Jacobian.cpp),
+ * so that the reference's own implicit loop converges to Res + Res_Diss = 0.
+ * Returns the RMS over the five equations of Res + Res_Diss (the quantity
+ * the loop drives to zero), sqrt(sum / (5 nNode)). */
+double ref_rhs_include_diss(void) {
+    double *c[5] = {Res1, Res2, Res3, Res4, Res5};
+    double *d[5] = {Res1_Diss, Res2_Diss, Res3_Diss, Res4_Diss, Res5_Diss};
+    double s = 0.0;
+    for (int i = 0; i < nNode; i++)
+        for (int k = 0; k < 5; k++) {
+            const double r = c[k][i] + d[k][i];
+            SolverBlockMatrix.B[i][k] = -r;
+            s += r * r;
+        }
+    return sqrt(s / (5.0 * nNode));
+}
+
 /* conv/diss are SoA [5][nNode]. */
 void ref_get_residual(double *conv, double *diss) {
     double *c[5] = {Res1, Res2, Res3, Res4, Res5};

@@ -95,7 +95,7 @@ def _load():
         ("ref_limiter", [], None), ("ref_apply_bc", [C.c_int], None), ("ref_residual", [C.c_int], None),
         ("ref_deltat", [C.c_int], None), ("ref_jacobian", [C.c_int, C.c_int], None),
         ("ref_block_gs", [C.c_int, C.c_int], C.c_double), ("ref_lusgs", [C.c_int], C.c_double),
-        ("ref_update", [C.c_double], None),
+        ("ref_update", [C.c_double], None), ("ref_rhs_include_diss", [], C.c_double),
         ("ref_get_residual", [P, P], None), ("ref_set_residual", [P, P], None),
         ("ref_get_deltat", [P], None), ("ref_set_deltat", [P], None),
         ("ref_get_extrema", [P], None), ("ref_get_farfield", [P], None),
@@ -164,6 +164,8 @@ def _session(mesh_arrays: dict, cfg: dict, Q: np.ndarray | None, steps: list, qu
             out.setdefault("lusgs_rms", []).append(lib.ref_lusgs(*args))
         elif op == "update":
             lib.ref_update(*args)
+        elif op == "rhs_full":
+            out.setdefault("rms_full", []).append(lib.ref_rhs_include_diss())
         elif op == "set_matrix":
             A, B = args
             lib.ref_set_matrix(_p(np.ascontiguousarray(A, np.float64)), _p(np.ascontiguousarray(B, np.float64)))

@@ -12,7 +12,7 @@ import pytest
 
 from cfdsolutions_b200 import Euler3DGPU
 from oracle import refharness
-from tests._util import CFG1, make_case, params_from, relerr, relerr_rows
+from tests._util import CFG1, low_pressure_spots, make_case, params_from, relerr, relerr_rows
 
 TOL = 1e-12
 
@@ -257,3 +257,34 @@ def test_low_mach_fix_residual_and_ghosts_match_reference(gpu_available, ref_ava
     assert relerr_rows(conv, ref["conv"]) <= TOL
     assert relerr_rows(diss, ref["diss"]) <= TOL
     assert relerr(dt, ref["deltat"]) <= TOL
+
+
+@pytest.mark.parametrize("spots", [False, True], ids=["smooth", "limiter-fix"])
+@pytest.mark.parametrize("lorder", [0, 1])
+def test_second_order_extrema_match_reference(gpu_available, ref_available, spots, lorder):
+    """Eigenvalue extrema of a second-order Roe residual (LSQ + Venkatakrishnan)
+    against the reference, also on states with low-pressure spots, where the
+    limiter's pressure corrections fire: the reference evaluates the residual
+    once with the corrected limiters, so the GPU's first pass (before the
+    fixes) must not count (1e-13)."""
+    cfg = dict(CFG1, order=1, limiter=1, limiter_order=lorder, venkat_k=5.0, mach=0.8, mach_min=0.8,
+               alpha_deg=1.25)
+    m, cfg, Q = make_case(n=8, seed=9, cfg=cfg, noise=0.02)
+    if spots:
+        Q = low_pressure_spots(Q, m.nnode, cfg["gamma"], seed=9)
+    ref = refharness.run(m, cfg, Q, [("begin", 0), ("gradient", 0), ("limiter",), ("bc", 0), ("residual", 1),
+                                     ("deltat", 0), ("get", "extrema"), ("get", "limiters"), ("get", "residual")])
+    with Euler3DGPU(m, params_from(cfg)) as s:
+        s.set_state(Q)
+        s.begin_iteration(0)
+        s.Compute_Least_Square_Gradient(0)
+        s.Compute_Limiter()
+        s.Apply_Boundary_Condition(0)
+        s.Compute_Residual(1)
+        s.Compute_DeltaT(0)
+        ext = s.get_extrema()
+        conv, _ = s.get_residual()
+    if spots:
+        assert (ref["limiters"] == 0).all(axis=0).sum() >= 3  # the corrections fired
+    assert relerr_rows(conv, ref["conv"]) <= TOL
+    assert np.abs(ext - ref["extrema"]).max() <= 1e-13 * np.abs(ref["extrema"]).max()
