@@ -28,6 +28,8 @@ PREC_FP64, PREC_FP32, PREC_BF16 = 0, 1, 2
 PC_NONE, PC_BLOCK_JACOBI, PC_ILU0, PC_ILU0_MC = 0, 1, 2, 3
 PREC_LOW_ONLY = 0x10
 JAC_CENTRAL, JAC_FORWARD, JAC_BACKWARD, JAC_ALTERNATE = 0, 1, 2, 3
+RMSFILE_EULER3D, RMSFILE_MPFLOW3D = 0, 1
+VARS_CONSERVATIVE, VARS_RUP, VARS_PUT, VARS_RUT = 0, 1, 2, 3
 BC_EULER_WALL, BC_FAR_FIELD, BC_INFLOW, BC_OUTFLOW = 0, 1, 2, 3
 GS_STATIC_MAX_ROWS = 16384
 PENDING = 1
@@ -135,6 +137,10 @@ SIGNATURES = {
     "cfd_gmres_default": (None, [C.POINTER(GmresOpts)]),
     "cfd_gmres": (I, [P, C.POINTER(GmresOpts), C.POINTER(GmresStats)]),
     "cfd_spmv": (I, [P, I, P, P]),
+    "cfd_rms_file_open": (I, [C.c_char_p, I, I, I, C.POINTER(P)]),
+    "cfd_rms_file_write": (I, [P, I, P, P, P]),
+    "cfd_rms_file_write_ctx": (I, [P, P, I, I]),
+    "cfd_rms_file_close": (I, [P]),
     "cfd_precond_apply": (I, [P, P, P]),
     "cfd_update": (I, [P, D]),
     "cfd_get_residual": (I, [P, P, P]),

@@ -24,7 +24,7 @@ CU_SOURCES = ["core.cu", "gradient.cu", "linsolve.cu", "ilu_mc.cu", "gs_static.c
 # per-file nvcc flags: the finite-difference Jacobian must round every
 # expression as written (no fused multiply-add) to reproduce the reference
 FILE_FLAGS = {"fd_jacobian.cu": ["-fmad=false"]}
-CXX_SOURCES = ["mesh.cpp", "vtk.cpp"]
+CXX_SOURCES = ["mesh.cpp", "vtk.cpp", "rmsio.cpp"]
 HEADERS = ["cfd_internal.h", "ctx.cuh", "kernels.cuh", "physics.cuh", "ilu_mc.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -548,6 +548,34 @@ int  cfd_vtk_write(const char *path, int nnode, const double *coords, int64_t nt
 int  cfd_restart_write(const char *path, int iteration, int nnode, int nghost, const double *Q);
 int  cfd_restart_read(const char *path, int *iteration, int nnode, int nghost, double *Q);
 
+/* ------------------------------------------ residual history (Residual.res)
+ * The text file the reference's RMS writers keep, one line per iteration.
+ *   CFD_RMSFILE_EULER3D  (Euler3D/src/RMSIO.cpp:21-97): iteration, RMS per
+ *     equation, RMS_Res, min/max time step, min/max lambda 1, 4, 5 (and the
+ *     preconditioner's min/max sigma when precond != 0);
+ *   CFD_RMSFILE_MPFLOW3D (MPFLOW3D/src/RMSIO.cpp:21-154): the same with every
+ *     RMS first given normalised by the scale MPFLOW3D accumulates over its
+ *     first five writes.
+ * Header, column names, widths and number formats as the reference's, so the
+ * file is byte-identical for the same values.  variables: the solution
+ * variables the column names refer to (CFD_VARS_*).  cfd_rms_file_write
+ * takes rms[6] as cfd_residual_rms gives it (per equation, then RMS_Res),
+ * extrema[8] in cfd_get_extrema's order and sigma[2] (min, max) when the file
+ * has a preconditioner; cfd_rms_file_write_ctx reads both from a context
+ * (non-preconditioned files).  close writes the closing rule line. */
+#define CFD_RMSFILE_EULER3D  0
+#define CFD_RMSFILE_MPFLOW3D 1
+#define CFD_VARS_CONSERVATIVE 0  /* VARIABLE_CONSERVATIVE / VARIABLE_CON */
+#define CFD_VARS_RUP          1  /* (rho, u, v, w, p) */
+#define CFD_VARS_PUT          2  /* (p, u, v, w, T)   */
+#define CFD_VARS_RUT          3  /* (rho, u, v, w, T) */
+typedef struct cfd_rms_file cfd_rms_file;
+int  cfd_rms_file_open(const char *path, int layout, int variables, int precond, cfd_rms_file **out);
+int  cfd_rms_file_write(cfd_rms_file *f, int iteration, const double rms[6], const double extrema[8],
+                        const double sigma[2]);
+int  cfd_rms_file_write_ctx(cfd_rms_file *f, cfd_ctx *ctx, int iteration, int include_diss);
+int  cfd_rms_file_close(cfd_rms_file *f);
+
 #ifdef __cplusplus
 }
 #endif

@@ -188,6 +188,26 @@ void mpf_update(double relax) {
     }
 }
 
+/* Residual arrays and extrema from the caller, then one RMS_Writer line
+ * (MPFLOW3D/src/RMSIO.cpp:98-154 computes the RMS from Res*_Conv + Res*_Diss);
+ * ext8 = {min/max lambda 1, 4, 5, min/max dt}, sigma2 = min/max sigma. */
+double mpf_rms_write(int iteration, const double *conv, const double *diss, const double *ext8,
+                     const double *sigma2) {
+    double *c[5] = {Res1_Conv, Res2_Conv, Res3_Conv, Res4_Conv, Res5_Conv};
+    double *d[5] = {Res1_Diss, Res2_Diss, Res3_Diss, Res4_Diss, Res5_Diss};
+    for (int k = 0; k < 5; k++) {
+        memcpy(c[k], conv + (size_t)k * nNode, (size_t)nNode * sizeof(double));
+        memcpy(d[k], diss + (size_t)k * nNode, (size_t)nNode * sizeof(double));
+    }
+    MinEigenLamda1 = ext8[0]; MaxEigenLamda1 = ext8[1];
+    MinEigenLamda4 = ext8[2]; MaxEigenLamda4 = ext8[3];
+    MinEigenLamda5 = ext8[4]; MaxEigenLamda5 = ext8[5];
+    MinDeltaT = ext8[6]; MaxDeltaT = ext8[7];
+    MinPrecondSigma = sigma2[0]; MaxPrecondSigma = sigma2[1];
+    return RMS_Writer(iteration);
+}
+void mpf_rms_close(void) { RMS_Writer_Finalize(); }
+
 /* conv/diss: SoA [5][nNode] (Res*_Conv, Res*_Diss). */
 void mpf_get_residual(double *conv, double *diss) {
     double *c[5] = {Res1_Conv, Res2_Conv, Res3_Conv, Res4_Conv, Res5_Conv};

@@ -157,6 +157,7 @@ def _load():
         ("mpf_nnz_blocks", [], C.c_int), ("mpf_get_crs", [P, P, P], None),
         ("mpf_get_matrix", [P, P, P], None), ("mpf_set_matrix", [P, P], None),
         ("mpf_transformation_matrix", [C.c_int, C.c_int, C.c_int, P], None),
+        ("mpf_rms_write", [C.c_int, P, P, P, P], C.c_double), ("mpf_rms_close", [], None),
     ]:
         fn = getattr(lib, name)
         fn.argtypes = args
@@ -206,6 +207,13 @@ def _session(mesh_arrays: dict, cfg: dict, R: np.ndarray | None, steps: list, qu
             out.setdefault("gs_rms", []).append(lib.mpf_block_gs(*args))
         elif op == "update":
             lib.mpf_update(*args)
+        elif op == "rms_write":
+            it, conv, diss, ext8, sig2 = args
+            out.setdefault("rms", []).append(lib.mpf_rms_write(
+                int(it), _p(np.ascontiguousarray(conv, np.float64)), _p(np.ascontiguousarray(diss, np.float64)),
+                _p(np.ascontiguousarray(ext8, np.float64)), _p(np.ascontiguousarray(sig2, np.float64))))
+        elif op == "rms_close":
+            lib.mpf_rms_close()
         elif op == "set_matrix":
             A, B = args
             lib.mpf_set_matrix(_p(np.ascontiguousarray(A, np.float64)), _p(np.ascontiguousarray(B, np.float64)))

@@ -166,6 +166,22 @@ double ref_rhs_include_diss(void) {
     return sqrt(s / (5.0 * nNode));
 }
 
+/* One line of the reference's residual file (RMS_Writer, Euler3D/src/RMSIO.cpp:85-97)
+ * with given values: rms6 = per-equation RMS and RMS_Res; ext8 = {min/max lambda 1,
+ * 4, 5, min/max dt}; sigma2 = min/max preconditioner sigma.  The file is the
+ * Residual.res that Solver_Init opened in the working directory. */
+void ref_rms_write(int iteration, const double *rms6, const double *ext8, const double *sigma2) {
+    double rms[5] = {rms6[0], rms6[1], rms6[2], rms6[3], rms6[4]};
+    RMS_Res = rms6[5];
+    MinEigenLamda1 = ext8[0]; MaxEigenLamda1 = ext8[1];
+    MinEigenLamda4 = ext8[2]; MaxEigenLamda4 = ext8[3];
+    MinEigenLamda5 = ext8[4]; MaxEigenLamda5 = ext8[5];
+    MinDeltaT = ext8[6]; MaxDeltaT = ext8[7];
+    MinPrecondSigma = sigma2[0]; MaxPrecondSigma = sigma2[1];
+    RMS_Writer(iteration, rms);
+}
+void ref_rms_close(void) { RMS_Writer_Finalize(); }
+
 /* conv/diss are SoA [5][nNode]. */
 void ref_get_residual(double *conv, double *diss) {
     double *c[5] = {Res1, Res2, Res3, Res4, Res5};

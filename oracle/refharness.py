@@ -96,6 +96,7 @@ def _load():
         ("ref_deltat", [C.c_int], None), ("ref_jacobian", [C.c_int, C.c_int], None),
         ("ref_block_gs", [C.c_int, C.c_int], C.c_double), ("ref_lusgs", [C.c_int], C.c_double),
         ("ref_update", [C.c_double], None), ("ref_rhs_include_diss", [], C.c_double),
+        ("ref_rms_write", [C.c_int, P, P, P], None), ("ref_rms_close", [], None),
         ("ref_get_residual", [P, P], None), ("ref_set_residual", [P, P], None),
         ("ref_get_deltat", [P], None), ("ref_set_deltat", [P], None),
         ("ref_get_extrema", [P], None), ("ref_get_farfield", [P], None),
@@ -164,6 +165,12 @@ def _session(mesh_arrays: dict, cfg: dict, Q: np.ndarray | None, steps: list, qu
             out.setdefault("lusgs_rms", []).append(lib.ref_lusgs(*args))
         elif op == "update":
             lib.ref_update(*args)
+        elif op == "rms_write":
+            it, rms6, ext8, sig2 = args
+            lib.ref_rms_write(int(it), _p(np.ascontiguousarray(rms6, np.float64)),
+                              _p(np.ascontiguousarray(ext8, np.float64)), _p(np.ascontiguousarray(sig2, np.float64)))
+        elif op == "rms_close":
+            lib.ref_rms_close()
         elif op == "rhs_full":
             out.setdefault("rms_full", []).append(lib.ref_rhs_include_diss())
         elif op == "set_matrix":
@@ -193,6 +200,8 @@ def _session(mesh_arrays: dict, cfg: dict, Q: np.ndarray | None, steps: list, qu
                 g = np.empty((15, nnode)); lib.ref_get_gradients(_p(g)); out["gradients"] = g
             elif what == "limiters":
                 p = np.empty((5, nnode)); lib.ref_get_limiters(_p(p)); out["limiters"] = p
+            elif what == "residual_file":
+                out["residual_file"] = Path("Residual.res").read_bytes() if Path("Residual.res").exists() else b""
             elif what == "matrix":
                 A = np.empty((nnz, 5, 5)); B = np.empty((nnode, 5)); X = np.empty((nnode, 5))
                 lib.ref_get_matrix(_p(A), _p(B), _p(X))
