@@ -162,6 +162,7 @@ SIGNATURES = {
     "cfd_mesh_export": (I, [P, P, P, P, P, P, P, P, P, P]),
     "cfd_mesh_export_cells": (I, [P, P, P, P]),
     "cfd_mesh_write_ugrid": (I, [P, C.c_char_p]),
+    "cfd_mesh_read_ugrid": (I, [C.c_char_p, I, P, I, C.POINTER(P)]),
     "cfd_set_mesh_from": (I, [P, P]),
     "cfd_mesh_free": (None, [P]),
     "cfd_perturbed_freestream": (I, [P, D, D, D, D, D, C.c_uint64, P]),

@@ -14,8 +14,13 @@ struct HostMesh {
     int nnode = 0, nghost = 0, nedge = 0, nbedge = 0;
     std::vector<double> coords;      // [3*nnode] xyz interleaved
     std::vector<int> tets;           // [4*ntet]
-    std::vector<int> tris;           // [3*ntri]
+    std::vector<int> pyrs;           // [5*npyr]   base quad 0-3, apex 4
+    std::vector<int> prisms;         // [6*nprism] triangles 0-1-2 and 3-4-5, sides 0-3, 1-4, 2-5
+    std::vector<int> hexes;          // [8*nhex]   bottom 0-1-2-3, top 4-5-6-7, sides i - i+4
+    std::vector<int> tris;           // [3*ntri]   boundary, outward right-hand normal
     std::vector<int> tri_bc;         // [ntri]
+    std::vector<int> quads;          // [4*nquad]  boundary, outward right-hand normal
+    std::vector<int> quad_bc;        // [nquad]
     std::vector<int> edge_nodes;     // [2*nedge]
     std::vector<double> edge_areav;  // [3*nedge]
     std::vector<int> bedge_nodes;    // [2*nbedge]
@@ -30,6 +35,7 @@ int build_box(HostMesh &m, int nx, int ny, int nz, double lx, double ly, double 
 int build_from_cells(HostMesh &m, int nnode, const double *coords, int64_t ntet, const int *tets,
                      int64_t ntri, const int *tris, const int *tri_bc);
 int write_ugrid(const HostMesh &m, const char *path, const int *tri_tag);
+int read_ugrid(HostMesh &m, const char *path, int ntag, const int *tag_bc, int renumber);
 
 void set_error(const char *fmt, ...);
 

@@ -2081,6 +2081,18 @@ int cfd_mesh_from_cells(int nnode, const double *coords, int64_t ntet, const int
     return CFD_OK;
 }
 
+int cfd_mesh_read_ugrid(const char *path, int ntag, const int *tag_bc, int numbering, cfd_mesh **out) {
+    if (!out || !path || (tag_bc && ntag < 1) || numbering < CFD_NUMBERING_NATURAL ||
+        numbering > CFD_NUMBERING_PATCH_RCM)
+        return CFD_ERR_ARG;
+    *out = nullptr;
+    cfd_mesh *m = new cfd_mesh();
+    int st = read_ugrid(m->m, path, ntag, tag_bc, numbering);
+    if (st) { delete m; return st; }
+    *out = m;
+    return CFD_OK;
+}
+
 int cfd_mesh_sizes(const cfd_mesh *mm, int64_t sizes[7]) {
     if (!mm || !sizes) return CFD_ERR_ARG;
     const HostMesh &m = mm->m;

@@ -51,10 +51,44 @@ inline void cross3(const double *a, const double *b, double *o) {
 }
 inline double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
-// Symmetric node graph of a tet mesh: CRS without diagonal, rows sorted.
-void build_graph(int nnode, const std::vector<int> &tets, std::vector<int> &ia, std::vector<int> &ja) {
-    const int64_t ntet = (int64_t)tets.size() / 4;
-    static const int pairs[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+// Local edges and faces of the volume element types in the node orders
+// above (the geometry of each type; the reference lists the same edges with
+// their two faces in Get_Edge_Nodes_Faces_Connectivity, Area_Volume.cpp:20-458).
+const int kTetEdges[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+const int kPyrEdges[8][2] = {{0, 1}, {0, 3}, {0, 4}, {1, 2}, {1, 4}, {2, 3}, {2, 4}, {3, 4}};
+const int kPrismEdges[9][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 4}, {2, 5}, {3, 4}, {3, 5}, {4, 5}};
+const int kHexEdges[12][2] = {{0, 1}, {0, 3}, {0, 4}, {1, 2}, {1, 5}, {2, 3},
+                              {2, 6}, {3, 7}, {4, 5}, {4, 7}, {5, 6}, {6, 7}};
+struct ElemType {
+    int nnode, nedge, nface;
+    const int (*edges)[2];
+    int face[6][4];  // node lists, -1 padded (triangles)
+};
+const ElemType kPyr = {5, 8, 5, kPyrEdges, {{0, 1, 2, 3}, {0, 1, 4, -1}, {1, 2, 4, -1}, {2, 3, 4, -1}, {3, 0, 4, -1}}};
+const ElemType kPrism = {6, 9, 5, kPrismEdges,
+                         {{0, 1, 2, -1}, {3, 4, 5, -1}, {0, 1, 4, 3}, {1, 2, 5, 4}, {2, 0, 3, 5}}};
+const ElemType kHex = {8, 12, 6, kHexEdges,
+                       {{0, 1, 2, 3}, {4, 5, 6, 7}, {0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {3, 0, 4, 7}}};
+
+// Every element edge of a mesh (tets and the other volume types), as calls
+// fn(a, b) with the two global node ids.
+template <typename F>
+void for_each_element_edge(const HostMesh &m, F fn) {
+    for (size_t t = 0; t + 3 < m.tets.size(); t += 4)
+        for (int p = 0; p < 6; p++) fn(m.tets[t + kTetEdges[p][0]], m.tets[t + kTetEdges[p][1]]);
+    const std::pair<const std::vector<int> *, const ElemType *> types[3] = {
+        {&m.pyrs, &kPyr}, {&m.prisms, &kPrism}, {&m.hexes, &kHex}};
+    for (const auto &tt : types) {
+        const std::vector<int> &v = *tt.first;
+        const ElemType &T = *tt.second;
+        for (size_t c = 0; c + T.nnode <= v.size(); c += T.nnode)
+            for (int p = 0; p < T.nedge; p++) fn(v[c + T.edges[p][0]], v[c + T.edges[p][1]]);
+    }
+}
+
+// Symmetric node graph of a mesh: CRS without diagonal, rows sorted.
+void build_graph(const HostMesh &msh, std::vector<int> &ia, std::vector<int> &ja) {
+    const int nnode = msh.nnode;
     // Upper-neighbour sets with a fixed per-node capacity, grown on overflow.
     int cap = 24;
     std::vector<int> cnt, up;
@@ -62,22 +96,19 @@ void build_graph(int nnode, const std::vector<int> &tets, std::vector<int> &ia, 
         cnt.assign(nnode, 0);
         up.assign((size_t)nnode * cap, -1);
         bool overflow = false;
-        for (int64_t t = 0; t < ntet && !overflow; t++) {
-            const int *v = &tets[4 * t];
-            for (int p = 0; p < 6; p++) {
-                int a = v[pairs[p][0]], b = v[pairs[p][1]];
-                if (a > b) std::swap(a, b);
-                int *row = &up[(size_t)a * cap];
-                int c = cnt[a], k = 0;
-                for (; k < c; k++)
-                    if (row[k] == b) break;
-                if (k == c) {
-                    if (c == cap) { overflow = true; break; }
-                    row[c] = b;
-                    cnt[a] = c + 1;
-                }
+        for_each_element_edge(msh, [&](int a, int b) {
+            if (overflow) return;
+            if (a > b) std::swap(a, b);
+            int *row = &up[(size_t)a * cap];
+            int c = cnt[a], k = 0;
+            for (; k < c; k++)
+                if (row[k] == b) break;
+            if (k == c) {
+                if (c == cap) { overflow = true; return; }
+                row[c] = b;
+                cnt[a] = c + 1;
             }
-        }
+        });
         if (!overflow) break;
         cap *= 2;
     }
@@ -228,7 +259,7 @@ std::vector<int> patch_rcm_order(int n, const std::vector<double> &xyz, const st
 static int build_dual(HostMesh &m) {
     const int nnode = m.nnode;
     const int64_t ntet = (int64_t)m.tets.size() / 4;
-    build_graph(nnode, m.tets, m.n2n_ia, m.n2n_ja);
+    build_graph(m, m.n2n_ia, m.n2n_ja);
 
     // Interior edges = upper half of the graph, ordered by (L, R).
     m.edge_nodes.clear();
@@ -297,9 +328,70 @@ static int build_dual(HostMesh &m) {
         return CFD_ERR_MESH;
     }
 
-    // Boundary edges: one per boundary-triangle vertex, own ghost node.
-    const int64_t ntri = (int64_t)m.tris.size() / 3;
-    m.nbedge = (int)(3 * ntri);
+    // Pyramids, prisms and hexahedra (Area_Volume.cpp:659-822): per element
+    // edge (a, b) the two triangles mid-edge -> face centroid -> element
+    // centroid over the two faces that share the edge, S = (g - m) x (f1 - m) / 2
+    // + (f2 - m) x (g - m) / 2, oriented from the lower to the higher node index;
+    // each end node gets the volumes of the small tetrahedra (node, m, f, g).
+    const std::pair<const std::vector<int> *, const ElemType *> types[3] = {
+        {&m.pyrs, &kPyr}, {&m.prisms, &kPrism}, {&m.hexes, &kHex}};
+    for (const auto &tt : types) {
+        const std::vector<int> &cells = *tt.first;
+        const ElemType &T = *tt.second;
+        // the two faces of each local edge
+        int ef[12][2];
+        for (int p = 0; p < T.nedge; p++) {
+            int k = 0;
+            for (int f = 0; f < T.nface && k < 2; f++) {
+                bool ha = false, hb = false;
+                for (int q = 0; q < 4 && T.face[f][q] >= 0; q++) {
+                    ha |= T.face[f][q] == T.edges[p][0];
+                    hb |= T.face[f][q] == T.edges[p][1];
+                }
+                if (ha && hb) ef[p][k++] = f;
+            }
+        }
+        for (size_t c = 0; c + T.nnode <= cells.size(); c += T.nnode) {
+            const int *v = &cells[c];
+            double g[3] = {0, 0, 0};
+            for (int k = 0; k < T.nnode; k++)
+                for (int d = 0; d < 3; d++) g[d] += m.coords[3 * (size_t)v[k] + d];
+            for (int d = 0; d < 3; d++) g[d] /= T.nnode;
+            for (int p = 0; p < T.nedge; p++) {
+                const int a = v[T.edges[p][0]], b = v[T.edges[p][1]];
+                const double *xa = &m.coords[3 * (size_t)a], *xb = &m.coords[3 * (size_t)b];
+                double mid[3], fc[2][3], rg[3], r1[3], r2[3], s1[3], s2[3], S[3];
+                for (int d = 0; d < 3; d++) mid[d] = (xa[d] + xb[d]) / 2.0;
+                for (int k = 0; k < 2; k++) {
+                    const int *fn = T.face[ef[p][k]];
+                    const int nf = fn[3] >= 0 ? 4 : 3;
+                    for (int d = 0; d < 3; d++) {
+                        double acc = 0.0;
+                        for (int q = 0; q < nf; q++) acc += m.coords[3 * (size_t)v[fn[q]] + d];
+                        fc[k][d] = acc / (double)nf;
+                    }
+                }
+                sub3(g, mid, rg); sub3(fc[0], mid, r1); sub3(fc[1], mid, r2);
+                cross3(rg, r1, s1);
+                cross3(r2, rg, s2);
+                for (int d = 0; d < 3; d++) S[d] = 0.5 * s1[d] + 0.5 * s2[d];
+                const int lo = std::min(a, b), hi = std::max(a, b);
+                double ab[3];
+                sub3(&m.coords[3 * (size_t)hi], &m.coords[3 * (size_t)lo], ab);
+                const double sgn = dot3(S, ab) >= 0.0 ? 1.0 : -1.0;
+                const int e = edge_id(lo, hi);
+                for (int d = 0; d < 3; d++) m.edge_areav[3 * (size_t)e + d] += sgn * S[d];
+                double da[3], db[3];
+                sub3(xa, mid, da); sub3(xb, mid, db);
+                m.cvol[a] += (std::fabs(dot3(da, s1)) + std::fabs(dot3(da, s2))) / 6.0;
+                m.cvol[b] += (std::fabs(dot3(db, s1)) + std::fabs(dot3(db, s2))) / 6.0;
+            }
+        }
+    }
+
+    // Boundary edges: one per boundary-triangle (then -quadrilateral) vertex, own ghost node.
+    const int64_t ntri = (int64_t)m.tris.size() / 3, nquad = (int64_t)m.quads.size() / 4;
+    m.nbedge = (int)(3 * ntri + 4 * nquad);
     m.nghost = m.nbedge;
     m.bedge_nodes.resize((size_t)2 * m.nbedge);
     m.bedge_areav.resize((size_t)3 * m.nbedge);
@@ -320,7 +412,55 @@ static int build_dual(HostMesh &m) {
             m.bedge_type[be] = m.tri_bc[t];
         }
     }
+    // Quadrilaterals (Area_Volume.cpp:556-656): in the reader's reversed order
+    // r = (q3, q2, q1, q0), vertex k gets -(V1 x V2 + V2 x V3) / 2 with V1, V3 to
+    // the midpoints of its edges to r[k+1] and r[k-1] and V2 to the centroid.
+    for (int64_t t = 0; t < nquad; t++) {
+        const int r[4] = {m.quads[4 * t + 3], m.quads[4 * t + 2], m.quads[4 * t + 1], m.quads[4 * t]};
+        double cen[3];
+        for (int d = 0; d < 3; d++)
+            cen[d] = (m.coords[3 * (size_t)r[0] + d] + m.coords[3 * (size_t)r[1] + d] +
+                      m.coords[3 * (size_t)r[2] + d] + m.coords[3 * (size_t)r[3] + d]) / 4.0;
+        for (int k = 0; k < 4; k++) {
+            const double *xn = &m.coords[3 * (size_t)r[k]];
+            const double *xp = &m.coords[3 * (size_t)r[(k + 1) & 3]];
+            const double *xq = &m.coords[3 * (size_t)r[(k + 3) & 3]];
+            double V1[3], V2[3], V3[3], c1[3], c2[3];
+            for (int d = 0; d < 3; d++) {
+                V1[d] = (xn[d] + xp[d]) / 2.0 - xn[d];
+                V2[d] = cen[d] - xn[d];
+                V3[d] = (xn[d] + xq[d]) / 2.0 - xn[d];
+            }
+            cross3(V1, V2, c1);
+            cross3(V2, V3, c2);
+            const int64_t be = 3 * ntri + 4 * t + k;
+            m.bedge_nodes[2 * be] = r[k];
+            m.bedge_nodes[2 * be + 1] = nnode + (int)be;
+            // the reference negates every boundary area afterwards (outward, Area_Volume.cpp:913-915)
+            for (int d = 0; d < 3; d++) m.bedge_areav[3 * be + d] = -1.0 * (0.5 * (c1[d] + c2[d]));
+            m.bedge_type[be] = m.quad_bc[t];
+        }
+    }
     return CFD_OK;
+}
+
+// Node renumbering of a cell mesh (CFD_NUMBERING_*) before its dual is built.
+static void renumber_nodes(HostMesh &m, int renumber) {
+    if (!renumber) return;
+    std::vector<int> ia, ja;
+    build_graph(m, ia, ja);
+    // perm[new] = old
+    std::vector<int> perm = renumber == CFD_NUMBERING_PATCH_RCM
+                                ? patch_rcm_order(m.nnode, m.coords, ia, ja, CFD_PATCH_NODES)
+                                : rcm_order(m.nnode, ia, ja);
+    std::vector<int> inv(m.nnode);
+    for (int i = 0; i < m.nnode; i++) inv[perm[i]] = i;
+    std::vector<double> c2(m.coords.size());
+    for (int i = 0; i < m.nnode; i++)
+        for (int d = 0; d < 3; d++) c2[3 * (size_t)i + d] = m.coords[3 * (size_t)perm[i] + d];
+    m.coords.swap(c2);
+    for (std::vector<int> *cells : {&m.tets, &m.pyrs, &m.prisms, &m.hexes, &m.tris, &m.quads})
+        for (auto &v : *cells) v = inv[v];
 }
 
 // Freudenthal split of hex (i,j,k) into 6 positive tets sharing the diagonal
@@ -397,22 +537,7 @@ int build_box(HostMesh &m, int nx, int ny, int nz, double lx, double ly, double 
             add_quad(nid(i, j, 0), nid(i, j + 1, 0), nid(i + 1, j + 1, 0), nid(i + 1, j, 0), face_bc[4]);
             add_quad(nid(i, j, nz), nid(i + 1, j, nz), nid(i + 1, j + 1, nz), nid(i, j + 1, nz), face_bc[5]);
         }
-    if (renumber) {
-        std::vector<int> ia, ja;
-        build_graph(m.nnode, m.tets, ia, ja);
-        // perm[new] = old
-        std::vector<int> perm = renumber == CFD_NUMBERING_PATCH_RCM
-                                    ? patch_rcm_order(m.nnode, m.coords, ia, ja, CFD_PATCH_NODES)
-                                    : rcm_order(m.nnode, ia, ja);
-        std::vector<int> inv(m.nnode);
-        for (int i = 0; i < m.nnode; i++) inv[perm[i]] = i;
-        std::vector<double> c2(m.coords.size());
-        for (int i = 0; i < m.nnode; i++)
-            for (int d = 0; d < 3; d++) c2[3 * (size_t)i + d] = m.coords[3 * (size_t)perm[i] + d];
-        m.coords.swap(c2);
-        for (auto &v : m.tets) v = inv[v];
-        for (auto &v : m.tris) v = inv[v];
-    }
+    renumber_nodes(m, renumber);
     return build_dual(m);
 }
 
@@ -431,26 +556,112 @@ int build_from_cells(HostMesh &m, int nnode, const double *coords, int64_t ntet,
     return build_dual(m);
 }
 
-// UGRID ASCII writer in the layout UGrid_Reader parses (Euler3D/src/MeshIO.cpp:50-216):
-// counts line, coordinates, 1-based triangles, tags, 1-based tets.  The reader
-// reverses triangle winding (MeshIO.cpp:22-45), so triangles are written with
-// their outward right-hand normal, as this builder stores them.
+// UGRID ASCII (Euler3D/src/MeshIO.cpp:50-216): counts line
+// "nNode nTri nQuad nTet nPyr nPrism nHex", coordinates, 1-based triangles,
+// quadrilaterals, their boundary tags, then the volume cells.  The reader
+// reverses the boundary faces' winding and permutes the pyramid's nodes
+// (UGrid_Translate_Winding, MeshIO.cpp:22-45): a file pyramid (p0..p4) is
+// (p0, p3, p4, p1, p2) in the base-then-apex order used here.  Boundary faces
+// are written with their outward right-hand normal, as this builder stores them.
+namespace {
+const int kPyrFromFile[5] = {0, 3, 4, 1, 2};  // internal[kPyrFromFile[k]] = file[k]
+}
+
 int write_ugrid(const HostMesh &m, const char *path, const int *tri_tag) {
     FILE *f = std::fopen(path, "w");
     if (!f) return CFD_ERR_IO;
-    const int64_t ntri = (int64_t)m.tris.size() / 3, ntet = (int64_t)m.tets.size() / 4;
-    std::fprintf(f, "%d %lld 0 %lld 0 0 0\n", m.nnode, (long long)ntri, (long long)ntet);
+    const int64_t ntri = (int64_t)m.tris.size() / 3, nquad = (int64_t)m.quads.size() / 4;
+    const int64_t ntet = (int64_t)m.tets.size() / 4, npyr = (int64_t)m.pyrs.size() / 5;
+    const int64_t npri = (int64_t)m.prisms.size() / 6, nhex = (int64_t)m.hexes.size() / 8;
+    std::fprintf(f, "%d %lld %lld %lld %lld %lld %lld\n", m.nnode, (long long)ntri, (long long)nquad, (long long)ntet,
+                 (long long)npyr, (long long)npri, (long long)nhex);
     for (int i = 0; i < m.nnode; i++)
         std::fprintf(f, "%.17g %.17g %.17g\n", m.coords[3 * (size_t)i], m.coords[3 * (size_t)i + 1],
                      m.coords[3 * (size_t)i + 2]);
     for (int64_t t = 0; t < ntri; t++)
         std::fprintf(f, "%d %d %d\n", m.tris[3 * t] + 1, m.tris[3 * t + 1] + 1, m.tris[3 * t + 2] + 1);
+    for (int64_t t = 0; t < nquad; t++)
+        std::fprintf(f, "%d %d %d %d\n", m.quads[4 * t] + 1, m.quads[4 * t + 1] + 1, m.quads[4 * t + 2] + 1,
+                     m.quads[4 * t + 3] + 1);
     for (int64_t t = 0; t < ntri; t++) std::fprintf(f, "%d\n", tri_tag ? tri_tag[t] : 1);
+    for (int64_t t = 0; t < nquad; t++) std::fprintf(f, "%d\n", 1);
     for (int64_t t = 0; t < ntet; t++)
         std::fprintf(f, "%d %d %d %d\n", m.tets[4 * t] + 1, m.tets[4 * t + 1] + 1, m.tets[4 * t + 2] + 1,
                      m.tets[4 * t + 3] + 1);
+    for (int64_t t = 0; t < npyr; t++) {
+        int fp[5];
+        for (int k = 0; k < 5; k++) fp[k] = m.pyrs[5 * t + kPyrFromFile[k]] + 1;
+        std::fprintf(f, "%d %d %d %d %d\n", fp[0], fp[1], fp[2], fp[3], fp[4]);
+    }
+    for (int64_t t = 0; t < npri; t++) {
+        const int *v = &m.prisms[6 * t];
+        std::fprintf(f, "%d %d %d %d %d %d\n", v[0] + 1, v[1] + 1, v[2] + 1, v[3] + 1, v[4] + 1, v[5] + 1);
+    }
+    for (int64_t t = 0; t < nhex; t++) {
+        const int *v = &m.hexes[8 * t];
+        std::fprintf(f, "%d %d %d %d %d %d %d %d\n", v[0] + 1, v[1] + 1, v[2] + 1, v[3] + 1, v[4] + 1, v[5] + 1,
+                     v[6] + 1, v[7] + 1);
+    }
     std::fclose(f);
     return CFD_OK;
+}
+
+int read_ugrid(HostMesh &m, const char *path, int ntag, const int *tag_bc, int renumber) {
+    FILE *f = std::fopen(path, "r");
+    if (!f) {
+        set_error("cfd_mesh_read_ugrid: cannot read %s", path);
+        return CFD_ERR_IO;
+    }
+    m = HostMesh();
+    long long n[7];
+    int st = CFD_OK;
+    auto fail = [&](const char *what) {
+        set_error("cfd_mesh_read_ugrid: %s: %s", path, what);
+        st = CFD_ERR_MESH;
+    };
+    if (std::fscanf(f, "%lld %lld %lld %lld %lld %lld %lld", &n[0], &n[1], &n[2], &n[3], &n[4], &n[5], &n[6]) != 7) {
+        fail("bad counts line");
+    } else if (n[0] <= 0 || n[0] > 0x7fffffff / 8 || n[1] < 0 || n[2] < 0 || n[3] < 0 || n[4] < 0 || n[5] < 0 ||
+               n[6] < 0 || (n[3] + n[4] + n[5] + n[6]) == 0) {
+        fail("counts out of range or no volume cells");
+    }
+    auto ints = [&](std::vector<int> &dst, long long count, int per) {
+        dst.resize((size_t)count * per);
+        for (auto &v : dst) {
+            int x;
+            if (std::fscanf(f, "%d", &x) != 1 || x < 1 || x > n[0]) { fail("bad node index"); return; }
+            v = x - 1;
+        }
+    };
+    if (st == CFD_OK) {
+        m.nnode = (int)n[0];
+        m.coords.resize(3 * (size_t)n[0]);
+        for (auto &x : m.coords)
+            if (std::fscanf(f, "%lf", &x) != 1) { fail("bad coordinates"); break; }
+    }
+    if (st == CFD_OK) ints(m.tris, n[1], 3);
+    if (st == CFD_OK) ints(m.quads, n[2], 4);
+    std::vector<int> tags((size_t)(n[1] + n[2]));
+    for (size_t k = 0; st == CFD_OK && k < tags.size(); k++) {
+        if (std::fscanf(f, "%d", &tags[k]) != 1) { fail("bad boundary tag"); break; }
+        if (tag_bc && (tags[k] < 1 || tags[k] > ntag)) { fail("boundary tag without a BC type"); break; }
+    }
+    if (st == CFD_OK) ints(m.tets, n[3], 4);
+    std::vector<int> pf;
+    if (st == CFD_OK) ints(pf, n[4], 5);
+    if (st == CFD_OK) ints(m.prisms, n[5], 6);
+    if (st == CFD_OK) ints(m.hexes, n[6], 8);
+    std::fclose(f);
+    if (st) return st;
+    m.pyrs.resize(pf.size());
+    for (size_t c = 0; c < pf.size(); c += 5)
+        for (int k = 0; k < 5; k++) m.pyrs[c + kPyrFromFile[k]] = pf[c + k];
+    m.tri_bc.resize((size_t)n[1]);
+    m.quad_bc.resize((size_t)n[2]);
+    for (long long k = 0; k < n[1]; k++) m.tri_bc[k] = tag_bc ? tag_bc[tags[k] - 1] : CFD_BC_FAR_FIELD;
+    for (long long k = 0; k < n[2]; k++) m.quad_bc[k] = tag_bc ? tag_bc[tags[n[1] + k] - 1] : CFD_BC_FAR_FIELD;
+    renumber_nodes(m, renumber);
+    return build_dual(m);
 }
 
 }  // namespace cfd

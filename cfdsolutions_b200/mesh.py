@@ -90,6 +90,21 @@ def box_mesh(n: int | tuple[int, int, int], lengths=(1.0, 1.0, 1.0), jitter: flo
         capi.lib.cfd_mesh_free(h)
 
 
+def read_ugrid(path: str, bc_types=None, numbering: int = 0) -> Mesh:
+    """Mixed-element UGRID mesh (tets, pyramids, prisms, hexahedra; boundary
+    triangles and quadrilaterals) and its median dual (``cfd_mesh_read_ugrid``).
+    ``bc_types[t-1]`` is the BC type of boundary tag t (None: far field)."""
+    h = C.c_void_p()
+    tb = None if bc_types is None else np.ascontiguousarray(bc_types, np.int32)
+    capi.check(capi.lib.cfd_mesh_read_ugrid(str(path).encode(), 0 if tb is None else tb.size,
+                                            None if tb is None else capi.ptr(tb), int(numbering), C.byref(h)),
+               "cfd_mesh_read_ugrid")
+    try:
+        return _export(h, False)
+    finally:
+        capi.lib.cfd_mesh_free(h)
+
+
 def from_cells(coords: np.ndarray, tets: np.ndarray, tris: np.ndarray, tri_bc: np.ndarray) -> Mesh:
     coords = np.ascontiguousarray(coords, np.float64)
     tets = np.ascontiguousarray(tets, np.int32)

@@ -458,6 +458,16 @@ int  cfd_mesh_export(const cfd_mesh *m, int *edge_nodes, double *edge_areav,
 int  cfd_mesh_export_cells(const cfd_mesh *m, int *tets, int *tris, int *tri_bc);
 /* UGRID ASCII in the layout of UGrid_Reader (Euler3D/src/MeshIO.cpp:50). */
 int  cfd_mesh_write_ugrid(const cfd_mesh *m, const char *path);
+/* Reads a UGRID ASCII mesh of tetrahedra, pyramids, prisms and hexahedra
+ * with boundary triangles and quadrilaterals (UGrid_Reader,
+ * Euler3D/src/MeshIO.cpp:50-216, its winding translation :22-45) and builds
+ * its median dual as Calculate_Area_Volume (Area_Volume.cpp:461-902): per
+ * element edge the two triangles mid-edge -> face centroid -> cell centroid,
+ * control volumes from the small tetrahedra, one boundary edge and ghost per
+ * boundary-face vertex (triangles first, then quadrilaterals).  Boundary tag t
+ * gets BC type tag_bc[t-1] (the BC file's list, ntag entries; NULL: far field
+ * everywhere).  numbering: CFD_NUMBERING_* applied before the dual is built. */
+int  cfd_mesh_read_ugrid(const char *path, int ntag, const int *tag_bc, int numbering, cfd_mesh **out);
 /* Convenience: cfd_set_mesh from a builder mesh. */
 int  cfd_set_mesh_from(cfd_ctx *ctx, const cfd_mesh *m);
 void cfd_mesh_free(cfd_mesh *m);
