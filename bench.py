@@ -57,14 +57,20 @@ def parse():
     ap.add_argument("--no-serve", action="store_true", help="skip the served batch")
     ap.add_argument("--no-lowmach", action="store_true", help="skip the low-Mach liquid channel solves")
     ap.add_argument("--no-linear", action="store_true", help="skip the linear-algebra kernel rooflines")
-    ap.add_argument("--serve-requests", type=int, default=64)
-    ap.add_argument("--serve-nmax", type=int, default=64, help="largest cube side of the served mix (config: 96)")
-    ap.add_argument("--serve-rate", type=float, default=2.0, help="Poisson arrival rate, requests per second")
-    ap.add_argument("--serve-workers", type=int, default=12)
+    ap.add_argument("--serve-requests", type=int, default=256)
+    ap.add_argument("--serve-nmax", type=int, default=96, help="largest cube side of the served mix")
+    ap.add_argument("--serve-rate", type=float, default=4.0,
+                    help="Poisson arrival rate of the whole mix, requests per second (the latency run takes every "
+                         "other request, so it sees half the rate)")
+    ap.add_argument("--serve-calibration", type=int, default=24, help="requests the autotuner calibrates on")
+    ap.add_argument("--serve-sequential", type=int, default=24,
+                    help="requests of the mix solved one at a time for the sequential FP64 baseline")
     ap.add_argument("--profile-linear", action="store_true",
                     help="small linear-solve case for ncu captures (Jacobian + one GMRES(30) call per precision)")
     ap.add_argument("--profile", action="store_true",
                     help="profiling case for ncu: two residual steps per kernel variant, no timing, no output line")
+    ap.add_argument("--profile-steady", type=int, default=0, metavar="ITERS",
+                    help="run the first ITERS implicit iterations of the steady solve on an --n cube (launch lists)")
     ap.add_argument("--profile-lowmach", type=int, default=0, metavar="ITERS",
                     help="ncu case: ITERS implicit iterations of the low-Mach channel (FP32 Jacobian), no output line")
     return ap.parse_args()
@@ -427,20 +433,32 @@ def serve_requests(count, nmax, rate, seed=7):
     return ns, machs, alphas, arrivals - arrivals[0]
 
 
-def serve_run(ns, machs, alphas, arrivals, workers, precision, dev):
-    """Submits the requests at their arrival times to a server with `workers`
-    concurrent solves (all at once when arrivals is None) and waits for all;
-    returns the results and the wall time from the first submission."""
-    from cfdsolutions_b200 import capi, default_params
-    from cfdsolutions_b200.serve import Server, request, steady_opts
+def serve_request_builder(ns, machs, alphas, precision):
+    """make_request(k, precond_update) of the seeded mix: request k with the
+    steady workload's physics and tolerances."""
+    from cfdsolutions_b200 import default_params
+    from cfdsolutions_b200.serve import request, steady_opts
 
-    reqs = []
-    for k, (n, m, a) in enumerate(zip(ns, machs, alphas)):
-        p = default_params(**dict(STEADY, mach=float(m), mach_min=float(m), alpha_deg=float(a)))
-        reqs.append(request(int(n), p, steady_opts(drop=STEADY_DROP, rtol=STEADY_RTOL, precision=precision,
-                                                   precond_update=STEADY_PC_UPDATE),
-                            mesh_seed=1000 + k, state_seed=2000 + k))
-    with Server(device=dev, workers=workers, budget_bytes=150e9) as srv:
+    def make(k, pu):
+        p = default_params(**dict(STEADY, mach=float(machs[k]), mach_min=float(machs[k]), alpha_deg=float(alphas[k])))
+        return request(int(ns[k]), p, steady_opts(drop=STEADY_DROP, rtol=STEADY_RTOL, precision=precision,
+                                                  precond_update=int(pu)),
+                       mesh_seed=1000 + k, state_seed=2000 + k)
+    return make
+
+
+def serve_run(make, ks, refresh, arrivals, schedule, dev):
+    """Submits requests ks (request k with refresh(k) as its preconditioner
+    refresh period) at their arrival times to a server with the given
+    (workers, batching, window_us) schedule -- all at once when arrivals are
+    zeros, one at a time (waiting for each) when arrivals is None -- and waits
+    for all; returns the results, the wall time from the first submission,
+    the peak reservation and the fused-launch counts."""
+    from cfdsolutions_b200.serve import Server
+
+    workers, batching, window = schedule
+    reqs = [make(k, refresh(k)) for k in ks]
+    with Server(device=dev, workers=workers, budget_bytes=150e9, batching=batching, window_us=window) as srv:
         t0 = time.perf_counter()
         if arrivals is None:  # sequential: one request at a time
             res = []
@@ -456,7 +474,8 @@ def serve_run(ns, machs, alphas, arrivals, workers, precision, dev):
             res = [srv.wait(i) for i in ids]
         wall = time.perf_counter() - t0
         peak = srv.stats()["peak_reserved_bytes"]
-    return res, wall, peak
+        fused = srv.batch_stats()
+    return res, wall, peak, fused
 
 
 def cpu_count():
@@ -585,6 +604,29 @@ def profile_lowmach_case(iters):
         ss.synchronize()
 
 
+def profile_steady_case(n, iters):
+    """`--profile-steady ITERS --n N`: the first ITERS implicit iterations of
+    the steady workload on an N^3 cube, FP64 then the FP32
+    low-precision-only system, for launch lists."""
+    from cfdsolutions_b200 import Euler3DGPU, box_mesh, capi, default_params, perturbed_freestream
+    from cfdsolutions_b200.mesh import NUMBERING_PATCH_RCM
+
+    m = box_mesh(n, jitter=0.15, seed=1234, rcm=NUMBERING_PATCH_RCM)
+    Q = perturbed_freestream(m, CFG["gamma"], CFG["mach"], CFG["alpha_deg"], noise=0.01, seed=1235)
+    for prec in (capi.PREC_FP64, capi.PREC_FP32 | capi.PREC_LOW_ONLY):
+        with Euler3DGPU(m, default_params(**STEADY)) as ss:
+            ss.set_state(Q)
+            capi.check(capi.lib.cfd_ilu_mc_order(ss.handle, None, None), "cfd_ilu_mc_order")
+            g = capi.GmresOpts(30, 30, STEADY_RTOL, capi.PC_ILU0_MC, prec, 1)
+            ss.synchronize()
+            t0 = time.perf_counter()
+            ss.solve_steady(max_iterations=iters, drop=STEADY_DROP, include_diss=1, linear_solver=1, gmres=g,
+                            precond_update=STEADY_PC_UPDATE)
+            ss.synchronize()
+            print(f"profile-steady precision {prec}: {iters} implicit iterations in "
+                  f"{time.perf_counter() - t0:.3f} s", flush=True)
+
+
 def profile_linear_case(n):
     """Small fixed case for ncu captures of the linear solver
     (`--profile-linear --n 64`): the steady workload's Jacobian at CFL 1000 on
@@ -629,6 +671,9 @@ def main():
         return
     if args.profile_lowmach:
         profile_lowmach_case(args.profile_lowmach)
+        return
+    if args.profile_steady:
+        profile_steady_case(args.n, args.profile_steady)
         return
     if args.profile_linear:
         profile_linear_case(args.n)
@@ -823,18 +868,32 @@ def main():
             lowmach["cpu_baseline"] = {"value": rate, "unit": "node-iterations/s", "cores": 1, "kind": "port",
                                        "sample": sample, "seconds_per_iteration": per_it, "gpu_fp64_value": gpu_rate}
 
-    # ---- served batch (continuous admission) vs sequential plain FP64 solves
+    # ---- served batch (config 5: continuous admission, fused residual launches,
+    # autotuned schedule) vs sequential plain FP64 solves
     serve = None
     if not args.no_serve:
         from cfdsolutions_b200 import capi
+        from cfdsolutions_b200.serve import SIZE_BUCKETS, autotune, size_bucket
         ns, machs, alphas, arr = serve_requests(args.serve_requests, args.serve_nmax, args.serve_rate)
         mixed = capi.PREC_FP32 | capi.PREC_LOW_ONLY
+        make = serve_request_builder(ns, machs, alphas, mixed)
+        make64 = serve_request_builder(ns, machs, alphas, capi.PREC_FP64)
+        calib = list(range(0, len(ns), max(1, len(ns) // args.serve_calibration)))[:args.serve_calibration]
         barrier()
-        res, wall, peak = serve_run(ns, machs, alphas, arr, args.serve_workers, mixed, dev)  # at the stated rate
+        tune = autotune(make, calib, device=dev)
+        refresh = lambda k: tune["precond_update"].get(size_bucket(int(ns[k])), STEADY_PC_UPDATE)  # noqa: E731
+        sched = tune["server"]
+        every = list(range(len(ns)))
         barrier()
-        sat, sat_wall, sat_peak = serve_run(ns, machs, alphas, np.zeros(len(ns)), args.serve_workers, mixed, dev)
+        # latency at the stated rate: every other request of the mix, arriving at their Poisson offsets
+        at_rate = every[::2]
+        res, wall, peak, fused = serve_run(make, at_rate, refresh, arr[::2], sched, dev)
         barrier()
-        seq, seq_wall, _ = serve_run(ns, machs, alphas, None, 1, capi.PREC_FP64, dev)
+        sat, sat_wall, sat_peak, sat_fused = serve_run(make, every, refresh, np.zeros(len(ns)), sched, dev)
+        barrier()
+        # sequential plain FP64 on a seeded subsample of the same mix (every k-th request)
+        seq_ks = every[::max(1, len(ns) // args.serve_sequential)][:args.serve_sequential]
+        seq, seq_wall, _, _ = serve_run(make64, seq_ks, lambda k: STEADY_PC_UPDATE, None, (1, False, 0.0), dev)
         # host wall clocks of the replicas' servers: the slowest rank sets each rate
         wall, sat_wall, seq_wall = (max_over_ranks(w, world, f"cuda:{dev}") for w in (wall, sat_wall, seq_wall))
         lat = np.array([r.latency for r in res])
@@ -844,10 +903,21 @@ def main():
         serve = {
             "metric": "served steady solves", "unit": "solves/s",
             "config": {"requests": args.serve_requests, "cube_side": f"log-uniform in [16, {args.serve_nmax}] hexes",
-                       "mach": "U[0.3, 0.85]", "alpha_deg": "U[-5, 10]", "arrivals": f"Poisson, {args.serve_rate}/s",
-                       "workers": args.serve_workers, "budget_gb": 150.0, "physics": "as steady",
+                       "mach": "U[0.3, 0.85]", "alpha_deg": "U[-5, 10]",
+                       "arrivals": f"capacity: all {len(ns)} at once; latency: every other request of the mix "
+                                   f"({len(at_rate)}) at Poisson arrivals of {args.serve_rate / 2:g}/s",
+                       "budget_gb": 150.0, "physics": "as steady",
                        "served_precision": "fp32 low-precision-only Jacobian + ILU(0)",
-                       "sequential": "plain fp64 solves one at a time through the same server (1 worker)"},
+                       "sequential": f"plain fp64 solves one at a time through the same server (1 worker, no "
+                                     f"fusion) on {len(seq_ks)} requests of the mix (every "
+                                     f"{max(1, len(ns) // args.serve_sequential)}th)"},
+            "autotuner": {"calibration_requests": len(calib), "workers": sched[0], "fused_residual_and_spmv_launches": sched[1],
+                          "window_us": sched[2],
+                          "precond_update_by_cube_side": {f"[{SIZE_BUCKETS[b][0]}, {min(SIZE_BUCKETS[b][1], 97)})": v
+                                                          for b, v in tune["precond_update"].items()},
+                          "timings": tune["timings"]},
+            # launches over a request table in the saturated run, and the requests' jobs they carried
+            "fused_launches": sat_fused,
             # capacity: all requests submitted at once; latency: at the stated arrival rate
             "value": aggregate_rate(len(sat), sat_wall, world), "wall_s": sat_wall,
             "saturated_p50_s": float(np.percentile(sat_lat, 50)), "saturated_p99_s": float(np.percentile(sat_lat, 99)),

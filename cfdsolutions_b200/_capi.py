@@ -173,6 +173,8 @@ SIGNATURES = {
     "cfd_server_state": (I, [P, I64, P]),
     "cfd_server_release": (I, [P, I64]),
     "cfd_server_stats": (I, [P, P]),
+    "cfd_server_set_batching": (I, [P, I, D]),
+    "cfd_server_batch_stats": (I, [P, P]),
     "cfd_server_destroy": (I, [P]),
     "cfd_restart_write": (I, [C.c_char_p, I, I, I, P]),
     "cfd_restart_read": (I, [C.c_char_p, C.POINTER(I), I, I, P]),

@@ -255,6 +255,52 @@ __global__ void __launch_bounds__(128, 3) k_residual_gather_rerun(GATHER_PARAMS,
     if (add_time) block_extrema3(mn, mx, ext);
 }
 
+// One launch of the gather residual over several contexts (a request table):
+// block b belongs to the job whose [block_begin, block_begin + ceil(nnode/128))
+// range holds it, and its threads run exactly the per-node code of
+// k_residual_gather on that job's arrays and parameters, so every node's
+// residual is bit-identical to the job's own launch.  The serving loop uses it
+// to fuse the interior residuals of the requests it runs side by side.
+template <int FLUX, bool SECOND, bool KAPPA0, bool LG>
+__global__ void __launch_bounds__(128, 3) k_residual_gather_batch(const __grid_constant__ GatherBatch B) {
+    int j = 0;
+    while (j + 1 < B.njobs && (int)blockIdx.x >= B.job[j + 1].block_begin) j++;
+    const GatherJob &J = B.job[j];
+    const int i = ((int)blockIdx.x - J.block_begin) * blockDim.x + threadIdx.x;
+    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
+    if (i < J.nnode)
+        residual_gather_node<FLUX, SECOND, KAPPA0, LG>(i, J.nnode, J.ldq, J.Q, J.grad, J.phi, J.xyz, J.sell_ptr,
+                                                        J.sell_nbr, J.sell_geo, J.deg, J.f, J.add_time, J.checks,
+                                                        J.roeflag, J.fixcount, J.res, J.resd, J.dtsum, J.lgrad, mn,
+                                                        mx);
+    if (J.add_time) block_extrema3(mn, mx, J.ext);
+}
+
+template <int FLUX>
+static int launch_gather_batch_flux(int key, const GatherBatch &b, cudaStream_t s) {
+    int blocks = 0;
+    for (int k = 0; k < b.njobs; k++) blocks += grid_for(b.job[k].nnode, 128);
+    if (blocks == 0) return CFD_OK;
+    switch (key & 7) {
+        case 0: k_residual_gather_batch<FLUX, false, false, false><<<blocks, 128, 0, s>>>(b); break;
+        case 4: k_residual_gather_batch<FLUX, true, false, false><<<blocks, 128, 0, s>>>(b); break;
+        case 6: k_residual_gather_batch<FLUX, true, true, false><<<blocks, 128, 0, s>>>(b); break;
+        case 7: k_residual_gather_batch<FLUX, true, true, true><<<blocks, 128, 0, s>>>(b); break;
+        default: return CFD_ERR_UNSUPPORTED;
+    }
+    CFD_LAUNCH_CHECK();
+    return CFD_OK;
+}
+
+int launch_gather_batch(int key, const GatherBatch &b, cudaStream_t s) {
+    switch (key >> 3) {
+        case CFD_FLUX_ROE: return launch_gather_batch_flux<CFD_FLUX_ROE>(key, b, s);
+        case CFD_FLUX_HLLC: return launch_gather_batch_flux<CFD_FLUX_HLLC>(key, b, s);
+        case CFD_FLUX_AUSM: return launch_gather_batch_flux<CFD_FLUX_AUSM>(key, b, s);
+        default: return CFD_ERR_UNSUPPORTED;
+    }
+}
+
 // Boundary edges of the gather residual: first order, flux into node_L only
 // (FluxTest.cpp:8044-8098).  One thread per node that has boundary edges
 // (`bnode`, increasing), launched after k_residual_gather: it continues the
@@ -1017,7 +1063,15 @@ static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, bool check_
 #define GATHER_LAUNCH_ARGS                                                                                          \
     c->nnode, c->ldq, c->Q.p, c->grad.p, c->phi.p, c->xyz.p, c->sell_ptr.p, c->sell_nbr.p, c->sell_geo.p, c->deg.p, \
         c->flow, add_time, checks, c->roeflag.p, c->fixcount.p, c->res.p, c->resd.p, c->dt.p, c->lgrad.p
-        if (lgk) {
+        const int key = batch_key(FLUX, SECOND, k0, lgk);
+        if (!gate && c->batcher && key >= 0) {
+            // the serving loop fuses this launch with other requests' (bit-identical per node)
+            GatherJob job{c->nnode, c->ldq, c->Q.p, c->grad.p, c->phi.p, c->xyz.p, c->sell_ptr.p, c->sell_nbr.p,
+                          c->sell_geo.p, c->deg.p, c->flow, add_time, checks, c->roeflag.p, c->fixcount.p,
+                          c->res.p, c->resd.p, c->dt.p, lgk ? c->lgrad.p : nullptr, ext, 0};
+            const int st = c->batch_submit(c->batcher, c, key, &job);
+            if (st) return st;
+        } else if (lgk) {
             k_residual_gather<FLUX, SECOND, SECOND, true>
                 <<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, ext);
         } else if (gate) {

@@ -113,8 +113,66 @@ struct Abmc {
 
 }  // namespace cfd
 
+namespace cfd {
+// One request's interior gather residual as a job of a fused launch
+// (k_residual_gather_batch): the arguments of k_residual_gather.
+struct GatherJob {
+    int nnode;
+    int64_t ldq;
+    const double *Q, *grad, *phi, *xyz;
+    const int64_t *sell_ptr;
+    const int *sell_nbr;
+    const double4 *sell_geo;
+    const int *deg;
+    Flow f;
+    int add_time, checks;
+    int *roeflag, *fixcount;
+    double *res, *resd, *dtsum;
+    const double *lgrad;
+    unsigned long long *ext;
+    int block_begin;  // first CTA of this job in the fused grid
+};
+constexpr int kBatchMax = 16;
+struct GatherBatch {
+    GatherJob job[kBatchMax];
+    int njobs;
+};
+static_assert(sizeof(GatherBatch) <= 32000, "the job table is passed as a kernel parameter");
+// key of the kernel instantiation a job needs: (FLUX, second order, frac = 0,
+// limited gradients); -1 when the fused launch does not carry that flux
+inline int batch_key(int flux, bool second, bool k0, bool lg) {
+    if (flux != CFD_FLUX_ROE && flux != CFD_FLUX_HLLC && flux != CFD_FLUX_AUSM) return -1;
+    return (flux << 3) | (second ? 4 : 0) | (k0 ? 2 : 0) | (lg ? 1 : 0);
+}
+int launch_gather_batch(int key, const GatherBatch &b, cudaStream_t s);
+
+// One request's block SpMV y = A x as a job of a fused launch
+// (k_bspmv_batch): A in the storage type of the key.
+struct SpmvJob {
+    int nrow;
+    const int *IA, *JA;
+    const void *A;
+    const double *x;
+    double *y;
+    int block_begin;  // first CTA of this job in the fused grid
+};
+struct SpmvBatch {
+    SpmvJob job[kBatchMax];
+    int njobs;
+};
+// keys of the fused SpMV launches: kSpmvKey + CFD_PREC_FP64 / FP32 / BF16
+constexpr int kSpmvKey = 64;
+int launch_spmv_batch(int key, const SpmvBatch &b, cudaStream_t s);
+}  // namespace cfd
+
 struct cfd_ctx {
     int device = 0;
+    // serving: a fuser of the interior residual and block SpMV launches of
+    // several contexts (nullptr: launches of its own); batch_submit takes a
+    // GatherJob (key < kSpmvKey) or an SpmvJob and returns once the fused
+    // launch is enqueued and this context's stream waits for it
+    void *batcher = nullptr;
+    int (*batch_submit)(void *batcher, cfd_ctx *c, int key, const void *job) = nullptr;
     int nsm = 148;  // SMs of the device (grids of the gated, usually empty passes)
     cudaStream_t stream = nullptr;
     cfd_params params{};

@@ -75,66 +75,162 @@ __device__ __forceinline__ void two_sum(double a, double b, double &s, double &e
     e = (a - (s - z)) + (b - z);
 }
 
-// Dot2 of k vectors V[j] (stride ld) against w, one (sum, compensation)
-// pair per vector per block.  Vectors are taken MD_CHUNK at a time so w is
-// read once per chunk.  Per vector: thread-strided compensated sums, then a
-// warp butterfly and a combine over the block's warps (error-free TwoSum is
-// symmetric in its arguments, so every lane of the butterfly holds the same
-// pair); the order depends only on the grid, so results repeat run to run.
+// One product of a Dot2 sum: (s, c) += x * b with TwoProd and TwoSum.
+__device__ __forceinline__ void dot2_acc(double x, double b, double &s, double &c) {
+    const double p = x * b;
+    const double pe = fma(x, b, -p);
+    double t, e;
+    two_sum(s, p, t, e);
+    s = t;
+    c += e + pe;
+}
+
 constexpr int MAXK = 64;
-constexpr int MD_CHUNK = 8;
 constexpr int MD_THREADS = 256;
+
+// The block's CH (sum, compensation) pairs of vectors j0 .. j0+nj-1 combined
+// and stored in part[block][j]: a warp butterfly (error-free TwoSum is
+// symmetric in its arguments, so every lane holds the same pair), then the
+// warps in order.
+template <int CH>
+__device__ __forceinline__ void dot2_block_store(double (&s)[CH], double (&c)[CH], int j0, int nj,
+                                                 double (*shs)[MD_THREADS / 32], double (*shc)[MD_THREADS / 32],
+                                                 double *__restrict__ part) {
+    constexpr int NW = MD_THREADS / 32;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int jj = 0; jj < CH; jj++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double so = __shfl_xor_sync(0xffffffffu, s[jj], o);
+            const double co = __shfl_xor_sync(0xffffffffu, c[jj], o);
+            double t, e;
+            two_sum(s[jj], so, t, e);
+            s[jj] = t;
+            c[jj] = (c[jj] + co) + e;
+        }
+        if (lane == 0) { shs[jj][wid] = s[jj]; shc[jj][wid] = c[jj]; }
+    }
+    __syncthreads();
+    if (wid == 0 && lane < nj) {
+        double ss = shs[lane][0], cc = shc[lane][0];
+        for (int q = 1; q < NW; q++) {
+            double t, e;
+            two_sum(ss, shs[lane][q], t, e);
+            ss = t;
+            cc = (cc + shc[lane][q]) + e;
+        }
+        part[(blockIdx.x * MAXK + j0 + lane) * 2] = ss;
+        part[(blockIdx.x * MAXK + j0 + lane) * 2 + 1] = cc;
+    }
+    __syncthreads();
+}
+
+// Dot2 of k vectors V[j] (stride ld) against w, one (sum, compensation)
+// pair per vector per block.  Vectors are taken CH at a time (w is read
+// once per chunk); each thread takes the elements i, i + G, i + 2G, ... of
+// the grid G in that order, U of them per step with all their loads issued
+// before the sums, so that U (CH + 1) loads are in flight per thread.  A
+// vector's sum does not depend on CH or U: only on the grid, so results
+// repeat run to run and between the instantiations.
+template <int CH, int U>
 __global__ void __launch_bounds__(MD_THREADS) k_mdot_partial(const double *__restrict__ V, int64_t ld, int k,
                                                              const double *__restrict__ w, int64_t n,
                                                              double *__restrict__ part) {
-    constexpr int NW = MD_THREADS / 32;
-    __shared__ double shs[MD_CHUNK][NW], shc[MD_CHUNK][NW];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int j0 = 0; j0 < k; j0 += MD_CHUNK) {
-        const int nj = min(MD_CHUNK, k - j0);
-        double s[MD_CHUNK], c[MD_CHUNK];
+    __shared__ double shs[CH][MD_THREADS / 32], shc[CH][MD_THREADS / 32];
+    const int64_t G = (int64_t)gridDim.x * blockDim.x;
+    for (int j0 = 0; j0 < k; j0 += CH) {
+        const int nj = min(CH, k - j0);
+        double s[CH], c[CH];
 #pragma unroll
-        for (int jj = 0; jj < MD_CHUNK; jj++) { s[jj] = 0.0; c[jj] = 0.0; }
-        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        for (int jj = 0; jj < CH; jj++) { s[jj] = 0.0; c[jj] = 0.0; }
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        for (; i + (U - 1) * G < n; i += U * G) {
+            double b[U], a[U][CH];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                b[u] = w[i + u * G];
+#pragma unroll
+                for (int jj = 0; jj < CH; jj++)
+                    if (jj < nj) a[u][jj] = V[(int64_t)(j0 + jj) * ld + i + u * G];
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++)
+#pragma unroll
+                for (int jj = 0; jj < CH; jj++)
+                    if (jj < nj) dot2_acc(a[u][jj], b[u], s[jj], c[jj]);
+        }
+        for (; i < n; i += G) {
             const double b = w[i];
 #pragma unroll
-            for (int jj = 0; jj < MD_CHUNK; jj++)
-                if (jj < nj) {
-                    const double a = V[(int64_t)(j0 + jj) * ld + i];
-                    const double p = a * b;
-                    const double pe = fma(a, b, -p);
-                    double t, e;
-                    two_sum(s[jj], p, t, e);
-                    s[jj] = t;
-                    c[jj] += e + pe;
+            for (int jj = 0; jj < CH; jj++)
+                if (jj < nj) dot2_acc(V[(int64_t)(j0 + jj) * ld + i], b, s[jj], c[jj]);
+        }
+        dot2_block_store<CH>(s, c, j0, nj, shs, shc, part);
+    }
+}
+
+// A Gram-Schmidt update and the next reduction in one pass over w:
+// w_i -= h_0 V_0i, then h_1 V_1i, ... (one fused multiply-add each, in j
+// order), then the Dot2 partials of <V_j, w> for j < k or, SELF, of <w, w>,
+// with k_mdot_partial's element order.  Each element's update is made and
+// stored by the thread that reads it back in the later chunks, so the
+// results are bit for bit those of the update followed by k_mdot_partial,
+// with V read from DRAM once (k <= CH) instead of twice and w once instead
+// of three times.
+template <bool SELF, int CH, int U>
+__global__ void __launch_bounds__(MD_THREADS) k_axpy_mdot_partial(const double *__restrict__ V, int64_t ld, int k,
+                                                                  const double *__restrict__ h, double *__restrict__ w,
+                                                                  int64_t n, double *__restrict__ part) {
+    __shared__ double shs[CH][MD_THREADS / 32], shc[CH][MD_THREADS / 32];
+    __shared__ double hs[MAXK];
+    for (int j = threadIdx.x; j < k; j += blockDim.x) hs[j] = h[j];
+    __syncthreads();
+    const int64_t G = (int64_t)gridDim.x * blockDim.x;
+    const int kd = SELF ? 1 : k;
+    for (int j0 = 0; j0 < kd; j0 += CH) {
+        const int nj = min(CH, kd - j0);
+        double s[CH], c[CH];
+#pragma unroll
+        for (int jj = 0; jj < CH; jj++) { s[jj] = 0.0; c[jj] = 0.0; }
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        for (; i + (U - 1) * G < n; i += U * G) {
+            double b[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) b[u] = w[i + u * G];
+            if (j0 == 0) {
+#pragma unroll 2
+                for (int j = 0; j < k; j++) {
+                    double v[U];
+#pragma unroll
+                    for (int u = 0; u < U; u++) v[u] = V[(int64_t)j * ld + i + u * G];
+#pragma unroll
+                    for (int u = 0; u < U; u++) b[u] -= hs[j] * v[u];
                 }
-        }
 #pragma unroll
-        for (int jj = 0; jj < MD_CHUNK; jj++) {
+                for (int u = 0; u < U; u++) w[i + u * G] = b[u];
+            }
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const double so = __shfl_xor_sync(0xffffffffu, s[jj], o);
-                const double co = __shfl_xor_sync(0xffffffffu, c[jj], o);
-                double t, e;
-                two_sum(s[jj], so, t, e);
-                s[jj] = t;
-                c[jj] = (c[jj] + co) + e;
-            }
-            if (lane == 0) { shs[jj][wid] = s[jj]; shc[jj][wid] = c[jj]; }
+            for (int u = 0; u < U; u++)
+#pragma unroll
+                for (int jj = 0; jj < CH; jj++)
+                    if (jj < nj) {
+                        // V_j again: the same thread has just read it (an L1 hit)
+                        const double x = SELF ? b[u] : V[(int64_t)(j0 + jj) * ld + i + u * G];
+                        dot2_acc(x, b[u], s[jj], c[jj]);
+                    }
         }
-        __syncthreads();
-        if (wid == 0 && lane < nj) {
-            double ss = shs[lane][0], cc = shc[lane][0];
-            for (int q = 1; q < NW; q++) {
-                double t, e;
-                two_sum(ss, shs[lane][q], t, e);
-                ss = t;
-                cc = (cc + shc[lane][q]) + e;
+        for (; i < n; i += G) {
+            double b = w[i];
+            if (j0 == 0) {
+                for (int j = 0; j < k; j++) b -= hs[j] * V[(int64_t)j * ld + i];
+                w[i] = b;
             }
-            part[(blockIdx.x * MAXK + j0 + lane) * 2] = ss;
-            part[(blockIdx.x * MAXK + j0 + lane) * 2 + 1] = cc;
+#pragma unroll
+            for (int jj = 0; jj < CH; jj++)
+                if (jj < nj) dot2_acc(SELF ? b : V[(int64_t)(j0 + jj) * ld + i], b, s[jj], c[jj]);
         }
-        __syncthreads();
+        dot2_block_store<CH>(s, c, j0, nj, shs, shc, part);
     }
 }
 
@@ -176,10 +272,30 @@ static const int kRedBlocks = 1184;  // 8 x 148 SMs
 constexpr int DOT_H1 = MAXK, DOT_H2 = 2 * MAXK, DOT_COL = 3 * MAXK, DOT_NRM = 4 * MAXK, DOT_LEN = 5 * MAXK;
 
 // out_dev[j] = <V_j, w>, j < k, compensated, deterministic; stays on the device.
+// The chunk width follows k and the elements per step shrink as it grows, to
+// keep the registers (and so the resident blocks) and the loads in flight up.
 static int mdot_dev(cfd_ctx *c, const double *V, int64_t ld, int k, const double *w, int64_t n, double *out_dev) {
-    k_mdot_partial<<<kRedBlocks, MD_THREADS, 0, c->stream>>>(V, ld, k, w, n, c->red.p);
+    if (k <= 1) k_mdot_partial<1, 8><<<kRedBlocks, MD_THREADS, 0, c->stream>>>(V, ld, k, w, n, c->red.p);
+    else if (k <= 4) k_mdot_partial<4, 4><<<kRedBlocks, MD_THREADS, 0, c->stream>>>(V, ld, k, w, n, c->red.p);
+    else k_mdot_partial<8, 2><<<kRedBlocks, MD_THREADS, 0, c->stream>>>(V, ld, k, w, n, c->red.p);
     CFD_LAUNCH_CHECK();
     k_mdot_final<<<k, 256, 0, c->stream>>>(c->red.p, kRedBlocks, k, out_dev);
+    CFD_LAUNCH_CHECK();
+    return CFD_OK;
+}
+
+// w -= V h (h = h_dev[0..k) on the device), then out_dev[j] = <V_j, w>
+// (j < k) or, self, out_dev[0] = <w, w>: the update and mdot_dev in one pass.
+static int axpy_mdot_dev(cfd_ctx *c, const double *V, int64_t ld, int k, const double *h_dev, double *w, int64_t n,
+                         bool self, double *out_dev) {
+    const int g = kRedBlocks, t = MD_THREADS;
+    double *part = c->red.p;
+    if (self) k_axpy_mdot_partial<true, 1, 4><<<g, t, 0, c->stream>>>(V, ld, k, h_dev, w, n, part);
+    else if (k <= 4) k_axpy_mdot_partial<false, 4, 4><<<g, t, 0, c->stream>>>(V, ld, k, h_dev, w, n, part);
+    else k_axpy_mdot_partial<false, 8, 2><<<g, t, 0, c->stream>>>(V, ld, k, h_dev, w, n, part);
+    CFD_LAUNCH_CHECK();
+    const int kd = self ? 1 : k;
+    k_mdot_final<<<kd, 256, 0, c->stream>>>(c->red.p, kRedBlocks, kd, out_dev);
     CFD_LAUNCH_CHECK();
     return CFD_OK;
 }
@@ -211,16 +327,6 @@ __global__ void k_arnoldi_column(int j, double *__restrict__ dots) {
 }
 
 // --------------------------------------------------------- vector kernels
-
-__global__ void k_axpy_multi(int64_t n, int k, const double *__restrict__ V, int64_t ld, const double *__restrict__ h,
-                             double *__restrict__ w) {
-    // w -= sum_j h_j V_j
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        double s = w[i];
-        for (int j = 0; j < k; j++) s -= h[j] * V[(int64_t)j * ld + i];
-        w[i] = s;
-    }
-}
 
 __global__ void k_scale_copy(int64_t n, double a, const double *__restrict__ x, double *__restrict__ y) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -275,11 +381,11 @@ __device__ __forceinline__ double ldA<float>(const float *p) { return (double)__
 template <>
 __device__ __forceinline__ double ldA<uint16_t>(const uint16_t *p) { return load_low(p); }
 
+// thread t of a block SpMV: row t/5, component t%5
 template <typename TA>
-__global__ void __launch_bounds__(160) k_bspmv(int nrow, const int *__restrict__ IA, const int *__restrict__ JA,
-                                               const TA *__restrict__ A, const double *__restrict__ x,
-                                               double *__restrict__ y) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void bspmv_thread(int t, int nrow, const int *__restrict__ IA, const int *__restrict__ JA,
+                                             const TA *__restrict__ A, const double *__restrict__ x,
+                                             double *__restrict__ y) {
     const int r = t / 5, m = t - 5 * r;
     if (r >= nrow) return;
     double s0 = 0.0, s1 = 0.0;
@@ -307,6 +413,39 @@ __global__ void __launch_bounds__(160) k_bspmv(int nrow, const int *__restrict__
         for (int q = 0; q < 5; q++) s0 = fma(ldA<TA>(a + q), __ldg(xv + q), s0);
     }
     y[(int64_t)r * 5 + m] = s0 + s1;
+}
+
+template <typename TA>
+__global__ void __launch_bounds__(160) k_bspmv(int nrow, const int *__restrict__ IA, const int *__restrict__ JA,
+                                               const TA *__restrict__ A, const double *__restrict__ x,
+                                               double *__restrict__ y) {
+    bspmv_thread<TA>(blockIdx.x * blockDim.x + threadIdx.x, nrow, IA, JA, A, x, y);
+}
+
+// Several requests' SpMVs in one launch (the serving loop's fused SpMV): CTA
+// b belongs to the job whose [block_begin, next block_begin) holds it, and
+// computes that job's rows exactly as k_bspmv's CTA b - block_begin would.
+template <typename TA>
+__global__ void __launch_bounds__(160) k_bspmv_batch(const __grid_constant__ SpmvBatch B) {
+    int j = 0;
+    while (j + 1 < B.njobs && (int)blockIdx.x >= B.job[j + 1].block_begin) j++;
+    const SpmvJob &J = B.job[j];
+    bspmv_thread<TA>(((int)blockIdx.x - J.block_begin) * 160 + (int)threadIdx.x, J.nrow, J.IA, J.JA,
+                     static_cast<const TA *>(J.A), J.x, J.y);
+}
+
+int launch_spmv_batch(int key, const SpmvBatch &b, cudaStream_t s) {
+    int blocks = 0;
+    for (int k = 0; k < b.njobs; k++) blocks += grid_for(5 * (int64_t)b.job[k].nrow, 160);
+    if (blocks == 0) return CFD_OK;
+    switch (key - kSpmvKey) {
+        case CFD_PREC_FP64: k_bspmv_batch<double><<<blocks, 160, 0, s>>>(b); break;
+        case CFD_PREC_FP32: k_bspmv_batch<float><<<blocks, 160, 0, s>>>(b); break;
+        case CFD_PREC_BF16: k_bspmv_batch<uint16_t><<<blocks, 160, 0, s>>>(b); break;
+        default: return CFD_ERR_UNSUPPORTED;
+    }
+    CFD_LAUNCH_CHECK();
+    return CFD_OK;
 }
 
 // ------------------------------------------------------ preconditioners
@@ -613,16 +752,27 @@ static int precond_apply(cfd_ctx *c, const Precond &pc, const double *r, double 
     return CFD_OK;
 }
 
-static void spmv(cfd_ctx *c, int prec, const double *x, double *y) {
+static int spmv(cfd_ctx *c, int prec, const double *x, double *y) {
     const int n = c->nnode;
     const int g = grid_for(5 * (int64_t)n, 160), b = 160;
     if (prec == CFD_PREC_FP64 && !c->a64_valid) prec = c->a_precision;  // low-precision-only system
-    if (prec == CFD_PREC_FP32 && c->A32.p)
-        k_bspmv<float><<<g, b, 0, c->stream>>>(n, c->IA.p, c->JA.p, c->A32.p, x, y);
-    else if (prec == CFD_PREC_BF16 && c->A16.p)
-        k_bspmv<uint16_t><<<g, b, 0, c->stream>>>(n, c->IA.p, c->JA.p, c->A16.p, x, y);
+    const void *A = prec == CFD_PREC_FP32 && c->A32.p   ? (const void *)c->A32.p
+                    : prec == CFD_PREC_BF16 && c->A16.p ? (const void *)c->A16.p
+                                                        : (const void *)c->A64.p;
+    if (A == c->A64.p) prec = CFD_PREC_FP64;
+    if (c->batcher) {
+        // the serving loop fuses this launch with other requests' (bit-identical per row)
+        const SpmvJob job{n, c->IA.p, c->JA.p, A, x, y, 0};
+        return c->batch_submit(c->batcher, c, kSpmvKey + prec, &job);
+    }
+    if (prec == CFD_PREC_FP32)
+        k_bspmv<float><<<g, b, 0, c->stream>>>(n, c->IA.p, c->JA.p, static_cast<const float *>(A), x, y);
+    else if (prec == CFD_PREC_BF16)
+        k_bspmv<uint16_t><<<g, b, 0, c->stream>>>(n, c->IA.p, c->JA.p, static_cast<const uint16_t *>(A), x, y);
     else
-        k_bspmv<double><<<g, b, 0, c->stream>>>(n, c->IA.p, c->JA.p, c->A64.p, x, y);
+        k_bspmv<double><<<g, b, 0, c->stream>>>(n, c->IA.p, c->JA.p, static_cast<const double *>(A), x, y);
+    CFD_LAUNCH_CHECK();
+    return CFD_OK;
 }
 
 static int vnorm(cfd_ctx *c, const double *x, int64_t n, double *out) {
@@ -664,16 +814,13 @@ static int gmres_inner(cfd_ctx *c, int aprec, const Precond &pc, int m, int max_
         for (; j < m && total < max_iters; j++, total++) {
             // w = A M^-1 v_j
             if ((st = precond_apply(c, pc, V + j * ld, tmp, zz))) return st;
-            spmv(c, aprec, zz, w);
-            CFD_LAUNCH_CHECK();
+            if ((st = spmv(c, aprec, zz, w))) return st;
             // CGS2 with the coefficients kept on the device; one read-back
             // of the Hessenberg column per step
             double *dd = c->dots.p;
             if ((st = mdot_dev(c, V, ld, j + 1, w, n5, dd + DOT_H1))) return st;
-            k_axpy_multi<<<1184, 256, 0, c->stream>>>(n5, j + 1, V, ld, dd + DOT_H1, w);
-            if ((st = mdot_dev(c, V, ld, j + 1, w, n5, dd + DOT_H2))) return st;
-            k_axpy_multi<<<1184, 256, 0, c->stream>>>(n5, j + 1, V, ld, dd + DOT_H2, w);
-            if ((st = mdot_dev(c, w, n5, 1, w, n5, dd + DOT_NRM))) return st;
+            if ((st = axpy_mdot_dev(c, V, ld, j + 1, dd + DOT_H1, w, n5, false, dd + DOT_H2))) return st;
+            if ((st = axpy_mdot_dev(c, V, ld, j + 1, dd + DOT_H2, w, n5, true, dd + DOT_NRM))) return st;
             k_arnoldi_column<<<1, MAXK, 0, c->stream>>>(j, dd);
             k_scale_copy_dev<<<1184, 256, 0, c->stream>>>(n5, dd + DOT_COL + MAXK - 1, w, V + (j + 1) * ld);
             CFD_LAUNCH_CHECK();
@@ -713,7 +860,7 @@ static int gmres_inner(cfd_ctx *c, int aprec, const Precond &pc, int m, int max_
         k_add<<<1184, 256, 0, c->stream>>>(n5, zz, d);
         CFD_LAUNCH_CHECK();
         // true residual for the restart: w = r - A d
-        spmv(c, aprec, d, tmp);
+        if ((st = spmv(c, aprec, d, tmp))) return st;
         k_sub<<<1184, 256, 0, c->stream>>>(n5, r, tmp, w);
         CFD_LAUNCH_CHECK();
         if ((st = vnorm(c, w, n5, &beta))) return st;
@@ -828,7 +975,7 @@ int cfd_gmres(cfd_ctx *c, const cfd_gmres_opts *o, cfd_gmres_stats *stats) {
     int left = opt.max_iters;
     for (int it = 0; it < nref && left > 0; it++) {
         // FP64 defect: r = B - A64 x
-        spmv(c, CFD_PREC_FP64, x, r);
+        if ((st = spmv(c, CFD_PREC_FP64, x, r))) return st;
         k_sub<<<1184, 256, 0, c->stream>>>(n5, c->B.p, r, r);
         CFD_LAUNCH_CHECK();
         double rn;
@@ -850,7 +997,7 @@ int cfd_gmres(cfd_ctx *c, const cfd_gmres_opts *o, cfd_gmres_stats *stats) {
         left -= its;
     }
     // final FP64 residual
-    spmv(c, CFD_PREC_FP64, x, r);
+    if ((st = spmv(c, CFD_PREC_FP64, x, r))) return st;
     k_sub<<<1184, 256, 0, c->stream>>>(n5, c->B.p, r, r);
     CFD_LAUNCH_CHECK();
     double rn;
@@ -872,9 +1019,7 @@ int cfd_spmv(cfd_ctx *c, int precision, const double *x, double *y) {
         return CFD_ERR_ARG;
     }
     CFD_CUDA(cudaSetDevice(c->device));
-    spmv(c, precision, x, y);
-    CFD_LAUNCH_CHECK();
-    return CFD_OK;
+    return spmv(c, precision, x, y);
 }
 
 int cfd_precond_apply(cfd_ctx *c, const double *r, double *z) {

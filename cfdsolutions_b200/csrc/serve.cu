@@ -15,6 +15,7 @@
 // what runs beside it.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -71,10 +72,158 @@ struct Job {
     bool done = false;
 };
 
+// Fuses the interior residual launches and the block SpMV launches of the
+// requests being solved side by side into one k_residual_gather_batch /
+// k_bspmv_batch launch over a request table.  A worker's cfd_residual (or
+// GMRES SpMV) hands its job to submit(), which records an event on the
+// worker's stream and waits until the batcher has launched a batch that
+// contains the job; the batcher waits for the events of the batch's jobs on
+// its own stream, launches, records each job's completion event, and the
+// worker's stream waits for that event before its next kernel.  A batch takes
+// the jobs of the first job's kernel (key) queued until as many jobs as
+// requests in their solves are waiting, or `window` after the first, up to
+// kBatchMax.  Each node's residual and each row's product are computed by the
+// same code as in the request's own launch, so results do not depend on the
+// batching.
+struct Batcher {
+    struct Pend {
+        int key;
+        cfd::GatherJob gather;  // key < kSpmvKey
+        cfd::SpmvJob spmv;      // key >= kSpmvKey
+        cudaEvent_t ev_in, ev_out;
+        bool launched;
+        int status;
+    };
+    int device = 0;
+    std::chrono::duration<double> window{50e-6};
+    std::atomic<int> solving{0};  // requests inside their solves: jobs worth waiting for
+    std::mutex mu;
+    std::condition_variable cv_sub, cv_done;
+    std::deque<Pend *> q;
+    bool stop = false, dead = false;
+    uint64_t batches[2] = {0, 0}, jobs[2] = {0, 0};  // [residual, SpMV]
+    std::thread th;
+
+    int launch(int key, const std::vector<Pend *> &take, cudaStream_t s) {
+        if (key >= cfd::kSpmvKey) {
+            cfd::SpmvBatch b;
+            b.njobs = (int)take.size();
+            int blk = 0;
+            for (int k = 0; k < b.njobs; k++) {
+                b.job[k] = take[k]->spmv;
+                b.job[k].block_begin = blk;
+                blk += (int)((5 * (int64_t)b.job[k].nrow + 159) / 160);
+            }
+            return cfd::launch_spmv_batch(key, b, s);
+        }
+        cfd::GatherBatch b;
+        b.njobs = (int)take.size();
+        int blk = 0;
+        for (int k = 0; k < b.njobs; k++) {
+            b.job[k] = take[k]->gather;
+            b.job[k].block_begin = blk;
+            blk += (b.job[k].nnode + 127) / 128;
+        }
+        return cfd::launch_gather_batch(key, b, s);
+    }
+
+    void run() {
+        cudaSetDevice(device);
+        cudaStream_t s = nullptr;
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+            std::lock_guard<std::mutex> lk(mu);
+            dead = true;
+            for (Pend *p : q) { p->status = CFD_ERR_CUDA; p->launched = true; }
+            q.clear();
+            cv_done.notify_all();
+            return;
+        }
+        for (;;) {
+            std::vector<Pend *> take;
+            int key;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_sub.wait(lk, [&] { return stop || !q.empty(); });
+                if (q.empty()) break;  // stop with nothing queued
+                const auto deadline = Clock::now() + std::chrono::duration_cast<Clock::duration>(window);
+                cv_sub.wait_until(lk, deadline, [&] {
+                    return stop || (int)q.size() >= std::min(cfd::kBatchMax, std::max(1, solving.load()));
+                });
+                key = q.front()->key;
+                for (auto it = q.begin(); it != q.end() && (int)take.size() < cfd::kBatchMax;) {
+                    if ((*it)->key == key) {
+                        take.push_back(*it);
+                        it = q.erase(it);
+                    } else {
+                        ++it;
+                    }
+                }
+            }
+            int st = CFD_OK;
+            for (Pend *p : take)
+                if (cudaStreamWaitEvent(s, p->ev_in, 0) != cudaSuccess) st = CFD_ERR_CUDA;
+            if (st == CFD_OK) st = launch(key, take, s);
+            for (Pend *p : take)
+                if (st == CFD_OK && cudaEventRecord(p->ev_out, s) != cudaSuccess) st = CFD_ERR_CUDA;
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                for (Pend *p : take) {
+                    p->status = st;
+                    p->launched = true;
+                }
+                const int kind = key >= cfd::kSpmvKey ? 1 : 0;
+                batches[kind]++;
+                jobs[kind] += take.size();
+            }
+            cv_done.notify_all();
+        }
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+    }
+};
+
+// per worker thread: the events of its fused jobs
+thread_local cudaEvent_t tl_ev_in = nullptr, tl_ev_out = nullptr;
+
+int batch_submit(void *b, cfd_ctx *c, int key, const void *job) {
+    Batcher *B = static_cast<Batcher *>(b);
+    if (!tl_ev_in) {
+        CFD_CUDA(cudaEventCreateWithFlags(&tl_ev_in, cudaEventDisableTiming));
+        CFD_CUDA(cudaEventCreateWithFlags(&tl_ev_out, cudaEventDisableTiming));
+    }
+    CFD_CUDA(cudaEventRecord(tl_ev_in, c->stream));
+    Batcher::Pend p{};
+    p.key = key;
+    if (key >= cfd::kSpmvKey) p.spmv = *static_cast<const cfd::SpmvJob *>(job);
+    else p.gather = *static_cast<const cfd::GatherJob *>(job);
+    p.ev_in = tl_ev_in;
+    p.ev_out = tl_ev_out;
+    p.launched = false;
+    p.status = CFD_OK;
+    {
+        std::unique_lock<std::mutex> lk(B->mu);
+        if (B->dead || B->stop) {
+            cfd::set_error("launch batcher: not running");
+            return CFD_ERR_STATE;
+        }
+        B->q.push_back(&p);
+        B->cv_sub.notify_one();
+        B->cv_done.wait(lk, [&] { return p.launched; });
+    }
+    if (p.status) {
+        cfd::set_error("launch batcher: fused launch failed (%d)", p.status);
+        return p.status;
+    }
+    CFD_CUDA(cudaStreamWaitEvent(c->stream, tl_ev_out, 0));
+    return CFD_OK;
+}
+
 }  // namespace
 
 struct cfd_server {
     int device = 0;
+    Batcher *batcher = nullptr;  // fuser of the requests' residual launches
+    bool batching = true;        // requests use it (cfd_server_set_batching)
     double budget = 0.0, reserved = 0.0, peak = 0.0;
     int active = 0;
     bool stop = false;
@@ -105,6 +254,10 @@ int run_job(int device, cudaStream_t s, const cfd_serve_request &r, cfd_serve_re
     do {
         if ((st = cfd_create(device, &ctx))) break;
         if ((st = cfd_set_stream(ctx, s))) break;
+        if (srv.batcher && srv.batching) {
+            ctx->batcher = srv.batcher;
+            ctx->batch_submit = batch_submit;
+        }
         if ((st = cfd_set_params(ctx, &r.params))) break;
         if ((st = cfd_set_mesh_from(ctx, mesh))) break;
         res.nnode = mesh->m.nnode;
@@ -118,7 +271,11 @@ int run_job(int device, cudaStream_t s, const cfd_serve_request &r, cfd_serve_re
             (st = cfd_ilu_mc_order(ctx, nullptr, nullptr)))
             break;
         res.t_start_solve = srv.now();
-        if ((st = cfd_solve_steady(ctx, &r.opts, &res.stats))) break;
+        Batcher *fuse = ctx->batcher ? srv.batcher : nullptr;
+        if (fuse) fuse->solving++;
+        st = cfd_solve_steady(ctx, &r.opts, &res.stats);
+        if (fuse) fuse->solving--;
+        if (st) break;
         if (r.keep_state) {
             keep.resize(Q.size());
             if ((st = cfd_get_state(ctx, keep.data()))) break;
@@ -179,6 +336,11 @@ void cfd_server::run_worker() {
     }
     cfd::g_alloc_async = false;
     cfd::g_alloc_stream = nullptr;
+    if (tl_ev_in) {
+        cudaEventDestroy(tl_ev_in);
+        cudaEventDestroy(tl_ev_out);
+        tl_ev_in = tl_ev_out = nullptr;
+    }
     cudaStreamDestroy(s);
 }
 
@@ -242,6 +404,9 @@ int cfd_server_create(int device, int workers, double budget_bytes, cfd_server *
     srv->device = device;
     srv->budget = budget_bytes;
     srv->t0 = Clock::now();
+    srv->batcher = new Batcher();
+    srv->batcher->device = device;
+    srv->batcher->th = std::thread([b = srv->batcher] { b->run(); });
     for (int w = 0; w < workers; w++) srv->workers.emplace_back([srv] { srv->run_worker(); });
     *out = srv;
     return CFD_OK;
@@ -324,7 +489,41 @@ int cfd_server_destroy(cfd_server *srv) {
     }
     srv->cv.notify_all();
     for (auto &t : srv->workers) t.join();
+    if (srv->batcher) {
+        {
+            std::lock_guard<std::mutex> lk(srv->batcher->mu);
+            srv->batcher->stop = true;
+        }
+        srv->batcher->cv_sub.notify_all();
+        srv->batcher->th.join();
+        delete srv->batcher;
+    }
     delete srv;
+    return CFD_OK;
+}
+
+int cfd_server_set_batching(cfd_server *srv, int enable, double window_us) {
+    if (!srv || !srv->batcher || !(window_us >= 0.0) || window_us > 1e6) {
+        cfd::set_error("cfd_server_set_batching: a server and a window in [0, 1e6] us");
+        return CFD_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (srv->active > 0 || !srv->queue.empty()) {
+        cfd::set_error("cfd_server_set_batching: set it before submitting requests");
+        return CFD_ERR_STATE;
+    }
+    srv->batching = enable != 0;
+    srv->batcher->window = std::chrono::duration<double>(window_us * 1e-6);
+    return CFD_OK;
+}
+
+int cfd_server_batch_stats(cfd_server *srv, double out[4]) {
+    if (!srv || !out) return CFD_ERR_ARG;
+    std::lock_guard<std::mutex> lk(srv->batcher->mu);
+    for (int k = 0; k < 2; k++) {
+        out[2 * k] = (double)srv->batcher->batches[k];
+        out[2 * k + 1] = (double)srv->batcher->jobs[k];
+    }
     return CFD_OK;
 }
 

@@ -78,10 +78,20 @@ class Result:
 
 
 class Server:
-    def __init__(self, device: int = 0, workers: int = 8, budget_bytes: float = 150e9):
+    def __init__(self, device: int = 0, workers: int = 8, budget_bytes: float = 150e9, batching: bool = True,
+                 window_us: float = 50.0):
         self._h = C.c_void_p()
         capi.check(capi.lib.cfd_server_create(int(device), int(workers), float(budget_bytes), C.byref(self._h)),
                    "cfd_server_create")
+        capi.check(capi.lib.cfd_server_set_batching(self._h, int(bool(batching)), float(window_us)),
+                   "cfd_server_set_batching")
+
+    def batch_stats(self) -> dict:
+        """Fused launches so far and the jobs they carried, per kernel kind."""
+        o = np.zeros(4)
+        capi.check(capi.lib.cfd_server_batch_stats(self._h, capi.ptr(o)), "cfd_server_batch_stats")
+        return {"residual": {"launches": int(o[0]), "jobs": int(o[1])},
+                "spmv": {"launches": int(o[2]), "jobs": int(o[3])}}
 
     def submit(self, req: capi.ServeRequest) -> int:
         i = C.c_int64()
@@ -130,4 +140,74 @@ class Server:
             pass
 
 
-__all__ = ["Server", "Result", "request", "steady_opts", "initial_state", "default_params"]
+# ------------------------------------------------------------------ autotuner
+SIZE_BUCKETS = ((16, 32), (32, 64), (64, 1 << 30))  # cube sides [lo, hi)
+
+
+def size_bucket(n: int) -> int:
+    for k, (lo, hi) in enumerate(SIZE_BUCKETS):
+        if lo <= n < hi:
+            return k
+    return 0 if n < SIZE_BUCKETS[0][0] else len(SIZE_BUCKETS) - 1
+
+
+def autotune(make_request, sample, device: int = 0, budget_bytes: float = 150e9,
+             server_candidates=((16, True, 0.0), (16, True, 50.0), (16, True, 500.0), (16, False, 0.0),
+                                (12, True, 50.0)),
+             refresh_candidates=(2, 5, 10)) -> dict:
+    """Measured choice of the serving schedule for a request mix.
+
+    ``make_request(k, precond_update)`` builds request k of the mix with the
+    given preconditioner refresh period; ``sample`` lists the request indices
+    to calibrate on.  Two searches, each timed on the GPU:
+
+    * per cube-size bucket (``SIZE_BUCKETS``), the implicit solve's ILU(0)
+      refresh period (``precond_update``): the bucket's median request of the
+      sample is solved alone under each candidate and the fastest wins;
+    * for the server, the worker count and the fusion of the requests'
+      residual and SpMV launches (on/off and the batcher's window): the
+      whole sample, submitted at once with the chosen refresh periods, runs
+      under each candidate and the highest solves per second wins.
+
+    Returns {"precond_update": {bucket: period}, "server": (workers,
+    batching, window_us), "timings": ...}.  The results of every request are
+    the same under every schedule up to the refresh period, which changes the
+    preconditioner and so the iterates (not the converged state)."""
+    import time
+
+    timings = {"refresh": {}, "server": {}}
+    by_bucket = {}
+    for k in sample:
+        by_bucket.setdefault(size_bucket(int(make_request(k, 1).nx)), []).append(k)
+    refresh = {}
+    with Server(device=device, workers=1, budget_bytes=budget_bytes) as srv:
+        for b, ks in sorted(by_bucket.items()):
+            ks = sorted(ks, key=lambda k: make_request(k, 1).nx)
+            k = ks[len(ks) // 2]
+            best = None
+            for pu in refresh_candidates:
+                t0 = time.perf_counter()
+                r = srv.wait(srv.submit(make_request(k, pu)))
+                dt = time.perf_counter() - t0
+                timings["refresh"][f"bucket{b}_n{make_request(k, 1).nx}_pu{pu}"] = dt
+                if r.status == 0 and (best is None or dt < best[0]):
+                    best = (dt, pu)
+            refresh[b] = best[1] if best else refresh_candidates[0]
+    pick = lambda k: refresh.get(size_bucket(int(make_request(k, 1).nx)), refresh_candidates[0])  # noqa: E731
+    best = None
+    for workers, batching, window in server_candidates:
+        with Server(device=device, workers=workers, budget_bytes=budget_bytes, batching=batching,
+                    window_us=window) as srv:
+            t0 = time.perf_counter()
+            ids = [srv.submit(make_request(k, pick(k))) for k in sample]
+            res = [srv.wait(i) for i in ids]
+            dt = time.perf_counter() - t0
+        rate = len(sample) / dt
+        timings["server"][f"w{workers}_{'fused' if batching else 'unfused'}_{window:g}us"] = rate
+        if all(r.status == 0 for r in res) and (best is None or rate > best[0]):
+            best = (rate, (workers, batching, window))
+    return {"precond_update": refresh, "server": best[1] if best else server_candidates[0], "timings": timings}
+
+
+__all__ = ["Server", "Result", "request", "steady_opts", "initial_state", "default_params", "autotune",
+           "size_bucket", "SIZE_BUCKETS"]

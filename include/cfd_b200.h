@@ -106,7 +106,7 @@ extern "C" {
 #define CFD_PC_BLOCK_JACOBI 1
 #define CFD_PC_ILU0      2  /* ILU(0) in the mesh (row) order, level-scheduled */
 #define CFD_PC_ILU0_MC   3  /* ILU(0) in block multicolour order: 32-row patches, patch graph coloured
-                               greedily, one launch per colour in factorisation and solves */
+                               by DSATUR, one launch per colour in factorisation and solves */
 
 /* Solver options; mirrors the reference parameter file keys named beside
  * each field (Euler3D/src/SolverParameters.cpp:184-700). */
@@ -523,7 +523,10 @@ typedef struct cfd_serve_result {
 } cfd_serve_result;
 
 /* workers: concurrent solves; budget_bytes: device memory the admitted
- * requests may reserve together (estimates, see DESIGN). */
+ * requests may reserve together (each request's estimate is
+ * 1.2 * (N*(1644 + 40*(m+6)) + 15.5*N*(A + M + 60)) + 16 MiB bytes for N
+ * nodes, GMRES restart m and A, M bytes per stored Jacobian and factor
+ * block). */
 int  cfd_server_create(int device, int workers, double budget_bytes, cfd_server **out);
 /* Queues a request; CFD_ERR_RANGE when its estimate exceeds the budget. */
 int  cfd_server_submit(cfd_server *srv, const cfd_serve_request *req, int64_t *id);
@@ -535,6 +538,17 @@ int  cfd_server_state(cfd_server *srv, int64_t id, double *Q);
 int  cfd_server_release(cfd_server *srv, int64_t id);
 /* {active, queued, reserved bytes, peak reserved bytes, server clock s} */
 int  cfd_server_stats(cfd_server *srv, double out[5]);
+/* Fused launches across requests (on by default, window 50 us): the
+ * interior residual launch and the GMRES block SpMV launches of each request
+ * in its solve are handed to a batcher, which launches the jobs of one kernel
+ * that are waiting when as many jobs as requests in their solves have
+ * arrived, or window_us after the first, as one kernel over a request table
+ * (k_residual_gather_batch, k_bspmv_batch); each request's results are the
+ * same bit for bit either way.  Set before the first submit.  batch_stats:
+ * {fused residual launches, residual jobs in them, fused SpMV launches, SpMV
+ * jobs in them}. */
+int  cfd_server_set_batching(cfd_server *srv, int enable, double window_us);
+int  cfd_server_batch_stats(cfd_server *srv, double out[4]);
 /* Running requests finish; queued ones are dropped. */
 int  cfd_server_destroy(cfd_server *srv);
 

@@ -26,14 +26,15 @@ def _requests(precision=capi.PREC_FP32 | capi.PREC_LOW_ONLY):
     return out
 
 
-def _run(reqs, workers, budget=20e9):
-    with Server(device=0, workers=workers, budget_bytes=budget) as srv:
+def _run(reqs, workers, budget=20e9, batching=True, window_us=50.0):
+    with Server(device=0, workers=workers, budget_bytes=budget, batching=batching, window_us=window_us) as srv:
         ids = [srv.submit(r) for r in reqs]
         res = [srv.wait(i) for i in ids]
         for r in res:
             assert r.status == 0, (r.status, r.message)
         states = [srv.state(i, r) for i, r in zip(ids, res)]
         stats = srv.stats()
+        stats.update(srv.batch_stats())
     return res, states, stats
 
 
@@ -82,3 +83,19 @@ def test_admission_keeps_reserved_memory_within_the_budget(gpu_available):
         with pytest.raises(capi.CfdError) as e:
             srv.submit(big)
         assert e.value.code == -9  # CFD_ERR_RANGE
+
+
+def test_fused_launches_change_nothing(gpu_available):
+    """With the requests' interior residuals and GMRES SpMVs fused into
+    launches over a request table (a wide window, so that several requests
+    share launches) every served state is bit-identical to the unfused
+    server's."""
+    reqs = _requests()
+    fused, s_fused, st = _run(reqs, workers=6, window_us=500.0)
+    plain, s_plain, st0 = _run(reqs, workers=6, batching=False)
+    for kind in ("residual", "spmv"):
+        assert st[kind]["jobs"] > st[kind]["launches"] > 0  # some launches carried several requests
+        assert st0[kind]["jobs"] == 0
+    for a, b, sa, sb in zip(fused, plain, s_fused, s_plain):
+        assert a.iterations == b.iterations and a.linear_iterations == b.linear_iterations
+        np.testing.assert_array_equal(sa, sb)
