@@ -153,6 +153,7 @@ SIGNATURES = {
     "cfd_get_system": (I, [P, P, P, P]),
     "cfd_set_system": (I, [P, P, P]),
     "cfd_residual_step": (I, [P, I, P, P, P]),
+    "cfd_set_step_pipeline": (I, [P, I]),
     "cfd_solve_steady": (I, [P, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
     "cfd_solve_unsteady": (I, [P, C.POINTER(UnsteadyOpts), C.POINTER(UnsteadyStats)]),
     "cfd_vtk_write": (I, [C.c_char_p, I, P, C.c_int64, P, P, C.c_int64, P, C.POINTER(Params), P, C.c_int64]),

@@ -37,11 +37,13 @@ static inline double bitsd(unsigned long long u) {
 
 // Characteristic ghost states, one thread per boundary edge
 // (Apply_Characteristic_Boundary_Condition, Euler3D/src/BC.cpp:1440-1487).
+// list: the boundary edges to update (nullptr: edges 0 .. nbedge-1)
 __global__ void k_apply_bc(int nbedge, int64_t ldq, double *__restrict__ Q, const int2 *__restrict__ bn,
                            const double4 *__restrict__ bg, const int *__restrict__ btype, Flow f,
-                           int *__restrict__ err) {
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nbedge) return;
+                           int *__restrict__ err, const int *__restrict__ list) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nbedge) return;
+    const int b = list ? list[t] : t;
     int2 nd = bn[b];
     double4 g = bg[b];
     double qI[5], qG[5], qB[5];
@@ -233,10 +235,12 @@ __device__ __forceinline__ void residual_gather_node(int i, GATHER_PARAMS, doubl
 }
 
 template <int FLUX, bool SECOND, bool KAPPA0 = false, bool LG = false>
-__global__ void __launch_bounds__(128, 3) k_residual_gather(GATHER_PARAMS, unsigned long long *__restrict__ ext) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// Nodes [lo, hi) (lo a multiple of the block size; the whole mesh is 0, nnode).
+__global__ void __launch_bounds__(128, 3) k_residual_gather(GATHER_PARAMS, unsigned long long *__restrict__ ext,
+                                                            int lo, int hi) {
+    const int i = lo + blockIdx.x * blockDim.x + threadIdx.x;
     double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
-    if (i < nnode) residual_gather_node<FLUX, SECOND, KAPPA0, LG>(i, GATHER_ARGS, mn, mx);
+    if (i < hi) residual_gather_node<FLUX, SECOND, KAPPA0, LG>(i, GATHER_ARGS, mn, mx);
     if (add_time) block_extrema3(mn, mx, ext);
 }
 
@@ -1073,14 +1077,14 @@ static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, bool check_
             if (st) return st;
         } else if (lgk) {
             k_residual_gather<FLUX, SECOND, SECOND, true>
-                <<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, ext);
+                <<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, ext, 0, c->nnode);
         } else if (gate) {
             auto kern = k0 ? k_residual_gather_rerun<FLUX, SECOND, SECOND> : k_residual_gather_rerun<FLUX, SECOND, false>;
             const int grid = std::min(grid_for(c->nnode, 128), 3 * c->nsm);
             kern<<<grid, 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, gate, ext);
         } else {
             auto kern = k0 ? k_residual_gather<FLUX, SECOND, SECOND> : k_residual_gather<FLUX, SECOND, false>;
-            kern<<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, ext);
+            kern<<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, ext, 0, c->nnode);
         }
 #undef GATHER_LAUNCH_ARGS
         if (c->nbnode > 0) {
@@ -1272,6 +1276,215 @@ static Levels *build_levels(const std::vector<int> &IA, const std::vector<int> &
 using namespace cfd;
 
 // ====================================================================== C ABI
+// ---------------------------------------------------- pipelined residual step
+// cfd_residual_step with a host state in and both residuals out overlaps its
+// copies with its kernels.  The nodes are cut into K chunks of >= 128K nodes
+// (multiples of 128).  The state goes up chunk by chunk on a copy stream;
+// chunk g's boundary ghosts and its Green-Gauss + limiter pass start when the
+// chunks holding its neighbours have arrived, chunk c's residual when the
+// gradients of the chunks holding its neighbours are formed, and its two
+// residual rows go down on a second copy stream while the next chunks are
+// computed.  Every kernel computes each node as the whole-mesh launch does,
+// and the limiter-fix passes run after the last chunk as in residual_with_fix;
+// when they changed some residual (a node failed a check), the residuals are
+// copied again whole after them.  Used for second order with Green-Gauss
+// gradients and a limiter on the gather kernel and a stream of the caller's;
+// otherwise the step runs its calls one after the other.
+static bool pipe_eligible(const cfd_ctx *c) {
+    const cfd_params &p = c->params;
+    return c->stream && !c->batcher && !patch_kernel(c) && p.order == CFD_ORDER_SECOND &&
+           p.gradient == CFD_GRAD_GG && p.limiter != CFD_LIMITER_NONE && c->pipe.request != 0 &&
+           c->pipe.request != 1;
+}
+
+static int pipe_build(cfd_ctx *c) {
+    StepPipe &P = c->pipe;
+    if (P.built) return CFD_OK;
+    const int n = c->nnode;
+    const int K = P.request > 1 ? std::min(P.request, n / 256) : std::min(16, n / 131072);
+    P.K = K;
+    P.built = true;
+    if (K <= 1) return CFD_OK;
+    P.lo.assign(K + 1, n);
+    for (int k = 0; k < K; k++) P.lo[k] = (int)(((int64_t)n * k / K) / 128 * 128);
+    // the chunk holding the farthest neighbour of each chunk's nodes (the
+    // graph's reach grows along a reverse Cuthill-McKee order)
+    auto chunk_of = [&](int node) { return (int)(std::upper_bound(P.lo.begin(), P.lo.end() - 1, node) - P.lo.begin()) - 1; };
+    P.dep.resize(K);
+    for (int k = 0; k < K; k++) {
+        int far = P.lo[k + 1] - 1;
+        for (int i = P.lo[k]; i < P.lo[k + 1]; i++)
+            for (int e = c->h_IA[i]; e < c->h_IA[i + 1]; e++) far = std::max(far, c->h_JA[e]);
+        P.dep[k] = std::max(k, chunk_of(far));
+    }
+    // a later chunk's neighbours lie no nearer: keep the dependencies monotone
+    for (int k = 1; k < K; k++) P.dep[k] = std::max(P.dep[k], P.dep[k - 1]);
+    // boundary edges by physical node, nodes with boundary edges
+    std::vector<int2> bn(c->nbedge);
+    std::vector<int> bnode(c->nbnode);
+    if (c->nbedge)
+        CFD_CUDA(cudaMemcpyAsync(bn.data(), c->bedge_nodes.p, sizeof(int2) * c->nbedge, cudaMemcpyDeviceToHost, c->stream));
+    if (c->nbnode)
+        CFD_CUDA(cudaMemcpyAsync(bnode.data(), c->bnode.p, sizeof(int) * c->nbnode, cudaMemcpyDeviceToHost, c->stream));
+    CFD_CUDA(stream_wait(c->stream));
+    std::vector<int> order(c->nbedge);
+    for (int b = 0; b < c->nbedge; b++) order[b] = b;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return bn[a].x < bn[b].x; });
+    P.bc_lo.assign(K + 1, c->nbedge);
+    P.bn_lo.assign(K + 1, c->nbnode);
+    for (int k = 0, b = 0; k < K; k++) {
+        while (b < c->nbedge && bn[order[b]].x < P.lo[k]) b++;
+        P.bc_lo[k] = b;
+        P.bn_lo[k] = (int)(std::lower_bound(bnode.begin(), bnode.end(), P.lo[k]) - bnode.begin());
+    }
+    CFD_CUDA(P.bc_list.alloc(std::max(1, c->nbedge)));
+    if (c->nbedge)
+        CFD_CUDA(cudaMemcpyAsync(P.bc_list.p, order.data(), sizeof(int) * c->nbedge, cudaMemcpyHostToDevice, c->stream));
+    CFD_CUDA(stream_wait(c->stream));
+    if (!P.s_in) CFD_CUDA(cudaStreamCreateWithFlags(&P.s_in, cudaStreamNonBlocking));
+    if (!P.s_out) CFD_CUDA(cudaStreamCreateWithFlags(&P.s_out, cudaStreamNonBlocking));
+    if (!P.ev_start) CFD_CUDA(cudaEventCreateWithFlags(&P.ev_start, cudaEventDisableTiming));
+    if (!P.ev_ghost) CFD_CUDA(cudaEventCreateWithFlags(&P.ev_ghost, cudaEventDisableTiming));
+    P.release_events();
+    P.ev_q.assign(K, nullptr);
+    P.ev_r.assign(K, nullptr);
+    for (int k = 0; k < K; k++) {
+        CFD_CUDA(cudaEventCreateWithFlags(&P.ev_q[k], cudaEventDisableTiming));
+        CFD_CUDA(cudaEventCreateWithFlags(&P.ev_r[k], cudaEventDisableTiming));
+    }
+    if (!P.h_flags) CFD_CUDA(cudaMallocHost(&P.h_flags, 4 * sizeof(int)));
+    return CFD_OK;
+}
+
+template <int FLUX>
+static int residual_step_pipelined_flux(cfd_ctx *c, int iteration, const double *Q_host, double *conv, double *diss) {
+    StepPipe &P = c->pipe;
+    const int n = c->nnode, K = P.K;
+    const int64_t nt = (int64_t)n + c->nghost;
+    const size_t dq = (size_t)c->ldq * sizeof(double), hq = (size_t)nt * sizeof(double), hr = (size_t)n * sizeof(double);
+    // cfd_set_state
+    c->phi_next_valid = false;
+    c->lgrad_valid = c->lgrad_pending = false;
+    CFD_CUDA(cudaEventRecord(P.ev_start, c->stream));
+    CFD_CUDA(cudaStreamWaitEvent(P.s_in, P.ev_start, 0));
+    CFD_CUDA(cudaStreamWaitEvent(P.s_out, P.ev_start, 0));
+    if (c->nghost)
+        CFD_CUDA(cudaMemcpy2DAsync(c->Q.p + n, dq, Q_host + n, hq, (size_t)c->nghost * sizeof(double), 5,
+                                   cudaMemcpyHostToDevice, P.s_in));
+    CFD_CUDA(cudaEventRecord(P.ev_ghost, P.s_in));
+    for (int k = 0; k < K; k++) {
+        const int lo = P.lo[k], hi = P.lo[k + 1];
+        CFD_CUDA(cudaMemcpy2DAsync(c->Q.p + lo, dq, Q_host + lo, hq, (size_t)(hi - lo) * sizeof(double), 5,
+                                   cudaMemcpyHostToDevice, P.s_in));
+        CFD_CUDA(cudaEventRecord(P.ev_q[k], P.s_in));
+    }
+    // cfd_begin_iteration (no state read), then the buffers and flags that
+    // cfd_gradient + cfd_limiter leave for the residual: the fused pass writes
+    // the limiters straight into phi
+    int st = cfd_begin_iteration(c, iteration);
+    if (st) return st;
+    c->flow.iteration = iteration;
+    const bool kappa0 = c->flow.frac == 0.0;
+    CFD_CUDA(c->grad.alloc((size_t)15 * n));
+    CFD_CUDA(c->phi_next.alloc((size_t)5 * n));
+    CFD_CUDA(c->phi.alloc((size_t)5 * n));
+    if (kappa0) CFD_CUDA(c->lgrad.alloc((size_t)15 * n));
+    c->has_grad = true;
+    c->phi_next_valid = false;
+    c->lgrad_valid = kappa0;
+    c->pc_fix_pending = true;
+    c->roe_fix_pending = is_roe_flux(FLUX);
+    CFD_CUDA(cudaMemsetAsync(c->fixcount.p, 0, 2 * sizeof(int), c->stream));
+    // residual_with_fix: the first pass's extrema go to the scratch copy
+    const bool check_roe = is_roe_flux(FLUX);
+    const int checks = (check_roe ? 1 : 0) | 2;
+    if (!c->ext_scratch.p) CFD_CUDA(c->ext_scratch.alloc(8));
+    k_ext_reset<<<1, 32, 0, c->stream>>>(c->ext_scratch.p);
+    CFD_LAUNCH_CHECK();
+    CFD_CUDA(cudaStreamWaitEvent(c->stream, P.ev_ghost, 0));
+    int g_done = -1;
+    for (int k = 0; k < K; k++) {
+        while (g_done < P.dep[k]) {
+            const int g = ++g_done;
+            CFD_CUDA(cudaStreamWaitEvent(c->stream, P.ev_q[P.dep[g]], 0));
+            const int nb = P.bc_lo[g + 1] - P.bc_lo[g];
+            if (nb > 0) {
+                k_apply_bc<<<grid_for(nb, 128), 128, 0, c->stream>>>(nb, c->ldq, c->Q.p, c->bedge_nodes.p,
+                                                                      c->bedge_geo.p, c->bedge_type.p, c->flow,
+                                                                      c->err.p, P.bc_list.p + P.bc_lo[g]);
+                CFD_LAUNCH_CHECK();
+            }
+            if ((st = gg_limiter_range(c, c->phi.p, P.lo[g], P.lo[g + 1]))) return st;
+        }
+        const int lo = P.lo[k], hi = P.lo[k + 1];
+        auto kern = kappa0 ? k_residual_gather<FLUX, true, true, true> : k_residual_gather<FLUX, true, false, false>;
+        kern<<<grid_for(hi - lo, 128), 128, 0, c->stream>>>(
+            n, c->ldq, c->Q.p, c->grad.p, c->phi.p, c->xyz.p, c->sell_ptr.p, c->sell_nbr.p, c->sell_geo.p, c->deg.p,
+            c->flow, 1, checks, c->roeflag.p, c->fixcount.p, c->res.p, c->resd.p, c->dt.p, c->lgrad.p,
+            c->ext_scratch.p, lo, hi);
+        CFD_LAUNCH_CHECK();
+        const int nbn = P.bn_lo[k + 1] - P.bn_lo[k];
+        if (nbn > 0) {
+            k_residual_bnd<FLUX><<<grid_for(nbn, 128), 128, 0, c->stream>>>(
+                nbn, c->bnode.p + P.bn_lo[k], n, c->ldq, c->Q.p, c->n2b_ptr.p, c->n2b.p, c->bedge_nodes.p,
+                c->bedge_geo.p, c->flow, 1, nullptr, c->res.p, c->resd.p, c->dt.p, c->ext_scratch.p);
+            CFD_LAUNCH_CHECK();
+        }
+        CFD_CUDA(cudaEventRecord(P.ev_r[k], c->stream));
+        CFD_CUDA(cudaStreamWaitEvent(P.s_out, P.ev_r[k], 0));
+        CFD_CUDA(cudaMemcpy2DAsync(conv + lo, hr, c->res.p + lo, hr, (size_t)(hi - lo) * sizeof(double), 5,
+                                   cudaMemcpyDeviceToHost, P.s_out));
+        CFD_CUDA(cudaMemcpy2DAsync(diss + lo, hr, c->resd.p + lo, hr, (size_t)(hi - lo) * sizeof(double), 5,
+                                   cudaMemcpyDeviceToHost, P.s_out));
+    }
+    // residual_with_fix after its first pass: the fixes, then the gated re-evaluation
+    const bool redo_roe = check_roe;
+    if (redo_roe) CFD_CUDA(c->work.alloc(std::max<size_t>(c->work.n, (size_t)5 * n)));
+    k_limiter_fix_apply<<<std::min(grid_for(n, 256), 4 * c->nsm), 256, 0, c->stream>>>(
+        n, c->fixcount.p, c->roeflag.p, redo_roe ? 1 : 0, c->phi.p, c->work.p);
+    CFD_LAUNCH_CHECK();
+    c->lgrad_valid = false;
+    if (redo_roe && (st = launch_roe_pressure_fix(c, c->fixcount.p))) return st;
+    c->roe_fix_pending = false;
+    c->pc_fix_pending = false;
+    k_ext_merge<<<1, 32, 0, c->stream>>>(c->fixcount.p, c->ext_scratch.p, c->ext.p);
+    CFD_LAUNCH_CHECK();
+    if ((st = launch_residual<FLUX, true>(c, 1, false, false, c->fixcount.p, c->ext.p))) return st;
+    if ((st = cfd_deltat(c, iteration))) return st;
+    CFD_CUDA(cudaMemcpyAsync(P.h_flags, c->fixcount.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CFD_CUDA(cudaMemcpyAsync(P.h_flags + 2, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CFD_CUDA(stream_wait(c->stream));
+    CFD_CUDA(stream_wait(P.s_out));
+    if (P.h_flags[0] || P.h_flags[1]) {
+        // a limiter fix re-evaluated the residual after some chunks went down
+        CFD_CUDA(cudaMemcpyAsync(conv, c->res.p, hr * 5, cudaMemcpyDeviceToHost, c->stream));
+        CFD_CUDA(cudaMemcpyAsync(diss, c->resd.p, hr * 5, cudaMemcpyDeviceToHost, c->stream));
+        CFD_CUDA(stream_wait(c->stream));
+    }
+    if (P.h_flags[2]) {
+        CFD_CUDA(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
+        set_error("device reported numerical failure (flags 0x%x)", P.h_flags[2]);
+        return CFD_ERR_NUMERIC;
+    }
+    return CFD_OK;
+}
+
+static int residual_step_pipelined(cfd_ctx *c, int iteration, const double *Q_host, double *conv, double *diss) {
+    switch (c->params.flux_scheme) {
+        case CFD_FLUX_ROE: return residual_step_pipelined_flux<CFD_FLUX_ROE>(c, iteration, Q_host, conv, diss);
+        case CFD_FLUX_HLLC: return residual_step_pipelined_flux<CFD_FLUX_HLLC>(c, iteration, Q_host, conv, diss);
+        case CFD_FLUX_AUSM: return residual_step_pipelined_flux<CFD_FLUX_AUSM>(c, iteration, Q_host, conv, diss);
+        case CFD_FLUX_ROE_LMFIX:
+            return residual_step_pipelined_flux<CFD_FLUX_ROE_LMFIX>(c, iteration, Q_host, conv, diss);
+        case CFD_FLUX_ROE_PRECOND:
+            return residual_step_pipelined_flux<CFD_FLUX_ROE_PRECOND>(c, iteration, Q_host, conv, diss);
+        case CFD_FLUX_ROE_THORNBER:
+            return residual_step_pipelined_flux<CFD_FLUX_ROE_THORNBER>(c, iteration, Q_host, conv, diss);
+        case CFD_FLUX_VANLEER: return residual_step_pipelined_flux<CFD_FLUX_VANLEER>(c, iteration, Q_host, conv, diss);
+        default: set_error("cfd_residual_step: bad flux scheme"); return CFD_ERR_ARG;
+    }
+}
+
 extern "C" {
 
 int cfd_abi_version(void) { return CFD_ABI_VERSION; }
@@ -1695,6 +1908,7 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
     CFD_CUDA(cudaMemsetAsync(c->resd.p, 0, sizeof(double) * 5 * nnode, s));
     CFD_CUDA(cudaMemsetAsync(c->dt.p, 0, sizeof(double) * nnode, s));
     CFD_CUDA(stream_wait(s));
+    c->pipe.built = false;  // the pipelined step's plan belongs to the mesh
     c->has_mesh = true;
     return cfd_set_freestream(c);
 }
@@ -1767,7 +1981,8 @@ int cfd_apply_bc(cfd_ctx *c, int iteration) {
     c->flow.iteration = iteration;
     if (c->nbedge == 0) return CFD_OK;
     k_apply_bc<<<grid_for(c->nbedge, 128), 128, 0, c->stream>>>(c->nbedge, c->ldq, c->Q.p, c->bedge_nodes.p,
-                                                                  c->bedge_geo.p, c->bedge_type.p, c->flow, c->err.p);
+                                                                  c->bedge_geo.p, c->bedge_type.p, c->flow, c->err.p,
+                                                                  nullptr);
     CFD_LAUNCH_CHECK();
     return CFD_OK;
 }
@@ -2053,9 +2268,20 @@ int cfd_set_system(cfd_ctx *c, const double *A, const double *B) {
     return CFD_OK;
 }
 
+int cfd_set_step_pipeline(cfd_ctx *c, int chunks) {
+    if (!c || chunks < -1) { set_error("cfd_set_step_pipeline: bad argument"); return CFD_ERR_ARG; }
+    c->pipe.request = chunks;
+    c->pipe.built = false;
+    return CFD_OK;
+}
+
 int cfd_residual_step(cfd_ctx *c, int iteration, const double *Q_host, double *conv_host, double *diss_host) {
     NEED_MESH("cfd_residual_step");
     int st;
+    if (Q_host && conv_host && diss_host && pipe_eligible(c)) {
+        if ((st = pipe_build(c))) return st;
+        if (c->pipe.K > 1) return residual_step_pipelined(c, iteration, Q_host, conv_host, diss_host);
+    }
     if (Q_host && (st = cfd_set_state(c, Q_host))) return st;
     if ((st = cfd_begin_iteration(c, iteration))) return st;
     if ((st = cfd_apply_bc(c, iteration))) return st;

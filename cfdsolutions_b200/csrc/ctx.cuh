@@ -97,6 +97,10 @@ struct Abmc {
     DevBuf<int4> hdr;                 // [nnzb] per lower block: slot of inv(U_pp), pairs, local slot
     DevBuf<int64_t> pair_ptr;         // [n+1] update pairs of each row
     DevBuf<int2> pairs;               // (slot of U_pj, local slot of (i,j))
+    // triangular solves: per row in launch order (colour, patch position, row)
+    DevBuf<int4> rowf;                // {row, first lower, first intra lower, diagonal}
+    DevBuf<int4> rowb;                // {row, first intra upper, first off-patch upper, row end}
+    DevBuf<int4> rowl;                // {forward level, patch's last, backward level, patch's last}
     // captured applies (one CUDA graph per factor / input / scratch / output
     // pointer set; the GMRES driver reuses a few such sets)
     struct Graph {
@@ -109,6 +113,38 @@ struct Abmc {
         graphs.clear();
     }
     ~Abmc() { clear_graphs(); }
+};
+
+// Plan of the pipelined residual step (cfd_residual_step with host buffers):
+// node chunks, their dependencies through the node graph's bandwidth, the
+// boundary edges and boundary nodes of each chunk, and the copy streams.
+struct StepPipe {
+    bool built = false;
+    int request = -1;              // cfd_set_step_pipeline: -1 automatic, 0/1 off, k: k chunks
+    int K = 0;                     // chunks (0, 1: the step runs unpipelined)
+    std::vector<int> lo;           // [K+1] node bounds, multiples of 128
+    std::vector<int> dep;          // [K] last chunk holding a neighbour of chunk c
+    std::vector<int> bc_lo;        // [K+1] bounds into bc_list
+    std::vector<int> bn_lo;        // [K+1] bounds into bnode
+    DevBuf<int> bc_list;           // boundary edges ordered by physical node
+    cudaStream_t s_in = nullptr, s_out = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_ghost = nullptr;
+    std::vector<cudaEvent_t> ev_q, ev_r;  // [K] state chunk arrived, residual chunk done
+    int *h_flags = nullptr;        // pinned: fix counters [2], device error word
+    void release_events() {
+        for (cudaEvent_t e : ev_q) cudaEventDestroy(e);
+        for (cudaEvent_t e : ev_r) cudaEventDestroy(e);
+        ev_q.clear();
+        ev_r.clear();
+    }
+    ~StepPipe() {
+        release_events();
+        if (ev_start) cudaEventDestroy(ev_start);
+        if (ev_ghost) cudaEventDestroy(ev_ghost);
+        if (s_in) cudaStreamDestroy(s_in);
+        if (s_out) cudaStreamDestroy(s_out);
+        if (h_flags) cudaFreeHost(h_flags);
+    }
 };
 
 }  // namespace cfd
@@ -272,6 +308,7 @@ struct cfd_ctx {
     cfd::DevBuf<double> dots;   // device dot results
     cfd::DevBuf<int> ilu_diag_inv_done;
     cfd::Abmc mc;               // block multicolour ILU(0) ordering
+    cfd::StepPipe pipe;         // pipelined cfd_residual_step
     bool pc_valid = false;      // M64/M32 hold factors of kind pc_kind, precision pc_prec
     int pc_kind = -1, pc_prec = -1;
     int krylov_m = 0;
@@ -329,5 +366,8 @@ enum : int {
 };
 
 int check_device_error(cfd_ctx *c);
+// fused Green-Gauss + limiter pass over nodes [lo, hi) (gradient.cu), limiters
+// to phi_out, the reconstructed-pressure check left to the residual
+int gg_limiter_range(cfd_ctx *c, double *phi_out, int lo, int hi);
 
 }  // namespace cfd

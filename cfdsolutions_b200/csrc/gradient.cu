@@ -304,9 +304,11 @@ __global__ void __launch_bounds__(128, 4) k_gg_limiter(int nnode, int64_t ldq, c
                                                     const double4 *__restrict__ sell_geo,
                                                     const double *__restrict__ xyz, const double *__restrict__ vol,
                                                     Flow f, double *__restrict__ g, double *__restrict__ phi,
-                                                    int *__restrict__ roeflag, double *__restrict__ lg) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nnode) return;
+                                                    int *__restrict__ roeflag, double *__restrict__ lg, int lo,
+                                                    int hi) {
+    // nodes [lo, hi); the whole mesh is 0, nnode
+    const int i = lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= hi) return;
     const int64_t sb = sell_ptr[i >> 5] + (i & 31);
     const int dgi = deg[i];
     roeflag[i] = 0;
@@ -490,10 +492,15 @@ static void launch_venkat(cfd_ctx *c) {
 }
 
 template <bool KAPPA0, bool PC>
-static void launch_gg_limiter(cfd_ctx *c, double *lg) {
-    k_gg_limiter<KAPPA0, PC><<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(
+static void launch_gg_limiter(cfd_ctx *c, double *lg, double *phi_out, int lo, int hi) {
+    k_gg_limiter<KAPPA0, PC><<<grid_for(hi - lo, 128), 128, 0, c->stream>>>(
         c->nnode, c->ldq, c->Q.p, c->sell_ptr.p, c->sell_nbr.p, c->deg.p, c->sell_geo.p, c->xyz.p, c->cvol.p, c->flow,
-        c->grad.p, c->phi_next.p, c->roeflag.p, lg);
+        c->grad.p, phi_out, c->roeflag.p, lg, lo, hi);
+}
+
+template <bool KAPPA0, bool PC>
+static void launch_gg_limiter(cfd_ctx *c, double *lg) {
+    launch_gg_limiter<KAPPA0, PC>(c, lg, c->phi_next.p, 0, c->nnode);
 }
 
 // Whether the next limiter leaves its reconstructed-pressure correction to
@@ -604,6 +611,14 @@ int cfd_limiter(cfd_ctx *c) {
 }  // extern "C"
 
 namespace cfd {
+int gg_limiter_range(cfd_ctx *c, double *phi_out, int lo, int hi) {
+    if (hi <= lo) return CFD_OK;
+    if (c->flow.frac == 0.0) launch_gg_limiter<true, false>(c, c->lgrad.p, phi_out, lo, hi);
+    else launch_gg_limiter<false, false>(c, nullptr, phi_out, lo, hi);
+    CFD_LAUNCH_CHECK();
+    return CFD_OK;
+}
+
 int launch_roe_pressure_fix(cfd_ctx *c, const int *gate) {
     const int n = c->nnode;
     // gated: usually a no-op, so a short grid that strides when it runs

@@ -239,39 +239,42 @@ struct IntraCap {
     static constexpr int K = sizeof(TM) == 8 ? 3 : 6;
 };
 
+// Off-patch blocks of a row whose columns a triangular solve fetches before
+// its dependency wait (the rest are read in its loop).
+constexpr int kMcPrefetch = 4;
+
 // Forward solve y = L^-1 r over the patches of one colour: five threads per
 // row (thread m forms component m).  Lower blocks in other patches belong to
 // earlier colours (complete in y) and are summed first; the row's blocks
 // inside the patch are staged in shared memory before the level loop, which
 // then only waits on shared memory.  Factors are in factorisation order
 // (entry u of row i at M[(IA[i] + u) * 25]); scol holds their columns.
+// CTA b takes the patch at position b of the colour: rowf / rowl hold its
+// rows' records in that order ({i, first lower, first intra lower, diagonal}
+// and {level, last level of the patch, ..}; i = -1 past the mesh), so the
+// first loads need no patch id.  Everything constant (records, staged blocks,
+// the first off-patch columns, r) is read before the wait; after it one
+// round trip fetches the earlier colours' y and their blocks together.
 template <typename TM>
-__global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value) k_mc_fwd(const int *__restrict__ patches, int n,
-                                                          const int *__restrict__ IA, const int *__restrict__ scol,
-                                                          const int4 *__restrict__ meta,
-                                                          const int2 *__restrict__ plev, const TM *__restrict__ M,
-                                                          const double *__restrict__ r, double *__restrict__ y) {
-    constexpr int K = IntraCap<TM>::K;
+__global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value)
+    k_mc_fwd(const int4 *__restrict__ rowf, const int4 *__restrict__ rowl, const int *__restrict__ scol,
+             const TM *__restrict__ M, const double *__restrict__ r, double *__restrict__ y) {
+    constexpr int K = IntraCap<TM>::K, PF = kMcPrefetch;
     constexpr int T = 5 * kMcRows;
     __shared__ double ys[T];
     __shared__ TM pa[K * 5][T];  // [t*5+c][thread]
     __shared__ unsigned char pj[K][T];
-    const int P = patches[blockIdx.x];
-    const int p0 = P * kMcRows, nr = min(kMcRows, n - p0);
     const int tid = threadIdx.x;
     const int q = tid / 5, m = tid - 5 * q;
-    const bool act = q < nr;
-    const int i = p0 + q;
+    const int4 rf = rowf[blockIdx.x * kMcRows + q];
+    const int4 rl = rowl[blockIdx.x * kMcRows + q];
+    const bool act = rf.x >= 0;
+    const int i = rf.x, p0 = i - q, base = rf.y, ui = rf.z, ue = rf.w, lev = rl.x;
     double s = 0.0;
-    int lev = -1, ui = 0, ue = 0, base = 0;
+    int col[PF];
     // the next colour's launch may start staging its constant factors now
     pdl_trigger();
     if (act) {
-        const int4 mt = meta[i];
-        base = IA[i];
-        lev = mt.w & 0xffff;
-        ui = base + mt.x;
-        ue = base + mt.y;
 #pragma unroll
         for (int t = 0; t < K; t++)
             if (ui + t < ue) {
@@ -280,20 +283,30 @@ __global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value) k_mc_fwd(
 #pragma unroll
                 for (int c = 0; c < 5; c++) pa[t * 5 + c][tid] = am[c];
             }
+#pragma unroll
+        for (int t = 0; t < PF; t++) col[t] = base + t < ui ? scol[base + t] : 0;
+        // r is complete before the first colour's launch starts, so before this one's
+        s = r[(int64_t)i * 5 + m];
     }
-    // r is complete before the first colour's launch starts, so before this one's
-    if (act) s = r[(int64_t)i * 5 + m];
     pdl_wait();  // the earlier colours' y are complete from here on
     if (act) {
+#pragma unroll
+        for (int t = 0; t < PF; t++)
+            if (base + t < ui) {
+                const TM *am = M + (int64_t)(base + t) * 25 + m * 5;
+                const double *yv = y + (int64_t)col[t] * 5;
+#pragma unroll
+                for (int c = 0; c < 5; c++) s = fma(-ld<TM>(am + c), yv[c], s);
+            }
 #pragma unroll 4
-        for (int u = base; u < ui; u++) {
+        for (int u = base + PF; u < ui; u++) {
             const TM *am = M + (int64_t)u * 25 + m * 5;
             const double *yv = y + (int64_t)scol[u] * 5;
 #pragma unroll
             for (int c = 0; c < 5; c++) s = fma(-ld<TM>(am + c), yv[c], s);
         }
     }
-    const int last = plev[P].x;
+    const int last = rl.y;
     for (int l = 0; l <= last; l++) {
         if (act && lev == l) {
 #pragma unroll
@@ -318,34 +331,29 @@ __global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value) k_mc_fwd(
 
 // Backward solve z = U^-1 y over the patches of one colour (colours in
 // decreasing order): upper blocks in other patches belong to later colours.
+// rowb holds {i, first intra upper, first off-patch upper, row end}; rowl
+// {.., .., level, last level}.  y is read after the wait: the last forward
+// colour may still be writing it when the first backward one starts.
 template <typename TM>
-__global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value) k_mc_bwd(const int *__restrict__ patches, int n,
-                                                          const int *__restrict__ IA, const int *__restrict__ scol,
-                                                          const int4 *__restrict__ meta,
-                                                          const int2 *__restrict__ plev, const TM *__restrict__ M,
-                                                          const double *__restrict__ y, double *__restrict__ z) {
-    constexpr int K = IntraCap<TM>::K;
+__global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value)
+    k_mc_bwd(const int4 *__restrict__ rowb, const int4 *__restrict__ rowl, const int *__restrict__ scol,
+             const TM *__restrict__ M, const double *__restrict__ y, double *__restrict__ z) {
+    constexpr int K = IntraCap<TM>::K, PF = kMcPrefetch;
     constexpr int T = 5 * kMcRows;
     __shared__ double zs[T], ts[T];
     __shared__ TM pa[K * 5][T];
     __shared__ unsigned char pj[K][T];
-    const int P = patches[blockIdx.x];
-    const int p0 = P * kMcRows, nr = min(kMcRows, n - p0);
     const int tid = threadIdx.x;
     const int q = tid / 5, m = tid - 5 * q;
-    const bool act = q < nr;
-    const int i = p0 + q;
+    const int4 rb = rowb[blockIdx.x * kMcRows + q];
+    const int4 rl = rowl[blockIdx.x * kMcRows + q];
+    const bool act = rb.x >= 0;
+    const int i = rb.x, p0 = i - q, u0 = rb.y, u1 = rb.z, end = rb.w, lev = rl.z;
     double s = 0.0;
-    int lev = -1, u0 = 0, u1 = 0, end = 0;
     TM dg[5];
+    int col[PF];
     pdl_trigger();
     if (act) {
-        const int4 mt = meta[i];
-        const int base = IA[i];
-        lev = mt.w >> 16;
-        u0 = base + mt.y + 1;  // first upper entry
-        u1 = u0 + mt.z;        // first upper entry outside the patch
-        end = IA[i + 1];
 #pragma unroll
         for (int t = 0; t < K; t++)
             if (u0 + t < u1) {
@@ -357,19 +365,29 @@ __global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value) k_mc_bwd(
         const TM *d = M + (int64_t)(u0 - 1) * 25 + m * 5;
 #pragma unroll
         for (int c = 0; c < 5; c++) dg[c] = d[c];
+#pragma unroll
+        for (int t = 0; t < PF; t++) col[t] = u1 + t < end ? scol[u1 + t] : 0;
     }
     pdl_wait();  // y and the later colours' z are complete from here on
     if (act) {
         s = y[(int64_t)i * 5 + m];
+#pragma unroll
+        for (int t = 0; t < PF; t++)
+            if (u1 + t < end) {
+                const TM *am = M + (int64_t)(u1 + t) * 25 + m * 5;
+                const double *zv = z + (int64_t)col[t] * 5;
+#pragma unroll
+                for (int c = 0; c < 5; c++) s = fma(-ld<TM>(am + c), zv[c], s);
+            }
 #pragma unroll 4
-        for (int u = u1; u < end; u++) {
+        for (int u = u1 + PF; u < end; u++) {
             const TM *am = M + (int64_t)u * 25 + m * 5;
             const double *zv = z + (int64_t)scol[u] * 5;
 #pragma unroll
             for (int c = 0; c < 5; c++) s = fma(-ld<TM>(am + c), zv[c], s);
         }
     }
-    const int last = plev[P].y;
+    const int last = rl.w;
     for (int l = 0; l <= last; l++) {
         const bool mine = act && lev == l;
         if (mine) {
@@ -545,6 +563,28 @@ int mc_build(cfd_ctx *c) {
         maxstage = std::max<int64_t>(maxstage, nlo + (pair_ptr[i + 1] - pair_ptr[i]));
         for (int k = base; k < IA[i + 1]; k++) where[JA[k]] = -1;
     }
+    // row records of the triangular solves, in launch order (colour, then
+    // position of the patch in the colour, then row in the patch)
+    std::vector<int4> rowf((size_t)np * kMcRows), rowb((size_t)np * kMcRows), rowl((size_t)np * kMcRows);
+    for (int pos = 0; pos < np; pos++) {
+        const int P = patches[pos];
+        for (int q = 0; q < kMcRows; q++) {
+            const int i = P * kMcRows + q;
+            const size_t e = (size_t)pos * kMcRows + q;
+            if (i < n) {
+                const int base = IA[i], u0 = base + meta[i].y + 1;
+                rowf[e] = make_int4(i, base, base + meta[i].x, base + meta[i].y);
+                rowb[e] = make_int4(i, u0, u0 + meta[i].z, IA[i + 1]);
+                rowl[e] = make_int4(lf[i], plev[P].x, lb[i], plev[P].y);
+            } else {
+                rowf[e] = rowb[e] = make_int4(-1, 0, 0, 0);
+                rowl[e] = make_int4(-1, plev[P].x, -1, plev[P].y);
+            }
+        }
+    }
+    CFD_CUDA(mc.rowf.upload(rowf.data(), rowf.size(), c->stream));
+    CFD_CUDA(mc.rowb.upload(rowb.data(), rowb.size(), c->stream));
+    CFD_CUDA(mc.rowl.upload(rowl.data(), rowl.size(), c->stream));
     mc.maxrow = maxrow;
     mc.maxlev = maxlev;
     mc.maxstage = maxstage;
@@ -609,16 +649,16 @@ static int mc_apply_launch(cfd_ctx *c, const TM *M, const double *r, double *tmp
         // the first colour starts after the stream's earlier work has completed
         // (no early start), so r is complete in every colour's launch
         lc.numAttrs = k == 0 ? 0 : 1;
-        CFD_CUDA(cudaLaunchKernelEx(&lc, k_mc_fwd<TM>, (const int *)(mc.patches.p + mc.cptr[k]), c->nnode,
-                                    (const int *)c->IA.p, (const int *)mc.scol.p, (const int4 *)mc.meta.p,
-                                    (const int2 *)mc.plev.p, M, r, tmp));
+        const size_t e = (size_t)mc.cptr[k] * kMcRows;
+        CFD_CUDA(cudaLaunchKernelEx(&lc, k_mc_fwd<TM>, (const int4 *)(mc.rowf.p + e), (const int4 *)(mc.rowl.p + e),
+                                    (const int *)mc.scol.p, M, r, tmp));
     }
     lc.numAttrs = 1;
     for (int k = mc.ncolor - 1; k >= 0; k--) {
         lc.gridDim = dim3(mc.cptr[k + 1] - mc.cptr[k]);
-        CFD_CUDA(cudaLaunchKernelEx(&lc, k_mc_bwd<TM>, (const int *)(mc.patches.p + mc.cptr[k]), c->nnode,
-                                    (const int *)c->IA.p, (const int *)mc.scol.p, (const int4 *)mc.meta.p,
-                                    (const int2 *)mc.plev.p, M, (const double *)tmp, z));
+        const size_t e = (size_t)mc.cptr[k] * kMcRows;
+        CFD_CUDA(cudaLaunchKernelEx(&lc, k_mc_bwd<TM>, (const int4 *)(mc.rowb.p + e), (const int4 *)(mc.rowl.p + e),
+                                    (const int *)mc.scol.p, M, (const double *)tmp, z));
     }
     CFD_LAUNCH_CHECK();
     return CFD_OK;

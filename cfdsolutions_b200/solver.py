@@ -184,6 +184,11 @@ class Euler3DGPU:
                    "cfd_residual_step")
         return conv, diss
 
+    def set_step_pipeline(self, chunks: int = -1):
+        """Chunks of the pipelined residual_step with host buffers (-1
+        automatic, 0/1 off; cfd_set_step_pipeline)."""
+        capi.check(capi.lib.cfd_set_step_pipeline(self._h, int(chunks)), "cfd_set_step_pipeline")
+
     def solve_steady(self, max_iterations=100, drop=1e-8, include_diss=1, linear_solver=1, linear_iters=10,
                      relax=1.0, gmres: capi.GmresOpts | None = None, precond_update: int = 1) -> capi.SolveStats:
         g = gmres if gmres is not None else capi.GmresOpts(30, 300, 1e-6, capi.PC_ILU0, capi.PREC_FP64, 1)

@@ -367,9 +367,17 @@ int  cfd_set_system(cfd_ctx *ctx, const double *A, const double *B);
 /* One residual evaluation of the hot path: begin_iteration + BC + (gradient
  * + limiter when second order) + residual + deltat.  With Q_host != NULL the
  * state is copied in first and, with conv_host/diss_host != NULL, the
- * residuals are copied back (the end-to-end form of the call). */
+ * residuals are copied back (the end-to-end form of the call).  In that
+ * form, for second order with Green-Gauss gradients and a limiter on a
+ * stream set by cfd_set_stream, the copies overlap the kernels: the state
+ * goes up and the residuals come down in node chunks while other chunks are
+ * computed (results identical to the unpipelined calls). */
 int  cfd_residual_step(cfd_ctx *ctx, int iteration, const double *Q_host,
                        double *conv_host, double *diss_host);
+/* Chunks of the pipelined cfd_residual_step: -1 automatic (the default: up to
+ * 16 chunks of >= 131072 nodes, none below 262144 nodes), 0 or 1 off, k >= 2
+ * k chunks (at most nnode / 256). */
+int  cfd_set_step_pipeline(cfd_ctx *ctx, int chunks);
 
 typedef struct cfd_solve_opts {
     int    max_iterations;   /* SOLVER_NITERATION                         */
