@@ -897,11 +897,23 @@ def main():
         barrier()
         sat, sat_wall, sat_peak, sat_fused = serve_run(make, every, refresh, np.zeros(len(ns)), sched, dev)
         barrier()
-        # sequential plain FP64 on a seeded subsample of the same mix (every k-th request)
-        seq_ks = every[::max(1, len(ns) // args.serve_sequential)][:args.serve_sequential]
+        # sequential plain FP64 on a subsample of the same mix spread evenly over its sizes (the
+        # smallest and the largest included); the whole mix's sequential time is each request's
+        # time interpolated in cube side between the sampled ones (log-log), since solve time
+        # grows ~ n^3 and a small sample's mean is dominated by where its largest member falls
+        by_size = sorted(every, key=lambda k: (int(ns[k]), k))
+        seq_ks = [by_size[i] for i in sorted(set(np.linspace(0, len(ns) - 1, args.serve_sequential).round()
+                                                   .astype(int).tolist()))]
         seq, seq_wall, _, _ = serve_run(make64, seq_ks, lambda k: STEADY_PC_UPDATE, None, (1, False, 0.0), dev)
+        side_t = {}
+        for k, r in zip(seq_ks, seq):
+            side_t.setdefault(int(ns[k]), []).append(r.latency)
+        xs = np.log(np.array(sorted(side_t)))
+        ys = np.log(np.array([np.mean(side_t[n]) for n in sorted(side_t)]))
+        seq_mix_s = float(np.exp(np.interp(np.log(ns.astype(float)), xs, ys)).sum())
         # host wall clocks of the replicas' servers: the slowest rank sets each rate
-        wall, sat_wall, seq_wall = (max_over_ranks(w, world, f"cuda:{dev}") for w in (wall, sat_wall, seq_wall))
+        wall, sat_wall, seq_wall, seq_mix_s = (max_over_ranks(w, world, f"cuda:{dev}")
+                                               for w in (wall, sat_wall, seq_wall, seq_mix_s))
         lat = np.array([r.latency for r in res])
         sat_lat = np.array([r.latency for r in sat])
         conv = lambda rs: sum(r.status == 0 and r.rms_last <= STEADY_DROP * r.rms_first for r in rs)  # noqa: E731
@@ -915,8 +927,9 @@ def main():
                        "budget_gb": 150.0, "physics": "as steady",
                        "served_precision": "fp32 low-precision-only Jacobian + ILU(0)",
                        "sequential": f"plain fp64 solves one at a time through the same server (1 worker, no "
-                                     f"fusion) on {len(seq_ks)} requests of the mix (every "
-                                     f"{max(1, len(ns) // args.serve_sequential)}th)"},
+                                     f"fusion) on {len(seq_ks)} requests of the mix spread evenly over its cube "
+                                     f"sides; value = requests / the mix's time, each request's time interpolated "
+                                     f"(log-log in cube side) between the sampled ones"},
             "autotuner": {"calibration_requests": len(calib), "workers": sched[0], "fused_residual_and_spmv_launches": sched[1],
                           "window_us": sched[2],
                           "precond_update_by_cube_side": {f"[{SIZE_BUCKETS[b][0]}, {min(SIZE_BUCKETS[b][1], 97)})": v
@@ -930,7 +943,9 @@ def main():
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "at_rate_solves_per_s": aggregate_rate(len(res), wall, world), "converged": ok, "requests_run": len(res) + len(sat),
             "peak_reserved_gb": max(peak, sat_peak) / 1e9,
-            "sequential_fp64": {"value": aggregate_rate(len(seq), seq_wall, world), "wall_s": seq_wall, "converged": ok_seq,
+            "sequential_fp64": {"value": aggregate_rate(len(ns), seq_mix_s, world), "mix_seconds": seq_mix_s,
+                                "sample_solves_per_s": aggregate_rate(len(seq), seq_wall, world),
+                                "sample_wall_s": seq_wall, "sample_requests": len(seq), "converged": ok_seq,
                                 "p50_solve_s": float(np.percentile([r.t_done - r.t_admit for r in seq], 50))},
         }
         serve["speedup_vs_sequential_fp64"] = serve["value"] / serve["sequential_fp64"]["value"]

@@ -80,9 +80,16 @@ struct Levels {
     int max_width = 0;
 };
 
+// Factors of one storage type in the triangular solves' packed layout
+// (lower slots, upper slots, inverted diagonal blocks; see k_mc_pack).
+template <typename TM>
+struct McPack {
+    DevBuf<TM> L, U, D;
+};
+
 // Block multicolour ordering of the ILU(0) preconditioner (ilu_mc.cu): rows
 // are grouped in patches of consecutive rows, the patch graph is coloured
-// greedily, and the factorisation order is colour by colour, row index within
+// (DSATUR), and the factorisation order is colour by colour, row index within
 // a colour.
 struct Abmc {
     bool built = false;
@@ -98,9 +105,18 @@ struct Abmc {
     DevBuf<int64_t> pair_ptr;         // [n+1] update pairs of each row
     DevBuf<int2> pairs;               // (slot of U_pj, local slot of (i,j))
     // triangular solves: per row in launch order (colour, patch position, row)
-    DevBuf<int4> rowf;                // {row, first lower, first intra lower, diagonal}
-    DevBuf<int4> rowb;                // {row, first intra upper, first off-patch upper, row end}
+    DevBuf<int4> rowf;                // {row, off-patch lower slots, lower slots, first lower slot in M}
+    DevBuf<int4> rowb;                // {row, intra-patch upper slots, upper slots, diagonal slot in M}
     DevBuf<int4> rowl;                // {forward level, patch's last, backward level, patch's last}
+    // packed layout: per patch position its first lower / upper slot row
+    // (slots of 32 rows x 25 entries), and each slot's column per row
+    int64_t nlslot = 0, nuslot = 0;
+    DevBuf<int64_t> lslot, uslot;     // [npatch+1]
+    DevBuf<int> colL, colU;           // [slots][32]
+    McPack<float> pk32;
+    McPack<double> pk64;
+    template <typename TM>
+    McPack<TM> &pack();
     // captured applies (one CUDA graph per factor / input / scratch / output
     // pointer set; the GMRES driver reuses a few such sets)
     struct Graph {
@@ -114,6 +130,10 @@ struct Abmc {
     }
     ~Abmc() { clear_graphs(); }
 };
+template <>
+inline McPack<float> &Abmc::pack<float>() { return pk32; }
+template <>
+inline McPack<double> &Abmc::pack<double>() { return pk64; }
 
 // Plan of the pipelined residual step (cfd_residual_step with host buffers):
 // node chunks, their dependencies through the node graph's bandwidth, the

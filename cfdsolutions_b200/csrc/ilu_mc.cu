@@ -247,18 +247,21 @@ constexpr int kMcPrefetch = 4;
 // row (thread m forms component m).  Lower blocks in other patches belong to
 // earlier colours (complete in y) and are summed first; the row's blocks
 // inside the patch are staged in shared memory before the level loop, which
-// then only waits on shared memory.  Factors are in factorisation order
-// (entry u of row i at M[(IA[i] + u) * 25]); scol holds their columns.
-// CTA b takes the patch at position b of the colour: rowf / rowl hold its
-// rows' records in that order ({i, first lower, first intra lower, diagonal}
-// and {level, last level of the patch, ..}; i = -1 past the mesh), so the
-// first loads need no patch id.  Everything constant (records, staged blocks,
-// the first off-patch columns, r) is read before the wait; after it one
-// round trip fetches the earlier colours' y and their blocks together.
+// then only waits on shared memory.  CTA b takes the patch at position b of
+// the colour and reads the factors in the packed layout k_mc_pack writes:
+// slot t of every row of the patch side by side, so that for each (slot,
+// component) the CTA's 160 threads read 160 consecutive values (thread q*5+m
+// the entry (m, c) of row q's block) instead of five 32-byte sectors per row.
+// rowf / rowl hold the rows' records ({i, off-patch lower slots, lower slots}
+// and {level, last level of the patch, ..}; i = -1 past the mesh), L / cl the
+// patch's factors and columns (off-patch slots: global columns, intra-patch
+// slots: patch-local ones).  Everything constant is read before the wait;
+// after it one round trip fetches the earlier colours' y.
 template <typename TM>
 __global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value)
-    k_mc_fwd(const int4 *__restrict__ rowf, const int4 *__restrict__ rowl, const int *__restrict__ scol,
-             const TM *__restrict__ M, const double *__restrict__ r, double *__restrict__ y) {
+    k_mc_fwd(const int4 *__restrict__ rowf, const int4 *__restrict__ rowl, const int64_t *__restrict__ lslot,
+             const int *__restrict__ colL, const TM *__restrict__ PL, const double *__restrict__ r,
+             double *__restrict__ y) {
     constexpr int K = IntraCap<TM>::K, PF = kMcPrefetch;
     constexpr int T = 5 * kMcRows;
     __shared__ double ys[T];
@@ -268,8 +271,11 @@ __global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value)
     const int q = tid / 5, m = tid - 5 * q;
     const int4 rf = rowf[blockIdx.x * kMcRows + q];
     const int4 rl = rowl[blockIdx.x * kMcRows + q];
+    const int64_t ls = lslot[blockIdx.x];
+    const TM *L = PL + ls * (25 * kMcRows) + tid;  // slot t, column c of the block: L[(t * 5 + c) * T]
+    const int *cl = colL + ls * kMcRows + q;       // column of slot t: cl[t * kMcRows]
     const bool act = rf.x >= 0;
-    const int i = rf.x, p0 = i - q, base = rf.y, ui = rf.z, ue = rf.w, lev = rl.x;
+    const int i = rf.x, nx = rf.y, nlo = rf.z, lev = rl.x;
     double s = 0.0;
     int col[PF];
     // the next colour's launch may start staging its constant factors now
@@ -277,14 +283,13 @@ __global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value)
     if (act) {
 #pragma unroll
         for (int t = 0; t < K; t++)
-            if (ui + t < ue) {
-                pj[t][tid] = (unsigned char)(scol[ui + t] - p0);
-                const TM *am = M + (int64_t)(ui + t) * 25 + m * 5;
+            if (nx + t < nlo) {
+                pj[t][tid] = (unsigned char)cl[(nx + t) * kMcRows];
 #pragma unroll
-                for (int c = 0; c < 5; c++) pa[t * 5 + c][tid] = am[c];
+                for (int c = 0; c < 5; c++) pa[t * 5 + c][tid] = L[((nx + t) * 5 + c) * T];
             }
 #pragma unroll
-        for (int t = 0; t < PF; t++) col[t] = base + t < ui ? scol[base + t] : 0;
+        for (int t = 0; t < PF; t++) col[t] = t < nx ? cl[t * kMcRows] : 0;
         // r is complete before the first colour's launch starts, so before this one's
         s = r[(int64_t)i * 5 + m];
     }
@@ -292,18 +297,16 @@ __global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value)
     if (act) {
 #pragma unroll
         for (int t = 0; t < PF; t++)
-            if (base + t < ui) {
-                const TM *am = M + (int64_t)(base + t) * 25 + m * 5;
+            if (t < nx) {
                 const double *yv = y + (int64_t)col[t] * 5;
 #pragma unroll
-                for (int c = 0; c < 5; c++) s = fma(-ld<TM>(am + c), yv[c], s);
+                for (int c = 0; c < 5; c++) s = fma(-ld<TM>(L + (t * 5 + c) * T), yv[c], s);
             }
 #pragma unroll 4
-        for (int u = base + PF; u < ui; u++) {
-            const TM *am = M + (int64_t)u * 25 + m * 5;
-            const double *yv = y + (int64_t)scol[u] * 5;
+        for (int t = PF; t < nx; t++) {
+            const double *yv = y + (int64_t)cl[t * kMcRows] * 5;
 #pragma unroll
-            for (int c = 0; c < 5; c++) s = fma(-ld<TM>(am + c), yv[c], s);
+            for (int c = 0; c < 5; c++) s = fma(-ld<TM>(L + (t * 5 + c) * T), yv[c], s);
         }
     }
     const int last = rl.y;
@@ -311,16 +314,15 @@ __global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value)
         if (act && lev == l) {
 #pragma unroll
             for (int t = 0; t < K; t++)
-                if (ui + t < ue) {
+                if (nx + t < nlo) {
                     const double *yv = ys + pj[t][tid] * 5;
 #pragma unroll
                     for (int c = 0; c < 5; c++) s = fma(-(double)pa[t * 5 + c][tid], yv[c], s);
                 }
-            for (int u = ui + K; u < ue; u++) {
-                const TM *am = M + (int64_t)u * 25 + m * 5;
-                const double *yv = ys + (scol[u] - p0) * 5;
+            for (int t = nx + K; t < nlo; t++) {
+                const double *yv = ys + cl[t * kMcRows] * 5;
 #pragma unroll
-                for (int c = 0; c < 5; c++) s = fma(-ld<TM>(am + c), yv[c], s);
+                for (int c = 0; c < 5; c++) s = fma(-ld<TM>(L + (t * 5 + c) * T), yv[c], s);
             }
             ys[tid] = s;
         }
@@ -331,13 +333,15 @@ __global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value)
 
 // Backward solve z = U^-1 y over the patches of one colour (colours in
 // decreasing order): upper blocks in other patches belong to later colours.
-// rowb holds {i, first intra upper, first off-patch upper, row end}; rowl
-// {.., .., level, last level}.  y is read after the wait: the last forward
-// colour may still be writing it when the first backward one starts.
+// rowb holds {i, intra-patch upper slots, upper slots, ..}; U / cu the
+// packed upper blocks (intra-patch slots first, patch-local columns) and D the
+// packed inverted diagonal blocks.  y is read after the wait: the last
+// forward colour may still be writing it when the first backward one starts.
 template <typename TM>
 __global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value)
-    k_mc_bwd(const int4 *__restrict__ rowb, const int4 *__restrict__ rowl, const int *__restrict__ scol,
-             const TM *__restrict__ M, const double *__restrict__ y, double *__restrict__ z) {
+    k_mc_bwd(const int4 *__restrict__ rowb, const int4 *__restrict__ rowl, const int64_t *__restrict__ uslot,
+             const int *__restrict__ colU, const TM *__restrict__ PU, const TM *__restrict__ PD,
+             const double *__restrict__ y, double *__restrict__ z) {
     constexpr int K = IntraCap<TM>::K, PF = kMcPrefetch;
     constexpr int T = 5 * kMcRows;
     __shared__ double zs[T], ts[T];
@@ -347,8 +351,12 @@ __global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value)
     const int q = tid / 5, m = tid - 5 * q;
     const int4 rb = rowb[blockIdx.x * kMcRows + q];
     const int4 rl = rowl[blockIdx.x * kMcRows + q];
+    const int64_t us = uslot[blockIdx.x];
+    const TM *U = PU + us * (25 * kMcRows) + tid;
+    const int *cu = colU + us * kMcRows + q;
+    const TM *D = PD + (int64_t)blockIdx.x * (25 * kMcRows) + tid;
     const bool act = rb.x >= 0;
-    const int i = rb.x, p0 = i - q, u0 = rb.y, u1 = rb.z, end = rb.w, lev = rl.z;
+    const int i = rb.x, nin = rb.y, nup = rb.z, lev = rl.z;
     double s = 0.0;
     TM dg[5];
     int col[PF];
@@ -356,35 +364,31 @@ __global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value)
     if (act) {
 #pragma unroll
         for (int t = 0; t < K; t++)
-            if (u0 + t < u1) {
-                pj[t][tid] = (unsigned char)(scol[u0 + t] - p0);
-                const TM *am = M + (int64_t)(u0 + t) * 25 + m * 5;
+            if (t < nin) {
+                pj[t][tid] = (unsigned char)cu[t * kMcRows];
 #pragma unroll
-                for (int c = 0; c < 5; c++) pa[t * 5 + c][tid] = am[c];
+                for (int c = 0; c < 5; c++) pa[t * 5 + c][tid] = U[(t * 5 + c) * T];
             }
-        const TM *d = M + (int64_t)(u0 - 1) * 25 + m * 5;
 #pragma unroll
-        for (int c = 0; c < 5; c++) dg[c] = d[c];
+        for (int c = 0; c < 5; c++) dg[c] = D[c * T];
 #pragma unroll
-        for (int t = 0; t < PF; t++) col[t] = u1 + t < end ? scol[u1 + t] : 0;
+        for (int t = 0; t < PF; t++) col[t] = nin + t < nup ? cu[(nin + t) * kMcRows] : 0;
     }
     pdl_wait();  // y and the later colours' z are complete from here on
     if (act) {
         s = y[(int64_t)i * 5 + m];
 #pragma unroll
         for (int t = 0; t < PF; t++)
-            if (u1 + t < end) {
-                const TM *am = M + (int64_t)(u1 + t) * 25 + m * 5;
+            if (nin + t < nup) {
                 const double *zv = z + (int64_t)col[t] * 5;
 #pragma unroll
-                for (int c = 0; c < 5; c++) s = fma(-ld<TM>(am + c), zv[c], s);
+                for (int c = 0; c < 5; c++) s = fma(-ld<TM>(U + ((nin + t) * 5 + c) * T), zv[c], s);
             }
 #pragma unroll 4
-        for (int u = u1 + PF; u < end; u++) {
-            const TM *am = M + (int64_t)u * 25 + m * 5;
-            const double *zv = z + (int64_t)scol[u] * 5;
+        for (int t = nin + PF; t < nup; t++) {
+            const double *zv = z + (int64_t)cu[t * kMcRows] * 5;
 #pragma unroll
-            for (int c = 0; c < 5; c++) s = fma(-ld<TM>(am + c), zv[c], s);
+            for (int c = 0; c < 5; c++) s = fma(-ld<TM>(U + (t * 5 + c) * T), zv[c], s);
         }
     }
     const int last = rl.w;
@@ -393,16 +397,15 @@ __global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value)
         if (mine) {
 #pragma unroll
             for (int t = 0; t < K; t++)
-                if (u0 + t < u1) {
+                if (t < nin) {
                     const double *zv = zs + pj[t][tid] * 5;
 #pragma unroll
                     for (int c = 0; c < 5; c++) s = fma(-(double)pa[t * 5 + c][tid], zv[c], s);
                 }
-            for (int u = u0 + K; u < u1; u++) {
-                const TM *am = M + (int64_t)u * 25 + m * 5;
-                const double *zv = zs + (scol[u] - p0) * 5;
+            for (int t = K; t < nin; t++) {
+                const double *zv = zs + cu[t * kMcRows] * 5;
 #pragma unroll
-                for (int c = 0; c < 5; c++) s = fma(-ld<TM>(am + c), zv[c], s);
+                for (int c = 0; c < 5; c++) s = fma(-ld<TM>(U + (t * 5 + c) * T), zv[c], s);
             }
             ts[tid] = s;
         }
@@ -416,6 +419,39 @@ __global__ void __launch_bounds__(5 * kMcRows, McMinBlocks<TM>::value)
         __syncthreads();
     }
     if (act) z[(int64_t)i * 5 + m] = zs[tid];
+}
+
+// The factors of M (factorisation order) copied into the triangular solves'
+// packed layout, one CTA per patch position: lower slot t, block entry (m, c)
+// of row q at PL[lslot * 800 + (t * 5 + c) * 160 + q * 5 + m], the upper slots
+// likewise in PU, the inverted diagonal block at PD[pos * 800 + c * 160 +
+// q * 5 + m].  Slots past a row's own count are left unwritten and never read.
+template <typename TM>
+__global__ void __launch_bounds__(5 * kMcRows) k_mc_pack(const int4 *__restrict__ rowf, const int4 *__restrict__ rowb,
+                                                        const int64_t *__restrict__ lslot,
+                                                        const int64_t *__restrict__ uslot, const TM *__restrict__ M,
+                                                        TM *__restrict__ PL, TM *__restrict__ PU,
+                                                        TM *__restrict__ PD) {
+    constexpr int T = 5 * kMcRows;
+    const int pos = blockIdx.x, tid = threadIdx.x;
+    const int q = tid / 5, m = tid - 5 * q;
+    const int4 rf = rowf[pos * kMcRows + q], rb = rowb[pos * kMcRows + q];
+    if (rf.x < 0) return;
+    const int64_t l0 = lslot[pos], u0 = uslot[pos];
+    TM *L = PL + l0 * (25 * kMcRows) + tid, *U = PU + u0 * (25 * kMcRows) + tid;
+    for (int t = 0; t < rf.z; t++) {
+        const TM *src = M + (int64_t)(rf.w + t) * 25 + m * 5;
+#pragma unroll
+        for (int c = 0; c < 5; c++) L[(t * 5 + c) * T] = src[c];
+    }
+    for (int t = 0; t < rb.z; t++) {
+        const TM *src = M + (int64_t)(rb.w + 1 + t) * 25 + m * 5;
+#pragma unroll
+        for (int c = 0; c < 5; c++) U[(t * 5 + c) * T] = src[c];
+    }
+    const TM *dsrc = M + (int64_t)rb.w * 25 + m * 5;
+#pragma unroll
+    for (int c = 0; c < 5; c++) PD[(int64_t)pos * (25 * kMcRows) + c * T + tid] = dsrc[c];
 }
 
 }  // namespace
@@ -563,28 +599,56 @@ int mc_build(cfd_ctx *c) {
         maxstage = std::max<int64_t>(maxstage, nlo + (pair_ptr[i + 1] - pair_ptr[i]));
         for (int k = base; k < IA[i + 1]; k++) where[JA[k]] = -1;
     }
-    // row records of the triangular solves, in launch order (colour, then
-    // position of the patch in the colour, then row in the patch)
+    // row records and packed-layout slots of the triangular solves, in launch
+    // order (colour, then position of the patch in the colour, then row)
     std::vector<int4> rowf((size_t)np * kMcRows), rowb((size_t)np * kMcRows), rowl((size_t)np * kMcRows);
+    std::vector<int64_t> lslot(np + 1, 0), uslot(np + 1, 0);
     for (int pos = 0; pos < np; pos++) {
         const int P = patches[pos];
+        int lmax = 0, umax = 0;
         for (int q = 0; q < kMcRows; q++) {
             const int i = P * kMcRows + q;
             const size_t e = (size_t)pos * kMcRows + q;
             if (i < n) {
-                const int base = IA[i], u0 = base + meta[i].y + 1;
-                rowf[e] = make_int4(i, base, base + meta[i].x, base + meta[i].y);
-                rowb[e] = make_int4(i, u0, u0 + meta[i].z, IA[i + 1]);
+                const int base = IA[i], diag = base + meta[i].y;
+                rowf[e] = make_int4(i, meta[i].x, meta[i].y, base);
+                rowb[e] = make_int4(i, meta[i].z, IA[i + 1] - diag - 1, diag);
                 rowl[e] = make_int4(lf[i], plev[P].x, lb[i], plev[P].y);
+                lmax = std::max(lmax, meta[i].y);
+                umax = std::max(umax, IA[i + 1] - diag - 1);
             } else {
                 rowf[e] = rowb[e] = make_int4(-1, 0, 0, 0);
                 rowl[e] = make_int4(-1, plev[P].x, -1, plev[P].y);
             }
         }
+        lslot[pos + 1] = lslot[pos] + lmax;
+        uslot[pos + 1] = uslot[pos] + umax;
     }
+    std::vector<int> colL((size_t)lslot[np] * kMcRows, 0), colU((size_t)uslot[np] * kMcRows, 0);
+    for (int pos = 0; pos < np; pos++) {
+        const int p0 = patches[pos] * kMcRows;
+        for (int q = 0; q < kMcRows; q++) {
+            const int4 rf = rowf[(size_t)pos * kMcRows + q], rb = rowb[(size_t)pos * kMcRows + q];
+            if (rf.x < 0) continue;
+            for (int t = 0; t < rf.z; t++) {
+                const int j = scol[rf.w + t];
+                colL[(size_t)(lslot[pos] + t) * kMcRows + q] = t < rf.y ? j : j - p0;
+            }
+            for (int t = 0; t < rb.z; t++) {
+                const int j = scol[rb.w + 1 + t];
+                colU[(size_t)(uslot[pos] + t) * kMcRows + q] = t < rb.y ? j - p0 : j;
+            }
+        }
+    }
+    mc.nlslot = lslot[np];
+    mc.nuslot = uslot[np];
     CFD_CUDA(mc.rowf.upload(rowf.data(), rowf.size(), c->stream));
     CFD_CUDA(mc.rowb.upload(rowb.data(), rowb.size(), c->stream));
     CFD_CUDA(mc.rowl.upload(rowl.data(), rowl.size(), c->stream));
+    CFD_CUDA(mc.lslot.upload(lslot.data(), lslot.size(), c->stream));
+    CFD_CUDA(mc.uslot.upload(uslot.data(), uslot.size(), c->stream));
+    CFD_CUDA(mc.colL.upload(colL.data(), std::max<size_t>(1, colL.size()), c->stream));
+    CFD_CUDA(mc.colU.upload(colU.data(), std::max<size_t>(1, colU.size()), c->stream));
     mc.maxrow = maxrow;
     mc.maxlev = maxlev;
     mc.maxstage = maxstage;
@@ -629,12 +693,30 @@ int mc_factor(cfd_ctx *c, const TA *A, TM *M) {
             mc.hdr.p, mc.pair_ptr.p, mc.pairs.p, A, M, c->err.p);
     }
     CFD_LAUNCH_CHECK();
+    // the triangular solves read the factors in their packed layout
+    McPack<TM> &pk = mc.pack<TM>();
+    const int np = mc.cptr[mc.ncolor];
+    const size_t nl = (size_t)mc.nlslot * 25 * kMcRows, nu = (size_t)mc.nuslot * 25 * kMcRows,
+                 nd = (size_t)np * 25 * kMcRows;
+    if (pk.L.n != std::max<size_t>(1, nl) || pk.U.n != std::max<size_t>(1, nu) || pk.D.n != nd) {
+        mc.clear_graphs();  // captured applies hold the old addresses
+        CFD_CUDA(pk.L.alloc(std::max<size_t>(1, nl)));
+        CFD_CUDA(pk.U.alloc(std::max<size_t>(1, nu)));
+        CFD_CUDA(pk.D.alloc(nd));
+    }
+    k_mc_pack<TM><<<np, 5 * kMcRows, 0, c->stream>>>(mc.rowf.p, mc.rowb.p, mc.lslot.p, mc.uslot.p, M, pk.L.p, pk.U.p,
+                                                      pk.D.p);
+    CFD_LAUNCH_CHECK();
     return CFD_OK;
 }
 
 template <typename TM>
 static int mc_apply_launch(cfd_ctx *c, const TM *M, const double *r, double *tmp, double *z) {
     Abmc &mc = c->mc;
+    (void)M;  // the solves read the packed copy mc_factor made of M
+    struct {
+        const TM *L, *U, *D;
+    } pk{mc.pack<TM>().L.p, mc.pack<TM>().U.p, mc.pack<TM>().D.p};
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     at[0].val.programmaticStreamSerializationAllowed = 1;
@@ -651,14 +733,16 @@ static int mc_apply_launch(cfd_ctx *c, const TM *M, const double *r, double *tmp
         lc.numAttrs = k == 0 ? 0 : 1;
         const size_t e = (size_t)mc.cptr[k] * kMcRows;
         CFD_CUDA(cudaLaunchKernelEx(&lc, k_mc_fwd<TM>, (const int4 *)(mc.rowf.p + e), (const int4 *)(mc.rowl.p + e),
-                                    (const int *)mc.scol.p, M, r, tmp));
+                                    (const int64_t *)(mc.lslot.p + mc.cptr[k]), (const int *)mc.colL.p,
+                                    (const TM *)pk.L, r, tmp));
     }
     lc.numAttrs = 1;
     for (int k = mc.ncolor - 1; k >= 0; k--) {
         lc.gridDim = dim3(mc.cptr[k + 1] - mc.cptr[k]);
         const size_t e = (size_t)mc.cptr[k] * kMcRows;
         CFD_CUDA(cudaLaunchKernelEx(&lc, k_mc_bwd<TM>, (const int4 *)(mc.rowb.p + e), (const int4 *)(mc.rowl.p + e),
-                                    (const int *)mc.scol.p, M, (const double *)tmp, z));
+                                    (const int64_t *)(mc.uslot.p + mc.cptr[k]), (const int *)mc.colU.p,
+                                    (const TM *)pk.U, (const TM *)(pk.D + e * 25), (const double *)tmp, z));
     }
     CFD_LAUNCH_CHECK();
     return CFD_OK;

@@ -51,8 +51,9 @@ double unit_pm1(uint64_t seed, uint64_t k) {
 // Device bytes of one request, from the box dimensions (the mesh is built
 // after admission): per node the state, residuals, gradients, limiters (two
 // buffers), geometry, incidence and (restart+1)+5 Krylov/work vectors; per block of the
-// Jacobian its stored copies, the preconditioner factors and the ordering
-// lists.  A tet-split box has ~7 interior edges per node, blocks = N + 2E.
+// Jacobian its stored copies, the preconditioner factors (three times their
+// size: the factors and the triangular solves' padded packed copy) and the
+// ordering lists.  A tet-split box has ~7 interior edges per node, blocks = N + 2E.
 double estimate_bytes(const cfd_serve_request &r) {
     const double N = (double)(r.nx + 1) * (r.ny + 1) * (r.nz + 1);
     const double nnzb = N * 15.5;
@@ -60,7 +61,7 @@ double estimate_bytes(const cfd_serve_request &r) {
     const bool low_only = (r.opts.gmres.precision & CFD_PREC_LOW_ONLY) != 0 && r.opts.linear_solver == 1;
     double a = low_only ? 0.0 : 200.0;
     if (r.opts.linear_solver == 1) a += gp == CFD_PREC_FP32 ? 100.0 : gp == CFD_PREC_BF16 ? 50.0 : 0.0;
-    const double m = r.opts.linear_solver == 1 ? (gp == CFD_PREC_FP64 ? 200.0 : 100.0) : 0.0;
+    const double m = r.opts.linear_solver == 1 ? 3.0 * (gp == CFD_PREC_FP64 ? 200.0 : 100.0) : 0.0;
     const double krylov = r.opts.linear_solver == 1 ? 40.0 * (r.opts.gmres.restart + 1 + 5) : 240.0;
     return 1.2 * (N * (1644.0 + krylov) + nnzb * (a + m + 60.0)) + (16 << 20);
 }

@@ -533,8 +533,8 @@ typedef struct cfd_serve_result {
 /* workers: concurrent solves; budget_bytes: device memory the admitted
  * requests may reserve together (each request's estimate is
  * 1.2 * (N*(1644 + 40*(m+6)) + 15.5*N*(A + M + 60)) + 16 MiB bytes for N
- * nodes, GMRES restart m and A, M bytes per stored Jacobian and factor
- * block). */
+ * nodes, GMRES restart m, A bytes per stored Jacobian block and M = 3 x
+ * the bytes per factor block, for the factors and their packed copy). */
 int  cfd_server_create(int device, int workers, double budget_bytes, cfd_server **out);
 /* Queues a request; CFD_ERR_RANGE when its estimate exceeds the budget. */
 int  cfd_server_submit(cfd_server *srv, const cfd_serve_request *req, int64_t *id);
