@@ -154,7 +154,7 @@ def size_bucket(n: int) -> int:
 def autotune(make_request, sample, device: int = 0, budget_bytes: float = 150e9,
              server_candidates=((16, True, 0.0), (16, True, 50.0), (16, True, 500.0), (16, False, 0.0),
                                 (12, True, 50.0)),
-             refresh_candidates=(2, 5, 10)) -> dict:
+             refresh_candidates=(5, 10, 20)) -> dict:
     """Measured choice of the serving schedule for a request mix.
 
     ``make_request(k, precond_update)`` builds request k of the mix with the
