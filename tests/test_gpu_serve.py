@@ -99,3 +99,25 @@ def test_fused_launches_change_nothing(gpu_available):
     for a, b, sa, sb in zip(fused, plain, s_fused, s_plain):
         assert a.iterations == b.iterations and a.linear_iterations == b.linear_iterations
         np.testing.assert_array_equal(sa, sb)
+
+
+def test_autotuner_picks_a_measured_schedule(gpu_available):
+    """autotune() times each refresh period on the sample's median request of
+    each size bucket and each server schedule on the whole sample, and returns
+    the fastest of the candidates it timed; every timed request converges."""
+    from cfdsolutions_b200.serve import autotune, size_bucket
+
+    sides = [6, 7, 9, 8]
+    p = default_params(**dict(BASE, mach=0.6, mach_min=0.6))
+
+    def make(k, pu):
+        return request(sides[k], p, steady_opts(max_iterations=400, drop=1e-8, rtol=0.1, precond_update=pu),
+                       mesh_seed=300 + k, state_seed=400 + k)
+
+    cands = ((2, True, 0.0), (2, False, 0.0))
+    tune = autotune(make, range(len(sides)), server_candidates=cands, refresh_candidates=(1, 4))
+    assert tune["server"] in cands
+    assert set(tune["precond_update"]) == {size_bucket(n) for n in sides}
+    assert all(v in (1, 4) for v in tune["precond_update"].values())
+    assert len(tune["timings"]["server"]) == len(cands)
+    assert all(rate > 0 for rate in tune["timings"]["server"].values())
