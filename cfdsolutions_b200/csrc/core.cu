@@ -1469,7 +1469,7 @@ static int residual_step_pipelined_flux(cfd_ctx *c, int iteration, const double 
     return CFD_OK;
 }
 
-static int residual_step_pipelined(cfd_ctx *c, int iteration, const double *Q_host, double *conv, double *diss) {
+static int residual_step_pipelined_any(cfd_ctx *c, int iteration, const double *Q_host, double *conv, double *diss) {
     switch (c->params.flux_scheme) {
         case CFD_FLUX_ROE: return residual_step_pipelined_flux<CFD_FLUX_ROE>(c, iteration, Q_host, conv, diss);
         case CFD_FLUX_HLLC: return residual_step_pipelined_flux<CFD_FLUX_HLLC>(c, iteration, Q_host, conv, diss);
@@ -1483,6 +1483,18 @@ static int residual_step_pipelined(cfd_ctx *c, int iteration, const double *Q_ho
         case CFD_FLUX_VANLEER: return residual_step_pipelined_flux<CFD_FLUX_VANLEER>(c, iteration, Q_host, conv, diss);
         default: set_error("cfd_residual_step: bad flux scheme"); return CFD_ERR_ARG;
     }
+}
+
+// The step's copies read and write the caller's host buffers: whatever path
+// the step leaves by, its copy streams have finished before it returns.
+static int residual_step_pipelined(cfd_ctx *c, int iteration, const double *Q_host, double *conv, double *diss) {
+    const int st = residual_step_pipelined_any(c, iteration, Q_host, conv, diss);
+    if (st) {
+        cudaStreamSynchronize(c->pipe.s_in);
+        cudaStreamSynchronize(c->pipe.s_out);
+        cudaStreamSynchronize(c->stream);
+    }
+    return st;
 }
 
 extern "C" {

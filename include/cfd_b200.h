@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define CFD_ABI_VERSION 4
+#define CFD_ABI_VERSION 5
 
 /* ------------------------------------------------------------ status codes */
 #define CFD_OK                 0

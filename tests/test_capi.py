@@ -30,7 +30,7 @@ def test_every_declared_symbol_is_exported():
 
 
 def test_abi_version_and_defaults():
-    assert capi.lib.cfd_abi_version() == 4
+    assert capi.lib.cfd_abi_version() == 5
     p = capi.Params()
     capi.lib.cfd_params_default(C.byref(p))
     assert p.gamma == 1.4 and p.flux_scheme == capi.FLUX_ROE and p.limiter == capi.LIMITER_NONE

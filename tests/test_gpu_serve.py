@@ -121,3 +121,16 @@ def test_autotuner_picks_a_measured_schedule(gpu_available):
     assert all(v in (1, 4) for v in tune["precond_update"].values())
     assert len(tune["timings"]["server"]) == len(cands)
     assert all(rate > 0 for rate in tune["timings"]["server"].values())
+
+
+def test_fused_launches_keep_precisions_apart(gpu_available):
+    """Requests with FP32 and BF16 Jacobians in one server: their SpMVs are
+    fused only with jobs of the same storage type (one kernel instantiation per
+    launch), and every served state is bit-identical to the unfused server's."""
+    reqs = _requests()[:3] + _requests(capi.PREC_BF16 | capi.PREC_LOW_ONLY)[3:]
+    fused, s_fused, st = _run(reqs, workers=6, window_us=500.0)
+    plain, s_plain, _ = _run(reqs, workers=6, batching=False)
+    assert st["spmv"]["jobs"] > st["spmv"]["launches"] > 0
+    for a, b, sa, sb in zip(fused, plain, s_fused, s_plain):
+        assert a.iterations == b.iterations and a.linear_iterations == b.linear_iterations
+        np.testing.assert_array_equal(sa, sb)
