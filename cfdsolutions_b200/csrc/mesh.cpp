@@ -16,12 +16,17 @@
 // The reference builds node2Edge in O(N*E) (Connectivity_Maps.cpp:766-780) and
 // renumbers with an O(N^2) Cuthill-McKee (Cuthill_Mckee_Reorder.cpp:17-155);
 // this builder is linear in the mesh size so 128^3-hex meshes build in seconds.
+// The node graph and the dual are gathered per node from node -> element
+// incidence lists, on up to 16 threads, in the order one loop over the
+// elements would sum them (the same bits); the renumbering's bisection and
+// patch graph run on threads too.
 #include "cfd_internal.h"
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 namespace cfd {
@@ -70,64 +75,114 @@ const ElemType kPrism = {6, 9, 5, kPrismEdges,
 const ElemType kHex = {8, 12, 6, kHexEdges,
                        {{0, 1, 2, 3}, {4, 5, 6, 7}, {0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {3, 0, 4, 7}}};
 
-// Every element edge of a mesh (tets and the other volume types), as calls
-// fn(a, b) with the two global node ids.
-template <typename F>
-void for_each_element_edge(const HostMesh &m, F fn) {
-    for (size_t t = 0; t + 3 < m.tets.size(); t += 4)
-        for (int p = 0; p < 6; p++) fn(m.tets[t + kTetEdges[p][0]], m.tets[t + kTetEdges[p][1]]);
-    const std::pair<const std::vector<int> *, const ElemType *> types[3] = {
-        {&m.pyrs, &kPyr}, {&m.prisms, &kPrism}, {&m.hexes, &kHex}};
-    for (const auto &tt : types) {
-        const std::vector<int> &v = *tt.first;
-        const ElemType &T = *tt.second;
-        for (size_t c = 0; c + T.nnode <= v.size(); c += T.nnode)
-            for (int p = 0; p < T.nedge; p++) fn(v[c + T.edges[p][0]], v[c + T.edges[p][1]]);
-    }
+// Ranges [0, n) is split into for parallel_ranges: up to 16, one below
+// 65,536 items.
+inline int range_count(int n) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    return n < 65536 ? 1 : (int)std::min(16u, hw);
 }
 
-// Symmetric node graph of a mesh: CRS without diagonal, rows sorted.
-void build_graph(const HostMesh &msh, std::vector<int> &ia, std::vector<int> &ja) {
-    const int nnode = msh.nnode;
-    // Upper-neighbour sets with a fixed per-node capacity, grown on overflow.
-    int cap = 24;
-    std::vector<int> cnt, up;
-    for (;;) {
-        cnt.assign(nnode, 0);
-        up.assign((size_t)nnode * cap, -1);
-        bool overflow = false;
-        for_each_element_edge(msh, [&](int a, int b) {
-            if (overflow) return;
-            if (a > b) std::swap(a, b);
-            int *row = &up[(size_t)a * cap];
-            int c = cnt[a], k = 0;
-            for (; k < c; k++)
-                if (row[k] == b) break;
-            if (k == c) {
-                if (c == cap) { overflow = true; return; }
-                row[c] = b;
-                cnt[a] = c + 1;
-            }
-        });
-        if (!overflow) break;
-        cap *= 2;
+// fn(t, lo, hi) for the range_count(n) contiguous ranges t of [0, n), one
+// thread each.  Every range writes only its own items.
+template <typename F>
+void parallel_ranges(int n, F fn) {
+    const int nt = range_count(n);
+    if (nt == 1) {
+        fn(0, 0, n);
+        return;
     }
-    std::vector<int> deg(nnode, 0);
-    for (int a = 0; a < nnode; a++) {
-        deg[a] += cnt[a];
-        for (int k = 0; k < cnt[a]; k++) deg[up[(size_t)a * cap + k]]++;
-    }
-    ia.assign(nnode + 1, 0);
-    for (int a = 0; a < nnode; a++) ia[a + 1] = ia[a] + deg[a];
-    ja.assign(ia[nnode], 0);
-    std::vector<int> fill(ia.begin(), ia.end() - 1);
-    for (int a = 0; a < nnode; a++)
-        for (int k = 0; k < cnt[a]; k++) {
-            int b = up[(size_t)a * cap + k];
-            ja[fill[a]++] = b;
-            ja[fill[b]++] = a;
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; t++)
+        th.emplace_back(fn, t, (int)((int64_t)n * t / nt), (int)((int64_t)n * (t + 1) / nt));
+    for (auto &x : th) x.join();
+}
+
+// The volume elements of a mesh as one sequence of keys: tetrahedra, then
+// pyramids, prisms and hexahedra, each in its own order (the order the
+// element loops of the dual visit them), with each node's incident elements
+// in increasing key order.
+struct Cells {
+    const int *v[4];     // node lists per type
+    int nn[4];           // nodes per element
+    int64_t off[5];      // first key of each type; off[4] = elements
+    const int (*edges[4])[2];
+    int nedge[4];
+    std::vector<int64_t> ptr;  // [nnode+1] into key
+    std::vector<int> key;
+
+    explicit Cells(const HostMesh &m) {
+        const std::vector<int> *lists[4] = {&m.tets, &m.pyrs, &m.prisms, &m.hexes};
+        const int nns[4] = {4, kPyr.nnode, kPrism.nnode, kHex.nnode};
+        const int (*eds[4])[2] = {kTetEdges, kPyrEdges, kPrismEdges, kHexEdges};
+        const int nes[4] = {6, kPyr.nedge, kPrism.nedge, kHex.nedge};
+        off[0] = 0;
+        for (int t = 0; t < 4; t++) {
+            v[t] = lists[t]->data();
+            nn[t] = nns[t];
+            edges[t] = eds[t];
+            nedge[t] = nes[t];
+            off[t + 1] = off[t] + (int64_t)lists[t]->size() / nns[t];
         }
-    for (int a = 0; a < nnode; a++) std::sort(ja.begin() + ia[a], ja.begin() + ia[a + 1]);
+        ptr.assign((size_t)m.nnode + 1, 0);
+        for (int t = 0; t < 4; t++)
+            for (int64_t e = 0; e < off[t + 1] - off[t]; e++)
+                for (int k = 0; k < nn[t]; k++) ptr[v[t][e * nn[t] + k] + 1]++;
+        for (int a = 0; a < m.nnode; a++) ptr[a + 1] += ptr[a];
+        key.resize(ptr[m.nnode]);
+        std::vector<int64_t> fill(ptr.begin(), ptr.end() - 1);
+        for (int t = 0; t < 4; t++)
+            for (int64_t e = 0; e < off[t + 1] - off[t]; e++)
+                for (int k = 0; k < nn[t]; k++) key[fill[v[t][e * nn[t] + k]]++] = (int)(off[t] + e);
+    }
+    int type_of(int k) const {
+        int t = 0;
+        while (k >= off[t + 1]) t++;
+        return t;
+    }
+};
+
+// Symmetric node graph of a mesh: CRS without diagonal, rows sorted.  Each
+// row is gathered from the node's incident elements (their edges through the
+// node), in parallel over node ranges.
+void build_graph(const HostMesh &msh, const Cells &cells, std::vector<int> &ia, std::vector<int> &ja) {
+    const int nnode = msh.nnode;
+    auto row = [&](int a, std::vector<int> &nb) {
+        nb.clear();
+        for (int64_t q = cells.ptr[a]; q < cells.ptr[a + 1]; q++) {
+            const int k = cells.key[q], t = cells.type_of(k);
+            const int *v = cells.v[t] + (int64_t)(k - cells.off[t]) * cells.nn[t];
+            for (int p = 0; p < cells.nedge[t]; p++) {
+                const int x = v[cells.edges[t][p][0]], y = v[cells.edges[t][p][1]];
+                if (x == a) nb.push_back(y);
+                else if (y == a) nb.push_back(x);
+            }
+        }
+        std::sort(nb.begin(), nb.end());
+        nb.erase(std::unique(nb.begin(), nb.end()), nb.end());
+    };
+    // rows of each range into that range's own buffer, then placed in one copy
+    ia.assign(nnode + 1, 0);
+    const int nt = range_count(nnode);
+    std::vector<std::vector<int>> part(nt);
+    std::vector<int> part_lo(nt, 0);
+    parallel_ranges(nnode, [&](int t, int lo, int hi) {
+        std::vector<int> nb, buf;
+        for (int a = lo; a < hi; a++) {
+            row(a, nb);
+            ia[a + 1] = (int)nb.size();
+            buf.insert(buf.end(), nb.begin(), nb.end());
+        }
+        part[t].swap(buf);
+        part_lo[t] = lo;
+    });
+    for (int a = 0; a < nnode; a++) ia[a + 1] += ia[a];
+    ja.assign(ia[nnode], 0);
+    for (int t = 0; t < nt; t++) std::copy(part[t].begin(), part[t].end(), ja.begin() + ia[part_lo[t]]);
+}
+
+void build_graph(const HostMesh &msh, std::vector<int> &ia, std::vector<int> &ja) {
+    const Cells cells(msh);
+    build_graph(msh, cells, ia, ja);
 }
 
 // Reverse Cuthill-McKee, O(N + E log d).  Start node: a pseudo-peripheral node
@@ -190,7 +245,7 @@ std::vector<int> rcm_order(int n, const std::vector<int> &ia, const std::vector<
 // Recursive coordinate bisection into patches of exactly `psz` nodes (the last
 // one may be smaller): split the longest extent at a multiple of psz near the
 // middle.  Returns nodes in patch-major order.
-void rcb_patches(const std::vector<double> &xyz, int psz, std::vector<int> &idx, int lo, int hi) {
+void rcb_patches(const std::vector<double> &xyz, int psz, std::vector<int> &idx, int lo, int hi, int depth = 0) {
     const int n = hi - lo;
     if (n <= psz) return;
     double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
@@ -209,8 +264,15 @@ void rcb_patches(const std::vector<double> &xyz, int psz, std::vector<int> &idx,
         const double va = xyz[3 * (size_t)a + ax], vb = xyz[3 * (size_t)b + ax];
         return va < vb || (va == vb && a < b);
     });
-    rcb_patches(xyz, psz, idx, lo, mid);
-    rcb_patches(xyz, psz, idx, mid, hi);
+    // the halves are independent: the first levels split across threads
+    if (depth < 3 && n >= 65536 && std::thread::hardware_concurrency() > 1) {
+        std::thread left([&] { rcb_patches(xyz, psz, idx, lo, mid, depth + 1); });
+        rcb_patches(xyz, psz, idx, mid, hi, depth + 1);
+        left.join();
+        return;
+    }
+    rcb_patches(xyz, psz, idx, lo, mid, depth + 1);
+    rcb_patches(xyz, psz, idx, mid, hi, depth + 1);
 }
 
 // Blocked reverse Cuthill-McKee: RCB patches of psz nodes, patches ordered by
@@ -226,17 +288,22 @@ std::vector<int> patch_rcm_order(int n, const std::vector<double> &xyz, const st
     const int np = (n + psz - 1) / psz;
     std::vector<int> pid(n);
     for (int k = 0; k < n; k++) pid[idx[k]] = k / psz;
-    // patch graph
+    // patch graph, each patch's row from its own nodes (patch p = idx[p*psz ..])
     std::vector<std::vector<int>> adj(np);
-    for (int a = 0; a < n; a++)
-        for (int k = ia[a]; k < ia[a + 1]; k++) {
-            const int pa = pid[a], pb = pid[ja[k]];
-            if (pa != pb) adj[pa].push_back(pb);
+    parallel_ranges(np, [&](int, int lo, int hi) {
+        for (int p = lo; p < hi; p++) {
+            std::vector<int> &r = adj[p];
+            for (int q = p * psz; q < std::min(n, (p + 1) * psz); q++) {
+                const int a = idx[q];
+                for (int k = ia[a]; k < ia[a + 1]; k++)
+                    if (pid[ja[k]] != p) r.push_back(pid[ja[k]]);
+            }
+            std::sort(r.begin(), r.end());
+            r.erase(std::unique(r.begin(), r.end()), r.end());
         }
+    });
     std::vector<int> pia(np + 1, 0), pja;
     for (int p = 0; p < np; p++) {
-        std::sort(adj[p].begin(), adj[p].end());
-        adj[p].erase(std::unique(adj[p].begin(), adj[p].end()), adj[p].end());
         pia[p + 1] = pia[p] + (int)adj[p].size();
         pja.insert(pja.end(), adj[p].begin(), adj[p].end());
     }
@@ -258,19 +325,31 @@ std::vector<int> patch_rcm_order(int n, const std::vector<double> &xyz, const st
 // Build the median-dual metrics of a tet mesh into m (coords/tets/tris set).
 static int build_dual(HostMesh &m) {
     const int nnode = m.nnode;
-    const int64_t ntet = (int64_t)m.tets.size() / 4;
-    build_graph(m, m.n2n_ia, m.n2n_ja);
+    const Cells cells(m);
+    build_graph(m, cells, m.n2n_ia, m.n2n_ja);
 
     // Interior edges = upper half of the graph, ordered by (L, R).
-    m.edge_nodes.clear();
     std::vector<int> eoff(nnode + 1, 0);  // first edge of each L
-    for (int a = 0; a < nnode; a++) {
-        eoff[a] = (int)(m.edge_nodes.size() / 2);
-        for (int k = m.n2n_ia[a]; k < m.n2n_ia[a + 1]; k++)
-            if (m.n2n_ja[k] > a) { m.edge_nodes.push_back(a); m.edge_nodes.push_back(m.n2n_ja[k]); }
-    }
-    eoff[nnode] = (int)(m.edge_nodes.size() / 2);
+    parallel_ranges(nnode, [&](int, int lo, int hi) {
+        for (int a = lo; a < hi; a++) {
+            const int *r = &m.n2n_ja[m.n2n_ia[a]], *r1 = &m.n2n_ja[0] + m.n2n_ia[a + 1];
+            eoff[a + 1] = (int)(r1 - std::upper_bound(r, r1, a));  // rows are sorted
+        }
+    });
+    for (int a = 0; a < nnode; a++) eoff[a + 1] += eoff[a];
     const int nedge = eoff[nnode];
+    m.edge_nodes.assign((size_t)2 * nedge, 0);
+    parallel_ranges(nnode, [&](int, int lo, int hi) {
+        for (int a = lo; a < hi; a++) {
+            int e = eoff[a];
+            for (int k = m.n2n_ia[a]; k < m.n2n_ia[a + 1]; k++)
+                if (m.n2n_ja[k] > a) {
+                    m.edge_nodes[2 * (size_t)e] = a;
+                    m.edge_nodes[2 * (size_t)e + 1] = m.n2n_ja[k];
+                    e++;
+                }
+        }
+    });
     m.nedge = nedge;
     m.edge_areav.assign((size_t)3 * nedge, 0.0);
     m.cvol.assign(nnode, 0.0);
@@ -285,61 +364,21 @@ static int build_dual(HostMesh &m) {
         return lo;
     };
 
+    // The dual is gathered per node, in parallel over node ranges: node a
+    // visits its incident elements in element order and adds, for every
+    // element edge (a, b) with b > a, the edge's dual-face area to edge (a, b),
+    // and its own share of every element to its control volume.  Each edge and
+    // each volume receives the same terms, formed by the same operations, in
+    // the same order as one loop over the elements would add them, so the
+    // results are the same bit for bit.
+    std::vector<int> bad_in(range_count(nnode), 0);  // tetrahedra with non-positive volume, per range
     static const int pairs[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
     static const int others[6][2] = {{2, 3}, {1, 3}, {1, 2}, {0, 3}, {0, 2}, {0, 1}};
-    int bad = 0;
-    for (int64_t t = 0; t < ntet; t++) {
-        const int *v = &m.tets[4 * t];
-        const double *x[4];
-        for (int k = 0; k < 4; k++) x[k] = &m.coords[3 * (size_t)v[k]];
-        double g[3];
-        for (int d = 0; d < 3; d++) g[d] = 0.25 * (x[0][d] + x[1][d] + x[2][d] + x[3][d]);
-        double e1[3], e2[3], e3[3], c[3];
-        sub3(x[1], x[0], e1); sub3(x[2], x[0], e2); sub3(x[3], x[0], e3);
-        cross3(e2, e3, c);
-        double vol = dot3(e1, c) / 6.0;
-        if (!(vol > 0.0)) bad++;
-        for (int k = 0; k < 4; k++) m.cvol[v[k]] += 0.25 * std::fabs(vol);
-        for (int p = 0; p < 6; p++) {
-            int ia_ = pairs[p][0], ib = pairs[p][1];
-            int ic = others[p][0], id = others[p][1];
-            double mid[3], f1[3], f2[3];
-            for (int d = 0; d < 3; d++) {
-                mid[d] = 0.5 * (x[ia_][d] + x[ib][d]);
-                f1[d] = (x[ia_][d] + x[ib][d] + x[ic][d]) / 3.0;
-                f2[d] = (x[ia_][d] + x[ib][d] + x[id][d]) / 3.0;
-            }
-            double r1[3], r2[3], rg[3], s1[3], s2[3], S[3];
-            sub3(f1, mid, r1); sub3(g, mid, rg); sub3(f2, mid, r2);
-            cross3(r1, rg, s1);
-            cross3(rg, r2, s2);
-            for (int d = 0; d < 3; d++) S[d] = 0.5 * (s1[d] + s2[d]);
-            // orient from the lower to the higher node index
-            int a = v[ia_], b = v[ib];
-            double ab[3];
-            sub3(&m.coords[3 * (size_t)std::max(a, b)], &m.coords[3 * (size_t)std::min(a, b)], ab);
-            double sgn = dot3(S, ab) >= 0.0 ? 1.0 : -1.0;
-            int e = edge_id(std::min(a, b), std::max(a, b));
-            for (int d = 0; d < 3; d++) m.edge_areav[3 * (size_t)e + d] += sgn * S[d];
-        }
-    }
-    if (bad) {
-        std::fprintf(stderr, "cfd mesh: %d tetrahedra with non-positive volume\n", bad);
-        return CFD_ERR_MESH;
-    }
-
-    // Pyramids, prisms and hexahedra (Area_Volume.cpp:659-822): per element
-    // edge (a, b) the two triangles mid-edge -> face centroid -> element
-    // centroid over the two faces that share the edge, S = (g - m) x (f1 - m) / 2
-    // + (f2 - m) x (g - m) / 2, oriented from the lower to the higher node index;
-    // each end node gets the volumes of the small tetrahedra (node, m, f, g).
-    const std::pair<const std::vector<int> *, const ElemType *> types[3] = {
-        {&m.pyrs, &kPyr}, {&m.prisms, &kPrism}, {&m.hexes, &kHex}};
-    for (const auto &tt : types) {
-        const std::vector<int> &cells = *tt.first;
-        const ElemType &T = *tt.second;
-        // the two faces of each local edge
-        int ef[12][2];
+    // the two faces of each local edge of the pyramid, prism and hexahedron
+    const ElemType *types[4] = {nullptr, &kPyr, &kPrism, &kHex};
+    int ef[4][12][2];
+    for (int tt = 1; tt < 4; tt++) {
+        const ElemType &T = *types[tt];
         for (int p = 0; p < T.nedge; p++) {
             int k = 0;
             for (int f = 0; f < T.nface && k < 2; f++) {
@@ -348,45 +387,110 @@ static int build_dual(HostMesh &m) {
                     ha |= T.face[f][q] == T.edges[p][0];
                     hb |= T.face[f][q] == T.edges[p][1];
                 }
-                if (ha && hb) ef[p][k++] = f;
+                if (ha && hb) ef[tt][p][k++] = f;
             }
         }
-        for (size_t c = 0; c + T.nnode <= cells.size(); c += T.nnode) {
-            const int *v = &cells[c];
-            double g[3] = {0, 0, 0};
-            for (int k = 0; k < T.nnode; k++)
-                for (int d = 0; d < 3; d++) g[d] += m.coords[3 * (size_t)v[k] + d];
-            for (int d = 0; d < 3; d++) g[d] /= T.nnode;
-            for (int p = 0; p < T.nedge; p++) {
-                const int a = v[T.edges[p][0]], b = v[T.edges[p][1]];
-                const double *xa = &m.coords[3 * (size_t)a], *xb = &m.coords[3 * (size_t)b];
-                double mid[3], fc[2][3], rg[3], r1[3], r2[3], s1[3], s2[3], S[3];
-                for (int d = 0; d < 3; d++) mid[d] = (xa[d] + xb[d]) / 2.0;
-                for (int k = 0; k < 2; k++) {
-                    const int *fn = T.face[ef[p][k]];
-                    const int nf = fn[3] >= 0 ? 4 : 3;
-                    for (int d = 0; d < 3; d++) {
-                        double acc = 0.0;
-                        for (int q = 0; q < nf; q++) acc += m.coords[3 * (size_t)v[fn[q]] + d];
-                        fc[k][d] = acc / (double)nf;
+    }
+    parallel_ranges(nnode, [&](int rt, int lo_node, int hi_node) {
+        for (int a = lo_node; a < hi_node; a++) {
+            double cv = 0.0;
+            for (int64_t q = cells.ptr[a]; q < cells.ptr[a + 1]; q++) {
+                const int key = cells.key[q], tt = cells.type_of(key);
+                const int *v = cells.v[tt] + (int64_t)(key - cells.off[tt]) * cells.nn[tt];
+                if (tt == 0) {
+                    // tetrahedron (Area_Volume.cpp:659-800): V/4 per vertex; per edge the
+                    // two triangles mid-edge -> face centroid -> tet centroid
+                    const double *x[4];
+                    for (int k = 0; k < 4; k++) x[k] = &m.coords[3 * (size_t)v[k]];
+                    double g[3];
+                    for (int d = 0; d < 3; d++) g[d] = 0.25 * (x[0][d] + x[1][d] + x[2][d] + x[3][d]);
+                    double e1[3], e2[3], e3[3], c[3];
+                    sub3(x[1], x[0], e1); sub3(x[2], x[0], e2); sub3(x[3], x[0], e3);
+                    cross3(e2, e3, c);
+                    const double vol = dot3(e1, c) / 6.0;
+                    if (!(vol > 0.0) && a == std::min(std::min(v[0], v[1]), std::min(v[2], v[3]))) bad_in[rt]++;
+                    cv += 0.25 * std::fabs(vol);
+                    for (int p = 0; p < 6; p++) {
+                        const int ia_ = pairs[p][0], ib = pairs[p][1];
+                        const int ea = v[ia_], eb = v[ib];
+                        if (std::min(ea, eb) != a) continue;  // the edge's lower node gathers it
+                        const int ic = others[p][0], id = others[p][1];
+                        double mid[3], f1[3], f2[3];
+                        for (int d = 0; d < 3; d++) {
+                            mid[d] = 0.5 * (x[ia_][d] + x[ib][d]);
+                            f1[d] = (x[ia_][d] + x[ib][d] + x[ic][d]) / 3.0;
+                            f2[d] = (x[ia_][d] + x[ib][d] + x[id][d]) / 3.0;
+                        }
+                        double r1[3], r2[3], rg[3], s1[3], s2[3], S[3];
+                        sub3(f1, mid, r1); sub3(g, mid, rg); sub3(f2, mid, r2);
+                        cross3(r1, rg, s1);
+                        cross3(rg, r2, s2);
+                        for (int d = 0; d < 3; d++) S[d] = 0.5 * (s1[d] + s2[d]);
+                        // orient from the lower to the higher node index
+                        double ab[3];
+                        sub3(&m.coords[3 * (size_t)std::max(ea, eb)], &m.coords[3 * (size_t)std::min(ea, eb)], ab);
+                        const double sgn = dot3(S, ab) >= 0.0 ? 1.0 : -1.0;
+                        const int e = edge_id(a, std::max(ea, eb));
+                        for (int d = 0; d < 3; d++) m.edge_areav[3 * (size_t)e + d] += sgn * S[d];
+                    }
+                    continue;
+                }
+                // pyramid, prism, hexahedron (Area_Volume.cpp:659-822): per element edge
+                // (a, b) the two triangles mid-edge -> face centroid -> element centroid
+                // over the two faces sharing the edge, S = (g - m) x (f1 - m) / 2 +
+                // (f2 - m) x (g - m) / 2, oriented from the lower to the higher node
+                // index; each end node gets the small tetrahedra (node, m, f, g).
+                const ElemType &T = *types[tt];
+                double g[3] = {0, 0, 0};
+                for (int k = 0; k < T.nnode; k++)
+                    for (int d = 0; d < 3; d++) g[d] += m.coords[3 * (size_t)v[k] + d];
+                for (int d = 0; d < 3; d++) g[d] /= T.nnode;
+                for (int p = 0; p < T.nedge; p++) {
+                    const int ea = v[T.edges[p][0]], eb = v[T.edges[p][1]];
+                    if (ea != a && eb != a) continue;
+                    const double *xa = &m.coords[3 * (size_t)ea], *xb = &m.coords[3 * (size_t)eb];
+                    double mid[3], fc[2][3], rg[3], r1[3], r2[3], s1[3], s2[3], S[3];
+                    for (int d = 0; d < 3; d++) mid[d] = (xa[d] + xb[d]) / 2.0;
+                    for (int k = 0; k < 2; k++) {
+                        const int *fn = T.face[ef[tt][p][k]];
+                        const int nf = fn[3] >= 0 ? 4 : 3;
+                        for (int d = 0; d < 3; d++) {
+                            double acc = 0.0;
+                            for (int r = 0; r < nf; r++) acc += m.coords[3 * (size_t)v[fn[r]] + d];
+                            fc[k][d] = acc / (double)nf;
+                        }
+                    }
+                    sub3(g, mid, rg); sub3(fc[0], mid, r1); sub3(fc[1], mid, r2);
+                    cross3(rg, r1, s1);
+                    cross3(r2, rg, s2);
+                    for (int d = 0; d < 3; d++) S[d] = 0.5 * s1[d] + 0.5 * s2[d];
+                    const int lo = std::min(ea, eb), hi = std::max(ea, eb);
+                    if (lo == a) {
+                        double ab[3];
+                        sub3(&m.coords[3 * (size_t)hi], &m.coords[3 * (size_t)lo], ab);
+                        const double sgn = dot3(S, ab) >= 0.0 ? 1.0 : -1.0;
+                        const int e = edge_id(lo, hi);
+                        for (int d = 0; d < 3; d++) m.edge_areav[3 * (size_t)e + d] += sgn * S[d];
+                    }
+                    if (ea == a) {
+                        double da[3];
+                        sub3(xa, mid, da);
+                        cv += (std::fabs(dot3(da, s1)) + std::fabs(dot3(da, s2))) / 6.0;
+                    } else {
+                        double db[3];
+                        sub3(xb, mid, db);
+                        cv += (std::fabs(dot3(db, s1)) + std::fabs(dot3(db, s2))) / 6.0;
                     }
                 }
-                sub3(g, mid, rg); sub3(fc[0], mid, r1); sub3(fc[1], mid, r2);
-                cross3(rg, r1, s1);
-                cross3(r2, rg, s2);
-                for (int d = 0; d < 3; d++) S[d] = 0.5 * s1[d] + 0.5 * s2[d];
-                const int lo = std::min(a, b), hi = std::max(a, b);
-                double ab[3];
-                sub3(&m.coords[3 * (size_t)hi], &m.coords[3 * (size_t)lo], ab);
-                const double sgn = dot3(S, ab) >= 0.0 ? 1.0 : -1.0;
-                const int e = edge_id(lo, hi);
-                for (int d = 0; d < 3; d++) m.edge_areav[3 * (size_t)e + d] += sgn * S[d];
-                double da[3], db[3];
-                sub3(xa, mid, da); sub3(xb, mid, db);
-                m.cvol[a] += (std::fabs(dot3(da, s1)) + std::fabs(dot3(da, s2))) / 6.0;
-                m.cvol[b] += (std::fabs(dot3(db, s1)) + std::fabs(dot3(db, s2))) / 6.0;
             }
+            m.cvol[a] = cv;
         }
+    });
+    int bad = 0;
+    for (int b : bad_in) bad += b;
+    if (bad) {
+        std::fprintf(stderr, "cfd mesh: %d tetrahedra with non-positive volume\n", bad);
+        return CFD_ERR_MESH;
     }
 
     // Boundary edges: one per boundary-triangle (then -quadrilateral) vertex, own ghost node.
