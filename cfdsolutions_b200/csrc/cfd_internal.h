@@ -9,6 +9,11 @@
 
 namespace cfd {
 
+// Threads the host mesh builder may use on the calling thread (0: up to 16).
+// The serving workers set a small number, so that a request's mesh build
+// does not take the cores the other workers' launches run on.
+inline thread_local int g_host_threads = 0;
+
 // Host mesh produced by the builder (mesh.cpp).
 struct HostMesh {
     int nnode = 0, nghost = 0, nedge = 0, nbedge = 0;

@@ -75,11 +75,12 @@ const ElemType kPrism = {6, 9, 5, kPrismEdges,
 const ElemType kHex = {8, 12, 6, kHexEdges,
                        {{0, 1, 2, 3}, {4, 5, 6, 7}, {0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {3, 0, 4, 7}}};
 
-// Ranges [0, n) is split into for parallel_ranges: up to 16, one below
-// 65,536 items.
+// Ranges [0, n) is split into for parallel_ranges: up to 16 (or the calling
+// thread's g_host_threads), one below 65,536 items.
 inline int range_count(int n) {
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    return n < 65536 ? 1 : (int)std::min(16u, hw);
+    const unsigned cap = g_host_threads > 0 ? (unsigned)g_host_threads : 16u;
+    return n < 65536 ? 1 : (int)std::min(cap, hw);
 }
 
 // fn(t, lo, hi) for the range_count(n) contiguous ranges t of [0, n), one
@@ -265,7 +266,7 @@ void rcb_patches(const std::vector<double> &xyz, int psz, std::vector<int> &idx,
         return va < vb || (va == vb && a < b);
     });
     // the halves are independent: the first levels split across threads
-    if (depth < 3 && n >= 65536 && std::thread::hardware_concurrency() > 1) {
+    if (depth < 3 && (1 << (depth + 1)) <= range_count(n) && n >= 65536) {
         std::thread left([&] { rcb_patches(xyz, psz, idx, lo, mid, depth + 1); });
         rcb_patches(xyz, psz, idx, mid, hi, depth + 1);
         left.join();

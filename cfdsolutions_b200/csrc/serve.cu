@@ -295,6 +295,7 @@ void cfd_server::run_worker() {
     cudaStream_t s = nullptr;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return;
     cfd::g_alloc_async = true;
+    cfd::g_host_threads = 2;  // mesh builds share the host with the other workers
     cfd::g_alloc_stream = s;
     for (;;) {
         int64_t id;
