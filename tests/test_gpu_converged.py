@@ -10,7 +10,7 @@ Euler3D's own B = -Res leaves the dissipation out), until the residual stops
 falling (its round-off floor).  The GPU solves the same steady problem with
 GMRES(30) + block-multicolour ILU(0) and FP64, FP32 or BF16 storage of the
 Jacobian.  Both are fixed points of the same discrete residual, so the
-converged density, momentum and energy must agree to the north star's 1e-8
+converged density, momentum and energy must agree to 1e-8
 (relative to each field's largest magnitude); observed: FP64 and FP32 about
 1e-11, BF16 the same after its slightly different path.
 """
