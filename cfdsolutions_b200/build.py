@@ -25,7 +25,7 @@ CU_SOURCES = ["core.cu", "gradient.cu", "linsolve.cu", "ilu_mc.cu", "gs_static.c
 # expression as written (no fused multiply-add) to reproduce the reference
 FILE_FLAGS = {"fd_jacobian.cu": ["-fmad=false"]}
 CXX_SOURCES = ["mesh.cpp", "vtk.cpp", "rmsio.cpp"]
-HEADERS = ["cfd_internal.h", "ctx.cuh", "kernels.cuh", "physics.cuh", "ilu_mc.cuh"]
+HEADERS = ["cfd_internal.h", "host_par.h", "ctx.cuh", "kernels.cuh", "physics.cuh", "ilu_mc.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "ctx.cuh"
+#include "host_par.h"
 #include "kernels.cuh"
 
 namespace cfd {
@@ -1686,10 +1687,12 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
     std::vector<double4> eg(nedge);
     {
         std::vector<double4> es(nedge);
-        for (int e = 0; e < nedge; e++) {
-            en[e] = make_int2(edge_nodes[2 * e], edge_nodes[2 * e + 1]);
-            geo(edge_areav + 3 * (size_t)e, eg[e], es[e]);
-        }
+        parallel_ranges(nedge, [&](int, int64_t lo, int64_t hi) {
+            for (int64_t e = lo; e < hi; e++) {
+                en[e] = make_int2(edge_nodes[2 * e], edge_nodes[2 * e + 1]);
+                geo(edge_areav + 3 * (size_t)e, eg[e], es[e]);
+            }
+        });
         std::vector<int2> bnv(nbedge);
         std::vector<double4> bgv(nbedge), bsv(nbedge);
         for (int e = 0; e < nbedge; e++) {
@@ -1716,7 +1719,9 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
     // physical graph, rows sorted (the reference's list order is insertion order;
     // gradients and limiters are order-insensitive to round-off)
     std::vector<int> gia(n2n_ia, n2n_ia + nnode + 1), gja(n2n_ja, n2n_ja + n2n_ia[nnode]);
-    for (int i = 0; i < nnode; i++) std::sort(gja.begin() + gia[i], gja.begin() + gia[i + 1]);
+    parallel_ranges(nnode, [&](int, int64_t lo, int64_t hi) {
+        for (int64_t i = lo; i < hi; i++) std::sort(gja.begin() + gia[i], gja.begin() + gia[i + 1]);
+    });
     CFD_CUDA(c->n2n_ia.upload(gia.data(), gia.size(), s));
     CFD_CUDA(c->n2n_ja.upload(gja.data(), gja.size(), s));
 
@@ -1732,16 +1737,18 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
             nb[fill[a]] = b; lst[fill[a]++] = e;
             nb[fill[b]] = a; lst[fill[b]++] = ~e;
         }
-        std::vector<int> idx;
-        for (int i = 0; i < nnode; i++) {
-            const int lo = ptr[i], hi = ptr[i + 1];
-            idx.resize(hi - lo);
-            std::iota(idx.begin(), idx.end(), lo);
-            std::sort(idx.begin(), idx.end(), [&](int x, int y) { return nb[x] < nb[y]; });
-            std::vector<int> tmp(hi - lo);
-            for (int k = 0; k < hi - lo; k++) tmp[k] = lst[idx[k]];
-            std::copy(tmp.begin(), tmp.end(), lst.begin() + lo);
-        }
+        parallel_ranges(nnode, [&](int, int64_t r0, int64_t r1) {
+            std::vector<int> idx, tmp;
+            for (int64_t i = r0; i < r1; i++) {
+                const int lo = ptr[i], hi = ptr[i + 1];
+                idx.resize(hi - lo);
+                std::iota(idx.begin(), idx.end(), lo);
+                std::sort(idx.begin(), idx.end(), [&](int x, int y) { return nb[x] < nb[y]; });
+                tmp.resize(hi - lo);
+                for (int k = 0; k < hi - lo; k++) tmp[k] = lst[idx[k]];
+                std::copy(tmp.begin(), tmp.end(), lst.begin() + lo);
+            }
+        });
         CFD_CUDA(c->n2e_ptr.upload(ptr.data(), ptr.size(), s));
         CFD_CUDA(c->n2e.upload(lst.data(), lst.size(), s));
         CFD_CUDA(stream_wait(s));
@@ -1759,15 +1766,17 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         }
         std::vector<int> sn(std::max<int64_t>(sp[nsl], 1), 0);
         std::vector<double4> sg(std::max<int64_t>(sp[nsl], 1), make_double4(0, 0, 0, 0));
-        for (int i = 0; i < nnode; i++) {
-            const int64_t b = sp[i >> 5] + (i & 31);
-            for (int k = ptr[i]; k < ptr[i + 1]; k++) {
-                const int t = lst[k], e = t >= 0 ? t : ~t;
-                const int64_t slot = b + 32 * (int64_t)(k - ptr[i]);
-                sn[slot] = t >= 0 ? en[e].y : ~en[e].x;
-                sg[slot] = eg[e];
+        parallel_ranges(nnode, [&](int, int64_t r0, int64_t r1) {
+            for (int64_t i = r0; i < r1; i++) {
+                const int64_t b = sp[i >> 5] + (i & 31);
+                for (int k = ptr[i]; k < ptr[i + 1]; k++) {
+                    const int t = lst[k], e = t >= 0 ? t : ~t;
+                    const int64_t slot = b + 32 * (int64_t)(k - ptr[i]);
+                    sn[slot] = t >= 0 ? en[e].y : ~en[e].x;
+                    sg[slot] = eg[e];
+                }
             }
-        }
+        });
         CFD_CUDA(c->sell_ptr.upload(sp.data(), sp.size(), s));
         CFD_CUDA(c->sell_nbr.upload(sn.data(), sn.size(), s));
         CFD_CUDA(c->sell_geo.upload(sg.data(), sg.size(), s));
@@ -1874,28 +1883,34 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         c->nnzb = c->h_IA[nnode];
         c->h_JA.assign(c->nnzb, 0);
         c->h_IAU.assign(nnode, 0);
-        for (int i = 0; i < nnode; i++) {
-            int k = c->h_IA[i];
-            bool placed = false;
-            for (int m = gia[i]; m < gia[i + 1]; m++) {
-                if (!placed && gja[m] > i) { c->h_IAU[i] = k; c->h_JA[k++] = i; placed = true; }
-                c->h_JA[k++] = gja[m];
+        parallel_ranges(nnode, [&](int, int64_t r0, int64_t r1) {
+            for (int i = (int)r0; i < (int)r1; i++) {
+                int k = c->h_IA[i];
+                bool placed = false;
+                for (int m = gia[i]; m < gia[i + 1]; m++) {
+                    if (!placed && gja[m] > i) { c->h_IAU[i] = k; c->h_JA[k++] = i; placed = true; }
+                    c->h_JA[k++] = gja[m];
+                }
+                if (!placed) { c->h_IAU[i] = k; c->h_JA[k++] = i; }
             }
-            if (!placed) { c->h_IAU[i] = k; c->h_JA[k++] = i; }
-        }
+        });
         auto slot = [&](int r, int col) {
             auto b = c->h_JA.begin() + c->h_IA[r], e = c->h_JA.begin() + c->h_IA[r + 1];
             auto it = std::lower_bound(b, e, col);
             return (int)(it - c->h_JA.begin());
         };
         std::vector<int> ts(c->nnzb);
-        for (int i = 0; i < nnode; i++)
-            for (int k = c->h_IA[i]; k < c->h_IA[i + 1]; k++) ts[k] = slot(c->h_JA[k], i);
+        parallel_ranges(nnode, [&](int, int64_t r0, int64_t r1) {
+            for (int i = (int)r0; i < (int)r1; i++)
+                for (int k = c->h_IA[i]; k < c->h_IA[i + 1]; k++) ts[k] = slot(c->h_JA[k], i);
+        });
         std::vector<int2> es(nedge);
-        for (int e = 0; e < nedge; e++) {
-            const int a = edge_nodes[2 * e], b = edge_nodes[2 * e + 1];
-            es[e] = make_int2(slot(a, b), slot(b, a));
-        }
+        parallel_ranges(nedge, [&](int, int64_t e0, int64_t e1) {
+            for (int64_t e = e0; e < e1; e++) {
+                const int a = edge_nodes[2 * e], b = edge_nodes[2 * e + 1];
+                es[e] = make_int2(slot(a, b), slot(b, a));
+            }
+        });
         CFD_CUDA(c->IA.upload(c->h_IA.data(), c->h_IA.size(), s));
         CFD_CUDA(c->JA.upload(c->h_JA.data(), c->h_JA.size(), s));
         CFD_CUDA(c->IAU.upload(c->h_IAU.data(), c->h_IAU.size(), s));

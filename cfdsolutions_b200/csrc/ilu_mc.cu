@@ -29,6 +29,7 @@
 #include "ctx.cuh"
 #include "kernels.cuh"
 #include "ilu_mc.cuh"
+#include "host_par.h"
 
 namespace cfd {
 
@@ -471,16 +472,18 @@ int mc_build(cfd_ctx *c) {
     // greedy colouring in patch order needs 13-14, i.e. fewer launches per
     // factorisation and per triangular solve.
     std::vector<std::vector<int>> adj(np);
-    for (int P = 0; P < np; P++) {
-        const int r0 = P * kMcRows, r1 = std::min(n, r0 + kMcRows);
-        for (int i = r0; i < r1; i++)
-            for (int k = IA[i]; k < IA[i + 1]; k++) {
-                const int Q = JA[k] / kMcRows;
-                if (Q != P) adj[P].push_back(Q);
-            }
-        std::sort(adj[P].begin(), adj[P].end());
-        adj[P].erase(std::unique(adj[P].begin(), adj[P].end()), adj[P].end());
-    }
+    parallel_ranges(np, [&](int, int64_t p0, int64_t p1) {
+        for (int P = (int)p0; P < (int)p1; P++) {
+            const int r0 = P * kMcRows, r1 = std::min(n, r0 + kMcRows);
+            for (int i = r0; i < r1; i++)
+                for (int k = IA[i]; k < IA[i + 1]; k++) {
+                    const int Q = JA[k] / kMcRows;
+                    if (Q != P) adj[P].push_back(Q);
+                }
+            std::sort(adj[P].begin(), adj[P].end());
+            adj[P].erase(std::unique(adj[P].begin(), adj[P].end()), adj[P].end());
+        }
+    });
     std::vector<int> color(np, -1);
     std::vector<uint64_t> seen(np, 0);  // colours among a patch's neighbours
     std::set<std::tuple<int, int, int>> open;  // (-saturation, -degree, patch)
@@ -518,9 +521,11 @@ int mc_build(cfd_ctx *c) {
     std::vector<int> slot(c->nnzb), scol(c->nnzb);
     std::vector<int4> meta(n);
     std::vector<int> lf(n, 0), lb(n, 0);
+    std::vector<int> maxrow_in(range_count(n), 0);
+    parallel_ranges(n, [&](int rt, int64_t i0, int64_t i1) {
     std::vector<std::pair<int64_t, int>> lo, up;
-    int maxrow = 0;
-    for (int i = 0; i < n; i++) {
+    int &maxrow = maxrow_in[rt];
+    for (int i = (int)i0; i < (int)i1; i++) {
         lo.clear();
         up.clear();
         const int64_t ki = key(i);
@@ -549,11 +554,15 @@ int mc_build(cfd_ctx *c) {
         meta[i] = make_int4(next, (int)lo.size(), nint, 0);
         maxrow = std::max(maxrow, IA[i + 1] - IA[i]);
     }
-    for (int64_t u = 0; u < c->nnzb; u++) scol[u] = JA[slot[u]];
-    // patch-local dependency levels
+    });
+    const int maxrow = *std::max_element(maxrow_in.begin(), maxrow_in.end());
+    parallel_ranges(c->nnzb, [&](int, int64_t u0, int64_t u1) {
+        for (int64_t u = u0; u < u1; u++) scol[u] = JA[slot[u]];
+    });
+    // patch-local dependency levels (a patch's rows depend only on its own rows)
     std::vector<int2> plev(np, make_int2(0, 0));
-    int maxlev = 0;
-    for (int P = 0; P < np; P++) {
+    parallel_ranges(np, [&](int, int64_t q0, int64_t q1) {
+    for (int P = (int)q0; P < (int)q1; P++) {
         const int r0 = P * kMcRows, r1 = std::min(n, r0 + kMcRows);
         for (int i = r0; i < r1; i++) {
             int l = 0;
@@ -568,37 +577,50 @@ int mc_build(cfd_ctx *c) {
             lb[i] = l;
             plev[P].y = std::max(plev[P].y, l);
         }
-        maxlev = std::max(maxlev, std::max(plev[P].x, plev[P].y));
     }
+    });
+    int maxlev = 0;
+    for (int P = 0; P < np; P++) maxlev = std::max(maxlev, std::max(plev[P].x, plev[P].y));
     for (int i = 0; i < n; i++) meta[i].w = lf[i] | (lb[i] << 16);
     // update lists of the factorisation: for lower block (i,p), the upper
     // blocks (p,j) of row p whose column j row i also holds
+    // Row i's pairs in order: for each lower block u, the upper entries v of
+    // row p = JA[slot[base+u]] whose column row i holds (its CRS-local slot by
+    // binary search, JA rows being sorted).  Counted, then written, per row.
     std::vector<int4> hdr(c->nnzb, make_int4(0, 0, 0, 0));
     std::vector<int64_t> pair_ptr(n + 1, 0);
-    std::vector<int2> pairs;
-    pairs.reserve((size_t)c->nnzb * 2);
-    std::vector<int> where(n, -1);  // local slot of column j in the current row
-    int maxstage = 1;
-    for (int i = 0; i < n; i++) {
-        const int base = IA[i];
-        for (int k = base; k < IA[i + 1]; k++) where[JA[k]] = k - base;
+    auto row_pairs = [&](int i, int2 *out) {  // returns the row's pair count; writes them when out != nullptr
+        const int base = IA[i], end = IA[i + 1];
         const int nlo = meta[i].y;
+        int total = 0;
         for (int u = 0; u < nlo; u++) {
             const int kk = slot[base + u], p = JA[kk];
             int cnt = 0;
             for (int v = IA[p] + meta[p].y + 1; v < IA[p + 1]; v++) {
                 const int j = scol[v];
-                if (where[j] >= 0) {
-                    pairs.push_back(make_int2(v, where[j]));
+                const int *it = std::lower_bound(&JA[base], &JA[0] + end, j);
+                if (it != &JA[0] + end && *it == j) {
+                    if (out) out[total + cnt] = make_int2(v, (int)(it - &JA[base]));
                     cnt++;
                 }
             }
-            hdr[base + u] = make_int4(IA[p] + meta[p].y, cnt, kk - base, 0);
+            if (out) hdr[base + u] = make_int4(IA[p] + meta[p].y, cnt, kk - base, 0);
+            total += cnt;
         }
-        pair_ptr[i + 1] = (int64_t)pairs.size();
-        maxstage = std::max<int64_t>(maxstage, nlo + (pair_ptr[i + 1] - pair_ptr[i]));
-        for (int k = base; k < IA[i + 1]; k++) where[JA[k]] = -1;
+        return total;
+    };
+    parallel_ranges(n, [&](int, int64_t i0, int64_t i1) {
+        for (int i = (int)i0; i < (int)i1; i++) pair_ptr[i + 1] = row_pairs(i, nullptr);
+    });
+    int maxstage = 1;
+    for (int i = 0; i < n; i++) {
+        maxstage = std::max<int64_t>(maxstage, meta[i].y + pair_ptr[i + 1]);
+        pair_ptr[i + 1] += pair_ptr[i];
     }
+    std::vector<int2> pairs(std::max<int64_t>(pair_ptr[n], 1));
+    parallel_ranges(n, [&](int, int64_t i0, int64_t i1) {
+        for (int i = (int)i0; i < (int)i1; i++) row_pairs(i, pairs.data() + pair_ptr[i]);
+    });
     // row records and packed-layout slots of the triangular solves, in launch
     // order (colour, then position of the patch in the colour, then row)
     std::vector<int4> rowf((size_t)np * kMcRows), rowb((size_t)np * kMcRows), rowl((size_t)np * kMcRows);
@@ -625,7 +647,8 @@ int mc_build(cfd_ctx *c) {
         uslot[pos + 1] = uslot[pos] + umax;
     }
     std::vector<int> colL((size_t)lslot[np] * kMcRows, 0), colU((size_t)uslot[np] * kMcRows, 0);
-    for (int pos = 0; pos < np; pos++) {
+    parallel_ranges(np, [&](int, int64_t q0, int64_t q1) {
+    for (int pos = (int)q0; pos < (int)q1; pos++) {
         const int p0 = patches[pos] * kMcRows;
         for (int q = 0; q < kMcRows; q++) {
             const int4 rf = rowf[(size_t)pos * kMcRows + q], rb = rowb[(size_t)pos * kMcRows + q];
@@ -640,6 +663,7 @@ int mc_build(cfd_ctx *c) {
             }
         }
     }
+    });
     mc.nlslot = lslot[np];
     mc.nuslot = uslot[np];
     CFD_CUDA(mc.rowf.upload(rowf.data(), rowf.size(), c->stream));
@@ -659,7 +683,7 @@ int mc_build(cfd_ctx *c) {
     CFD_CUDA(mc.plev.upload(plev.data(), plev.size(), c->stream));
     CFD_CUDA(mc.hdr.upload(hdr.data(), hdr.size(), c->stream));
     CFD_CUDA(mc.pair_ptr.upload(pair_ptr.data(), pair_ptr.size(), c->stream));
-    CFD_CUDA(mc.pairs.upload(pairs.data(), pairs.size(), c->stream));
+    CFD_CUDA(mc.pairs.upload(pairs.data(), (size_t)pair_ptr[n], c->stream));
     CFD_CUDA(stream_wait(c->stream));  // host vectors go out of scope
     mc.built = true;
     return CFD_OK;

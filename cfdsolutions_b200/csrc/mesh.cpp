@@ -21,6 +21,7 @@
 // elements would sum them (the same bits); the renumbering's bisection and
 // patch graph run on threads too.
 #include "cfd_internal.h"
+#include "host_par.h"
 
 #include <algorithm>
 #include <cmath>
@@ -74,29 +75,6 @@ const ElemType kPrism = {6, 9, 5, kPrismEdges,
                          {{0, 1, 2, -1}, {3, 4, 5, -1}, {0, 1, 4, 3}, {1, 2, 5, 4}, {2, 0, 3, 5}}};
 const ElemType kHex = {8, 12, 6, kHexEdges,
                        {{0, 1, 2, 3}, {4, 5, 6, 7}, {0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {3, 0, 4, 7}}};
-
-// Ranges [0, n) is split into for parallel_ranges: up to 16 (or the calling
-// thread's g_host_threads), one below 65,536 items.
-inline int range_count(int n) {
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const unsigned cap = g_host_threads > 0 ? (unsigned)g_host_threads : 16u;
-    return n < 65536 ? 1 : (int)std::min(cap, hw);
-}
-
-// fn(t, lo, hi) for the range_count(n) contiguous ranges t of [0, n), one
-// thread each.  Every range writes only its own items.
-template <typename F>
-void parallel_ranges(int n, F fn) {
-    const int nt = range_count(n);
-    if (nt == 1) {
-        fn(0, 0, n);
-        return;
-    }
-    std::vector<std::thread> th;
-    for (int t = 0; t < nt; t++)
-        th.emplace_back(fn, t, (int)((int64_t)n * t / nt), (int)((int64_t)n * (t + 1) / nt));
-    for (auto &x : th) x.join();
-}
 
 // The volume elements of a mesh as one sequence of keys: tetrahedra, then
 // pyramids, prisms and hexahedra, each in its own order (the order the
