@@ -1568,6 +1568,8 @@ int cfd_set_stream(cfd_ctx *c, void *stream) {
     return CFD_OK;
 }
 
+static int build_patch_layout(cfd_ctx *c);
+
 int cfd_set_params(cfd_ctx *c, const cfd_params *p) {
     if (!c || !p) { set_error("cfd_set_params: NULL"); return CFD_ERR_ARG; }
     c->phi_next_valid = false;
@@ -1605,6 +1607,11 @@ int cfd_set_params(cfd_ctx *c, const cfd_params *p) {
     }
     c->params = *p;
     compute_flow(c, 0);
+    if (c->has_mesh && p->residual_kernel == 1 && !c->patch_built) {
+        CFD_CUDA(cudaSetDevice(c->device));
+        const int st = build_patch_layout(c);
+        if (st) return st;
+    }
     return CFD_OK;
 }
 
@@ -1612,6 +1619,98 @@ int cfd_synchronize(cfd_ctx *c) {
     if (!c) return CFD_ERR_ARG;
     CFD_CUDA(cudaSetDevice(c->device));
     CFD_CUDA(stream_wait(c->stream));
+    return CFD_OK;
+}
+
+// Patch layout of the residual kernel variant (residual_kernel = 1), from the
+// installed mesh's node -> edge incidence and edge arrays (read back from the
+// device): node ranges of CFD_PATCH_NODES nodes; per patch its halo
+// (neighbours outside the range, sorted), every interior edge touching the
+// patch with patch-local endpoint indices (owned 0..np-1, halo np..), and per
+// owned node its incident edges as patch-local edge indices in increasing
+// order (the fixed summation order).  Only callers of that kernel pay for it.
+static int build_patch_layout(cfd_ctx *c) {
+    const int nnode = c->nnode, nedge = c->nedge;
+    cudaStream_t s = c->stream;
+    std::vector<int> ptr(nnode + 1), lst;
+    std::vector<int2> en(nedge);
+    std::vector<double4> eg(nedge);
+    CFD_CUDA(cudaMemcpyAsync(ptr.data(), c->n2e_ptr.p, sizeof(int) * (nnode + 1), cudaMemcpyDeviceToHost, s));
+    CFD_CUDA(stream_wait(s));
+    lst.resize(ptr[nnode]);
+    if (ptr[nnode]) CFD_CUDA(cudaMemcpyAsync(lst.data(), c->n2e.p, sizeof(int) * ptr[nnode], cudaMemcpyDeviceToHost, s));
+    if (nedge) {
+        CFD_CUDA(cudaMemcpyAsync(en.data(), c->edge_nodes.p, sizeof(int2) * nedge, cudaMemcpyDeviceToHost, s));
+        CFD_CUDA(cudaMemcpyAsync(eg.data(), c->edge_geo.p, sizeof(double4) * nedge, cudaMemcpyDeviceToHost, s));
+    }
+    CFD_CUDA(stream_wait(s));
+    {
+        const int P = CFD_PATCH_NODES;
+        const int np = (nnode + P - 1) / P;
+        std::vector<int> pptr(np + 1, 0), hptr(np + 1, 0), halo, stamp(nedge, -1), local(nedge, 0);
+        std::vector<int> iptr(nnode + 1, 0), ilist, pl;
+        std::vector<double4> pg;
+        std::vector<int> hstamp(nnode, -1), hloc(nnode, 0);
+        ilist.reserve(ptr[nnode]);
+        pl.reserve((size_t)nedge + nedge / 2);
+        pg.reserve((size_t)nedge + nedge / 2);
+        int nlocmax = 0;
+        for (int p = 0; p < np; p++) {
+            const int n0 = p * P, n1 = std::min(nnode, n0 + P), nown = n1 - n0;
+            // halo, sorted by global index
+            std::vector<int> h;
+            for (int i = n0; i < n1; i++)
+                for (int k = ptr[i]; k < ptr[i + 1]; k++) {
+                    const int sg = lst[k], e = sg >= 0 ? sg : ~sg;
+                    const int j = sg >= 0 ? en[e].y : en[e].x;
+                    if ((j < n0 || j >= n1) && hstamp[j] != p) { hstamp[j] = p; h.push_back(j); }
+                }
+            std::sort(h.begin(), h.end());
+            for (size_t q = 0; q < h.size(); q++) hloc[h[q]] = nown + (int)q;
+            halo.insert(halo.end(), h.begin(), h.end());
+            hptr[p + 1] = (int)halo.size();
+            nlocmax = std::max(nlocmax, nown + (int)h.size());
+            auto lid = [&](int g) { return (g >= n0 && g < n1) ? g - n0 : hloc[g]; };
+            int cnt = 0;
+            for (int i = n0; i < n1; i++)
+                for (int k = ptr[i]; k < ptr[i + 1]; k++) {
+                    const int sg = lst[k], e = sg >= 0 ? sg : ~sg;
+                    if (stamp[e] != p) {
+                        stamp[e] = p;
+                        local[e] = cnt++;
+                        pl.push_back(lid(en[e].x) | (lid(en[e].y) << 16));
+                        pg.push_back(eg[e]);
+                    }
+                }
+            for (int i = n0; i < n1; i++) {
+                const size_t b = ilist.size();
+                for (int k = ptr[i]; k < ptr[i + 1]; k++) {
+                    const int sg = lst[k], e = sg >= 0 ? sg : ~sg;
+                    ilist.push_back((local[e] << 1) | (sg < 0 ? 1 : 0));
+                }
+                std::sort(ilist.begin() + b, ilist.end());
+                iptr[i + 1] = (int)ilist.size();
+            }
+            pptr[p + 1] = pptr[p] + cnt;
+        }
+        if (ilist.empty()) ilist.push_back(0);  // keep the device arrays non-empty
+        if (halo.empty()) halo.push_back(0);
+        if (pl.empty()) { pl.push_back(0); pg.push_back(make_double4(0, 0, 0, 0)); }
+        c->npatch = np;
+        c->patch_nlocmax = nlocmax;
+        c->use_patch = nlocmax < 65536 && patch_smem_bytes(nlocmax, true) <= kPatchSmemMax;
+        if (c->use_patch) {
+            CFD_CUDA(c->pe_ptr.upload(pptr.data(), pptr.size(), s));
+            CFD_CUDA(c->pe_loc.upload(pl.data(), pl.size(), s));
+            CFD_CUDA(c->pe_geo.upload(pg.data(), pg.size(), s));
+            CFD_CUDA(c->ph_ptr.upload(hptr.data(), hptr.size(), s));
+            CFD_CUDA(c->halo.upload(halo.data(), halo.size(), s));
+            CFD_CUDA(c->inc_ptr.upload(iptr.data(), iptr.size(), s));
+            CFD_CUDA(c->inc.upload(ilist.data(), ilist.size(), s));
+            CFD_CUDA(stream_wait(s));
+        }
+    }
+    c->patch_built = true;
     return CFD_OK;
 }
 
@@ -1783,76 +1882,12 @@ int cfd_set_mesh(cfd_ctx *c, int nnode, int nghost, int nedge, const int *edge_n
         CFD_CUDA(c->deg.upload(dg.data(), dg.size(), s));
         CFD_CUDA(stream_wait(s));
     }
-    // ---- patch layout of the residual kernel: node ranges of CFD_PATCH_NODES
-    // nodes; per patch its halo (neighbours outside the range, sorted), every
-    // interior edge touching the patch with patch-local endpoint indices
-    // (owned 0..np-1, halo np..), and per owned node its incident edges as
-    // patch-local edge indices in increasing order (the fixed summation order).
-    {
-        const int P = CFD_PATCH_NODES;
-        const int np = (nnode + P - 1) / P;
-        std::vector<int> pptr(np + 1, 0), hptr(np + 1, 0), halo, stamp(nedge, -1), local(nedge, 0);
-        std::vector<int> iptr(nnode + 1, 0), ilist, pl;
-        std::vector<double4> pg;
-        std::vector<int> hstamp(nnode, -1), hloc(nnode, 0);
-        ilist.reserve(ptr[nnode]);
-        pl.reserve((size_t)nedge + nedge / 2);
-        pg.reserve((size_t)nedge + nedge / 2);
-        int nlocmax = 0;
-        for (int p = 0; p < np; p++) {
-            const int n0 = p * P, n1 = std::min(nnode, n0 + P), nown = n1 - n0;
-            // halo, sorted by global index
-            std::vector<int> h;
-            for (int i = n0; i < n1; i++)
-                for (int k = ptr[i]; k < ptr[i + 1]; k++) {
-                    const int sg = lst[k], e = sg >= 0 ? sg : ~sg;
-                    const int j = sg >= 0 ? en[e].y : en[e].x;
-                    if ((j < n0 || j >= n1) && hstamp[j] != p) { hstamp[j] = p; h.push_back(j); }
-                }
-            std::sort(h.begin(), h.end());
-            for (size_t q = 0; q < h.size(); q++) hloc[h[q]] = nown + (int)q;
-            halo.insert(halo.end(), h.begin(), h.end());
-            hptr[p + 1] = (int)halo.size();
-            nlocmax = std::max(nlocmax, nown + (int)h.size());
-            auto lid = [&](int g) { return (g >= n0 && g < n1) ? g - n0 : hloc[g]; };
-            int cnt = 0;
-            for (int i = n0; i < n1; i++)
-                for (int k = ptr[i]; k < ptr[i + 1]; k++) {
-                    const int sg = lst[k], e = sg >= 0 ? sg : ~sg;
-                    if (stamp[e] != p) {
-                        stamp[e] = p;
-                        local[e] = cnt++;
-                        pl.push_back(lid(en[e].x) | (lid(en[e].y) << 16));
-                        pg.push_back(eg[e]);
-                    }
-                }
-            for (int i = n0; i < n1; i++) {
-                const size_t b = ilist.size();
-                for (int k = ptr[i]; k < ptr[i + 1]; k++) {
-                    const int sg = lst[k], e = sg >= 0 ? sg : ~sg;
-                    ilist.push_back((local[e] << 1) | (sg < 0 ? 1 : 0));
-                }
-                std::sort(ilist.begin() + b, ilist.end());
-                iptr[i + 1] = (int)ilist.size();
-            }
-            pptr[p + 1] = pptr[p] + cnt;
-        }
-        if (ilist.empty()) ilist.push_back(0);  // keep the device arrays non-empty
-        if (halo.empty()) halo.push_back(0);
-        if (pl.empty()) { pl.push_back(0); pg.push_back(make_double4(0, 0, 0, 0)); }
-        c->npatch = np;
-        c->patch_nlocmax = nlocmax;
-        c->use_patch = nlocmax < 65536 && patch_smem_bytes(nlocmax, true) <= kPatchSmemMax;
-        if (c->use_patch) {
-            CFD_CUDA(c->pe_ptr.upload(pptr.data(), pptr.size(), s));
-            CFD_CUDA(c->pe_loc.upload(pl.data(), pl.size(), s));
-            CFD_CUDA(c->pe_geo.upload(pg.data(), pg.size(), s));
-            CFD_CUDA(c->ph_ptr.upload(hptr.data(), hptr.size(), s));
-            CFD_CUDA(c->halo.upload(halo.data(), halo.size(), s));
-            CFD_CUDA(c->inc_ptr.upload(iptr.data(), iptr.size(), s));
-            CFD_CUDA(c->inc.upload(ilist.data(), ilist.size(), s));
-            CFD_CUDA(stream_wait(s));
-        }
+    // ---- patch layout of the residual kernel (variant): built when that kernel is requested
+    c->patch_built = false;
+    c->use_patch = false;
+    if (c->params.residual_kernel == 1) {
+        const int st = build_patch_layout(c);
+        if (st) return st;
     }
     CFD_CUDA(c->roeflag.alloc(nnode));
     CFD_CUDA(c->fixcount.alloc(2));

@@ -280,6 +280,7 @@ struct cfd_ctx {
     cfd::DevBuf<int> inc_ptr, inc;    // per node: (patch-local edge << 1) | (node is R), increasing
     int npatch = 0, patch_nlocmax = 0;
     bool use_patch = false;
+    bool patch_built = false;  // the layout exists (built when residual_kernel = 1 is first asked for)
     // limiter fixes decided by the residual (see cfd_limiter): per node bit 0 =
     // Roe-average pressure fix, bit 1 = reconstructed-pressure correction;
     // fixcount = [nodes failing the Roe check, nodes failing the pressure check]

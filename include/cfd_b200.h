@@ -131,7 +131,8 @@ typedef struct cfd_params {
     double cfl_min;          /* CFL_MIN                      */
     double cfl_max;          /* CFL_MAX                      */
     double venkat_k;         /* VENKAT_K_THRESHOLD           */
-    int    residual_kernel;  /* 0: node-gather kernel (sliced-ELL), 1: shared-memory patch kernel */
+    int    residual_kernel;  /* 0: node-gather kernel (sliced-ELL), 1: shared-memory patch kernel
+                                (its layout is built when 1 is first set on a context with a mesh) */
     /* Stiffened-gas constant p_inf / p_ref (0: the reference's ideal gas).
      * p = (gamma - 1) rho e - gamma pinf, c^2 = gamma (p + pinf) / rho; the
      * freestream keeps rho = 1, p = 1 and c = sqrt(gamma (1 + pinf)).  No
