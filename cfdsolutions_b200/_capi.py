@@ -49,7 +49,7 @@ class Params(C.Structure):
         ("gamma", C.c_double), ("mach", C.c_double), ("mach_min", C.c_double), ("alpha_deg", C.c_double),
         ("beta_deg", C.c_double), ("cfl_min", C.c_double), ("cfl_max", C.c_double), ("venkat_k", C.c_double),
         ("residual_kernel", C.c_int), ("pinf", C.c_double), ("precond_method", C.c_int), ("precond_type", C.c_int),
-        ("precond_mach", C.c_double), ("outflow_pressure", C.c_double),
+        ("precond_mach", C.c_double), ("outflow_pressure", C.c_double), ("variables", C.c_int),
     ]
 
 

@@ -205,7 +205,7 @@ __device__ __forceinline__ void residual_gather_node(int i, GATHER_PARAMS, doubl
                 qL[v] = own_is_L ? fo[v] : fn[v];
                 qR[v] = own_is_L ? fn[v] : fo[v];
             }
-            if (SECOND && !roe_c2_of<FLUX>() && (checks & 1) && roe_avg_pressure(qL, qR, f.gamma, f.gpinf) < 0.0)
+            if (SECOND && !roe_c2_of<FLUX>() && (checks & 1) && roe_avg_pressure(qL, qR, f) < 0.0)
                 bad |= 1;
             double cf[5], df[5], lam[3], c2 = 1.0;
             const double lmax = edge_flux<FLUX>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam,
@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(PATCH_CHUNK, 2) k_residual_patch(
                 }
 #pragma unroll
                 for (int v = 0; v < 5; v++) { qL[v] = rL[v]; qR[v] = rR[v]; }
-                if (check_roe && roe_avg_pressure(qL, qR, f.gamma, f.gpinf) < 0.0) {
+                if (check_roe && roe_avg_pressure(qL, qR, f) < 0.0) {
                     roeflag[a < nown ? n0 + a : halo[h0 + a - nown]] = 1;
                     roeflag[b < nown ? n0 + b : halo[h0 + b - nown]] = 1;
                     atomicAdd(&fixcount[0], 1);
@@ -661,7 +661,7 @@ __global__ void __launch_bounds__(128) k_jac_edges(int nedge, int64_t ldq, const
     const double ha = 0.5 * g.w;
     const unsigned act = __ballot_sync(0xffffffffu, live);
     for (int half = 0; half < 2; half++) {
-        euler_flux_jacobian(half == 0 ? qR : qL, g.x, g.y, g.z, f.gamma, f.gpinf, J);
+        flux_jacobian(half == 0 ? qR : qL, g.x, g.y, g.z, f, J);
 #pragma unroll
         for (int k = 0; k < 25; k++) stage[w][lane][k] = half == 0 ? ha * (J[k] - Ab[k]) : -ha * (J[k] + Ab[k]);
         __syncwarp();
@@ -706,6 +706,17 @@ __global__ void __launch_bounds__(32 * JAC_WARPS) k_jac_rows_warp(
         for (int k = 1; k < 25; k++)
             if (k == m) cm = C[k];
         d = cm * vd;
+    } else if (f.rup && add_time) {
+        // (V/dt) dQ/d(rho,u,v,w,p) (Roe_Jacobian.cpp:241-264 with PRECOND_METHOD_NONE)
+        double qi[5], M[25];
+#pragma unroll
+        for (int v = 0; v < 5; v++) qi[v] = Q[v * ldq + i];
+        state_time_matrix(qi, f, M);
+        double cm = M[0];
+#pragma unroll
+        for (int k = 1; k < 25; k++)
+            if (k == m) cm = M[k];
+        d = cm * vd;
     } else {
         d = (m % 6 == 0) ? vd : 0.0;
     }
@@ -747,6 +758,13 @@ __global__ void __launch_bounds__(128) k_jac_rows(
         pc_node_cinv(qi, f, D);
 #pragma unroll
         for (int k = 0; k < 25; k++) D[k] *= vd;
+    } else if (f.rup && add_time) {
+        double qi[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) qi[v] = Q[v * ldq + i];
+        state_time_matrix(qi, f, D);
+#pragma unroll
+        for (int k = 0; k < 25; k++) D[k] *= vd;
     } else {
 #pragma unroll
         for (int k = 0; k < 25; k++) D[k] = (k % 6 == 0) ? vd : 0.0;
@@ -783,7 +801,7 @@ __global__ void __launch_bounds__(128) k_jac_rows(
         } else {
             roe_abs_jacobian(qL, qR, g.x, g.y, g.z, f, Ab);
         }
-        euler_flux_jacobian(qL, g.x, g.y, g.z, f.gamma, f.gpinf, J);
+        flux_jacobian(qL, g.x, g.y, g.z, f, J);
         const double ha = 0.5 * g.w;
 #pragma unroll
         for (int m = 0; m < 25; m++) D[m] += ha * (J[m] + Ab[m]);
@@ -951,11 +969,12 @@ __global__ void k_update(int nnode, int64_t ldq, double relax, const double *__r
 __global__ void k_freestream(int n, int64_t ldq, Flow f, double *__restrict__ Q) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const bool r = f.rup != 0;
     Q[i] = f.inf_rho;
-    Q[ldq + i] = f.inf_rho * f.inf_u;
-    Q[2 * ldq + i] = f.inf_rho * f.inf_v;
-    Q[3 * ldq + i] = f.inf_rho * f.inf_w;
-    Q[4 * ldq + i] = f.inf_rho * f.inf_et;
+    Q[ldq + i] = r ? f.inf_u : f.inf_rho * f.inf_u;
+    Q[2 * ldq + i] = r ? f.inf_v : f.inf_rho * f.inf_v;
+    Q[3 * ldq + i] = r ? f.inf_w : f.inf_rho * f.inf_w;
+    Q[4 * ldq + i] = r ? f.inf_p : f.inf_rho * f.inf_et;
 }
 
 // ------------------------------------------------------------- host helpers
@@ -1024,6 +1043,7 @@ static void compute_flow(cfd_ctx *c, int iteration) {
     f.pc_type = p.precond_type;
     f.pc_mach = p.precond_mach;
     f.pc_outflow_p = p.outflow_pressure != 0.0 ? p.outflow_pressure : pr;
+    f.rup = p.variables == CFD_VARS_RUP ? 1 : 0;
     f.order = p.order;
     f.limiter = p.limiter;
     f.limiter_smooth = p.limiter_smooth;
@@ -1595,6 +1615,10 @@ int cfd_set_params(cfd_ctx *c, const cfd_params *p) {
     }
     if (!(p->pinf >= 0.0 && p->pinf < 1.0e300)) {
         set_error("cfd_set_params: pinf must be finite and >= 0");
+        return CFD_ERR_ARG;
+    }
+    if (p->variables != CFD_VARS_CONSERVATIVE && p->variables != CFD_VARS_RUP) {
+        set_error("cfd_set_params: variables must be CFD_VARS_CONSERVATIVE or CFD_VARS_RUP");
         return CFD_ERR_ARG;
     }
     if (p->residual_kernel < 0 || p->residual_kernel > 1) {

@@ -394,6 +394,11 @@ extern "C" int cfd_jacobian_fd(cfd_ctx *c, int add_time, int include_diss, int m
         set_error("cfd_jacobian_fd: method must be CFD_JAC_CENTRAL, _FORWARD, _BACKWARD or _ALTERNATE");
         return CFD_ERR_ARG;
     }
+    if (c->params.variables != CFD_VARS_CONSERVATIVE) {
+        // Euler3D's difference quotients perturb conservative states (Roe_Jacobian.cpp:236-775)
+        set_error("cfd_jacobian_fd: conservative variables only");
+        return CFD_ERR_UNSUPPORTED;
+    }
     if (c->params.flux_scheme != CFD_FLUX_ROE && c->params.flux_scheme != CFD_FLUX_ROE_LMFIX) {
         // Compute_Jacobian_FiniteDifference_Roe differences the Roe flux (Roe_Jacobian.cpp:236)
         set_error("cfd_jacobian_fd: the finite-difference Jacobian is defined for the Roe flux (with or "

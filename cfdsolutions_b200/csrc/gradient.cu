@@ -463,6 +463,10 @@ __global__ void __launch_bounds__(128) k_roe_pressure_fix(int nnode, int64_t ldq
                                                                      g[(3 * v + 1) * (int64_t)nnode + j] * ry +
                                                                      g[(3 * v + 2) * (int64_t)nnode + j] * rz));
             }
+            if (f.rup) {
+                if (roe_avg_pressure_rup(qa, qb, f) < 0.0) neg = true;
+                continue;
+            }
             // Compute_RoeVariables (Roe_Fluxes.cpp:3609-3633)
             const double ra = qa[0], rb = qb[0];
             const double ua = qa[1] / ra, va = qa[2] / ra, wa = qa[3] / ra;

@@ -235,7 +235,23 @@ __host__ __device__ constexpr bool is_roe_flux(int flux) {
 // Compute_Limiter_RoePressureCorrection, Limiters.cpp:311-356).
 // For the stiffened gas the value returned is p + pinf of the Roe state (its
 // c^2 = (g - 1) h holds for either gas), the quantity whose sign matters.
-__device__ __forceinline__ double roe_avg_pressure(const double qa[5], const double qb[5], double g, double gpinf) {
+// Roe-averaged p + pinf of two reconstructed (rho, u, v, w, p) face states:
+// Compute_RoeAverage_Q and Material_Get_Pressure with VARIABLE_RUP
+// (MPFLOW3D/src/Limiters.cpp:350-352), p + pinf = (gamma - 1) rho (ht - q^2/2) / gamma.
+__device__ __forceinline__ double roe_avg_pressure_rup(const double qa[5], const double qb[5], const Flow &f) {
+    const double ra = qa[0], rb = qb[0];
+    const double k = f.gamma * f.inv_gm1;
+    const double ha = k * (qa[4] + f.pinf) / ra + 0.5 * (qa[1] * qa[1] + qa[2] * qa[2] + qa[3] * qa[3]);
+    const double hb = k * (qb[4] + f.pinf) / rb + 0.5 * (qb[1] * qb[1] + qb[2] * qb[2] + qb[3] * qb[3]);
+    const double rho = sqrt(ra * rb), sg = rho / (ra + rho);
+    const double u = qa[1] + sg * (qb[1] - qa[1]), v = qa[2] + sg * (qb[2] - qa[2]), w = qa[3] + sg * (qb[3] - qa[3]);
+    const double ht = ha + sg * (hb - ha);
+    return f.gm1 * rho * (ht - 0.5 * (u * u + v * v + w * w)) / f.gamma;
+}
+
+__device__ __forceinline__ double roe_avg_pressure(const double qa[5], const double qb[5], const Flow &f) {
+    if (f.rup) return roe_avg_pressure_rup(qa, qb, f);
+    const double g = f.gamma, gpinf = f.gpinf;
     const double ra = qa[0], rb = qb[0];
     const double ia = 1.0 / ra, ib = 1.0 / rb;
     const double ua = qa[1] * ia, va = qa[2] * ia, wa = qa[3] * ia;
@@ -255,6 +271,7 @@ __device__ __forceinline__ double roe_avg_pressure(const double qa[5], const dou
 // (Euler3D/src/Limiters.cpp:296-301): p < 0, without the division when rho > 0
 // (p + pinf < 0 for the stiffened gas).
 __device__ __forceinline__ bool recon_pressure_negative(const double q[5], const Flow &f) {
+    if (f.rup) return q[4] + f.pinf < 0.0;  // Material_Get_Pressure of a RUP state (Limiters.cpp:296-297)
     const double m2 = q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
     return q[0] > 0.0 ? (2.0 * q[0] * (q[4] - f.pinf) < m2) : (f.gm1 * ((q[4] - f.pinf) - (0.5 / q[0]) * m2) < 0.0);
 }

@@ -1041,6 +1041,11 @@ int cfd_solve_unsteady(cfd_ctx *c, const cfd_unsteady_opts *o, cfd_unsteady_stat
         set_error("cfd_solve_unsteady: dt > 0, steps >= 0 and inner_iterations >= 1");
         return CFD_ERR_ARG;
     }
+    if (c->params.variables != CFD_VARS_CONSERVATIVE) {
+        // the physical-time terms difference conservative states (Solver_Unsteady_Implicit.cpp)
+        set_error("cfd_solve_unsteady: conservative variables only");
+        return CFD_ERR_UNSUPPORTED;
+    }
     const int n = c->nnode;
     DevBuf<double> qn, qn1;
     CFD_CUDA(qn.alloc((size_t)5 * n));

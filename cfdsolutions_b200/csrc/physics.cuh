@@ -2,8 +2,11 @@
 // the generic non-dimensionalisation (or the stiffened gas
 // p = (gamma - 1) rho e - gamma pinf, which is the ideal gas at pinf = 0), Roe / HLLC / AUSM+ edge fluxes,
 // characteristic ghost states and the approximate Roe flux Jacobian.
-// Conservative variables (rho, rho u, rho v, rho w, rho et) throughout, as
-// Euler3D with VARIABLE_TYPE=VARIABLE_CONSERVATIVE.
+// The state holds either the conservative variables (rho, rho u, rho v, rho w,
+// rho et), as Euler3D with VARIABLE_TYPE=VARIABLE_CONSERVATIVE, or (rho, u, v,
+// w, p), as MPFLOW3D with VARIABLE_RUP (Flow::rup): the face properties, ghost
+// states and Jacobian columns follow the state's variables, the fluxes are
+// the conservation-law fluxes either way.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -32,6 +35,7 @@ struct Flow {
     // reference Mach and the pressure its subsonic outflow imposes
     int pc_method, pc_type;
     double pc_mach, pc_outflow_p;
+    int rup;              // state in (rho, u, v, w, p) (CFD_VARS_RUP), else conservative
 };
 
 struct Face {
@@ -42,18 +46,57 @@ struct Face {
 // with the stiffened-gas terms: p = (gamma - 1)(rho et - rho q^2 / 2) - gamma pinf and
 // c^2 = gamma (p + pinf) / rho.  At pinf = 0 both added terms are exact zeros, so
 // the ideal-gas results are bit-identical.  c is only formed when `want_c`.
+// RUP states (MPFLOW3D Material_Get_Properties, VARIABLE_RUP branch,
+// MPFLOW3D/src/Material.cpp:591-599) take rho, u, v, w, p as stored and
+// ht = gamma (p + pinf) / ((gamma - 1) rho) + q^2 / 2.
 __device__ __forceinline__ void eos_face(const double q[5], double nx, double ny, double nz, const Flow &f,
                                          bool want_c, Face &s) {
     s.rho = q[0];
     const double ri = 1.0 / s.rho;
-    s.u = q[1] * ri;
-    s.v = q[2] * ri;
-    s.w = q[3] * ri;
-    const double q2 = s.u * s.u + s.v * s.v + s.w * s.w;
-    s.p = f.gm1 * (q[4] - 0.5 * s.rho * q2) - f.gpinf;
-    s.ht = (q[4] + s.p) * ri;
+    if (f.rup) {
+        s.u = q[1];
+        s.v = q[2];
+        s.w = q[3];
+        s.p = q[4];
+        s.ht = f.gamma * f.inv_gm1 * (s.p + f.pinf) * ri + 0.5 * (s.u * s.u + s.v * s.v + s.w * s.w);
+    } else {
+        s.u = q[1] * ri;
+        s.v = q[2] * ri;
+        s.w = q[3] * ri;
+        const double q2 = s.u * s.u + s.v * s.v + s.w * s.w;
+        s.p = f.gm1 * (q[4] - 0.5 * s.rho * q2) - f.gpinf;
+        s.ht = (q[4] + s.p) * ri;
+    }
     s.ubar = s.u * nx + s.v * ny + s.w * nz;
     s.c = want_c ? sqrt(f.gamma * (s.p + f.pinf) * ri) : 0.0;
+}
+
+// A state from (rho, u, v, w, p) in the state's variables; the conservative
+// total energy by Get_TotalEnergy (Material.cpp:1012-1040),
+// rho e = (p + gamma pinf) / (gamma - 1).
+__device__ __forceinline__ void store_state(double rho, double u, double v, double w, double p, const Flow &f,
+                                            double q[5]) {
+    if (f.rup) {
+        q[0] = rho; q[1] = u; q[2] = v; q[3] = w; q[4] = p;
+        return;
+    }
+    const double et = (p + f.gpinf) / (f.gm1 * rho) + 0.5 * (u * u + v * v + w * w);
+    q[0] = rho;
+    q[1] = rho * u;
+    q[2] = rho * v;
+    q[3] = rho * w;
+    q[4] = rho * et;
+}
+
+// dQ_cons/d(rho,u,v,w,p) at (rho, u, v, w) (Compute_Transformation_Conservative_To_RUP,
+// MPFLOW3D/src/Material.cpp:1172-1236), row-major; the same for either gas.
+__device__ __forceinline__ void dcons_drup(double rho, double u, double v, double w, const Flow &f, double M[25]) {
+    M[0] = 1.0;  M[1] = 0.0;     M[2] = 0.0;     M[3] = 0.0;     M[4] = 0.0;
+    M[5] = u;    M[6] = rho;     M[7] = 0.0;     M[8] = 0.0;     M[9] = 0.0;
+    M[10] = v;   M[11] = 0.0;    M[12] = rho;    M[13] = 0.0;    M[14] = 0.0;
+    M[15] = w;   M[16] = 0.0;    M[17] = 0.0;    M[18] = rho;    M[19] = 0.0;
+    M[20] = 0.5 * (u * u + v * v + w * w);
+    M[21] = rho * u; M[22] = rho * v; M[23] = rho * w; M[24] = f.inv_gm1;
 }
 
 // Kermani entropy fix on the acoustic eigenvalues (Euler3D/src/Roe_EntropyFix.cpp:19-59).
@@ -250,13 +293,7 @@ __device__ __forceinline__ int characteristic_bc(const double qI[5], const doubl
         default: break;
     }
     if (p_b + f.pinf < 0.0) status = status ? status : 1;
-    // Get_TotalEnergy (Material.cpp:1012-1040), rho e = (p + gamma pinf) / (gamma - 1)
-    const double et = (p_b + f.gpinf) / (f.gm1 * rho_b) + 0.5 * (u_b * u_b + v_b * v_b + w_b * w_b);
-    qB[0] = rho_b;
-    qB[1] = rho_b * u_b;
-    qB[2] = rho_b * v_b;
-    qB[3] = rho_b * w_b;
-    qB[4] = rho_b * et;
+    store_state(rho_b, u_b, v_b, w_b, p_b, f, qB);
     return status;
 }
 
@@ -277,6 +314,40 @@ __device__ __forceinline__ void euler_flux_jacobian(const double q[5], double nx
     J[10] = g1 * ek * ny - v * ub; J[11] = v * nx - g1 * u * ny; J[12] = ub - g2 * v * ny;     J[13] = v * nz - g1 * w * ny; J[14] = g1 * ny;
     J[15] = g1 * ek * nz - w * ub; J[16] = w * nx - g1 * u * nz; J[17] = w * ny - g1 * v * nz; J[18] = ub - g2 * w * nz;     J[19] = g1 * nz;
     J[20] = (g1 * ek - ht) * ub;   J[21] = ht * nx - g1 * u * ub; J[22] = ht * ny - g1 * v * ub; J[23] = ht * nz - g1 * w * ub; J[24] = g * ub;
+}
+
+// dF.n/dW for W = (rho, u, v, w, p) (Compute_Flux_Jacobian_Euler_Convective,
+// VARIABLE_RUP, MPFLOW3D/src/CompressibleUtils.cpp:85-186), with
+// rho ht = gamma (p + pinf) / (gamma - 1) + rho q^2 / 2.
+__device__ __forceinline__ void rup_flux_jacobian(const double q[5], double nx, double ny, double nz, const Flow &f,
+                                                  double J[25]) {
+    const double rho = q[0], u = q[1], v = q[2], w = q[3];
+    const double ub = u * nx + v * ny + w * nz, q2 = u * u + v * v + w * w;
+    const double ht = f.gamma * f.inv_gm1 * (q[4] + f.pinf) / rho + 0.5 * q2;
+    J[0] = ub;             J[1] = rho * nx;               J[2] = rho * ny;               J[3] = rho * nz;               J[4] = 0.0;
+    J[5] = u * ub;         J[6] = rho * (ub + u * nx);    J[7] = rho * u * ny;           J[8] = rho * u * nz;           J[9] = nx;
+    J[10] = v * ub;        J[11] = rho * v * nx;          J[12] = rho * (ub + v * ny);   J[13] = rho * v * nz;          J[14] = ny;
+    J[15] = w * ub;        J[16] = rho * w * nx;          J[17] = rho * w * ny;          J[18] = rho * (ub + w * nz);   J[19] = nz;
+    J[20] = 0.5 * q2 * ub; J[21] = rho * (u * ub + ht * nx); J[22] = rho * (v * ub + ht * ny); J[23] = rho * (w * ub + ht * nz);
+    J[24] = f.gamma * f.inv_gm1 * ub;
+}
+
+// Convective flux Jacobian with respect to the state's variables.
+__device__ __forceinline__ void flux_jacobian(const double q[5], double nx, double ny, double nz, const Flow &f,
+                                              double J[25]) {
+    if (f.rup) rup_flux_jacobian(q, nx, ny, nz, f, J);
+    else euler_flux_jacobian(q, nx, ny, nz, f.gamma, f.gpinf, J);
+}
+
+// Pseudo-time matrix dQ_cons/dW of a node (V/dt times it is added to the
+// diagonal block; the identity for conservative states).
+__device__ __forceinline__ void state_time_matrix(const double q[5], const Flow &f, double M[25]) {
+    if (f.rup) {
+        dcons_drup(q[0], q[1], q[2], q[3], f, M);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 25; k++) M[k] = (k % 6 == 0) ? 1.0 : 0.0;
+    }
 }
 
 // Roe dissipation matrix |A| = M P |Lambda| P^-1 M^-1 (Compute_RoeAJacobian,
@@ -316,20 +387,26 @@ __device__ __forceinline__ void roe_abs_jacobian(const double qL[5], const doubl
     D[20] = 0.0;
     for (int j = 0; j < 3; j++) D[21 + j] = 0.5 * rho * c * Ed * n[j];
     D[24] = 0.5 * (E1 + E2);
-    // M^-1 = dq_RUP/dQ_cons (Compute_Transformation_RUP_To_Conservative, Material.cpp:1240-1300)
+    // M^-1 = dq_RUP/dQ_cons (Compute_Transformation_RUP_To_Conservative, Material.cpp:1240-1300);
+    // with RUP states the columns stay in (rho,u,v,w,p): Mop |A| with Mpr = I
+    // (Compute_Dissipation_Matrix_Roe_Optimized, MPFLOW3D/src/Roe_Fluxes.cpp:3185-3199)
     const double ri = 1.0 / rho, phi = 0.5 * f.gm1 * q2;
-    double Mi[25] = {1.0, 0.0, 0.0, 0.0, 0.0,
-                     -u * ri, ri, 0.0, 0.0, 0.0,
-                     -v * ri, 0.0, ri, 0.0, 0.0,
-                     -w * ri, 0.0, 0.0, ri, 0.0,
-                     phi, -u * f.gm1, -v * f.gm1, -w * f.gm1, f.gm1};
     double DM[25];
-    for (int i = 0; i < 5; i++)
-        for (int j = 0; j < 5; j++) {
-            double s = 0.0;
-            for (int k = 0; k < 5; k++) s += D[5 * i + k] * Mi[5 * k + j];
-            DM[5 * i + j] = s;
-        }
+    if (f.rup) {
+        for (int k = 0; k < 25; k++) DM[k] = D[k];
+    } else {
+        double Mi[25] = {1.0, 0.0, 0.0, 0.0, 0.0,
+                         -u * ri, ri, 0.0, 0.0, 0.0,
+                         -v * ri, 0.0, ri, 0.0, 0.0,
+                         -w * ri, 0.0, 0.0, ri, 0.0,
+                         phi, -u * f.gm1, -v * f.gm1, -w * f.gm1, f.gm1};
+        for (int i = 0; i < 5; i++)
+            for (int j = 0; j < 5; j++) {
+                double s = 0.0;
+                for (int k = 0; k < 5; k++) s += D[5 * i + k] * Mi[5 * k + j];
+                DM[5 * i + j] = s;
+            }
+    }
     // M = dQ_cons/dq_RUP
     for (int j = 0; j < 5; j++) {
         const double d0 = DM[j], d1 = DM[5 + j], d2 = DM[10 + j], d3 = DM[15 + j], d4 = DM[20 + j];
@@ -345,7 +422,9 @@ __device__ __forceinline__ void roe_abs_jacobian(const double qL[5], const doubl
 // MPFLOW3D/src/Roe_Fluxes.cpp:1141-1165): with z = min(1, max(M_L, M_R)) the
 // face velocities become u_L' = ((1+z) u_L + (1-z) u_R)/2 and symmetrically
 // u_R'; density and total energy stay, so the pressure follows the changed
-// kinetic energy.  The Roe flux is then formed from the modified states.
+// kinetic energy.  With RUP states the velocities are blended at fixed
+// density and pressure (Roe_Fluxes.cpp:1161-1168).  The Roe flux is then
+// formed from the modified states.
 __device__ __forceinline__ void thornber_states(const double qL[5], const double qR[5], const Flow &f,
                                                 double mL[5], double mR[5]) {
     Face L, R;
@@ -356,14 +435,22 @@ __device__ __forceinline__ void thornber_states(const double qL[5], const double
     const double z = fmin(1.0, fmax(ml, mr));
     mL[0] = qL[0];
     mR[0] = qR[0];
+    mL[4] = qL[4];
+    mR[4] = qR[4];
+    if (f.rup) {
+#pragma unroll
+        for (int i = 1; i < 4; i++) {
+            mL[i] = 0.5 * ((1.0 + z) * qL[i] + (1.0 - z) * qR[i]);
+            mR[i] = 0.5 * ((1.0 + z) * qR[i] + (1.0 - z) * qL[i]);
+        }
+        return;
+    }
 #pragma unroll
     for (int i = 1; i < 4; i++) {
         const double ul = qL[i] / qL[0], ur = qR[i] / qR[0];
         mL[i] = qL[0] * (0.5 * ((1.0 + z) * ul + (1.0 - z) * ur));
         mR[i] = qR[0] * (0.5 * ((1.0 + z) * ur + (1.0 - z) * ul));
     }
-    mL[4] = qL[4];
-    mR[4] = qR[4];
 }
 
 // ---------------------------------------------------------------------------
@@ -456,17 +543,23 @@ __device__ __forceinline__ void pc_left_row(int k, const PcSys &S, double nx, do
 }
 
 // out = Mop Kinv R |Lambda| L Mpr dQ at the system's averaged state, with
-// Mpr = d(rho,u,v,w,p)/dQ and Mop its inverse (the same for either gas).
+// Mpr = d(rho,u,v,w,p)/dQ and Mop its inverse (the same for either gas);
+// Mpr = I when dQ is already a (rho,u,v,w,p) difference (RUP states).
 __device__ __forceinline__ void pc_dissipation(const PcSys &S, double nx, double ny, double nz, const Flow &f,
                                                const double dQ[5], double out[5]) {
     const double rho = S.rho, u = S.u, v = S.v, w = S.w, ri = 1.0 / rho;
     const double q2 = u * u + v * v + w * w;
     double dq[5];
-    dq[0] = dQ[0];
-    dq[1] = (dQ[1] - u * dQ[0]) * ri;
-    dq[2] = (dQ[2] - v * dQ[0]) * ri;
-    dq[3] = (dQ[3] - w * dQ[0]) * ri;
-    dq[4] = f.gm1 * (0.5 * q2 * dQ[0] - u * dQ[1] - v * dQ[2] - w * dQ[3] + dQ[4]);
+    if (f.rup) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) dq[k] = dQ[k];
+    } else {
+        dq[0] = dQ[0];
+        dq[1] = (dQ[1] - u * dQ[0]) * ri;
+        dq[2] = (dQ[2] - v * dQ[0]) * ri;
+        dq[3] = (dQ[3] - w * dQ[0]) * ri;
+        dq[4] = f.gm1 * (0.5 * q2 * dQ[0] - u * dQ[1] - v * dQ[2] - w * dQ[3] + dQ[4]);
+    }
     double a[5];
 #pragma unroll
     for (int k = 0; k < 5; k++) {
@@ -569,7 +662,8 @@ __device__ __forceinline__ void pc_abs_jacobian(const double qL[5], const double
 }
 
 // Pseudo-time matrix Cinv = Mop Kinv Mpr at a node state (beta from the
-// node's Mach; Roe_Jacobian.cpp:241-264 adds (V/dt) Cinv to the diagonal).
+// node's Mach; Roe_Jacobian.cpp:241-264 adds (V/dt) Cinv to the diagonal);
+// Mpr = I for RUP states.
 __device__ __forceinline__ void pc_node_cinv(const double q[5], const Flow &f, double C[25]) {
     Face F;
     eos_face(q, 1.0, 0.0, 0.0, f, true, F);
@@ -583,11 +677,16 @@ __device__ __forceinline__ void pc_node_cinv(const double q[5], const Flow &f, d
 #pragma unroll
     for (int j = 0; j < 5; j++) {
         double m[5];
-        m[0] = j == 0 ? 1.0 : 0.0;
-        m[1] = (j == 0 ? -u : (j == 1 ? 1.0 : 0.0)) / rho;
-        m[2] = (j == 0 ? -v : (j == 2 ? 1.0 : 0.0)) / rho;
-        m[3] = (j == 0 ? -w : (j == 3 ? 1.0 : 0.0)) / rho;
-        m[4] = f.gm1 * (j == 0 ? 0.5 * q2 : (j == 4 ? 1.0 : (j == 1 ? -u : (j == 2 ? -v : -w))));
+        if (f.rup) {
+#pragma unroll
+            for (int k = 0; k < 5; k++) m[k] = k == j ? 1.0 : 0.0;
+        } else {
+            m[0] = j == 0 ? 1.0 : 0.0;
+            m[1] = (j == 0 ? -u : (j == 1 ? 1.0 : 0.0)) / rho;
+            m[2] = (j == 0 ? -v : (j == 2 ? 1.0 : 0.0)) / rho;
+            m[3] = (j == 0 ? -w : (j == 3 ? 1.0 : 0.0)) / rho;
+            m[4] = f.gm1 * (j == 0 ? 0.5 * q2 : (j == 4 ? 1.0 : (j == 1 ? -u : (j == 2 ? -v : -w))));
+        }
         double z0 = m[0] + kc0 * m[4], z1 = m[1] + u * kr * m[4], z2 = m[2] + v * kr * m[4], z3 = m[3] + w * kr * m[4];
         double z4 = k4 * m[4];
         C[j] = z0;
@@ -735,13 +834,7 @@ __device__ __forceinline__ int precond_characteristic_bc(const double qI[5], con
             break;
         default: break;  // 1, 6, 10: freestream
     }
-    const double rb = xb[0], ub = xb[1], vb = xb[2], wb = xb[3], pb = xb[4];
-    const double et = (pb + f.gpinf) / (f.gm1 * rb) + 0.5 * (ub * ub + vb * vb + wb * wb);
-    qB[0] = rb;
-    qB[1] = rb * ub;
-    qB[2] = rb * vb;
-    qB[3] = rb * wb;
-    qB[4] = rb * et;
+    store_state(xb[0], xb[1], xb[2], xb[3], xb[4], f, qB);
     return status;
 }
 

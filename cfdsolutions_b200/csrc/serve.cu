@@ -377,8 +377,15 @@ int cfd_initial_state(const cfd_mesh *m, const cfd_params *p, const double noise
         for (int d = 0; d < 3; d++)
             v[d] = u0[d] * (phys ? 1.0 + noise[1] * unit_pm1(seed, (uint64_t)((1 + d) * N + i)) : 1.0);
         const double pr = 1.0 * (phys ? 1.0 + noise[2] * unit_pm1(seed, (uint64_t)(4 * N + i)) : 1.0);
-        const double et = (pr + gamma * pinf) / ((gamma - 1.0) * rho) + 0.5 * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
         Q[i] = rho;
+        if (p->variables == CFD_VARS_RUP) {
+            Q[n + i] = v[0];
+            Q[2 * n + i] = v[1];
+            Q[3 * n + i] = v[2];
+            Q[4 * n + i] = pr;
+            continue;
+        }
+        const double et = (pr + gamma * pinf) / ((gamma - 1.0) * rho) + 0.5 * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
         Q[n + i] = rho * v[0];
         Q[2 * n + i] = rho * v[1];
         Q[3 * n + i] = rho * v[2];

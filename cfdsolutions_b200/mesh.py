@@ -164,3 +164,20 @@ def write_vtk(mesh: Mesh, path: str, params, Q: np.ndarray, tri_tag: np.ndarray 
     capi.check(capi.lib.cfd_vtk_write(str(path).encode(), mesh.nnode, capi.ptr(coords), tris.shape[0], capi.ptr(tris),
                                       None if tag is None else capi.ptr(tag), tets.shape[0], capi.ptr(tets),
                                       C.byref(params), capi.ptr(Q), Q.shape[1]), "cfd_vtk_write")
+
+
+def to_rup(Q: np.ndarray, gamma: float, pinf: float = 0.0) -> np.ndarray:
+    """Conservative state SoA [5, n] -> (rho, u, v, w, p) (CFD_VARS_RUP;
+    MPFLOW3D Material_Transformations, VARIABLE_CON -> VARIABLE_RUP), with
+    p = (gamma - 1)(rho et - rho q^2 / 2) - gamma pinf."""
+    Q = np.asarray(Q, np.float64)
+    r = Q[0]
+    u, v, w = Q[1] / r, Q[2] / r, Q[3] / r
+    p = (gamma - 1.0) * (Q[4] - 0.5 * r * (u * u + v * v + w * w)) - gamma * pinf
+    return np.stack([r, u, v, w, p])
+
+
+def to_conservative(R: np.ndarray, gamma: float, pinf: float = 0.0) -> np.ndarray:
+    """(rho, u, v, w, p) SoA [5, n] -> conservative, rho et = (p + gamma pinf) / (gamma - 1) + rho q^2 / 2."""
+    r, u, v, w, p = np.asarray(R, np.float64)
+    return np.stack([r, r * u, r * v, r * w, (p + gamma * pinf) / (gamma - 1.0) + 0.5 * r * (u * u + v * v + w * w)])

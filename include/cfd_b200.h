@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define CFD_ABI_VERSION 5
+#define CFD_ABI_VERSION 6
 
 /* ------------------------------------------------------------ status codes */
 #define CFD_OK                 0
@@ -102,6 +102,13 @@ extern "C" {
                                    low-precision matrix (no FP64 copy); the outer FP64 correction is then the
                                    caller's nonlinear defect, and GMRES works with the stored matrix */
 
+/* Solution variables (VARIABLE_TYPE, MPFLOW3D/include/SolverParameters.h:296-302): cfd_params.variables
+ * (CONSERVATIVE or RUP) and the column names of cfd_rms_file_open (all four) */
+#define CFD_VARS_CONSERVATIVE 0  /* VARIABLE_CONSERVATIVE / VARIABLE_CON: (rho, rho u, rho v, rho w, rho et) */
+#define CFD_VARS_RUP          1  /* VARIABLE_RUP: (rho, u, v, w, p) */
+#define CFD_VARS_PUT          2  /* (p, u, v, w, T)   */
+#define CFD_VARS_RUT          3  /* (rho, u, v, w, T) */
+
 #define CFD_PC_NONE      0  /* GMRES right preconditioner */
 #define CFD_PC_BLOCK_JACOBI 1
 #define CFD_PC_ILU0      2  /* ILU(0) in the mesh (row) order, level-scheduled */
@@ -149,6 +156,25 @@ typedef struct cfd_params {
     int    precond_type;
     double precond_mach;
     double outflow_pressure;
+    /* VARIABLE_TYPE: the variables the state Q holds, which the gradients and
+     * limiters act on, the second-order faces are reconstructed in, the
+     * boundary ghost states are written in, and the Jacobian's columns and the
+     * update X refer to.
+     *   CFD_VARS_CONSERVATIVE: Euler3D's formulation (and the layout at the top
+     *     of this file);
+     *   CFD_VARS_RUP: (rho, u, v, w, p), MPFLOW3D's implicit formulation
+     *     (GUAGE_PRESSURE 0): faces take p directly (Material_Get_Properties,
+     *     MPFLOW3D/src/Material.cpp:591-599), Thornber blends the velocities
+     *     at fixed rho and p (Roe_Fluxes.cpp:1161-1168), and the Jacobian is
+     *     d/d(rho,u,v,w,p): the convective blocks dF/dW at the nodes
+     *     (CompressibleUtils.cpp:85-186), the dissipation Mop |A| at the Roe
+     *     state (Roe_Fluxes.cpp:3185-3199) and the pseudo-time term
+     *     (V/dt) Mop [Kinv] (Roe_Jacobian.cpp:241-264).  The residual is still
+     *     the conservation-law residual.  Not on cfd_jacobian_fd or
+     *     cfd_solve_unsteady (CFD_ERR_UNSUPPORTED).
+     * The stiffened gas keeps its pressure exact in RUP (no gamma pinf
+     * cancellation). */
+    int    variables;
 } cfd_params;
 
 /* Fills p with the defaults used by the reference parameter files of this
@@ -197,7 +223,8 @@ int  cfd_get_state(cfd_ctx *ctx, double *Q);
  * cfd_gradient needs cfd_gradient again before cfd_limiter. */
 int  cfd_state_device_ptr(cfd_ctx *ctx, double **dQ, int64_t *ld);
 /* Freestream state per node (Solver_Set_Initial_Conditions,
- * Euler3D/src/Solver.cpp:339-393) on the device. */
+ * Euler3D/src/Solver.cpp:339-393) on the device, in the variables of the
+ * context's cfd_params. */
 int  cfd_set_freestream(cfd_ctx *ctx);
 
 /* --------------------------------------------- hot path (device-resident)
@@ -491,7 +518,7 @@ int  cfd_perturbed_freestream(const cfd_mesh *m, double gamma, double mach, doub
 /* The same for any gas of p (gamma, pinf, mach, alpha, beta): the freestream
  * of p with density, velocity and pressure noise of their own amplitudes
  * noise[0..2] (same hash streams as above); with pinf = 0 and three equal
- * amplitudes it equals cfd_perturbed_freestream. */
+ * amplitudes it equals cfd_perturbed_freestream.  Q is in p->variables. */
 int  cfd_initial_state(const cfd_mesh *m, const cfd_params *p, const double noise[3], uint64_t seed, double *Q);
 
 /* ------------------------------------------------------------ serving loop
@@ -598,10 +625,6 @@ int  cfd_restart_read(const char *path, int *iteration, int nnode, int nghost, d
  * (non-preconditioned files).  close writes the closing rule line. */
 #define CFD_RMSFILE_EULER3D  0
 #define CFD_RMSFILE_MPFLOW3D 1
-#define CFD_VARS_CONSERVATIVE 0  /* VARIABLE_CONSERVATIVE / VARIABLE_CON */
-#define CFD_VARS_RUP          1  /* (rho, u, v, w, p) */
-#define CFD_VARS_PUT          2  /* (p, u, v, w, T)   */
-#define CFD_VARS_RUT          3  /* (rho, u, v, w, T) */
 typedef struct cfd_rms_file cfd_rms_file;
 int  cfd_rms_file_open(const char *path, int layout, int variables, int precond, cfd_rms_file **out);
 int  cfd_rms_file_write(cfd_rms_file *f, int iteration, const double rms[6], const double extrema[8],

@@ -41,9 +41,21 @@ typedef struct { double rho, u, v, w, et, p, ht, ubar, c; } face_t;
 
 /* Compute_EOS_Variables_Face, conservative branch (Material.cpp:216-248),
  * extended to the stiffened gas p = (g - 1) rho e - g pinf, c^2 = g (p + pinf) / rho
- * (pinf = 0: the reference's ideal gas). */
-static void eos_face(const double *q, double nx, double ny, double nz, double g, double pinf, face_t *s) {
+ * (pinf = 0: the reference's ideal gas).  With p->variables == 1 the state is
+ * (rho, u, v, w, p), taken as stored (MPFLOW3D Material_Get_Properties,
+ * VARIABLE_RUP, MPFLOW3D/src/Material.cpp:591-599). */
+static void eos_face(const double *q, double nx, double ny, double nz, const orc_params *p, face_t *s) {
+    double g = p->gamma, pinf = p->pinf;
     s->rho = q[0];
+    if (p->variables == 1) {
+        s->u = q[1]; s->v = q[2]; s->w = q[3]; s->p = q[4];
+        double q2 = s->u * s->u + s->v * s->v + s->w * s->w;
+        s->et = (s->p + g * pinf) / ((g - 1.0) * s->rho) + 0.5 * q2;
+        s->ht = s->et + s->p / s->rho;
+        s->c = sqrt((g * (s->p + pinf)) / s->rho);
+        s->ubar = s->u * nx + s->v * ny + s->w * nz;
+        return;
+    }
     s->u = q[1] / s->rho;
     s->v = q[2] / s->rho;
     s->w = q[3] / s->rho;
@@ -53,6 +65,15 @@ static void eos_face(const double *q, double nx, double ny, double nz, double g,
     s->ht = (s->rho * s->et + s->p) / s->rho;
     s->c = sqrt((g * (s->p + pinf)) / s->rho);
     s->ubar = s->u * nx + s->v * ny + s->w * nz;
+}
+
+/* A ghost state from (rho, u, v, w, p) in the state's variables (Get_TotalEnergy,
+ * Material.cpp:1012-1040, for conservative states). */
+static void put_state(double rb, double ub, double vb, double wb, double pb, const orc_params *p, double *qB) {
+    if (p->variables == 1) { qB[0] = rb; qB[1] = ub; qB[2] = vb; qB[3] = wb; qB[4] = pb; return; }
+    double et = ub * ub + vb * vb + wb * wb;
+    et = (pb + p->gamma * p->pinf) / ((p->gamma - 1.0) * rb) + 0.5 * et;
+    qB[0] = rb; qB[1] = rb * ub; qB[2] = rb * vb; qB[3] = rb * wb; qB[4] = rb * et;
 }
 
 /* ---- Low-Mach preconditioned Roe of the Turkel family (MPFLOW3D) ----------
@@ -173,8 +194,8 @@ static void mm5g(double A[5][5], double B[5][5], double C[5][5]) {
 static double pc_edge(const double *qL, const double *qR, const double *n, const orc_params *p, face_t *Lf, face_t *Rf,
                       double avg[4], pc_sys_t *S) {
     double g = p->gamma;
-    eos_face(qL, n[0], n[1], n[2], g, p->pinf, Lf);
-    eos_face(qR, n[0], n[1], n[2], g, p->pinf, Rf);
+    eos_face(qL, n[0], n[1], n[2], p, Lf);
+    eos_face(qR, n[0], n[1], n[2], p, Rf);
     double rho, u, v, w, ht, c;
     if (p->pc_avg == 1) { /* simple mean, |c^2| (Euler3D FluxTest.cpp:3927-3940) */
         rho = 0.5 * (Rf->rho + Lf->rho);
@@ -201,9 +222,12 @@ static double pc_edge(const double *qL, const double *qR, const double *n, const
 
 /* |A|_p = Mop Kinv R |Lambda| L Mpr (Compute_Dissipation_Matrix_Roe_Precondition_Turkel,
  * Roe_Fluxes.cpp:3440-3810). */
-static void pc_absA(const pc_sys_t *S, const double avg[4], double g, double A[5][5]) {
+static void pc_absA(const pc_sys_t *S, const double avg[4], const orc_params *p, double A[5][5]) {
     double Mpr[5][5], Mop[5][5], T[5][5], U[5][5], V[5][5];
-    pc_transforms(avg[0], avg[1], avg[2], avg[3], g, Mpr, Mop);
+    pc_transforms(avg[0], avg[1], avg[2], avg[3], p->gamma, Mpr, Mop);
+    if (p->variables == 1) /* the state's own (rho, u, v, w, p): Mpr = I */
+        for (int i = 0; i < 5; i++)
+            for (int j = 0; j < 5; j++) Mpr[i][j] = i == j ? 1.0 : 0.0;
     for (int i = 0; i < 5; i++)
         for (int j = 0; j < 5; j++) U[i][j] = S->lam[i] * S->L[i][j];       /* |Lambda| L */
     mm5g((double (*)[5])S->R, U, T);                                       /* R |Lambda| L */
@@ -224,7 +248,7 @@ static double roe_pc(const double *qL, const double *qR, const double *n, double
     double mL = L.rho * L.ubar, mR = R.rho * R.ubar;
     double FL[5] = {mL, L.u * mL + L.p * n[0], L.v * mL + L.p * n[1], L.w * mL + L.p * n[2], L.ht * mL};
     double FR[5] = {mR, R.u * mR + R.p * n[0], R.v * mR + R.p * n[1], R.w * mR + R.p * n[2], R.ht * mR};
-    pc_absA(&S, avg, p->gamma, A);
+    pc_absA(&S, avg, p, A);
     for (int i = 0; i < 5; i++) {
         double fa = 0.0;
         for (int j = 0; j < 5; j++) fa += A[i][j] * (qR[j] - qL[j]);
@@ -240,7 +264,7 @@ static double roe_pc(const double *qL, const double *qR, const double *n, double
 static void pc_node_cinv(const double *q, const orc_params *p, double C[5][5]) {
     face_t F;
     double n0[3] = {1.0, 0.0, 0.0};
-    eos_face(q, n0[0], n0[1], n0[2], p->gamma, p->pinf, &F);
+    eos_face(q, n0[0], n0[1], n0[2], p, &F);
     double mach = sqrt(F.u * F.u + F.v * F.v + F.w * F.w) / F.c;
     double beta = pc_beta(p, mach, 0.0), alpha, delta;
     pc_params(p, beta, &alpha, &delta);
@@ -248,6 +272,9 @@ static void pc_node_cinv(const double *q, const orc_params *p, double C[5][5]) {
                                     (alpha * F.v) / (beta * F.rho * c2), (alpha * F.w) / (beta * F.rho * c2), 1.0 / beta};
     double Mpr[5][5], Mop[5][5], K[5][5] = {{0}}, T[5][5];
     pc_transforms(F.rho, F.u, F.v, F.w, p->gamma, Mpr, Mop);
+    if (p->variables == 1)
+        for (int i = 0; i < 5; i++)
+            for (int j = 0; j < 5; j++) Mpr[i][j] = i == j ? 1.0 : 0.0;
     for (int i = 0; i < 5; i++) { K[i][i] = i == 4 ? 0.0 : 1.0; K[i][4] += kc[i]; }
     mm5g(Mop, K, T);
     mm5g(T, Mpr, C);
@@ -291,10 +318,10 @@ static int bc_state_pc(const double *qI, const double *qG, const double *areav, 
     unit(areav, n, &mag);
     face_t I, G, O;
     double q0[5];
-    eos_face(qI, n[0], n[1], n[2], p->gamma, p->pinf, &I);
-    eos_face(qG, n[0], n[1], n[2], p->gamma, p->pinf, &G);
+    eos_face(qI, n[0], n[1], n[2], p, &I);
+    eos_face(qG, n[0], n[1], n[2], p, &G);
     for (int k = 0; k < 5; k++) q0[k] = 0.5 * (qI[k] + qG[k]);
-    eos_face(q0, n[0], n[1], n[2], p->gamma, p->pinf, &O);
+    eos_face(q0, n[0], n[1], n[2], p, &O);
     double mach = sqrt(O.u * O.u + O.v * O.v + O.w * O.w) / O.c;
     double mI = sqrt(I.u * I.u + I.v * I.v + I.w * I.w) / I.c, mG = sqrt(G.u * G.u + G.v * G.v + G.w * G.w) / G.c;
     double beta = pc_beta(p, mach, dmax(mI, mG)), alpha, delta;
@@ -364,9 +391,7 @@ static int bc_state_pc(const double *qI, const double *qG, const double *areav, 
             break;
         default: break; /* 1, 6, 10: freestream */
     }
-    double rb = xb[0], ub = xb[1], vb = xb[2], wb = xb[3], pb = xb[4];
-    double et = (pb + p->gamma * p->pinf) / ((p->gamma - 1.0) * rb) + 0.5 * (ub * ub + vb * vb + wb * wb);
-    qB[0] = rb; qB[1] = rb * ub; qB[2] = rb * vb; qB[3] = rb * wb; qB[4] = rb * et;
+    put_state(xb[0], xb[1], xb[2], xb[3], xb[4], p, qB);
     return st;
 }
 
@@ -379,10 +404,10 @@ static int bc_state(const double *qI, const double *qG, const double *areav, int
     unit(areav, n, &mag);
     face_t I, G, O;
     double q0[5];
-    eos_face(qI, n[0], n[1], n[2], p->gamma, p->pinf, &I);
-    eos_face(qG, n[0], n[1], n[2], p->gamma, p->pinf, &G);
+    eos_face(qI, n[0], n[1], n[2], p, &I);
+    eos_face(qG, n[0], n[1], n[2], p, &G);
     for (int k = 0; k < 5; k++) q0[k] = 0.5 * (qI[k] + qG[k]);
-    eos_face(q0, n[0], n[1], n[2], p->gamma, p->pinf, &O);
+    eos_face(q0, n[0], n[1], n[2], p, &O);
     double l1 = O.ubar, l4 = l1 + O.c, l5 = l1 - O.c;
     double pb = inf[5], rb = inf[0], ub = inf[1], vb = inf[2], wb = inf[3];
     double outflow_p = 0.935 * inf[5];
@@ -441,9 +466,7 @@ static int bc_state(const double *qI, const double *qG, const double *areav, int
         default: break;
     }
     if (pb + p->pinf < 0.0) st = st ? st : 1;
-    double et = ub * ub + vb * vb + wb * wb;
-    et = (pb + p->gamma * p->pinf) / ((p->gamma - 1.0) * rb) + 0.5 * et;   /* Get_TotalEnergy, Material.cpp:1012-1040 */
-    qB[0] = rb; qB[1] = rb * ub; qB[2] = rb * vb; qB[3] = rb * wb; qB[4] = rb * et;
+    put_state(rb, ub, vb, wb, pb, p, qB);
     return st;
 }
 
@@ -478,11 +501,20 @@ static void entropy_fix(double ubL, double cL, double ubR, double cR, double ub,
  * u_R' symmetric; density and total energy unchanged. */
 static void thornber(const double *qL, const double *qR, const orc_params *p, double *mL, double *mR) {
     face_t L, R;
-    eos_face(qL, 1.0, 0.0, 0.0, p->gamma, p->pinf, &L);
-    eos_face(qR, 1.0, 0.0, 0.0, p->gamma, p->pinf, &R);
+    eos_face(qL, 1.0, 0.0, 0.0, p, &L);
+    eos_face(qR, 1.0, 0.0, 0.0, p, &R);
     double z = dmin(1.0, dmax(sqrt(L.u * L.u + L.v * L.v + L.w * L.w) / L.c,
                               sqrt(R.u * R.u + R.v * R.v + R.w * R.w) / R.c));
     mL[0] = qL[0]; mR[0] = qR[0]; mL[4] = qL[4]; mR[4] = qR[4];
+    if (p->variables == 1) { /* velocities blended at fixed rho and p (MPFLOW3D Roe_Fluxes.cpp:1161-1168) */
+        for (int i = 1; i < 4; i++) {
+            double t1 = 0.5 * ((1.0 + z) * qL[i] + (1.0 - z) * qR[i]);
+            double t2 = 0.5 * ((1.0 + z) * qR[i] + (1.0 - z) * qL[i]);
+            mL[i] = t1;
+            mR[i] = t2;
+        }
+        return;
+    }
     for (int i = 1; i < 4; i++) {
         double t1 = 0.5 * ((1.0 + z) * qL[i] / qL[0] + (1.0 - z) * qR[i] / qR[0]);
         double t2 = 0.5 * ((1.0 + z) * qR[i] / qR[0] + (1.0 - z) * qL[i] / qL[0]);
@@ -496,8 +528,8 @@ static double roe(const double *qL, const double *qR, const double *n, double ar
                   double *conv, double *diss, double lam[3]) {
     face_t L, R;
     double g = p->gamma;
-    eos_face(qL, n[0], n[1], n[2], g, p->pinf, &L);
-    eos_face(qR, n[0], n[1], n[2], g, p->pinf, &R);
+    eos_face(qL, n[0], n[1], n[2], p, &L);
+    eos_face(qR, n[0], n[1], n[2], p, &R);
     double FL[5], FR[5];
     FL[0] = L.rho * L.ubar; FL[1] = L.u * FL[0] + L.p * n[0]; FL[2] = L.v * FL[0] + L.p * n[1];
     FL[3] = L.w * FL[0] + L.p * n[2]; FL[4] = L.ht * FL[0];
@@ -585,8 +617,8 @@ static double hllc(const double *qL, const double *qR, const double *n, double a
                    double *conv, double *diss) {
     face_t L, R;
     double g = p->gamma;
-    eos_face(qL, n[0], n[1], n[2], g, p->pinf, &L);
-    eos_face(qR, n[0], n[1], n[2], g, p->pinf, &R);
+    eos_face(qL, n[0], n[1], n[2], p, &L);
+    eos_face(qR, n[0], n[1], n[2], p, &R);
     double rho = sqrt(R.rho * L.rho), sigma = rho / (L.rho + rho);
     double u = L.u + sigma * (R.u - L.u), v = L.v + sigma * (R.v - L.v), w = L.w + sigma * (R.w - L.w);
     double ht = L.ht + sigma * (R.ht - L.ht);
@@ -625,8 +657,8 @@ static double vanleer(const double *qL, const double *qR, const double *n, doubl
                       double *conv, double *diss) {
     face_t L, R;
     double g = p->gamma, nx = n[0], ny = n[1], nz = n[2];
-    eos_face(qL, nx, ny, nz, g, p->pinf, &L);
-    eos_face(qR, nx, ny, nz, g, p->pinf, &R);
+    eos_face(qL, nx, ny, nz, p, &L);
+    eos_face(qR, nx, ny, nz, p, &R);
     double rho_a = 0.5 * (L.rho + R.rho), ub_a = 0.5 * ((L.u + R.u) * nx + (L.v + R.v) * ny + (L.w + R.w) * nz);
     double p_a = 0.5 * (L.p + R.p), c_a = sqrt(g * p_a / rho_a);
     double lmax = dmax(fabs(ub_a), dmax(fabs(ub_a + c_a), fabs(ub_a - c_a)));
@@ -674,8 +706,8 @@ static double ausmp(const double *qL, const double *qR, const double *n, double 
                     double *conv, double *diss) {
     face_t L, R;
     double g = p->gamma;
-    eos_face(qL, n[0], n[1], n[2], g, p->pinf, &L);
-    eos_face(qR, n[0], n[1], n[2], g, p->pinf, &R);
+    eos_face(qL, n[0], n[1], n[2], p, &L);
+    eos_face(qR, n[0], n[1], n[2], p, &R);
     double k = 2.0 * (g - 1.0) / (g + 1.0);
     double csL = sqrt(k * L.ht), csR = sqrt(k * R.ht);
     double c12 = dmin(csL * csL / dmax(csL, L.ubar), csR * csR / dmax(csR, -R.ubar));
@@ -903,7 +935,8 @@ void orc_limiter(const orc_mesh *m, const orc_params *p, const double *Q, const 
                 q[v] = qc[v] + ph[v] * (frac * (Q[IDX(v, j, ld)] - qc[v]) + (1.0 - frac) * gr);
             }
             /* p < 0 (Limiters.cpp:296-301); for the stiffened gas p + pinf < 0 */
-            double pc = (p->gamma - 1.0) * ((q[4] - p->pinf) - (0.5 / q[0]) * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]));
+            double pc = p->variables == 1 ? q[4] + p->pinf
+                                          : (p->gamma - 1.0) * ((q[4] - p->pinf) - (0.5 / q[0]) * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]));
             if (pc < 0.0)
                 for (int v = 0; v < 5; v++) ph[v] = 0.0;
         }
@@ -924,8 +957,8 @@ void orc_limiter(const orc_mesh *m, const orc_params *p, const double *Q, const 
             }
             /* Compute_RoeVariables (Roe_Fluxes.cpp:3609-3633) */
             face_t A, B;
-            eos_face(qa, 0, 0, 0, p->gamma, p->pinf, &A);
-            eos_face(qb, 0, 0, 0, p->gamma, p->pinf, &B);
+            eos_face(qa, 0, 0, 0, p, &A);
+            eos_face(qb, 0, 0, 0, p, &B);
             double rho = sqrt(B.rho * A.rho), sg = rho / (A.rho + rho);
             double u = A.u + sg * (B.u - A.u), v = A.v + sg * (B.v - A.v), w = A.w + sg * (B.w - A.w);
             double ht = A.ht + sg * (B.ht - A.ht);
@@ -978,6 +1011,26 @@ static void flux_jac(const double *q, const double *n, double g, double pinf, do
     J[0][4] = 0.0; J[1][4] = (g - 1.0) * nx; J[2][4] = (g - 1.0) * ny; J[3][4] = (g - 1.0) * nz; J[4][4] = g * ub;
 }
 
+/* dF.n/d(rho, u, v, w, p) (Compute_Flux_Jacobian_Euler_Convective, VARIABLE_RUP,
+ * MPFLOW3D/src/CompressibleUtils.cpp:85-186), rho ht = g (p + pinf) / (g - 1) + rho q^2 / 2. */
+static void flux_jac_rup(const double *q, const double *n, double g, double pinf, double J[5][5]) {
+    double rho = q[0], u = q[1], v = q[2], w = q[3], pr = q[4];
+    double ub = u * n[0] + v * n[1] + w * n[2], q2 = u * u + v * v + w * w;
+    double ht = g * (pr + pinf) / ((g - 1.0) * rho) + 0.5 * q2;
+    double vel[3] = {u, v, w};
+    J[0][0] = ub;
+    for (int d = 0; d < 3; d++) J[0][1 + d] = rho * n[d];
+    J[0][4] = 0.0;
+    for (int k = 0; k < 3; k++) {
+        J[1 + k][0] = vel[k] * ub;
+        for (int d = 0; d < 3; d++) J[1 + k][1 + d] = rho * vel[k] * n[d] + (k == d ? rho * ub : 0.0);
+        J[1 + k][4] = n[k];
+    }
+    J[4][0] = 0.5 * q2 * ub;
+    for (int d = 0; d < 3; d++) J[4][1 + d] = rho * (vel[d] * ub + ht * n[d]);
+    J[4][4] = g / (g - 1.0) * ub;
+}
+
 static void mm5(double A[5][5], double B[5][5], double C[5][5]) {
     for (int i = 0; i < 5; i++)
         for (int j = 0; j < 5; j++) {
@@ -990,8 +1043,8 @@ static void mm5(double A[5][5], double B[5][5], double C[5][5]) {
 static void roe_absA(const double *qL, const double *qR, const double *n, const orc_params *p, double A[5][5]) {
     face_t L, R;
     double g = p->gamma;
-    eos_face(qL, n[0], n[1], n[2], g, p->pinf, &L);
-    eos_face(qR, n[0], n[1], n[2], g, p->pinf, &R);
+    eos_face(qL, n[0], n[1], n[2], p, &L);
+    eos_face(qR, n[0], n[1], n[2], p, &R);
     double rho = sqrt(R.rho * L.rho), sigma = rho / (L.rho + rho);
     double u = L.u + sigma * (R.u - L.u), v = L.v + sigma * (R.v - L.v), w = L.w + sigma * (R.w - L.w);
     double ht = L.ht + sigma * (R.ht - L.ht);
@@ -1015,6 +1068,16 @@ static void roe_absA(const double *qL, const double *qR, const double *n, const 
     Lm[0][0] = Lm[1][1] = Lm[2][2] = E[0]; Lm[3][3] = E[1]; Lm[4][4] = E[2];
     double T[5][5], Ti[5][5], LT[5][5];
     mm5(M, P, T);
+    if (p->variables == 1) {
+        /* columns in (rho, u, v, w, p): Mop |A| (MPFLOW3D Compute_Dissipation_Matrix_Roe_Optimized,
+         * Roe_Fluxes.cpp:3185-3199, Mpr = I); mpf_form 1 carries its E1 (1 - ny^2) w-momentum
+         * diagonal (:3146), i.e. |A|[3][3] + E0 (nz^2 - ny^2) in (rho, u, v, w, p) */
+        mm5(Lm, Pi, LT);
+        mm5(T, LT, A);
+        if (p->mpf_form == 1)
+            for (int a = 0; a < 5; a++) A[a][3] += M[a][3] * E[0] * (nz * nz - ny * ny);
+        return;
+    }
     mm5(Pi, Mi, Ti);
     mm5(Lm, Ti, LT);
     mm5(T, LT, A);
@@ -1037,6 +1100,13 @@ void orc_jacobian(const orc_mesh *m, const orc_params *p, const double *Q, const
             pc_node_cinv(q, p, C);
             for (int a = 0; a < 5; a++)
                 for (int b = 0; b < 5; b++) A[25 * (size_t)IAU[i] + 5 * a + b] = m->vol[i] / dt[i] * C[a][b];
+        } else if (add_time && p->variables == 1) {
+            /* (V / dt) dQ/d(rho, u, v, w, p) (MPFLOW3D Roe_Jacobian.cpp:241-264, PRECOND_METHOD_NONE) */
+            double q[5], Mpr[5][5], Mop[5][5];
+            for (int k = 0; k < 5; k++) q[k] = Q[IDX(k, i, ld)];
+            pc_transforms(q[0], q[1], q[2], q[3], p->gamma, Mpr, Mop);
+            for (int a = 0; a < 5; a++)
+                for (int b = 0; b < 5; b++) A[25 * (size_t)IAU[i] + 5 * a + b] = m->vol[i] / dt[i] * Mop[a][b];
         } else if (add_time)
             for (int k = 0; k < 5; k++) A[25 * (size_t)IAU[i] + 6 * k] = m->vol[i] / dt[i];
     }
@@ -1049,14 +1119,19 @@ void orc_jacobian(const orc_mesh *m, const orc_params *p, const double *Q, const
             double n[3], area, qL[5], qR[5], JL[5][5], JR[5][5], Ab[5][5];
             unit(ea + 3 * (size_t)e, n, &area);
             for (int k = 0; k < 5; k++) { qL[k] = Q[IDX(k, L, ld)]; qR[k] = Q[IDX(k, R, ld)]; }
-            flux_jac(qL, n, p->gamma, p->pinf, JL);
-            flux_jac(qR, n, p->gamma, p->pinf, JR);
+            if (p->variables == 1) {
+                flux_jac_rup(qL, n, p->gamma, p->pinf, JL);
+                flux_jac_rup(qR, n, p->gamma, p->pinf, JR);
+            } else {
+                flux_jac(qL, n, p->gamma, p->pinf, JL);
+                flux_jac(qR, n, p->gamma, p->pinf, JR);
+            }
             if (p->flux == 4) {
                 face_t Lf, Rf;
                 pc_sys_t S;
                 double avg[4];
                 pc_edge(qL, qR, n, p, &Lf, &Rf, avg, &S);
-                pc_absA(&S, avg, p->gamma, Ab);
+                pc_absA(&S, avg, p, Ab);
             } else if (p->flux == 5) {
                 double mL[5], mR[5];
                 thornber(qL, qR, p, mL, mR);

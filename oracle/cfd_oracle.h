@@ -33,6 +33,8 @@ typedef struct {
      * exactly as written, whose w-momentum diagonal reads E1 (1 - ny^2); 2 the
      * same matrix form with E1 (1 - nz^2) */
     int mpf_form;
+    /* state variables: 0 conservative, 1 (rho, u, v, w, p) (MPFLOW3D VARIABLE_RUP) */
+    int variables;
 } orc_params;
 
 typedef struct {

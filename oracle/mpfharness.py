@@ -254,15 +254,19 @@ def run(mesh, cfg: dict, Q: np.ndarray | None, steps: list, quiet: bool = True, 
     residual, BC and time step, not its implicit Jacobian, which needs RUP) and
     the state passes unchanged; otherwise it is handed to MPFLOW3D as RUP and a
     returned ``state`` is converted back to conservative variables
-    (``state_rup`` keeps MPFLOW3D's own)."""
+    (``state_rup`` keeps MPFLOW3D's own).  With ``cfg["variables"] == 1`` (the
+    library's CFD_VARS_RUP) ``Q`` is already (rho, u, v, w, p) and passes
+    unchanged both ways."""
     if not available():
         raise FileNotFoundError(f"{MPF_LIB} not built (make -C oracle ref)")
     con = cfg.get("mpf_variable", "rup") == "con"
-    R = None if Q is None else (np.asarray(Q, np.float64) if con else cons_to_rup(np.asarray(Q, np.float64)))
+    own = not con and cfg.get("variables", 0) == 1  # Q already holds (rho, u, v, w, p)
+    R = None if Q is None else (np.asarray(Q, np.float64) if (con or own) else cons_to_rup(np.asarray(Q, np.float64)))
     ctx = mp.get_context("spawn")
     with ctx.Pool(1) as pool:
         out = pool.apply_async(_session, (_mesh_dict(mesh), cfg, R, steps, quiet)).get(timeout)
     if "state" in out and not con:
         out["state_rup"] = out["state"]
-        out["state"] = rup_to_cons(out["state"])
+        if not own:
+            out["state"] = rup_to_cons(out["state"])
     return out

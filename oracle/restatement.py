@@ -23,7 +23,7 @@ class Params(C.Structure):
                 ("entropy_fix", C.c_int), ("global_time", C.c_int), ("ls_weight", C.c_int), ("gradient", C.c_int),
                 ("iteration", C.c_int), ("zpg_iteration", C.c_int), ("pinf", C.c_double),
                 ("pc_method", C.c_int), ("pc_type", C.c_int), ("pc_mach", C.c_double), ("outflow_p", C.c_double),
-                ("pc_avg", C.c_int), ("mpf_form", C.c_int)]
+                ("pc_avg", C.c_int), ("mpf_form", C.c_int), ("variables", C.c_int)]
 
 
 class MeshC(C.Structure):
@@ -173,7 +173,7 @@ def params(cfg: dict, iteration: int = 0) -> Params:
                   g("limiter_smooth", 0), g("entropy_fix", 0), g("global_time", 0), g("ls_weight", 0),
                   g("gradient", 0), iteration, g("zpg_iteration", 0), g("pinf", 0.0),
                   g("precond_method", 0), g("precond_type", 0), g("precond_mach", 0.0), g("outflow_pressure", 0.0),
-                  g("precond_average", 0), g("mpf_form", 0))
+                  g("precond_average", 0), g("mpf_form", 0), g("variables", 0))
 
 
 def first_order_step(mesh, cfg: dict, Q: np.ndarray, gs_sweeps: int = 10) -> dict:

@@ -79,6 +79,17 @@ JAC_CASES = [
 ]
 
 
+# The library's RUP formulation (cfd_params.variables = CFD_VARS_RUP) against
+# MPFLOW3D's own (VARIABLE_RUP): the same state handed over unchanged.
+RUP = dict(variables=1)
+RUP_PASS_CASES = [(n, dict(c, **RUP), bc) for n, c, bc in PRECOND_CASES
+                  if n in ("turkel_local", "eriksson_global", "btw_urlocal", "turkel_local_o2", "turkel_channel_o2")]
+RUP_EDGE_CASES = [(n, dict(c, **RUP)) for n, c in EDGE_CASES
+                  if n in ("roe", "roe_o2_venkat", "roe_o2_bj_smooth", "hllc", "hllc_o2", "thornber", "thornber_o2")]
+# the whole Jacobian in (rho,u,v,w,p) columns, with the pseudo-time term, and B
+RUP_JAC_CASES = [(n, dict(c, **RUP)) for n, c in JAC_CASES] + [("roe_o2_venkat", dict(CFG1, **SECOND, **RUP))]
+
+
 def mesh_for(face_bc):
     if face_bc is None:
         return box_mesh(5, jitter=0.15, seed=11)
@@ -98,6 +109,27 @@ def mpf_pass(m, cfg, Q):
     """MPFLOW3D (conservative variables): gradient + limiter, BC, residual, time step."""
     from oracle import mpfharness
     return mpfharness.run(m, dict(cfg, mpf_variable="con"), Q, PASS_STEPS)
+
+
+def rup_case(cfg, face_bc=None):
+    """A case's mesh, configuration and state in (rho, u, v, w, p)."""
+    from cfdsolutions_b200 import to_rup
+    m, cfg, Q = case(cfg, face_bc)
+    return m, cfg, to_rup(Q, cfg.get("gamma", 1.4), cfg.get("pinf", 0.0))
+
+
+def mpf_pass_rup(m, cfg, R):
+    """MPFLOW3D in its RUP variables: gradient + limiter, BC, residual, time step."""
+    from oracle import mpfharness
+    return mpfharness.run(m, cfg, R, PASS_STEPS)
+
+
+def mpf_jacobian_rup(m, cfg, R):
+    """MPFLOW3D's implicit path on a RUP state: the pass, then the Jacobian
+    with the pseudo-time term.  Returns (post-BC state, A, B)."""
+    from oracle import mpfharness
+    out = mpfharness.run(m, cfg, R, PASS_STEPS + [("jacobian", 1, 0), ("get", "matrix")])
+    return out["state"], out["A"], out["B"]
 
 
 def mpf_jacobians(m, cfg, Q):

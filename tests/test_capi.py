@@ -30,7 +30,7 @@ def test_every_declared_symbol_is_exported():
 
 
 def test_abi_version_and_defaults():
-    assert capi.lib.cfd_abi_version() == 5
+    assert capi.lib.cfd_abi_version() == 6
     p = capi.Params()
     capi.lib.cfd_params_default(C.byref(p))
     assert p.gamma == 1.4 and p.flux_scheme == capi.FLUX_ROE and p.limiter == capi.LIMITER_NONE
@@ -128,5 +128,31 @@ def test_perturbed_freestream_matches_the_freestream_without_noise():
         Q2 = np.empty((5, n))
         capi.check(capi.lib.cfd_perturbed_freestream(h, 1.4, 0.7, 3.0, 1.0, 0.02, 9, capi.ptr(Q2)), "pf")
         np.testing.assert_array_equal(Q1, Q2)
+    finally:
+        capi.lib.cfd_mesh_free(h)
+
+
+def test_initial_state_in_rup_variables():
+    """cfd_initial_state with variables = CFD_VARS_RUP writes the same
+    perturbed freestream as (rho, u, v, w, p); to_rup / to_conservative
+    convert between the two to round-off, ideal and stiffened gas."""
+    from cfdsolutions_b200 import default_params, to_conservative, to_rup
+
+    fb = np.ones(6, np.int32)
+    h = C.c_void_p()
+    capi.check(capi.lib.cfd_mesh_box(4, 4, 4, 1.0, 1.0, 1.0, 0.1, 3, 0, capi.ptr(fb), C.byref(h)), "cfd_mesh_box")
+    try:
+        m = box_mesh(4, jitter=0.1, seed=3)
+        n = m.nnode + m.nghost
+        noise = np.array([0.02, 0.03, 0.01])
+        for gamma, pinf in ((1.4, 0.0), (4.4, 6000.0)):
+            p = default_params(gamma=gamma, pinf=pinf, mach=0.3)
+            Qc, Qr = np.empty((5, n)), np.empty((5, n))
+            capi.check(capi.lib.cfd_initial_state(h, C.byref(p), capi.ptr(noise), 5, capi.ptr(Qc)), "is")
+            p.variables = 1
+            capi.check(capi.lib.cfd_initial_state(h, C.byref(p), capi.ptr(noise), 5, capi.ptr(Qr)), "is")
+            np.testing.assert_allclose(to_rup(Qc, gamma, pinf), Qr, rtol=1e-9 if pinf else 1e-14, atol=1e-14)
+            np.testing.assert_allclose(to_conservative(Qr, gamma, pinf), Qc, rtol=1e-14, atol=1e-14)
+            assert np.all(Qr[4] > 0.98) and np.all(Qr[4] < 1.02)  # the pressure itself, not rho et
     finally:
         capi.lib.cfd_mesh_free(h)

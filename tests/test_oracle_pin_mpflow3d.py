@@ -98,3 +98,57 @@ def test_pseudo_time_term_and_rhs_match_mpflow3d(mpf_available, name, cfg):
     theirs = (A[1] - A[0])[s.IAU]
     assert _mpf.rel(mine, theirs) <= 1e-12
     assert _mpf.rel(B1, B) <= 1e-12
+
+
+# ---------------------------------------------------------------- RUP variables
+@pytest.mark.parametrize("name,cfg,face_bc", _mpf.RUP_PASS_CASES, ids=[c[0] for c in _mpf.RUP_PASS_CASES])
+def test_rup_preconditioned_pass_matches_mpflow3d(mpf_available, name, cfg, face_bc):
+    """The restatement with (rho, u, v, w, p) states against MPFLOW3D's
+    VARIABLE_RUP: ghost states of the preconditioned characteristic BC written
+    in RUP, gradients and limiters of the RUP variables, faces reconstructed in
+    them (HigherOrderReconstructQ.cpp:21-72), residual and time step."""
+    m, cfg, R = _mpf.rup_case(cfg, face_bc)
+    ref = _mpf.mpf_pass_rup(m, cfg, R)
+    o = _restatement_pass(m, cfg, R)
+    assert _mpf.rel(o["state"][:, m.nnode:], ref["state"][:, m.nnode:]) <= 1e-13
+    assert relerr_rows(o["conv"], ref["conv"]) <= 1e-12
+    assert relerr_rows(o["diss"], ref["diss"]) <= 1e-12
+    assert _mpf.rel(o["deltat"], ref["deltat"]) <= 1e-13
+    assert _mpf.rel(o["extrema"], ref["extrema"]) <= 1e-13
+
+
+@pytest.mark.parametrize("name,cfg", _mpf.RUP_EDGE_CASES, ids=[c[0] for c in _mpf.RUP_EDGE_CASES])
+def test_rup_edge_loop_matches_mpflow3d_on_its_ghost_states(mpf_available, name, cfg):
+    """Roe (MPFLOW3D's matrix form as written, ``mpf_form=1``), HLLC and
+    Thornber (velocities blended at fixed rho and p) on RUP states, first and
+    second order, from MPFLOW3D's own post-BC state."""
+    m, cfg, R = _mpf.rup_case(cfg)
+    ref = _mpf.mpf_pass_rup(m, cfg, R)
+    o = _restatement_pass(m, dict(cfg, mpf_form=1), ref["state"], apply_bc=False)
+    assert relerr_rows(o["conv"], ref["conv"]) <= 1e-12
+    assert relerr_rows(o["diss"], ref["diss"]) <= 1e-12
+    assert _mpf.rel(o["deltat"], ref["deltat"]) <= 1e-13
+    if cfg["flux_scheme"] != 1:
+        assert _mpf.rel(o["extrema"], ref["extrema"]) <= 1e-13
+
+
+@pytest.mark.parametrize("name,cfg", _mpf.RUP_JAC_CASES, ids=[c[0] for c in _mpf.RUP_JAC_CASES])
+def test_rup_jacobian_matches_mpflow3d(mpf_available, name, cfg):
+    """MPFLOW3D's whole implicit system in (rho, u, v, w, p) columns: the
+    convective blocks dF/dW at the nodes (CompressibleUtils.cpp:85-186), the
+    dissipation Mop |A| at the Roe state (Roe_Fluxes.cpp:3009-3203, its
+    w-momentum entry as written, ``mpf_form=1``; Turkel family :3440-3810), the
+    pseudo-time term (V/dt) Mop [Kinv] (Roe_Jacobian.cpp:241-264) and
+    B = -(Res_Conv + Res_Diss), from MPFLOW3D's post-BC state."""
+    m, cfg, R = _mpf.rup_case(cfg)
+    Rb, A, B = _mpf.mpf_jacobian_rup(m, cfg, R)
+    s = restatement.Session(m, dict(cfg, mpf_form=1))
+    grad = phi = None
+    if cfg.get("order", 0) == 1:
+        grad = s.gradient(Rb, cfg.get("gradient", 0))
+        phi = s.limiter(Rb, grad)
+    conv, diss, dts, _ = s.residual(Rb, grad, phi)
+    dt, _ = s.deltat(dts)
+    A1, B1 = s.jacobian(Rb, dt, conv, diss, add_time=1, include_diss=1)
+    assert _mpf.rel(A1, A) <= 1e-12
+    assert _mpf.rel(B1, B) <= 1e-12
