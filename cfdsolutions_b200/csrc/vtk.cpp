@@ -102,6 +102,20 @@ extern "C" int cfd_vtk_write(const char *path, int nnode, const double *coords, 
     }
     const double g = p->gamma, pinf = p->pinf, R = 1.0 / g;
     const double *Q1 = Q, *Q2 = Q + ld, *Q3 = Q + 2 * ld, *Q4 = Q + 3 * ld, *Q5 = Q + 4 * ld;
+    // a (rho, u, v, w, p) state (CFD_VARS_RUP) is written through its conservative form
+    std::vector<double> qc;
+    if (p->variables == CFD_VARS_RUP) {
+        qc.resize((size_t)5 * nnode);
+        for (int i = 0; i < nnode; i++) {
+            const double r = Q1[i], u = Q2[i], v = Q3[i], w = Q4[i];
+            qc[i] = r;
+            qc[(size_t)nnode + i] = r * u;
+            qc[(size_t)2 * nnode + i] = r * v;
+            qc[(size_t)3 * nnode + i] = r * w;
+            qc[(size_t)4 * nnode + i] = (Q5[i] + g * pinf) / (g - 1.0) + 0.5 * r * (u * u + v * v + w * w);
+        }
+        Q1 = qc.data(); Q2 = Q1 + nnode; Q3 = Q2 + nnode; Q4 = Q3 + nnode; Q5 = Q4 + nnode;
+    }
     std::fprintf(fp, "# vtk DataFile Version 2.0\n");
     std::fprintf(fp, "Solver solution data\n");
     std::fprintf(fp, "ASCII \n");

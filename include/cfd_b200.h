@@ -596,7 +596,8 @@ int  cfd_server_destroy(cfd_server *srv);
  * pressure, temperature, Mach number, velocity vector of the nnode physical
  * nodes of Q, SoA [5][ld]).  Byte-identical to the reference's file for the
  * same mesh and state with pinf = 0 (derived fields in its operation order);
- * with pinf > 0 pressure, temperature and Mach follow the stiffened gas. */
+ * with pinf > 0 pressure, temperature and Mach follow the stiffened gas.  Q is
+ * in p->variables (a RUP state is written through its conservative form). */
 int  cfd_vtk_write(const char *path, int nnode, const double *coords, int64_t ntri, const int *tris,
                    const int *tri_tag, int64_t ntet, const int *tets, const cfd_params *p, const double *Q,
                    int64_t ld);

@@ -59,3 +59,20 @@ def test_vtk_stiffened_gas_fields(tmp_path):
     np.testing.assert_allclose(field("Pressure"), 1.0, rtol=0, atol=1e-10)
     np.testing.assert_allclose(field("Temperature"), 6001.0 * 4.4, rtol=1e-12)
     np.testing.assert_allclose(field("Mach"), 0.0062, rtol=1e-12)
+
+
+def test_vtk_rup_state_writes_the_conservative_file(tmp_path):
+    """A (rho, u, v, w, p) state with variables = CFD_VARS_RUP gives the file
+    of the same state in conservative variables (fields to print precision)."""
+    from cfdsolutions_b200 import to_rup
+    from cfdsolutions_b200.mesh import perturbed_freestream
+    m = box_mesh(3, jitter=0.1, seed=1, with_cells=True)
+    Q = perturbed_freestream(m, 1.4, 0.5, 2.0, noise=0.02, seed=4)
+    write_vtk(m, tmp_path / "c.vtk", default_params(), Q)
+    write_vtk(m, tmp_path / "r.vtk", default_params(variables=1), to_rup(Q, 1.4))
+    a = (tmp_path / "c.vtk").read_text().splitlines()
+    b = (tmp_path / "r.vtk").read_text().splitlines()
+    assert len(a) == len(b)
+    for x, y in zip(a, b):
+        if x != y:
+            np.testing.assert_allclose([float(t) for t in y.split()], [float(t) for t in x.split()], rtol=1e-13)
