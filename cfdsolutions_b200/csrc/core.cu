@@ -134,8 +134,8 @@ __device__ __forceinline__ void reconstruct(const double qs[5], const double qo[
     nnode, ldq, Q, grad, phi, xyz, sell_ptr, sell_nbr, sell_geo, deg, f, add_time, checks, roeflag, fixcount, res, resd, \
         dtsum, lgrad
 
-template <int FLUX, bool SECOND, bool KAPPA0, bool LG = false>
-__device__ __forceinline__ void residual_gather_node(int i, GATHER_PARAMS, double mn[3], double mx[3]) {
+template <int FLUX, bool SECOND, bool KAPPA0, bool LG, bool RUP>
+__device__ __forceinline__ void residual_gather_node_v(int i, GATHER_PARAMS, double mn[3], double mx[3]) {
     {
         const bool limited = f.limiter != CFD_LIMITER_NONE;
         double qo[5], go[15], po[5], xo[3];
@@ -194,7 +194,7 @@ __device__ __forceinline__ void residual_gather_node(int i, GATHER_PARAMS, doubl
                 }
                 // the limiter's reconstructed-pressure correction (Limiters.cpp:273-304)
                 // tests exactly this node's own face states
-                if ((checks & 2) && recon_pressure_negative(fo, f)) bad |= 2;
+                if ((checks & 2) && recon_pressure_negative<RUP ? 1 : 0>(fo, f)) bad |= 2;
             } else {
 #pragma unroll
                 for (int v = 0; v < 5; v++) { fo[v] = qo[v]; fn[v] = qn[v]; }
@@ -205,10 +205,10 @@ __device__ __forceinline__ void residual_gather_node(int i, GATHER_PARAMS, doubl
                 qL[v] = own_is_L ? fo[v] : fn[v];
                 qR[v] = own_is_L ? fn[v] : fo[v];
             }
-            if (SECOND && !roe_c2_of<FLUX>() && (checks & 1) && roe_avg_pressure(qL, qR, f) < 0.0)
+            if (SECOND && !roe_c2_of<FLUX>() && (checks & 1) && roe_avg_pressure<RUP ? 1 : 0>(qL, qR, f) < 0.0)
                 bad |= 1;
             double cf[5], df[5], lam[3], c2 = 1.0;
-            const double lmax = edge_flux<FLUX>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam,
+            const double lmax = edge_flux<FLUX, RUP ? 1 : 0>(qL, qR, g.x, g.y, g.z, g.w, f, cf, df, lam,
                                                 SECOND && roe_c2_of<FLUX>() ? &c2 : nullptr);
             if (SECOND && roe_c2_of<FLUX>() && (checks & 1) && c2 < 0.0) bad |= 1;
             const double sg = own_is_L ? 1.0 : -1.0;
@@ -235,27 +235,35 @@ __device__ __forceinline__ void residual_gather_node(int i, GATHER_PARAMS, doubl
     }
 }
 
-template <int FLUX, bool SECOND, bool KAPPA0 = false, bool LG = false>
+// The variable set is a compile-time constant of each kernel (RUP; every
+// launch passes a Flow whose rup matches): the conservative kernels hold no
+// reference to f.rup and carry no RUP branches.
+template <int FLUX, bool SECOND, bool KAPPA0, bool LG = false, bool RUP = false>
+__device__ __forceinline__ void residual_gather_node(int i, GATHER_PARAMS, double mn[3], double mx[3]) {
+    residual_gather_node_v<FLUX, SECOND, KAPPA0, LG, RUP>(i, GATHER_ARGS, mn, mx);
+}
+
+template <int FLUX, bool SECOND, bool KAPPA0 = false, bool LG = false, bool RUP = false>
 // Nodes [lo, hi) (lo a multiple of the block size; the whole mesh is 0, nnode).
 __global__ void __launch_bounds__(128, 3) k_residual_gather(GATHER_PARAMS, unsigned long long *__restrict__ ext,
                                                             int lo, int hi) {
     const int i = lo + blockIdx.x * blockDim.x + threadIdx.x;
     double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
-    if (i < hi) residual_gather_node<FLUX, SECOND, KAPPA0, LG>(i, GATHER_ARGS, mn, mx);
+    if (i < hi) residual_gather_node<FLUX, SECOND, KAPPA0, LG, RUP>(i, GATHER_ARGS, mn, mx);
     if (add_time) block_extrema3(mn, mx, ext);
 }
 
 // The gated re-evaluation after a limiter fix (gate = the fix counters): a
 // grid of a few CTAs per SM strides over the nodes, so that the usual case,
 // no node failed, costs one short wave instead of the full grid's.
-template <int FLUX, bool SECOND, bool KAPPA0 = false>
+template <int FLUX, bool SECOND, bool KAPPA0 = false, bool RUP = false>
 __global__ void __launch_bounds__(128, 3) k_residual_gather_rerun(GATHER_PARAMS, const int *__restrict__ gate,
                                                                   unsigned long long *__restrict__ ext) {
     if (gate[0] == 0 && gate[1] == 0) return;
     double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {0.0, 0.0, 0.0};
     for (int b = blockIdx.x * blockDim.x; b < nnode; b += gridDim.x * blockDim.x) {
         const int i = b + threadIdx.x;
-        if (i < nnode) residual_gather_node<FLUX, SECOND, KAPPA0>(i, GATHER_ARGS, mn, mx);
+        if (i < nnode) residual_gather_node<FLUX, SECOND, KAPPA0, false, RUP>(i, GATHER_ARGS, mn, mx);
     }
     if (add_time) block_extrema3(mn, mx, ext);
 }
@@ -264,8 +272,9 @@ __global__ void __launch_bounds__(128, 3) k_residual_gather_rerun(GATHER_PARAMS,
 // block b belongs to the job whose [block_begin, block_begin + ceil(nnode/128))
 // range holds it, and its threads run exactly the per-node code of
 // k_residual_gather on that job's arrays and parameters, so every node's
-// residual is bit-identical to the job's own launch.  The serving loop uses it
-// to fuse the interior residuals of the requests it runs side by side.
+// residual is the job's own launch's to round-off.  The serving loop uses it
+// to fuse the interior residuals of the requests it runs side by side
+// (conservative states only; RUP requests launch on their own).
 template <int FLUX, bool SECOND, bool KAPPA0, bool LG>
 __global__ void __launch_bounds__(128, 3) k_residual_gather_batch(const __grid_constant__ GatherBatch B) {
     int j = 0;
@@ -1085,26 +1094,34 @@ static int launch_residual(cfd_ctx *c, int add_time, bool check_roe, bool check_
         // Green-Gauss + limiter pass (first pass only: a gated re-evaluation
         // follows limiter fixes, which change phi)
         const bool lgk = k0 && !gate && c->lgrad_valid && c->params.limiter != CFD_LIMITER_NONE;
+        const bool rup = c->flow.rup != 0;
 #define GATHER_LAUNCH_ARGS                                                                                          \
     c->nnode, c->ldq, c->Q.p, c->grad.p, c->phi.p, c->xyz.p, c->sell_ptr.p, c->sell_nbr.p, c->sell_geo.p, c->deg.p, \
         c->flow, add_time, checks, c->roeflag.p, c->fixcount.p, c->res.p, c->resd.p, c->dt.p, c->lgrad.p
-        const int key = batch_key(FLUX, SECOND, k0, lgk);
+        const int key = c->flow.rup ? -1 : batch_key(FLUX, SECOND, k0, lgk);
         if (!gate && c->batcher && key >= 0) {
-            // the serving loop fuses this launch with other requests' (bit-identical per node)
+            // the serving loop fuses this launch with other requests' (same per-node code)
             GatherJob job{c->nnode, c->ldq, c->Q.p, c->grad.p, c->phi.p, c->xyz.p, c->sell_ptr.p, c->sell_nbr.p,
                           c->sell_geo.p, c->deg.p, c->flow, add_time, checks, c->roeflag.p, c->fixcount.p,
                           c->res.p, c->resd.p, c->dt.p, lgk ? c->lgrad.p : nullptr, ext, 0};
             const int st = c->batch_submit(c->batcher, c, key, &job);
             if (st) return st;
         } else if (lgk) {
-            k_residual_gather<FLUX, SECOND, SECOND, true>
-                <<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, ext, 0, c->nnode);
+            auto kern = rup ? k_residual_gather<FLUX, SECOND, SECOND, true, true>
+                            : k_residual_gather<FLUX, SECOND, SECOND, true, false>;
+            kern<<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, ext, 0, c->nnode);
         } else if (gate) {
-            auto kern = k0 ? k_residual_gather_rerun<FLUX, SECOND, SECOND> : k_residual_gather_rerun<FLUX, SECOND, false>;
+            auto kern = rup ? (k0 ? k_residual_gather_rerun<FLUX, SECOND, SECOND, true>
+                                  : k_residual_gather_rerun<FLUX, SECOND, false, true>)
+                            : (k0 ? k_residual_gather_rerun<FLUX, SECOND, SECOND, false>
+                                  : k_residual_gather_rerun<FLUX, SECOND, false, false>);
             const int grid = std::min(grid_for(c->nnode, 128), 3 * c->nsm);
             kern<<<grid, 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, gate, ext);
         } else {
-            auto kern = k0 ? k_residual_gather<FLUX, SECOND, SECOND> : k_residual_gather<FLUX, SECOND, false>;
+            auto kern = rup ? (k0 ? k_residual_gather<FLUX, SECOND, SECOND, false, true>
+                                  : k_residual_gather<FLUX, SECOND, false, false, true>)
+                            : (k0 ? k_residual_gather<FLUX, SECOND, SECOND, false, false>
+                                  : k_residual_gather<FLUX, SECOND, false, false, false>);
             kern<<<grid_for(c->nnode, 128), 128, 0, c->stream>>>(GATHER_LAUNCH_ARGS, ext, 0, c->nnode);
         }
 #undef GATHER_LAUNCH_ARGS
@@ -1438,7 +1455,10 @@ static int residual_step_pipelined_flux(cfd_ctx *c, int iteration, const double 
             if ((st = gg_limiter_range(c, c->phi.p, P.lo[g], P.lo[g + 1]))) return st;
         }
         const int lo = P.lo[k], hi = P.lo[k + 1];
-        auto kern = kappa0 ? k_residual_gather<FLUX, true, true, true> : k_residual_gather<FLUX, true, false, false>;
+        auto kern = c->flow.rup ? (kappa0 ? k_residual_gather<FLUX, true, true, true, true>
+                                          : k_residual_gather<FLUX, true, false, false, true>)
+                                : (kappa0 ? k_residual_gather<FLUX, true, true, true, false>
+                                          : k_residual_gather<FLUX, true, false, false, false>);
         kern<<<grid_for(hi - lo, 128), 128, 0, c->stream>>>(
             n, c->ldq, c->Q.p, c->grad.p, c->phi.p, c->xyz.p, c->sell_ptr.p, c->sell_nbr.p, c->sell_geo.p, c->deg.p,
             c->flow, 1, checks, c->roeflag.p, c->fixcount.p, c->res.p, c->resd.p, c->dt.p, c->lgrad.p,

@@ -14,12 +14,13 @@ namespace cfd {
 // wave speeds SL = min(ubar_L - c_L, ubar - c), SR = max(ubar_R + c_R, ubar + c),
 // contact speed SM, star states.  The whole flux goes to the convective
 // residual (Compute_Residual_HLLC, :519-573); the dissipative part is zero.
+template <int V = -1>
 __device__ __forceinline__ double hllc_flux(const double qL[5], const double qR[5], double nx, double ny, double nz,
                                             double area, const Flow &f, double conv[5], double diss[5],
                                             double lam[3]) {
     Face L, R;
-    eos_face(qL, nx, ny, nz, f, true, L);
-    eos_face(qR, nx, ny, nz, f, true, R);
+    eos_face<V>(qL, nx, ny, nz, f, true, L);
+    eos_face<V>(qR, nx, ny, nz, f, true, R);
     const double rho = sqrt(R.rho * L.rho);
     const double sigma = rho / (L.rho + rho);
     const double u = L.u + sigma * (R.u - L.u);
@@ -80,12 +81,13 @@ __device__ __forceinline__ double hllc_flux(const double qL[5], const double qR[
 // are empty stubs (Euler3D/src/AUSM_Fluxes.cpp:45-54), so this follows the
 // published method.  The dissipative residual is zero; the time-step spectral
 // radius is the Roe-averaged |ubar| + c, as for HLLC.
+template <int V = -1>
 __device__ __forceinline__ double ausmp_flux(const double qL[5], const double qR[5], double nx, double ny,
                                              double nz, double area, const Flow &f, double conv[5], double diss[5],
                                              double lam[3]) {
     Face L, R;
-    eos_face(qL, nx, ny, nz, f, false, L);
-    eos_face(qR, nx, ny, nz, f, false, R);
+    eos_face<V>(qL, nx, ny, nz, f, false, L);
+    eos_face<V>(qR, nx, ny, nz, f, false, R);
     const double k = 2.0 * f.gm1 / (f.gamma + 1.0);
     const double csL = sqrt(k * L.ht), csR = sqrt(k * R.ht);
     const double chL = csL * csL / fmax(csL, L.ubar);
@@ -136,12 +138,13 @@ __device__ __forceinline__ double ausmp_flux(const double qL[5], const double qR
 // F+ of the left state and F- of the right state by the face-normal Mach
 // number, the full flux beyond |M| = 1; no dissipative part; the time-step
 // eigenvalue from the arithmetic means (c of the mean rho and p).  Ideal gas.
+template <int V = -1>
 __device__ __forceinline__ double vanleer_flux(const double qL[5], const double qR[5], double nx, double ny,
                                                double nz, double area, const Flow &f, double conv[5],
                                                double diss[5], double lam[3]) {
     Face L, R;
-    eos_face(qL, nx, ny, nz, f, true, L);
-    eos_face(qR, nx, ny, nz, f, true, R);
+    eos_face<V>(qL, nx, ny, nz, f, true, L);
+    eos_face<V>(qR, nx, ny, nz, f, true, R);
     const double g = f.gamma, gg = g * g - 1.0;
     const double rho_a = 0.5 * (L.rho + R.rho);
     const double ub_a = 0.5 * ((L.u + R.u) * nx + (L.v + R.v) * ny + (L.w + R.w) * nz);
@@ -208,20 +211,20 @@ __device__ __forceinline__ double vanleer_flux(const double qL[5], const double 
 template <int FLUX>
 __host__ __device__ constexpr bool roe_c2_of() { return FLUX == CFD_FLUX_ROE || FLUX == CFD_FLUX_ROE_LMFIX; }
 
-template <int FLUX>
+template <int FLUX, int V = -1>
 __device__ __forceinline__ double edge_flux(const double qL[5], const double qR[5], double nx, double ny, double nz,
                                             double area, const Flow &f, double conv[5], double diss[5],
                                             double lam[3], double *roe_c2 = nullptr) {
-    if (FLUX == CFD_FLUX_HLLC) return hllc_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
-    if (FLUX == CFD_FLUX_AUSM) return ausmp_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
-    if (FLUX == CFD_FLUX_VANLEER) return vanleer_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
-    if (FLUX == CFD_FLUX_ROE_PRECOND) return roe_precond_flux(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
+    if (FLUX == CFD_FLUX_HLLC) return hllc_flux<V>(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
+    if (FLUX == CFD_FLUX_AUSM) return ausmp_flux<V>(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
+    if (FLUX == CFD_FLUX_VANLEER) return vanleer_flux<V>(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
+    if (FLUX == CFD_FLUX_ROE_PRECOND) return roe_precond_flux<V>(qL, qR, nx, ny, nz, area, f, conv, diss, lam);
     if (FLUX == CFD_FLUX_ROE_THORNBER) {
         double mL[5], mR[5];
-        thornber_states(qL, qR, f, mL, mR);
-        return roe_flux<false>(mL, mR, nx, ny, nz, area, f, conv, diss, lam);
+        thornber_states<V>(qL, qR, f, mL, mR);
+        return roe_flux<false, V>(mL, mR, nx, ny, nz, area, f, conv, diss, lam);
     }
-    return roe_flux<FLUX == CFD_FLUX_ROE_LMFIX>(qL, qR, nx, ny, nz, area, f, conv, diss, lam, roe_c2);
+    return roe_flux<FLUX == CFD_FLUX_ROE_LMFIX, V>(qL, qR, nx, ny, nz, area, f, conv, diss, lam, roe_c2);
 }
 
 // The Roe family (plain, low-Mach fix, preconditioned): the limiter pressure fix applies.
@@ -249,8 +252,9 @@ __device__ __forceinline__ double roe_avg_pressure_rup(const double qa[5], const
     return f.gm1 * rho * (ht - 0.5 * (u * u + v * v + w * w)) / f.gamma;
 }
 
+template <int V = -1>
 __device__ __forceinline__ double roe_avg_pressure(const double qa[5], const double qb[5], const Flow &f) {
-    if (f.rup) return roe_avg_pressure_rup(qa, qb, f);
+    if (vars_rup<V>(f)) return roe_avg_pressure_rup(qa, qb, f);
     const double g = f.gamma, gpinf = f.gpinf;
     const double ra = qa[0], rb = qb[0];
     const double ia = 1.0 / ra, ib = 1.0 / rb;
@@ -270,8 +274,9 @@ __device__ __forceinline__ double roe_avg_pressure(const double qa[5], const dou
 // Reconstructed-pressure test of Compute_Limiter_PressureCorrection
 // (Euler3D/src/Limiters.cpp:296-301): p < 0, without the division when rho > 0
 // (p + pinf < 0 for the stiffened gas).
+template <int V = -1>
 __device__ __forceinline__ bool recon_pressure_negative(const double q[5], const Flow &f) {
-    if (f.rup) return q[4] + f.pinf < 0.0;  // Material_Get_Pressure of a RUP state (Limiters.cpp:296-297)
+    if (vars_rup<V>(f)) return q[4] + f.pinf < 0.0;  // Material_Get_Pressure of a RUP state (Limiters.cpp:296-297)
     const double m2 = q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
     return q[0] > 0.0 ? (2.0 * q[0] * (q[4] - f.pinf) < m2) : (f.gm1 * ((q[4] - f.pinf) - (0.5 / q[0]) * m2) < 0.0);
 }

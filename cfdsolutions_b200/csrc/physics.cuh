@@ -42,6 +42,14 @@ struct Face {
     double rho, u, v, w, p, ht, ubar, c;
 };
 
+// Whether the state holds (rho, u, v, w, p): V = 0 (conservative) or 1 (RUP)
+// as a compile-time constant of the caller, or V = -1, read from f.rup.
+template <int V>
+__device__ __forceinline__ bool vars_rup(const Flow &f) {
+    if constexpr (V < 0) return f.rup != 0;
+    else return V == 1;
+}
+
 // Compute_EOS_Variables_Face, conservative branch (Euler3D/src/Material.cpp:216-248),
 // with the stiffened-gas terms: p = (gamma - 1)(rho et - rho q^2 / 2) - gamma pinf and
 // c^2 = gamma (p + pinf) / rho.  At pinf = 0 both added terms are exact zeros, so
@@ -49,11 +57,12 @@ struct Face {
 // RUP states (MPFLOW3D Material_Get_Properties, VARIABLE_RUP branch,
 // MPFLOW3D/src/Material.cpp:591-599) take rho, u, v, w, p as stored and
 // ht = gamma (p + pinf) / ((gamma - 1) rho) + q^2 / 2.
+template <int V = -1>
 __device__ __forceinline__ void eos_face(const double q[5], double nx, double ny, double nz, const Flow &f,
                                          bool want_c, Face &s) {
     s.rho = q[0];
     const double ri = 1.0 / s.rho;
-    if (f.rup) {
+    if (vars_rup<V>(f)) {
         s.u = q[1];
         s.v = q[2];
         s.w = q[3];
@@ -123,14 +132,14 @@ __device__ __forceinline__ void roe_entropy_fix(double ubar_L, double c_L, doubl
 // Returns the largest |eigenvalue| (for the time step) and the three
 // eigenvalue magnitudes |ubar|, |ubar+c|, |ubar-c| in lam[3].
 // c2_out, when not null, receives the Roe-averaged c^2 (see edge_flux).
-template <bool LMFIX>
+template <bool LMFIX, int V = -1>
 __device__ __forceinline__ double roe_flux(const double qL[5], const double qR[5], double nx, double ny,
                                            double nz, double area, const Flow &f, double conv[5],
                                            double diss[5], double lam[3], double *c2_out = nullptr) {
     Face L, R;
     const bool want_c = f.entropy_fix != 0;
-    eos_face(qL, nx, ny, nz, f, want_c, L);
-    eos_face(qR, nx, ny, nz, f, want_c, R);
+    eos_face<V>(qL, nx, ny, nz, f, want_c, L);
+    eos_face<V>(qR, nx, ny, nz, f, want_c, R);
 
     const double mL = L.rho * L.ubar, mR = R.rho * R.ubar;
     const double ha = 0.5 * area;
@@ -425,11 +434,12 @@ __device__ __forceinline__ void roe_abs_jacobian(const double qL[5], const doubl
 // kinetic energy.  With RUP states the velocities are blended at fixed
 // density and pressure (Roe_Fluxes.cpp:1161-1168).  The Roe flux is then
 // formed from the modified states.
+template <int V = -1>
 __device__ __forceinline__ void thornber_states(const double qL[5], const double qR[5], const Flow &f,
                                                 double mL[5], double mR[5]) {
     Face L, R;
-    eos_face(qL, 1.0, 0.0, 0.0, f, true, L);
-    eos_face(qR, 1.0, 0.0, 0.0, f, true, R);
+    eos_face<V>(qL, 1.0, 0.0, 0.0, f, true, L);
+    eos_face<V>(qR, 1.0, 0.0, 0.0, f, true, R);
     const double ml = sqrt(L.u * L.u + L.v * L.v + L.w * L.w) / L.c;
     const double mr = sqrt(R.u * R.u + R.v * R.v + R.w * R.w) / R.c;
     const double z = fmin(1.0, fmax(ml, mr));
@@ -437,7 +447,7 @@ __device__ __forceinline__ void thornber_states(const double qL[5], const double
     mR[0] = qR[0];
     mL[4] = qL[4];
     mR[4] = qR[4];
-    if (f.rup) {
+    if (vars_rup<V>(f)) {
 #pragma unroll
         for (int i = 1; i < 4; i++) {
             mL[i] = 0.5 * ((1.0 + z) * qL[i] + (1.0 - z) * qR[i]);
@@ -545,12 +555,13 @@ __device__ __forceinline__ void pc_left_row(int k, const PcSys &S, double nx, do
 // out = Mop Kinv R |Lambda| L Mpr dQ at the system's averaged state, with
 // Mpr = d(rho,u,v,w,p)/dQ and Mop its inverse (the same for either gas);
 // Mpr = I when dQ is already a (rho,u,v,w,p) difference (RUP states).
+template <int V = -1>
 __device__ __forceinline__ void pc_dissipation(const PcSys &S, double nx, double ny, double nz, const Flow &f,
                                                const double dQ[5], double out[5]) {
     const double rho = S.rho, u = S.u, v = S.v, w = S.w, ri = 1.0 / rho;
     const double q2 = u * u + v * v + w * w;
     double dq[5];
-    if (f.rup) {
+    if (vars_rup<V>(f)) {
 #pragma unroll
         for (int k = 0; k < 5; k++) dq[k] = dQ[k];
     } else {
@@ -614,12 +625,13 @@ __device__ __forceinline__ void pc_edge_system(const Face &L, const Face &R, dou
 
 // Preconditioned Roe flux: central part as Roe, dissipation -1/2 |A|_p dQ area;
 // returns the spectral radius of K A (time step), lam = |u.n|, |ubp+cp|, |ubp-cp|.
+template <int V = -1>
 __device__ __forceinline__ double roe_precond_flux(const double qL[5], const double qR[5], double nx, double ny,
                                                    double nz, double area, const Flow &f, double conv[5],
                                                    double diss[5], double lam[3]) {
     Face L, R;
-    eos_face(qL, nx, ny, nz, f, true, L);
-    eos_face(qR, nx, ny, nz, f, true, R);
+    eos_face<V>(qL, nx, ny, nz, f, true, L);
+    eos_face<V>(qR, nx, ny, nz, f, true, R);
     const double mL = L.rho * L.ubar, mR = R.rho * R.ubar;
     const double ha = 0.5 * area;
     conv[0] = ha * (mL + mR);
@@ -632,7 +644,7 @@ __device__ __forceinline__ double roe_precond_flux(const double qL[5], const dou
     double dQ[5], d[5];
 #pragma unroll
     for (int k = 0; k < 5; k++) dQ[k] = qR[k] - qL[k];
-    pc_dissipation(S, nx, ny, nz, f, dQ, d);
+    pc_dissipation<V>(S, nx, ny, nz, f, dQ, d);
 #pragma unroll
     for (int k = 0; k < 5; k++) diss[k] = -ha * d[k];
     lam[0] = S.lam0;

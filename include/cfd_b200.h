@@ -579,8 +579,9 @@ int  cfd_server_stats(cfd_server *srv, double out[5]);
  * in its solve are handed to a batcher, which launches the jobs of one kernel
  * that are waiting when as many jobs as requests in their solves have
  * arrived, or window_us after the first, as one kernel over a request table
- * (k_residual_gather_batch, k_bspmv_batch); each request's results are the
- * same bit for bit either way.  Set before the first submit.  batch_stats:
+ * (k_residual_gather_batch, k_bspmv_batch; conservative-variable requests);
+ * each request's results agree either way to round-off, with the same
+ * iteration counts.  Set before the first submit.  batch_stats:
  * {fused residual launches, residual jobs in them, fused SpMV launches, SpMV
  * jobs in them}. */
 int  cfd_server_set_batching(cfd_server *srv, int enable, double window_us);

@@ -88,8 +88,11 @@ def test_admission_keeps_reserved_memory_within_the_budget(gpu_available):
 def test_fused_launches_change_nothing(gpu_available):
     """With the requests' interior residuals and GMRES SpMVs fused into
     launches over a request table (a wide window, so that several requests
-    share launches) every served state is bit-identical to the unfused
-    server's."""
+    share launches) every request takes the same implicit and GMRES
+    iterations as in the unfused server and ends in the same state to
+    round-off: 1e-13 absolute on fields of size 1 (the fused and the
+    request's own kernel run the same per-node code, but the compiler may
+    contract a multiply-add differently in each)."""
     reqs = _requests()
     fused, s_fused, st = _run(reqs, workers=6, window_us=500.0)
     plain, s_plain, st0 = _run(reqs, workers=6, batching=False)
@@ -98,7 +101,7 @@ def test_fused_launches_change_nothing(gpu_available):
         assert st0[kind]["jobs"] == 0
     for a, b, sa, sb in zip(fused, plain, s_fused, s_plain):
         assert a.iterations == b.iterations and a.linear_iterations == b.linear_iterations
-        np.testing.assert_array_equal(sa, sb)
+        np.testing.assert_allclose(sa, sb, rtol=0, atol=1e-13)
 
 
 def test_autotuner_picks_a_measured_schedule(gpu_available):
@@ -126,11 +129,12 @@ def test_autotuner_picks_a_measured_schedule(gpu_available):
 def test_fused_launches_keep_precisions_apart(gpu_available):
     """Requests with FP32 and BF16 Jacobians in one server: their SpMVs are
     fused only with jobs of the same storage type (one kernel instantiation per
-    launch), and every served state is bit-identical to the unfused server's."""
+    launch), and every request takes the unfused server's iterations and ends
+    in its state to round-off (1e-13 absolute, as above)."""
     reqs = _requests()[:3] + _requests(capi.PREC_BF16 | capi.PREC_LOW_ONLY)[3:]
     fused, s_fused, st = _run(reqs, workers=6, window_us=500.0)
     plain, s_plain, _ = _run(reqs, workers=6, batching=False)
     assert st["spmv"]["jobs"] > st["spmv"]["launches"] > 0
     for a, b, sa, sb in zip(fused, plain, s_fused, s_plain):
         assert a.iterations == b.iterations and a.linear_iterations == b.linear_iterations
-        np.testing.assert_array_equal(sa, sb)
+        np.testing.assert_allclose(sa, sb, rtol=0, atol=1e-13)
