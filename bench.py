@@ -341,13 +341,16 @@ def lowmach_solves(dev, stream, timed_once):
     """Config of the low-Mach liquid channel: time to the residual drop, plain
     FP64 and FP32 Jacobian/ILU(0); the converged states (continued untimed at
     the final CFL to the round-off floor of the stiffened EOS) compared."""
-    from cfdsolutions_b200 import Euler3DGPU, capi, default_params
+    from cfdsolutions_b200 import Euler3DGPU, capi, default_params, to_rup
 
     m, Q = lowmach_case(LOWMACH_MESH)
     out, states = {"config": lowmach_config(m)}, {}
-    for name, prec in (("fp64", capi.PREC_FP64), ("fp32", capi.PREC_FP32 | capi.PREC_LOW_ONLY)):
-        with Euler3DGPU(m, default_params(**LOWMACH), device=dev, stream=stream.cuda_stream) as ss:
-            ss.set_state(Q)
+    # fp64_rup: the FP64 solve with the state stored as (rho, u, v, w, p) (MPFLOW3D's VARIABLE_RUP)
+    for name, prec, variables in (("fp64", capi.PREC_FP64, 0), ("fp32", capi.PREC_FP32 | capi.PREC_LOW_ONLY, 0),
+                                  ("fp64_rup", capi.PREC_FP64, 1)):
+        cfg = dict(LOWMACH, variables=variables)
+        with Euler3DGPU(m, default_params(**cfg), device=dev, stream=stream.cuda_stream) as ss:
+            ss.set_state(Q if variables == 0 else to_rup(Q, LOWMACH["gamma"], LOWMACH["pinf"]))
             capi.check(capi.lib.cfd_ilu_mc_order(ss.handle, None, None), "cfd_ilu_mc_order")
             g = capi.GmresOpts(30, 30, STEADY_RTOL, capi.PC_ILU0_MC, prec, 1)
             box = {}
@@ -361,11 +364,12 @@ def lowmach_solves(dev, stream, timed_once):
             out[name] = {"seconds": ms / 1e3, "newton_iterations": st.iterations,
                          "gmres_iterations": st.linear_iterations, "rms_drop": st.rms_last / st.rms_first,
                          "converged": bool(st.rms_last <= STEADY_DROP * st.rms_first)}
-            ss.set_params(default_params(**dict(LOWMACH, cfl_min=LOWMACH["cfl_max"], cfl_ramp=0)))
+            ss.set_params(default_params(**dict(cfg, cfl_min=LOWMACH["cfl_max"], cfl_ramp=0)))
             st2 = ss.solve_steady(max_iterations=100, drop=1e-4, include_diss=1, linear_solver=1, gmres=g,
                                   precond_update=LOWMACH_PC_UPDATE)
             out[name]["rms_drop_compared"] = st2.rms_last / st.rms_first
-            states[name] = ss.get_state()[:, :m.nnode]
+            if variables == 0:
+                states[name] = ss.get_state()[:, :m.nnode]
     ref = states["fp64"]
     mom = float(np.abs(ref[1:4]).max())
     err = 0.0
@@ -374,6 +378,9 @@ def lowmach_solves(dev, stream, timed_once):
         err = max(err, float(np.abs(states["fp32"][v] - ref[v]).max()) / scale)
     out["fp32"]["max_rel_err_vs_fp64"] = err
     out["fp32"]["speedup_vs_fp64"] = out["fp64"]["seconds"] / out["fp32"]["seconds"]
+    out["fp64_rup"]["note"] = ("state stored as (rho, u, v, w, p): the pressure carries no gamma pinf "
+                               "cancellation, so rms_drop_compared (the continued solve) falls below the "
+                               "conservative floor")
     return m, out
 
 
