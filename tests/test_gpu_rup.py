@@ -189,3 +189,31 @@ def test_gpu_rup_stiffened_steady_solve_goes_below_the_conservative_floor(gpu_av
     (rho, u, v, w, p) the same solve goes on to a 1e-12 drop."""
     drop, its = _water_channel_drop(1, 1e-12)
     assert drop <= 1e-12, (drop, its)
+
+
+def test_gpu_rup_option_checks(gpu_available):
+    """variables other than CFD_VARS_CONSERVATIVE / CFD_VARS_RUP is
+    CFD_ERR_ARG; the finite-difference Jacobian and the physical-time driver,
+    written for conservative states, return CFD_ERR_UNSUPPORTED on a RUP
+    context and leave it usable."""
+    from cfdsolutions_b200 import capi, default_params
+    m, cfg, Q = _mpf.case(dict(_mpf.CFG1))
+    with Euler3DGPU(m, params_from(cfg)) as s:
+        with pytest.raises(capi.CfdError) as e:
+            s.set_params(default_params(**dict(cfg, variables=2)))
+        assert e.value.code == -1  # CFD_ERR_ARG
+        s.set_params(default_params(**dict(cfg, variables=1)))
+        s.set_state(to_rup(Q, cfg["gamma"]))
+        s.begin_iteration(0)
+        s.Apply_Boundary_Condition(0)
+        s.Compute_Residual(1)
+        s.Compute_DeltaT(0)
+        with pytest.raises(capi.CfdError) as e:
+            s.Compute_Jacobian_FiniteDifference(1, 0)
+        assert e.value.code == -8  # CFD_ERR_UNSUPPORTED
+        with pytest.raises(capi.CfdError) as e:
+            s.solve_unsteady(0.1, 1)
+        assert e.value.code == -8
+        s.Compute_Jacobian(1, 0, include_diss=1)
+        _, B, _ = s.get_system()
+        assert np.isfinite(B).all()
